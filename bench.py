@@ -1,0 +1,397 @@
+"""Benchmark of the neo-Hookean hot path on B200.
+
+Workload: the 64^3-cube five-tet box (274,625 vertices, 1,310,720 tets, 3,494,465 3x3
+blocks) with per-element mu log-uniform in [1e3, 1e5], nu ~ U[0.30, 0.45], bottom face
+fixed, gravity -9.8 z, density 1000 (seeded synthetic data).
+
+One step = one FP64 evaluation of energy + gradient + exact block-CSR Hessian of the whole
+mesh. `value` is tets/s over K device-timed steps with inputs resident in HBM; `e2e` is the
+same metric through the C ABI (lpg_fem_eval) with pinned HOST buffers, i.e. including the
+H2D copy of u and the D2H copy of the gradient and the Hessian (reference CSC order) every
+step. The Newton time-to-1e-8 (relative gradient norm, Armijo backtracking) of the mixed
+FP32/FP64 path and of the FP64 path is reported beside it.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--no-newton]
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "neo-Hookean tets/s (E+∇+BSR Hessian); Newton time-to-1e-8, mixed vs FP64"
+N_CUBES = 64
+
+
+def workload_config():
+    from litepgo_b200 import mesh
+
+    V, T, nnzb = mesh.box_counts(N_CUBES)
+    return {
+        "workload": f"gravity box {N_CUBES}^3 cubes x 5 tets (V={V}, T={T}, nnzb={nnzb}), per-element mu "
+                    "log-uniform [1e3,1e5], nu U[0.30,0.45], z=0 fixed, gravity -9.8, rho 1000, seed 0",
+        "step": "one FP64 E + gradient + exact 3x3 block-CSR Hessian evaluation of the whole mesh",
+        "state": "u = (A - I) X + 1e-3 N(0,1), A = I + 0.1 N(0,1) (seed 11)",
+        "l2": "working set per step ~412 MB (element records 126 MB, Hessian 252 MB) > 126 MB L2",
+        "tets": T, "vertices": V, "nnzb": nnzb,
+    }
+
+
+def state(X):
+    rng = np.random.default_rng(11)
+    A = np.eye(3) + 0.1 * rng.standard_normal((3, 3))
+    return (X @ A.T - X + 0.001 * rng.standard_normal(X.shape)).ravel()
+
+
+def algorithmic_bytes(T, V, nnzb, precision="f64"):
+    """Compulsory traffic of one E+grad+H evaluation: per tet indices, record (G, vol, theta),
+    per vertex u in and gradient out, 9 values per block out."""
+    if precision == "f64":
+        return T * (16 + 72 + 8 + 16) + V * (24 + 24) + 72 * nnzb
+    return T * (16 + 36 + 4 + 8) + V * (12 + 12) + 36 * nnzb
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", self.gpu, "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the assembly kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "assemble_f64_exact_64cube.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(X, tets, theta, u_full, seconds=12.0):
+    """The oracle (the reference's CPU algorithm restated in C++/OpenMP) on the host cores:
+    E + gradient + exact CSC Hessian, repeated for about `seconds` on the full mesh."""
+    import oracle
+
+    oracle.set_threads(0)
+    threads = oracle.get_threads()
+    m = oracle.OracleMesh(X, tets, theta)
+    m.eval(u_full, True, 1)  # cold call
+    n, t0 = 0, time.perf_counter()
+    while True:
+        m.eval(u_full, True, 1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 20:
+            break
+    return {"value": n * tets.shape[0] / el, "unit": "tets/s", "cores": threads, "kind": "port",
+            "sample": f"{n} full evaluations (E+grad+exact CSC Hessian) of the {tets.shape[0]}-tet mesh, "
+                      f"{el:.1f} s wall, OpenMP {threads} threads, median-free mean"}
+
+
+def dist_setup(n_gpus):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args):
+    rank, world, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    from litepgo_b200 import workloads
+
+    g = workloads.gravity_box(N_CUBES, seed=0)
+    u = state(g["X"])
+    import oracle
+
+    oracle.set_threads(0)
+    threads = oracle.get_threads()
+    m = oracle.OracleMesh(g["X"], g["tets"], g["theta"])
+    T = g["tets"].shape[0]
+    for _ in range(max(args.warmup, 0)):
+        m.eval(u, True, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        m.eval(u, True, 1)
+    el = time.perf_counter() - t0
+    value = args.steps * T / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": "tets/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full evaluations (E+grad+exact CSC Hessian) of the {T}-tet mesh "
+                                   f"by the C++/OpenMP restatement of the reference CPU path, {threads} threads"},
+        "e2e": {"value": value, "unit": "tets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference itself cannot be built here (Eigen 5 / oneTBB / nanobind fetched at configure time, "
+                "no network); this arm times its algorithm restated in oracle/",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def newton_times(fem_energy, g, torch):
+    """Newton to a 1e-8 relative gradient norm with Armijo backtracking: mixed vs FP64."""
+    from litepgo_b200 import dof, energy, solver
+
+    import scipy.sparse as sp
+
+    n = g["X"].size
+    load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -g["f"])
+    total = energy.WeightedSumEnergy([(fem_energy, 1.0), (load, 1.0)])
+    fixed = dof.DofReduction(n, g["fixed"])
+    out = {}
+    x0 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for prec in ("mixed", "f64"):
+        opts = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo",
+                                    precision=prec, max_iterations=100, cg_tolerance=1e-2, cg_max_iterations=20000)
+        t0 = time.perf_counter()
+        r = solver.newton_solve(total, fixed, x0, opts)
+        wall = time.perf_counter() - t0
+        out[prec] = {"status": r.status.name, "seconds": r.seconds, "wall_seconds": wall, "iterations": r.iterations,
+                     "cg_iterations": int(r.cg_iterations), "relative_gradient": r.gradient_norm / max(r.gradient_norm0, 1e-300),
+                     "line_search_evaluations": r.line_search_evaluations}
+        out[prec + "_x"] = r.x
+    xm, xf = out.pop("mixed_x"), out.pop("f64_x")
+    out["max_abs_diff_mixed_vs_f64"] = float((xm - xf).abs().max().item())
+    if out["mixed"]["seconds"] > 0:
+        out["speedup_mixed_vs_f64"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
+    return out
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    from litepgo_b200 import _native as N
+    from litepgo_b200 import energy, fem, workloads
+
+    g = workloads.gravity_box(N_CUBES, seed=0)
+    X, tets, theta = g["X"], g["tets"], g["theta"]
+    T, V = tets.shape[0], X.shape[0]
+    u_host = state(X)
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    u = torch.as_tensor(u_host, device=dev)
+    grad = torch.empty(3 * V, dtype=torch.float64, device=dev)
+    hess = torch.empty(e.nnz, dtype=torch.float64, device=dev)
+    Exact = energy.HessianKind.Exact
+
+    def step():
+        return e.eval_device(u, gradient=True, hessian=Exact, grad_out=grad, hess_out=hess)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local if world > 1 else torch.cuda.current_device()) as clocks:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, world)
+    ms_per_step = ms / args.steps
+    value = world * T * args.steps / (ms * 1e-3)
+    gpu_launches = 2 * args.steps  # assembly kernel + energy reduction per step
+
+    # Roofline of the assembly kernel: CUDA events on its launching stream, L2 flushed between launches.
+    ma, me = ctypes.c_double(), ctypes.c_double()
+    N.check(N.lib.lpg_fem_set_stream(e.handle, ctypes.c_void_p(stream.cuda_stream)))
+    N.check(N.lib.lpg_fem_time_eval(e.handle, N.vptr(u), N.vptr(grad), int(Exact), N.PRECISION_F64, N.LAYOUT_BSR,
+                                    N.vptr(hess), 10, 1, ctypes.byref(ma), ctypes.byref(me)))
+    ab = algorithmic_bytes(T, V, e.nnzb, "f64")
+    peak, peak_kind = measured_peak()
+    achieved = ab / (ma.value * 1e-3) / 1e9
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "assemble_kernel<double, true, 1>", "kernel_ms": ma.value,
+                "algorithmic_bytes": ab, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    # Mixed (FP32 element arithmetic + FP32 Hessian) kernel, reported beside it.
+    hess32 = torch.empty(e.nnz, dtype=torch.float32, device=dev)
+    ma32, me32 = ctypes.c_double(), ctypes.c_double()
+    N.check(N.lib.lpg_fem_time_eval(e.handle, N.vptr(u), N.vptr(grad), int(Exact), N.PRECISION_MIXED, N.LAYOUT_BSR,
+                                    N.vptr(hess32), 10, 1, ctypes.byref(ma32), ctypes.byref(me32)))
+    ab32 = algorithmic_bytes(T, V, e.nnzb, "f32")
+    mixed = {"tets_per_s_kernel": T / (ma32.value * 1e-3), "kernel_ms": ma32.value,
+             "achieved_gbs": ab32 / (ma32.value * 1e-3) / 1e9, "frac": ab32 / (ma32.value * 1e-3) / 1e9 / peak,
+             "algorithmic_bytes": ab32}
+
+    # End to end through the C ABI with pinned host buffers (H2D of u, D2H of gradient + CSC Hessian).
+    u_pin = torch.as_tensor(u_host).pin_memory()
+    g_pin = torch.empty(3 * V, dtype=torch.float64).pin_memory()
+    h_pin = torch.empty(e.nnz, dtype=torch.float64).pin_memory()
+    N.check(N.lib.lpg_fem_set_stream(e.handle, None))
+    E = ctypes.c_double()
+
+    def e2e_step():
+        N.check(N.lib.lpg_fem_eval(e.handle, N.vptr(u_pin), N.MEM_HOST, ctypes.byref(E), N.vptr(g_pin), int(Exact),
+                                   N.PRECISION_F64, N.LAYOUT_CSC, N.vptr(h_pin), N.MEM_HOST))
+
+    for _ in range(2):
+        e2e_step()
+    k_e2e = max(3, min(args.steps, 10))
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": world * T * k_e2e / e2e_s, "unit": "tets/s", "h2d_bytes_per_step": 8 * 3 * V,
+           "d2h_bytes_per_step": 8 * 3 * V + 8 * e.nnz + 8, "steps": k_e2e,
+           "timing": "wall clock around synchronous lpg_fem_eval calls (pinned host buffers, CSC layout)"}
+
+    newton = None
+    if not args.no_newton:
+        try:
+            newton = newton_times(e, g, torch)
+        except Exception as exc:  # reported, not hidden
+            newton = {"error": f"{type(exc).__name__}: {exc}"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(X, tets, theta, u_host)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded structured five-tet box)",
+            "config": dict(workload_config(), parallelism=f"replicas x{world}"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+            "clocks": clocks.summary(), "mixed_precision_kernel": mixed, "newton_time_to_1e-8": newton,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

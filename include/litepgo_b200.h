@@ -1,0 +1,237 @@
+/*
+ * litepgo_b200.h -- C ABI of the B200 (sm_100a) volumetric neo-Hookean hot path.
+ *
+ * This is the drop-in boundary for litepgo's
+ *   VolumetricFemEnergy<NeoHookean, TetP1Basis, TetCentroidQuadrature>
+ * energy / gradient / Hessian interface, its Newton solve and the adjoint
+ * equilibrium sensitivity. Every entry point cites the reference interface it
+ * replaces (paths inside annajcy/litepgo).
+ *
+ * Conventions kept from the reference:
+ *   - unknowns are displacements u, F = I + B u_e
+ *     (src/core/fem/assembly/volumetric_fem_energy.hpp:186-192);
+ *   - DOF = 3 * vertex + component (src/core/dof/vertex_dof_map.hpp:43-50);
+ *   - theta = [lambda, mu] (src/core/fem/material/volumetric/neo_hookean.hpp:9);
+ *   - 3x3 matrices (Fp) are column-major, index i + 3 j;
+ *   - the Hessian is the full symmetric matrix; its pattern is exported both as
+ *     3x3 block-CSR (row_ptr, col_idx) and as the reference's scalar CSC with
+ *     both triangles and int32 indices (src/core/common/types.hpp:18-22).
+ *
+ * Errors: every call returns an int status; no exception crosses the ABI. The
+ * message of the last failure on the calling thread is lpg_last_error().
+ *   LPG_EINVAL  <- std::invalid_argument (bad sizes, indices, theta)
+ *   LPG_EDOMAIN <- std::domain_error     (det F <= 0, non-finite values)
+ *   LPG_EBUSY   <- BusyScope's std::logic_error on overlapping calls
+ *                  (src/core/common/busy_scope.hpp:11-26)
+ *   LPG_ENOCONV <- a solve that did not converge
+ *   LPG_ECUDA   <- a CUDA runtime failure
+ *   LPG_ELOGIC  <- a broken contract (std::logic_error)
+ *
+ * Memory: the library owns its device buffers. Array arguments carry an
+ * explicit LPG_MEM_HOST / LPG_MEM_DEVICE flag. Device pointers must be device
+ * memory of the handle's GPU. A handle owns one CUDA stream (or the stream set
+ * with lpg_fem_set_stream); calls on one handle must not overlap.
+ */
+#ifndef LITEPGO_B200_H
+#define LITEPGO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LPG_ABI_VERSION 1
+
+enum lpg_status {
+    LPG_OK = 0,
+    LPG_EINVAL = 1,
+    LPG_EDOMAIN = 2,
+    LPG_EBUSY = 3,
+    LPG_ENOCONV = 4,
+    LPG_ECUDA = 5,
+    LPG_ELOGIC = 6
+};
+
+/* HessianKind (src/core/energy/scalar/energy.hpp:6-13) plus the analytic surrogate. */
+enum lpg_hessian_kind {
+    LPG_HESSIAN_NONE = 0,
+    LPG_HESSIAN_EXACT = 1,
+    LPG_HESSIAN_PROJECTED = 2,          /* 12x12 eigenvalue clamp, mesh_energy.cpp:16-27 */
+    LPG_HESSIAN_PROJECTED_ANALYTIC = 3  /* clamp of the 9x9 material tangent (not in the reference) */
+};
+
+enum lpg_precision {
+    LPG_PRECISION_F64 = 0,  /* all element arithmetic and outputs in FP64 */
+    LPG_PRECISION_MIXED = 1 /* element arithmetic + Hessian in FP32; energy/gradient sums in FP64 */
+};
+
+enum lpg_memory { LPG_MEM_HOST = 0, LPG_MEM_DEVICE = 1 };
+
+enum lpg_layout {
+    LPG_LAYOUT_BSR = 0, /* nnzb blocks of 9 values, row-major 3x3 */
+    LPG_LAYOUT_CSC = 1  /* the reference's scalar CSC value order (9 * nnzb values) */
+};
+
+typedef struct lpg_fem* lpg_fem_t;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* lpg_last_error(void);
+int lpg_abi_version(void);
+/* Writes a short build description (CUDA version, arch) into buf. */
+int lpg_build_info(char* buf, size_t size);
+
+/*
+ * Host-only (no GPU needed): block-CSR pattern of a tet mesh, the same pattern that
+ * lpg_fem_pattern_bsr returns. Validates the connectivity like MeshTopology
+ * (src/core/mesh/mesh_topology.hpp:25-44). Call with col_idx == NULL to get *nnzb first.
+ */
+int lpg_mesh_pattern_bsr(int num_vertices, int num_tets, const int32_t* tets, int64_t* nnzb, int32_t* row_ptr,
+                         int32_t* col_idx);
+
+/*
+ * Host-only summary of the assembly plan: out[0] nnzb, out[1] (row, element) pairs,
+ * out[2] warp tiles, out[3] pairs per tile capacity, out[4] most rows in one tile,
+ * out[5] contributor entries (4 per pair).
+ */
+int lpg_mesh_plan_summary(int num_vertices, int num_tets, const int32_t* tets, int64_t out[6]);
+
+/*
+ * Creates the element data and assembly plan of one tet mesh on `device`.
+ * Replaces the constructor
+ *   VolumetricFemEnergy(const VertexDofMap&, rest_positions, Fp, theta, int batch_size)
+ *   (src/core/fem/assembly/volumetric_fem_energy.hpp:29-65)
+ * together with MeshEnergy / EnergyAssembler set-up
+ *   (src/core/energy/scalar/mesh_energy.cpp:29-42, src/core/dof/energy_assembler.cpp:22-68).
+ *   X      : num_vertices * 3 rest positions (host), used when Xe == NULL
+ *   tets   : num_tets * 4 vertex indices (host)
+ *   Xe     : optional num_tets * 12 per-element rest corners (the reference's one
+ *            rest-position Response per element); NULL uses X[tets]
+ *   theta  : num_tets * 2 when theta_per_element != 0, else 2 shared values
+ *   Fp     : num_tets * 9 column-major plastic gradients, or NULL for identity
+ * Fails with LPG_EINVAL for out-of-range or repeated cell indices and for
+ * degenerate or inverted rest tets (volumetric_element.hpp:35-36).
+ */
+int lpg_fem_create(int num_vertices, const double* X, int num_tets, const int32_t* tets, const double* Xe,
+                   const double* theta, int theta_per_element, const double* Fp, int device, lpg_fem_t* out);
+int lpg_fem_destroy(lpg_fem_t h);
+
+/* Uses `stream` (a cudaStream_t) for all later work of this handle; NULL = the handle's own stream. */
+int lpg_fem_set_stream(lpg_fem_t h, void* stream);
+
+/* Sizes: vertices, tets, DOFs (3V), nnzb (3x3 blocks) and nnz (= 9 nnzb). Any pointer may be NULL. */
+int lpg_fem_sizes(lpg_fem_t h, int* num_vertices, int* num_tets, int* num_dofs, int64_t* nnzb, int64_t* nnz);
+
+/* Block-CSR pattern of the Hessian: row_ptr[V+1], col_idx[nnzb] (host). */
+int lpg_fem_pattern_bsr(lpg_fem_t h, int32_t* row_ptr, int32_t* col_idx);
+
+/* Scalar CSC pattern identical to EnergyAssembler::hessian_pattern()
+ * (energy_assembler.cpp:38-47): outer[3V+1], inner[nnz] (host). */
+int lpg_fem_pattern_csc(lpg_fem_t h, int32_t* outer, int32_t* inner);
+
+/*
+ * Energy, gradient and Hessian in one assembly. Replaces
+ *   Energy::eval(x, gradient, optional<HessianKind>)  (src/core/energy/scalar/energy.hpp:29-30)
+ * as implemented by MeshEnergy::eval_values + EnergyAssembler::assemble
+ *   (src/core/energy/scalar/mesh_energy.cpp:48-87, src/core/dof/energy_assembler.cpp:123-170).
+ *   u       : num_dofs displacements (io_mem)
+ *   energy  : host double (may be NULL)
+ *   grad    : num_dofs doubles (io_mem) or NULL
+ *   hessian : lpg_hessian_kind; values written to hess (hess_mem) in `layout`
+ *             as doubles (LPG_PRECISION_F64) or floats (LPG_PRECISION_MIXED)
+ * Sums are deterministic and atomic-free: each block is accumulated in element
+ * order, as the reference's per-column contribution lists do.
+ */
+int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, double* grad, int hessian, int precision,
+                 int layout, void* hess, int hess_mem);
+
+/*
+ * Profiling helper (no reference counterpart): enqueues `launches` evaluations of device
+ * arrays on the handle's stream and reports, from CUDA events recorded on that stream, the
+ * mean duration of the assembly kernel alone (ms_assemble) and of one whole evaluation
+ * including projection and the energy reduction (ms_eval). With flush_l2 != 0 a 512 MB
+ * buffer is written before each launch, outside the measured intervals.
+ */
+int lpg_fem_time_eval(lpg_fem_t h, const double* u, double* grad, int hessian, int precision, int layout, void* hess,
+                      int launches, int flush_l2, double* ms_assemble, double* ms_eval);
+
+/* Per-element energies vol * W (num_tets doubles, io_mem). */
+int lpg_fem_element_energies(lpg_fem_t h, const double* u, int io_mem, double* elem_energy);
+
+/*
+ * Largest safe step along du: Energy::max_feasible_step(x, dx)
+ *   (src/core/energy/scalar/energy.cpp:35-46) via MeshEnergy::feasible_step
+ *   (mesh_energy.cpp:88-107) and eval_positive_det_feasible_step
+ *   (src/core/fem/kinematics/positive_det_feasible_step.cpp:13-84).
+ */
+int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io_mem, double* alpha);
+
+/*
+ * Parameter VJP of the force response: per element [d/dlambda, d/dmu] of w . g(u).
+ * Replaces VolumetricFemForceMaterialResponse::eval_vjp
+ *   (src/core/fem/assembly/detail/volumetric_fem_force_response.hpp:155-179 through
+ *   src/core/energy/response/mesh_response.cpp:70-98) with an ElementDofMap
+ *   (per-element output, num_tets * 2) or ConstantDofMap (summed in element order, 2).
+ */
+int lpg_fem_force_vjp_theta(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element,
+                            double* out);
+
+/* Options of newton_solve (src/core/solver/newton.hpp:13-20) plus the GPU linear solve. */
+typedef struct {
+    double gradient_tolerance;  /* required; see stop_rule */
+    int max_iterations;         /* default 50 */
+    int hessian;                /* lpg_hessian_kind, default LPG_HESSIAN_PROJECTED */
+    int max_line_search_steps;  /* default 30 */
+    double line_search_shrink;  /* default 0.5 */
+    int stop_rule;              /* 0: max|g_free| <= tol (newton.cpp:34-36); 1: ||g_free||_2 <= tol ||g_free(x0)||_2 */
+    int accept_rule;            /* 0: E(trial) <= E + 16 eps max(1,|E|) (newton.cpp:83-86); 1: Armijo c=1e-4 plus that noise */
+    int precision;              /* lpg_precision of the Hessian and PCG; residual and energy stay FP64 */
+    double cg_tolerance;        /* forcing-term cap: relative PCG residual min(cg_tolerance, sqrt(||g||/||g0||)) */
+    int cg_max_iterations;      /* per Newton iteration */
+} lpg_newton_options;
+
+typedef struct {
+    int status;                  /* 0 Converged, 1 MaxIterations, 2 StepTooSmall, 3 NoDescentDirection (newton.hpp:22-31) */
+    int iterations;              /* accepted steps */
+    double energy;
+    double gradient_norm;        /* of the chosen stop rule */
+    double gradient_norm0;       /* ||g_free(x0)||_2 */
+    int64_t cg_iterations;       /* total PCG iterations */
+    int line_search_evaluations;
+    double seconds;              /* device time of the solve */
+} lpg_newton_result;
+
+void lpg_newton_default_options(lpg_newton_options* options);
+
+/*
+ * Minimises E(u) = elastic(u) - f_ext . u over the free DOFs from x0; fixed DOFs keep
+ * their x0 values. Replaces
+ *   newton_solve(Energy&, const DofReduction&, x0, const NewtonOptions&, SparseSolver&, on_iteration)
+ *   (src/core/solver/newton.hpp:67-69, newton.cpp:112-183)
+ * where the load is the reference's QuadraticEnergy with b = -f_ext in a WeightedSumEnergy
+ * (quadratic_energy.hpp:10-20, weighted_sum_energy.hpp:16-47), and the direct
+ * SparseSolver is replaced by block-Jacobi PCG on the 3x3 block-CSR Hessian.
+ *   fixed_dofs : num_fixed unique DOF indices (host)
+ *   f_ext      : num_dofs or NULL (io_mem)
+ *   x0, x_out  : num_dofs (io_mem)
+ */
+int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed_dofs, int num_fixed, const double* f_ext, const double* x0,
+                     int io_mem, const lpg_newton_options* options, double* x_out, lpg_newton_result* result);
+
+/*
+ * Adjoint of the static equilibrium: solves K_ff lambda = dLdu_free with the EXACT
+ * Hessian at u_star and returns dtheta = -(dg/dtheta)^T lambda, per element
+ * (num_tets * 2) or summed (2). Replaces the transpose branch of
+ *   StaticEquilibriumResponse::evaluate (src/core/solver/static_equilibrium_response.cpp:43-88)
+ * with its residual check ||K lambda - rhs|| <= 1e-8 (1 + ||rhs||) (:61-68).
+ * lambda_out (num_dofs, io_mem) may be NULL.
+ */
+int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, const int32_t* fixed_dofs,
+                      int num_fixed, int io_mem, int precision, double cg_tolerance, int per_element, double* dtheta,
+                      double* lambda_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

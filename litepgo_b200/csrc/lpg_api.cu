@@ -1,0 +1,507 @@
+// lpg_api.cu -- the C ABI (include/litepgo_b200.h): handle, element records, I/O.
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lpg_internal.h"
+#include "lpg_solver.h"
+
+namespace lpg {
+
+thread_local std::string g_last_error;
+
+void fail(int code, const std::string& what) { throw Error{code, what}; }
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(LPG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return LPG_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return LPG_ELOGIC;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return LPG_ELOGIC;
+    }
+}
+
+DeviceBuffer::~DeviceBuffer() {
+    if (ptr) cudaFree(ptr);
+}
+void* DeviceBuffer::ensure(size_t n) {
+    if (n <= bytes) return ptr;
+    if (ptr) LPG_CUDA(cudaFree(ptr));
+    ptr = nullptr;
+    bytes = 0;
+    LPG_CUDA(cudaMalloc(&ptr, n > 0 ? n : 1));
+    bytes = n;
+    return ptr;
+}
+
+namespace {
+
+template <class T> T* upload(DeviceBuffer& b, const std::vector<T>& v) {
+    T* p = b.as<T>(v.size());
+    if (!v.empty()) LPG_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return p;
+}
+
+// 3x3 row-major helpers for the element records.
+double det3(const double* a) {
+    return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) + a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+void inv3(const double* a, double* r) {
+    const double d = det3(a);
+    r[0] = (a[4] * a[8] - a[5] * a[7]) / d;
+    r[1] = (a[2] * a[7] - a[1] * a[8]) / d;
+    r[2] = (a[1] * a[5] - a[2] * a[4]) / d;
+    r[3] = (a[5] * a[6] - a[3] * a[8]) / d;
+    r[4] = (a[0] * a[8] - a[2] * a[6]) / d;
+    r[5] = (a[2] * a[3] - a[0] * a[5]) / d;
+    r[6] = (a[3] * a[7] - a[4] * a[6]) / d;
+    r[7] = (a[1] * a[6] - a[0] * a[7]) / d;
+    r[8] = (a[0] * a[4] - a[1] * a[3]) / d;
+}
+
+} // namespace
+
+// Maps status bits to the reference's exception classes and messages.
+void raise_status(unsigned st) {
+    if (st & ST_BAD_INPUT) fail(LPG_EINVAL, "Energy: x must have num_dofs finite entries");
+    if (st & ST_BAD_THETA) fail(LPG_EINVAL, "NeoHookean requires finite lambda >= 0 and mu > 0");
+    if (st & ST_NONFINITE_F) fail(LPG_EDOMAIN, "VolumetricFemEnergy: non-finite deformation gradient");
+    if (st & ST_BAD_DET) fail(LPG_EDOMAIN, "NeoHookean requires finite det(Fe) > 0");
+    if (st & ST_NONFINITE_OUT) fail(LPG_EDOMAIN, "VolumetricElement3D: non-finite integrated outputs");
+}
+
+} // namespace lpg
+
+using namespace lpg;
+
+struct BusyGuard {
+    std::atomic<bool>& b;
+    explicit BusyGuard(std::atomic<bool>& f) : b(f) {
+        if (b.exchange(true)) fail(LPG_EBUSY, "MeshEnergy is already in use by another call");
+    }
+    ~BusyGuard() { b.store(false); }
+};
+
+lpg_fem::~lpg_fem() {
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+void lpg_fem::sync() { LPG_CUDA(cudaStreamSynchronize(stream)); }
+
+unsigned lpg_fem::take_status() {
+    unsigned st = 0;
+    LPG_CUDA(cudaMemcpyAsync(&st, d_status.ptr, sizeof st, cudaMemcpyDeviceToHost, stream));
+    LPG_CUDA(cudaMemsetAsync(d_status.ptr, 0, sizeof(unsigned), stream));
+    sync();
+    return st;
+}
+
+// Device pointer of an input array: the caller's when device memory, else staged.
+const double* lpg_fem::stage_in(const double* p, int mem, DeviceBuffer& buf, size_t n) {
+    if (!p) return nullptr;
+    if (mem == LPG_MEM_DEVICE) return p;
+    if (mem != LPG_MEM_HOST) fail(LPG_EINVAL, "invalid memory flag");
+    double* d = buf.as<double>(n);
+    LPG_CUDA(cudaMemcpyAsync(d, p, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    return d;
+}
+
+void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int precision, int layout, void* dhess,
+                         double* delem, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+    if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
+        fail(LPG_EINVAL, "Energy: invalid Hessian kind");
+    if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
+    if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC) fail(LPG_EINVAL, "invalid Hessian layout");
+    EvalArgs a;
+    a.u = du;
+    a.grad = dgrad;
+    a.hess = hessian != LPG_HESSIAN_NONE ? dhess : nullptr;
+    a.layout = layout;
+    a.tile_energy = d_tile_energy.as<double>(std::max(dm.ntiles, 1));
+    a.energy = d_energy.as<double>(1);
+    a.elem_energy = delem;
+    a.status = d_status.as<unsigned>(1);
+    a.ev_begin = ev_begin;
+    a.ev_end = ev_end;
+    if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {
+        void* proj = d_proj.ensure(project_bytes(dm, precision));
+        launch_project(dm, precision, hessian, du, proj, a.status, stream);
+        a.proj = proj;
+    }
+    launch_eval(dm, precision, hessian, a, stream);
+}
+
+extern "C" {
+
+const char* lpg_last_error(void) { return g_last_error.c_str(); }
+int lpg_abi_version(void) { return LPG_ABI_VERSION; }
+
+int lpg_build_info(char* buf, size_t size) {
+    return guarded([&] {
+        int rt = 0, drv = 0;
+        cudaRuntimeGetVersion(&rt);
+        cudaDriverGetVersion(&drv);
+        std::snprintf(buf, size, "litepgo_b200 abi %d; CUDA runtime %d, driver %d; built for sm_100a", LPG_ABI_VERSION,
+                      rt, drv);
+    });
+}
+
+int lpg_mesh_pattern_bsr(int V, int T, const int32_t* tets, int64_t* nnzb, int32_t* row_ptr, int32_t* col_idx) {
+    return guarded([&] {
+        if (T > 0 && !tets) fail(LPG_EINVAL, "lpg_mesh_pattern_bsr: null tets");
+        HostPlan p;
+        build_plan(V, T, tets, p);
+        if (nnzb) *nnzb = p.nnzb();
+        if (row_ptr) std::copy(p.row_ptr.begin(), p.row_ptr.end(), row_ptr);
+        if (col_idx) std::copy(p.col_idx.begin(), p.col_idx.end(), col_idx);
+    });
+}
+
+int lpg_mesh_plan_summary(int V, int T, const int32_t* tets, int64_t out[6]) {
+    return guarded([&] {
+        if (T > 0 && !tets) fail(LPG_EINVAL, "lpg_mesh_plan_summary: null tets");
+        HostPlan p;
+        build_plan(V, T, tets, p);
+        int max_rows = 0;
+        for (int t = 0; t < p.ntiles(); ++t) max_rows = std::max(max_rows, p.tile_row_ptr[t + 1] - p.tile_row_ptr[t]);
+        out[0] = p.nnzb();
+        out[1] = static_cast<int64_t>(p.pair_elem.size());
+        out[2] = p.ntiles();
+        out[3] = p.cap;
+        out[4] = max_rows;
+        out[5] = static_cast<int64_t>(p.contrib.size());
+    });
+}
+
+int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const double* Xe, const double* theta,
+                   int theta_per_element, const double* Fp, int device, lpg_fem_t* out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!out) fail(LPG_EINVAL, "lpg_fem_create: null output handle");
+        if (T > 0 && (!tets || !theta || (!X && !Xe))) fail(LPG_EINVAL, "lpg_fem_create: null input array");
+        auto h = std::make_unique<lpg_fem>();
+        h->device = device;
+        LPG_CUDA(cudaSetDevice(device));
+        LPG_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+        build_plan(V, T, tets, h->plan);
+        // Element records (VolumetricElement3D ctor, volumetric_element.hpp:23-39, and the
+        // sampled B of deformation_gradient_sampling_response.hpp:24-41).
+        std::vector<double> rec(12 * static_cast<size_t>(T));
+        std::vector<double> fpinv(Fp ? 9 * static_cast<size_t>(T) : 0);
+        for (int e = 0; e < T; ++e) {
+            double Xc[4][3];
+            for (int a = 0; a < 4; ++a)
+                for (int k = 0; k < 3; ++k)
+                    Xc[a][k] = Xe ? Xe[12 * static_cast<size_t>(e) + 3 * a + k] : X[3 * static_cast<size_t>(tets[4 * e + a]) + k];
+            bool finite = true;
+            for (int a = 0; a < 4; ++a)
+                for (int k = 0; k < 3; ++k) finite = finite && std::isfinite(Xc[a][k]);
+            if (!finite) fail(LPG_EINVAL, "VolumetricElement3D: invalid reference Jacobian");
+            double J[9]; // row-major, column j = X_{j+1} - X_0
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) J[3 * i + j] = Xc[j + 1][i] - Xc[0][i];
+            const double det = det3(J);
+            const double w = det / 6.0;
+            if (!std::isfinite(det) || det <= 0 || !std::isfinite(w))
+                fail(LPG_EINVAL, "VolumetricElement3D: invalid reference determinant or volume weight");
+            double G[9];
+            inv3(J, G); // rows of J^-1 = grad N_1..3
+            for (double g : G)
+                if (!std::isfinite(g)) fail(LPG_EINVAL, "Deformation gradient sampling: non-finite physical gradient");
+            double vol = w;
+            if (Fp) {
+                double P[9]; // row-major from column-major input
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) P[3 * i + j] = Fp[9 * static_cast<size_t>(e) + i + 3 * j];
+                bool pf = true;
+                for (double v : P) pf = pf && std::isfinite(v);
+                if (!pf) fail(LPG_EINVAL, "MultiplicativeKinematics requires finite F and Fp");
+                const double dp = det3(P);
+                if (!std::isfinite(dp) || dp <= 0) fail(LPG_EDOMAIN, "MultiplicativeKinematics requires finite det(Fp) > 0");
+                double Pi[9];
+                inv3(P, Pi);
+                double G2[9];
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j)
+                        G2[3 * i + j] = G[3 * i] * Pi[j] + G[3 * i + 1] * Pi[3 + j] + G[3 * i + 2] * Pi[6 + j];
+                std::memcpy(G, G2, sizeof G);
+                std::memcpy(&fpinv[9 * static_cast<size_t>(e)], Pi, sizeof Pi);
+                vol = w * dp;
+            }
+            double* r = &rec[12 * static_cast<size_t>(e)];
+            std::memcpy(r, G, sizeof G);
+            r[9] = vol;
+            r[10] = theta_per_element ? theta[2 * static_cast<size_t>(e)] : theta[0];
+            r[11] = theta_per_element ? theta[2 * static_cast<size_t>(e) + 1] : theta[1];
+        }
+        std::vector<float> rec32(rec.begin(), rec.end());
+        const HostPlan& p = h->plan;
+        DevMesh& m = h->dm;
+        m.V = V;
+        m.T = T;
+        m.ntiles = p.ntiles();
+        m.cap = p.cap;
+        m.nnzb = p.nnzb();
+        m.row_ptr = upload(h->b_row_ptr, p.row_ptr);
+        m.col_idx = upload(h->b_col_idx, p.col_idx);
+        m.inc_ptr = upload(h->b_inc_ptr, p.inc_ptr);
+        m.tile_pair_ptr = upload(h->b_tile_pair_ptr, p.tile_pair_ptr);
+        m.tile_row_ptr = upload(h->b_tile_row_ptr, p.tile_row_ptr);
+        m.tile_rows = upload(h->b_tile_rows, p.tile_rows);
+        m.tile_slot_ptr = upload(h->b_tile_slot_ptr, p.tile_slot_ptr);
+        m.slot_off = upload(h->b_slot_off, p.slot_off);
+        m.contrib = upload(h->b_contrib, p.contrib);
+        m.pair_elem = upload(h->b_pair_elem, p.pair_elem);
+        std::vector<int32_t> tv(tets, tets + 4 * static_cast<size_t>(T));
+        m.tets = reinterpret_cast<int4*>(upload(h->b_tets, tv));
+        m.rec64 = upload(h->b_rec64, rec);
+        m.rec32 = upload(h->b_rec32, rec32);
+        if (Fp) {
+            std::vector<float> f32(fpinv.begin(), fpinv.end());
+            m.fpinv64 = upload(h->b_fpinv64, fpinv);
+            m.fpinv32 = upload(h->b_fpinv32, f32);
+        }
+        LPG_CUDA(cudaMemset(h->d_status.as<unsigned>(1), 0, sizeof(unsigned)));
+        LPG_CUDA(cudaDeviceSynchronize());
+        *out = h.release();
+    });
+}
+
+int lpg_fem_destroy(lpg_fem_t h) {
+    return guarded([&] {
+        if (!h) return;
+        cudaSetDevice(h->device);
+        if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+        if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+        delete h;
+    });
+}
+
+int lpg_fem_set_stream(lpg_fem_t h, void* stream) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    });
+}
+
+int lpg_fem_sizes(lpg_fem_t h, int* V, int* T, int* n, int64_t* nnzb, int64_t* nnz) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        if (V) *V = h->dm.V;
+        if (T) *T = h->dm.T;
+        if (n) *n = 3 * h->dm.V;
+        if (nnzb) *nnzb = h->dm.nnzb;
+        if (nnz) *nnz = 9 * h->dm.nnzb;
+    });
+}
+
+int lpg_fem_pattern_bsr(lpg_fem_t h, int32_t* row_ptr, int32_t* col_idx) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        if (row_ptr) std::copy(h->plan.row_ptr.begin(), h->plan.row_ptr.end(), row_ptr);
+        if (col_idx) std::copy(h->plan.col_idx.begin(), h->plan.col_idx.end(), col_idx);
+    });
+}
+
+int lpg_fem_pattern_csc(lpg_fem_t h, int32_t* outer, int32_t* inner) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        const HostPlan& p = h->plan;
+        // Column 3v + k holds rows 3w + i for the sorted block columns w of row v.
+        for (int v = 0; v < p.V; ++v) {
+            const int s0 = p.row_ptr[v], nb = p.row_ptr[v + 1] - s0;
+            for (int k = 0; k < 3; ++k) {
+                const int64_t start = 9 * static_cast<int64_t>(s0) + 3 * static_cast<int64_t>(nb) * k;
+                if (outer) outer[3 * v + k] = static_cast<int32_t>(start);
+                if (inner)
+                    for (int q = 0; q < nb; ++q)
+                        for (int i = 0; i < 3; ++i) inner[start + 3 * q + i] = 3 * p.col_idx[s0 + q] + i;
+            }
+        }
+        if (outer) outer[3 * p.V] = static_cast<int32_t>(9 * p.nnzb());
+    });
+}
+
+int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, double* grad, int hessian, int precision,
+                 int layout, void* hess, int hess_mem) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        if (!u && n > 0) fail(LPG_EINVAL, "lpg_fem_eval: null u");
+        if (hessian != LPG_HESSIAN_NONE && !hess) fail(LPG_EINVAL, "lpg_fem_eval: null Hessian output");
+        const double* du = h->stage_in(u, io_mem, h->d_u, n);
+        double* dgrad = nullptr;
+        if (grad) dgrad = io_mem == LPG_MEM_DEVICE ? grad : h->d_grad.as<double>(n);
+        const size_t hbytes = 9 * static_cast<size_t>(h->dm.nnzb) * (precision == LPG_PRECISION_F64 ? 8 : 4);
+        void* dhess = nullptr;
+        if (hessian != LPG_HESSIAN_NONE) {
+            if (hess_mem != LPG_MEM_HOST && hess_mem != LPG_MEM_DEVICE) fail(LPG_EINVAL, "invalid memory flag");
+            dhess = hess_mem == LPG_MEM_DEVICE ? hess : h->d_hess.ensure(hbytes);
+        }
+        h->eval_async(du, dgrad, hessian, precision, layout, dhess, nullptr);
+        double e = 0;
+        LPG_CUDA(cudaMemcpyAsync(&e, h->d_energy.ptr, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+        if (grad && io_mem == LPG_MEM_HOST)
+            LPG_CUDA(cudaMemcpyAsync(grad, dgrad, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        if (dhess && hess_mem == LPG_MEM_HOST)
+            LPG_CUDA(cudaMemcpyAsync(hess, dhess, hbytes, cudaMemcpyDeviceToHost, h->stream));
+        raise_status(h->take_status());
+        if (!std::isfinite(e)) fail(LPG_EDOMAIN, "MeshEnergy: non-finite energy sum");
+        if (energy) *energy = e;
+    });
+}
+
+int lpg_fem_time_eval(lpg_fem_t h, const double* u, double* grad, int hessian, int precision, int layout, void* hess,
+                      int launches, int flush_l2, double* ms_assemble, double* ms_eval) {
+    return guarded([&] {
+        if (!h || !u || launches <= 0) fail(LPG_EINVAL, "lpg_fem_time_eval: invalid arguments");
+        if (hessian != LPG_HESSIAN_NONE && !hess) fail(LPG_EINVAL, "lpg_fem_time_eval: null Hessian output");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t flush_bytes = size_t(512) << 20; // four times the 126 MB L2
+        void* fl = flush_l2 ? h->d_flush.ensure(flush_bytes) : nullptr;
+        std::vector<cudaEvent_t> ev(4 * static_cast<size_t>(launches));
+        for (auto& e : ev) LPG_CUDA(cudaEventCreate(&e));
+        for (int i = 0; i < launches; ++i) {
+            if (fl) LPG_CUDA(cudaMemsetAsync(fl, i & 0xff, flush_bytes, h->stream));
+            LPG_CUDA(cudaEventRecord(ev[4 * i], h->stream));
+            h->eval_async(u, grad, hessian, precision, layout, hess, nullptr, ev[4 * i + 1], ev[4 * i + 2]);
+            LPG_CUDA(cudaEventRecord(ev[4 * i + 3], h->stream));
+        }
+        const unsigned st = h->take_status();
+        double ta = 0, te = 0;
+        for (int i = 0; i < launches; ++i) {
+            float a = 0, b = 0;
+            LPG_CUDA(cudaEventElapsedTime(&a, ev[4 * i + 1], ev[4 * i + 2]));
+            LPG_CUDA(cudaEventElapsedTime(&b, ev[4 * i], ev[4 * i + 3]));
+            ta += a;
+            te += b;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        raise_status(st);
+        if (ms_assemble) *ms_assemble = ta / launches;
+        if (ms_eval) *ms_eval = te / launches;
+    });
+}
+
+int lpg_fem_element_energies(lpg_fem_t h, const double* u, int io_mem, double* elem_energy) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        const double* du = h->stage_in(u, io_mem, h->d_u, n);
+        double* de = io_mem == LPG_MEM_DEVICE ? elem_energy : h->d_vjp.as<double>(std::max(h->dm.T, 1));
+        h->eval_async(du, nullptr, LPG_HESSIAN_NONE, LPG_PRECISION_F64, LPG_LAYOUT_BSR, nullptr, de);
+        if (io_mem == LPG_MEM_HOST && h->dm.T > 0)
+            LPG_CUDA(cudaMemcpyAsync(elem_energy, de, h->dm.T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        raise_status(h->take_status());
+    });
+}
+
+int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io_mem, double* alpha) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        const double* d_u = h->stage_in(u, io_mem, h->d_u, n);
+        const double* d_du = h->stage_in(du, io_mem, h->d_u2, n);
+        const int nb = feasible_blocks(h->dm);
+        double* bm = h->d_block.as<double>(std::max(nb, 1));
+        double* al = h->d_alpha.as<double>(1);
+        launch_feasible(h->dm, d_u, d_du, bm, nb, al, h->d_status.as<unsigned>(1), h->stream);
+        double v = 1;
+        LPG_CUDA(cudaMemcpyAsync(&v, al, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+        const unsigned st = h->take_status();
+        // Energy::max_feasible_step validates x and dx first (energy.cpp:35-41).
+        if (st & ST_BAD_INPUT) fail(LPG_EINVAL, "Energy::max_feasible_step: x and dx must have num_dofs finite entries");
+        raise_status(st);
+        if (!(v >= 0.0 && v <= 1.0)) fail(LPG_ELOGIC, "Energy::max_feasible_step: the energy returned a value outside [0, 1]");
+        if (alpha) *alpha = v;
+    });
+}
+
+int lpg_fem_force_vjp_theta(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        const double* d_u = h->stage_in(u, io_mem, h->d_u, n);
+        const double* d_w = h->stage_in(w, io_mem, h->d_u2, n);
+        const size_t T = static_cast<size_t>(h->dm.T);
+        double* pe = (per_element && io_mem == LPG_MEM_DEVICE) ? out : h->d_vjp.as<double>(std::max<size_t>(2 * T, 2));
+        launch_force_vjp(h->dm, d_u, d_w, pe, h->d_status.as<unsigned>(1), h->stream);
+        if (per_element) {
+            if (io_mem == LPG_MEM_HOST && T > 0)
+                LPG_CUDA(cudaMemcpyAsync(out, pe, 2 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            const int nb = static_cast<int>(std::min<size_t>(1024, (T + 4095) / 4096));
+            double* part = h->d_block.as<double>(std::max(2 * nb, 2));
+            double* res = io_mem == LPG_MEM_DEVICE ? out : h->d_alpha.as<double>(2);
+            launch_sum_pairs(pe, static_cast<int>(T), part, nb, res, h->stream);
+            if (io_mem == LPG_MEM_HOST)
+                LPG_CUDA(cudaMemcpyAsync(out, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        }
+        raise_status(h->take_status());
+    });
+}
+
+void lpg_newton_default_options(lpg_newton_options* o) {
+    if (!o) return;
+    o->gradient_tolerance = std::nan("");
+    o->max_iterations = 50;
+    o->hessian = LPG_HESSIAN_PROJECTED;
+    o->max_line_search_steps = 30;
+    o->line_search_shrink = 0.5;
+    o->stop_rule = 0;
+    o->accept_rule = 0;
+    o->precision = LPG_PRECISION_F64;
+    o->cg_tolerance = 1e-2;
+    o->cg_max_iterations = 20000;
+}
+
+int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double* f_ext, const double* x0,
+                     int io_mem, const lpg_newton_options* o, double* x_out, lpg_newton_result* res) {
+    return guarded([&] {
+        if (!h || !o || !x0 || !x_out) fail(LPG_EINVAL, "lpg_newton_solve: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        newton_solve(*h, fixed, nfixed, f_ext, x0, io_mem, *o, x_out, res);
+    });
+}
+
+int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed,
+                      int io_mem, int precision, double cg_tolerance, int per_element, double* dtheta,
+                      double* lambda_out) {
+    return guarded([&] {
+        if (!h || !u_star || !dLdu || !dtheta) fail(LPG_EINVAL, "lpg_adjoint_theta: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        adjoint_theta(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, per_element, dtheta,
+                      lambda_out);
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,875 @@
+// lpg_assemble.cu -- sm_100a kernels of the neo-Hookean element pass.
+//
+// Element arithmetic follows the reference NeoHookean (src/core/fem/material/volumetric/
+// neo_hookean.cpp:14-60) on a TetP1 element with centroid quadrature
+// (src/core/fem/assembly/volumetric_fem_energy.hpp:78-123, dof_derivatives.cpp:22-51),
+// written in closed form: with grad N_a the P1 shape gradients, h_a = F^-T grad N_a and
+// p = lambda log J - mu,
+//   E_e   = vol * psi,   psi = mu/2 (|F|^2 - 3) - mu log J + lambda/2 (log J)^2
+//   g_a   = vol * P grad N_a,   P = mu F + p F^-T
+//   H_ab  = vol * [ mu (grad N_a . grad N_b) I + lambda h_a h_b^T - p h_b h_a^T ]
+// which equals vol * B^T (d2W/dF2) B for B = kron(grad N^T, I3).
+//
+// Assembly (replacing EnergyAssembler::assemble, src/core/dof/energy_assembler.cpp:123-170)
+// is fused and atomic-free: one warp owns a tile of whole block rows; each lane evaluates one
+// (row vertex, incident element) pair and leaves its four 3x3 blocks in shared memory; the
+// warp then sums every block slot of its rows over the slot's contributor list, which is in
+// ascending element order (the reference's per-column order, energy_assembler.cpp:49-54).
+// Block entries are formed with explicit round-to-nearest products so that H_ba is the exact
+// transpose of H_ab; the assembled matrix is bitwise symmetric.
+
+#include <cstdint>
+#include <cstdio>
+
+#include "lpg_internal.h"
+
+namespace lpg {
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+
+template <typename R> struct M;
+template <> struct M<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double log1p_(double x) { return log1p(x); }
+    static __device__ __forceinline__ double log_(double x) { return log(x); }
+    static __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+};
+template <> struct M<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float log1p_(float x) { return log1pf(x); }
+    static __device__ __forceinline__ float log_(float x) { return logf(x); }
+    static __device__ __forceinline__ bool finite(float x) { return isfinite(x); }
+};
+
+template <typename R> __device__ __forceinline__ const R* rec_ptr(const DevMesh& m);
+template <> __device__ __forceinline__ const double* rec_ptr<double>(const DevMesh& m) { return m.rec64; }
+template <> __device__ __forceinline__ const float* rec_ptr<float>(const DevMesh& m) { return m.rec32; }
+template <typename R> __device__ __forceinline__ const R* fpinv_ptr(const DevMesh& m);
+template <> __device__ __forceinline__ const double* fpinv_ptr<double>(const DevMesh& m) { return m.fpinv64; }
+template <> __device__ __forceinline__ const float* fpinv_ptr<float>(const DevMesh& m) { return m.fpinv32; }
+
+// 12-value element record, loaded with 16-byte vector loads.
+template <typename R> __device__ __forceinline__ void load_rec(const R* rec, int e, R* r);
+template <> __device__ __forceinline__ void load_rec<double>(const double* rec, int e, double* r) {
+    const double2* p = reinterpret_cast<const double2*>(rec + 12 * static_cast<size_t>(e));
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double2 v = __ldg(p + k);
+        r[2 * k] = v.x;
+        r[2 * k + 1] = v.y;
+    }
+}
+template <> __device__ __forceinline__ void load_rec<float>(const float* rec, int e, float* r) {
+    const float4* p = reinterpret_cast<const float4*>(rec + 12 * static_cast<size_t>(e));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 v = __ldg(p + k);
+        r[4 * k] = v.x;
+        r[4 * k + 1] = v.y;
+        r[4 * k + 2] = v.z;
+        r[4 * k + 3] = v.w;
+    }
+}
+
+// Kinematics of one element: shape gradients n[a], F, F^-T, log J, psi.
+template <typename R> struct Kin {
+    R n[4][3];
+    R F[9];   // row-major
+    R FiT[9]; // row-major
+    R logJ, psi, vol, lam, mu;
+};
+
+// Returns status bits. u is FP64; edge differences are formed in FP64 and rounded once.
+template <typename R>
+__device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const int4 tv, const double* __restrict__ u,
+                                               Kin<R>& k) {
+    using X = M<R>;
+    unsigned st = 0;
+    R rec[12];
+    load_rec<R>(rec_ptr<R>(m), e, rec);
+    const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
+    double u0[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) u0[i] = u[3 * static_cast<size_t>(vs[0]) + i];
+    R Ds[3][3]; // Ds[i][c] = u_{c+1,i} - u_{0,i}
+    bool in_ok = isfinite(u0[0]) && isfinite(u0[1]) && isfinite(u0[2]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double uc = u[3 * static_cast<size_t>(vs[c + 1]) + i];
+            in_ok = in_ok && isfinite(uc);
+            Ds[i][c] = static_cast<R>(uc - u0[i]);
+        }
+    }
+    if (!in_ok) st |= ST_BAD_INPUT;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) k.n[c + 1][j] = rec[3 * c + j];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) k.n[0][j] = -(k.n[1][j] + k.n[2][j] + k.n[3][j]);
+    k.vol = rec[9];
+    k.lam = rec[10];
+    k.mu = rec[11];
+    if (!(X::finite(k.lam) && X::finite(k.mu) && k.lam >= R(0) && k.mu > R(0))) st |= ST_BAD_THETA;
+    // Displacement gradient H = Ds G (G rows = grad N_1..3), F = offset + H.
+    R H[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            H[3 * i + j] = X::fma(Ds[i][2], rec[6 + j], X::fma(Ds[i][1], rec[3 + j], X::mul(Ds[i][0], rec[j])));
+    const R* fpi = fpinv_ptr<R>(m);
+    R J, sqm3; // J and |F|^2 - 3
+    if (fpi == nullptr) {
+#pragma unroll
+        for (int t = 0; t < 9; ++t) k.F[t] = H[t];
+        k.F[0] += R(1);
+        k.F[4] += R(1);
+        k.F[8] += R(1);
+        // det(I + H) - 1 = tr H + (sum of principal 2x2 minors of H) + det H, free of cancellation.
+        const R c1 = H[0] + H[4] + H[8];
+        const R c2 = (H[0] * H[4] - H[1] * H[3]) + (H[0] * H[8] - H[2] * H[6]) + (H[4] * H[8] - H[5] * H[7]);
+        const R c3 = H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
+                     H[2] * (H[3] * H[7] - H[4] * H[6]);
+        const R Jm1 = c1 + c2 + c3;
+        J = R(1) + Jm1;
+        k.logJ = X::log1p_(Jm1);
+        R hh = 0;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) hh = X::fma(H[t], H[t], hh);
+        sqm3 = R(2) * c1 + hh;
+    } else {
+        const R* o = fpi + 9 * static_cast<size_t>(e);
+#pragma unroll
+        for (int t = 0; t < 9; ++t) k.F[t] = __ldg(o + t) + H[t];
+        const R* F = k.F;
+        J = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) + F[2] * (F[3] * F[7] - F[4] * F[6]);
+        k.logJ = X::log_(J);
+        R ff = 0;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) ff = X::fma(F[t], F[t], ff);
+        sqm3 = ff - R(3);
+    }
+    bool f_ok = true;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) f_ok = f_ok && X::finite(k.F[t]);
+    if (!f_ok) st |= ST_NONFINITE_F;
+    else if (!(J > R(0)) || !X::finite(J)) st |= ST_BAD_DET;
+    const R* F = k.F;
+    const R iJ = R(1) / J;
+    // F^-T = cof(F) / det F.
+    k.FiT[0] = (F[4] * F[8] - F[5] * F[7]) * iJ;
+    k.FiT[1] = (F[5] * F[6] - F[3] * F[8]) * iJ;
+    k.FiT[2] = (F[3] * F[7] - F[4] * F[6]) * iJ;
+    k.FiT[3] = (F[2] * F[7] - F[1] * F[8]) * iJ;
+    k.FiT[4] = (F[0] * F[8] - F[2] * F[6]) * iJ;
+    k.FiT[5] = (F[1] * F[6] - F[0] * F[7]) * iJ;
+    k.FiT[6] = (F[1] * F[5] - F[2] * F[4]) * iJ;
+    k.FiT[7] = (F[2] * F[3] - F[0] * F[5]) * iJ;
+    k.FiT[8] = (F[0] * F[4] - F[1] * F[3]) * iJ;
+    k.psi = R(0.5) * k.mu * sqm3 - k.mu * k.logJ + R(0.5) * k.lam * k.logJ * k.logJ;
+    return st;
+}
+
+template <typename R> struct HOut;
+template <> struct HOut<double> { using T = double; };
+template <> struct HOut<float> { using T = float; };
+
+// Packed upper-triangle index of a symmetric 9x9 matrix.
+__host__ __device__ constexpr int sym9(int r, int c) {
+    return r <= c ? r * 9 - (r * (r - 1)) / 2 + (c - r) : c * 9 - (c * (c - 1)) / 2 + (r - c);
+}
+
+// Orthonormal basis of {x in R^4 : sum x = 0}: q = 1/2 [[1,1,1],[1,-1,-1],[-1,1,-1],[-1,-1,1]].
+// P1 shape gradients satisfy grad N = q (q^T grad N), so the element Hessian is
+// kron(q, I3) M kron(q, I3)^T for the 9x9 matrix M below, and clamping M's eigenvalues
+// clamps the element Hessian's (its remaining three eigenvalues are the zero translations).
+template <typename R> __device__ __forceinline__ R qbasis(int a, int j) {
+    const int sgn = (a == 0) ? 1 : ((a == j + 1) ? 1 : -1);
+    return sgn > 0 ? R(0.5) : R(-0.5);
+}
+
+struct TileMeta {
+    int row[32];
+    int slot0[32];
+    int nb[32];
+    int spre[33];
+    int ppre[33];
+};
+
+// Fused element pass + assembly. WG: gradient, WH: Hessian (0 none, 1 exact, 2 from the
+// projected tangents in a.proj), energy always.
+template <typename R, bool WG, int WH>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const DevMesh m, const EvalArgs a) {
+    using X = M<R>;
+    using HT = typename HOut<R>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x * kWarpsPerBlock + warp;
+    if (tile >= m.ntiles) return;
+    const int cap = m.cap;
+    // Per-warp shared layout: H blocks (cap*36 R), g (cap*3 R), meta.
+    const size_t per_warp = static_cast<size_t>(cap) * (WH ? 36 : 0) * sizeof(R) +
+                            static_cast<size_t>(cap) * (WG ? 3 : 0) * sizeof(R) + sizeof(TileMeta);
+    unsigned char* base = smem_raw + per_warp * warp;
+    R* sH = reinterpret_cast<R*>(base);
+    R* sg = sH + (WH ? cap * 36 : 0);
+    TileMeta* meta = reinterpret_cast<TileMeta*>(sg + (WG ? cap * 3 : 0));
+
+    const int p0 = m.tile_pair_ptr[tile];
+    const int np = m.tile_pair_ptr[tile + 1] - p0;
+    unsigned st = 0;
+    double e_acc = 0.0;
+    for (int q = lane; q < np; q += 32) {
+        const int pe = m.pair_elem[p0 + q];
+        const int e = pe & ((1 << 30) - 1);
+        const int la = static_cast<unsigned>(pe) >> 30;
+        const int4 tv = __ldg(m.tets + e);
+        Kin<R> k;
+        st |= kinematics<R>(m, e, tv, a.u, k);
+        if (la == 0) {
+            const R Ee = k.vol * k.psi;
+            e_acc += static_cast<double>(Ee);
+            if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
+            if (!X::finite(Ee)) st |= ST_NONFINITE_OUT;
+        }
+        R na[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) na[j] = la == 0 ? k.n[0][j] : la == 1 ? k.n[1][j] : la == 2 ? k.n[2][j] : k.n[3][j];
+        const R p = X::fma(k.lam, k.logJ, -k.mu);
+        if (WG) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                R s = 0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) s = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), na[j], s);
+                sg[3 * q + i] = k.vol * s;
+            }
+        }
+        if (WH == 1) {
+            R h[4][3];
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    h[b][i] = X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
+            R ha[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) ha[i] = la == 0 ? h[0][i] : la == 1 ? h[1][i] : la == 2 ? h[2][i] : h[3][i];
+            const R lv = X::mul(k.vol, k.lam);
+            const R pv = X::mul(k.vol, p);
+            const R mv = X::mul(k.vol, k.mu);
+            R* out = sH + 36 * q;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const R gg = X::fma(na[2], k.n[b][2], X::fma(na[1], k.n[b][1], X::mul(na[0], k.n[b][0])));
+                const R mg = X::mul(mv, gg);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk) {
+                        const R x = X::mul(ha[i], h[b][kk]);
+                        const R y = X::mul(h[b][i], ha[kk]);
+                        R v = X::fma(lv, x, X::mul(-pv, y));
+                        if (i == kk) v = X::add(v, mg);
+                        out[9 * b + 3 * i + kk] = v;
+                    }
+            }
+        } else if (WH == 2) {
+            // Projected: blocks from the clamped per-element tangent Mp (9x9 over (i, j') with
+            // index 3 j' + i, packed upper triangle) in the orthonormal basis q of {sum = 0}:
+            //   H_ab(i, k) = sum_{j', l'} q_a(j') q_b(l') Mp(3 j' + i, 3 l' + k).
+            const R* Mp = reinterpret_cast<const R*>(a.proj) + 45 * static_cast<size_t>(e);
+            R Y[3][9]; // Y[i][3 l' + k] = sum_j' q_a(j') Mp(3 j' + i, 3 l' + k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    R s = 0;
+#pragma unroll
+                    for (int jp = 0; jp < 3; ++jp) s = X::fma(qbasis<R>(la, jp), __ldg(Mp + sym9(3 * jp + i, c)), s);
+                    Y[i][c] = s;
+                }
+            R* out = sH + 36 * q;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk) {
+                        R s = 0;
+#pragma unroll
+                        for (int lp = 0; lp < 3; ++lp) s = X::fma(qbasis<R>(b, lp), Y[i][3 * lp + kk], s);
+                        out[9 * b + 3 * i + kk] = s;
+                    }
+        }
+    }
+    // Row metadata of the tile.
+    const int r0 = m.tile_row_ptr[tile];
+    const int nr = m.tile_row_ptr[tile + 1] - r0;
+    int my_nb = 0, my_deg = 0;
+    if (lane < nr) {
+        const int r = m.tile_rows[r0 + lane];
+        meta->row[lane] = r;
+        meta->slot0[lane] = m.row_ptr[r];
+        my_nb = m.row_ptr[r + 1] - m.row_ptr[r];
+        my_deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
+        meta->nb[lane] = my_nb;
+    }
+    int snb = my_nb, sdeg = my_deg;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int a1 = __shfl_up_sync(0xffffffffu, snb, off);
+        const int a2 = __shfl_up_sync(0xffffffffu, sdeg, off);
+        if (lane >= off) {
+            snb += a1;
+            sdeg += a2;
+        }
+    }
+    meta->spre[lane + 1] = snb;
+    meta->ppre[lane + 1] = sdeg;
+    if (lane == 0) {
+        meta->spre[0] = 0;
+        meta->ppre[0] = 0;
+    }
+    __syncwarp();
+    const int nslots = meta->spre[nr];
+    if (WH) {
+        const uint16_t* soff = m.slot_off + m.tile_slot_ptr[tile] + tile;
+        const uint8_t* con = m.contrib + 4 * static_cast<size_t>(p0);
+        HT* hout = reinterpret_cast<HT*>(a.hess);
+        int j = 0;
+        for (int o = lane; o < 9 * nslots; o += 32) {
+            const int s = o / 9;
+            const int kk = o - 9 * s;
+            while (meta->spre[j + 1] <= s) ++j;
+            const int c0 = soff[s], c1 = soff[s + 1];
+            R v = 0;
+            for (int c = c0; c < c1; ++c) {
+                const int bt = con[c];
+                v = X::add(v, sH[36 * (bt >> 2) + 9 * (bt & 3) + kk]);
+            }
+            if (!X::finite(v)) st |= ST_NONFINITE_OUT;
+            const int qs = s - meta->spre[j];
+            size_t pos;
+            if (a.layout == LPG_LAYOUT_BSR) {
+                pos = 9 * static_cast<size_t>(meta->slot0[j] + qs) + kk;
+            } else {
+                const int i = kk / 3, c = kk - 3 * i;
+                pos = 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * qs + c;
+            }
+            hout[pos] = static_cast<HT>(v);
+        }
+    }
+    if (WG && lane < 3 * nr) {
+        const int j = lane / 3, c = lane - 3 * j;
+        R v = 0;
+        for (int q = meta->ppre[j]; q < meta->ppre[j + 1]; ++q) v = X::add(v, sg[3 * q + c]);
+        if (!X::finite(v)) st |= ST_NONFINITE_OUT;
+        a.grad[3 * static_cast<size_t>(meta->row[j]) + c] = static_cast<double>(v);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) e_acc += __shfl_xor_sync(0xffffffffu, e_acc, off);
+    if (lane == 0) a.tile_energy[tile] = e_acc;
+    st = __reduce_or_sync(0xffffffffu, st);
+    if (lane == 0 && st) atomicOr(a.status, st);
+}
+
+// Deterministic sum of n doubles into *out with one block (fixed thread -> index map and tree).
+__global__ void __launch_bounds__(1024) sum_kernel(const double* __restrict__ x, int n, double* out) {
+    __shared__ double s[32];
+    double v = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += x[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (threadIdx.x == 0) *out = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Feasible step: eval_positive_det_feasible_step (positive_det_feasible_step.cpp:13-84)
+// on F = I + Ds G and dF = dDs G, per element, then the minimum (mesh_energy.cpp:88-107).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double det3r(const double* a) { // row-major
+    return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) + a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+
+// Column j of a row-major 3x3 is (a[j], a[3+j], a[6+j]).
+__device__ double positive_det_step(const double* A, const double* dA, unsigned& st) {
+    const double detA = det3r(A);
+    if (!isfinite(detA) || detA <= 0) {
+        st |= ST_BAD_DET;
+        return 0;
+    }
+    double a[9], d[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        double s = 0, t = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            s = fmax(s, fabs(A[3 * i + j]));
+            t = fmax(t, fabs(dA[3 * i + j]));
+        }
+        const double scale = fmax(s, t);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            a[3 * i + j] = A[3 * i + j] / scale;
+            d[3 * i + j] = dA[3 * i + j] / scale;
+        }
+    }
+    // Columns x_j = (m[j], m[3+j], m[6+j]); triple product x . (y cross z).
+    auto triple = [](const double* x, int jx, const double* y, int jy, const double* z, int jz) {
+        const double x0 = x[jx], x1 = x[3 + jx], x2 = x[6 + jx];
+        const double y0 = y[jy], y1 = y[3 + jy], y2 = y[6 + jy];
+        const double z0 = z[jz], z1 = z[3 + jz], z2 = z[6 + jz];
+        return x0 * (y1 * z2 - y2 * z1) + x1 * (y2 * z0 - y0 * z2) + x2 * (y0 * z1 - y1 * z0);
+    };
+    const double c0 = det3r(a);
+    const double c1 = triple(d, 0, a, 1, a, 2) + triple(a, 0, d, 1, a, 2) + triple(a, 0, a, 1, d, 2);
+    const double c2 = triple(d, 0, d, 1, a, 2) + triple(d, 0, a, 1, d, 2) + triple(a, 0, d, 1, d, 2);
+    const double c3 = det3r(d);
+    if (!(c0 > 0)) return 0;
+    const double eps = 2.220446049250313e-16;
+    auto value = [&](double t) { return fma(fma(fma(c3, t, c2), t, c1), t, c0); };
+    auto tol = [&](double t) { return 64 * eps * (((fabs(c3) * t + fabs(c2)) * t + fabs(c1)) * t + c0); };
+    double knots[4] = {0, 1, 0, 0};
+    int count = 2;
+    auto add_knot = [&](double t) {
+        if (t > 0 && t < 1) knots[count++] = t;
+    };
+    const double qa = 3 * c3, qb = 2 * c2, qc = c1;
+    if (qa == 0) {
+        if (qb != 0) add_knot(-qc / qb);
+    } else {
+        double disc = fma(qb, qb, -4 * qa * qc);
+        const double err = 8 * eps * (qb * qb + fabs(4 * qa * qc));
+        if (disc >= -err) {
+            disc = fmax(0.0, disc);
+            const double q = -0.5 * (qb + copysign(sqrt(disc), qb));
+            if (q == 0)
+                add_knot(-qb / (2 * qa));
+            else {
+                add_knot(q / qa);
+                add_knot(qc / q);
+            }
+        }
+    }
+    for (int i = 1; i < count; ++i)
+        for (int j = i; j > 0 && knots[j - 1] > knots[j]; --j) {
+            const double t = knots[j - 1];
+            knots[j - 1] = knots[j];
+            knots[j] = t;
+        }
+    for (int i = 1; i < count; ++i) {
+        double lo = knots[i - 1], hi = knots[i];
+        if (value(hi) > tol(hi)) continue;
+        // Bisection ends when the midpoint equals an end; 1100 halvings cover any bracket in [0, 1].
+        for (int it = 0; it < 1100; ++it) {
+            const double mid = lo + (hi - lo) / 2;
+            if (mid == lo || mid == hi) break;
+            if (value(mid) > tol(mid))
+                lo = mid;
+            else
+                hi = mid;
+        }
+        return 0.9 * lo;
+    }
+    return 1;
+}
+
+__global__ void __launch_bounds__(256) feasible_kernel(const DevMesh m, const double* __restrict__ u,
+                                                       const double* __restrict__ du, double* block_min,
+                                                       unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double alpha = 1.0;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int4 tv = __ldg(m.tets + e);
+        const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
+        double rec[12];
+        load_rec<double>(m.rec64, e, rec);
+        double Ds[9], dDs[9];
+        bool ok = true, dok = true;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double a0 = u[3 * static_cast<size_t>(vs[0]) + i], ac = u[3 * static_cast<size_t>(vs[c + 1]) + i];
+                const double b0 = du[3 * static_cast<size_t>(vs[0]) + i], bc = du[3 * static_cast<size_t>(vs[c + 1]) + i];
+                ok = ok && isfinite(a0) && isfinite(ac);
+                dok = dok && isfinite(b0) && isfinite(bc);
+                Ds[3 * i + c] = ac - a0;
+                dDs[3 * i + c] = bc - b0;
+            }
+        if (!ok || !dok) st |= ST_BAD_INPUT;
+        const double lam = rec[10], mu = rec[11];
+        if (!(isfinite(lam) && isfinite(mu) && lam >= 0 && mu > 0)) st |= ST_BAD_THETA;
+        double F[9], dF[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                F[3 * i + j] = Ds[3 * i] * rec[j] + Ds[3 * i + 1] * rec[3 + j] + Ds[3 * i + 2] * rec[6 + j];
+                dF[3 * i + j] = dDs[3 * i] * rec[j] + dDs[3 * i + 1] * rec[3 + j] + dDs[3 * i + 2] * rec[6 + j];
+            }
+        if (m.fpinv64) {
+#pragma unroll
+            for (int t = 0; t < 9; ++t) F[t] += m.fpinv64[9 * static_cast<size_t>(e) + t];
+        } else {
+            F[0] += 1;
+            F[4] += 1;
+            F[8] += 1;
+        }
+        bool fin = true;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) fin = fin && isfinite(F[t]) && isfinite(dF[t]);
+        if (!fin)
+            st |= ST_NONFINITE_F;
+        else if (st == 0)
+            alpha = positive_det_step(F, dF, st);
+    }
+    // Block minimum (order-independent, hence deterministic).
+    __shared__ double s[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) alpha = fmin(alpha, __shfl_xor_sync(0xffffffffu, alpha, off));
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = alpha;
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = s[0];
+        for (int w = 1; w < (blockDim.x >> 5); ++w) v = fmin(v, s[w]);
+        block_min[blockIdx.x] = v;
+    }
+}
+
+__global__ void __launch_bounds__(1024) min_kernel(const double* __restrict__ x, int n, double* out) {
+    __shared__ double s[32];
+    double v = 1.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v = fmin(v, x[i]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 1.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if (threadIdx.x == 0) *out = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Force-response parameter VJP (detail/volumetric_fem_force_response.hpp:155-179 with
+// NeoHookean::eval_d2W_dF_dtheta, neo_hookean.cpp:88-101): per element
+//   d/dlambda = vol log J  sum_a w_a . (F^-T grad N_a)
+//   d/dmu     = vol        sum_a w_a . ((F - F^-T) grad N_a)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) force_vjp_kernel(const DevMesh m, const double* __restrict__ u,
+                                                        const double* __restrict__ w, double* out, unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int4 tv = __ldg(m.tets + e);
+        Kin<double> k;
+        st |= kinematics<double>(m, e, tv, u, k);
+        const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
+        double sl = 0, sm = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double wi = w[3 * static_cast<size_t>(vs[b]) + i];
+                double hf = 0, ff = 0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    hf += k.FiT[3 * i + j] * k.n[b][j];
+                    ff += k.F[3 * i + j] * k.n[b][j];
+                }
+                sl += wi * hf;
+                sm += wi * (ff - hf);
+            }
+        }
+        double dl = k.vol * k.logJ * sl, dm = k.vol * sm;
+        if (m.fpinv64) {
+            // With a plastic field the record's G and vol already carry Fp^-1 and det Fp.
+        }
+        if (!isfinite(dl) || !isfinite(dm)) st |= ST_NONFINITE_OUT;
+        out[2 * static_cast<size_t>(e)] = dl;
+        out[2 * static_cast<size_t>(e) + 1] = dm;
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// Deterministic column sums of an (n x 2) array: partial sums per block, then one block.
+__global__ void __launch_bounds__(256) sum_pairs_partial(const double* __restrict__ x, int n, double* partial) {
+    __shared__ double s0[8], s1[8];
+    double a = 0, b = 0;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * per, hi = min(n, lo + per);
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        a += x[2 * static_cast<size_t>(i)];
+        b += x[2 * static_cast<size_t>(i) + 1];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s0[threadIdx.x >> 5] = a;
+        s1[threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x0 = 0, x1 = 0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) {
+            x0 += s0[w];
+            x1 += s1[w];
+        }
+        partial[2 * blockIdx.x] = x0;
+        partial[2 * blockIdx.x + 1] = x1;
+    }
+}
+__global__ void sum_pairs_final(const double* __restrict__ partial, int nb, double* out) {
+    if (threadIdx.x == 0) {
+        double x0 = 0, x1 = 0;
+        for (int i = 0; i < nb; ++i) {
+            x0 += partial[2 * i];
+            x1 += partial[2 * i + 1];
+        }
+        out[0] = x0;
+        out[1] = x1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Projected Hessian (HessianKind::Projected, mesh_energy.cpp:16-27): per element the 9x9
+// matrix M with H_e = kron(q, I3) M kron(q, I3)^T,
+//   M(3j'+i, 3l'+k) = vol [mu d_ik S_j'l' + lambda f_ij' f_kl' - p f_il' f_kj'],
+//   Rq = q^T grad N (3x3), S = Rq Rq^T, f = F^-T Rq^T,
+// is clamped to its non-negative eigenvalues: kept as is when an LDL^T test shows it
+// positive definite, else by cyclic Jacobi (Golub & Van Loan, Alg. 8.5.3). The result is
+// stored packed (45 values per element) for the assembly kernel.
+// ---------------------------------------------------------------------------
+constexpr int kProjThreads = 64;
+constexpr int kProjStride = 127; // 45 (M) + 81 (V) + 1: odd stride, conflict-free 8-byte lanes
+
+template <typename R> struct Eps;
+template <> struct Eps<double> { static constexpr double v = 2.220446049250313e-16; };
+template <> struct Eps<float> { static constexpr float v = 1.1920929e-7f; };
+
+template <typename R>
+__global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, const double* __restrict__ u,
+                                                               R* __restrict__ proj, unsigned* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* A = reinterpret_cast<R*>(smem_raw) + kProjStride * threadIdx.x;
+    R* V = A + 45;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int4 tv = __ldg(m.tets + e);
+        Kin<R> k;
+        st |= kinematics<R>(m, e, tv, u, k);
+        const R p = k.lam * k.logJ - k.mu;
+        R Rq[3][3];
+#pragma unroll
+        for (int jp = 0; jp < 3; ++jp)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                R s = 0;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) s += qbasis<R>(a, jp) * k.n[a][j];
+                Rq[jp][j] = s;
+            }
+        R S[3][3], f[3][3];
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+#pragma unroll
+            for (int y = 0; y < 3; ++y) {
+                S[x][y] = Rq[x][0] * Rq[y][0] + Rq[x][1] * Rq[y][1] + Rq[x][2] * Rq[y][2];
+                f[x][y] = k.FiT[3 * x] * Rq[y][0] + k.FiT[3 * x + 1] * Rq[y][1] + k.FiT[3 * x + 2] * Rq[y][2];
+            }
+#pragma unroll
+        for (int jp = 0; jp < 3; ++jp)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int lp = 0; lp < 3; ++lp)
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk) {
+                        const int r = 3 * jp + i, c = 3 * lp + kk;
+                        if (r > c) continue;
+                        R v = k.lam * f[i][jp] * f[kk][lp] - p * f[i][lp] * f[kk][jp];
+                        if (i == kk) v += k.mu * S[jp][lp];
+                        A[sym9(r, c)] = k.vol * v;
+                    }
+        // LDL^T positive-definiteness test in the V area (row-major 9x9 scratch).
+        bool pd = true;
+        for (int j = 0; j < 9 && pd; ++j) {
+            R d = A[sym9(j, j)];
+            for (int t = 0; t < j; ++t) d -= V[9 * j + t] * V[9 * j + t] * V[9 * t + t];
+            if (!(d > R(0))) {
+                pd = false;
+                break;
+            }
+            V[9 * j + j] = d;
+            for (int i = j + 1; i < 9; ++i) {
+                R s = A[sym9(i, j)];
+                for (int t = 0; t < j; ++t) s -= V[9 * i + t] * V[9 * j + t] * V[9 * t + t];
+                V[9 * i + j] = s / d;
+            }
+        }
+        R* out = proj + 45 * static_cast<size_t>(e);
+        if (pd) {
+            for (int t = 0; t < 45; ++t) out[t] = A[t];
+        } else {
+            for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
+            R total = 0;
+            for (int t = 0; t < 45; ++t) total += A[t] * A[t];
+            for (int sweep = 0; sweep < 20; ++sweep) {
+                R off = 0;
+                for (int r = 0; r < 9; ++r)
+                    for (int c = r + 1; c < 9; ++c) off += A[sym9(r, c)] * A[sym9(r, c)];
+                if (!(off > R(16) * Eps<R>::v * Eps<R>::v * total)) break;
+                for (int pp = 0; pp < 8; ++pp)
+                    for (int qq = pp + 1; qq < 9; ++qq) {
+                        const R apq = A[sym9(pp, qq)];
+                        if (apq == R(0)) continue;
+                        const R app = A[sym9(pp, pp)], aqq = A[sym9(qq, qq)];
+                        const R tau = (aqq - app) / (R(2) * apq);
+                        const R t = (tau >= R(0) ? R(1) : R(-1)) / (fabs(tau) + sqrt(R(1) + tau * tau));
+                        const R c = R(1) / sqrt(R(1) + t * t), sn = t * c;
+                        for (int kx = 0; kx < 9; ++kx) {
+                            if (kx == pp || kx == qq) continue;
+                            const R akp = A[sym9(kx, pp)], akq = A[sym9(kx, qq)];
+                            A[sym9(kx, pp)] = c * akp - sn * akq;
+                            A[sym9(kx, qq)] = sn * akp + c * akq;
+                        }
+                        A[sym9(pp, pp)] = app - t * apq;
+                        A[sym9(qq, qq)] = aqq + t * apq;
+                        A[sym9(pp, qq)] = R(0);
+                        for (int kx = 0; kx < 9; ++kx) {
+                            const R vkp = V[9 * kx + pp], vkq = V[9 * kx + qq];
+                            V[9 * kx + pp] = c * vkp - sn * vkq;
+                            V[9 * kx + qq] = sn * vkp + c * vkq;
+                        }
+                    }
+            }
+            R lam9[9];
+            for (int t = 0; t < 9; ++t) lam9[t] = fmax(A[sym9(t, t)], R(0));
+            for (int r = 0; r < 9; ++r)
+                for (int c = r; c < 9; ++c) {
+                    R s = 0;
+                    for (int t = 0; t < 9; ++t) s += V[9 * r + t] * lam9[t] * V[9 * c + t];
+                    out[sym9(r, c)] = s;
+                }
+        }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+template <typename R, bool WG, int WH> size_t smem_bytes(int cap) {
+    return kWarpsPerBlock * (static_cast<size_t>(cap) * (WH ? 36 : 0) * sizeof(R) +
+                             static_cast<size_t>(cap) * (WG ? 3 : 0) * sizeof(R) + sizeof(TileMeta));
+}
+
+template <typename R, bool WG, int WH> void launch_assemble(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    const size_t sm = smem_bytes<R, WG, WH>(m.cap);
+    static bool configured = false;
+    if (!configured) {
+        LPG_CUDA(cudaFuncSetAttribute(assemble_kernel<R, WG, WH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem_bytes<R, WG, WH>(64))));
+        configured = true;
+    }
+    const int blocks = (m.ntiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
+    if (blocks > 0) assemble_kernel<R, WG, WH><<<blocks, 32 * kWarpsPerBlock, sm, s>>>(m, a);
+    if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
+    LPG_CUDA(cudaGetLastError());
+}
+
+template <typename R> void launch_eval_t(const DevMesh& m, int hessian, const EvalArgs& a, cudaStream_t s) {
+    const bool wg = a.grad != nullptr;
+    const int wh = a.hess == nullptr ? 0 : (hessian == LPG_HESSIAN_EXACT ? 1 : 2);
+    if (wg && wh == 1) launch_assemble<R, true, 1>(m, a, s);
+    else if (wg && wh == 2) launch_assemble<R, true, 2>(m, a, s);
+    else if (!wg && wh == 1) launch_assemble<R, false, 1>(m, a, s);
+    else if (!wg && wh == 2) launch_assemble<R, false, 2>(m, a, s);
+    else if (wg) launch_assemble<R, true, 0>(m, a, s);
+    else launch_assemble<R, false, 0>(m, a, s);
+}
+
+} // namespace
+
+void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s) {
+    if (precision == LPG_PRECISION_F64)
+        launch_eval_t<double>(m, hessian, a, s);
+    else
+        launch_eval_t<float>(m, hessian, a, s);
+    sum_kernel<<<1, 1024, 0, s>>>(a.tile_energy, m.ntiles, a.energy);
+    LPG_CUDA(cudaGetLastError());
+}
+
+size_t project_bytes(const DevMesh& m, int precision) {
+    return static_cast<size_t>(m.T) * 45 * (precision == LPG_PRECISION_F64 ? sizeof(double) : sizeof(float));
+}
+
+void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
+                    cudaStream_t s) {
+    if (hessian != LPG_HESSIAN_PROJECTED) fail(LPG_EINVAL, "projected Hessian kind not available");
+    const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
+    if (blocks == 0) return;
+    if (precision == LPG_PRECISION_F64) {
+        const size_t sm = sizeof(double) * kProjStride * kProjThreads;
+        static bool configured = false;
+        if (!configured) {
+            LPG_CUDA(cudaFuncSetAttribute(project_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(sm)));
+            configured = true;
+        }
+        project_kernel<double><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<double*>(proj), status);
+    } else {
+        const size_t sm = sizeof(float) * kProjStride * kProjThreads;
+        project_kernel<float><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<float*>(proj), status);
+    }
+    LPG_CUDA(cudaGetLastError());
+}
+
+int feasible_blocks(const DevMesh& m) { return (m.T + 255) / 256; }
+
+void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
+                     double* alpha, unsigned* status, cudaStream_t s) {
+    if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status);
+    min_kernel<<<1, 1024, 0, s>>>(block_min, nblocks, alpha);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out, unsigned* status,
+                      cudaStream_t s) {
+    if (m.T > 0) force_vjp_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, u, w, out, status);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s) {
+    if (nblocks > 0) sum_pairs_partial<<<nblocks, 256, 0, s>>>(per_elem, T, partial);
+    sum_pairs_final<<<1, 32, 0, s>>>(partial, nblocks, out2);
+    LPG_CUDA(cudaGetLastError());
+}
+
+} // namespace lpg

@@ -1,0 +1,101 @@
+// lpg_internal.h -- shared host-side definitions of the litepgo_b200 CUDA library.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/litepgo_b200.h"
+
+namespace lpg {
+
+// Device status word bits, OR-ed by kernels that find a bad element or input.
+enum : unsigned {
+    ST_BAD_INPUT = 1u << 0,    // non-finite u / du           -> LPG_EINVAL
+    ST_BAD_THETA = 1u << 1,    // lambda < 0, mu <= 0, NaN     -> LPG_EINVAL
+    ST_NONFINITE_F = 1u << 2,  // non-finite F or increment    -> LPG_EDOMAIN
+    ST_BAD_DET = 1u << 3,      // det F <= 0                   -> LPG_EDOMAIN
+    ST_NONFINITE_OUT = 1u << 4 // non-finite E, g or H         -> LPG_EDOMAIN
+};
+
+struct Error {
+    int code;
+    std::string what;
+};
+[[noreturn]] void fail(int code, const std::string& what);
+void check_cuda(cudaError_t e, const char* what);
+#define LPG_CUDA(call) ::lpg::check_cuda((call), #call)
+
+// Host-side assembly plan (built once per mesh, lpg_plan.cpp).
+//
+// Rows of the 3x3 block-CSR Hessian are vertices. A "pair" is (row vertex v, element e
+// incident to v, local index a of v in e); each pair produces the 4 blocks H_{a,b},
+// b = 0..3, of row v and the gradient piece g_a. Pairs are grouped into warp tiles of at
+// most `cap` pairs (whole rows only); a tile owns every block slot of its rows, so a warp
+// reduces its slots on chip in element order with no atomics.
+struct HostPlan {
+    int V = 0, T = 0;
+    int cap = 32;
+    std::vector<int32_t> row_ptr, col_idx;   // BSR pattern (V+1, nnzb)
+    std::vector<int32_t> inc_ptr;            // V+1: pairs per row, natural order
+    std::vector<int32_t> tile_pair_ptr;      // ntiles+1
+    std::vector<int32_t> tile_row_ptr;       // ntiles+1
+    std::vector<int32_t> tile_rows;          // rows of each tile, ascending
+    std::vector<int32_t> tile_slot_ptr;      // ntiles+1 (cumulative slot counts)
+    std::vector<uint16_t> slot_off;          // nnzb + ntiles: contributor offsets per tile slot
+    std::vector<uint8_t> contrib;            // 4 * npairs: (pair_local << 2) | b, per slot in element order
+    std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
+    int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
+    int64_t nnzb() const { return static_cast<int64_t>(col_idx.size()); }
+};
+
+// Validates connectivity (mesh_topology.hpp:25-44) and builds the plan.
+void build_plan(int V, int T, const int32_t* tets, HostPlan& plan);
+
+// Device mirror of the plan and of the per-element records.
+struct DevMesh {
+    int V = 0, T = 0, ntiles = 0, cap = 32;
+    int64_t nnzb = 0;
+    int32_t *row_ptr = nullptr, *col_idx = nullptr, *inc_ptr = nullptr;
+    int32_t *tile_pair_ptr = nullptr, *tile_row_ptr = nullptr, *tile_rows = nullptr, *tile_slot_ptr = nullptr;
+    uint16_t* slot_off = nullptr;
+    uint8_t* contrib = nullptr;
+    int32_t* pair_elem = nullptr;
+    int4* tets = nullptr;
+    // Per-element record: G (3x3 row-major, rows = grad N_1..3 in rest coordinates, times Fp^-1),
+    // vol (= det(Dm)/6 * det Fp), lambda, mu. 12 values, 16-byte aligned.
+    double* rec64 = nullptr;
+    float* rec32 = nullptr;
+    // Fp^-1 row-major (9 per element) when the mesh has a plastic field, else null.
+    double* fpinv64 = nullptr;
+    float* fpinv32 = nullptr;
+};
+
+// ---- kernel launchers (lpg_assemble.cu) ----
+struct EvalArgs {
+    const double* u = nullptr;  // device, 3V
+    double* grad = nullptr;     // device, 3V or null
+    void* hess = nullptr;       // device values or null
+    int layout = LPG_LAYOUT_BSR;
+    double* tile_energy = nullptr; // device, ntiles (always written)
+    double* energy = nullptr;      // device scalar (always written)
+    double* elem_energy = nullptr; // device, T, or null
+    const void* proj = nullptr;    // projected per-element 9x9 tangents (hessian PROJECTED*), or null
+    unsigned* status = nullptr;    // device status word
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr; // optional: bracket the assembly kernel
+};
+void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s);
+// Per-element clamped tangents for the projected Hessians (45 values / element, upper triangle).
+void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
+                    cudaStream_t s);
+size_t project_bytes(const DevMesh& m, int precision);
+void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
+                     double* alpha, unsigned* status, cudaStream_t s);
+int feasible_blocks(const DevMesh& m);
+void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out_per_elem, unsigned* status,
+                      cudaStream_t s);
+void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s);
+
+} // namespace lpg

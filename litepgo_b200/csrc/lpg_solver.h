@@ -1,0 +1,55 @@
+// lpg_solver.h -- the handle behind lpg_fem_t and the solver entry points.
+#pragma once
+
+#include <atomic>
+#include <cstddef>
+
+#include "lpg_internal.h"
+
+namespace lpg {
+
+// Owned device allocation that only grows.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer();
+    void* ensure(size_t n);
+    template <class T> T* as(size_t count) { return static_cast<T*>(ensure(count * sizeof(T))); }
+};
+
+void raise_status(unsigned st);
+
+} // namespace lpg
+
+struct lpg_fem {
+    int device = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    lpg::HostPlan plan;
+    lpg::DevMesh dm;
+    std::atomic<bool> busy{false};
+    // Plan and element data.
+    lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tile_pair_ptr, b_tile_row_ptr, b_tile_rows, b_tile_slot_ptr,
+        b_slot_off, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot;
+    // Scratch of the evaluation entry points.
+    lpg::DeviceBuffer d_status, d_tile_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
+    // Solver state (Newton / PCG / adjoint).
+    lpg::DeviceBuffer s_x, s_g, s_f, s_d, s_trial, s_mask, s_hess, s_hess64, s_dinv, s_r, s_z, s_p, s_ap, s_xcg, s_r64,
+        s_b64, s_scal, s_part, s_flag, d_flush;
+    ~lpg_fem();
+    void sync();
+    unsigned take_status();
+    const double* stage_in(const double* p, int mem, lpg::DeviceBuffer& buf, size_t n);
+    // Enqueues one evaluation on the handle's stream (no synchronisation).
+    void eval_async(const double* du, double* dgrad, int hessian, int precision, int layout, void* dhess,
+                    double* delem, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr);
+};
+
+namespace lpg {
+void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
+                  const lpg_newton_options& o, double* x_out, lpg_newton_result* res);
+void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                   int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out);
+} // namespace lpg

@@ -1,0 +1,468 @@
+"""Volumetric neo-Hookean FEM on the GPU, mirroring litepgo.fem for the TetP1 path.
+
+``VolumetricFemEnergy[NeoHookean, TetP1Basis, TetCentroidQuadrature](displacement_map,
+rest_position_fields, Fp, theta, batch_size=256)`` keeps the reference constructor
+(src/binding/fem/assembly/volumetric_fem_energy.cpp:41-47; src/python/fem.py:155-233) and
+the Energy interface ``eval / eval_value / eval_gradient / eval_hessian / max_feasible_step``
+(src/binding/energy/scalar/energy.cpp:26-48). Fields are sampled once at the centroid
+(volumetric_fem_energy.hpp:58-63). Hessians are returned as scipy.sparse.csc_matrix with the
+reference's pattern (both triangles, sorted rows). All arithmetic runs in the CUDA library;
+``batch_size`` is validated and kept for interface compatibility (results do not depend on
+it, as the reference's batch-invariance test requires, tests/python/test_fem_batch_size.py).
+
+Arrays are accepted wherever the reference takes per-element Response lists:
+rest positions as (V, 3) vertex positions or (T, 4, 3) corners, Fp as (9,) or (T, 9)
+column-major, theta as (2,) or (T, 2) [lambda, mu].
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from .dof import ConstantDofMap, ElementDofMap, VertexDofMap
+from .energy import AffineResponse, Energy, HessianKind
+
+__all__ = [
+    "NeoHookean",
+    "TetP1Basis",
+    "TetCentroidQuadrature",
+    "InterpolatedResponse",
+    "Template",
+    "VolumetricFemEnergy",
+    "VolumetricFemForceMaterialResponse",
+    "VolumetricFemEnergyTetP1",
+    "VolumetricFemForceMaterialResponseTetP1",
+]
+
+
+class NeoHookean:
+    """W = det(Fp) psi(F Fp^-1), theta = [lambda, mu] (neo_hookean.hpp:9-33)."""
+
+    num_parameters = 2
+
+
+class TetP1Basis:
+    """Linear tetrahedron shape functions (tet_p1_basis.cpp:7-15)."""
+
+    num_basis_functions = 4
+
+    @staticmethod
+    def eval_N(xi):
+        xi = np.asarray(xi, dtype=np.float64)
+        return np.array([1 - xi.sum(), xi[0], xi[1], xi[2]])
+
+    @staticmethod
+    def eval_dN_dxi(xi):
+        return np.array([[-1.0, -1, -1], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+
+
+class TetCentroidQuadrature:
+    """One point at the centroid, weight 1/6 (tet_centroid_quadrature.hpp:9-23)."""
+
+    num_points = 1
+
+    @staticmethod
+    def points():
+        return np.full((1, 3), 0.25)
+
+    @staticmethod
+    def weights():
+        return np.array([1.0 / 6.0])
+
+
+class _InterpolatedResponseTetP1:
+    """xi -> coefficients^T N(xi) (src/core/fem/response/interpolated_response.hpp:13-63)."""
+
+    def __init__(self, coefficients):
+        c = np.asarray(coefficients, dtype=np.float64)
+        if c.ndim != 2 or c.shape[0] != 4:
+            raise ValueError("InterpolatedResponse[TetP1Basis] requires (4, k) coefficients")
+        self.coefficients = c.copy()
+
+    @property
+    def num_inputs(self):
+        return 3
+
+    @property
+    def num_outputs(self):
+        return self.coefficients.shape[1]
+
+    def eval_value(self, xi):
+        return self.coefficients.T @ TetP1Basis.eval_N(xi)
+
+
+class Template:
+    """A template of the reference indexed by argument tuple, e.g. VolumetricFemEnergy[M, B, Q]."""
+
+    def __init__(self, name, instances):
+        self.__name__ = name
+        self._instances = dict(instances)
+
+    def __getitem__(self, args):
+        key = args if isinstance(args, tuple) else (args,)
+        try:
+            return self._instances[key]
+        except KeyError:
+            names = ", ".join(getattr(a, "__name__", repr(a)) for a in key)
+            avail = "; ".join(
+                f"{self.__name__}[{', '.join(a.__name__ for a in k)}]" for k in self._instances)
+            raise TypeError(f"{self.__name__}[{names}] is not instantiated; available: {avail}") from None
+
+    @property
+    def instances(self):
+        return dict(self._instances)
+
+    def __repr__(self):
+        return f"<template litepgo_b200.fem.{self.__name__}>"
+
+
+InterpolatedResponse = Template("InterpolatedResponse", {(TetP1Basis,): _InterpolatedResponseTetP1})
+
+_CENTROID = np.full(3, 0.25)
+
+
+def _sample_fields(fields, count, width, what):
+    """Per-element field values at the centroid as a (count, width) array, or (width,) if shared."""
+    if fields is None:
+        return None
+    if isinstance(fields, np.ndarray) or (isinstance(fields, (list, tuple)) and fields and
+                                          isinstance(fields[0], (int, float, np.floating))):
+        a = np.asarray(fields, dtype=np.float64)
+        if a.shape == (width,):
+            return a
+        if a.shape == (count, width):
+            return np.ascontiguousarray(a)
+        raise ValueError(f"VolumetricFemEnergy: {what} must have shape ({width},) or ({count}, {width})")
+    fields = list(fields)
+    if len(fields) != count:
+        raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
+    out = np.empty((count, width))
+    cache = {}
+    for e, f in enumerate(fields):
+        if f is None or getattr(f, "num_inputs", 3) != 3 or getattr(f, "num_outputs", width) != width:
+            raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
+        key = id(f)
+        if key not in cache:
+            cache[key] = np.asarray(f.eval_value(_CENTROID), dtype=np.float64)
+        out[e] = cache[key]
+    if len(cache) == 1:
+        return out[0].copy()
+    return out
+
+
+def _rest_geometry(fields, num_vertices, count):
+    """(X, Xe): vertex positions (V, 3) or per-element corners (T, 12)."""
+    if isinstance(fields, np.ndarray):
+        a = np.asarray(fields, dtype=np.float64)
+        if a.shape == (num_vertices, 3) or (a.ndim == 1 and a.size == 3 * num_vertices):
+            return np.ascontiguousarray(a.reshape(-1, 3)), None
+        if a.shape == (count, 4, 3) or a.shape == (count, 12):
+            return None, np.ascontiguousarray(a.reshape(count, 12))
+        raise ValueError("VolumetricFemEnergy: rest positions must be (V, 3) or (T, 4, 3)")
+    fields = list(fields)
+    if len(fields) != count:
+        raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
+    Xe = np.empty((count, 12))
+    for e, f in enumerate(fields):
+        c = getattr(f, "coefficients", None)
+        if c is None or np.shape(c) != (4, 3):
+            raise ValueError("VolumetricFemEnergy: incompatible displacement basis")
+        Xe[e] = np.asarray(c, dtype=np.float64).ravel()
+    return None, Xe
+
+
+def _device_index():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            return torch.cuda.current_device()
+    except ImportError:  # pragma: no cover - torch is part of the image
+        pass
+    return 0
+
+
+class _Input:
+    """A vector argument as (pointer, memory flag), keeping NumPy copies alive."""
+
+    def __init__(self, x, n, name="x", check_finite=True):
+        self.tensor = None
+        if hasattr(x, "is_cuda") and x.is_cuda:
+            import torch
+
+            if x.dtype != torch.float64 or x.ndim != 1 or x.numel() != n:
+                raise ValueError(f"Energy: {name} must be a one-dimensional float64 tensor with num_dofs entries")
+            self.tensor = x.contiguous()
+            self.ptr, self.mem = N.vptr(self.tensor), N.MEM_DEVICE
+            self.array = None
+        else:
+            if hasattr(x, "detach"):
+                x = x.detach().cpu().numpy()
+            a = np.ascontiguousarray(x, dtype=np.float64)
+            if a.ndim != 1 or a.size != n or (check_finite and not np.all(np.isfinite(a))):
+                raise ValueError(f"Energy::eval: {name} must have num_dofs finite entries")
+            self.array = a
+            self.ptr, self.mem = N.vptr(a), N.MEM_HOST
+
+
+class VolumetricFemEnergyTetP1(Energy):
+    """VolumetricFemEnergy[NeoHookean, TetP1Basis, TetCentroidQuadrature] on one GPU."""
+
+    def __init__(self, displacement_map, rest_position_fields, Fp, theta, batch_size=256):
+        if isinstance(batch_size, bool) or int(batch_size) <= 0:
+            raise ValueError("MeshEnergy: invalid batch size")
+        if not isinstance(displacement_map, VertexDofMap) or displacement_map.dofs_per_vertex != 3:
+            raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
+        self.batch_size = int(batch_size)
+        T = displacement_map.num_elements
+        V = displacement_map.num_vertices
+        X, Xe = _rest_geometry(rest_position_fields, V, T)
+        th = _sample_fields(theta, T, 2, "theta")
+        if th is None:
+            raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
+        fp = _sample_fields(Fp, T, 9, "Fp")
+        if fp is not None:
+            eye = np.eye(3).ravel()
+            if (fp.ndim == 1 and np.array_equal(fp, eye)) or (fp.ndim == 2 and np.all(fp == eye)):
+                fp = None  # identity plastic field: the record carries no Fp^-1
+            elif fp.ndim == 1:
+                fp = np.ascontiguousarray(np.broadcast_to(fp, (T, 9)))
+        self._init(V, displacement_map.cells, X, Xe, th, fp)
+        self.map = displacement_map
+
+    @classmethod
+    def from_arrays(cls, X, tets, theta, Fp=None, batch_size=256):
+        """Builds the energy from rest positions (V, 3), cells (T, 4) and theta (2,) or (T, 2)."""
+        from .mesh import TetTopology
+
+        X = np.asarray(X, dtype=np.float64).reshape(-1, 3)
+        topo = TetTopology(X.shape[0], tets)
+        return cls(VertexDofMap(topo, 3), X, Fp, theta, batch_size)
+
+    def _init(self, V, cells, X, Xe, theta, Fp):
+        self._h = None
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        T = cells.shape[0]
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        per_element = 1 if theta.ndim == 2 else 0
+        if Fp is not None:
+            Fp = np.ascontiguousarray(Fp, dtype=np.float64).reshape(T, 9)
+        if X is None and Xe is None:
+            raise ValueError("VolumetricFemEnergy: missing rest positions")
+        h = ctypes.c_void_p()
+        self.device = _device_index()
+        N.check(N.lib.lpg_fem_create(V, N.dptr(X), T, N.iptr(cells), N.dptr(Xe), N.dptr(theta), per_element,
+                                     N.dptr(Fp), self.device, ctypes.byref(h)))
+        self._h = h
+        self._theta = theta
+        V_, T_, n_ = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nnzb, nnz = ctypes.c_int64(), ctypes.c_int64()
+        N.check(N.lib.lpg_fem_sizes(h, ctypes.byref(V_), ctypes.byref(T_), ctypes.byref(n_), ctypes.byref(nnzb),
+                                    ctypes.byref(nnz)))
+        self.num_vertices, self.num_elements, self.num_dofs = V_.value, T_.value, n_.value
+        self.nnzb, self.nnz = nnzb.value, nnz.value
+        self._csc = None
+        self._bsr = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            N.lib.lpg_fem_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- patterns ----
+    def pattern_csc(self):
+        if self._csc is None:
+            outer = np.empty(self.num_dofs + 1, dtype=np.int32)
+            inner = np.empty(self.nnz, dtype=np.int32)
+            N.check(N.lib.lpg_fem_pattern_csc(self._h, N.iptr(outer), N.iptr(inner)))
+            self._csc = (outer, inner)
+        return self._csc
+
+    def pattern_bsr(self):
+        if self._bsr is None:
+            row_ptr = np.empty(self.num_vertices + 1, dtype=np.int32)
+            col_idx = np.empty(self.nnzb, dtype=np.int32)
+            N.check(N.lib.lpg_fem_pattern_bsr(self._h, N.iptr(row_ptr), N.iptr(col_idx)))
+            self._bsr = (row_ptr, col_idx)
+        return self._bsr
+
+    # ---- Energy interface ----
+    def _set_stream_for(self, *inputs):
+        """Device inputs: run on torch's current stream so their producers are ordered first."""
+        if any(i is not None and i.mem == N.MEM_DEVICE for i in inputs):
+            import torch
+
+            N.check(N.lib.lpg_fem_set_stream(self._h, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        else:
+            N.check(N.lib.lpg_fem_set_stream(self._h, None))
+
+    def eval(self, x, gradient=False, hessian=None, precision="f64"):
+        """(value, gradient or None, csc_matrix or None) in one assembly."""
+        import scipy.sparse as sp
+
+        kind = _hessian_kind(hessian)
+        prec = _precision(precision)
+        xi = _Input(x, self.num_dofs)
+        self._set_stream_for(xi)
+        E = ctypes.c_double()
+        g = np.empty(self.num_dofs) if gradient else None
+        vals = np.empty(self.nnz, dtype=np.float64 if prec == N.PRECISION_F64 else np.float32) if kind else None
+        N.check(N.lib.lpg_fem_eval(self._h, xi.ptr, N.MEM_HOST if xi.mem == N.MEM_HOST else N.MEM_DEVICE,
+                                   ctypes.byref(E), N.vptr(g) if xi.mem == N.MEM_HOST else None, kind, prec,
+                                   N.LAYOUT_CSC, N.vptr(vals), N.MEM_HOST))
+        if g is not None and xi.mem == N.MEM_DEVICE:
+            g = self.eval_device(xi.tensor, gradient=True)[1].cpu().numpy()
+        H = None
+        if kind:
+            outer, inner = self.pattern_csc()
+            H = sp.csc_matrix((vals.astype(np.float64, copy=False), inner, outer), shape=(self.num_dofs,) * 2)
+        return E.value, g, H
+
+    def eval_value(self, x):
+        return self.eval(x)[0]
+
+    def eval_gradient(self, x):
+        return self.eval(x, gradient=True)[1]
+
+    def eval_hessian(self, x, kind=HessianKind.Exact):
+        return self.eval(x, hessian=kind)[2]
+
+    def max_feasible_step(self, x, dx):
+        xi = _Input(x, self.num_dofs, "x")
+        di = _Input(dx, self.num_dofs, "dx")
+        if xi.mem != di.mem:
+            raise ValueError("max_feasible_step: x and dx must live on the same device")
+        self._set_stream_for(xi, di)
+        a = ctypes.c_double()
+        N.check(N.lib.lpg_fem_feasible_step(self._h, xi.ptr, di.ptr, xi.mem, ctypes.byref(a)))
+        return a.value
+
+    def element_energies(self, x):
+        xi = _Input(x, self.num_dofs)
+        out = np.empty(self.num_elements)
+        self._set_stream_for(xi)
+        if xi.mem == N.MEM_DEVICE:
+            import torch
+
+            t = torch.empty(self.num_elements, dtype=torch.float64, device=xi.tensor.device)
+            N.check(N.lib.lpg_fem_element_energies(self._h, xi.ptr, N.MEM_DEVICE, N.vptr(t)))
+            return t
+        N.check(N.lib.lpg_fem_element_energies(self._h, xi.ptr, N.MEM_HOST, N.vptr(out)))
+        return out
+
+    # ---- device-resident evaluation ----
+    def eval_device(self, u, gradient=True, hessian=None, precision="f64", layout="bsr", grad_out=None,
+                    hess_out=None):
+        """Energy (float), gradient and Hessian values as CUDA tensors, without host copies.
+
+        ``u`` is a CUDA float64 tensor of num_dofs entries. The Hessian values come in
+        block-CSR order (nnzb blocks of 3x3, row-major) or the reference's CSC order.
+        """
+        import torch
+
+        kind = _hessian_kind(hessian)
+        prec = _precision(precision)
+        lay = N.LAYOUT_BSR if layout == "bsr" else N.LAYOUT_CSC
+        xi = _Input(u, self.num_dofs)
+        if xi.mem != N.MEM_DEVICE:
+            raise ValueError("eval_device requires a CUDA tensor")
+        dev = xi.tensor.device
+        g = None
+        if gradient:
+            g = grad_out if grad_out is not None else torch.empty(self.num_dofs, dtype=torch.float64, device=dev)
+        H = None
+        if kind:
+            dt = torch.float64 if prec == N.PRECISION_F64 else torch.float32
+            H = hess_out if hess_out is not None else torch.empty(self.nnz, dtype=dt, device=dev)
+        self._set_stream_for(xi)
+        E = ctypes.c_double()
+        N.check(N.lib.lpg_fem_eval(self._h, xi.ptr, N.MEM_DEVICE, ctypes.byref(E), N.vptr(g), kind, prec, lay,
+                                   N.vptr(H), N.MEM_DEVICE))
+        return E.value, g, H
+
+
+def _hessian_kind(hessian):
+    if hessian is None or hessian is False:
+        return N.HESSIAN_NONE
+    k = int(hessian)
+    if k not in (N.HESSIAN_EXACT, N.HESSIAN_PROJECTED):
+        raise ValueError("Energy: invalid Hessian kind")
+    return k
+
+
+def _precision(p):
+    if p in ("f64", "fp64", N.PRECISION_F64):
+        return N.PRECISION_F64
+    if p in ("mixed", "fp32", N.PRECISION_MIXED):
+        return N.PRECISION_MIXED
+    raise ValueError("precision must be 'f64' or 'mixed'")
+
+
+class VolumetricFemForceMaterialResponseTetP1:
+    """Force response p -> g(u; p) at a fixed displacement, differentiated in theta.
+
+    Mirrors VolumetricFemForceMaterialResponse[NeoHookean, TetP1Basis, TetCentroidQuadrature]
+    (src/core/fem/assembly/volumetric_fem_force_material_response.hpp; binding
+    src/binding/detail/fem_helpers.hpp:76-98). ConstantDofMap shares one [lambda, mu];
+    ElementDofMap gives each element its own block.
+    """
+
+    def __init__(self, parameter_map, displacement_map, rest_position_fields, displacement, Fp, batch_size=256):
+        if isinstance(batch_size, bool) or int(batch_size) <= 0:
+            raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
+        if not isinstance(parameter_map, (ConstantDofMap, ElementDofMap)):
+            raise TypeError("parameter_map must be a ConstantDofMap or an ElementDofMap")
+        width = parameter_map.num_dofs if isinstance(parameter_map, ConstantDofMap) else parameter_map.dofs_per_element
+        if parameter_map.num_elements != displacement_map.num_elements:
+            raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
+        if width != 2:
+            raise ValueError("VolumetricFemForceResponse: invalid parameter count")
+        self.per_element = isinstance(parameter_map, ElementDofMap)
+        self.parameter_map = parameter_map
+        u = np.ascontiguousarray(displacement, dtype=np.float64)
+        if u.size != displacement_map.num_dofs or not np.all(np.isfinite(u)):
+            raise ValueError("VolumetricFemForceResponse: incompatible map, displacement or responses")
+        # theta does not enter d g / d theta (P is linear in theta); any valid value builds the mesh.
+        self._energy = VolumetricFemEnergyTetP1(displacement_map, rest_position_fields, Fp, np.array([1.0, 1.0]))
+        self.displacement = u
+        self.num_inputs = parameter_map.num_dofs
+        self.num_outputs = displacement_map.num_dofs
+
+    def _check_p(self, p):
+        p = np.asarray(p, dtype=np.float64).ravel()
+        if p.size != self.num_inputs:
+            raise ValueError("Response: p must have num_inputs entries")
+        th = p.reshape(-1, 2)
+        if not np.all(np.isfinite(th)) or np.any(th[:, 0] < 0) or np.any(th[:, 1] <= 0):
+            raise ValueError("NeoHookean requires finite lambda >= 0 and mu > 0")
+        return p
+
+    def eval_vjp(self, p, w):
+        """(d g / d theta)^T w: (2,) for a ConstantDofMap, (2 T,) for an ElementDofMap."""
+        self._check_p(p)
+        wv = np.ascontiguousarray(w, dtype=np.float64)
+        if wv.size != self.num_outputs:
+            raise ValueError("Response: weights must have num_outputs entries")
+        T = self._energy.num_elements
+        out = np.empty(2 * T if self.per_element else 2)
+        N.check(N.lib.lpg_fem_force_vjp_theta(self._energy.handle, N.vptr(self.displacement), N.vptr(wv), N.MEM_HOST,
+                                              1 if self.per_element else 0, N.vptr(out)))
+        return out
+
+
+VolumetricFemEnergy = Template("VolumetricFemEnergy",
+                               {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyTetP1})
+VolumetricFemForceMaterialResponse = Template(
+    "VolumetricFemForceMaterialResponse",
+    {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceMaterialResponseTetP1})
+
+# A constant field helper matching the reference tests' constant_fields(value, count).
+def constant_fields(value, count):
+    v = np.asarray(value, dtype=np.float64).ravel()
+    return [AffineResponse(np.zeros((v.size, 3)), v)] * count

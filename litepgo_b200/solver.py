@@ -1,0 +1,197 @@
+"""Nonlinear solvers mirroring litepgo.solver for the volumetric FEM path.
+
+newton_solve(energy, fixed, x0, options, solver=None, on_iteration=None) keeps the binding's
+signature (src/binding/solver/newton.cpp:62-82) and the semantics of newton.cpp:112-183;
+the direct sparse solver is replaced by block-Jacobi PCG on the GPU block-CSR Hessian, so
+``solver`` must be None. NewtonOptions keeps the reference fields and defaults
+(src/core/solver/newton.hpp:13-20) and adds the GPU linear-solve controls.
+
+StaticEquilibriumResponse(num_parameters, fixed, initial, options, make_energy,
+make_response) mirrors src/core/solver/static_equilibrium_response.hpp:15-32: p -> u*(p)
+from the same initial state on every call; eval_vjp solves the adjoint with the EXACT
+Hessian and returns -(dg/dtheta)^T lambda (static_equilibrium_response.cpp:43-88).
+"""
+
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _native as N
+from .energy import HessianKind, WeightedSumEnergy
+
+__all__ = ["NewtonOptions", "NewtonStatus", "NewtonResult", "newton_solve", "StaticEquilibriumResponse"]
+
+
+class NewtonStatus(enum.IntEnum):
+    Converged = 0
+    MaxIterations = 1
+    StepTooSmall = 2
+    NoDescentDirection = 3
+
+
+class NewtonOptions:
+    """Options of newton_solve.
+
+    Reference fields: gradient_tolerance (required), max_iterations=50,
+    hessian=HessianKind.Projected, max_line_search_steps=30, line_search_shrink=0.5.
+    GPU additions: stop_rule ("max_abs": max |g_free| <= tol, the reference rule; "relative":
+    ||g_free||_2 <= tol ||g_free(x0)||_2), accept_rule ("noise": the reference's decrease
+    within 16 eps; "armijo": sufficient decrease c = 1e-4 plus that noise), precision
+    ("f64" or "mixed": FP32 Hessian and PCG, FP64 energy and residual), cg_tolerance (cap of
+    the PCG forcing term) and cg_max_iterations.
+    """
+
+    def __init__(self, gradient_tolerance=float("nan"), max_iterations=50, hessian=HessianKind.Projected,
+                 max_line_search_steps=30, line_search_shrink=0.5, stop_rule="max_abs", accept_rule="noise",
+                 precision="f64", cg_tolerance=1e-2, cg_max_iterations=20000):
+        self.gradient_tolerance = gradient_tolerance
+        self.max_iterations = max_iterations
+        self.hessian = hessian
+        self.max_line_search_steps = max_line_search_steps
+        self.line_search_shrink = line_search_shrink
+        self.stop_rule = stop_rule
+        self.accept_rule = accept_rule
+        self.precision = precision
+        self.cg_tolerance = cg_tolerance
+        self.cg_max_iterations = cg_max_iterations
+
+    def to_c(self):
+        o = N.NewtonOptionsC()
+        o.gradient_tolerance = float(self.gradient_tolerance)
+        o.max_iterations = int(self.max_iterations)
+        o.hessian = int(self.hessian)
+        o.max_line_search_steps = int(self.max_line_search_steps)
+        o.line_search_shrink = float(self.line_search_shrink)
+        o.stop_rule = {"max_abs": 0, "relative": 1}[self.stop_rule]
+        o.accept_rule = {"noise": 0, "armijo": 1}[self.accept_rule]
+        o.precision = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
+        o.cg_tolerance = float(self.cg_tolerance)
+        o.cg_max_iterations = int(self.cg_max_iterations)
+        return o
+
+
+class NewtonResult:
+    def __init__(self, status, x, energy, gradient_norm, iterations, gradient_norm0=0.0, cg_iterations=0,
+                 line_search_evaluations=0, seconds=0.0):
+        self.status = NewtonStatus(status)
+        self.x = x
+        self.energy = energy
+        self.gradient_norm = gradient_norm
+        self.iterations = iterations
+        self.gradient_norm0 = gradient_norm0
+        self.cg_iterations = cg_iterations
+        self.line_search_evaluations = line_search_evaluations
+        self.seconds = seconds
+
+    def __repr__(self):
+        return (f"NewtonResult(status={self.status.name}, iterations={self.iterations}, energy={self.energy:.6e}, "
+                f"gradient_norm={self.gradient_norm:.3e}, cg_iterations={self.cg_iterations})")
+
+
+def _split_energy(energy):
+    from .fem import VolumetricFemEnergyTetP1
+
+    if isinstance(energy, VolumetricFemEnergyTetP1):
+        return energy, None
+    if isinstance(energy, WeightedSumEnergy):
+        fem, f = energy.split()
+        return fem, (f if np.any(f) else None)
+    raise TypeError("newton_solve: energy must be a VolumetricFemEnergy or a WeightedSumEnergy of one plus loads")
+
+
+def newton_solve(energy, fixed, x0, options, solver=None, on_iteration=None):
+    """Minimises energy over the free DOFs of ``fixed`` from x0 on the GPU."""
+    if solver is not None:
+        raise ValueError("newton_solve: the GPU path solves with block-Jacobi PCG; pass solver=None")
+    if on_iteration is not None:
+        raise ValueError("newton_solve: per-iteration callbacks are not available on the GPU path")
+    fem, f = _split_energy(energy)
+    n = fem.num_dofs
+    if fixed.num_dofs != n:
+        raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
+    is_dev = hasattr(x0, "is_cuda") and x0.is_cuda
+    if is_dev:
+        import torch
+
+        x0t = x0.detach().contiguous()
+        if x0t.dtype != torch.float64 or x0t.numel() != n:
+            raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
+        xo = torch.empty_like(x0t)
+        ft = None if f is None else torch.as_tensor(f, device=x0t.device)
+        N.check(N.lib.lpg_fem_set_stream(fem.handle, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        ptrs = (N.vptr(ft), N.vptr(x0t), N.vptr(xo), N.MEM_DEVICE)
+    else:
+        x0a = np.ascontiguousarray(x0, dtype=np.float64)
+        if x0a.size != n:
+            raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
+        xo = np.empty(n)
+        fa = None if f is None else np.ascontiguousarray(f)
+        N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
+        ptrs = (N.vptr(fa), N.vptr(x0a), N.vptr(xo), N.MEM_HOST)
+    fixed_arr = np.ascontiguousarray(fixed.fixed_dofs, dtype=np.int32)
+    res = N.NewtonResultC()
+    opts = options.to_c()
+    N.check(N.lib.lpg_newton_solve(fem.handle, N.iptr(fixed_arr), int(fixed_arr.size), ptrs[0], ptrs[1], ptrs[3],
+                                   ctypes.byref(opts), ptrs[2], ctypes.byref(res)))
+    return NewtonResult(res.status, xo, res.energy, res.gradient_norm, res.iterations, res.gradient_norm0,
+                        res.cg_iterations, res.line_search_evaluations, res.seconds)
+
+
+class StaticEquilibriumResponse:
+    """p -> equilibrium displacement; eval_vjp by one adjoint solve on the GPU."""
+
+    def __init__(self, num_parameters, fixed, initial, options, make_energy, make_response, precision="f64",
+                 adjoint_tolerance=1e-10):
+        initial = np.asarray(initial, dtype=np.float64)
+        o = options
+        if (int(num_parameters) <= 0 or initial.size != fixed.num_dofs or not np.all(np.isfinite(initial))
+                or make_energy is None or make_response is None or not np.isfinite(o.gradient_tolerance)
+                or o.gradient_tolerance < 0 or o.max_iterations < 0 or o.max_line_search_steps < 1
+                or not (0 < o.line_search_shrink < 1)):
+            raise ValueError("StaticEquilibriumResponse: invalid initial state, options or callbacks")
+        self.num_inputs = int(num_parameters)
+        self.num_outputs = fixed.num_dofs
+        self.fixed = fixed
+        self.initial = initial.copy()
+        self.options = options
+        self.make_energy = make_energy
+        self.make_response = make_response
+        self.precision = precision
+        self.adjoint_tolerance = adjoint_tolerance
+
+    def _solve(self, p):
+        p = np.asarray(p, dtype=np.float64).ravel()
+        if p.size != self.num_inputs or not np.all(np.isfinite(p)):
+            raise ValueError("Response: p must have num_inputs finite entries")
+        potential = self.make_energy(p)
+        if potential is None or potential.num_dofs != self.num_outputs:
+            raise ValueError("StaticEquilibriumResponse: incompatible energy")
+        result = newton_solve(potential, self.fixed, self.initial, self.options)
+        if result.status != NewtonStatus.Converged:
+            raise ValueError("StaticEquilibriumResponse: equilibrium did not converge")
+        return p, potential, result.x
+
+    def eval_value(self, p):
+        return self._solve(p)[2]
+
+    def eval_vjp(self, p, w):
+        p, potential, x = self._solve(p)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        if w.size != self.num_outputs:
+            raise ValueError("Response: weights must have num_outputs entries")
+        if self.fixed.num_free == 0:
+            return np.zeros(self.num_inputs)
+        force = self.make_response(x)
+        if force is None or force.num_inputs != self.num_inputs or force.num_outputs != self.num_outputs:
+            raise ValueError("StaticEquilibriumResponse: incompatible force response")
+        fem, _ = _split_energy(potential)
+        T = fem.num_elements
+        out = np.empty(2 * T if force.per_element else 2)
+        fixed_arr = np.ascontiguousarray(self.fixed.fixed_dofs, dtype=np.int32)
+        prec = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
+        N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
+        N.check(N.lib.lpg_adjoint_theta(fem.handle, N.vptr(x), N.vptr(w), N.iptr(fixed_arr), int(fixed_arr.size),
+                                        N.MEM_HOST, prec, float(self.adjoint_tolerance),
+                                        1 if force.per_element else 0, N.vptr(out), None))
+        return out
