@@ -379,6 +379,26 @@ def run_ours(args):
     return 0
 
 
+def run_kernels_only():
+    """Three launches each of the FP64 exact, FP32 exact and FP64 projected assembly on the
+    bench workload, nothing else (the command profiled by ncu)."""
+    import torch
+
+    from litepgo_b200 import energy, fem, workloads
+
+    torch.cuda.set_device(0)
+    g = workloads.gravity_box(N_CUBES, seed=0)
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(g["X"], g["tets"], g["theta"])
+    u = torch.as_tensor(state(g["X"]), device="cuda")
+    for kind, prec in ((energy.HessianKind.Exact, "f64"), (energy.HessianKind.Exact, "mixed"),
+                       (energy.HessianKind.Projected, "f64")):
+        for _ in range(3):
+            e.eval_device(u, gradient=True, hessian=kind, precision=prec)
+    torch.cuda.synchronize()
+    print("kernels ok")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,7 +407,11 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-newton", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only-kernels", action="store_true",
+                    help="run 3 evaluations of each assembly variant and exit (a short command for ncu)")
     args = ap.parse_args()
+    if args.only_kernels:
+        return run_kernels_only()
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -229,6 +229,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
     double e_acc = 0.0;
     for (int q = lane; q < np; q += 32) {
         const int pe = m.pair_elem[p0 + q];
+        // Slot-sorted positions of this pair's four blocks (one byte each).
+        const unsigned pos4 = __ldg(reinterpret_cast<const unsigned*>(m.contrib) + p0 + q);
         const int e = pe & ((1 << 30) - 1);
         const int la = static_cast<unsigned>(pe) >> 30;
         const int4 tv = __ldg(m.tets + e);
@@ -266,9 +268,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
             const R lv = X::mul(k.vol, k.lam);
             const R pv = X::mul(k.vol, p);
             const R mv = X::mul(k.vol, k.mu);
-            R* out = sH + 36 * q;
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
+                R* out = sH + 9 * ((pos4 >> (8 * b)) & 0xffu);
                 const R gg = X::fma(na[2], k.n[b][2], X::fma(na[1], k.n[b][1], X::mul(na[0], k.n[b][0])));
                 const R mg = X::mul(mv, gg);
 #pragma unroll
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
                         const R y = X::mul(h[b][i], ha[kk]);
                         R v = X::fma(lv, x, X::mul(-pv, y));
                         if (i == kk) v = X::add(v, mg);
-                        out[9 * b + 3 * i + kk] = v;
+                        out[3 * i + kk] = v;
                     }
             }
         } else if (WH == 2) {
@@ -297,7 +299,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
                     for (int jp = 0; jp < 3; ++jp) s = X::fma(qbasis<R>(la, jp), __ldg(Mp + sym9(3 * jp + i, c)), s);
                     Y[i][c] = s;
                 }
-            R* out = sH + 36 * q;
 #pragma unroll
             for (int b = 0; b < 4; ++b)
 #pragma unroll
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
                         R s = 0;
 #pragma unroll
                         for (int lp = 0; lp < 3; ++lp) s = X::fma(qbasis<R>(b, lp), Y[i][3 * lp + kk], s);
-                        out[9 * b + 3 * i + kk] = s;
+                        sH[9 * ((pos4 >> (8 * b)) & 0xffu) + 3 * i + kk] = s;
                     }
         }
     }
@@ -343,7 +344,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
     const int nslots = meta->spre[nr];
     if (WH) {
         const uint16_t* soff = m.slot_off + m.tile_slot_ptr[tile] + tile;
-        const uint8_t* con = m.contrib + 4 * static_cast<size_t>(p0);
         HT* hout = reinterpret_cast<HT*>(a.hess);
         int j = 0;
         for (int o = lane; o < 9 * nslots; o += 32) {
@@ -352,10 +352,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
             while (meta->spre[j + 1] <= s) ++j;
             const int c0 = soff[s], c1 = soff[s + 1];
             R v = 0;
-            for (int c = c0; c < c1; ++c) {
-                const int bt = con[c];
-                v = X::add(v, sH[36 * (bt >> 2) + 9 * (bt & 3) + kk]);
-            }
+            for (int c = c0; c < c1; ++c) v = X::add(v, sH[9 * c + kk]);
             if (!X::finite(v)) st |= ST_NONFINITE_OUT;
             const int qs = s - meta->spre[j];
             size_t pos;
@@ -368,12 +365,14 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const Dev
             hout[pos] = static_cast<HT>(v);
         }
     }
-    if (WG && lane < 3 * nr) {
-        const int j = lane / 3, c = lane - 3 * j;
-        R v = 0;
-        for (int q = meta->ppre[j]; q < meta->ppre[j + 1]; ++q) v = X::add(v, sg[3 * q + c]);
-        if (!X::finite(v)) st |= ST_NONFINITE_OUT;
-        a.grad[3 * static_cast<size_t>(meta->row[j]) + c] = static_cast<double>(v);
+    if (WG) {
+        for (int o = lane; o < 3 * nr; o += 32) {
+            const int j = o / 3, c = o - 3 * j;
+            R v = 0;
+            for (int q = meta->ppre[j]; q < meta->ppre[j + 1]; ++q) v = X::add(v, sg[3 * q + c]);
+            if (!X::finite(v)) st |= ST_NONFINITE_OUT;
+            a.grad[3 * static_cast<size_t>(meta->row[j]) + c] = static_cast<double>(v);
+        }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) e_acc += __shfl_xor_sync(0xffffffffu, e_acc, off);

@@ -44,8 +44,10 @@ struct HostPlan {
     std::vector<int32_t> tile_row_ptr;       // ntiles+1
     std::vector<int32_t> tile_rows;          // rows of each tile, ascending
     std::vector<int32_t> tile_slot_ptr;      // ntiles+1 (cumulative slot counts)
-    std::vector<uint16_t> slot_off;          // nnzb + ntiles: contributor offsets per tile slot
-    std::vector<uint8_t> contrib;            // 4 * npairs: (pair_local << 2) | b, per slot in element order
+    std::vector<uint16_t> slot_off;          // nnzb + ntiles: start of each tile slot in the slot-sorted blocks
+    // 4 * npairs: position of block b of each pair in its tile's slot-sorted block list; a slot's
+    // blocks are contiguous there and ordered by element, the reference's summation order.
+    std::vector<uint8_t> contrib;
     std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
     int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
     int64_t nnzb() const { return static_cast<int64_t>(col_idx.size()); }

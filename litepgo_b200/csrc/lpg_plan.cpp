@@ -144,7 +144,11 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
             slots += nb_v;
         }
         offs.push_back(static_cast<uint16_t>(tile_contrib.size()));
-        std::copy(tile_contrib.begin(), tile_contrib.end(), p.contrib.begin() + 4 * pair_base);
+        // Inverse of the slot-sorted contributor list: where pair `local` puts block b.
+        for (size_t idx = 0; idx < tile_contrib.size(); ++idx) {
+            const int c = tile_contrib[idx];
+            p.contrib[4 * pair_base + 4 * (c >> 2) + (c & 3)] = static_cast<uint8_t>(idx);
+        }
         p.slot_off.insert(p.slot_off.end(), offs.begin(), offs.end());
         p.tile_pair_ptr[t + 1] = static_cast<int32_t>(pair_cursor);
         p.tile_row_ptr[t + 1] = static_cast<int32_t>(p.tile_rows.size());

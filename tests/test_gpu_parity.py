@@ -116,7 +116,7 @@ def test_mixed_precision_error_bounds(cfg1):
     Er, gr, vr = orc.eval(w["u"], True, 1)
     assert abs(E - Er) <= 2e-6 * abs(Er)
     assert rel_err(g, gr) <= 2e-5
-    assert rel_err(H.data, vr) <= 2e-6
+    assert rel_err(H.data, vr) <= 1e-5
     _, _, Hp = gpu.eval(w["u"], hessian=Projected, precision="mixed")
     _, _, vp = orc.eval(w["u"], False, 2)
     assert rel_err(Hp.data, vp) <= 1e-4
