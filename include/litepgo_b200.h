@@ -168,6 +168,21 @@ int lpg_fem_element_energies(lpg_fem_t h, const double* u, int io_mem, double* e
 int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io_mem, double* alpha);
 
 /*
+ * The feasible step of lpg_fem_feasible_step, for callers that cannot allocate device memory
+ * when they call it (inside a CUDA stream capture, or under a framework that owns the device
+ * memory pool). This entry point has no counterpart in the reference: it is the same
+ * computation with its scratch in a fixed ~512 KB array inside the library image instead of
+ * a cudaMalloc'd buffer, so it calls no cudaMalloc / cudaFree. u and du are DEVICE arrays of
+ * num_dofs doubles; *alpha is written on the host. Limits and rules:
+ *   - meshes of at most 16,777,216 tets; larger ones fail with LPG_EINVAL;
+ *   - the array is shared by every call on a device and keeps the last call's contents
+ *     (each call clears what it needs), so calls that overlap on the GPU race: order them;
+ *   - the first call on a device looks the array's device address up (cudaGetSymbolAddress
+ *     with that device current); make that first call before any stream capture begins.
+ */
+int lpg_fem_feasible_step_noalloc(lpg_fem_t h, const double* u, const double* du, double* alpha);
+
+/*
  * Parameter VJP of the force response: per element [d/dlambda, d/dmu] of w . g(u).
  * Replaces VolumetricFemForceMaterialResponse::eval_vjp
  *   (src/core/fem/assembly/detail/volumetric_fem_force_response.hpp:155-179 through

@@ -75,6 +75,7 @@ SIGNATURES = [
     ("lpg_fem_time_eval", _int, [_vp, _vp, _vp, _int, _int, _int, _vp, _int, _int, _dp, _dp]),
     ("lpg_fem_element_energies", _int, [_vp, _vp, _int, _vp]),
     ("lpg_fem_feasible_step", _int, [_vp, _vp, _vp, _int, _dp]),
+    ("lpg_fem_feasible_step_noalloc", _int, [_vp, _vp, _vp, _dp]),
     ("lpg_fem_force_vjp_theta", _int, [_vp, _vp, _vp, _int, _int, _vp]),
     ("lpg_newton_default_options", None, [ctypes.POINTER(NewtonOptionsC)]),
     ("lpg_newton_solve", _int, [_vp, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC), _vp,
