@@ -267,7 +267,10 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         m.tile_row_ptr = upload(h->b_tile_row_ptr, p.tile_row_ptr);
         m.tile_rows = upload(h->b_tile_rows, p.tile_rows);
         m.tile_slot_ptr = upload(h->b_tile_slot_ptr, p.tile_slot_ptr);
-        m.slot_off = upload(h->b_slot_off, p.slot_off);
+        m.slot_desc = upload(h->b_slot_desc, p.slot_desc);
+        m.diag_slot = upload(h->b_diag_slot, p.diag_slot);
+        m.unused_rows = upload(h->b_unused, p.unused_rows);
+        m.num_unused = static_cast<int>(p.unused_rows.size());
         m.contrib = upload(h->b_contrib, p.contrib);
         m.pair_elem = upload(h->b_pair_elem, p.pair_elem);
         std::vector<int32_t> tv(tets, tets + 4 * static_cast<size_t>(T));

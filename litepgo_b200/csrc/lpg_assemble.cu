@@ -18,6 +18,7 @@
 // Block entries are formed with explicit round-to-nearest products so that H_ba is the exact
 // transpose of H_ab; the assembled matrix is bitwise symmetric.
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -27,6 +28,21 @@ namespace lpg {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
+
+// Occupancy targets of the assembly kernel (resident blocks per SM the register allocation must
+// allow) and whether its warps persist over several tiles; tuned per precision on B200.
+#ifndef LPG_ASSEMBLE_MIN_BLOCKS_F64
+#define LPG_ASSEMBLE_MIN_BLOCKS_F64 6
+#endif
+#ifndef LPG_ASSEMBLE_MIN_BLOCKS_F32
+#define LPG_ASSEMBLE_MIN_BLOCKS_F32 8
+#endif
+#ifndef LPG_ASSEMBLE_PERSISTENT
+#define LPG_ASSEMBLE_PERSISTENT 1
+#endif
+template <typename R> struct MinBlocks;
+template <> struct MinBlocks<double> { static constexpr int value = LPG_ASSEMBLE_MIN_BLOCKS_F64; };
+template <> struct MinBlocks<float> { static constexpr int value = LPG_ASSEMBLE_MIN_BLOCKS_F32; };
 
 template <typename R> struct M;
 template <> struct M<double> {
@@ -85,6 +101,10 @@ template <typename R> struct Kin {
 };
 
 // Returns status bits. u is FP64; edge differences are formed in FP64 and rounded once.
+// FP64: det F and log det F as the reference computes them (neo_hookean.cpp:14-23). FP32:
+// det F - 1 from the invariants of the displacement gradient and log1p, which keeps log J
+// accurate near the rest state. Validity is checked once on J; the rare failure path then
+// tells a non-finite input from a non-finite F and from det F <= 0.
 template <typename R>
 __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const int4 tv, const double* __restrict__ u,
                                                Kin<R>& k) {
@@ -93,21 +113,16 @@ __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const in
     R rec[12];
     load_rec<R>(rec_ptr<R>(m), e, rec);
     const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
-    double u0[3];
+    double uu[4][3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) u0[i] = u[3 * static_cast<size_t>(vs[0]) + i];
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) uu[c][i] = __ldg(u + 3 * static_cast<size_t>(vs[c]) + i);
     R Ds[3][3]; // Ds[i][c] = u_{c+1,i} - u_{0,i}
-    bool in_ok = isfinite(u0[0]) && isfinite(u0[1]) && isfinite(u0[2]);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const double uc = u[3 * static_cast<size_t>(vs[c + 1]) + i];
-            in_ok = in_ok && isfinite(uc);
-            Ds[i][c] = static_cast<R>(uc - u0[i]);
-        }
-    }
-    if (!in_ok) st |= ST_BAD_INPUT;
+        for (int i = 0; i < 3; ++i) Ds[i][c] = static_cast<R>(uu[c + 1][i] - uu[0][i]);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -117,8 +132,7 @@ __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const in
     k.vol = rec[9];
     k.lam = rec[10];
     k.mu = rec[11];
-    if (!(X::finite(k.lam) && X::finite(k.mu) && k.lam >= R(0) && k.mu > R(0))) st |= ST_BAD_THETA;
-    // Displacement gradient H = Ds G (G rows = grad N_1..3), F = offset + H.
+    if (!(k.lam >= R(0) && k.mu > R(0) && k.lam < R(INFINITY) && k.mu < R(INFINITY))) st |= ST_BAD_THETA;
     R H[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -126,14 +140,37 @@ __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const in
         for (int j = 0; j < 3; ++j)
             H[3 * i + j] = X::fma(Ds[i][2], rec[6 + j], X::fma(Ds[i][1], rec[3 + j], X::mul(Ds[i][0], rec[j])));
     const R* fpi = fpinv_ptr<R>(m);
-    R J, sqm3; // J and |F|^2 - 3
     if (fpi == nullptr) {
 #pragma unroll
         for (int t = 0; t < 9; ++t) k.F[t] = H[t];
         k.F[0] += R(1);
         k.F[4] += R(1);
         k.F[8] += R(1);
-        // det(I + H) - 1 = tr H + (sum of principal 2x2 minors of H) + det H, free of cancellation.
+    } else {
+        const R* o = fpi + 9 * static_cast<size_t>(e);
+#pragma unroll
+        for (int t = 0; t < 9; ++t) k.F[t] = __ldg(o + t) + H[t];
+    }
+    const R* F = k.F;
+    R C[9]; // cofactors: F^-T = C / det F
+    C[0] = F[4] * F[8] - F[5] * F[7];
+    C[1] = F[5] * F[6] - F[3] * F[8];
+    C[2] = F[3] * F[7] - F[4] * F[6];
+    C[3] = F[2] * F[7] - F[1] * F[8];
+    C[4] = F[0] * F[8] - F[2] * F[6];
+    C[5] = F[1] * F[6] - F[0] * F[7];
+    C[6] = F[1] * F[5] - F[2] * F[4];
+    C[7] = F[2] * F[3] - F[0] * F[5];
+    C[8] = F[0] * F[4] - F[1] * F[3];
+    R J, sqm3;
+    if (sizeof(R) == 8 || fpi != nullptr) {
+        J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+        k.logJ = X::log_(J);
+        R ff = 0;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) ff = X::fma(F[t], F[t], ff);
+        sqm3 = ff - R(3);
+    } else {
         const R c1 = H[0] + H[4] + H[8];
         const R c2 = (H[0] * H[4] - H[1] * H[3]) + (H[0] * H[8] - H[2] * H[6]) + (H[4] * H[8] - H[5] * H[7]);
         const R c3 = H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
@@ -145,36 +182,22 @@ __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const in
 #pragma unroll
         for (int t = 0; t < 9; ++t) hh = X::fma(H[t], H[t], hh);
         sqm3 = R(2) * c1 + hh;
-    } else {
-        const R* o = fpi + 9 * static_cast<size_t>(e);
-#pragma unroll
-        for (int t = 0; t < 9; ++t) k.F[t] = __ldg(o + t) + H[t];
-        const R* F = k.F;
-        J = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) + F[2] * (F[3] * F[7] - F[4] * F[6]);
-        k.logJ = X::log_(J);
-        R ff = 0;
-#pragma unroll
-        for (int t = 0; t < 9; ++t) ff = X::fma(F[t], F[t], ff);
-        sqm3 = ff - R(3);
     }
-    bool f_ok = true;
-#pragma unroll
-    for (int t = 0; t < 9; ++t) f_ok = f_ok && X::finite(k.F[t]);
-    if (!f_ok) st |= ST_NONFINITE_F;
-    else if (!(J > R(0)) || !X::finite(J)) st |= ST_BAD_DET;
-    const R* F = k.F;
     const R iJ = R(1) / J;
-    // F^-T = cof(F) / det F.
-    k.FiT[0] = (F[4] * F[8] - F[5] * F[7]) * iJ;
-    k.FiT[1] = (F[5] * F[6] - F[3] * F[8]) * iJ;
-    k.FiT[2] = (F[3] * F[7] - F[4] * F[6]) * iJ;
-    k.FiT[3] = (F[2] * F[7] - F[1] * F[8]) * iJ;
-    k.FiT[4] = (F[0] * F[8] - F[2] * F[6]) * iJ;
-    k.FiT[5] = (F[1] * F[6] - F[0] * F[7]) * iJ;
-    k.FiT[6] = (F[1] * F[5] - F[2] * F[4]) * iJ;
-    k.FiT[7] = (F[2] * F[3] - F[0] * F[5]) * iJ;
-    k.FiT[8] = (F[0] * F[4] - F[1] * F[3]) * iJ;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) k.FiT[t] = C[t] * iJ;
     k.psi = R(0.5) * k.mu * sqm3 - k.mu * k.logJ + R(0.5) * k.lam * k.logJ * k.logJ;
+    if (!(J > R(0) && J < R(INFINITY) && k.psi == k.psi && k.psi < R(INFINITY) && k.psi > R(-INFINITY))) {
+        bool in_ok = true, f_ok = true;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) in_ok = in_ok && isfinite(uu[c][i]);
+#pragma unroll
+        for (int t = 0; t < 9; ++t) f_ok = f_ok && X::finite(F[t]);
+        st |= !in_ok ? ST_BAD_INPUT : !f_ok ? ST_NONFINITE_F : !(J > R(0)) || !X::finite(J) ? ST_BAD_DET
+                                                                                          : ST_NONFINITE_OUT;
+    }
     return st;
 }
 
@@ -200,185 +223,316 @@ struct TileMeta {
     int row[32];
     int slot0[32];
     int nb[32];
-    int spre[33];
-    int ppre[33];
+    int dq[32];   // position of the diagonal block within the row
+    int ppre[33]; // the pairs of row j are [ppre[j], ppre[j + 1])
 };
 
-// Fused element pass + assembly. WG: gradient, WH: Hessian (0 none, 1 exact, 2 from the
-// projected tangents in a.proj), energy always.
+// Shared memory of one warp: off-diagonal blocks [9][3 cap + 1], slot descriptors [3 cap], metadata.
+template <typename R, int WH> __host__ __device__ constexpr size_t smem_per_warp(int cap) {
+    return ((WH ? (9 * static_cast<size_t>(3 * cap + 1) * sizeof(R) + 3 * static_cast<size_t>(cap) * 4) : 0) +
+            sizeof(TileMeta) + 15) / 16 * 16;
+}
+
+// Inclusive scan of the 12 per-pair values (gradient piece, diagonal block) over the lanes of
+// each row segment; segment heads are the set bits of `heads` (bit l = a row starts at lane l).
+// The fixed Hillis-Steele pattern makes the row sums deterministic.
+template <typename R> __device__ __forceinline__ void segmented_scan(R (&v)[12], unsigned heads, int lane) {
+    const unsigned upto = heads & (0xffffffffu >> (31 - lane));
+    const int seg = upto ? 31 - __clz(upto) : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        R t[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) t[k] = __shfl_up_sync(0xffffffffu, v[k], off);
+        if (lane - off >= seg)
+#pragma unroll
+            for (int k = 0; k < 12; ++k) v[k] = M<R>::add(t[k], v[k]);
+    }
+}
+
+// Evaluates pair q of the tile: returns E_e (a = 0 only), leaves g_a and the diagonal block
+// H_aa in v[0..2], v[3..11] and the three off-diagonal blocks at their slot-sorted positions.
 template <typename R, bool WG, int WH>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) assemble_kernel(const DevMesh m, const EvalArgs a) {
+__device__ __forceinline__ unsigned eval_pair(const DevMesh& m, const EvalArgs& a, int pe, unsigned pos4, int4 tv, R* sH,
+                                              int P, R (&v)[12], double& e_acc) {
+    using X = M<R>;
+    const int e = pe & ((1 << 30) - 1);
+    const int la = static_cast<unsigned>(pe) >> 30;
+    Kin<R> k;
+    const unsigned st = kinematics<R>(m, e, tv, a.u, k);
+    if (la == 0) {
+        const R Ee = k.vol * k.psi;
+        e_acc += static_cast<double>(Ee);
+        if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
+    }
+    R na[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) na[j] = la == 0 ? k.n[0][j] : la == 1 ? k.n[1][j] : la == 2 ? k.n[2][j] : k.n[3][j];
+    const R p = X::fma(k.lam, k.logJ, -k.mu);
+    if (WG) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            R s = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) s = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), na[j], s);
+            v[i] = k.vol * s;
+        }
+    }
+    if (WH == 1) {
+        R h[4][3];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                h[b][i] = X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
+        R ha[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) ha[i] = la == 0 ? h[0][i] : la == 1 ? h[1][i] : la == 2 ? h[2][i] : h[3][i];
+        const R lv = X::mul(k.vol, k.lam);
+        const R pv = X::mul(k.vol, p);
+        const R mv = X::mul(k.vol, k.mu);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int pos = (pos4 >> (8 * b)) & 0xffu;
+            const R gg = X::fma(na[2], k.n[b][2], X::fma(na[1], k.n[b][1], X::mul(na[0], k.n[b][0])));
+            const R mg = X::mul(mv, gg);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                    const R x = X::mul(ha[i], h[b][kk]);
+                    const R y = X::mul(h[b][i], ha[kk]);
+                    R val = X::fma(lv, x, X::mul(-pv, y));
+                    if (i == kk) val = X::add(val, mg);
+                    if (b == la)
+                        v[3 + 3 * i + kk] = val;
+                    else
+                        sH[(3 * i + kk) * P + pos] = val;
+                }
+        }
+    } else if (WH == 2) {
+        // Projected: blocks from the clamped per-element tangent Mp (9x9 over (i, j') with
+        // index 3 j' + i, packed upper triangle) in the orthonormal basis q of {sum = 0}:
+        //   H_ab(i, k) = sum_{j', l'} q_a(j') q_b(l') Mp(3 j' + i, 3 l' + k).
+        const R* Mp = reinterpret_cast<const R*>(a.proj) + 45 * static_cast<size_t>(e);
+        R Y[3][9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                R s = 0;
+#pragma unroll
+                for (int jp = 0; jp < 3; ++jp) s = X::fma(qbasis<R>(la, jp), __ldg(Mp + sym9(3 * jp + i, c)), s);
+                Y[i][c] = s;
+            }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int pos = (pos4 >> (8 * b)) & 0xffu;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                    R s = 0;
+#pragma unroll
+                    for (int lp = 0; lp < 3; ++lp) s = X::fma(qbasis<R>(b, lp), Y[i][3 * lp + kk], s);
+                    if (b == la)
+                        v[3 + 3 * i + kk] = s;
+                    else
+                        sH[(3 * i + kk) * P + pos] = s;
+                }
+        }
+    }
+    return st;
+}
+
+// Fused element pass + assembly. WG: gradient, WH: Hessian (0 none, 1 exact, 2 from the
+// projected tangents in a.proj), energy always. CHUNKS = pairs per lane (1, or 2 for tiles of
+// up to 64 pairs).
+template <typename R, bool WG, int WH, int CHUNKS>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) assemble_kernel(const DevMesh m,
+                                                                                            const EvalArgs a) {
     using X = M<R>;
     using HT = typename HOut<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile = blockIdx.x * kWarpsPerBlock + warp;
+    const int nw = gridDim.x * kWarpsPerBlock;
+    int tile = blockIdx.x * kWarpsPerBlock + warp;
     if (tile >= m.ntiles) return;
-    const int cap = m.cap;
-    // Per-warp shared layout: H blocks (cap*36 R), g (cap*3 R), meta.
-    const size_t per_warp = static_cast<size_t>(cap) * (WH ? 36 : 0) * sizeof(R) +
-                            static_cast<size_t>(cap) * (WG ? 3 : 0) * sizeof(R) + sizeof(TileMeta);
-    unsigned char* base = smem_raw + per_warp * warp;
+    const int cap = 32 * CHUNKS;
+    const int P = 3 * cap + 1;
+    unsigned char* base = smem_raw + smem_per_warp<R, WH>(cap) * warp;
     R* sH = reinterpret_cast<R*>(base);
-    R* sg = sH + (WH ? cap * 36 : 0);
-    TileMeta* meta = reinterpret_cast<TileMeta*>(sg + (WG ? cap * 3 : 0));
+    uint32_t* sdesc = reinterpret_cast<uint32_t*>(base + (WH ? 9 * static_cast<size_t>(P) * sizeof(R) : 0));
+    TileMeta* meta = reinterpret_cast<TileMeta*>(base + (WH ? 9 * static_cast<size_t>(P) * sizeof(R) + 12 * cap : 0));
 
-    const int p0 = m.tile_pair_ptr[tile];
-    const int np = m.tile_pair_ptr[tile + 1] - p0;
     unsigned st = 0;
-    double e_acc = 0.0;
-    for (int q = lane; q < np; q += 32) {
-        const int pe = m.pair_elem[p0 + q];
-        // Slot-sorted positions of this pair's four blocks (one byte each).
-        const unsigned pos4 = __ldg(reinterpret_cast<const unsigned*>(m.contrib) + p0 + q);
-        const int e = pe & ((1 << 30) - 1);
-        const int la = static_cast<unsigned>(pe) >> 30;
-        const int4 tv = __ldg(m.tets + e);
-        Kin<R> k;
-        st |= kinematics<R>(m, e, tv, a.u, k);
-        if (la == 0) {
-            const R Ee = k.vol * k.psi;
-            e_acc += static_cast<double>(Ee);
-            if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
-            if (!X::finite(Ee)) st |= ST_NONFINITE_OUT;
+    // Index chain of the next tile: pair records first, then the vertex ids of their elements, so
+    // that a tile's element records and displacements are one dependent load away.
+    int np_n = 0;
+    int pe_n[CHUNKS];
+    unsigned pos_n[CHUNKS];
+    int4 tv_n[CHUNKS];
+    auto load_index = [&](int t) {
+        const int p0n = __ldg(m.tile_pair_ptr + t);
+        np_n = __ldg(m.tile_pair_ptr + t + 1) - p0n;
+#pragma unroll
+        for (int c = 0; c < CHUNKS; ++c) {
+            const int q = 32 * c + lane;
+            pe_n[c] = q < np_n ? __ldg(m.pair_elem + p0n + q) : 0;
+            pos_n[c] = q < np_n ? __ldg(reinterpret_cast<const unsigned*>(m.contrib) + p0n + q) : 0u;
         }
-        R na[3];
+    };
+    auto load_tets = [&]() {
 #pragma unroll
-        for (int j = 0; j < 3; ++j) na[j] = la == 0 ? k.n[0][j] : la == 1 ? k.n[1][j] : la == 2 ? k.n[2][j] : k.n[3][j];
-        const R p = X::fma(k.lam, k.logJ, -k.mu);
-        if (WG) {
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                R s = 0;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) s = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), na[j], s);
-                sg[3 * q + i] = k.vol * s;
+        for (int c = 0; c < CHUNKS; ++c)
+            tv_n[c] = 32 * c + lane < np_n ? __ldg(m.tets + (pe_n[c] & ((1 << 30) - 1))) : make_int4(0, 0, 0, 0);
+    };
+    load_index(tile);
+    load_tets();
+    for (; tile < m.ntiles; tile += nw) {
+        const int np = np_n;
+        int pe[CHUNKS];
+        unsigned pos[CHUNKS];
+        int4 tv[CHUNKS];
+    #pragma unroll
+        for (int c = 0; c < CHUNKS; ++c) {
+            pe[c] = pe_n[c];
+            pos[c] = pos_n[c];
+            tv[c] = tv_n[c];
+        }
+        const int tnext = tile + nw;
+        if (tnext < m.ntiles) load_index(tnext); // the next tile's pairs, ahead of this tile's work
+        const int r0 = m.tile_row_ptr[tile];
+        const int nr = m.tile_row_ptr[tile + 1] - r0;
+        const int s0 = m.tile_slot_ptr[tile];
+        const int ns = m.tile_slot_ptr[tile + 1] - s0;
+        // Row metadata and the pair prefix of the tile's rows (every row has at least one pair).
+        int deg = 0;
+        if (lane < nr) {
+            const int r = m.tile_rows[r0 + lane];
+            const int sb = m.row_ptr[r];
+            meta->row[lane] = r;
+            meta->slot0[lane] = sb;
+            meta->nb[lane] = m.row_ptr[r + 1] - sb;
+            meta->dq[lane] = m.diag_slot[r] - sb;
+            deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
+        }
+        int incl = deg;
+    #pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += t;
+        }
+        const int start = incl - deg; // first pair of row `lane`
+        meta->ppre[lane + 1] = incl;
+        if (lane == 0) meta->ppre[0] = 0;
+        if (WH)
+            for (int s = lane; s < ns; s += 32) sdesc[s] = __ldg(m.slot_desc + s0 + s);
+        const bool head = lane < nr;
+        const unsigned heads_lo = __reduce_or_sync(0xffffffffu, head && start < 32 ? 1u << start : 0u);
+        const unsigned heads_hi = __reduce_or_sync(0xffffffffu, head && start >= 32 ? 1u << (start - 32) : 0u);
+        __syncwarp();
+
+        double e_acc = 0.0;
+        R carry[12];
+    #pragma unroll
+        for (int c = 0; c < CHUNKS; ++c) {
+            const int q = 32 * c + lane;
+            R v[12];
+    #pragma unroll
+            for (int t = 0; t < 12; ++t) v[t] = R(0);
+            if (q < np) st |= eval_pair<R, WG, WH>(m, a, pe[c], pos[c], tv[c], sH, P, v, e_acc);
+            if (c == CHUNKS - 1 && tnext < m.ntiles) load_tets(); // vertex ids of the next tile's elements
+            const unsigned heads = c == 0 ? heads_lo : heads_hi;
+            segmented_scan<R>(v, heads, lane);
+            if (c == 1) {
+                // A row running on from chunk 0 adds chunk 0's partial (its last lane) once, at its end.
+                const bool cont = (heads & (0xffffffffu >> (31 - lane))) == 0;
+                if (cont)
+    #pragma unroll
+                    for (int t = 0; t < 12; ++t) v[t] = X::add(carry[t], v[t]);
             }
-        }
-        if (WH == 1) {
-            R h[4][3];
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    h[b][i] = X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
-            R ha[3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) ha[i] = la == 0 ? h[0][i] : la == 1 ? h[1][i] : la == 2 ? h[2][i] : h[3][i];
-            const R lv = X::mul(k.vol, k.lam);
-            const R pv = X::mul(k.vol, p);
-            const R mv = X::mul(k.vol, k.mu);
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                R* out = sH + 9 * ((pos4 >> (8 * b)) & 0xffu);
-                const R gg = X::fma(na[2], k.n[b][2], X::fma(na[1], k.n[b][1], X::mul(na[0], k.n[b][0])));
-                const R mg = X::mul(mv, gg);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const R x = X::mul(ha[i], h[b][kk]);
-                        const R y = X::mul(h[b][i], ha[kk]);
-                        R v = X::fma(lv, x, X::mul(-pv, y));
-                        if (i == kk) v = X::add(v, mg);
-                        out[3 * i + kk] = v;
+            if (CHUNKS == 2 && c == 0)
+    #pragma unroll
+                for (int t = 0; t < 12; ++t) carry[t] = __shfl_sync(0xffffffffu, v[t], 31);
+            // The last lane of each row segment in this chunk writes the row's gradient and diagonal block.
+            const unsigned next_heads = (lane == 31) ? (c == 0 ? (heads_hi & 1u) : 0u) : (heads >> (lane + 1)) & 1u;
+            const bool row_ends_here = q < np && (q == np - 1 || next_heads);
+            if (row_ends_here) {
+                const unsigned long long all = (static_cast<unsigned long long>(heads_hi) << 32) | heads_lo;
+                const unsigned long long upto = (q == 63) ? all : (all & ((2ull << q) - 1));
+                const int j = __popcll(upto) - 1;
+                const int r = meta->row[j];
+                if (WG) {
+    #pragma unroll
+                    for (int t = 0; t < 3; ++t) {
+                        if (!X::finite(v[t])) st |= ST_NONFINITE_OUT;
+                        a.grad[3 * static_cast<size_t>(r) + t] = static_cast<double>(v[t]);
                     }
-            }
-        } else if (WH == 2) {
-            // Projected: blocks from the clamped per-element tangent Mp (9x9 over (i, j') with
-            // index 3 j' + i, packed upper triangle) in the orthonormal basis q of {sum = 0}:
-            //   H_ab(i, k) = sum_{j', l'} q_a(j') q_b(l') Mp(3 j' + i, 3 l' + k).
-            const R* Mp = reinterpret_cast<const R*>(a.proj) + 45 * static_cast<size_t>(e);
-            R Y[3][9]; // Y[i][3 l' + k] = sum_j' q_a(j') Mp(3 j' + i, 3 l' + k)
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int c = 0; c < 9; ++c) {
-                    R s = 0;
-#pragma unroll
-                    for (int jp = 0; jp < 3; ++jp) s = X::fma(qbasis<R>(la, jp), __ldg(Mp + sym9(3 * jp + i, c)), s);
-                    Y[i][c] = s;
                 }
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        R s = 0;
-#pragma unroll
-                        for (int lp = 0; lp < 3; ++lp) s = X::fma(qbasis<R>(b, lp), Y[i][3 * lp + kk], s);
-                        sH[9 * ((pos4 >> (8 * b)) & 0xffu) + 3 * i + kk] = s;
+                if (WH) {
+                    HT* hout = reinterpret_cast<HT*>(a.hess);
+                    const int dq = meta->dq[j];
+    #pragma unroll
+                    for (int t = 0; t < 9; ++t) {
+                        if (!X::finite(v[3 + t])) st |= ST_NONFINITE_OUT;
+                        const int i = t / 3, cc = t - 3 * (t / 3);
+                        const size_t pos = a.layout == LPG_LAYOUT_BSR
+                                               ? 9 * static_cast<size_t>(meta->slot0[j] + dq) + t
+                                               : 9 * static_cast<size_t>(meta->slot0[j]) +
+                                                     static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * dq + cc;
+                        hout[pos] = static_cast<HT>(v[3 + t]);
                     }
-        }
-    }
-    // Row metadata of the tile.
-    const int r0 = m.tile_row_ptr[tile];
-    const int nr = m.tile_row_ptr[tile + 1] - r0;
-    int my_nb = 0, my_deg = 0;
-    if (lane < nr) {
-        const int r = m.tile_rows[r0 + lane];
-        meta->row[lane] = r;
-        meta->slot0[lane] = m.row_ptr[r];
-        my_nb = m.row_ptr[r + 1] - m.row_ptr[r];
-        my_deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
-        meta->nb[lane] = my_nb;
-    }
-    int snb = my_nb, sdeg = my_deg;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int a1 = __shfl_up_sync(0xffffffffu, snb, off);
-        const int a2 = __shfl_up_sync(0xffffffffu, sdeg, off);
-        if (lane >= off) {
-            snb += a1;
-            sdeg += a2;
-        }
-    }
-    meta->spre[lane + 1] = snb;
-    meta->ppre[lane + 1] = sdeg;
-    if (lane == 0) {
-        meta->spre[0] = 0;
-        meta->ppre[0] = 0;
-    }
-    __syncwarp();
-    const int nslots = meta->spre[nr];
-    if (WH) {
-        const uint16_t* soff = m.slot_off + m.tile_slot_ptr[tile] + tile;
-        HT* hout = reinterpret_cast<HT*>(a.hess);
-        int j = 0;
-        for (int o = lane; o < 9 * nslots; o += 32) {
-            const int s = o / 9;
-            const int kk = o - 9 * s;
-            while (meta->spre[j + 1] <= s) ++j;
-            const int c0 = soff[s], c1 = soff[s + 1];
-            R v = 0;
-            for (int c = c0; c < c1; ++c) v = X::add(v, sH[9 * c + kk]);
-            if (!X::finite(v)) st |= ST_NONFINITE_OUT;
-            const int qs = s - meta->spre[j];
-            size_t pos;
-            if (a.layout == LPG_LAYOUT_BSR) {
-                pos = 9 * static_cast<size_t>(meta->slot0[j] + qs) + kk;
-            } else {
-                const int i = kk / 3, c = kk - 3 * i;
-                pos = 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * qs + c;
+                }
             }
-            hout[pos] = static_cast<HT>(v);
         }
-    }
-    if (WG) {
-        for (int o = lane; o < 3 * nr; o += 32) {
-            const int j = o / 3, c = o - 3 * j;
-            R v = 0;
-            for (int q = meta->ppre[j]; q < meta->ppre[j + 1]; ++q) v = X::add(v, sg[3 * q + c]);
-            if (!X::finite(v)) st |= ST_NONFINITE_OUT;
-            a.grad[3 * static_cast<size_t>(meta->row[j]) + c] = static_cast<double>(v);
+        __syncwarp();
+        // Off-diagonal slots: 27 lanes = 3 slots x 9 entries per pass; a slot's blocks are contiguous.
+        if (WH && lane < 27) {
+            HT* hout = reinterpret_cast<HT*>(a.hess);
+            const int sub = lane / 9, kk = lane - 9 * (lane / 9);
+            const int total = 3 * np;
+            const R* col = sH + kk * P;
+            for (int s = sub; s < ns; s += 3) {
+                const uint32_t d = sdesc[s];
+                const int c0 = d & 0xffu;
+                const int c1 = s + 1 < ns ? (sdesc[s + 1] & 0xffu) : total;
+                const int j = (d >> 8) & 31u;
+                const int qs = d >> 13;
+                R val = 0;
+                for (int c = c0; c < c1; ++c) val = X::add(val, col[c]);
+                if (!X::finite(val)) st |= ST_NONFINITE_OUT;
+                size_t pos;
+                if (a.layout == LPG_LAYOUT_BSR) {
+                    pos = 9 * static_cast<size_t>(meta->slot0[j] + qs) + kk;
+                } else {
+                    const int i = kk / 3, cc = kk - 3 * (kk / 3);
+                    pos = 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * qs + cc;
+                }
+                hout[pos] = static_cast<HT>(val);
+            }
         }
+    #pragma unroll
+        for (int off = 16; off > 0; off >>= 1) e_acc += __shfl_xor_sync(0xffffffffu, e_acc, off);
+        if (lane == 0) {
+            a.tile_energy[tile] = e_acc;
+            if (!isfinite(e_acc)) st |= ST_NONFINITE_OUT;
+        }
+        __syncwarp();
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) e_acc += __shfl_xor_sync(0xffffffffu, e_acc, off);
-    if (lane == 0) a.tile_energy[tile] = e_acc;
     st = __reduce_or_sync(0xffffffffu, st);
     if (lane == 0 && st) atomicOr(a.status, st);
+}
+
+// Gradient rows of vertices that no element references are zero.
+__global__ void zero_rows_kernel(double* __restrict__ grad, const int* __restrict__ rows, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const size_t r = rows[i];
+        grad[3 * r] = 0;
+        grad[3 * r + 1] = 0;
+        grad[3 * r + 2] = 0;
+    }
 }
 
 // Deterministic sum of n doubles into *out with one block (fixed thread -> index map and tree).
@@ -783,35 +937,50 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
-template <typename R, bool WG, int WH> size_t smem_bytes(int cap) {
-    return kWarpsPerBlock * (static_cast<size_t>(cap) * (WH ? 36 : 0) * sizeof(R) +
-                             static_cast<size_t>(cap) * (WG ? 3 : 0) * sizeof(R) + sizeof(TileMeta));
-}
-
-template <typename R, bool WG, int WH> void launch_assemble(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
-    const size_t sm = smem_bytes<R, WG, WH>(m.cap);
+template <typename R, bool WG, int WH, int CHUNKS> void launch_assemble(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    const size_t sm = kWarpsPerBlock * smem_per_warp<R, WH>(32 * CHUNKS);
     static bool configured = false;
     if (!configured) {
-        LPG_CUDA(cudaFuncSetAttribute(assemble_kernel<R, WG, WH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(smem_bytes<R, WG, WH>(64))));
+        LPG_CUDA(cudaFuncSetAttribute(assemble_kernel<R, WG, WH, CHUNKS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sm)));
         configured = true;
     }
-    const int blocks = (m.ntiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    // Persistent warps: as many blocks as are resident at once, each warp looping over tiles.
+    static int resident = 0;
+    if (resident == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        LPG_CUDA(cudaGetDevice(&dev));
+        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, assemble_kernel<R, WG, WH, CHUNKS>,
+                                                               32 * kWarpsPerBlock, sm));
+        resident = std::max(1, sms * std::max(per_sm, 1));
+    }
+    const int all = (m.ntiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int blocks = LPG_ASSEMBLE_PERSISTENT ? std::min(resident, all) : all;
     if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-    if (blocks > 0) assemble_kernel<R, WG, WH><<<blocks, 32 * kWarpsPerBlock, sm, s>>>(m, a);
+    if (blocks > 0) assemble_kernel<R, WG, WH, CHUNKS><<<blocks, 32 * kWarpsPerBlock, sm, s>>>(m, a);
     if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
     LPG_CUDA(cudaGetLastError());
+}
+
+template <typename R, bool WG, int WH> void launch_chunks(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    if (m.cap <= 32)
+        launch_assemble<R, WG, WH, 1>(m, a, s);
+    else
+        launch_assemble<R, WG, WH, 2>(m, a, s);
 }
 
 template <typename R> void launch_eval_t(const DevMesh& m, int hessian, const EvalArgs& a, cudaStream_t s) {
     const bool wg = a.grad != nullptr;
     const int wh = a.hess == nullptr ? 0 : (hessian == LPG_HESSIAN_EXACT ? 1 : 2);
-    if (wg && wh == 1) launch_assemble<R, true, 1>(m, a, s);
-    else if (wg && wh == 2) launch_assemble<R, true, 2>(m, a, s);
-    else if (!wg && wh == 1) launch_assemble<R, false, 1>(m, a, s);
-    else if (!wg && wh == 2) launch_assemble<R, false, 2>(m, a, s);
-    else if (wg) launch_assemble<R, true, 0>(m, a, s);
-    else launch_assemble<R, false, 0>(m, a, s);
+    if (wg && wh == 1) launch_chunks<R, true, 1>(m, a, s);
+    else if (wg && wh == 2) launch_chunks<R, true, 2>(m, a, s);
+    else if (!wg && wh == 1) launch_chunks<R, false, 1>(m, a, s);
+    else if (!wg && wh == 2) launch_chunks<R, false, 2>(m, a, s);
+    else if (wg) launch_chunks<R, true, 0>(m, a, s);
+    else launch_chunks<R, false, 0>(m, a, s);
+    if (wg && m.num_unused > 0)
+        zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
 }
 
 } // namespace

@@ -43,11 +43,17 @@ struct HostPlan {
     std::vector<int32_t> tile_pair_ptr;      // ntiles+1
     std::vector<int32_t> tile_row_ptr;       // ntiles+1
     std::vector<int32_t> tile_rows;          // rows of each tile, ascending
-    std::vector<int32_t> tile_slot_ptr;      // ntiles+1 (cumulative slot counts)
-    std::vector<uint16_t> slot_off;          // nnzb + ntiles: start of each tile slot in the slot-sorted blocks
-    // 4 * npairs: position of block b of each pair in its tile's slot-sorted block list; a slot's
-    // blocks are contiguous there and ordered by element, the reference's summation order.
+    std::vector<int32_t> tile_slot_ptr;      // ntiles+1 (cumulative off-diagonal slot counts)
+    // One descriptor per off-diagonal slot, in tile order: bits 0-7 the slot's first block in the
+    // tile's slot-sorted block list, bits 8-12 the row within the tile, bits 13+ the slot's
+    // position within its row. A slot's blocks are contiguous in that list and ordered by
+    // element, the reference's summation order.
+    std::vector<uint32_t> slot_desc;
+    // 4 * npairs: position of off-diagonal block b of each pair in the slot-sorted list
+    // (0xff for the diagonal block b == a, which is reduced in registers).
     std::vector<uint8_t> contrib;
+    std::vector<int32_t> diag_slot;          // V: block index of (v, v), -1 for an unused vertex
+    std::vector<int32_t> unused_rows;        // vertices referenced by no element (not in any tile)
     std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
     int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
     int64_t nnzb() const { return static_cast<int64_t>(col_idx.size()); }
@@ -62,8 +68,11 @@ struct DevMesh {
     int64_t nnzb = 0;
     int32_t *row_ptr = nullptr, *col_idx = nullptr, *inc_ptr = nullptr;
     int32_t *tile_pair_ptr = nullptr, *tile_row_ptr = nullptr, *tile_rows = nullptr, *tile_slot_ptr = nullptr;
-    uint16_t* slot_off = nullptr;
+    uint32_t* slot_desc = nullptr;
     uint8_t* contrib = nullptr;
+    int32_t* diag_slot = nullptr;
+    int32_t* unused_rows = nullptr;
+    int num_unused = 0;
     int32_t* pair_elem = nullptr;
     int4* tets = nullptr;
     // Per-element record: G (3x3 row-major, rows = grad N_1..3 in rest coordinates, times Fp^-1),

@@ -53,8 +53,6 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
     p.cap = maxdeg > 32 ? 64 : 32;
     // Block-CSR pattern: sorted unique neighbours (including the vertex itself).
     p.row_ptr.assign(static_cast<size_t>(V) + 1, 0);
-    std::vector<int32_t> nb;
-    std::vector<std::vector<int32_t>> rows_tmp;
     {
         std::vector<int32_t> cols;
         cols.reserve(static_cast<size_t>(npairs) * 2);
@@ -83,8 +81,13 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
     std::vector<int> tile_pairs;
     std::vector<Open> open;
     constexpr int kWindow = 8;
+    p.unused_rows.clear();
     for (int v = 0; v < V; ++v) {
         const int deg = p.inc_ptr[v + 1] - p.inc_ptr[v];
+        if (deg == 0) {
+            p.unused_rows.push_back(v); // no element references v: zero gradient, no Hessian slots
+            continue;
+        }
         int chosen = -1;
         for (size_t k = 0; k < open.size(); ++k)
             if (open[k].pairs + deg <= p.cap && open[k].rows < 32) {
@@ -112,17 +115,21 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
     p.tile_rows.clear();
     p.tile_rows.reserve(V);
     p.pair_elem.resize(static_cast<size_t>(npairs));
-    p.contrib.resize(static_cast<size_t>(npairs) * 4);
-    p.slot_off.clear();
-    p.slot_off.reserve(static_cast<size_t>(p.nnzb()) + ntiles);
-    std::vector<std::vector<uint8_t>> bucket;
+    p.contrib.assign(static_cast<size_t>(npairs) * 4, 0xff);
+    p.slot_desc.clear();
+    p.slot_desc.reserve(static_cast<size_t>(p.nnzb()));
+    p.diag_slot.assign(static_cast<size_t>(V), -1);
+    for (int v = 0; v < V; ++v)
+        for (int k = p.row_ptr[v]; k < p.row_ptr[v + 1]; ++k)
+            if (p.col_idx[k] == v) p.diag_slot[v] = k;
+    std::vector<std::vector<int>> bucket;
     int64_t pair_cursor = 0;
     for (int t = 0; t < ntiles; ++t) {
         const int64_t pair_base = pair_cursor;
         int64_t slots = 0;
-        std::vector<uint8_t> tile_contrib;
-        std::vector<uint16_t> offs;
-        for (int v : tiles[t]) {
+        int count = 0; // off-diagonal blocks of the tile placed so far
+        for (int j = 0; j < static_cast<int>(tiles[t].size()); ++j) {
+            const int v = tiles[t][j];
             p.tile_rows.push_back(v);
             const int r0 = p.row_ptr[v], nb_v = p.row_ptr[v + 1] - p.row_ptr[v];
             bucket.assign(static_cast<size_t>(nb_v), {});
@@ -132,24 +139,21 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
                 const int e = inc[k] & ((1 << 30) - 1);
                 for (int b = 0; b < 4; ++b) {
                     const int w = tets[4 * static_cast<size_t>(e) + b];
+                    if (w == v) continue; // the diagonal block is reduced in registers
                     const int32_t* beg = p.col_idx.data() + r0;
                     const int q = static_cast<int>(std::lower_bound(beg, beg + nb_v, w) - beg);
-                    bucket[q].push_back(static_cast<uint8_t>((local << 2) | b));
+                    bucket[q].push_back(4 * local + b);
                 }
             }
+            // Off-diagonal slots in column order; each slot's blocks contiguous, in element order.
             for (int q = 0; q < nb_v; ++q) {
-                offs.push_back(static_cast<uint16_t>(tile_contrib.size()));
-                tile_contrib.insert(tile_contrib.end(), bucket[q].begin(), bucket[q].end());
+                if (p.col_idx[r0 + q] == v) continue;
+                p.slot_desc.push_back(static_cast<uint32_t>(count) | (static_cast<uint32_t>(j) << 8) |
+                                      (static_cast<uint32_t>(q) << 13));
+                for (int c : bucket[q]) p.contrib[4 * pair_base + c] = static_cast<uint8_t>(count++);
+                ++slots;
             }
-            slots += nb_v;
         }
-        offs.push_back(static_cast<uint16_t>(tile_contrib.size()));
-        // Inverse of the slot-sorted contributor list: where pair `local` puts block b.
-        for (size_t idx = 0; idx < tile_contrib.size(); ++idx) {
-            const int c = tile_contrib[idx];
-            p.contrib[4 * pair_base + 4 * (c >> 2) + (c & 3)] = static_cast<uint8_t>(idx);
-        }
-        p.slot_off.insert(p.slot_off.end(), offs.begin(), offs.end());
         p.tile_pair_ptr[t + 1] = static_cast<int32_t>(pair_cursor);
         p.tile_row_ptr[t + 1] = static_cast<int32_t>(p.tile_rows.size());
         p.tile_slot_ptr[t + 1] = static_cast<int32_t>(p.tile_slot_ptr[t] + slots);

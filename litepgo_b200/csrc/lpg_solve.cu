@@ -574,18 +574,7 @@ void make_mask(lpg_fem& h, const int32_t* fixed, int nfixed, double* mask) {
     LPG_CUDA(cudaStreamSynchronize(h.stream));
 }
 
-const int* diag_slots(lpg_fem& h) {
-    if (!h.b_diag_slot.ptr) {
-        const HostPlan& p = h.plan;
-        std::vector<int32_t> d(static_cast<size_t>(std::max(p.V, 1)), -1);
-        for (int v = 0; v < p.V; ++v)
-            for (int k = p.row_ptr[v]; k < p.row_ptr[v + 1]; ++k)
-                if (p.col_idx[k] == v) d[v] = k;
-        int32_t* dd = h.b_diag_slot.as<int32_t>(d.size());
-        LPG_CUDA(cudaMemcpy(dd, d.data(), d.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    }
-    return static_cast<const int*>(h.b_diag_slot.ptr);
-}
+const int* diag_slots(lpg_fem& h) { return h.dm.diag_slot; }
 
 } // namespace
 
