@@ -151,7 +151,11 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
  * arrays on the handle's stream and reports, from CUDA events recorded on that stream, the
  * mean duration of the assembly kernel alone (ms_assemble) and of one whole evaluation
  * including projection and the energy reduction (ms_eval). With flush_l2 != 0 a 512 MB
- * buffer is written before each launch, outside the measured intervals.
+ * buffer is written before each launch, outside the measured intervals. Besides
+ * LPG_LAYOUT_BSR and LPG_LAYOUT_CSC, layout 2 selects the solvers' internal block layout:
+ * rows are cut into SpMV tiles of consecutive rows (at most 32 blocks and 32 rows per tile, a
+ * row without blocks counting as one, a longer row alone), and entry t (row-major) of block
+ * k of the tile holding blocks [k0, k0 + n) is at 9 k0 + t n + (k - k0).
  */
 int lpg_fem_time_eval(lpg_fem_t h, const double* u, double* grad, int hessian, int precision, int layout, void* hess,
                       int launches, int flush_l2, double* ms_assemble, double* ms_eval);

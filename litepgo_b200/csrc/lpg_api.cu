@@ -100,6 +100,7 @@ struct BusyGuard {
 };
 
 lpg_fem::~lpg_fem() {
+    if (pcg_graph) cudaGraphExecDestroy(pcg_graph);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -128,13 +129,14 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
         fail(LPG_EINVAL, "Energy: invalid Hessian kind");
     if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
-    if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC) fail(LPG_EINVAL, "invalid Hessian layout");
+    if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC && layout != kLayoutTiled)
+        fail(LPG_EINVAL, "invalid Hessian layout");
     EvalArgs a;
     a.u = du;
     a.grad = dgrad;
     a.hess = hessian != LPG_HESSIAN_NONE ? dhess : nullptr;
     a.layout = layout;
-    a.tile_energy = d_tile_energy.as<double>(std::max(dm.ntiles, 1));
+    a.tile_energy = d_tile_energy.as<double>(static_cast<size_t>(dm.ntiles) + 256); // tiles, then partial sums
     a.energy = d_energy.as<double>(1);
     a.elem_energy = delem;
     a.status = d_status.as<unsigned>(1);
@@ -273,6 +275,9 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         m.num_unused = static_cast<int>(p.unused_rows.size());
         m.contrib = upload(h->b_contrib, p.contrib);
         m.pair_elem = upload(h->b_pair_elem, p.pair_elem);
+        m.spmv_tile_row = upload(h->b_spmv_tiles, p.spmv_tile_row);
+        m.n_spmv_tiles = static_cast<int>(p.spmv_tile_row.size()) - 1;
+        m.spmv_row_tile = upload(h->b_spmv_row_tile, p.spmv_row_tile);
         std::vector<int32_t> tv(tets, tets + 4 * static_cast<size_t>(T));
         m.tets = reinterpret_cast<int4*>(upload(h->b_tets, tv));
         m.rec64 = upload(h->b_rec64, rec);
@@ -352,6 +357,7 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
         const size_t n = 3 * static_cast<size_t>(h->dm.V);
         if (!u && n > 0) fail(LPG_EINVAL, "lpg_fem_eval: null u");
         if (hessian != LPG_HESSIAN_NONE && !hess) fail(LPG_EINVAL, "lpg_fem_eval: null Hessian output");
+        if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC) fail(LPG_EINVAL, "invalid Hessian layout");
         const double* du = h->stage_in(u, io_mem, h->d_u, n);
         double* dgrad = nullptr;
         if (grad) dgrad = io_mem == LPG_MEM_DEVICE ? grad : h->d_grad.as<double>(n);

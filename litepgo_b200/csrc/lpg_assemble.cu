@@ -225,7 +225,21 @@ struct TileMeta {
     int nb[32];
     int dq[32];   // position of the diagonal block within the row
     int ppre[33]; // the pairs of row j are [ppre[j], ppre[j + 1])
+    int tk0[32];  // first block and block count of the row's SpMV tile (tiled layout)
+    int tn[32];
 };
+
+// Position of entry t (row-major) of block q of tile row j in the output layout.
+__device__ __forceinline__ size_t out_pos(int layout, const TileMeta* meta, int j, int q, int t) {
+    const int64_t k = static_cast<int64_t>(meta->slot0[j]) + q;
+    if (layout == LPG_LAYOUT_BSR) return static_cast<size_t>(9 * k + t);
+    if (layout == LPG_LAYOUT_CSC) {
+        const int i = t / 3, c = t - 3 * (t / 3);
+        return 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * q + c;
+    }
+    const int64_t k0 = meta->tk0[j];
+    return static_cast<size_t>(9 * k0 + static_cast<int64_t>(t) * meta->tn[j] + (k - k0));
+}
 
 // Shared memory of one warp: off-diagonal blocks [9][3 cap + 1], slot descriptors [3 cap], metadata.
 template <typename R, int WH> __host__ __device__ constexpr size_t smem_per_warp(int cap) {
@@ -415,6 +429,12 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
             meta->slot0[lane] = sb;
             meta->nb[lane] = m.row_ptr[r + 1] - sb;
             meta->dq[lane] = m.diag_slot[r] - sb;
+            if (a.layout == kLayoutTiled) {
+                const int st = m.spmv_row_tile[r];
+                const int k0 = m.row_ptr[m.spmv_tile_row[st]];
+                meta->tk0[lane] = k0;
+                meta->tn[lane] = m.row_ptr[m.spmv_tile_row[st + 1]] - k0;
+            }
             deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
         }
         int incl = deg;
@@ -476,19 +496,35 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
     #pragma unroll
                     for (int t = 0; t < 9; ++t) {
                         if (!X::finite(v[3 + t])) st |= ST_NONFINITE_OUT;
-                        const int i = t / 3, cc = t - 3 * (t / 3);
-                        const size_t pos = a.layout == LPG_LAYOUT_BSR
-                                               ? 9 * static_cast<size_t>(meta->slot0[j] + dq) + t
-                                               : 9 * static_cast<size_t>(meta->slot0[j]) +
-                                                     static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * dq + cc;
-                        hout[pos] = static_cast<HT>(v[3 + t]);
+                        hout[out_pos(a.layout, meta, j, dq, t)] = static_cast<HT>(v[3 + t]);
                     }
                 }
             }
         }
         __syncwarp();
-        // Off-diagonal slots: 27 lanes = 3 slots x 9 entries per pass; a slot's blocks are contiguous.
-        if (WH && lane < 27) {
+        // Off-diagonal slots; a slot's blocks are contiguous in the slot-sorted list. In the
+        // tiled layout, lanes take consecutive slots of one entry (consecutive addresses);
+        // otherwise 27 lanes take 3 slots x 9 entries per pass.
+        if (WH && a.layout == kLayoutTiled && ns > 0) {
+            HT* hout = reinterpret_cast<HT*>(a.hess);
+            const int total = 3 * np;
+            int kk = lane / ns, s = lane - ns * (lane / ns);
+            for (; kk < 9;) {
+                const uint32_t d = sdesc[s];
+                const int c0 = d & 0xffu;
+                const int c1 = s + 1 < ns ? (sdesc[s + 1] & 0xffu) : total;
+                const R* col = sH + kk * P;
+                R val = 0;
+                for (int c = c0; c < c1; ++c) val = X::add(val, col[c]);
+                if (!X::finite(val)) st |= ST_NONFINITE_OUT;
+                hout[out_pos(kLayoutTiled, meta, (d >> 8) & 31u, d >> 13, kk)] = static_cast<HT>(val);
+                s += 32;
+                while (s >= ns) {
+                    s -= ns;
+                    ++kk;
+                }
+            }
+        } else if (WH && lane < 27) {
             HT* hout = reinterpret_cast<HT*>(a.hess);
             const int sub = lane / 9, kk = lane - 9 * (lane / 9);
             const int total = 3 * np;
@@ -502,14 +538,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
                 R val = 0;
                 for (int c = c0; c < c1; ++c) val = X::add(val, col[c]);
                 if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                size_t pos;
-                if (a.layout == LPG_LAYOUT_BSR) {
-                    pos = 9 * static_cast<size_t>(meta->slot0[j] + qs) + kk;
-                } else {
-                    const int i = kk / 3, cc = kk - 3 * (kk / 3);
-                    pos = 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * qs + cc;
-                }
-                hout[pos] = static_cast<HT>(val);
+                hout[out_pos(a.layout, meta, j, qs, kk)] = static_cast<HT>(val);
             }
         }
     #pragma unroll
@@ -535,20 +564,36 @@ __global__ void zero_rows_kernel(double* __restrict__ grad, const int* __restric
     }
 }
 
-// Deterministic sum of n doubles into *out with one block (fixed thread -> index map and tree).
-__global__ void __launch_bounds__(1024) sum_kernel(const double* __restrict__ x, int n, double* out) {
-    __shared__ double s[32];
+// Deterministic sum of n doubles: kSumBlocks blocks sum fixed contiguous chunks (fixed thread ->
+// index map and tree), then one block sums the partials in order.
+constexpr int kSumBlocks = 256;
+__global__ void __launch_bounds__(256) sum_partial_kernel(const double* __restrict__ x, int n, double* part) {
+    __shared__ double s[8];
+    const int chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
     double v = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v += x[i];
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) v += x[i];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) t += s[w];
+        part[blockIdx.x] = t;
+    }
+}
+__global__ void __launch_bounds__(256) sum_final_kernel(const double* __restrict__ part, int nb, double* out) {
+    __shared__ double s[8];
+    double v = threadIdx.x < nb ? part[threadIdx.x] : 0.0;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (threadIdx.x == 0) *out = v;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) t += s[w];
+        *out = t;
     }
 }
 
@@ -990,7 +1035,9 @@ void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a
         launch_eval_t<double>(m, hessian, a, s);
     else
         launch_eval_t<float>(m, hessian, a, s);
-    sum_kernel<<<1, 1024, 0, s>>>(a.tile_energy, m.ntiles, a.energy);
+    // Per-tile energies -> partials (stored after the tiles) -> total.
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(a.tile_energy, m.ntiles, a.tile_energy + m.ntiles);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.tile_energy + m.ntiles, kSumBlocks, a.energy);
     LPG_CUDA(cudaGetLastError());
 }
 

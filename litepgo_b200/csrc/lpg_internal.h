@@ -55,6 +55,8 @@ struct HostPlan {
     std::vector<int32_t> diag_slot;          // V: block index of (v, v), -1 for an unused vertex
     std::vector<int32_t> unused_rows;        // vertices referenced by no element (not in any tile)
     std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
+    std::vector<int32_t> spmv_tile_row;      // SpMV tiles: first row of each, plus V
+    std::vector<int32_t> spmv_row_tile;      // V: SpMV tile of each row
     int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
     int64_t nnzb() const { return static_cast<int64_t>(col_idx.size()); }
 };
@@ -74,6 +76,9 @@ struct DevMesh {
     int32_t* unused_rows = nullptr;
     int num_unused = 0;
     int32_t* pair_elem = nullptr;
+    int32_t* spmv_tile_row = nullptr;
+    int32_t* spmv_row_tile = nullptr;
+    int n_spmv_tiles = 0;
     int4* tets = nullptr;
     // Per-element record: G (3x3 row-major, rows = grad N_1..3 in rest coordinates, times Fp^-1),
     // vol (= det(Dm)/6 * det Fp), lambda, mu. 12 values, 16-byte aligned.
@@ -83,6 +88,19 @@ struct DevMesh {
     double* fpinv64 = nullptr;
     float* fpinv32 = nullptr;
 };
+
+// Internal Hessian layout of the solvers: within each SpMV tile (blocks [k0, k0 + n)), entry
+// t of block k is at 9 k0 + t n + (k - k0), so lanes reading consecutive blocks coalesce.
+constexpr int kLayoutTiled = 2;
+
+// Position of entry t (row-major in the 3x3 block) of block k in the tiled layout.
+__host__ __device__ inline size_t tiled_pos(const int32_t* row_ptr, const int32_t* tile_row, const int32_t* row_tile,
+                                            int row, int64_t k, int t) {
+    const int tile = row_tile[row];
+    const int64_t k0 = row_ptr[tile_row[tile]];
+    const int64_t n = row_ptr[tile_row[tile + 1]] - k0;
+    return static_cast<size_t>(9 * k0 + t * n + (k - k0));
+}
 
 // ---- kernel launchers (lpg_assemble.cu) ----
 struct EvalArgs {

@@ -72,6 +72,29 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
         }
         p.col_idx.swap(cols);
     }
+    // SpMV tiles: runs of consecutive rows holding at most 32 blocks (a row without blocks counts
+    // as one), one warp lane per block; a row with more than 32 blocks is a tile of its own.
+    p.spmv_tile_row.assign(1, 0);
+    {
+        int lanes = 0, rows = 0;
+        for (int v = 0; v < V; ++v) {
+            const int need = std::max(1, p.row_ptr[v + 1] - p.row_ptr[v]);
+            if (rows > 0 && (lanes + need > 32 || rows == 32)) {
+                p.spmv_tile_row.push_back(v);
+                lanes = rows = 0;
+            }
+            lanes += need;
+            ++rows;
+            if (need > 32) {
+                p.spmv_tile_row.push_back(v + 1);
+                lanes = rows = 0;
+            }
+        }
+        if (rows > 0) p.spmv_tile_row.push_back(V);
+        p.spmv_row_tile.assign(static_cast<size_t>(V), 0);
+        for (size_t t = 0; t + 1 < p.spmv_tile_row.size(); ++t)
+            for (int v = p.spmv_tile_row[t]; v < p.spmv_tile_row[t + 1]; ++v) p.spmv_row_tile[v] = static_cast<int32_t>(t);
+    }
     // Warp tiles: whole rows, at most `cap` pairs and 32 rows per tile. First fit over a
     // short window of open tiles keeps rows of one tile close in memory.
     struct Open {

@@ -22,7 +22,6 @@ namespace lpg {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kSpmvGroup = 16;
 constexpr double kEps = 2.220446049250313e-16;
 
 int red_blocks(size_t n) { return static_cast<int>(std::max<size_t>(1, std::min<size_t>(512, (n + 4095) / 4096))); }
@@ -143,76 +142,217 @@ __global__ void __launch_bounds__(1024) stats_final(const double* __restrict__ p
     }
 }
 
-// y = mask (K x) on the 3x3 block-CSR matrix; a group of 16 lanes walks one block row's
-// values contiguously (coalesced), then reduces its three sums with shuffles. With DOT,
-// part[block] = sum_i x_i y_i.
-template <typename TK, typename TV, typename TO, bool DOT>
-__global__ void __launch_bounds__(kThreads) bsr_spmv(const int* __restrict__ row_ptr, const int* __restrict__ col_idx,
-                                                     const TK* __restrict__ val, const TV* __restrict__ x,
-                                                     const double* __restrict__ mask, TO* __restrict__ y, int V,
-                                                     double* part, const int* done) {
+struct PcgState {
+    double rz, pAp, alpha, beta, rr, bb, tol2;
+    int done, breakdown, iters, max_iters;
+    unsigned count_a, count_b; // completion counters of the last-block reductions
+};
+
+// 4-wide vector access of padded per-vertex vectors (16-byte float4, two 16-byte double2).
+__device__ __forceinline__ void ld4(const float* p, float v[4]) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+}
+// Coherent loads, for vectors the same kernel also writes.
+__device__ __forceinline__ void ld4c(const float* p, float v[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+}
+__device__ __forceinline__ void ld4c(const double* p, double v[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, float a, float b, float c) {
+    *reinterpret_cast<float4*>(p) = make_float4(a, b, c, 0.f);
+}
+__device__ __forceinline__ void st4(double* p, double a, double b, double c) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+    reinterpret_cast<double2*>(p)[1] = make_double2(c, 0.0);
+}
+// Three components of vertex v of a vector with S (3 or 4) values per vertex.
+template <int S, typename T> __device__ __forceinline__ void ld3(const T* p, size_t v, T out[3]) {
+    if constexpr (S == 4) {
+        T t[4];
+        ld4(p + 4 * v, t);
+        out[0] = t[0], out[1] = t[1], out[2] = t[2];
+    } else {
+        out[0] = p[3 * v], out[1] = p[3 * v + 1], out[2] = p[3 * v + 2];
+    }
+}
+template <int S, typename T> __device__ __forceinline__ void st3(T* p, size_t v, T a, T b, T c) {
+    if constexpr (S == 4) {
+        st4(p + 4 * v, a, b, c);
+    } else {
+        p[3 * v] = a, p[3 * v + 1] = b, p[3 * v + 2] = c;
+    }
+}
+
+// Entry t (row-major) of the diagonal block of vertex v in the tiled layout, or -1.
+__device__ __forceinline__ int64_t diag_entry(const DevMesh& m, int v, int t) {
+    const int k = m.diag_slot[v];
+    if (k < 0) return -1;
+    return static_cast<int64_t>(tiled_pos(m.row_ptr, m.spmv_tile_row, m.spmv_row_tile, v, k, t));
+}
+
+// y = mask (K x) on the 3x3 block-CSR matrix stored in the tiled layout (entry t of block k of
+// the SpMV tile [k0, k0 + n) at 9 k0 + t n + k - k0). Rows are packed into warp tiles of
+// consecutive rows with at most 32 blocks (one lane per block; a longer row has a tile of its
+// own and its lanes loop), so each of the nine value loads of a warp is one contiguous run;
+// each lane gathers its column's x, and a segmented warp scan sums each row. Vectors hold S
+// values per vertex: S = 4 for the padded PCG vectors (4th value zero, one 16-byte load per
+// gathered vertex in FP32), S = 3 for plain FP64 vectors. With PCG the vector is formed on
+// the fly as z + beta p_old (beta from the state; the row owners write it to p_new), and the
+// block of the grid that finishes last reduces the partial p.Ap sums into alpha; otherwise,
+// with DOT, part[block] = sum x.y. Both reductions use a fixed order.
+template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S>
+__global__ void __launch_bounds__(kThreads) spmv_tiles(const DevMesh m, const TK* __restrict__ val,
+                                                       const TV* __restrict__ x, const TV* __restrict__ p_old,
+                                                       const TV* __restrict__ mask, TO* __restrict__ y,
+                                                       TV* __restrict__ p_new, PcgState* st, double* part) {
     __shared__ double sh[kThreads / 32];
-    if (done && *done) return;
+    __shared__ bool last;
     using A = typename std::conditional<(sizeof(TK) == 4 && sizeof(TV) == 4), float, double>::type;
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int v = gid / kSpmvGroup;
-    const int lg = threadIdx.x & (kSpmvGroup - 1);
-    A a0 = 0, a1 = 0, a2 = 0;
-    if (v < V) {
-        const int s0 = row_ptr[v], nb = row_ptr[v + 1] - s0;
-        const TK* rv = val + 9 * static_cast<size_t>(s0);
-        for (int j = lg; j < 9 * nb; j += kSpmvGroup) {
-            const int s = j / 9;
-            const int r = j - 9 * s;
-            const int i = r / 3;
-            const int k = r - 3 * i;
-            const int c = __ldg(col_idx + s0 + s);
-            const A t = static_cast<A>(rv[j]) * static_cast<A>(x[3 * static_cast<size_t>(c) + k]);
-            if (i == 0) a0 += t;
-            else if (i == 1) a1 += t;
-            else a2 += t;
+    if (PCG && st->done) return;
+    const TV beta = PCG ? static_cast<TV>(st->beta) : TV(0);
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    double dot = 0;
+    for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < m.n_spmv_tiles; t += nwarps) {
+        const int r0 = __ldg(m.spmv_tile_row + t);
+        const int nrows = __ldg(m.spmv_tile_row + t + 1) - r0;
+        const int k0 = __ldg(m.row_ptr + r0);
+        const int ntb = __ldg(m.row_ptr + r0 + nrows) - k0;
+        int s = 0, nb = 0;
+        if (lane < nrows) {
+            s = __ldg(m.row_ptr + r0 + lane);
+            nb = __ldg(m.row_ptr + r0 + lane + 1) - s;
+        }
+        const int need = lane < nrows ? max(nb, 1) : 0;
+        int incl = need;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += u;
+        }
+        const int start = incl - need;
+        const unsigned heads = __reduce_or_sync(0xffffffffu, lane < nrows ? 1u << min(start, 31) : 0u);
+        const unsigned upto = heads & (0xffffffffu >> (31 - lane));
+        const int jr = __popc(upto) - 1;
+        const int s_r = __shfl_sync(0xffffffffu, s, jr);
+        const int nb_r = __shfl_sync(0xffffffffu, nb, jr);
+        const int start_r = __shfl_sync(0xffffffffu, start, jr);
+        const int lanes_r = nrows == 1 ? min(max(nb_r, 1), 32) : max(nb_r, 1);
+        const TK* vt = val + 9 * static_cast<size_t>(k0);
+        A a0 = 0, a1 = 0, a2 = 0;
+        const int step = nrows == 1 ? 32 : (1 << 30);
+        for (int b = lane - start_r; b < nb_r && lane - start_r < lanes_r; b += step) {
+            const int k = s_r + b;
+            const size_t c = static_cast<size_t>(__ldg(m.col_idx + k));
+            TV xz[3];
+            ld3<S>(x, c, xz);
+            if (PCG) {
+                TV xp[3];
+                ld3<S>(p_old, c, xp);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) xz[i] = xz[i] + beta * xp[i];
+            }
+            const A xv[3] = {static_cast<A>(xz[0]), static_cast<A>(xz[1]), static_cast<A>(xz[2])};
+            const TK* vk = vt + (k - k0);
+            A kv[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vk + static_cast<size_t>(e) * ntb));
+            a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
+            a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
+            a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
+        }
+        // Segmented inclusive scan over the lanes of each row (fixed pattern).
+        const int seg = 31 - __clz(upto);
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const A t0 = __shfl_up_sync(0xffffffffu, a0, off);
+            const A t1 = __shfl_up_sync(0xffffffffu, a1, off);
+            const A t2 = __shfl_up_sync(0xffffffffu, a2, off);
+            if (lane - off >= seg) {
+                a0 = t0 + a0;
+                a1 = t1 + a1;
+                a2 = t2 + a2;
+            }
+        }
+        if (jr < nrows && lane == start_r + lanes_r - 1) {
+            const size_t o = static_cast<size_t>(r0 + jr);
+            TV mv[3];
+            ld3<S>(mask, o, mv);
+            const A yv[3] = {static_cast<A>(mv[0]) * a0, static_cast<A>(mv[1]) * a1, static_cast<A>(mv[2]) * a2};
+            st3<S, TO>(y, o, static_cast<TO>(yv[0]), static_cast<TO>(yv[1]), static_cast<TO>(yv[2]));
+            if (PCG) {
+                TV xz[3], xp[3];
+                ld3<S>(x, o, xz);
+                ld3<S>(p_old, o, xp);
+                TV pv[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    pv[i] = xz[i] + beta * xp[i];
+                    dot += static_cast<double>(pv[i]) * static_cast<double>(yv[i]);
+                }
+                st3<S, TV>(p_new, o, pv[0], pv[1], pv[2]);
+            } else if (DOT) {
+                TV xz[3];
+                ld3<S>(x, o, xz);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) dot += static_cast<double>(xz[i]) * static_cast<double>(yv[i]);
+            }
         }
     }
-#pragma unroll
-    for (int off = kSpmvGroup / 2; off > 0; off >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, off);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, off);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+    if (!PCG && !DOT) return;
+    dot = block_sum(dot, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = dot;
+        // The last block to finish turns the partial sums into alpha (this thread wrote part).
+        if (PCG) {
+            __threadfence();
+            last = atomicAdd(&st->count_a, 1u) == gridDim.x - 1;
+        }
     }
-    double d = 0;
-    if (v < V && lg == 0) {
-        const size_t o = 3 * static_cast<size_t>(v);
-        const A y0 = mask ? static_cast<A>(mask[o]) * a0 : a0;
-        const A y1 = mask ? static_cast<A>(mask[o + 1]) * a1 : a1;
-        const A y2 = mask ? static_cast<A>(mask[o + 2]) * a2 : a2;
-        y[o] = static_cast<TO>(y0);
-        y[o + 1] = static_cast<TO>(y1);
-        y[o + 2] = static_cast<TO>(y2);
-        if (DOT)
-            d = static_cast<double>(x[o]) * static_cast<double>(y0) + static_cast<double>(x[o + 1]) * static_cast<double>(y1) +
-                static_cast<double>(x[o + 2]) * static_cast<double>(y2);
-    }
-    if (DOT) {
-        d = block_sum(d, sh);
-        if (threadIdx.x == 0) part[blockIdx.x] = d;
+    if (!PCG) return;
+    __syncthreads();
+    if (!last) return;
+    double v = 0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) v += __ldcg(part + i);
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        st->count_a = 0;
+        st->pAp = v;
+        if (!(v > 0.0) || !isfinite(v)) {
+            st->breakdown = 1;
+            st->done = 1;
+        } else {
+            st->alpha = st->rz / v;
+        }
     }
 }
 
 // Inverse of each masked 3x3 diagonal block (identity on fixed components; identity for a
-// vertex without a diagonal block), the block-Jacobi preconditioner.
+// vertex without a diagonal block), the block-Jacobi preconditioner, stored as 3 padded rows
+// of 4 per vertex.
 template <typename TK, typename R>
-__global__ void __launch_bounds__(kThreads) block_jacobi(const TK* __restrict__ val, const int* __restrict__ diag_slot,
+__global__ void __launch_bounds__(kThreads) block_jacobi(const DevMesh m, const TK* __restrict__ val,
                                                          const double* __restrict__ mask, R* __restrict__ dinv, int V) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
     double b[9];
-    const int s = diag_slot[v];
-    const double m[3] = {mask[3 * static_cast<size_t>(v)], mask[3 * static_cast<size_t>(v) + 1],
-                         mask[3 * static_cast<size_t>(v) + 2]};
+    const double mk[3] = {mask[3 * static_cast<size_t>(v)], mask[3 * static_cast<size_t>(v) + 1],
+                          mask[3 * static_cast<size_t>(v) + 2]};
     for (int i = 0; i < 3; ++i)
         for (int k = 0; k < 3; ++k) {
-            const double kv = s >= 0 ? static_cast<double>(val[9 * static_cast<size_t>(s) + 3 * i + k]) : (i == k ? 1.0 : 0.0);
-            b[3 * i + k] = m[i] * m[k] * kv + (i == k ? 1.0 - m[i] : 0.0);
+            const int64_t pos = diag_entry(m, v, 3 * i + k);
+            const double kv = pos >= 0 ? static_cast<double>(val[pos]) : (i == k ? 1.0 : 0.0);
+            b[3 * i + k] = mk[i] * mk[k] * kv + (i == k ? 1.0 - mk[i] : 0.0);
         }
     const double det = b[0] * (b[4] * b[8] - b[5] * b[7]) - b[1] * (b[3] * b[8] - b[5] * b[6]) +
                        b[2] * (b[3] * b[7] - b[4] * b[6]);
@@ -234,39 +374,46 @@ __global__ void __launch_bounds__(kThreads) block_jacobi(const TK* __restrict__ 
         for (int i = 0; i < 3; ++i) r[4 * i] = (b[4 * i] != 0 && isfinite(b[4 * i])) ? 1.0 / b[4 * i] : 1.0;
     }
     for (int i = 0; i < 3; ++i)
-        for (int k = 0; k < 3; ++k) dinv[9 * static_cast<size_t>(v) + 3 * i + k] = static_cast<R>(m[i] * m[k] * r[3 * i + k]);
+        st4(dinv + 12 * static_cast<size_t>(v) + 4 * i, static_cast<R>(mk[i] * mk[0] * r[3 * i]),
+            static_cast<R>(mk[i] * mk[1] * r[3 * i + 1]), static_cast<R>(mk[i] * mk[2] * r[3 * i + 2]));
 }
 
-struct PcgState {
-    double rz, pAp, alpha, beta, rr, bb, tol2;
-    int done, breakdown, iters, max_iters;
-};
-
-__device__ __forceinline__ void apply_dinv(const float* D, const float* r, float* z) {
-    for (int i = 0; i < 3; ++i) z[i] = D[3 * i] * r[0] + D[3 * i + 1] * r[1] + D[3 * i + 2] * r[2];
-}
-__device__ __forceinline__ void apply_dinv(const double* D, const double* r, double* z) {
-    for (int i = 0; i < 3; ++i) z[i] = D[3 * i] * r[0] + D[3 * i + 1] * r[1] + D[3 * i + 2] * r[2];
+// z = D r with D the 3 padded rows of a vertex's preconditioner block.
+template <typename R> __device__ __forceinline__ void apply_dinv(const R* D, const R* r, R* z) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R d[4];
+        ld4(D + 4 * i, d);
+        z[i] = d[0] * r[0] + d[1] * r[1] + d[2] * r[2];
+    }
 }
 
-// r = mask b, x = 0, z = M^-1 r, p = z; part = {r.z, r.r} per block.
+// b4 = mask b64 as padded R (4 per vertex, 4th zero).
 template <typename R>
-__global__ void __launch_bounds__(kThreads) pcg_init(const R* __restrict__ b, const double* __restrict__ mask,
-                                                     const R* __restrict__ dinv, R* x, R* r, R* z, R* p, int V,
-                                                     double* part) {
-    __shared__ double sh[kThreads / 32];
+__global__ void pad_rhs(const double* __restrict__ b, const double* __restrict__ mask, R* __restrict__ b4, int V) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const size_t o = 3 * static_cast<size_t>(v);
+    st4(b4 + 4 * static_cast<size_t>(v), static_cast<R>(mask[o] * b[o]), static_cast<R>(mask[o + 1] * b[o + 1]),
+        static_cast<R>(mask[o + 2] * b[o + 2]));
+}
+
+// r = b, x = 0, z = M^-1 r, p_old = 0; part = {r.z, r.r} per block (grid-stride, fixed grid).
+template <typename R>
+__global__ void __launch_bounds__(kThreads) pcg_init(const R* __restrict__ b, const R* __restrict__ dinv, R* x, R* r,
+                                                     R* z, R* p_old, int V, double* part) {
+    __shared__ double sh[kThreads / 32];
     double rz = 0, rr = 0;
-    if (v < V) {
-        R rv[3], zv[3];
-        for (int i = 0; i < 3; ++i) rv[i] = static_cast<R>(mask[3 * static_cast<size_t>(v) + i]) * b[3 * static_cast<size_t>(v) + i];
-        apply_dinv(dinv + 9 * static_cast<size_t>(v), rv, zv);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const size_t o = 4 * static_cast<size_t>(v);
+        R rv[4], zv[3];
+        ld4(b + o, rv);
+        apply_dinv(dinv + 12 * static_cast<size_t>(v), rv, zv);
+        st4(x + o, R(0), R(0), R(0));
+        st4(r + o, rv[0], rv[1], rv[2]);
+        st4(z + o, zv[0], zv[1], zv[2]);
+        st4(p_old + o, R(0), R(0), R(0));
         for (int i = 0; i < 3; ++i) {
-            const size_t o = 3 * static_cast<size_t>(v) + i;
-            x[o] = 0;
-            r[o] = rv[i];
-            z[o] = zv[i];
-            p[o] = zv[i];
             rz += static_cast<double>(rv[i]) * zv[i];
             rr += static_cast<double>(rv[i]) * rv[i];
         }
@@ -287,50 +434,45 @@ __global__ void __launch_bounds__(1024) pcg_start(PcgState* st, const double* pa
     st->rz = rz;
     st->rr = rr;
     st->bb = rr;
+    st->beta = 0;
     st->tol2 = tol * tol * rr;
     st->iters = 0;
     st->breakdown = 0;
     st->max_iters = max_iters;
+    st->count_a = 0;
+    st->count_b = 0;
     st->done = (rr == 0.0 || max_iters <= 0) ? 1 : 0;
 }
 
-__global__ void __launch_bounds__(1024) pcg_alpha(PcgState* st, const double* part, int nb) {
-    if (st->done) return;
-    __shared__ double res[1];
-    reduce_partials<1>(part, nb, res);
-    if (threadIdx.x != 0) return;
-    const double pap = res[0];
-    st->pAp = pap;
-    if (!(pap > 0.0) || !isfinite(pap)) {
-        st->breakdown = 1;
-        st->done = 1;
-        return;
-    }
-    st->alpha = st->rz / pap;
-}
-
+// x += alpha p, r -= alpha Ap, z = M^-1 r and the partial r.z, r.r; the last block to finish
+// computes beta and the stopping test.
 template <typename R>
-__global__ void __launch_bounds__(kThreads) pcg_update(const PcgState* st, const double* __restrict__ mask,
-                                                       const R* __restrict__ dinv, R* x, R* r, R* z,
+__global__ void __launch_bounds__(kThreads) pcg_update(PcgState* st, const R* __restrict__ dinv, R* x, R* r, R* z,
                                                        const R* __restrict__ p, const R* __restrict__ Ap, int V,
                                                        double* part) {
     __shared__ double sh[kThreads / 32];
+    __shared__ bool last;
     if (st->done) return;
     const R alpha = static_cast<R>(st->alpha);
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
     double rz = 0, rr = 0;
-    if (v < V) {
-        R rv[3], zv[3];
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const size_t o = 4 * static_cast<size_t>(v);
+        R xv[4], pv[4], rv[4], av[4], zv[3];
+        ld4c(x + o, xv);
+        ld4(p + o, pv);
+        ld4c(r + o, rv);
+        ld4(Ap + o, av);
+#pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const size_t o = 3 * static_cast<size_t>(v) + i;
-            x[o] += alpha * p[o];
-            rv[i] = r[o] - alpha * Ap[o];
-            r[o] = rv[i];
+            xv[i] += alpha * pv[i];
+            rv[i] = rv[i] - alpha * av[i];
         }
-        apply_dinv(dinv + 9 * static_cast<size_t>(v), rv, zv);
+        apply_dinv(dinv + 12 * static_cast<size_t>(v), rv, zv);
+        st4(x + o, xv[0], xv[1], xv[2]);
+        st4(r + o, rv[0], rv[1], rv[2]);
+        st4(z + o, zv[0], zv[1], zv[2]);
+#pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const size_t o = 3 * static_cast<size_t>(v) + i;
-            z[o] = zv[i];
             rz += static_cast<double>(rv[i]) * zv[i];
             rr += static_cast<double>(rv[i]) * rv[i];
         }
@@ -340,31 +482,29 @@ __global__ void __launch_bounds__(kThreads) pcg_update(const PcgState* st, const
     if (threadIdx.x == 0) {
         part[2 * blockIdx.x] = rz;
         part[2 * blockIdx.x + 1] = rr;
+        __threadfence(); // this thread wrote the partials
+        last = atomicAdd(&st->count_b, 1u) == gridDim.x - 1;
     }
-}
-
-__global__ void __launch_bounds__(1024) pcg_beta(PcgState* st, const double* part, int nb) {
-    if (st->done) return;
-    __shared__ double res[2];
-    reduce_partials<2>(part, nb, res);
-    if (threadIdx.x != 0) return;
-    const double rz = res[0], rr = res[1];
-    st->iters += 1;
-    st->rr = rr;
-    if (rr <= st->tol2 || st->iters >= st->max_iters || !isfinite(rr)) {
-        st->done = 1;
-        return;
+    __syncthreads();
+    if (!last) return;
+    double a = 0, b = 0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+        a += __ldcg(part + 2 * i);
+        b += __ldcg(part + 2 * i + 1);
     }
-    st->beta = rz / st->rz;
-    st->rz = rz;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads) pcg_pupdate(const PcgState* st, const R* __restrict__ z, R* p, size_t n) {
-    if (st->done) return;
-    const R beta = static_cast<R>(st->beta);
-    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    if (i < n) p[i] = z[i] + beta * p[i];
+    a = block_sum(a, sh);
+    b = block_sum(b, sh);
+    if (threadIdx.x == 0) {
+        st->count_b = 0;
+        st->iters += 1;
+        st->rr = b;
+        if (b <= st->tol2 || st->iters >= st->max_iters || !isfinite(b)) {
+            st->done = 1;
+        } else {
+            st->beta = a / st->rz;
+            st->rz = a;
+        }
+    }
 }
 
 template <typename A, typename B> __global__ void convert_kernel(const A* __restrict__ a, B* __restrict__ b, size_t n) {
@@ -372,11 +512,11 @@ template <typename A, typename B> __global__ void convert_kernel(const A* __rest
     if (i < n) b[i] = static_cast<B>(a[i]);
 }
 
-// x64 += xR ; optional r64 = b - y (masked) is done by a separate kernel.
+// x64 += x (x padded, 4 per vertex).
 template <typename R>
 __global__ void add_kernel(double* __restrict__ x64, const R* __restrict__ xr, size_t n) {
     const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
-    if (i < n) x64[i] += static_cast<double>(xr[i]);
+    if (i < n) x64[i] += static_cast<double>(xr[4 * (i / 3) + i % 3]);
 }
 __global__ void residual_kernel(const double* __restrict__ b, const double* __restrict__ y,
                                 const double* __restrict__ mask, double* __restrict__ r, size_t n) {
@@ -403,29 +543,29 @@ __global__ void axpy_trial(const double* __restrict__ x, double alpha, const dou
     mv = __reduce_or_sync(0xffffffffu, mv);
     if ((threadIdx.x & 31) == 0 && mv) atomicOr(moved, 1);
 }
-__global__ void shift_diag(double* val64, float* val32, const int* __restrict__ diag_slot, int V, double shift) {
+__global__ void shift_diag(const DevMesh m, double* val64, float* val32, double shift) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const int s = diag_slot[v];
-    if (s < 0) return;
+    if (v >= m.V) return;
     for (int i = 0; i < 3; ++i) {
-        if (val64) val64[9 * static_cast<size_t>(s) + 4 * i] += shift;
-        if (val32) val32[9 * static_cast<size_t>(s) + 4 * i] += static_cast<float>(shift);
+        const int64_t pos = diag_entry(m, v, 4 * i);
+        if (pos < 0) return;
+        if (val64) val64[pos] += shift;
+        if (val32) val32[pos] += static_cast<float>(shift);
     }
 }
-__global__ void diag_absmax_partial(const double* val64, const float* val32, const int* __restrict__ diag_slot,
-                                    const double* __restrict__ mask, int V, double* part) {
+__global__ void diag_absmax_partial(const DevMesh m, const double* val64, const float* val32,
+                                    const double* __restrict__ mask, double* part) {
     __shared__ double sh[kThreads / 32];
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    double m = 0;
-    if (v < V && diag_slot[v] >= 0) {
-        const size_t s = diag_slot[v];
-        for (int i = 0; i < 3; ++i)
-            if (mask[3 * static_cast<size_t>(v) + i] != 0)
-                m = fmax(m, fabs(val64 ? val64[9 * s + 4 * i] : static_cast<double>(val32[9 * s + 4 * i])));
-    }
-    m = block_max(m, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = m;
+    double mx = 0;
+    if (v < m.V)
+        for (int i = 0; i < 3; ++i) {
+            const int64_t pos = diag_entry(m, v, 4 * i);
+            if (pos >= 0 && mask[3 * static_cast<size_t>(v) + i] != 0)
+                mx = fmax(mx, fabs(val64 ? val64[pos] : static_cast<double>(val32[pos])));
+        }
+    mx = block_max(mx, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = mx;
 }
 __global__ void max_final(const double* part, int nb, double* out) {
     if (threadIdx.x != 0) return;
@@ -435,6 +575,18 @@ __global__ void max_final(const double* part, int nb, double* out) {
 }
 
 inline int grid(size_t n, int threads = kThreads) { return static_cast<int>((n + threads - 1) / threads); }
+
+// Grid of at most `work` blocks that fits in one wave of the device (blocks resident per SM
+// for this kernel x SM count), for the grid-stride kernels: a second partial wave would
+// double their time.
+template <typename Kern> int one_wave(Kern kernel, size_t work) {
+    int dev = 0, sms = 0, per = 0;
+    LPG_CUDA(cudaGetDevice(&dev));
+    LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0));
+    const size_t wave = static_cast<size_t>(std::max(per, 1)) * static_cast<size_t>(std::max(sms, 1));
+    return static_cast<int>(std::max<size_t>(1, std::min(work, wave)));
+}
 
 // ---------------------------------------------------------------------------
 // Host-side helpers bound to one handle.
@@ -475,16 +627,20 @@ struct Solver {
         return e - energy_dot_f(x, f);
     }
 
-    template <typename R>
-    void spmv(const void* K, bool k64, const R* x, const double* mask, R* y, double* part, const int* done, bool dot) {
-        const int blocks = grid(static_cast<size_t>(V) * kSpmvGroup);
-        if (k64) {
-            if (dot) bsr_spmv<double, R, R, true><<<blocks, kThreads, 0, s>>>(h.dm.row_ptr, h.dm.col_idx, static_cast<const double*>(K), x, mask, y, V, part, done);
-            else bsr_spmv<double, R, R, false><<<blocks, kThreads, 0, s>>>(h.dm.row_ptr, h.dm.col_idx, static_cast<const double*>(K), x, mask, y, V, part, done);
-        } else {
-            if (dot) bsr_spmv<float, R, R, true><<<blocks, kThreads, 0, s>>>(h.dm.row_ptr, h.dm.col_idx, static_cast<const float*>(K), x, mask, y, V, part, done);
-            else bsr_spmv<float, R, R, false><<<blocks, kThreads, 0, s>>>(h.dm.row_ptr, h.dm.col_idx, static_cast<const float*>(K), x, mask, y, V, part, done);
-        }
+    // One warp per SpMV tile at a time (8 per block), grid-stride over the tiles.
+    template <typename Kern> int spmv_grid(Kern k) const {
+        return one_wave(k, (static_cast<size_t>(h.dm.n_spmv_tiles) + 7) / 8);
+    }
+    template <typename Kern> int vec_grid(Kern k) const { return one_wave(k, grid(static_cast<size_t>(V))); }
+
+    // y64 = mask (K x64) in FP64 with K stored as TK.
+    void residual_spmv(const void* K, bool k64, const double* x64, const double* mask, double* y64) {
+        if (k64)
+            spmv_tiles<double, double, double, false, false, 3><<<spmv_grid(spmv_tiles<double, double, double, false, false, 3>), kThreads, 0, s>>>(
+                h.dm, static_cast<const double*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
+        else
+            spmv_tiles<float, double, double, false, false, 3><<<spmv_grid(spmv_tiles<float, double, double, false, false, 3>), kThreads, 0, s>>>(
+                h.dm, static_cast<const float*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
         LPG_CUDA(cudaGetLastError());
     }
 
@@ -494,46 +650,86 @@ struct Solver {
         double rel = 0; // final ||b - K x|| / ||b|| in FP64
     };
 
-    // Solves mask K x = mask b (FP64 b, x): inner PCG in precision R on matrix Kin (typed R),
-    // FP64 residual refinement against Kres (FP64 values when res64, else Kin's values).
+    // Enqueues `pairs` x 2 PCG iterations on stream gs (two launches per iteration; p_new and
+    // p_old swap roles every iteration).
+    template <typename R>
+    void enqueue_iterations(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA,
+                            R* pB, R* Ap, PcgState* st, double* part, int pairs) {
+        const int sg = spmv_grid(spmv_tiles<R, R, R, true, false, 4>), ug = vec_grid(pcg_update<R>);
+        for (int i = 0; i < pairs; ++i) {
+            spmv_tiles<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
+            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pB, Ap, V, part);
+            spmv_tiles<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pB, mask4, Ap, pA, st, part);
+            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pA, Ap, V, part);
+        }
+    }
+
+    // Solves mask K x = mask b (FP64 b, x): inner PCG in precision R on Kin (values of type R),
+    // FP64 residual refinement against Kres (FP64 values when res64, else Kin's values). The
+    // iterations run as a replayed CUDA graph of 32 iterations; the host checks the device
+    // state after each replay.
     template <typename R>
     PcgOut pcg(const void* Kin, const R* dinv, const void* Kres, bool res64, const double* mask, const double* b64,
                double* x64, double tol, int max_iters, int max_refine) {
         PcgOut out;
-        R* x = h.s_xcg.as<R>(n);
-        R* r = h.s_r.as<R>(n);
-        R* z = h.s_z.as<R>(n);
-        R* p = h.s_p.as<R>(n);
-        R* Ap = h.s_ap.as<R>(n);
-        R* bR = reinterpret_cast<R*>(h.s_trial.as<double>(n)); // scratch, reused
+        // The PCG vectors are padded to 4 values per vertex (4th value zero).
+        const size_t n4 = 4 * static_cast<size_t>(V);
+        R* x = h.s_xcg.as<R>(n4);
+        R* r = h.s_r.as<R>(n4);
+        R* z = h.s_z.as<R>(n4);
+        R* pA = h.s_p.as<R>(n4);
+        R* pB = h.s_p2.as<R>(n4);
+        R* Ap = h.s_ap.as<R>(n4);
+        R* bR = h.s_trial.as<R>(n4);
+        R* mask4 = h.s_mask4.as<R>(n4);
         double* r64 = h.s_r64.as<double>(n);
         double* y64 = h.s_b64.as<double>(n);
-        const int spmv_blocks = grid(static_cast<size_t>(V) * kSpmvGroup);
-        const int vb = grid(static_cast<size_t>(V));
-        double* part = h.s_part.as<double>(std::max(4 * 1024, 2 * std::max(spmv_blocks, vb)));
+        const int vg = vec_grid(pcg_init<R>);
+        const int pg = std::max(spmv_grid(spmv_tiles<R, R, R, true, false, 4>), vec_grid(pcg_update<R>));
+        double* part = h.s_part.as<double>(std::max(4 * 1024, 2 * std::max(pg, vg)));
         PcgState* st = reinterpret_cast<PcgState*>(h.s_scal.as<double>(64));
         LPG_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), s));
         LPG_CUDA(cudaMemcpyAsync(r64, b64, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         const double bnorm = std::sqrt(stats<double, double>(b64, nullptr, mask)[1]);
         if (bnorm == 0) return out;
+        pad_rhs<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(mask, mask, mask4, V); // 0/1 values: mask^2 = mask
+        // The graph of 16 iteration pairs, captured on the handle's own stream and cached.
+        constexpr int kPairs = 16;
+        constexpr int kKey = 12;
+        const void* key[kKey] = {Kin, dinv, mask4, x, r, z, pA, pB, Ap, st, part,
+                                 reinterpret_cast<const void*>(sizeof(R) * 1000003u + V)};
+        bool same = h.pcg_graph != nullptr;
+        for (int i = 0; i < kKey && same; ++i) same = h.pcg_graph_key[i] == key[i];
+        cudaStream_t gs = h.own_stream;
+        if (!same) {
+            if (h.pcg_graph) {
+                cudaGraphExecDestroy(h.pcg_graph);
+                h.pcg_graph = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            LPG_CUDA(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+            enqueue_iterations<R>(gs, static_cast<const R*>(Kin), dinv, mask4, x, r, z, pA, pB, Ap, st, part, kPairs);
+            LPG_CUDA(cudaStreamEndCapture(gs, &g));
+            LPG_CUDA(cudaGraphInstantiate(&h.pcg_graph, g, 0));
+            cudaGraphDestroy(g);
+            for (int i = 0; i < kKey; ++i) h.pcg_graph_key[i] = key[i];
+        }
+        cudaEvent_t ev;
+        LPG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         double rnorm = bnorm;
         for (int ref = 0; ref <= max_refine; ++ref) {
             const double inner_tol = std::min(0.5, std::max(tol * bnorm / rnorm, sizeof(R) == 4 ? 1e-6 : 1e-14));
-            convert_kernel<double, R><<<grid(n), kThreads, 0, s>>>(r64, bR, n);
-            pcg_init<R><<<vb, kThreads, 0, s>>>(bR, mask, dinv, x, r, z, p, V, part);
-            pcg_start<<<1, 1024, 0, s>>>(st, part, vb, inner_tol, max_iters - static_cast<int>(out.iters));
+            pad_rhs<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(r64, mask, bR, V);
+            pcg_init<R><<<vg, kThreads, 0, s>>>(bR, dinv, x, r, z, pA, V, part);
+            pcg_start<<<1, 1024, 0, s>>>(st, part, vg, inner_tol, max_iters - static_cast<int>(out.iters));
             LPG_CUDA(cudaGetLastError());
             PcgState hs{};
             for (;;) {
-                constexpr int kChunk = 16;
-                for (int it = 0; it < kChunk; ++it) {
-                    spmv<R>(Kin, sizeof(R) == 8 ? true : false, p, mask, Ap, part, &st->done, true);
-                    pcg_alpha<<<1, 1024, 0, s>>>(st, part, spmv_blocks);
-                    pcg_update<R><<<vb, kThreads, 0, s>>>(st, mask, dinv, x, r, z, p, Ap, V, part);
-                    pcg_beta<<<1, 1024, 0, s>>>(st, part, vb);
-                    pcg_pupdate<R><<<grid(n), kThreads, 0, s>>>(st, z, p, n);
-                }
-                LPG_CUDA(cudaGetLastError());
+                LPG_CUDA(cudaEventRecord(ev, s));
+                LPG_CUDA(cudaStreamWaitEvent(gs, ev, 0));
+                LPG_CUDA(cudaGraphLaunch(h.pcg_graph, gs));
+                LPG_CUDA(cudaEventRecord(ev, gs));
+                LPG_CUDA(cudaStreamWaitEvent(s, ev, 0));
                 LPG_CUDA(cudaMemcpyAsync(&hs, st, sizeof hs, cudaMemcpyDeviceToHost, s));
                 LPG_CUDA(cudaStreamSynchronize(s));
                 if (hs.done) break;
@@ -542,22 +738,17 @@ struct Solver {
             if (hs.breakdown) {
                 out.breakdown = true;
                 // Negative curvature on the first step: keep the preconditioned residual direction.
-                if (hs.iters == 0) LPG_CUDA(cudaMemcpyAsync(x, p, n * sizeof(R), cudaMemcpyDeviceToDevice, s));
+                if (hs.iters == 0) LPG_CUDA(cudaMemcpyAsync(x, pB, n4 * sizeof(R), cudaMemcpyDeviceToDevice, s));
             }
             add_kernel<R><<<grid(n), kThreads, 0, s>>>(x64, x, n);
-            // FP64 residual r64 = mask (b - Kres x64).
-            if (res64)
-                bsr_spmv<double, double, double, false><<<spmv_blocks, kThreads, 0, s>>>(
-                    h.dm.row_ptr, h.dm.col_idx, static_cast<const double*>(Kres), x64, mask, y64, V, nullptr, nullptr);
-            else
-                bsr_spmv<float, double, double, false><<<spmv_blocks, kThreads, 0, s>>>(
-                    h.dm.row_ptr, h.dm.col_idx, static_cast<const float*>(Kres), x64, mask, y64, V, nullptr, nullptr);
+            residual_spmv(Kres, res64, x64, mask, y64);
             residual_kernel<<<grid(n), kThreads, 0, s>>>(b64, y64, mask, r64, n);
             LPG_CUDA(cudaGetLastError());
             rnorm = std::sqrt(stats<double, double>(r64, nullptr, mask)[1]);
             out.rel = rnorm / bnorm;
             if (out.breakdown || !(rnorm > tol * bnorm) || out.iters >= max_iters || !std::isfinite(rnorm)) break;
         }
+        cudaEventDestroy(ev);
         return out;
     }
 };
@@ -573,8 +764,6 @@ void make_mask(lpg_fem& h, const int32_t* fixed, int nfixed, double* mask) {
     LPG_CUDA(cudaMemcpyAsync(mask, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, h.stream));
     LPG_CUDA(cudaStreamSynchronize(h.stream));
 }
-
-const int* diag_slots(lpg_fem& h) { return h.dm.diag_slot; }
 
 } // namespace
 
@@ -596,7 +785,6 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
     cudaStream_t s = h.stream;
     double* mask = h.s_mask.as<double>(std::max<size_t>(n, 1));
     make_mask(h, fixed, nfixed, mask);
-    const int* dslot = diag_slots(h);
     cudaEvent_t ev0, ev1;
     LPG_CUDA(cudaEventCreate(&ev0));
     LPG_CUDA(cudaEventCreate(&ev1));
@@ -617,7 +805,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
     const bool f64 = o.precision == LPG_PRECISION_F64;
     const size_t hbytes = 9 * static_cast<size_t>(h.dm.nnzb) * (f64 ? 8 : 4);
     void* K = h.s_hess.ensure(std::max<size_t>(hbytes, 8));
-    void* dinv = h.s_dinv.ensure(9 * static_cast<size_t>(std::max(V, 1)) * (f64 ? 8 : 4));
+    void* dinv = h.s_dinv.ensure(12 * static_cast<size_t>(std::max(V, 1)) * (f64 ? 8 : 4));
     double* rhs = h.s_g.as<double>(2 * std::max<size_t>(n, 1)) + std::max<size_t>(n, 1); // second half of s_g
     int* moved = reinterpret_cast<int*>(h.s_flag.as<int>(4));
     lpg_newton_result R{};
@@ -652,7 +840,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         // Energy and FP64 gradient (the Newton residual).
         double E;
         if (f64) {
-            h.eval_async(x, g, o.hessian, LPG_PRECISION_F64, LPG_LAYOUT_BSR, K, nullptr);
+            h.eval_async(x, g, o.hessian, LPG_PRECISION_F64, kLayoutTiled, K, nullptr);
             if (f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
             double e = 0;
             LPG_CUDA(cudaMemcpyAsync(&e, h.d_energy.ptr, sizeof e, cudaMemcpyDeviceToHost, s));
@@ -672,7 +860,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         if (converged) return finish(0);
         if (it == o.max_iterations) return finish(1);
         if (!f64) {
-            h.eval_async(x, nullptr, o.hessian, LPG_PRECISION_MIXED, LPG_LAYOUT_BSR, K, nullptr);
+            h.eval_async(x, nullptr, o.hessian, LPG_PRECISION_MIXED, kLayoutTiled, K, nullptr);
             raise_status(h.take_status());
         }
         // Descent direction with diagonal shifts (newton.cpp:55-72).
@@ -682,8 +870,8 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
             const int vb = grid(static_cast<size_t>(V));
             double* part = h.s_part.as<double>(std::max(4 * 1024, vb));
             double* outm = h.s_scal.as<double>(64) + 40;
-            diag_absmax_partial<<<vb, kThreads, 0, s>>>(f64 ? static_cast<double*>(K) : nullptr,
-                                                       f64 ? nullptr : static_cast<float*>(K), dslot, mask, V, part);
+            diag_absmax_partial<<<vb, kThreads, 0, s>>>(h.dm, f64 ? static_cast<double*>(K) : nullptr,
+                                                       f64 ? nullptr : static_cast<float*>(K), mask, part);
             max_final<<<1, 32, 0, s>>>(part, vb, outm);
             double m = 0;
             LPG_CUDA(cudaMemcpyAsync(&m, outm, sizeof m, cudaMemcpyDeviceToHost, s));
@@ -698,11 +886,11 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
             Solver::PcgOut po;
             if (f64) {
                 block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(
-                    static_cast<double*>(K), dslot, mask, static_cast<double*>(dinv), V);
+                    h.dm, static_cast<double*>(K), mask, static_cast<double*>(dinv), V);
                 po = S.pcg<double>(K, static_cast<double*>(dinv), K, true, mask, rhs, d, eta, o.cg_max_iterations, 0);
             } else {
                 block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(
-                    static_cast<float*>(K), dslot, mask, static_cast<float*>(dinv), V);
+                    h.dm, static_cast<float*>(K), mask, static_cast<float*>(dinv), V);
                 po = S.pcg<float>(K, static_cast<float*>(dinv), K, false, mask, rhs, d, eta, o.cg_max_iterations, 3);
             }
             R.cg_iterations += po.iters;
@@ -712,8 +900,8 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
                 break;
             }
             if (shifts == 10) break;
-            shift_diag<<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(f64 ? static_cast<double*>(K) : nullptr,
-                                                                       f64 ? nullptr : static_cast<float*>(K), dslot, V, shift);
+            shift_diag<<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, f64 ? static_cast<double*>(K) : nullptr,
+                                                                       f64 ? nullptr : static_cast<float*>(K), shift);
             shift *= 10.0;
         }
         if (!found) return finish(3);
@@ -759,7 +947,6 @@ void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const i
     cudaStream_t s = h.stream;
     double* mask = h.s_mask.as<double>(std::max<size_t>(n, 1));
     make_mask(h, fixed, nfixed, mask);
-    const int* dslot = diag_slots(h);
     const double* u = h.stage_in(u_star, io_mem, h.d_u, n);
     const double* w = h.stage_in(dLdu, io_mem, h.d_u2, n);
     double* lam = h.s_d.as<double>(std::max<size_t>(n, 1));
@@ -769,21 +956,21 @@ void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const i
     if (n > 0 && ws[1] > 0) {
         // Exact FP64 Hessian at u*: the residual matrix of the refinement (static_equilibrium_response.cpp:58).
         double* K64 = h.s_hess64.as<double>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
-        h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, LPG_LAYOUT_BSR, K64, nullptr);
+        h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutTiled, K64, nullptr);
         raise_status(h.take_status());
         double* rhs = h.s_g.as<double>(std::max<size_t>(n, 1));
         LPG_CUDA(cudaMemcpyAsync(rhs, w, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         Solver::PcgOut po;
         if (precision == LPG_PRECISION_F64) {
-            double* dinv = h.s_dinv.as<double>(9 * static_cast<size_t>(std::max(V, 1)));
-            block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(K64, dslot, mask, dinv, V);
+            double* dinv = h.s_dinv.as<double>(12 * static_cast<size_t>(std::max(V, 1)));
+            block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K64, mask, dinv, V);
             po = S.pcg<double>(K64, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 2);
         } else {
             float* K32 = h.s_hess.as<float>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
             const size_t nv = 9 * static_cast<size_t>(h.dm.nnzb);
             if (nv) convert_kernel<double, float><<<grid(nv), kThreads, 0, s>>>(K64, K32, nv);
-            float* dinv = h.s_dinv.as<float>(9 * static_cast<size_t>(std::max(V, 1)));
-            block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(K32, dslot, mask, dinv, V);
+            float* dinv = h.s_dinv.as<float>(12 * static_cast<size_t>(std::max(V, 1)));
+            block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K32, mask, dinv, V);
             po = S.pcg<float>(K32, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 30);
         }
         if (po.breakdown) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: singular or indefinite equilibrium stiffness");

@@ -32,12 +32,15 @@ struct lpg_fem {
     std::atomic<bool> busy{false};
     // Plan and element data.
     lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tile_pair_ptr, b_tile_row_ptr, b_tile_rows, b_tile_slot_ptr,
-        b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused;
+        b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused, b_spmv_tiles, b_spmv_row_tile;
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_status, d_tile_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
     // Solver state (Newton / PCG / adjoint).
     lpg::DeviceBuffer s_x, s_g, s_f, s_d, s_trial, s_mask, s_hess, s_hess64, s_dinv, s_r, s_z, s_p, s_ap, s_xcg, s_r64,
-        s_b64, s_scal, s_part, s_flag, d_flush;
+        s_b64, s_scal, s_part, s_flag, d_flush, s_p2, s_mask4;
+    // CUDA graph of a chunk of PCG iterations, reused while its pointers stay the same.
+    cudaGraphExec_t pcg_graph = nullptr;
+    const void* pcg_graph_key[12] = {};
     ~lpg_fem();
     void sync();
     unsigned take_status();

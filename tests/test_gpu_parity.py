@@ -275,3 +275,74 @@ def test_valence_above_32():
     assert abs(E - Er) <= TOL64 * abs(Er)
     assert rel_err(g, gr) <= TOL64
     assert rel_err(H.data, vr) <= TOL64
+
+
+def spmv_tile_rows(row_ptr):
+    """First row of each SpMV tile (and V): runs of consecutive rows with at most 32 blocks
+    and 32 rows (a row without blocks counts as one block), a longer row on its own."""
+    V = row_ptr.size - 1
+    starts, lanes, rows = [0], 0, 0
+    for v in range(V):
+        need = max(1, int(row_ptr[v + 1] - row_ptr[v]))
+        if rows > 0 and (lanes + need > 32 or rows == 32):
+            starts.append(v)
+            lanes = rows = 0
+        lanes += need
+        rows += 1
+        if need > 32:
+            starts.append(v + 1)
+            lanes = rows = 0
+    if rows > 0:
+        starts.append(V)
+    return np.array(starts)
+
+
+def tiled_values(e, u, hessian, precision, layout):
+    import ctypes
+
+    from litepgo_b200 import _native as N
+
+    dt = torch.float64 if precision == N.PRECISION_F64 else torch.float32
+    hess = torch.full((9 * e.nnzb,), float("nan"), dtype=dt, device="cuda")
+    ud = torch.as_tensor(u, device="cuda")
+    ma, me = ctypes.c_double(), ctypes.c_double()
+    N.check(N.lib.lpg_fem_time_eval(e.handle, N.vptr(ud), None, int(hessian), precision, layout, N.vptr(hess), 1, 0,
+                                    ctypes.byref(ma), ctypes.byref(me)))
+    return hess.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["box", "ragged", "valence"])
+def test_solver_tiled_layout_is_a_permutation_of_bsr(case):
+    """The Newton / adjoint solvers keep the Hessian tile-interleaved (entry t of block k of the
+    SpMV tile [k0, k0 + n) at 9 k0 + t n + k - k0); it must hold the BSR values bit for bit."""
+    from litepgo_b200 import _native as N
+
+    rng = np.random.default_rng(12)
+    if case == "box":
+        w = workloads.deformed_box(5, seed=2)
+        X, tets, theta, u = w["X"], w["tets"], w["theta"], w["u"]
+    elif case == "ragged":
+        X, t = mesh.make_box(4)
+        tets = t[np.random.default_rng(5).random(t.shape[0]) < 0.6]
+        theta, u = np.array([1.4e5, 3.4e4]), 0.01 * rng.standard_normal(X.size)
+    else:
+        k = 40
+        ang = np.linspace(0, 2 * np.pi, k, endpoint=False)
+        X = np.vstack([[0, 0, 0], [0, 0, 1], np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1)])
+        tets = np.array([[0, 2 + i, 2 + (i + 1) % k, 1] for i in range(k)], np.int32)
+        theta, u = np.array([2.0, 3.0]), 0.01 * rng.standard_normal(X.size)
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta)
+    row_ptr, _ = e.pattern_bsr()
+    starts = spmv_tile_rows(row_ptr)
+    perm = np.empty(9 * e.nnzb, np.int64)  # perm[bsr position] = tiled position
+    for r0, r1 in zip(starts[:-1], starts[1:]):
+        k0, k1 = int(row_ptr[r0]), int(row_ptr[r1])
+        ks = np.arange(k0, k1)
+        for t in range(9):
+            perm[9 * ks + t] = 9 * k0 + t * (k1 - k0) + (ks - k0)
+    assert np.array_equal(np.sort(perm), np.arange(9 * e.nnzb))
+    for hk in (Exact, Projected):
+        for prec in (N.PRECISION_F64, N.PRECISION_MIXED):
+            bsr = tiled_values(e, u, hk, prec, N.LAYOUT_BSR)
+            tiled = tiled_values(e, u, hk, prec, 2)
+            assert np.array_equal(tiled[perm], bsr)
