@@ -316,7 +316,7 @@ def run_ours(args):
     achieved = ab / (ma.value * 1e-3) / 1e9
     traffic = profile_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "assemble_kernel<double, true, 1>", "kernel_ms": ma.value,
+                "traffic": traffic, "kernel": "cluster_kernel<double, gradient, exact Hessian>", "kernel_ms": ma.value,
                 "algorithmic_bytes": ab, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
     # Mixed (FP32 element arithmetic + FP32 Hessian) kernel, reported beside it.
     hess32 = torch.empty(e.nnz, dtype=torch.float32, device=dev)
@@ -399,6 +399,30 @@ def run_kernels_only():
     return 0
 
 
+def run_newton_only(prec, iterations):
+    """A Newton solve of the bench workload cut at `iterations` Newton iterations, run twice
+    (the second with the PCG graph cached): a short command for ncu launch lists."""
+    import scipy.sparse as sp
+    import torch
+
+    from litepgo_b200 import dof, energy, fem, solver, workloads
+
+    torch.cuda.set_device(0)
+    g = workloads.gravity_box(N_CUBES, seed=0)
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(g["X"], g["tets"], g["theta"])
+    n = g["X"].size
+    total = energy.WeightedSumEnergy([(e, 1.0), (energy.QuadraticEnergy(sp.csc_matrix((n, n)), -g["f"]), 1.0)])
+    fixed = dof.DofReduction(n, g["fixed"])
+    x0 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    opts = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo", precision=prec,
+                                max_iterations=iterations, cg_tolerance=1e-2, cg_max_iterations=20000)
+    for _ in range(2):
+        r = solver.newton_solve(total, fixed, x0, opts)
+        print(json.dumps({"precision": prec, "status": r.status.name, "iterations": r.iterations,
+                          "cg_iterations": int(r.cg_iterations), "seconds": r.seconds}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -409,9 +433,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only-kernels", action="store_true",
                     help="run 3 evaluations of each assembly variant and exit (a short command for ncu)")
+    ap.add_argument("--only-newton", choices=("mixed", "f64"), default=None,
+                    help="run a Newton solve cut at --newton-iterations iterations and exit (for ncu launch lists)")
+    ap.add_argument("--newton-iterations", type=int, default=2)
     args = ap.parse_args()
     if args.only_kernels:
         return run_kernels_only()
+    if args.only_newton:
+        return run_newton_only(args.only_newton, args.newton_iterations)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -98,6 +98,18 @@ int lpg_mesh_pattern_bsr(int num_vertices, int num_tets, const int32_t* tets, in
 int lpg_mesh_plan_summary(int num_vertices, int num_tets, const int32_t* tets, int64_t out[6]);
 
 /*
+ * Host-only summary of the vertex clusters of the element-once assembly (no reference
+ * counterpart; it replaces the per-column contribution lists of EnergyAssembler,
+ * src/core/dof/energy_assembler.cpp:49-68, for the Exact Hessian): out[0] clusters,
+ * out[1] most rows in one cluster, out[2] most elements in one cluster, out[3] element
+ * evaluations per pass (sum over clusters), out[4] block contributor entries (16 per tet).
+ * The plan's invariants are checked (LPG_ELOGIC if one fails): every referenced vertex is
+ * owned by one cluster, every element's energy is counted once, and every block of every
+ * owned row lists exactly the elements that share its two vertices, in ascending order.
+ */
+int lpg_mesh_cluster_summary(int num_vertices, int num_tets, const int32_t* tets, int64_t out[5]);
+
+/*
  * Creates the element data and assembly plan of one tet mesh on `device`.
  * Replaces the constructor
  *   VolumetricFemEnergy(const VertexDofMap&, rest_positions, Fp, theta, int batch_size)

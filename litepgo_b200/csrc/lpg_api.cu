@@ -136,7 +136,8 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.grad = dgrad;
     a.hess = hessian != LPG_HESSIAN_NONE ? dhess : nullptr;
     a.layout = layout;
-    a.tile_energy = d_tile_energy.as<double>(static_cast<size_t>(dm.ntiles) + 256); // tiles, then partial sums
+    // Per-tile (or per-cluster) energies, then partial sums.
+    a.tile_energy = d_tile_energy.as<double>(static_cast<size_t>(std::max(dm.ntiles, dm.ncl)) + 256);
     a.energy = d_energy.as<double>(1);
     a.elem_energy = delem;
     a.status = d_status.as<unsigned>(1);
@@ -189,6 +190,28 @@ int lpg_mesh_plan_summary(int V, int T, const int32_t* tets, int64_t out[6]) {
         out[3] = p.cap;
         out[4] = max_rows;
         out[5] = static_cast<int64_t>(p.contrib.size());
+    });
+}
+
+int lpg_mesh_cluster_summary(int V, int T, const int32_t* tets, int64_t out[5]) {
+    return guarded([&] {
+        if (T > 0 && !tets) fail(LPG_EINVAL, "lpg_mesh_cluster_summary: null tets");
+        HostPlan p;
+        build_plan(V, T, tets, p);
+        check_clusters(p, tets);
+        const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
+        int64_t max_rows = 0, max_els = 0;
+        for (int c = 0; c < ncl; ++c) {
+            max_rows = std::max<int64_t>(max_rows, p.cl_row_ptr[c + 1] - p.cl_row_ptr[c]);
+            max_els = std::max<int64_t>(max_els, p.cl_el_ptr[c + 1] - p.cl_el_ptr[c]);
+        }
+        out[0] = ncl;
+        out[1] = max_rows;
+        out[2] = max_els;
+        out[3] = static_cast<int64_t>(p.cl_els.size());
+        int64_t contributors = 0;
+        for (uint32_t de : p.cl_slot_ent) contributors += de >> 20;
+        out[4] = contributors;
     });
 }
 
@@ -278,6 +301,22 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         m.spmv_tile_row = upload(h->b_spmv_tiles, p.spmv_tile_row);
         m.n_spmv_tiles = static_cast<int>(p.spmv_tile_row.size()) - 1;
         m.spmv_row_tile = upload(h->b_spmv_row_tile, p.spmv_row_tile);
+        m.ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
+        m.cl_row_ptr = upload(h->b_cl[0], p.cl_row_ptr);
+        m.cl_rows = upload(h->b_cl[1], p.cl_rows);
+        m.cl_el_ptr = upload(h->b_cl[2], p.cl_el_ptr);
+        m.cl_els = upload(h->b_cl[3], p.cl_els);
+        m.cl_slot_ptr = upload(h->b_cl[4], p.cl_slot_ptr);
+        m.cl_noff = upload(h->b_cl[5], p.cl_noff);
+        m.cl_slot = upload(h->b_cl[6], p.cl_slot);
+        m.cl_slot_ent = upload(h->b_cl[7], p.cl_slot_ent);
+        m.cl_ent_ptr = upload(h->b_cl[8], p.cl_ent_ptr);
+        m.cl_ents = upload(h->b_cl[9], p.cl_ents);
+        m.cl_max_slots = m.cl_max_ents = 0;
+        for (int c = 0; c < m.ncl; ++c) {
+            m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);
+            m.cl_max_ents = std::max(m.cl_max_ents, p.cl_ent_ptr[c + 1] - p.cl_ent_ptr[c]);
+        }
         std::vector<int32_t> tv(tets, tets + 4 * static_cast<size_t>(T));
         m.tets = reinterpret_cast<int4*>(upload(h->b_tets, tv));
         m.rec64 = upload(h->b_rec64, rec);

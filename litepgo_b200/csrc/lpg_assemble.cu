@@ -22,6 +22,8 @@
 #include <cstdint>
 #include <cstdio>
 
+#include <cuda_pipeline.h>
+
 #include "lpg_internal.h"
 
 namespace lpg {
@@ -982,6 +984,297 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
+// ---------------------------------------------------------------------------
+// Element-once assembly over vertex clusters (Exact Hessian, gradient, energy).
+//
+// One thread block per cluster of owned rows. Phase 1 evaluates every element incident to
+// the cluster once (one thread per element) and keeps, per element, h_a = F^-T grad N_a,
+// the gradient pieces g_a = vol P grad N_a, vol lambda, vol p and vol mu (grad N_a . grad N_b)
+// in shared memory. Phase 2 gives each block slot of the cluster's rows to one thread, which
+// sums the slot's contributions in ascending element order in registers and stores the
+// block once: no atomics, and an off-diagonal slot is evaluated in the orientation of its
+// lower-numbered vertex so that the two blocks of an edge are exact transposes.
+// ---------------------------------------------------------------------------
+#ifndef LPG_CLUSTER_THREADS
+#define LPG_CLUSTER_THREADS 128
+#endif
+#ifndef LPG_CLUSTER_MIN_BLOCKS_F64
+#define LPG_CLUSTER_MIN_BLOCKS_F64 3
+#endif
+#ifndef LPG_CLUSTER_MIN_BLOCKS_F32
+#define LPG_CLUSTER_MIN_BLOCKS_F32 6
+#endif
+constexpr int kClThreads = LPG_CLUSTER_THREADS;
+template <typename R> struct ClMinBlocks;
+template <> struct ClMinBlocks<double> { static constexpr int value = LPG_CLUSTER_MIN_BLOCKS_F64; };
+template <> struct ClMinBlocks<float> { static constexpr int value = LPG_CLUSTER_MIN_BLOCKS_F32; };
+
+// Index of the unordered vertex pair (a, b) of a tet among its 10.
+__device__ __forceinline__ int pair10(int a, int b) {
+    const int lo = min(a, b), hi = max(a, b);
+    return lo * 4 - (lo * (lo - 1)) / 2 + (hi - lo);
+}
+
+// Shared memory of the cluster kernel: energy partials, per-element data, the row table, and
+// the cluster's slot words and contributor lists (sized by the mesh's largest cluster).
+template <typename R, bool WG, bool WH> constexpr size_t cl_smem_fixed() {
+    return 32 * sizeof(double) + sizeof(R) * static_cast<size_t>(kClusterElems) * ((WH ? 24 : 0) + (WG ? 12 : 0)) +
+           5 * kClusterRows * sizeof(int);
+}
+template <typename R, bool WG, bool WH> size_t cl_smem_bytes(const DevMesh& m) {
+    const size_t slots = (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16;
+    return cl_smem_fixed<R, WG, WH>() + slots + 2 * static_cast<size_t>(m.cl_max_ents);
+}
+
+__device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int tk0, int tn, int q, int t) {
+    if (layout == LPG_LAYOUT_BSR) return 9 * static_cast<size_t>(slot0 + q) + t;
+    if (layout == LPG_LAYOUT_CSC) {
+        const int i = t / 3, c = t - 3 * (t / 3);
+        return 9 * static_cast<size_t>(slot0) + static_cast<size_t>(i) * 3 * nb + 3 * q + c;
+    }
+    return 9 * static_cast<size_t>(tk0) + static_cast<size_t>(t) * tn + (slot0 + q - tk0);
+}
+
+template <typename R, bool WG, bool WH>
+__global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_kernel(const DevMesh m, const EvalArgs a) {
+    using X = M<R>;
+    using HT = typename HOut<R>::T;
+    constexpr int E = kClusterElems;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* red = reinterpret_cast<double*>(smem_raw);
+    R* sh = reinterpret_cast<R*>(smem_raw + 32 * sizeof(double));
+    R* hv = sh;                        // [12][E] h_a components (WH)
+    R* cc = sh + 12 * E;               // [10][E] vol mu grad N_a . grad N_b (WH)
+    R* lp = sh + 22 * E;               // [2][E] vol lambda, vol p (WH)
+    R* gv = sh + (WH ? 24 * E : 0);    // [12][E] g_a components (WG)
+    int* rt = reinterpret_cast<int*>(sh + static_cast<size_t>(E) * ((WH ? 24 : 0) + (WG ? 12 : 0)));
+    uint32_t* sslot = reinterpret_cast<uint32_t*>(smem_raw + cl_smem_fixed<R, WG, WH>());
+    uint32_t* sslote = sslot + m.cl_max_slots;
+    uint16_t* sent = reinterpret_cast<uint16_t*>(smem_raw + cl_smem_fixed<R, WG, WH>() +
+                                                 (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16);
+    const int tid = threadIdx.x, bd = blockDim.x;
+    unsigned st = 0;
+    // The first element of each thread is fetched one cluster ahead.
+    uint32_t pf_ew = 0;
+    int4 pf_tv = make_int4(0, 0, 0, 0);
+    auto prefetch = [&](int cl) {
+        if (cl < m.ncl) {
+            const int e0 = __ldg(m.cl_el_ptr + cl);
+            if (tid < __ldg(m.cl_el_ptr + cl + 1) - e0) {
+                pf_ew = __ldg(m.cl_els + e0 + tid);
+                pf_tv = __ldg(m.tets + (pf_ew & 0x7fffffffu));
+            }
+        }
+    };
+    prefetch(blockIdx.x);
+    for (int cl = blockIdx.x; cl < m.ncl; cl += gridDim.x) {
+        // Stage the cluster's slot words and contributor lists (asynchronous copies).
+        const int s0 = __ldg(m.cl_slot_ptr + cl), ns = __ldg(m.cl_slot_ptr + cl + 1) - s0;
+        if (WG || WH) {
+            const int eb = __ldg(m.cl_ent_ptr + cl), n16 = (__ldg(m.cl_ent_ptr + cl + 1) - eb) / 8;
+            for (int i = tid; i < ns; i += bd) {
+                __pipeline_memcpy_async(sslot + i, m.cl_slot + s0 + i, 4);
+                __pipeline_memcpy_async(sslote + i, m.cl_slot_ent + s0 + i, 4);
+            }
+            for (int i = tid; i < n16; i += bd)
+                __pipeline_memcpy_async(reinterpret_cast<uint4*>(sent) + i, reinterpret_cast<const uint4*>(m.cl_ents + eb) + i, 16);
+            __pipeline_commit();
+        }
+        // Phase 1: the cluster's elements, once each.
+        const int e0 = __ldg(m.cl_el_ptr + cl), ne = __ldg(m.cl_el_ptr + cl + 1) - e0;
+        double eacc = 0;
+        for (int el = tid; el < ne; el += bd) {
+            const uint32_t ew = el == tid ? pf_ew : __ldg(m.cl_els + e0 + el);
+            const int e = static_cast<int>(ew & 0x7fffffffu);
+            const int4 tv = el == tid ? pf_tv : __ldg(m.tets + e);
+            Kin<R> k;
+            st |= kinematics<R>(m, e, tv, a.u, k);
+            if (ew >> 31) {
+                const R Ee = k.vol * k.psi;
+                eacc += static_cast<double>(Ee);
+                if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
+            }
+            const R p = X::fma(k.lam, k.logJ, -k.mu);
+            if (WG) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        R s = 0;
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+                            s = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[b][j], s);
+                        gv[(3 * b + i) * E + el] = k.vol * s;
+                    }
+            }
+            if (WH) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        hv[(3 * b + i) * E + el] =
+                            X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
+                lp[el] = X::mul(k.vol, k.lam);
+                lp[E + el] = X::mul(k.vol, p);
+                const R mv = X::mul(k.vol, k.mu);
+#pragma unroll
+                for (int x = 0; x < 4; ++x)
+#pragma unroll
+                    for (int y = x; y < 4; ++y)
+                        cc[pair10(x, y) * E + el] =
+                            X::mul(mv, X::fma(k.n[x][2], k.n[y][2], X::fma(k.n[x][1], k.n[y][1], X::mul(k.n[x][0], k.n[y][0]))));
+            }
+        }
+        // Energy of the cluster's own elements: fixed thread order, fixed tree.
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, off);
+        if ((tid & 31) == 0) red[tid >> 5] = eacc;
+        // Row table: vertex, first block, block count, and the SpMV tile of the row (tiled layout).
+        const int r0 = __ldg(m.cl_row_ptr + cl), nr = __ldg(m.cl_row_ptr + cl + 1) - r0;
+        for (int j = tid; j < nr; j += bd) {
+            const int v = __ldg(m.cl_rows + r0 + j);
+            const int sb = __ldg(m.row_ptr + v);
+            rt[j] = v;
+            rt[kClusterRows + j] = sb;
+            rt[2 * kClusterRows + j] = __ldg(m.row_ptr + v + 1) - sb;
+            if (a.layout == kLayoutTiled) {
+                const int t = __ldg(m.spmv_row_tile + v);
+                const int k0 = __ldg(m.row_ptr + __ldg(m.spmv_tile_row + t));
+                rt[3 * kClusterRows + j] = k0;
+                rt[4 * kClusterRows + j] = __ldg(m.row_ptr + __ldg(m.spmv_tile_row + t + 1)) - k0;
+            }
+        }
+        prefetch(cl + gridDim.x);
+        if (WG || WH) __pipeline_wait_prior(0);
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0;
+            for (int w = 0; w < (bd >> 5); ++w) t += red[w];
+            a.tile_energy[cl] = t;
+            if (!isfinite(t)) st |= ST_NONFINITE_OUT;
+        }
+        // Phase 2: one thread per block slot (off-diagonal slots first, then diagonal slots,
+        // so that warps mostly hold slots of one kind).
+        if (WG || WH) {
+            const int noff = __ldg(m.cl_noff + cl);
+            HT* hout = reinterpret_cast<HT*>(a.hess);
+            for (int s = (WH ? 0 : noff) + tid; s < ns; s += bd) {
+                const uint32_t d = sslot[s], de = sslote[s];
+                const int j = d & 0xffu, q = (d >> 8) & 0x3fffffu;
+                const uint16_t* en = sent + (de & 0xfffffu);
+                const int cnt = static_cast<int>(de >> 20);
+                const int slot0 = rt[kClusterRows + j], nb = rt[2 * kClusterRows + j];
+                const int tk0 = rt[3 * kClusterRows + j], tn = rt[4 * kClusterRows + j];
+                if (d >> 31) {
+                    // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient.
+                    R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
+                    for (int c = 0; c < cnt; ++c) {
+                        const int w = en[c];
+                        const int el = w >> 4, la = (w >> 2) & 3;
+                        if (WG) {
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) gs[i] = X::add(gs[i], gv[(3 * la + i) * E + el]);
+                        }
+                        if (WH) {
+                            // H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
+                            const R hh[3] = {hv[(3 * la) * E + el], hv[(3 * la + 1) * E + el], hv[(3 * la + 2) * E + el]};
+                            const R dv = X::add(lp[el], -lp[E + el]), mg = cc[pair10(la, la) * E + el];
+                            int u = 0;
+#pragma unroll
+                            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                                for (int kk = i; kk < 3; ++kk, ++u) {
+                                    acc[u] = X::fma(dv, X::mul(hh[i], hh[kk]), acc[u]);
+                                    if (i == kk) acc[u] = X::add(acc[u], mg);
+                                }
+                        }
+                    }
+                    const int v = rt[j];
+                    if (WG) {
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            if (!X::finite(gs[i])) st |= ST_NONFINITE_OUT;
+                            a.grad[3 * static_cast<size_t>(v) + i] = static_cast<double>(gs[i]);
+                        }
+                    }
+                    if (WH) {
+                        constexpr int sym3[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+#pragma unroll
+                        for (int t = 0; t < 9; ++t) {
+                            const R val = acc[sym3[t]];
+                            if (!X::finite(val)) st |= ST_NONFINITE_OUT;
+                            hout[cl_pos(a.layout, slot0, nb, tk0, tn, q, t)] = static_cast<HT>(val);
+                        }
+                    }
+                } else if (WH) {
+                    // Off-diagonal block in the orientation of the lower vertex (a) -> higher (b):
+                    //   C += vol lambda h_a h_b^T - vol p h_b h_a^T + vol mu (grad N_a . grad N_b) I.
+                    R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                    for (int c = 0; c < cnt; ++c) {
+                        const int w = en[c];
+                        const int el = w >> 4, ra = (w >> 2) & 3, cb = w & 3;
+                        R ha[3], hb[3];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            ha[i] = hv[(3 * ra + i) * E + el];
+                            hb[i] = hv[(3 * cb + i) * E + el];
+                        }
+                        const R lv = lp[el], pv = lp[E + el], mg = cc[pair10(ra, cb) * E + el];
+                        R A[3], B[3];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            A[i] = X::mul(lv, ha[i]);
+                            B[i] = X::mul(-pv, ha[i]);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int kk = 0; kk < 3; ++kk) {
+                                acc[3 * i + kk] = X::fma(B[kk], hb[i], X::fma(A[i], hb[kk], acc[3 * i + kk]));
+                                if (i == kk) acc[3 * i + kk] = X::add(acc[3 * i + kk], mg);
+                            }
+                    }
+                    const bool tr = (d >> 30) & 1u;
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) {
+                        const int i = t / 3, kk = t - 3 * (t / 3);
+                        const R val = tr ? acc[3 * kk + i] : acc[t];
+                        if (!X::finite(val)) st |= ST_NONFINITE_OUT;
+                        hout[cl_pos(a.layout, slot0, nb, tk0, tn, q, t)] = static_cast<HT>(val);
+                    }
+                }
+            }
+        }
+        __syncthreads(); // the next cluster reuses the shared element data
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((tid & 31) == 0 && st) atomicOr(a.status, st);
+}
+
+template <typename R, bool WG, bool WH> void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    const size_t sm = cl_smem_bytes<R, WG, WH>(m);
+    // Resident blocks for this shared-memory size (cached for the last size seen).
+    thread_local size_t cached_sm = 0;
+    thread_local int resident = 0;
+    if (cached_sm != sm) {
+        int dev = 0, sms = 0, per_sm = 0, optin = 0;
+        LPG_CUDA(cudaGetDevice(&dev));
+        LPG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (sm > static_cast<size_t>(optin)) fail(LPG_EINVAL, "mesh cluster needs more shared memory than the GPU has");
+        LPG_CUDA(cudaFuncSetAttribute(cluster_kernel<R, WG, WH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sm)));
+        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_kernel<R, WG, WH>, kClThreads, sm));
+        resident = std::max(1, sms * std::max(per_sm, 1));
+        cached_sm = sm;
+    }
+    const int blocks = std::min(resident, m.ncl);
+    if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
+    if (blocks > 0) cluster_kernel<R, WG, WH><<<blocks, kClThreads, sm, s>>>(m, a);
+    if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
+    LPG_CUDA(cudaGetLastError());
+}
+
 template <typename R, bool WG, int WH, int CHUNKS> void launch_assemble(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = kWarpsPerBlock * smem_per_warp<R, WH>(32 * CHUNKS);
     static bool configured = false;
@@ -1015,29 +1308,32 @@ template <typename R, bool WG, int WH> void launch_chunks(const DevMesh& m, cons
         launch_assemble<R, WG, WH, 2>(m, a, s);
 }
 
-template <typename R> void launch_eval_t(const DevMesh& m, int hessian, const EvalArgs& a, cudaStream_t s) {
+// Launches the element pass; returns the number of per-unit energies it wrote to tile_energy.
+// The Exact Hessian, gradient and energy use the element-once cluster kernel; the projected
+// Hessian uses the pair kernel over the per-element clamped tangents.
+template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const EvalArgs& a, cudaStream_t s) {
     const bool wg = a.grad != nullptr;
     const int wh = a.hess == nullptr ? 0 : (hessian == LPG_HESSIAN_EXACT ? 1 : 2);
-    if (wg && wh == 1) launch_chunks<R, true, 1>(m, a, s);
-    else if (wg && wh == 2) launch_chunks<R, true, 2>(m, a, s);
-    else if (!wg && wh == 1) launch_chunks<R, false, 1>(m, a, s);
-    else if (!wg && wh == 2) launch_chunks<R, false, 2>(m, a, s);
-    else if (wg) launch_chunks<R, true, 0>(m, a, s);
-    else launch_chunks<R, false, 0>(m, a, s);
+    int units = m.ncl;
+    if (wg && wh == 1) launch_cluster<R, true, true>(m, a, s);
+    else if (wg && wh == 2) launch_chunks<R, true, 2>(m, a, s), units = m.ntiles;
+    else if (!wg && wh == 1) launch_cluster<R, false, true>(m, a, s);
+    else if (!wg && wh == 2) launch_chunks<R, false, 2>(m, a, s), units = m.ntiles;
+    else if (wg) launch_cluster<R, true, false>(m, a, s);
+    else launch_cluster<R, false, false>(m, a, s);
     if (wg && m.num_unused > 0)
         zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
+    return units;
 }
 
 } // namespace
 
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s) {
-    if (precision == LPG_PRECISION_F64)
-        launch_eval_t<double>(m, hessian, a, s);
-    else
-        launch_eval_t<float>(m, hessian, a, s);
-    // Per-tile energies -> partials (stored after the tiles) -> total.
-    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(a.tile_energy, m.ntiles, a.tile_energy + m.ntiles);
-    sum_final_kernel<<<1, 256, 0, s>>>(a.tile_energy + m.ntiles, kSumBlocks, a.energy);
+    const int units = precision == LPG_PRECISION_F64 ? launch_eval_t<double>(m, hessian, a, s)
+                                                      : launch_eval_t<float>(m, hessian, a, s);
+    // Per-unit energies -> partials (stored after the units) -> total.
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(a.tile_energy, units, a.tile_energy + units);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.tile_energy + units, kSumBlocks, a.energy);
     LPG_CUDA(cudaGetLastError());
 }
 

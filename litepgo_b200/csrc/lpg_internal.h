@@ -57,12 +57,40 @@ struct HostPlan {
     std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
     std::vector<int32_t> spmv_tile_row;      // SpMV tiles: first row of each, plus V
     std::vector<int32_t> spmv_row_tile;      // V: SpMV tile of each row
+    // Vertex clusters of the element-once assembly (one thread block per cluster): the rows a
+    // cluster owns, the elements incident to them (ascending; bit 31 set on the elements whose
+    // energy the cluster counts, those whose first vertex it owns), and its block slots,
+    // off-diagonal first, then diagonal. Slot word: bits 0-7 the row within the cluster, bits
+    // 8-29 the slot's position within its row, bit 30 "store the transpose", bit 31 diagonal.
+    // Entry word of a slot: bits 0-19 first contributor (within the cluster), 20-31 count.
+    // Contributors (uint16): element within the cluster << 4 | a << 2 | b, where (a, b) are
+    // the local indices of the lower- and higher-numbered vertex of the slot (a = b diagonal).
+    std::vector<int32_t> cl_row_ptr, cl_rows;
+    std::vector<int32_t> cl_el_ptr;
+    std::vector<uint32_t> cl_els;
+    std::vector<int32_t> cl_slot_ptr, cl_noff;
+    std::vector<uint32_t> cl_slot, cl_slot_ent;
+    std::vector<int32_t> cl_ent_ptr;
+    std::vector<uint16_t> cl_ents;
     int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
     int64_t nnzb() const { return static_cast<int64_t>(col_idx.size()); }
 };
 
+// Size limits of an assembly cluster: owned rows, and distinct incident elements (the
+// element data of a cluster is held in shared memory).
+#ifndef LPG_CLUSTER_ROWS
+#define LPG_CLUSTER_ROWS 24
+#endif
+#ifndef LPG_CLUSTER_ELEMS
+#define LPG_CLUSTER_ELEMS 224
+#endif
+constexpr int kClusterRows = LPG_CLUSTER_ROWS;
+constexpr int kClusterElems = LPG_CLUSTER_ELEMS;
+
 // Validates connectivity (mesh_topology.hpp:25-44) and builds the plan.
 void build_plan(int V, int T, const int32_t* tets, HostPlan& plan);
+// Checks the cluster plan's invariants (throws LPG_ELOGIC on a violation).
+void check_clusters(const HostPlan& plan, const int32_t* tets);
 
 // Device mirror of the plan and of the per-element records.
 struct DevMesh {
@@ -79,6 +107,11 @@ struct DevMesh {
     int32_t* spmv_tile_row = nullptr;
     int32_t* spmv_row_tile = nullptr;
     int n_spmv_tiles = 0;
+    int ncl = 0, cl_max_slots = 0, cl_max_ents = 0;
+    int32_t *cl_row_ptr = nullptr, *cl_rows = nullptr, *cl_el_ptr = nullptr, *cl_slot_ptr = nullptr, *cl_noff = nullptr,
+            *cl_ent_ptr = nullptr;
+    uint32_t *cl_els = nullptr, *cl_slot = nullptr, *cl_slot_ent = nullptr;
+    uint16_t* cl_ents = nullptr;
     int4* tets = nullptr;
     // Per-element record: G (3x3 row-major, rows = grad N_1..3 in rest coordinates, times Fp^-1),
     // vol (= det(Dm)/6 * det Fp), lambda, mu. 12 values, 16-byte aligned.

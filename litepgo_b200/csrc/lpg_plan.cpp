@@ -17,6 +17,137 @@
 
 namespace lpg {
 
+namespace {
+
+// Vertex clusters for the element-once assembly. A cluster grows breadth-first over the vertex
+// adjacency from the lowest unassigned vertex until it owns kClusterRows rows or one more row
+// would bring its distinct incident elements above kClusterElems (such a row is left for a
+// later cluster). Each block slot of an owned row lists its contributing elements in ascending
+// element order (the reference's summation order per block); an off-diagonal slot is
+// evaluated in the orientation of its lower-numbered vertex, so slot (v, w) and slot (w, v)
+// are computed by the same operations and are exact transposes.
+void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>& inc) {
+    const int V = p.V, T = p.T;
+    constexpr int kMaskE = (1 << 30) - 1;
+    std::vector<int32_t> cl_of(static_cast<size_t>(V), -1), qstamp(static_cast<size_t>(V), -1);
+    std::vector<int32_t> estamp(static_cast<size_t>(T), -1);
+    std::vector<int32_t> queue;
+    int ncl = 0;
+    for (int seed = 0; seed < V; ++seed) {
+        if (cl_of[seed] >= 0 || p.inc_ptr[seed + 1] == p.inc_ptr[seed]) continue;
+        const int c = ncl++;
+        queue.assign(1, seed);
+        qstamp[seed] = c;
+        int nr = 0, ne = 0;
+        for (size_t qi = 0; qi < queue.size() && nr < kClusterRows; ++qi) {
+            const int v = queue[qi];
+            if (cl_of[v] >= 0) continue;
+            int add = 0;
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) add += estamp[inc[k] & kMaskE] != c;
+            if (ne + add > kClusterElems) continue;
+            cl_of[v] = c;
+            ++nr;
+            ne += add;
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) estamp[inc[k] & kMaskE] = c;
+            for (int k = p.row_ptr[v]; k < p.row_ptr[v + 1]; ++k) {
+                const int w = p.col_idx[k];
+                if (cl_of[w] < 0 && qstamp[w] != c && p.inc_ptr[w + 1] > p.inc_ptr[w]) {
+                    qstamp[w] = c;
+                    queue.push_back(w);
+                }
+            }
+        }
+    }
+    // Rows of each cluster, ascending.
+    p.cl_row_ptr.assign(static_cast<size_t>(ncl) + 1, 0);
+    for (int v = 0; v < V; ++v)
+        if (cl_of[v] >= 0) ++p.cl_row_ptr[cl_of[v] + 1];
+    for (int c = 0; c < ncl; ++c) p.cl_row_ptr[c + 1] += p.cl_row_ptr[c];
+    p.cl_rows.assign(static_cast<size_t>(p.cl_row_ptr[ncl]), 0);
+    {
+        std::vector<int32_t> fill(p.cl_row_ptr.begin(), p.cl_row_ptr.end() - 1);
+        for (int v = 0; v < V; ++v)
+            if (cl_of[v] >= 0) p.cl_rows[fill[cl_of[v]]++] = v;
+    }
+    p.cl_el_ptr.assign(1, 0);
+    p.cl_slot_ptr.assign(1, 0);
+    p.cl_ent_ptr.assign(1, 0);
+    p.cl_els.clear();
+    p.cl_noff.clear();
+    p.cl_slot.clear();
+    p.cl_slot_ent.clear();
+    p.cl_ents.clear();
+    std::vector<int32_t> eloc(static_cast<size_t>(T), -1), els;
+    std::vector<std::vector<uint16_t>> bucket;
+    std::vector<std::vector<uint16_t>> diag;
+    for (int c = 0; c < ncl; ++c) {
+        const int r0 = p.cl_row_ptr[c], nr = p.cl_row_ptr[c + 1] - r0;
+        els.clear();
+        for (int j = 0; j < nr; ++j) {
+            const int v = p.cl_rows[r0 + j];
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) els.push_back(inc[k] & kMaskE);
+        }
+        std::sort(els.begin(), els.end());
+        els.erase(std::unique(els.begin(), els.end()), els.end());
+        for (size_t i = 0; i < els.size(); ++i) {
+            const int e = els[i];
+            eloc[e] = static_cast<int32_t>(i);
+            const bool owner = cl_of[tets[4 * static_cast<size_t>(e)]] == c;
+            p.cl_els.push_back(static_cast<uint32_t>(e) | (owner ? 0x80000000u : 0u));
+        }
+        p.cl_el_ptr.push_back(static_cast<int32_t>(p.cl_els.size()));
+        const size_t ent0 = p.cl_ents.size();
+        diag.assign(static_cast<size_t>(nr), {});
+        int noff = 0;
+        for (int j = 0; j < nr; ++j) {
+            const int v = p.cl_rows[r0 + j];
+            const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
+            bucket.assign(static_cast<size_t>(nb), {});
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
+                const int e = inc[k] & kMaskE, a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> 30);
+                const uint16_t el = static_cast<uint16_t>(eloc[e] << 4);
+                for (int b = 0; b < 4; ++b) {
+                    const int w = tets[4 * static_cast<size_t>(e) + b];
+                    if (w == v) {
+                        diag[j].push_back(static_cast<uint16_t>(el | (a << 2) | a));
+                        continue;
+                    }
+                    const int32_t* beg = p.col_idx.data() + rb;
+                    const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
+                    bucket[q].push_back(static_cast<uint16_t>(v < w ? (el | (a << 2) | b) : (el | (b << 2) | a)));
+                }
+            }
+            for (int q = 0; q < nb; ++q) {
+                const int w = p.col_idx[rb + q];
+                if (w == v) continue;
+                p.cl_slot.push_back(static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (v > w ? 1u << 30 : 0u));
+                p.cl_slot_ent.push_back(static_cast<uint32_t>(p.cl_ents.size() - ent0) |
+                                        (static_cast<uint32_t>(bucket[q].size()) << 20));
+                p.cl_ents.insert(p.cl_ents.end(), bucket[q].begin(), bucket[q].end());
+                ++noff;
+            }
+        }
+        for (int j = 0; j < nr; ++j) {
+            const int v = p.cl_rows[r0 + j];
+            const int q = p.diag_slot[v] - p.row_ptr[v];
+            p.cl_slot.push_back(static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (1u << 31));
+            p.cl_slot_ent.push_back(static_cast<uint32_t>(p.cl_ents.size() - ent0) |
+                                    (static_cast<uint32_t>(diag[j].size()) << 20));
+            p.cl_ents.insert(p.cl_ents.end(), diag[j].begin(), diag[j].end());
+        }
+        if (p.cl_ents.size() - ent0 >= (1u << 20) ||
+            p.cl_ents.size() >= static_cast<size_t>(std::numeric_limits<int32_t>::max()))
+            fail(LPG_EINVAL, "mesh too large for the assembly plan's index ranges");
+        while (p.cl_ents.size() % 8 != 0) p.cl_ents.push_back(0); // 16-byte aligned per cluster
+        p.cl_noff.push_back(noff);
+        p.cl_slot_ptr.push_back(static_cast<int32_t>(p.cl_slot.size()));
+        p.cl_ent_ptr.push_back(static_cast<int32_t>(p.cl_ents.size()));
+        for (int e : els) eloc[e] = -1;
+    }
+}
+
+} // namespace
+
 void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
     if (V < 0 || T < 0) fail(LPG_EINVAL, "MeshTopology requires a non-negative vertex count");
     if (V > std::numeric_limits<int>::max() / 3) fail(LPG_EINVAL, "VertexDofMap requires total DOFs fitting in int");
@@ -181,6 +312,95 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
         p.tile_row_ptr[t + 1] = static_cast<int32_t>(p.tile_rows.size());
         p.tile_slot_ptr[t + 1] = static_cast<int32_t>(p.tile_slot_ptr[t] + slots);
     }
+    build_clusters(p, tets, inc);
+}
+
+void check_clusters(const HostPlan& p, const int32_t* tets) {
+    const int V = p.V, T = p.T;
+    const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
+    auto bad = [](const char* what) { fail(LPG_ELOGIC, std::string("assembly cluster plan: ") + what); };
+    auto vert = [&](int e, int a) { return tets[4 * static_cast<size_t>(e) + a]; };
+    // Incidence (vertex -> elements, ascending), independent of the plan's own.
+    std::vector<int32_t> ptr(static_cast<size_t>(V) + 1, 0), inc(4 * static_cast<size_t>(T));
+    for (size_t k = 0; k < 4 * static_cast<size_t>(T); ++k) ++ptr[tets[k] + 1];
+    for (int v = 0; v < V; ++v) ptr[v + 1] += ptr[v];
+    {
+        std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (int e = 0; e < T; ++e)
+            for (int a = 0; a < 4; ++a) inc[fill[vert(e, a)]++] = e;
+    }
+    std::vector<int> owner(static_cast<size_t>(V), -1), energy_count(static_cast<size_t>(T), 0);
+    for (int c = 0; c < ncl; ++c)
+        for (int k = p.cl_row_ptr[c]; k < p.cl_row_ptr[c + 1]; ++k) {
+            if (owner[p.cl_rows[k]] >= 0) bad("vertex owned twice");
+            owner[p.cl_rows[k]] = c;
+        }
+    for (int v = 0; v < V; ++v)
+        if ((owner[v] >= 0) != (ptr[v + 1] > ptr[v])) bad("referenced vertex without a cluster");
+    for (int c = 0; c < ncl; ++c) {
+        const int e0 = p.cl_el_ptr[c], ne = p.cl_el_ptr[c + 1] - e0;
+        if (p.cl_row_ptr[c + 1] - p.cl_row_ptr[c] > kClusterRows || ne > kClusterElems) bad("cluster over its limits");
+        for (int i = 0; i < ne; ++i) {
+            const int e = static_cast<int>(p.cl_els[e0 + i] & 0x7fffffffu);
+            if (i > 0 && e <= static_cast<int>(p.cl_els[e0 + i - 1] & 0x7fffffffu)) bad("elements not ascending");
+            bool touches = false;
+            for (int a = 0; a < 4; ++a) touches = touches || owner[vert(e, a)] == c;
+            if (!touches) bad("element not incident to the cluster");
+            if (p.cl_els[e0 + i] >> 31) {
+                if (owner[vert(e, 0)] != c) bad("energy counted by a non-owner");
+                ++energy_count[e];
+            }
+        }
+        const int s0 = p.cl_slot_ptr[c], ns = p.cl_slot_ptr[c + 1] - s0;
+        int rows_slots = 0;
+        for (int k = p.cl_row_ptr[c]; k < p.cl_row_ptr[c + 1]; ++k)
+            rows_slots += p.row_ptr[p.cl_rows[k] + 1] - p.row_ptr[p.cl_rows[k]];
+        if (ns != rows_slots) bad("slot count differs from the rows' blocks");
+        std::vector<char> seen(static_cast<size_t>(rows_slots), 0);
+        std::vector<int> first(static_cast<size_t>(p.cl_row_ptr[c + 1] - p.cl_row_ptr[c]) + 1, 0);
+        for (int j = 0; j + 1 < static_cast<int>(first.size()); ++j) {
+            const int v = p.cl_rows[p.cl_row_ptr[c] + j];
+            first[j + 1] = first[j] + p.row_ptr[v + 1] - p.row_ptr[v];
+        }
+        for (int s = 0; s < ns; ++s) {
+            const uint32_t d = p.cl_slot[s0 + s], de = p.cl_slot_ent[s0 + s];
+            const int j = d & 0xffu, q = (d >> 8) & 0x3fffffu;
+            const bool diag = d >> 31, tr = (d >> 30) & 1u;
+            if ((s >= p.cl_noff[c]) != diag) bad("slot order");
+            if (j >= static_cast<int>(first.size()) - 1) bad("slot row outside the cluster");
+            const int v = p.cl_rows[p.cl_row_ptr[c] + j];
+            if (q >= p.row_ptr[v + 1] - p.row_ptr[v]) bad("slot position outside its row");
+            if (seen[first[j] + q]++) bad("slot listed twice");
+            const int w = p.col_idx[p.row_ptr[v] + q];
+            if (diag != (v == w) || tr != (v > w)) bad("slot flags");
+            const int lo = std::min(v, w), hi = std::max(v, w);
+            // Expected contributors: the elements holding both vertices, ascending.
+            std::vector<int> expect;
+            for (int k = ptr[v]; k < ptr[v + 1]; ++k) {
+                const int e = inc[k];
+                bool has = false;
+                for (int a = 0; a < 4; ++a) has = has || vert(e, a) == w;
+                if (has) expect.push_back(e);
+            }
+            if ((de >> 20) != expect.size()) bad("slot contributor count");
+            const size_t off = p.cl_ent_ptr[c] + (de & 0xfffffu);
+            for (size_t t = 0; t < expect.size(); ++t) {
+                const uint16_t en = p.cl_ents[off + t];
+                const int el = en >> 4, a = (en >> 2) & 3, b = en & 3;
+                if (el >= ne) bad("contributor outside the cluster");
+                const int e = static_cast<int>(p.cl_els[e0 + el] & 0x7fffffffu);
+                if (e != expect[t]) bad("contributor list differs from the elements sharing the block");
+                if (vert(e, a) != lo || vert(e, b) != hi) bad("contributor local indices");
+            }
+        }
+    }
+    for (int e = 0; e < T; ++e)
+        if (energy_count[e] != 1) bad("element energy not counted exactly once");
+    size_t contributors = 0;
+    for (uint32_t de : p.cl_slot_ent) contributors += de >> 20;
+    if (contributors != 16 * static_cast<size_t>(T)) bad("contributor total differs from 16 per element");
+    for (int c = 0; c < ncl; ++c)
+        if (p.cl_ent_ptr[c] % 8 != 0) bad("contributor lists not 16-byte aligned");
 }
 
 } // namespace lpg

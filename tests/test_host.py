@@ -125,6 +125,44 @@ def test_plan_valence_above_32_uses_64_pair_tiles():
     assert cap == 64 and pairs == 4 * k
 
 
+def cluster_summary(X, tets):
+    out = np.zeros(5, np.int64)
+    tets = np.ascontiguousarray(tets, dtype=np.int32)
+    N.check(N.lib.lpg_mesh_cluster_summary(X.shape[0], tets.shape[0], N.iptr(tets), out.ctypes.data_as(N._i64p)))
+    return out
+
+
+def _fan(k):
+    ang = np.linspace(0, 2 * np.pi, k, endpoint=False)
+    X = np.vstack([[0, 0, 0], [0, 0, 1], np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1)])
+    return X, np.array([[0, 2 + i, 2 + (i + 1) % k, 1] for i in range(k)], np.int32)
+
+
+@pytest.mark.parametrize("case", ["box2", "box10", "box24", "ragged", "fan40", "shuffled"])
+def test_cluster_plan_invariants(case):
+    """The element-once assembly's clusters: the library checks every invariant itself
+    (ownership, energy counted once, exact and ordered contributor lists per block)."""
+    rng = np.random.default_rng(4)
+    if case.startswith("box"):
+        X, tets = mesh.make_box(int(case[3:]))
+    elif case == "ragged":
+        X, t = mesh.make_box(6)
+        tets = t[rng.random(t.shape[0]) < 0.6]
+    elif case == "fan40":
+        X, tets = _fan(40)
+    else:  # vertex numbering with no locality
+        X, t = mesh.make_box(8)
+        perm = rng.permutation(X.shape[0])
+        tets = perm[t].astype(np.int32)
+    ncl, max_rows, max_els, evals, entries = cluster_summary(X, tets)
+    T = tets.shape[0]
+    assert entries == 16 * T
+    assert 1 <= max_rows <= 24 and max_els <= 224
+    assert T <= evals <= 4 * T  # each element once per cluster owning one of its vertices
+    if case == "box24":
+        assert evals <= 2.6 * T  # compact clusters on a structured box
+
+
 def _header_functions():
     names = set()
     for h in (ROOT / "include").glob("*.h"):
