@@ -262,6 +262,31 @@ int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, con
                       int num_fixed, int io_mem, int precision, double cg_tolerance, int per_element, double* dtheta,
                       double* lambda_out);
 
+/*
+ * Rest-position sensitivity of the elastic force (no reference counterpart: the reference
+ * differentiates its force response in theta and Fp only). out = (dg/dX)^T w, where g is
+ * the gradient of the elastic energy in u and X the vertex rest positions (num_dofs values,
+ * io_mem). Needs a handle created from vertex positions (Xe == NULL) without a plastic field
+ * (LPG_EINVAL otherwise). Per element d(w . g_e)/dX, summed per vertex in element order.
+ */
+int lpg_fem_force_vjp_rest(lpg_fem_t h, const double* u, const double* w, int io_mem, double* out);
+
+/*
+ * Adjoint rest-position sensitivity: the adjoint solve of lpg_adjoint_theta, then
+ * dX = -(dg/dX)^T lambda (num_dofs values, io_mem). Same requirements as
+ * lpg_fem_force_vjp_rest. lambda_out (num_dofs, io_mem) may be NULL.
+ */
+int lpg_adjoint_rest(lpg_fem_t h, const double* u_star, const double* dLdu, const int32_t* fixed_dofs, int num_fixed,
+                     int io_mem, int precision, double cg_tolerance, double* dX, double* lambda_out);
+
+/*
+ * Replaces the Lame parameters [lambda, mu] (num_tets * 2 when theta_per_element, else 2;
+ * host) of an existing handle, keeping its plan and rest geometry (no reference
+ * counterpart; the reference builds a new energy for new parameters). Values are checked at
+ * evaluation like the constructor's (lambda >= 0, mu > 0).
+ */
+int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,9 @@ SIGNATURES = [
     ("lpg_newton_solve", _int, [_vp, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC), _vp,
                                 ctypes.POINTER(NewtonResultC)]),
     ("lpg_adjoint_theta", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _int, _vp, _vp]),
+    ("lpg_fem_force_vjp_rest", _int, [_vp, _vp, _vp, _int, _vp]),
+    ("lpg_adjoint_rest", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _vp, _vp]),
+    ("lpg_fem_set_theta", _int, [_vp, _dp, _int]),
 ]
 
 EXPORTED = [name for name, _, _ in SIGNATURES]

@@ -227,6 +227,7 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         LPG_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
         h->stream = h->own_stream;
         build_plan(V, T, tets, h->plan);
+        h->from_vertices = Xe == nullptr;
         // Element records (VolumetricElement3D ctor, volumetric_element.hpp:23-39, and the
         // sampled B of deformation_gradient_sampling_response.hpp:24-41).
         std::vector<double> rec(12 * static_cast<size_t>(T));
@@ -537,6 +538,54 @@ int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         newton_solve(*h, fixed, nfixed, f_ext, x0, io_mem, *o, x_out, res);
+    });
+}
+
+int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        if (!theta && h->dm.T > 0) fail(LPG_EINVAL, "lpg_fem_set_theta: null theta");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = theta_per_element ? 2 * static_cast<size_t>(h->dm.T) : 2;
+        for (size_t k = 0; k < n && h->dm.T > 0; ++k)
+            if (!std::isfinite(theta[k])) fail(LPG_EINVAL, "VolumetricFemEnergy: theta must be finite");
+        if (h->dm.T == 0) return;
+        double* d = h->d_u2.as<double>(n);
+        LPG_CUDA(cudaMemcpyAsync(d, theta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        launch_set_theta(h->dm, d, theta_per_element, h->stream);
+        LPG_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int lpg_fem_force_vjp_rest(lpg_fem_t h, const double* u, const double* w, int io_mem, double* out) {
+    return guarded([&] {
+        if (!h || !out) fail(LPG_EINVAL, "lpg_fem_force_vjp_rest: null argument");
+        if (!h->from_vertices || h->dm.fpinv64)
+            fail(LPG_EINVAL, "rest-position sensitivity needs vertex rest positions and no plastic field");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        const double* d_u = h->stage_in(u, io_mem, h->d_u, n);
+        const double* d_w = h->stage_in(w, io_mem, h->d_u2, n);
+        double* d_out = io_mem == LPG_MEM_DEVICE ? out : h->d_grad.as<double>(std::max<size_t>(n, 1));
+        double* pe = h->d_vjp.as<double>(std::max<size_t>(12 * static_cast<size_t>(h->dm.T), 1));
+        launch_rest_vjp(h->dm, d_u, d_w, pe, 1.0, d_out, h->d_status.as<unsigned>(1), h->stream);
+        if (io_mem == LPG_MEM_HOST && n > 0)
+            LPG_CUDA(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        raise_status(h->take_status());
+    });
+}
+
+int lpg_adjoint_rest(lpg_fem_t h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed,
+                     int io_mem, int precision, double cg_tolerance, double* dX, double* lambda_out) {
+    return guarded([&] {
+        if (!h || !u_star || !dLdu || !dX) fail(LPG_EINVAL, "lpg_adjoint_rest: null argument");
+        if (!h->from_vertices || h->dm.fpinv64)
+            fail(LPG_EINVAL, "rest-position sensitivity needs vertex rest positions and no plastic field");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        adjoint_rest(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, dX, lambda_out);
     });
 }
 

@@ -1275,6 +1275,118 @@ template <typename R, bool WG, bool WH> void launch_cluster(const DevMesh& m, co
     LPG_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// Rest-position sensitivity of the elastic force. For one element with s = w . g_e =
+// vol P : grad w (grad w = sum_a w_a grad N_a^T, H = F - I, Q = dP/dF [grad w] =
+// mu grad w + lambda (F^-T : grad w) F^-T - p F^-T grad w^T F^-T):
+//   d s / d X_a = vol M grad N_a,   M = (P : grad w) I - H^T Q - grad w^T P,
+// from d(Dm^-1) = -Dm^-1 dDm Dm^-1 and d vol = vol tr(Dm^-1 dDm). Per element 12 values;
+// a per-vertex pass sums them over the incident elements in element order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) rest_vjp_kernel(const DevMesh m, const double* __restrict__ u,
+                                                       const double* __restrict__ w, double* __restrict__ out,
+                                                       unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int4 tv = __ldg(m.tets + e);
+    Kin<double> k;
+    unsigned st = kinematics<double>(m, e, tv, u, k);
+    const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
+    double Wg[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}; // row-major grad w
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double wi = __ldg(w + 3 * static_cast<size_t>(vs[a]) + i);
+            if (!isfinite(wi)) st |= ST_BAD_INPUT;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) Wg[3 * i + j] = fma(wi, k.n[a][j], Wg[3 * i + j]);
+        }
+    const double p = fma(k.lam, k.logJ, -k.mu);
+    double P[9], tr = 0, PW = 0;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+        P[t] = fma(k.mu, k.F[t], p * k.FiT[t]);
+        tr = fma(k.FiT[t], Wg[t], tr);
+        PW = fma(P[t], Wg[t], PW);
+    }
+    double FW[9]; // F^-T grad w^T
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int l = 0; l < 3; ++l)
+            FW[3 * i + l] = k.FiT[3 * i] * Wg[3 * l] + k.FiT[3 * i + 1] * Wg[3 * l + 1] + k.FiT[3 * i + 2] * Wg[3 * l + 2];
+    double Q[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double flip = FW[3 * i] * k.FiT[j] + FW[3 * i + 1] * k.FiT[3 + j] + FW[3 * i + 2] * k.FiT[6 + j];
+            Q[3 * i + j] = k.mu * Wg[3 * i + j] + k.lam * tr * k.FiT[3 * i + j] - p * flip;
+        }
+    double Mx[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double s = r == c ? PW : 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double Hir = k.F[3 * i + r] - (i == r ? 1.0 : 0.0);
+                s -= Hir * Q[3 * i + c] + Wg[3 * i + r] * P[3 * i + c];
+            }
+            Mx[3 * r + c] = s;
+        }
+    double* o = out + 12 * static_cast<size_t>(e);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const double v = k.vol * (Mx[3 * r] * k.n[a][0] + Mx[3 * r + 1] * k.n[a][1] + Mx[3 * r + 2] * k.n[a][2]);
+            if (!isfinite(v)) st |= ST_NONFINITE_OUT;
+            o[3 * a + r] = v;
+        }
+    if (st) atomicOr(status, st);
+}
+
+// out[v] = sign * sum over the elements of v (ascending) of the per-element vertex values
+// (12 per element); vertices of no element are left to zero_rows_kernel.
+__global__ void __launch_bounds__(128) vertex_gather_kernel(const DevMesh m, const double* __restrict__ per_elem,
+                                                            double sign, double* __restrict__ out) {
+    for (int cl = blockIdx.x; cl < m.ncl; cl += gridDim.x) {
+        const int s0 = __ldg(m.cl_slot_ptr + cl), ns = __ldg(m.cl_slot_ptr + cl + 1) - s0;
+        const int e0 = __ldg(m.cl_el_ptr + cl), r0 = __ldg(m.cl_row_ptr + cl);
+        const uint16_t* ents = m.cl_ents + __ldg(m.cl_ent_ptr + cl);
+        for (int s = __ldg(m.cl_noff + cl) + threadIdx.x; s < ns; s += blockDim.x) {
+            const uint32_t d = __ldg(m.cl_slot + s0 + s), de = __ldg(m.cl_slot_ent + s0 + s);
+            const int v = __ldg(m.cl_rows + r0 + (d & 0xffu));
+            const uint16_t* en = ents + (de & 0xfffffu);
+            double acc[3] = {0, 0, 0};
+            for (int c = 0; c < static_cast<int>(de >> 20); ++c) {
+                const int wd = __ldg(en + c);
+                const size_t e = __ldg(m.cl_els + e0 + (wd >> 4)) & 0x7fffffffu;
+                const int a = (wd >> 2) & 3;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) acc[i] += __ldg(per_elem + 12 * e + 3 * a + i);
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) out[3 * static_cast<size_t>(v) + i] = sign * acc[i];
+        }
+    }
+}
+
+// Lame parameters of every element record (FP64 and FP32 copies).
+__global__ void set_theta_kernel(double* rec64, float* rec32, const double* __restrict__ theta, int per_element, int T) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const double lam = per_element ? theta[2 * static_cast<size_t>(e)] : theta[0];
+    const double mu = per_element ? theta[2 * static_cast<size_t>(e) + 1] : theta[1];
+    rec64[12 * static_cast<size_t>(e) + 10] = lam;
+    rec64[12 * static_cast<size_t>(e) + 11] = mu;
+    rec32[12 * static_cast<size_t>(e) + 10] = static_cast<float>(lam);
+    rec32[12 * static_cast<size_t>(e) + 11] = static_cast<float>(mu);
+}
+
 template <typename R, bool WG, int WH, int CHUNKS> void launch_assemble(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = kWarpsPerBlock * smem_per_warp<R, WH>(32 * CHUNKS);
     static bool configured = false;
@@ -1334,6 +1446,21 @@ void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a
     // Per-unit energies -> partials (stored after the units) -> total.
     sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(a.tile_energy, units, a.tile_energy + units);
     sum_final_kernel<<<1, 256, 0, s>>>(a.tile_energy + units, kSumBlocks, a.energy);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_rest_vjp(const DevMesh& m, const double* u, const double* w, double* per_elem, double sign, double* out,
+                     unsigned* status, cudaStream_t s) {
+    if (m.T > 0) {
+        rest_vjp_kernel<<<(m.T + 127) / 128, 128, 0, s>>>(m, u, w, per_elem, status);
+        vertex_gather_kernel<<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, sign, out);
+    }
+    if (m.num_unused > 0) zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(out, m.unused_rows, m.num_unused);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cudaStream_t s) {
+    if (m.T > 0) set_theta_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m.rec64, m.rec32, theta, per_element, m.T);
     LPG_CUDA(cudaGetLastError());
 }
 

@@ -158,6 +158,10 @@ void launch_feasible(const DevMesh& m, const double* u, const double* du, double
 int feasible_blocks(const DevMesh& m);
 void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out_per_elem, unsigned* status,
                       cudaStream_t s);
+// Rest-position force VJP: out (3V) = sign * (d g / d X)^T w; per_elem: 12 T doubles of scratch.
+void launch_rest_vjp(const DevMesh& m, const double* u, const double* w, double* per_elem, double sign, double* out,
+                     unsigned* status, cudaStream_t s);
+void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cudaStream_t s);
 void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s);
 
 } // namespace lpg

@@ -936,14 +936,18 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
     }
 }
 
-void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
-                   int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out) {
+namespace {
+
+// The adjoint solve of StaticEquilibriumResponse (static_equilibrium_response.cpp:43-68): the
+// Exact FP64 Hessian K at u*, then mask K lambda = mask dL/du by PCG with FP64 refinement and
+// the reference's residual check. Returns lambda (device) and u* (device) through out-params.
+void adjoint_solve(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                   int precision, double cg_tolerance, const double** u_dev, double** lam_dev) {
     if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
     if (!(cg_tolerance > 0) || !std::isfinite(cg_tolerance)) fail(LPG_EINVAL, "adjoint: cg_tolerance must be positive");
     Solver S(h);
     const size_t n = S.n;
     const int V = S.V;
-    const size_t T = static_cast<size_t>(h.dm.T);
     cudaStream_t s = h.stream;
     double* mask = h.s_mask.as<double>(std::max<size_t>(n, 1));
     make_mask(h, fixed, nfixed, mask);
@@ -951,33 +955,52 @@ void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const i
     const double* w = h.stage_in(dLdu, io_mem, h.d_u2, n);
     double* lam = h.s_d.as<double>(std::max<size_t>(n, 1));
     LPG_CUDA(cudaMemsetAsync(lam, 0, n * sizeof(double), s));
+    *u_dev = u;
+    *lam_dev = lam;
     const auto ws = S.stats<double, double>(w, nullptr, mask);
     if (!std::isfinite(ws[1])) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: nonfinite sensitivity right-hand side");
-    if (n > 0 && ws[1] > 0) {
-        // Exact FP64 Hessian at u*: the residual matrix of the refinement (static_equilibrium_response.cpp:58).
-        double* K64 = h.s_hess64.as<double>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
-        h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutTiled, K64, nullptr);
-        raise_status(h.take_status());
-        double* rhs = h.s_g.as<double>(std::max<size_t>(n, 1));
-        LPG_CUDA(cudaMemcpyAsync(rhs, w, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        Solver::PcgOut po;
-        if (precision == LPG_PRECISION_F64) {
-            double* dinv = h.s_dinv.as<double>(12 * static_cast<size_t>(std::max(V, 1)));
-            block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K64, mask, dinv, V);
-            po = S.pcg<double>(K64, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 2);
-        } else {
-            float* K32 = h.s_hess.as<float>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
-            const size_t nv = 9 * static_cast<size_t>(h.dm.nnzb);
-            if (nv) convert_kernel<double, float><<<grid(nv), kThreads, 0, s>>>(K64, K32, nv);
-            float* dinv = h.s_dinv.as<float>(12 * static_cast<size_t>(std::max(V, 1)));
-            block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K32, mask, dinv, V);
-            po = S.pcg<float>(K32, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 30);
-        }
-        if (po.breakdown) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: singular or indefinite equilibrium stiffness");
-        // Residual check (static_equilibrium_response.cpp:61-68) in FP64 with the exact Hessian.
-        const double bn = std::sqrt(ws[1]);
-        if (!(po.rel * bn <= 1e-8 * (1.0 + bn))) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: inaccurate sensitivity solve");
+    if (n == 0 || !(ws[1] > 0)) return;
+    // Exact FP64 Hessian at u*: the residual matrix of the refinement (static_equilibrium_response.cpp:58).
+    double* K64 = h.s_hess64.as<double>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
+    h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutTiled, K64, nullptr);
+    raise_status(h.take_status());
+    double* rhs = h.s_g.as<double>(std::max<size_t>(n, 1));
+    LPG_CUDA(cudaMemcpyAsync(rhs, w, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    Solver::PcgOut po;
+    if (precision == LPG_PRECISION_F64) {
+        double* dinv = h.s_dinv.as<double>(12 * static_cast<size_t>(std::max(V, 1)));
+        block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K64, mask, dinv, V);
+        po = S.pcg<double>(K64, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 2);
+    } else {
+        float* K32 = h.s_hess.as<float>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
+        const size_t nv = 9 * static_cast<size_t>(h.dm.nnzb);
+        if (nv) convert_kernel<double, float><<<grid(nv), kThreads, 0, s>>>(K64, K32, nv);
+        float* dinv = h.s_dinv.as<float>(12 * static_cast<size_t>(std::max(V, 1)));
+        block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K32, mask, dinv, V);
+        po = S.pcg<float>(K32, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 30);
     }
+    if (po.breakdown) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: singular or indefinite equilibrium stiffness");
+    // Residual check (static_equilibrium_response.cpp:61-68) in FP64 with the exact Hessian.
+    const double bn = std::sqrt(ws[1]);
+    if (!(po.rel * bn <= 1e-8 * (1.0 + bn))) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: inaccurate sensitivity solve");
+}
+
+void copy_lambda(lpg_fem& h, const double* lam, int io_mem, double* lambda_out) {
+    if (!lambda_out) return;
+    const size_t n = 3 * static_cast<size_t>(h.dm.V);
+    LPG_CUDA(cudaMemcpyAsync(lambda_out, lam, n * sizeof(double),
+                             io_mem == LPG_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h.stream));
+}
+
+} // namespace
+
+void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                   int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out) {
+    const double* u = nullptr;
+    double* lam = nullptr;
+    adjoint_solve(h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, &u, &lam);
+    cudaStream_t s = h.stream;
+    const size_t T = static_cast<size_t>(h.dm.T);
     // dtheta = -(dg/dtheta)^T lambda.
     double* pe = h.d_vjp.as<double>(std::max<size_t>(2 * T, 2));
     launch_force_vjp(h.dm, u, lam, pe, h.d_status.as<unsigned>(1), s);
@@ -997,11 +1020,27 @@ void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const i
     for (double& v : host) v = -v;
     if (io_mem == LPG_MEM_DEVICE) {
         if (!host.empty()) LPG_CUDA(cudaMemcpyAsync(dtheta, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        if (lambda_out) LPG_CUDA(cudaMemcpyAsync(lambda_out, lam, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     } else {
         std::copy(host.begin(), host.end(), dtheta);
-        if (lambda_out) LPG_CUDA(cudaMemcpyAsync(lambda_out, lam, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     }
+    copy_lambda(h, lam, io_mem, lambda_out);
+    LPG_CUDA(cudaStreamSynchronize(s));
+}
+
+void adjoint_rest(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                  int precision, double cg_tolerance, double* dX, double* lambda_out) {
+    const double* u = nullptr;
+    double* lam = nullptr;
+    adjoint_solve(h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, &u, &lam);
+    cudaStream_t s = h.stream;
+    const size_t n = 3 * static_cast<size_t>(h.dm.V);
+    // dX = -(dg/dX)^T lambda.
+    double* out = io_mem == LPG_MEM_DEVICE ? dX : h.d_grad.as<double>(std::max<size_t>(n, 1));
+    double* pe = h.d_vjp.as<double>(std::max<size_t>(12 * static_cast<size_t>(h.dm.T), 1));
+    launch_rest_vjp(h.dm, u, lam, pe, -1.0, out, h.d_status.as<unsigned>(1), s);
+    raise_status(h.take_status());
+    if (io_mem == LPG_MEM_HOST && n > 0) LPG_CUDA(cudaMemcpyAsync(dX, out, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    copy_lambda(h, lam, io_mem, lambda_out);
     LPG_CUDA(cudaStreamSynchronize(s));
 }
 

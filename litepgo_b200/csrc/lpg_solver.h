@@ -26,6 +26,7 @@ void raise_status(unsigned st);
 
 struct lpg_fem {
     int device = 0;
+    bool from_vertices = true; // rest geometry given as vertex positions (no per-element corners)
     cudaStream_t own_stream = nullptr, stream = nullptr;
     lpg::HostPlan plan;
     lpg::DevMesh dm;
@@ -56,4 +57,6 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
                   const lpg_newton_options& o, double* x_out, lpg_newton_result* res);
 void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                    int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out);
+void adjoint_rest(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                  int precision, double cg_tolerance, double* dX, double* lambda_out);
 } // namespace lpg

@@ -71,6 +71,23 @@ class QuadraticEnergy(Energy):
     def is_linear(self):
         return self.A.nnz == 0 or not np.any(self.A.data)
 
+    def eval(self, x, gradient=False, hessian=None):
+        """(1/2 x^T A x + b^T x, A x + b, A) on the host (quadratic_energy.hpp:10-20)."""
+        if hasattr(x, "detach"):
+            x = x.detach().cpu().numpy()
+        x = np.asarray(x, dtype=np.float64).ravel()
+        if x.size != self.num_dofs or not np.all(np.isfinite(x)):
+            raise ValueError("Energy::eval: x must have num_dofs finite entries")
+        Ax = self.A @ x
+        value = 0.5 * float(x @ Ax) + float(self.b @ x)
+        return value, (Ax + self.b if gradient else None), (self.A.copy() if hessian else None)
+
+    def eval_value(self, x):
+        return self.eval(x)[0]
+
+    def eval_gradient(self, x):
+        return self.eval(x, gradient=True)[1]
+
 
 class WeightedSumEnergy(Energy):
     """E(x) = sum_i w_i E_i(x) over terms with the same DOFs (a list of (energy, weight))."""

@@ -33,6 +33,7 @@ __all__ = [
     "VolumetricFemForceMaterialResponse",
     "VolumetricFemEnergyTetP1",
     "VolumetricFemForceMaterialResponseTetP1",
+    "VolumetricFemForceRestPositionResponseTetP1",
 ]
 
 
@@ -267,9 +268,18 @@ class VolumetricFemEnergyTetP1(Energy):
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and N is not None and getattr(N, "lib", None) is not None:
             N.lib.lpg_fem_destroy(h)
             self._h = None
+
+    def set_theta(self, theta):
+        """Replaces [lambda, mu] ((2,) or (num_elements, 2)) in place, keeping the plan and the
+        rest geometry (no reference counterpart: the reference builds a new energy)."""
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        if th.shape not in ((2,), (self.num_elements, 2)):
+            raise ValueError("VolumetricFemEnergy: theta must have shape (2,) or (num_elements, 2)")
+        N.check(N.lib.lpg_fem_set_theta(self._h, N.dptr(th), 1 if th.ndim == 2 else 0))
+        self._theta = th
 
     @property
     def handle(self):
@@ -453,6 +463,50 @@ class VolumetricFemForceMaterialResponseTetP1:
         out = np.empty(2 * T if self.per_element else 2)
         N.check(N.lib.lpg_fem_force_vjp_theta(self._energy.handle, N.vptr(self.displacement), N.vptr(wv), N.MEM_HOST,
                                               1 if self.per_element else 0, N.vptr(out)))
+        return out
+
+
+class VolumetricFemForceRestPositionResponseTetP1:
+    """Force response X -> g(u; X) in the vertex rest positions at a fixed displacement.
+
+    No reference counterpart: the reference differentiates its force response in theta
+    (VolumetricFemForceMaterialResponse) and Fp only. ``eval_vjp(X, w)`` returns
+    (dg/dX)^T w (num_dofs values) with X the (V, 3) rest positions, flattened; used as the
+    ``make_response`` of a StaticEquilibriumResponse over rest positions. Needs vertex rest
+    positions and no plastic field.
+    """
+
+    def __init__(self, displacement_map, displacement, theta):
+        if not isinstance(displacement_map, VertexDofMap) or displacement_map.dofs_per_vertex != 3:
+            raise ValueError("VolumetricFemForceResponse: incompatible map, displacement or responses")
+        u = np.ascontiguousarray(displacement, dtype=np.float64)
+        if u.size != displacement_map.num_dofs or not np.all(np.isfinite(u)):
+            raise ValueError("VolumetricFemForceResponse: incompatible map, displacement or responses")
+        self.map = displacement_map
+        self.theta = np.ascontiguousarray(theta, dtype=np.float64)
+        self.displacement = u
+        self.num_inputs = self.num_outputs = displacement_map.num_dofs
+        self._energy = None
+        self._X = None
+
+    def _energy_at(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+        if X.shape[0] != self.map.num_vertices or not np.all(np.isfinite(X)):
+            raise ValueError("Response: p must hold num_vertices finite rest positions")
+        if self._energy is None or not np.array_equal(X, self._X):
+            self._energy = VolumetricFemEnergyTetP1(self.map, X, None, self.theta)
+            self._X = X.copy()
+        return self._energy
+
+    def eval_vjp(self, X, w):
+        """(dg/dX)^T w at the rest positions X (num_dofs values)."""
+        e = self._energy_at(X)
+        wv = np.ascontiguousarray(w, dtype=np.float64)
+        if wv.size != self.num_outputs:
+            raise ValueError("Response: weights must have num_outputs entries")
+        out = np.empty(self.num_inputs)
+        N.check(N.lib.lpg_fem_set_stream(e.handle, None))
+        N.check(N.lib.lpg_fem_force_vjp_rest(e.handle, N.vptr(self.displacement), N.vptr(wv), N.MEM_HOST, N.vptr(out)))
         return out
 
 

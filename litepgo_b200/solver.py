@@ -159,18 +159,22 @@ class StaticEquilibriumResponse:
         self.make_response = make_response
         self.precision = precision
         self.adjoint_tolerance = adjoint_tolerance
+        self._last = None  # (p, potential, x) of the last solve, reused for the same p
 
     def _solve(self, p):
         p = np.asarray(p, dtype=np.float64).ravel()
         if p.size != self.num_inputs or not np.all(np.isfinite(p)):
             raise ValueError("Response: p must have num_inputs finite entries")
+        if self._last is not None and np.array_equal(self._last[0], p):
+            return self._last
         potential = self.make_energy(p)
         if potential is None or potential.num_dofs != self.num_outputs:
             raise ValueError("StaticEquilibriumResponse: incompatible energy")
         result = newton_solve(potential, self.fixed, self.initial, self.options)
         if result.status != NewtonStatus.Converged:
             raise ValueError("StaticEquilibriumResponse: equilibrium did not converge")
-        return p, potential, result.x
+        self._last = (p.copy(), potential, np.array(result.x, copy=True))
+        return self._last
 
     def eval_value(self, p):
         return self._solve(p)[2]
@@ -186,10 +190,18 @@ class StaticEquilibriumResponse:
         if force is None or force.num_inputs != self.num_inputs or force.num_outputs != self.num_outputs:
             raise ValueError("StaticEquilibriumResponse: incompatible force response")
         fem, _ = _split_energy(potential)
-        T = fem.num_elements
-        out = np.empty(2 * T if force.per_element else 2)
         fixed_arr = np.ascontiguousarray(self.fixed.fixed_dofs, dtype=np.int32)
         prec = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
+        from .fem import VolumetricFemForceRestPositionResponseTetP1
+
+        if isinstance(force, VolumetricFemForceRestPositionResponseTetP1):
+            out = np.empty(self.num_inputs)
+            N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
+            N.check(N.lib.lpg_adjoint_rest(fem.handle, N.vptr(x), N.vptr(w), N.iptr(fixed_arr), int(fixed_arr.size),
+                                           N.MEM_HOST, prec, float(self.adjoint_tolerance), N.vptr(out), None))
+            return out
+        T = fem.num_elements
+        out = np.empty(2 * T if force.per_element else 2)
         N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
         N.check(N.lib.lpg_adjoint_theta(fem.handle, N.vptr(x), N.vptr(w), N.iptr(fixed_arr), int(fixed_arr.size),
                                         N.MEM_HOST, prec, float(self.adjoint_tolerance),

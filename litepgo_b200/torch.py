@@ -1,0 +1,107 @@
+"""PyTorch adapters of litepgo.torch for this package (src/python/torch.py:126-175).
+
+``energy(potential, x)`` and ``response(model, x)`` are first-order outer autograd adapters
+like the reference's: only the explicit tensor input is differentiable; an energy saves its
+gradient in the forward pass, a response is differentiated through its VJP (reverse mode)
+or JVP (forward mode, where the model has one) at a saved copy of the input. The reference
+takes one-dimensional CPU float64 tensors; CUDA float64 tensors are accepted here too, and an
+energy of a CUDA tensor is evaluated and differentiated on that device without host copies.
+The torch-material classes of the reference (TorchVolumetricMaterial, TorchShellMaterial) are
+not part of this path.
+"""
+
+import numpy as np
+import torch
+from torch.autograd.function import once_differentiable
+
+from .energy import QuadraticEnergy, WeightedSumEnergy
+from .fem import VolumetricFemEnergyTetP1
+
+__all__ = ["energy", "response"]
+
+
+def _check(x):
+    if not isinstance(x, torch.Tensor):
+        raise TypeError("expected a torch.Tensor")
+    if x.dtype != torch.float64 or x.ndim != 1 or x.device.type not in ("cpu", "cuda"):
+        raise ValueError("expected a one-dimensional float64 tensor on the CPU or a CUDA device")
+
+
+def _host(x):
+    return x.detach().cpu().numpy().copy()
+
+
+def _on_device(potential, x, need_gradient):
+    """(value, gradient tensor or None) of potential at a CUDA tensor x, on x's device."""
+    if isinstance(potential, VolumetricFemEnergyTetP1):
+        value, g, _ = potential.eval_device(x.detach(), gradient=need_gradient)
+        return value, g
+    if isinstance(potential, WeightedSumEnergy):
+        fem, f = potential.split()
+        value, g, _ = fem.eval_device(x.detach(), gradient=need_gradient)
+        ft = torch.as_tensor(f, device=x.device)
+        value -= float(torch.dot(ft, x.detach()))
+        return value, (g - ft if g is not None else None)
+    if isinstance(potential, QuadraticEnergy) and potential.is_linear:
+        b = torch.as_tensor(potential.b, device=x.device)
+        return float(torch.dot(b, x.detach())), (b.clone() if need_gradient else None)
+    value, g, _ = potential.eval(_host(x), gradient=need_gradient)
+    return value, (torch.as_tensor(np.asarray(g), device=x.device) if need_gradient else None)
+
+
+class _Energy(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, potential, need_gradient):
+        if x.is_cuda:
+            value, gradient = _on_device(potential, x, need_gradient)
+            if need_gradient:
+                ctx.save_for_backward(gradient)
+        else:
+            values = _host(x)
+            if need_gradient:
+                value, gradient, _ = potential.eval(values, gradient=True)
+                ctx.save_for_backward(torch.from_numpy(np.array(gradient, copy=True)))
+            else:
+                value = potential.eval_value(values)
+        return torch.tensor(value, dtype=torch.float64, device=x.device)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, upstream):
+        (gradient,) = ctx.saved_tensors
+        return upstream * gradient, None, None
+
+
+class _Response(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, model):
+        ctx.values = _host(x)
+        ctx.device = x.device
+        ctx.model = model
+        value = model.eval_value(ctx.values)
+        return torch.as_tensor(np.array(value, dtype=np.float64, copy=True), device=x.device)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, upstream):
+        gradient = ctx.model.eval_vjp(ctx.values, _host(upstream))
+        return torch.as_tensor(np.array(gradient, dtype=np.float64, copy=True), device=ctx.device), None
+
+    @staticmethod
+    def jvp(ctx, tangent, _model):
+        if not hasattr(ctx.model, "eval_jvp"):
+            raise NotImplementedError(f"{type(ctx.model).__name__} has no forward-mode product (eval_jvp)")
+        product = ctx.model.eval_jvp(ctx.values, _host(tangent))
+        return torch.as_tensor(np.array(product, dtype=np.float64, copy=True), device=ctx.device)
+
+
+def energy(potential, x):
+    """Evaluates an Energy at x (CPU or CUDA float64 1-D); differentiates with respect to x only."""
+    _check(x)
+    return _Energy.apply(x, potential, torch.is_grad_enabled() and x.requires_grad)
+
+
+def response(model, x):
+    """Evaluates a Response; reverse / forward AD use its VJP / JVP, differentiating x only."""
+    _check(x)
+    return _Response.apply(x, model)

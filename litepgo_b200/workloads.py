@@ -8,6 +8,9 @@ Every workload is generated from numpy.random.default_rng(seed); there is no dat
 - gravity_box: n^3 cubes, per-element mu log-uniform in [1e3, 1e5] and Poisson ratio
   nu ~ U[0.30, 0.45] (lambda = 2 mu nu / (1 - 2 nu)), bottom face z = 0 fixed,
   gravity (0, 0, -9.8) with density 1000 lumped as f_a = rho g vol_e / 4 (exact for P1).
+- adjoint_box: n^3 cubes with per-element [lambda, mu] = [1.4e5, 3.4e4] (the parameters of
+  an adjoint fit), bottom face fixed, gravity as above, and target parameters whose mu is
+  perturbed to mu (1 + 0.2 N(0, 1)) (clipped below at 0.05 mu).
 - compressed_box: 0.6x axial compression along z plus per-vertex noise 0.05 h N(0, 1)
   (h = 1/n), resampled until every element has det F in [0.2, 3.0].
 """
@@ -16,7 +19,7 @@ import numpy as np
 
 from .mesh import make_box
 
-__all__ = ["deformed_box", "gravity_box", "compressed_box", "lame", "gravity_load", "det_F"]
+__all__ = ["deformed_box", "gravity_box", "adjoint_box", "compressed_box", "lame", "gravity_load", "det_F"]
 
 
 def lame(mu, nu):
@@ -73,6 +76,19 @@ def gravity_box(n=64, seed=0, rho=1000.0):
     fixed = (3 * bottom[:, None] + np.arange(3)).ravel().astype(np.int32)
     f = gravity_load(X, tets, rho)
     return dict(X=X, tets=tets, theta=theta, fixed=fixed, f=f, u0=np.zeros(X.size), seed=seed, n=n)
+
+
+def adjoint_box(n=32, seed=0, mu=3.4e4, lam=1.4e5, rho=1000.0):
+    X, tets = make_box(n)
+    rng = np.random.default_rng(seed)
+    T = tets.shape[0]
+    theta = np.tile(np.array([lam, mu]), (T, 1))
+    target = theta.copy()
+    target[:, 1] = mu * np.maximum(1.0 + 0.2 * rng.standard_normal(T), 0.05)
+    bottom = np.flatnonzero(X[:, 2] == 0.0)
+    fixed = (3 * bottom[:, None] + np.arange(3)).ravel().astype(np.int32)
+    return dict(X=X, tets=tets, theta=theta, target_theta=target, fixed=fixed, f=gravity_load(X, tets, rho),
+                u0=np.zeros(X.size), seed=seed, n=n)
 
 
 def compressed_box(n=128, seed=0, mu=3.4e4, lam=1.4e5):

@@ -753,6 +753,62 @@ void force_vjp_theta(orc_mesh& m, const double* u, const double* wvec, double* o
     });
 }
 
+// Rest-position sensitivity of the force (no reference counterpart; pinned by central finite
+// differences of the force in the rest positions). Per element s = w_e . g_e = vol P : grad w;
+// with H = F - I and Q = A : grad w (A the material tangent of nh_A),
+//   d s / d X_a = vol M grad N_a,  M = (P : grad w) I - H^T Q - grad w^T P.
+// Per-vertex sums run over the elements in ascending order.
+void force_vjp_rest(orc_mesh& m, const double* u, const double* wvec, double* out) {
+    if (m.has_Fp) fail(ORC_EINVAL, "rest-position sensitivity needs vertex rest positions and no plastic field");
+    std::vector<double> pe(12 * static_cast<size_t>(m.T));
+    for_elements(m.T, [&](int e) {
+        double c[12], we[12];
+        gather_local(m, e, u, c);
+        gather_local(m, e, wvec, we);
+        const M3 F = element_F(m, e, c);
+        const M3 I = eye3();
+        const M3 P = nh_P(F, I, elem_theta(m, e));
+        double A[81];
+        nh_A(F, I, elem_theta(m, e), A);
+        const double* B = m.B.data() + static_cast<size_t>(e) * 108;
+        double gN[4][3];
+        for (int a = 0; a < 4; ++a)
+            for (int j = 0; j < 3; ++j) gN[a][j] = B[(3 * j) + 9 * (3 * a)];
+        M3 Wg{};
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                double t = 0;
+                for (int a = 0; a < 4; ++a) t += we[3 * a + i] * gN[a][j];
+                Wg[i + 3 * j] = t;
+            }
+        M3 Q{};
+        double PW = 0;
+        for (int r = 0; r < 9; ++r) {
+            double t = 0;
+            for (int col = 0; col < 9; ++col) t += A[r + 9 * col] * Wg[col];
+            Q[r] = t;
+            PW += P[r] * Wg[r];
+        }
+        M3 Mx{};
+        for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) {
+                double t = k == l ? PW : 0.0;
+                for (int i = 0; i < 3; ++i) t -= (at(F, i, k) - I[i + 3 * k]) * at(Q, i, l) + at(Wg, i, k) * at(P, i, l);
+                Mx[k + 3 * l] = t;
+            }
+        for (int a = 0; a < 4; ++a)
+            for (int k = 0; k < 3; ++k) {
+                double t = 0;
+                for (int l = 0; l < 3; ++l) t += at(Mx, k, l) * gN[a][l];
+                pe[12 * static_cast<size_t>(e) + 3 * a + k] = m.w[e] * t;
+            }
+    });
+    std::fill(out, out + m.n, 0.0);
+    for (int e = 0; e < m.T; ++e)
+        for (int a = 0; a < 4; ++a)
+            for (int k = 0; k < 3; ++k) out[3 * m.tets[4 * e + a] + k] += pe[12 * static_cast<size_t>(e) + 3 * a + k];
+}
+
 // ---------------------------------------------------------------------------
 // Free-DOF reduction (dof_reduction.cpp, reduced_matrix.cpp) and linear solvers.
 // ---------------------------------------------------------------------------
@@ -1110,6 +1166,10 @@ int orc_mesh_feasible_step(orc_mesh* m, const double* u, const double* du, doubl
 
 int orc_mesh_force_vjp_theta(orc_mesh* m, const double* u, const double* w, double* out) {
     return guarded([&] { force_vjp_theta(*m, u, w, out); });
+}
+
+int orc_mesh_force_vjp_rest(orc_mesh* m, const double* u, const double* w, double* out) {
+    return guarded([&] { force_vjp_rest(*m, u, w, out); });
 }
 
 // newton_solve (newton.cpp:112-183) with the load term E = elastic - f . u, plus the

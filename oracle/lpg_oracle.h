@@ -80,6 +80,9 @@ int orc_mesh_feasible_step(orc_mesh* m, const double* u, const double* du, doubl
  * per-element [d/dlambda, d/dmu] of w . g (T*2). The reference returns the positive
  * displacement gradient (force response) products; the equilibrium VJP negates it. */
 int orc_mesh_force_vjp_theta(orc_mesh* m, const double* u, const double* w, double* out);
+/* (d g / d X)^T w for the vertex rest positions X (3V), no plastic field; restated from the
+ * shape derivative of the element force (the reference has no such derivative). */
+int orc_mesh_force_vjp_rest(orc_mesh* m, const double* u, const double* w, double* out);
 
 /* ---- Newton (newton.cpp) over E(u) = elastic(u) - f_ext . u ---- */
 typedef struct {

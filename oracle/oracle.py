@@ -82,6 +82,7 @@ def lib():
                                     _c_double_p, _c_double_p, _c_double_p]
         L.orc_mesh_feasible_step.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_mesh_force_vjp_theta.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
+        L.orc_mesh_force_vjp_rest.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_newton_solve.argtypes = [ctypes.c_void_p, _c_int_p, ctypes.c_int, _c_double_p, _c_double_p,
                                        ctypes.POINTER(NewtonOptions), _c_double_p, ctypes.POINTER(NewtonResult)]
         L.orc_adjoint_theta.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_int_p, ctypes.c_int, ctypes.c_int,
@@ -243,6 +244,13 @@ class OracleMesh:
         out = np.empty((self.num_tets, 2))
         _check(lib().orc_mesh_force_vjp_theta(self._h, _dp(np.ascontiguousarray(u, float)),
                                               _dp(np.ascontiguousarray(w, float)), _dp(out)))
+        return out
+
+    def force_vjp_rest(self, u, w):
+        """(d g / d X)^T w over the vertex rest positions (3V)."""
+        out = np.empty(self.num_dofs)
+        _check(lib().orc_mesh_force_vjp_rest(self._h, _dp(np.ascontiguousarray(u, float)),
+                                             _dp(np.ascontiguousarray(w, float)), _dp(out)))
         return out
 
     def newton(self, fixed, x0, f_ext=None, tol=1e-9, max_iterations=50, hessian=2, max_line_search_steps=30,

@@ -173,3 +173,47 @@ def test_equilibrium_adjoint_matches_resolve_fd():
             col = (solve(p + e)[1] - solve(p - e)[1]) / (2 * h)
             assert abs(w @ col - jtw[c]) < 2e-7 * (1 + abs(jtw[c]))
     assert np.all(u[:9] == initial[:9])
+
+
+def _rest_fd(X, cells, theta, u, w, h=1e-6):
+    """Central finite differences of w . g(u; X) in every rest coordinate."""
+    out = np.empty(X.size)
+    for k in range(X.size):
+        Xp, Xm = X.copy().ravel(), X.copy().ravel()
+        Xp[k] += h
+        Xm[k] -= h
+        gp = oracle.OracleMesh(Xp.reshape(-1, 3), cells, theta).eval(u, True, 0)[1]
+        gm = oracle.OracleMesh(Xm.reshape(-1, 3), cells, theta).eval(u, True, 0)[1]
+        out[k] = (w @ gp - w @ gm) / (2 * h)
+    return out
+
+
+@pytest.mark.parametrize("state", [1, 2])
+def test_rest_position_vjp_matches_finite_differences(state):
+    """The rest-position force VJP has no reference counterpart: its oracle restatement is
+    pinned against central differences of the oracle's own force."""
+    u = two_tet_states()[state]
+    w = np.sin(np.arange(u.size) + 0.7)
+    m = two_tet_mesh()
+    got = m.force_vjp_rest(u, w)
+    fd = _rest_fd(TWO_TET_X, TWO_TET_CELLS, TWO_TET_THETA, u, w)
+    assert np.max(np.abs(got - fd)) <= 1e-6 * max(1.0, np.max(np.abs(fd)))
+
+
+def test_rest_position_vjp_box_per_element_theta():
+    w_ = workloads.deformed_box(2, seed=4)
+    X, cells, theta, u = w_["X"], w_["tets"], w_["theta"], w_["u"]
+    rng = np.random.default_rng(3)
+    th = np.column_stack([theta[0] * (1 + 0.3 * rng.random(cells.shape[0])), theta[1] * (1 + 0.3 * rng.random(cells.shape[0]))])
+    w = rng.standard_normal(u.size)
+    got = oracle.OracleMesh(X, cells, th).force_vjp_rest(u, w)
+    fd = np.empty(X.size)
+    h = 1e-6
+    for k in range(X.size):
+        Xp, Xm = X.copy().ravel(), X.copy().ravel()
+        Xp[k] += h
+        Xm[k] -= h
+        gp = oracle.OracleMesh(Xp.reshape(-1, 3), cells, th).eval(u, True, 0)[1]
+        gm = oracle.OracleMesh(Xm.reshape(-1, 3), cells, th).eval(u, True, 0)[1]
+        fd[k] = (w @ gp - w @ gm) / (2 * h)
+    assert np.max(np.abs(got - fd)) <= 1e-6 * np.max(np.abs(fd))
