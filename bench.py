@@ -120,7 +120,7 @@ class ClockSampler:
 
 def profile_traffic():
     """Per-launch DRAM bytes of the assembly kernel from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "assemble_f64_exact_64cube.md"
+    p = ROOT / "profiles" / "cluster_kernel_f64_exact_64cube.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
