@@ -164,13 +164,23 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
  * mean duration of the assembly kernel alone (ms_assemble) and of one whole evaluation
  * including projection and the energy reduction (ms_eval). With flush_l2 != 0 a 512 MB
  * buffer is written before each launch, outside the measured intervals. Besides
- * LPG_LAYOUT_BSR and LPG_LAYOUT_CSC, layout 2 selects the solvers' internal block layout:
- * rows are cut into SpMV tiles of consecutive rows (at most 32 blocks and 32 rows per tile, a
- * row without blocks counting as one, a longer row alone), and entry t (row-major) of block
- * k of the tile holding blocks [k0, k0 + n) is at 9 k0 + t n + (k - k0).
+ * LPG_LAYOUT_BSR and LPG_LAYOUT_CSC, layout 2 selects the solvers' sliced-ELL layout of
+ * lpg_fem_solver_layout (hess then holds 9 * num_slots values; padding entries are not
+ * written).
  */
 int lpg_fem_time_eval(lpg_fem_t h, const double* u, double* grad, int hessian, int precision, int layout, void* hess,
                       int launches, int flush_l2, double* ms_assemble, double* ms_eval);
+
+/*
+ * The block layout the Newton and adjoint solvers keep the Hessian in (no reference
+ * counterpart): sliced ELL with chunks of 32 rows, rows sorted by block count (descending,
+ * stable) within windows of 128 rows. Chunk c holds rows sell_row[32 c + l] (l = 0..31, -1
+ * past the last row) and slots [sell_ptr[c], sell_ptr[c + 1]), 32 per block column of its
+ * longest row; block q of the row in lane l is slot sell_ptr[c] + 32 q + l, and entry t
+ * (row-major) of that block is value 9 sell_ptr[c] + 32 (9 q + t) + l. Any output may be NULL;
+ * sell_ptr has num_chunks + 1 entries, sell_row 32 * num_chunks.
+ */
+int lpg_fem_solver_layout(lpg_fem_t h, int64_t* num_slots, int* num_chunks, int32_t* sell_ptr, int32_t* sell_row);
 
 /* Per-element energies vol * W (num_tets doubles, io_mem). */
 int lpg_fem_element_energies(lpg_fem_t h, const double* u, int io_mem, double* elem_energy);

@@ -74,6 +74,7 @@ SIGNATURES = [
     ("lpg_fem_pattern_csc", _int, [_vp, _ip, _ip]),
     ("lpg_fem_eval", _int, [_vp, _vp, _int, _dp, _vp, _int, _int, _int, _vp, _int]),
     ("lpg_fem_time_eval", _int, [_vp, _vp, _vp, _int, _int, _int, _vp, _int, _int, _dp, _dp]),
+    ("lpg_fem_solver_layout", _int, [_vp, _i64p, ctypes.POINTER(_int), _ip, _ip]),
     ("lpg_fem_element_energies", _int, [_vp, _vp, _int, _vp]),
     ("lpg_fem_feasible_step", _int, [_vp, _vp, _vp, _int, _dp]),
     ("lpg_fem_feasible_step_noalloc", _int, [_vp, _vp, _vp, _dp]),

@@ -129,7 +129,7 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
         fail(LPG_EINVAL, "Energy: invalid Hessian kind");
     if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
-    if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC && layout != kLayoutTiled)
+    if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC && layout != kLayoutSell)
         fail(LPG_EINVAL, "invalid Hessian layout");
     EvalArgs a;
     a.u = du;
@@ -299,9 +299,11 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         m.num_unused = static_cast<int>(p.unused_rows.size());
         m.contrib = upload(h->b_contrib, p.contrib);
         m.pair_elem = upload(h->b_pair_elem, p.pair_elem);
-        m.spmv_tile_row = upload(h->b_spmv_tiles, p.spmv_tile_row);
-        m.n_spmv_tiles = static_cast<int>(p.spmv_tile_row.size()) - 1;
-        m.spmv_row_tile = upload(h->b_spmv_row_tile, p.spmv_row_tile);
+        m.sell_ptr = upload(h->b_sell[0], p.sell_ptr);
+        m.sell_row = upload(h->b_sell[1], p.sell_row);
+        m.sell_col = upload(h->b_sell[2], p.sell_col);
+        m.sell_base = upload(h->b_sell[3], p.sell_base);
+        m.n_sell = static_cast<int>(p.sell_ptr.size()) - 1;
         m.ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
         m.cl_row_ptr = upload(h->b_cl[0], p.cl_row_ptr);
         m.cl_rows = upload(h->b_cl[1], p.cl_rows);
@@ -366,6 +368,17 @@ int lpg_fem_pattern_bsr(lpg_fem_t h, int32_t* row_ptr, int32_t* col_idx) {
         if (!h) fail(LPG_EINVAL, "null handle");
         if (row_ptr) std::copy(h->plan.row_ptr.begin(), h->plan.row_ptr.end(), row_ptr);
         if (col_idx) std::copy(h->plan.col_idx.begin(), h->plan.col_idx.end(), col_idx);
+    });
+}
+
+int lpg_fem_solver_layout(lpg_fem_t h, int64_t* num_slots, int* num_chunks, int32_t* sell_ptr, int32_t* sell_row) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        const HostPlan& p = h->plan;
+        if (num_slots) *num_slots = p.sell_ptr.back();
+        if (num_chunks) *num_chunks = static_cast<int>(p.sell_ptr.size()) - 1;
+        if (sell_ptr) std::copy(p.sell_ptr.begin(), p.sell_ptr.end(), sell_ptr);
+        if (sell_row) std::copy(p.sell_row.begin(), p.sell_row.end(), sell_row);
     });
 }
 

@@ -227,8 +227,7 @@ struct TileMeta {
     int nb[32];
     int dq[32];   // position of the diagonal block within the row
     int ppre[33]; // the pairs of row j are [ppre[j], ppre[j + 1])
-    int tk0[32];  // first block and block count of the row's SpMV tile (tiled layout)
-    int tn[32];
+    int sb[32];   // the row's sliced-ELL base (solver layout)
 };
 
 // Position of entry t (row-major) of block q of tile row j in the output layout.
@@ -239,8 +238,7 @@ __device__ __forceinline__ size_t out_pos(int layout, const TileMeta* meta, int 
         const int i = t / 3, c = t - 3 * (t / 3);
         return 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * q + c;
     }
-    const int64_t k0 = meta->tk0[j];
-    return static_cast<size_t>(9 * k0 + static_cast<int64_t>(t) * meta->tn[j] + (k - k0));
+    return static_cast<size_t>(meta->sb[j]) + 32 * static_cast<size_t>(9 * q + t);
 }
 
 // Shared memory of one warp: off-diagonal blocks [9][3 cap + 1], slot descriptors [3 cap], metadata.
@@ -431,12 +429,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
             meta->slot0[lane] = sb;
             meta->nb[lane] = m.row_ptr[r + 1] - sb;
             meta->dq[lane] = m.diag_slot[r] - sb;
-            if (a.layout == kLayoutTiled) {
-                const int st = m.spmv_row_tile[r];
-                const int k0 = m.row_ptr[m.spmv_tile_row[st]];
-                meta->tk0[lane] = k0;
-                meta->tn[lane] = m.row_ptr[m.spmv_tile_row[st + 1]] - k0;
-            }
+            if (a.layout == kLayoutSell) meta->sb[lane] = m.sell_base[r];
             deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
         }
         int incl = deg;
@@ -504,29 +497,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
             }
         }
         __syncwarp();
-        // Off-diagonal slots; a slot's blocks are contiguous in the slot-sorted list. In the
-        // tiled layout, lanes take consecutive slots of one entry (consecutive addresses);
-        // otherwise 27 lanes take 3 slots x 9 entries per pass.
-        if (WH && a.layout == kLayoutTiled && ns > 0) {
-            HT* hout = reinterpret_cast<HT*>(a.hess);
-            const int total = 3 * np;
-            int kk = lane / ns, s = lane - ns * (lane / ns);
-            for (; kk < 9;) {
-                const uint32_t d = sdesc[s];
-                const int c0 = d & 0xffu;
-                const int c1 = s + 1 < ns ? (sdesc[s + 1] & 0xffu) : total;
-                const R* col = sH + kk * P;
-                R val = 0;
-                for (int c = c0; c < c1; ++c) val = X::add(val, col[c]);
-                if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                hout[out_pos(kLayoutTiled, meta, (d >> 8) & 31u, d >> 13, kk)] = static_cast<HT>(val);
-                s += 32;
-                while (s >= ns) {
-                    s -= ns;
-                    ++kk;
-                }
-            }
-        } else if (WH && lane < 27) {
+        // Off-diagonal slots: 27 lanes = 3 slots x 9 entries per pass; a slot's blocks are contiguous.
+        if (WH && lane < 27) {
             HT* hout = reinterpret_cast<HT*>(a.hess);
             const int sub = lane / 9, kk = lane - 9 * (lane / 9);
             const int total = 3 * np;
@@ -1026,13 +998,13 @@ template <typename R, bool WG, bool WH> size_t cl_smem_bytes(const DevMesh& m) {
     return cl_smem_fixed<R, WG, WH>() + slots + 2 * static_cast<size_t>(m.cl_max_ents);
 }
 
-__device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int tk0, int tn, int q, int t) {
+__device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, int q, int t) {
     if (layout == LPG_LAYOUT_BSR) return 9 * static_cast<size_t>(slot0 + q) + t;
     if (layout == LPG_LAYOUT_CSC) {
         const int i = t / 3, c = t - 3 * (t / 3);
         return 9 * static_cast<size_t>(slot0) + static_cast<size_t>(i) * 3 * nb + 3 * q + c;
     }
-    return 9 * static_cast<size_t>(tk0) + static_cast<size_t>(t) * tn + (slot0 + q - tk0);
+    return static_cast<size_t>(sb) + 32 * static_cast<size_t>(9 * q + t);
 }
 
 template <typename R, bool WG, bool WH>
@@ -1129,7 +1101,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, off);
         if ((tid & 31) == 0) red[tid >> 5] = eacc;
-        // Row table: vertex, first block, block count, and the SpMV tile of the row (tiled layout).
+        // Row table: vertex, first block, block count, and the row's sliced-ELL base (solver layout).
         const int r0 = __ldg(m.cl_row_ptr + cl), nr = __ldg(m.cl_row_ptr + cl + 1) - r0;
         for (int j = tid; j < nr; j += bd) {
             const int v = __ldg(m.cl_rows + r0 + j);
@@ -1137,12 +1109,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
             rt[j] = v;
             rt[kClusterRows + j] = sb;
             rt[2 * kClusterRows + j] = __ldg(m.row_ptr + v + 1) - sb;
-            if (a.layout == kLayoutTiled) {
-                const int t = __ldg(m.spmv_row_tile + v);
-                const int k0 = __ldg(m.row_ptr + __ldg(m.spmv_tile_row + t));
-                rt[3 * kClusterRows + j] = k0;
-                rt[4 * kClusterRows + j] = __ldg(m.row_ptr + __ldg(m.spmv_tile_row + t + 1)) - k0;
-            }
+            if (a.layout == kLayoutSell) rt[3 * kClusterRows + j] = __ldg(m.sell_base + v);
         }
         prefetch(cl + gridDim.x);
         if (WG || WH) __pipeline_wait_prior(0);
@@ -1164,7 +1131,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
                 const uint16_t* en = sent + (de & 0xfffffu);
                 const int cnt = static_cast<int>(de >> 20);
                 const int slot0 = rt[kClusterRows + j], nb = rt[2 * kClusterRows + j];
-                const int tk0 = rt[3 * kClusterRows + j], tn = rt[4 * kClusterRows + j];
+                const int sb = rt[3 * kClusterRows + j];
                 if (d >> 31) {
                     // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient.
                     R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
@@ -1203,7 +1170,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
                         for (int t = 0; t < 9; ++t) {
                             const R val = acc[sym3[t]];
                             if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                            hout[cl_pos(a.layout, slot0, nb, tk0, tn, q, t)] = static_cast<HT>(val);
+                            hout[cl_pos(a.layout, slot0, nb, sb, q, t)] = static_cast<HT>(val);
                         }
                     }
                 } else if (WH) {
@@ -1240,7 +1207,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
                         const int i = t / 3, kk = t - 3 * (t / 3);
                         const R val = tr ? acc[3 * kk + i] : acc[t];
                         if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                        hout[cl_pos(a.layout, slot0, nb, tk0, tn, q, t)] = static_cast<HT>(val);
+                        hout[cl_pos(a.layout, slot0, nb, sb, q, t)] = static_cast<HT>(val);
                     }
                 }
             }

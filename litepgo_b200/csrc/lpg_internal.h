@@ -17,7 +17,7 @@ enum : unsigned {
     ST_BAD_THETA = 1u << 1,    // lambda < 0, mu <= 0, NaN     -> LPG_EINVAL
     ST_NONFINITE_F = 1u << 2,  // non-finite F or increment    -> LPG_EDOMAIN
     ST_BAD_DET = 1u << 3,      // det F <= 0                   -> LPG_EDOMAIN
-    ST_NONFINITE_OUT = 1u << 4 // non-finite E, g or H         -> LPG_EDOMAIN
+    ST_NONFINITE_OUT = 1u << 4  // non-finite E, g or H         -> LPG_EDOMAIN
 };
 
 struct Error {
@@ -55,8 +55,13 @@ struct HostPlan {
     std::vector<int32_t> diag_slot;          // V: block index of (v, v), -1 for an unused vertex
     std::vector<int32_t> unused_rows;        // vertices referenced by no element (not in any tile)
     std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
-    std::vector<int32_t> spmv_tile_row;      // SpMV tiles: first row of each, plus V
-    std::vector<int32_t> spmv_row_tile;      // V: SpMV tile of each row
+    // Sliced-ELL copy of the pattern for the solvers (SELL-32 with rows sorted by block count
+    // within windows of kSellWindow rows): chunk c holds 32 rows (sell_row, -1 past the end)
+    // and sell_ptr[c + 1] - sell_ptr[c] = 32 x (its longest row) block slots; block slot q of
+    // the row in lane l is slot sell_ptr[c] + 32 q + l, its column sell_col (the row itself
+    // for a padding slot), and entry t of its 3x3 block is value 9 sell_ptr[c] + (9 q + t) 32 + l,
+    // i.e. sell_base[row] + 32 (9 q + t).
+    std::vector<int32_t> sell_ptr, sell_row, sell_col, sell_base;
     // Vertex clusters of the element-once assembly (one thread block per cluster): the rows a
     // cluster owns, the elements incident to them (ascending; bit 31 set on the elements whose
     // energy the cluster counts, those whose first vertex it owns), and its block slots,
@@ -78,6 +83,8 @@ struct HostPlan {
 
 // Size limits of an assembly cluster: owned rows, and distinct incident elements (the
 // element data of a cluster is held in shared memory).
+constexpr int kSellWindow = 128;
+
 #ifndef LPG_CLUSTER_ROWS
 #define LPG_CLUSTER_ROWS 24
 #endif
@@ -104,9 +111,8 @@ struct DevMesh {
     int32_t* unused_rows = nullptr;
     int num_unused = 0;
     int32_t* pair_elem = nullptr;
-    int32_t* spmv_tile_row = nullptr;
-    int32_t* spmv_row_tile = nullptr;
-    int n_spmv_tiles = 0;
+    int32_t *sell_ptr = nullptr, *sell_row = nullptr, *sell_col = nullptr, *sell_base = nullptr;
+    int n_sell = 0; // SELL chunks
     int ncl = 0, cl_max_slots = 0, cl_max_ents = 0;
     int32_t *cl_row_ptr = nullptr, *cl_rows = nullptr, *cl_el_ptr = nullptr, *cl_slot_ptr = nullptr, *cl_noff = nullptr,
             *cl_ent_ptr = nullptr;
@@ -122,18 +128,8 @@ struct DevMesh {
     float* fpinv32 = nullptr;
 };
 
-// Internal Hessian layout of the solvers: within each SpMV tile (blocks [k0, k0 + n)), entry
-// t of block k is at 9 k0 + t n + (k - k0), so lanes reading consecutive blocks coalesce.
-constexpr int kLayoutTiled = 2;
-
-// Position of entry t (row-major in the 3x3 block) of block k in the tiled layout.
-__host__ __device__ inline size_t tiled_pos(const int32_t* row_ptr, const int32_t* tile_row, const int32_t* row_tile,
-                                            int row, int64_t k, int t) {
-    const int tile = row_tile[row];
-    const int64_t k0 = row_ptr[tile_row[tile]];
-    const int64_t n = row_ptr[tile_row[tile + 1]] - k0;
-    return static_cast<size_t>(9 * k0 + t * n + (k - k0));
-}
+// Internal Hessian layout of the solvers: the sliced-ELL order of HostPlan::sell_*.
+constexpr int kLayoutSell = 2;
 
 // ---- kernel launchers (lpg_assemble.cu) ----
 struct EvalArgs {

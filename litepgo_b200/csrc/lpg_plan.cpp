@@ -203,28 +203,47 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
         }
         p.col_idx.swap(cols);
     }
-    // SpMV tiles: runs of consecutive rows holding at most 32 blocks (a row without blocks counts
-    // as one), one warp lane per block; a row with more than 32 blocks is a tile of its own.
-    p.spmv_tile_row.assign(1, 0);
+    // Sliced ELL (SELL-32): rows sorted by block count (descending, then by index) within
+    // windows of kSellWindow rows, cut into chunks of 32; each chunk is as wide as its longest
+    // row and padding slots point at the row itself (their values stay zero).
     {
-        int lanes = 0, rows = 0;
-        for (int v = 0; v < V; ++v) {
-            const int need = std::max(1, p.row_ptr[v + 1] - p.row_ptr[v]);
-            if (rows > 0 && (lanes + need > 32 || rows == 32)) {
-                p.spmv_tile_row.push_back(v);
-                lanes = rows = 0;
+        const int nch = (V + 31) / 32;
+        std::vector<int32_t> order(static_cast<size_t>(V));
+        for (int v = 0; v < V; ++v) order[v] = v;
+        for (int w0 = 0; w0 < V; w0 += kSellWindow) {
+            const int w1 = std::min(V, w0 + kSellWindow);
+            std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int a, int b) {
+                return p.row_ptr[a + 1] - p.row_ptr[a] > p.row_ptr[b + 1] - p.row_ptr[b];
+            });
+        }
+        p.sell_ptr.assign(static_cast<size_t>(nch) + 1, 0);
+        p.sell_row.assign(32 * static_cast<size_t>(nch), -1);
+        p.sell_base.assign(static_cast<size_t>(V), 0);
+        int64_t slots = 0;
+        for (int c = 0; c < nch; ++c) {
+            int width = 0;
+            for (int l = 0; l < 32 && 32 * c + l < V; ++l) {
+                const int r = order[32 * c + l];
+                p.sell_row[32 * static_cast<size_t>(c) + l] = r;
+                width = std::max(width, p.row_ptr[r + 1] - p.row_ptr[r]);
+                p.sell_base[r] = static_cast<int32_t>(std::min<int64_t>(9 * slots + l, std::numeric_limits<int32_t>::max()));
             }
-            lanes += need;
-            ++rows;
-            if (need > 32) {
-                p.spmv_tile_row.push_back(v + 1);
-                lanes = rows = 0;
+            slots += 32 * static_cast<int64_t>(width);
+            if (9 * slots + 9 * 32 >= std::numeric_limits<int32_t>::max())
+                fail(LPG_EINVAL, "mesh too large for the solver's int32 Hessian offsets");
+            p.sell_ptr[c + 1] = static_cast<int32_t>(slots);
+        }
+        p.sell_col.assign(static_cast<size_t>(slots), 0);
+        for (int c = 0; c < nch; ++c) {
+            const int width = (p.sell_ptr[c + 1] - p.sell_ptr[c]) / 32;
+            for (int l = 0; l < 32; ++l) {
+                const int r = p.sell_row[32 * static_cast<size_t>(c) + l];
+                const int nb = r < 0 ? 0 : p.row_ptr[r + 1] - p.row_ptr[r];
+                for (int q = 0; q < width; ++q)
+                    p.sell_col[p.sell_ptr[c] + 32 * static_cast<size_t>(q) + l] =
+                        q < nb ? p.col_idx[p.row_ptr[r] + q] : std::max(r, 0);
             }
         }
-        if (rows > 0) p.spmv_tile_row.push_back(V);
-        p.spmv_row_tile.assign(static_cast<size_t>(V), 0);
-        for (size_t t = 0; t + 1 < p.spmv_tile_row.size(); ++t)
-            for (int v = p.spmv_tile_row[t]; v < p.spmv_tile_row[t + 1]; ++v) p.spmv_row_tile[v] = static_cast<int32_t>(t);
     }
     // Warp tiles: whole rows, at most `cap` pairs and 32 rows per tile. First fit over a
     // short window of open tiles keeps rows of one tile close in memory.

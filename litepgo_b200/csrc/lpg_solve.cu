@@ -193,28 +193,27 @@ template <int S, typename T> __device__ __forceinline__ void st3(T* p, size_t v,
     }
 }
 
-// Entry t (row-major) of the diagonal block of vertex v in the tiled layout, or -1.
+// Entry t (row-major) of the diagonal block of vertex v in the sliced-ELL layout, or -1.
 __device__ __forceinline__ int64_t diag_entry(const DevMesh& m, int v, int t) {
     const int k = m.diag_slot[v];
     if (k < 0) return -1;
-    return static_cast<int64_t>(tiled_pos(m.row_ptr, m.spmv_tile_row, m.spmv_row_tile, v, k, t));
+    return static_cast<int64_t>(m.sell_base[v]) + 32 * static_cast<int64_t>(9 * (k - m.row_ptr[v]) + t);
 }
 
-// y = mask (K x) on the 3x3 block-CSR matrix stored in the tiled layout (entry t of block k of
-// the SpMV tile [k0, k0 + n) at 9 k0 + t n + k - k0). Rows are packed into warp tiles of
-// consecutive rows with at most 32 blocks (one lane per block; a longer row has a tile of its
-// own and its lanes loop), so each of the nine value loads of a warp is one contiguous run;
-// each lane gathers its column's x, and a segmented warp scan sums each row. Vectors hold S
-// values per vertex: S = 4 for the padded PCG vectors (4th value zero, one 16-byte load per
-// gathered vertex in FP32), S = 3 for plain FP64 vectors. With PCG the vector is formed on
-// the fly as z + beta p_old (beta from the state; the row owners write it to p_new), and the
-// block of the grid that finishes last reduces the partial p.Ap sums into alpha; otherwise,
-// with DOT, part[block] = sum x.y. Both reductions use a fixed order.
+// y = mask (K x) on the 3x3 block matrix in the sliced-ELL layout (SELL-32): one warp per
+// chunk of 32 rows, one lane per row, block slot q of every lane read together, so each of the
+// nine value loads and the column load of a slot is one contiguous 128-byte (FP32) run, and a
+// lane's slots are independent (no cross-lane reduction). Vectors hold S values per vertex: 4
+// for the padded PCG vectors (4th value zero, one 16-byte load per gathered vertex in FP32),
+// 3 for plain FP64 vectors. With PCG the vector is z + beta p_old (beta from the state; each
+// row writes it to p_new), and the block of the grid that finishes last reduces the partial
+// p.Ap sums into alpha; otherwise, with DOT, part[block] = sum x.y. Both reductions use a
+// fixed order.
 template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S>
-__global__ void __launch_bounds__(kThreads) spmv_tiles(const DevMesh m, const TK* __restrict__ val,
-                                                       const TV* __restrict__ x, const TV* __restrict__ p_old,
-                                                       const TV* __restrict__ mask, TO* __restrict__ y,
-                                                       TV* __restrict__ p_new, PcgState* st, double* part) {
+__global__ void __launch_bounds__(kThreads) spmv_sell(const DevMesh m, const TK* __restrict__ val,
+                                                      const TV* __restrict__ x, const TV* __restrict__ p_old,
+                                                      const TV* __restrict__ mask, TO* __restrict__ y,
+                                                      TV* __restrict__ p_new, PcgState* st, double* part) {
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
     using A = typename std::conditional<(sizeof(TK) == 4 && sizeof(TV) == 4), float, double>::type;
@@ -223,69 +222,35 @@ __global__ void __launch_bounds__(kThreads) spmv_tiles(const DevMesh m, const TK
     const int lane = threadIdx.x & 31;
     const int nwarps = gridDim.x * (blockDim.x >> 5);
     double dot = 0;
-    for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < m.n_spmv_tiles; t += nwarps) {
-        const int r0 = __ldg(m.spmv_tile_row + t);
-        const int nrows = __ldg(m.spmv_tile_row + t + 1) - r0;
-        const int k0 = __ldg(m.row_ptr + r0);
-        const int ntb = __ldg(m.row_ptr + r0 + nrows) - k0;
-        int s = 0, nb = 0;
-        if (lane < nrows) {
-            s = __ldg(m.row_ptr + r0 + lane);
-            nb = __ldg(m.row_ptr + r0 + lane + 1) - s;
-        }
-        const int need = lane < nrows ? max(nb, 1) : 0;
-        int incl = need;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl += u;
-        }
-        const int start = incl - need;
-        const unsigned heads = __reduce_or_sync(0xffffffffu, lane < nrows ? 1u << min(start, 31) : 0u);
-        const unsigned upto = heads & (0xffffffffu >> (31 - lane));
-        const int jr = __popc(upto) - 1;
-        const int s_r = __shfl_sync(0xffffffffu, s, jr);
-        const int nb_r = __shfl_sync(0xffffffffu, nb, jr);
-        const int start_r = __shfl_sync(0xffffffffu, start, jr);
-        const int lanes_r = nrows == 1 ? min(max(nb_r, 1), 32) : max(nb_r, 1);
-        const TK* vt = val + 9 * static_cast<size_t>(k0);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < m.n_sell; c += nwarps) {
+        const int row = __ldg(m.sell_row + 32 * static_cast<size_t>(c) + lane);
+        const int s0 = __ldg(m.sell_ptr + c);
+        const int width = (__ldg(m.sell_ptr + c + 1) - s0) >> 5;
+        const int* cp = m.sell_col + s0 + lane;
+        const TK* vp = val + 9 * static_cast<size_t>(s0) + lane;
         A a0 = 0, a1 = 0, a2 = 0;
-        const int step = nrows == 1 ? 32 : (1 << 30);
-        for (int b = lane - start_r; b < nb_r && lane - start_r < lanes_r; b += step) {
-            const int k = s_r + b;
-            const size_t c = static_cast<size_t>(__ldg(m.col_idx + k));
+#pragma unroll 4
+        for (int q = 0; q < width; ++q) {
+            const size_t col = static_cast<size_t>(__ldg(cp + 32 * q));
             TV xz[3];
-            ld3<S>(x, c, xz);
+            ld3<S>(x, col, xz);
             if (PCG) {
                 TV xp[3];
-                ld3<S>(p_old, c, xp);
+                ld3<S>(p_old, col, xp);
 #pragma unroll
                 for (int i = 0; i < 3; ++i) xz[i] = xz[i] + beta * xp[i];
             }
             const A xv[3] = {static_cast<A>(xz[0]), static_cast<A>(xz[1]), static_cast<A>(xz[2])};
-            const TK* vk = vt + (k - k0);
+            const TK* vq = vp + 288 * static_cast<size_t>(q);
             A kv[9];
 #pragma unroll
-            for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vk + static_cast<size_t>(e) * ntb));
+            for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
             a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
             a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
             a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
         }
-        // Segmented inclusive scan over the lanes of each row (fixed pattern).
-        const int seg = 31 - __clz(upto);
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const A t0 = __shfl_up_sync(0xffffffffu, a0, off);
-            const A t1 = __shfl_up_sync(0xffffffffu, a1, off);
-            const A t2 = __shfl_up_sync(0xffffffffu, a2, off);
-            if (lane - off >= seg) {
-                a0 = t0 + a0;
-                a1 = t1 + a1;
-                a2 = t2 + a2;
-            }
-        }
-        if (jr < nrows && lane == start_r + lanes_r - 1) {
-            const size_t o = static_cast<size_t>(r0 + jr);
+        if (row >= 0) {
+            const size_t o = static_cast<size_t>(row);
             TV mv[3];
             ld3<S>(mask, o, mv);
             const A yv[3] = {static_cast<A>(mv[0]) * a0, static_cast<A>(mv[1]) * a1, static_cast<A>(mv[2]) * a2};
@@ -627,20 +592,22 @@ struct Solver {
         return e - energy_dot_f(x, f);
     }
 
-    // One warp per SpMV tile at a time (8 per block), grid-stride over the tiles.
+    // One warp per sliced-ELL chunk at a time (8 per block), grid-stride, one wave of blocks.
     template <typename Kern> int spmv_grid(Kern k) const {
-        return one_wave(k, (static_cast<size_t>(h.dm.n_spmv_tiles) + 7) / 8);
+        return one_wave(k, (static_cast<size_t>(h.dm.n_sell) + 7) / 8);
     }
     template <typename Kern> int vec_grid(Kern k) const { return one_wave(k, grid(static_cast<size_t>(V))); }
 
     // y64 = mask (K x64) in FP64 with K stored as TK.
     void residual_spmv(const void* K, bool k64, const double* x64, const double* mask, double* y64) {
         if (k64)
-            spmv_tiles<double, double, double, false, false, 3><<<spmv_grid(spmv_tiles<double, double, double, false, false, 3>), kThreads, 0, s>>>(
-                h.dm, static_cast<const double*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
+            spmv_sell<double, double, double, false, false, 3>
+                <<<spmv_grid(spmv_sell<double, double, double, false, false, 3>), kThreads, 0, s>>>(
+                    h.dm, static_cast<const double*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
         else
-            spmv_tiles<float, double, double, false, false, 3><<<spmv_grid(spmv_tiles<float, double, double, false, false, 3>), kThreads, 0, s>>>(
-                h.dm, static_cast<const float*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
+            spmv_sell<float, double, double, false, false, 3>
+                <<<spmv_grid(spmv_sell<float, double, double, false, false, 3>), kThreads, 0, s>>>(
+                    h.dm, static_cast<const float*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
         LPG_CUDA(cudaGetLastError());
     }
 
@@ -655,11 +622,11 @@ struct Solver {
     template <typename R>
     void enqueue_iterations(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA,
                             R* pB, R* Ap, PcgState* st, double* part, int pairs) {
-        const int sg = spmv_grid(spmv_tiles<R, R, R, true, false, 4>), ug = vec_grid(pcg_update<R>);
+        const int sg = spmv_grid(spmv_sell<R, R, R, true, false, 4>), ug = vec_grid(pcg_update<R>);
         for (int i = 0; i < pairs; ++i) {
-            spmv_tiles<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
+            spmv_sell<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
             pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pB, Ap, V, part);
-            spmv_tiles<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pB, mask4, Ap, pA, st, part);
+            spmv_sell<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pB, mask4, Ap, pA, st, part);
             pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pA, Ap, V, part);
         }
     }
@@ -685,7 +652,7 @@ struct Solver {
         double* r64 = h.s_r64.as<double>(n);
         double* y64 = h.s_b64.as<double>(n);
         const int vg = vec_grid(pcg_init<R>);
-        const int pg = std::max(spmv_grid(spmv_tiles<R, R, R, true, false, 4>), vec_grid(pcg_update<R>));
+        const int pg = std::max(spmv_grid(spmv_sell<R, R, R, true, false, 4>), vec_grid(pcg_update<R>));
         double* part = h.s_part.as<double>(std::max(4 * 1024, 2 * std::max(pg, vg)));
         PcgState* st = reinterpret_cast<PcgState*>(h.s_scal.as<double>(64));
         LPG_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), s));
@@ -803,8 +770,10 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
     const double* x0d = h.stage_in(x0, io_mem, h.d_u, n);
     LPG_CUDA(cudaMemcpyAsync(x, x0d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     const bool f64 = o.precision == LPG_PRECISION_F64;
-    const size_t hbytes = 9 * static_cast<size_t>(h.dm.nnzb) * (f64 ? 8 : 4);
+    // Hessian in the sliced-ELL layout; its padding slots are zeroed once and never written.
+    const size_t hbytes = 9 * static_cast<size_t>(h.plan.sell_ptr.back()) * (f64 ? 8 : 4);
     void* K = h.s_hess.ensure(std::max<size_t>(hbytes, 8));
+    LPG_CUDA(cudaMemsetAsync(K, 0, hbytes, s));
     void* dinv = h.s_dinv.ensure(12 * static_cast<size_t>(std::max(V, 1)) * (f64 ? 8 : 4));
     double* rhs = h.s_g.as<double>(2 * std::max<size_t>(n, 1)) + std::max<size_t>(n, 1); // second half of s_g
     int* moved = reinterpret_cast<int*>(h.s_flag.as<int>(4));
@@ -840,7 +809,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         // Energy and FP64 gradient (the Newton residual).
         double E;
         if (f64) {
-            h.eval_async(x, g, o.hessian, LPG_PRECISION_F64, kLayoutTiled, K, nullptr);
+            h.eval_async(x, g, o.hessian, LPG_PRECISION_F64, kLayoutSell, K, nullptr);
             if (f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
             double e = 0;
             LPG_CUDA(cudaMemcpyAsync(&e, h.d_energy.ptr, sizeof e, cudaMemcpyDeviceToHost, s));
@@ -860,7 +829,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         if (converged) return finish(0);
         if (it == o.max_iterations) return finish(1);
         if (!f64) {
-            h.eval_async(x, nullptr, o.hessian, LPG_PRECISION_MIXED, kLayoutTiled, K, nullptr);
+            h.eval_async(x, nullptr, o.hessian, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr);
             raise_status(h.take_status());
         }
         // Descent direction with diagonal shifts (newton.cpp:55-72).
@@ -961,8 +930,11 @@ void adjoint_solve(lpg_fem& h, const double* u_star, const double* dLdu, const i
     if (!std::isfinite(ws[1])) fail(LPG_EDOMAIN, "StaticEquilibriumResponse: nonfinite sensitivity right-hand side");
     if (n == 0 || !(ws[1] > 0)) return;
     // Exact FP64 Hessian at u*: the residual matrix of the refinement (static_equilibrium_response.cpp:58).
-    double* K64 = h.s_hess64.as<double>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
-    h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutTiled, K64, nullptr);
+    // Sliced-ELL Hessians; padding slots zeroed (never written by the assembly).
+    const size_t nv = 9 * static_cast<size_t>(h.plan.sell_ptr.back());
+    double* K64 = h.s_hess64.as<double>(std::max<size_t>(nv, 1));
+    LPG_CUDA(cudaMemsetAsync(K64, 0, nv * sizeof(double), s));
+    h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutSell, K64, nullptr);
     raise_status(h.take_status());
     double* rhs = h.s_g.as<double>(std::max<size_t>(n, 1));
     LPG_CUDA(cudaMemcpyAsync(rhs, w, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -972,8 +944,7 @@ void adjoint_solve(lpg_fem& h, const double* u_star, const double* dLdu, const i
         block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K64, mask, dinv, V);
         po = S.pcg<double>(K64, dinv, K64, true, mask, rhs, lam, cg_tolerance, 200000, 2);
     } else {
-        float* K32 = h.s_hess.as<float>(std::max<size_t>(9 * static_cast<size_t>(h.dm.nnzb), 1));
-        const size_t nv = 9 * static_cast<size_t>(h.dm.nnzb);
+        float* K32 = h.s_hess.as<float>(std::max<size_t>(nv, 1));
         if (nv) convert_kernel<double, float><<<grid(nv), kThreads, 0, s>>>(K64, K32, nv);
         float* dinv = h.s_dinv.as<float>(12 * static_cast<size_t>(std::max(V, 1)));
         block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(h.dm, K32, mask, dinv, V);

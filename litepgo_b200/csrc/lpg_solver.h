@@ -33,8 +33,9 @@ struct lpg_fem {
     std::atomic<bool> busy{false};
     // Plan and element data.
     lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tile_pair_ptr, b_tile_row_ptr, b_tile_rows, b_tile_slot_ptr,
-        b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused, b_spmv_tiles, b_spmv_row_tile;
+        b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused;
     lpg::DeviceBuffer b_cl[10]; // assembly clusters
+    lpg::DeviceBuffer b_sell[4]; // sliced-ELL pattern of the solvers
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_status, d_tile_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
     // Solver state (Newton / PCG / adjoint).

@@ -277,33 +277,26 @@ def test_valence_above_32():
     assert rel_err(H.data, vr) <= TOL64
 
 
-def spmv_tile_rows(row_ptr):
-    """First row of each SpMV tile (and V): runs of consecutive rows with at most 32 blocks
-    and 32 rows (a row without blocks counts as one block), a longer row on its own."""
-    V = row_ptr.size - 1
-    starts, lanes, rows = [0], 0, 0
-    for v in range(V):
-        need = max(1, int(row_ptr[v + 1] - row_ptr[v]))
-        if rows > 0 and (lanes + need > 32 or rows == 32):
-            starts.append(v)
-            lanes = rows = 0
-        lanes += need
-        rows += 1
-        if need > 32:
-            starts.append(v + 1)
-            lanes = rows = 0
-    if rows > 0:
-        starts.append(V)
-    return np.array(starts)
+def sell_layout(e):
+    import ctypes
+
+    from litepgo_b200 import _native as N
+
+    nslots, nch = ctypes.c_int64(), ctypes.c_int()
+    N.check(N.lib.lpg_fem_solver_layout(e.handle, ctypes.byref(nslots), ctypes.byref(nch), None, None))
+    ptr = np.empty(nch.value + 1, np.int32)
+    rows = np.empty(32 * nch.value, np.int32)
+    N.check(N.lib.lpg_fem_solver_layout(e.handle, None, None, N.iptr(ptr), N.iptr(rows)))
+    return nslots.value, ptr, rows
 
 
-def tiled_values(e, u, hessian, precision, layout):
+def solver_values(e, u, hessian, precision, layout, nvalues):
     import ctypes
 
     from litepgo_b200 import _native as N
 
     dt = torch.float64 if precision == N.PRECISION_F64 else torch.float32
-    hess = torch.full((9 * e.nnzb,), float("nan"), dtype=dt, device="cuda")
+    hess = torch.full((nvalues,), float("nan"), dtype=dt, device="cuda")
     ud = torch.as_tensor(u, device="cuda")
     ma, me = ctypes.c_double(), ctypes.c_double()
     N.check(N.lib.lpg_fem_time_eval(e.handle, N.vptr(ud), None, int(hessian), precision, layout, N.vptr(hess), 1, 0,
@@ -312,9 +305,9 @@ def tiled_values(e, u, hessian, precision, layout):
 
 
 @pytest.mark.parametrize("case", ["box", "ragged", "valence"])
-def test_solver_tiled_layout_is_a_permutation_of_bsr(case):
-    """The Newton / adjoint solvers keep the Hessian tile-interleaved (entry t of block k of the
-    SpMV tile [k0, k0 + n) at 9 k0 + t n + k - k0); it must hold the BSR values bit for bit."""
+def test_solver_sliced_ell_layout_is_a_permutation_of_bsr(case):
+    """The Newton / adjoint solvers keep the Hessian in sliced ELL (chunks of 32 rows sorted by
+    block count within 128-row windows, slot-major); it must hold the BSR values bit for bit."""
     from litepgo_b200 import _native as N
 
     rng = np.random.default_rng(12)
@@ -333,16 +326,34 @@ def test_solver_tiled_layout_is_a_permutation_of_bsr(case):
         theta, u = np.array([2.0, 3.0]), 0.01 * rng.standard_normal(X.size)
     e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta)
     row_ptr, _ = e.pattern_bsr()
-    starts = spmv_tile_rows(row_ptr)
-    perm = np.empty(9 * e.nnzb, np.int64)  # perm[bsr position] = tiled position
-    for r0, r1 in zip(starts[:-1], starts[1:]):
-        k0, k1 = int(row_ptr[r0]), int(row_ptr[r1])
-        ks = np.arange(k0, k1)
-        for t in range(9):
-            perm[9 * ks + t] = 9 * k0 + t * (k1 - k0) + (ks - k0)
-    assert np.array_equal(np.sort(perm), np.arange(9 * e.nnzb))
+    nb = np.diff(row_ptr)
+    V = X.shape[0]
+    nslots, ptr, rows = sell_layout(e)
+    # The layout's own rules: every row once, sorted by block count within 128-row windows,
+    # each chunk as wide as its longest row.
+    order = rows[rows >= 0]
+    assert np.array_equal(np.sort(order), np.arange(V)) and np.all(rows[V:] == -1)
+    for w0 in range(0, V, 128):
+        win = order[w0:w0 + 128]
+        assert np.array_equal(np.sort(win), np.arange(w0, min(V, w0 + 128)))
+        assert np.all(np.diff(nb[win]) <= 0)
+    for c in range(ptr.size - 1):
+        rc = rows[32 * c:32 * c + 32]
+        rc = rc[rc >= 0]
+        assert ptr[c + 1] - ptr[c] == 32 * nb[rc].max(initial=0)
+    assert nslots == ptr[-1]
+    perm = np.empty(9 * e.nnzb, np.int64)  # perm[bsr position] = sliced-ELL position
+    for c in range(ptr.size - 1):
+        for lane in range(32):
+            r = rows[32 * c + lane]
+            if r < 0:
+                continue
+            q = np.arange(nb[r])
+            for t in range(9):
+                perm[9 * (row_ptr[r] + q) + t] = 9 * ptr[c] + 32 * (9 * q + t) + lane
+    assert np.unique(perm).size == perm.size and perm.max() < 9 * nslots
     for hk in (Exact, Projected):
         for prec in (N.PRECISION_F64, N.PRECISION_MIXED):
-            bsr = tiled_values(e, u, hk, prec, N.LAYOUT_BSR)
-            tiled = tiled_values(e, u, hk, prec, 2)
-            assert np.array_equal(tiled[perm], bsr)
+            bsr = solver_values(e, u, hk, prec, N.LAYOUT_BSR, 9 * e.nnzb)
+            sell = solver_values(e, u, hk, prec, 2, 9 * nslots)
+            assert np.array_equal(sell[perm], bsr)
