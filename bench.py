@@ -63,33 +63,70 @@ def algorithmic_bytes(T, V, nnzb, precision="f64"):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event reasons sampled every 2 ms during the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    Reads NVML in a background thread (read-only queries; the device is matched to the CUDA
+    device by PCI bus id); falls back to nvidia-smi at its 200 ms cadence without NVML.
+    """
 
-    def __init__(self, gpu_index):
-        self.gpu = str(gpu_index)
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, cuda_device):
+        self.cuda_device = cuda_device
+        self.samples = []  # (sm_mhz, reasons bitmask)
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.thread = None
         self.proc = None
         self.lines = []
 
+    def _handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.cuda_device)
+        try:
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_device)
+
+    def _poll(self, nv, h):
+        reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), int(reasons_fn(h))))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-i", self.gpu, "-lms", "200"], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            nv, h = self._handle()
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
             self.thread.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+        except Exception:
+            self.thread = None
+            try:
+                fields = "clocks.sm,clocks.max.sm,clocks_event_reasons.active"
+                self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits",
+                                              "-i", str(self.cuda_device), "-lms", "200"], stdout=subprocess.PIPE,
+                                             stderr=subprocess.DEVNULL, text=True)
+                threading.Thread(target=lambda: self.lines.extend(l.strip() for l in self.proc.stdout),
+                                 daemon=True).start()
+            except (FileNotFoundError, OSError):
+                self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
+        if self.thread is not None:
+            time.sleep(0.004)
+            self.stop.set()
+            self.thread.join(timeout=2)
         if self.proc:
             time.sleep(0.25)
             self.proc.terminate()
@@ -97,25 +134,20 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-
-    def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
+                self.samples.append((float(parts[0]), int(parts[2], 16)))
+                self.max_mhz = float(parts[1])
+            except (ValueError, IndexError):
                 continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        reasons = sorted(n for n, bit in self.REASONS.items() if any(r & bit for _, r in self.samples))
+        return {"sm_mhz": statistics.median(s for s, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples)}
 
 
 def profile_traffic():
@@ -251,6 +283,11 @@ def newton_times(fem_energy, g, torch):
     for prec in ("mixed", "f64"):
         opts = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo",
                                     precision=prec, max_iterations=100, cg_tolerance=1e-2, cg_max_iterations=20000)
+        # Untimed warm-up solve (2 Newton iterations): buffers of this precision and its PCG
+        # graph exist before the timed solve, as in a solver called repeatedly.
+        warm = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo",
+                                    precision=prec, max_iterations=2, cg_tolerance=1e-2, cg_max_iterations=20000)
+        solver.newton_solve(total, fixed, x0, warm)
         t0 = time.perf_counter()
         r = solver.newton_solve(total, fixed, x0, opts)
         wall = time.perf_counter() - t0

@@ -209,8 +209,13 @@ __device__ __forceinline__ int64_t diag_entry(const DevMesh& m, int v, int t) {
 // row writes it to p_new), and the block of the grid that finishes last reduces the partial
 // p.Ap sums into alpha; otherwise, with DOT, part[block] = sum x.y. Both reductions use a
 // fixed order.
+// Resident blocks per SM the register allocation must allow (8 x 256 threads: 32 registers);
+// more resident warps hide the gathers' latency better than the registers they cost.
+#ifndef LPG_SPMV_MIN_BLOCKS
+#define LPG_SPMV_MIN_BLOCKS 8
+#endif
 template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S>
-__global__ void __launch_bounds__(kThreads) spmv_sell(const DevMesh m, const TK* __restrict__ val,
+__global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS) spmv_sell(const DevMesh m, const TK* __restrict__ val,
                                                       const TV* __restrict__ x, const TV* __restrict__ p_old,
                                                       const TV* __restrict__ mask, TO* __restrict__ y,
                                                       TV* __restrict__ p_new, PcgState* st, double* part) {
@@ -592,10 +597,10 @@ struct Solver {
         return e - energy_dot_f(x, f);
     }
 
-    // One warp per sliced-ELL chunk at a time (8 per block), grid-stride, one wave of blocks.
-    template <typename Kern> int spmv_grid(Kern k) const {
-        return one_wave(k, (static_cast<size_t>(h.dm.n_sell) + 7) / 8);
-    }
+    // One warp per sliced-ELL chunk (8 per block). Not persistent: with about one chunk per
+    // resident warp, a grid-stride loop would leave a fifth of the warps with two chunks and the
+    // rest idle; later blocks instead start as earlier ones finish.
+    template <typename Kern> int spmv_grid(Kern) const { return std::max(1, (h.dm.n_sell + 7) / 8); }
     template <typename Kern> int vec_grid(Kern k) const { return one_wave(k, grid(static_cast<size_t>(V))); }
 
     // y64 = mask (K x64) in FP64 with K stored as TK.
