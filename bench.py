@@ -460,6 +460,69 @@ def run_newton_only(prec, iterations):
     return 0
 
 
+def run_stress(steps):
+    """The 128^3 compression stress case: per-result error of the mixed path against FP64,
+    assembly GB/s of both kernels, and Newton time-to-1e-8 (relative gradient, Armijo) with the
+    top and bottom faces held at the compressed state, mixed vs FP64. The Newton uses the
+    projected Hessian until the gradient has fallen by 1e3, then the Exact one (exact_below): from
+    this noisy state the projected Hessian alone converges only linearly near the solution, and
+    the Exact one alone is indefinite far from it. Prints one JSON line."""
+    import torch
+
+    from litepgo_b200 import _native as N
+    from litepgo_b200 import dof, energy, fem, solver, workloads
+
+    torch.cuda.set_device(0)
+    w = workloads.compressed_box(128, seed=0)
+    X, tets, u_host = w["X"], w["tets"], w["u"]
+    T, V = tets.shape[0], X.shape[0]
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, w["theta"])
+    u = torch.as_tensor(u_host, device="cuda")
+    Exact = energy.HessianKind.Exact
+    E64, g64, H64 = e.eval_device(u, gradient=True, hessian=Exact, precision="f64")
+    E32, g32, H32 = e.eval_device(u, gradient=True, hessian=Exact, precision="mixed")
+    errors = {"energy": abs(E32 - E64) / abs(E64),
+              "gradient": float((g32 - g64).abs().max() / g64.abs().max()),
+              "hessian": float((H32.double() - H64).abs().max() / H64.abs().max())}
+    del H32
+    peak, _ = measured_peak()
+    kernels = {}
+    for prec, name, dt in ((N.PRECISION_F64, "f64", torch.float64), (N.PRECISION_MIXED, "mixed", torch.float32)):
+        hess = H64 if prec == N.PRECISION_F64 else torch.empty(e.nnz, dtype=dt, device="cuda")
+        ma, me = ctypes.c_double(), ctypes.c_double()
+        N.check(N.lib.lpg_fem_set_stream(e.handle, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        N.check(N.lib.lpg_fem_time_eval(e.handle, N.vptr(u), N.vptr(g64), int(Exact), prec, N.LAYOUT_BSR,
+                                        N.vptr(hess), steps, 1, ctypes.byref(ma), ctypes.byref(me)))
+        ab = algorithmic_bytes(T, V, e.nnzb, "f64" if name == "f64" else "f32")
+        gbs = ab / (ma.value * 1e-3) / 1e9
+        kernels[name] = {"kernel_ms": ma.value, "tets_per_s": T / (ma.value * 1e-3), "achieved_gbs": gbs,
+                         "frac_of_measured_hbm": gbs / peak, "algorithmic_bytes": ab}
+    del H64
+    N.check(N.lib.lpg_fem_set_stream(e.handle, None))
+    top_bottom = np.flatnonzero((X[:, 2] == 0.0) | (X[:, 2] == 1.0))
+    fixed = dof.DofReduction(3 * V, (3 * top_bottom[:, None] + np.arange(3)).ravel())
+    newton = {}
+    for prec in ("mixed", "f64"):
+        opts = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo",
+                                    precision=prec, max_iterations=300, cg_tolerance=1e-2, cg_max_iterations=50000,
+                                    exact_below=1e-3)
+        r = solver.newton_solve(e, fixed, u, opts)
+        newton[prec] = {"status": r.status.name, "seconds": r.seconds, "iterations": r.iterations,
+                        "cg_iterations": int(r.cg_iterations), "energy": r.energy,
+                        "relative_gradient": r.gradient_norm / max(r.gradient_norm0, 1e-300)}
+        newton[prec + "_x"] = r.x
+    xm, xf = newton.pop("mixed_x"), newton.pop("f64_x")
+    newton["max_abs_diff_mixed_vs_f64"] = float((xm - xf).abs().max())
+    if newton["mixed"]["seconds"] > 0:
+        newton["speedup_mixed_vs_f64"] = newton["f64"]["seconds"] / newton["mixed"]["seconds"]
+    print(json.dumps({"workload": "compressed box 128^3 cubes x 5 tets (V=2146689, T=10485760, nnzb=27608193), "
+                                  "z scaled by 0.6 plus 0.05 h N(0,1) per vertex, det F in [0.2, 3.0], seed "
+                                  f"{w['seed']}; Newton (projected, Exact below 1e-3 relative gradient): top and bottom faces "
+                                  "held, interior relaxed",
+                      "mixed_vs_f64_errors": errors, "assembly": kernels, "newton_time_to_1e-8": newton}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -473,7 +536,11 @@ def main():
     ap.add_argument("--only-newton", choices=("mixed", "f64"), default=None,
                     help="run a Newton solve cut at --newton-iterations iterations and exit (for ncu launch lists)")
     ap.add_argument("--newton-iterations", type=int, default=2)
+    ap.add_argument("--stress", action="store_true",
+                    help="run the 128^3 compression stress case (errors, assembly GB/s, Newton) and exit")
     args = ap.parse_args()
+    if args.stress:
+        return run_stress(max(args.steps, 3))
     if args.only_kernels:
         return run_kernels_only()
     if args.only_newton:

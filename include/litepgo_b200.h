@@ -230,6 +230,9 @@ typedef struct {
     int precision;              /* lpg_precision of the Hessian and PCG; residual and energy stay FP64 */
     double cg_tolerance;        /* forcing-term cap: relative PCG residual min(cg_tolerance, sqrt(||g||/||g0||)) */
     int cg_max_iterations;      /* per Newton iteration */
+    double exact_below;         /* not in the reference; default 0 (off): once ||g_free||_2 <= exact_below
+                                   ||g_free(x0)||_2, use the Exact Hessian instead of `hessian` (near a stable
+                                   equilibrium it is positive definite, and Newton converges quadratically) */
 } lpg_newton_options;
 
 typedef struct {

@@ -42,6 +42,7 @@ class NewtonOptionsC(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("cg_tolerance", ctypes.c_double),
         ("cg_max_iterations", ctypes.c_int),
+        ("exact_below", ctypes.c_double),
     ]
 
 

@@ -542,6 +542,7 @@ void lpg_newton_default_options(lpg_newton_options* o) {
     o->precision = LPG_PRECISION_F64;
     o->cg_tolerance = 1e-2;
     o->cg_max_iterations = 20000;
+    o->exact_below = 0.0;
 }
 
 int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double* f_ext, const double* x0,

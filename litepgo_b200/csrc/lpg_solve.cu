@@ -747,6 +747,8 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         fail(LPG_EINVAL, "newton_solve: max_iterations must be >= 0 and max_line_search_steps >= 1");
     if (!(o.line_search_shrink > 0.0 && o.line_search_shrink < 1.0))
         fail(LPG_EINVAL, "newton_solve: line_search_shrink must lie in (0, 1)");
+    if (!(o.exact_below >= 0.0) || !std::isfinite(o.exact_below))
+        fail(LPG_EINVAL, "newton_solve: exact_below must be finite and non-negative");
     if (o.hessian != LPG_HESSIAN_EXACT && o.hessian != LPG_HESSIAN_PROJECTED)
         fail(LPG_EINVAL, "newton_solve: invalid Hessian kind");
     if (o.precision != LPG_PRECISION_F64 && o.precision != LPG_PRECISION_MIXED)
@@ -810,11 +812,13 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         return;
     }
     double gnorm0 = -1;
+    bool exact = false; // the exact_below switch, decided on the previous iteration's gradient
     for (int it = 0;; ++it) {
+        const int hk = exact ? LPG_HESSIAN_EXACT : o.hessian;
         // Energy and FP64 gradient (the Newton residual).
         double E;
         if (f64) {
-            h.eval_async(x, g, o.hessian, LPG_PRECISION_F64, kLayoutSell, K, nullptr);
+            h.eval_async(x, g, hk, LPG_PRECISION_F64, kLayoutSell, K, nullptr);
             if (f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
             double e = 0;
             LPG_CUDA(cudaMemcpyAsync(&e, h.d_energy.ptr, sizeof e, cudaMemcpyDeviceToHost, s));
@@ -826,6 +830,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         const auto gs = S.stats<double, double>(g, nullptr, mask);
         const double g2 = std::sqrt(gs[1]), gmax = gs[2];
         if (gnorm0 < 0) gnorm0 = g2;
+        if (o.exact_below > 0 && g2 <= o.exact_below * gnorm0) exact = true;
         R.energy = E;
         R.gradient_norm = o.stop_rule == 0 ? gmax : g2;
         R.gradient_norm0 = gnorm0;
@@ -834,7 +839,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         if (converged) return finish(0);
         if (it == o.max_iterations) return finish(1);
         if (!f64) {
-            h.eval_async(x, nullptr, o.hessian, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr);
+            h.eval_async(x, nullptr, hk, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr);
             raise_status(h.take_status());
         }
         // Descent direction with diagonal shifts (newton.cpp:55-72).

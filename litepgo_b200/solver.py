@@ -39,12 +39,13 @@ class NewtonOptions:
     ||g_free||_2 <= tol ||g_free(x0)||_2), accept_rule ("noise": the reference's decrease
     within 16 eps; "armijo": sufficient decrease c = 1e-4 plus that noise), precision
     ("f64" or "mixed": FP32 Hessian and PCG, FP64 energy and residual), cg_tolerance (cap of
-    the PCG forcing term) and cg_max_iterations.
+    the PCG forcing term), cg_max_iterations, and exact_below (0 = off: once the gradient norm
+    falls to exact_below times its initial value, the Exact Hessian replaces ``hessian``).
     """
 
     def __init__(self, gradient_tolerance=float("nan"), max_iterations=50, hessian=HessianKind.Projected,
                  max_line_search_steps=30, line_search_shrink=0.5, stop_rule="max_abs", accept_rule="noise",
-                 precision="f64", cg_tolerance=1e-2, cg_max_iterations=20000):
+                 precision="f64", cg_tolerance=1e-2, cg_max_iterations=20000, exact_below=0.0):
         self.gradient_tolerance = gradient_tolerance
         self.max_iterations = max_iterations
         self.hessian = hessian
@@ -55,6 +56,7 @@ class NewtonOptions:
         self.precision = precision
         self.cg_tolerance = cg_tolerance
         self.cg_max_iterations = cg_max_iterations
+        self.exact_below = exact_below
 
     def to_c(self):
         o = N.NewtonOptionsC()
@@ -68,6 +70,7 @@ class NewtonOptions:
         o.precision = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
         o.cg_tolerance = float(self.cg_tolerance)
         o.cg_max_iterations = int(self.cg_max_iterations)
+        o.exact_below = float(self.exact_below)
         return o
 
 
