@@ -523,6 +523,71 @@ def run_stress(steps):
     return 0
 
 
+def run_batch():
+    """Config 3: 256 uneven boxes (cube counts per axis U{4..24}) solved as one batch by
+    solver.batch_newton_solve (relative gradient 1e-8, Armijo; projected Hessian, Exact once every
+    unfinished mesh's gradient has fallen by 1e3), mixed and FP64; meshes/s and the
+    per-mesh p50 / p99 completion times, beside the same meshes solved one call each (a sample of
+    32). Prints one JSON line."""
+    import scipy.sparse as sp
+    import torch
+
+    from litepgo_b200 import dof, energy, fem, solver, workloads
+
+    torch.cuda.set_device(0)
+    b = workloads.batch_boxes(count=256, seed=0)
+    X, tets, voff, eoff = b["X"], b["tets"], b["vertex_offsets"], b["element_offsets"]
+    n = X.size
+
+    def total_energy(Xs, ts, f):
+        e = fem.VolumetricFemEnergyTetP1.from_arrays(Xs, ts, b["theta"])
+        return energy.WeightedSumEnergy([(e, 1.0), (energy.QuadraticEnergy(sp.csc_matrix((f.size, f.size)), -f), 1.0)])
+
+    union = total_energy(X, tets, b["f"])
+    fixed = dof.DofReduction(n, b["fixed"])
+    x0 = torch.as_tensor(b["u0"], device="cuda")
+    out = {"workload": f"256 boxes, cube counts per axis U{{4..24}}, spacing 1/16, seed {b['seed']}: "
+                       f"V={X.shape[0]}, T={tets.shape[0]} (mean {tets.shape[0] / 256:.0f} tets per mesh); "
+                       "per-mesh affine state A = I + 0.1 N(0,1), bottom face fixed, gravity",
+           "rule": "relative gradient 1e-8, Armijo, exact_below 1e-3"}
+    for prec in ("mixed", "f64"):
+        opts = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo",
+                                    precision=prec, max_iterations=100, cg_tolerance=1e-2, exact_below=1e-3)
+        warm = solver.NewtonOptions(gradient_tolerance=1e-8, stop_rule="relative", accept_rule="armijo",
+                                    precision=prec, max_iterations=1, cg_tolerance=1e-2)
+        solver.batch_newton_solve(union, voff, eoff, fixed, x0, warm)
+        torch.cuda.synchronize()
+        _, per, total = solver.batch_newton_solve(union, voff, eoff, fixed, x0, opts)
+        t = np.array([p.seconds for p in per])
+        it = np.array([p.iterations for p in per])
+        tc = np.array([p.seconds for p in per if p.status == 0])
+        out[prec] = {"seconds": total.seconds, "meshes_per_s": 256 / total.seconds,
+                     "per_mesh_p50_s": float(np.percentile(t, 50)), "per_mesh_p99_s": float(np.percentile(t, 99)),
+                     "converged_p50_s": float(np.percentile(tc, 50)), "converged_p99_s": float(np.percentile(tc, 99)),
+                     "converged": int(sum(p.status == 0 for p in per)), "newton_iterations_max": int(it.max()),
+                     "newton_iterations_p50": float(np.median(it)), "lockstep_cg_iterations": int(total.cg_iterations)}
+        # The same meshes one call each (first 32): per-mesh seconds and the implied meshes/s.
+        single = []
+        for m in range(32):
+            v0, v1, e0, e1 = voff[m], voff[m + 1], eoff[m], eoff[m + 1]
+            fm = b["f"][3 * v0:3 * v1]
+            fx = b["fixed"][(b["fixed"] >= 3 * v0) & (b["fixed"] < 3 * v1)] - 3 * v0
+            em = total_energy(X[v0:v1], tets[e0:e1] - v0, fm)
+            xm0 = x0[3 * v0:3 * v1].contiguous()
+            solver.newton_solve(em, dof.DofReduction(3 * (v1 - v0), fx), xm0, warm)
+            t0 = time.perf_counter()
+            r = solver.newton_solve(em, dof.DofReduction(3 * (v1 - v0), fx), xm0, opts)
+            single.append((time.perf_counter() - t0, int(r.status), r.iterations))
+        out[prec]["one_call_per_mesh_sample"] = {
+            "meshes": 32, "mean_s": float(np.mean([s_[0] for s_ in single])),
+            "meshes_per_s": 1.0 / float(np.mean([s_[0] for s_ in single])),
+            "converged": sum(s_[1] == 0 for s_ in single),
+            "batch_statuses_of_these": [int(p.status) for p in per[:32]],
+            "single_iterations": [s_[2] for s_ in single], "batch_iterations": [int(p.iterations) for p in per[:32]]}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -538,7 +603,11 @@ def main():
     ap.add_argument("--newton-iterations", type=int, default=2)
     ap.add_argument("--stress", action="store_true",
                     help="run the 128^3 compression stress case (errors, assembly GB/s, Newton) and exit")
+    ap.add_argument("--batch", action="store_true",
+                    help="run the 256-mesh batched Newton (meshes/s, per-mesh p50/p99) and exit")
     args = ap.parse_args()
+    if args.batch:
+        return run_batch()
     if args.stress:
         return run_stress(max(args.steps, 3))
     if args.only_kernels:

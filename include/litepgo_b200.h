@@ -263,6 +263,35 @@ void lpg_newton_default_options(lpg_newton_options* options);
 int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed_dofs, int num_fixed, const double* f_ext, const double* x0,
                      int io_mem, const lpg_newton_options* options, double* x_out, lpg_newton_result* result);
 
+/* Per-mesh outcome of lpg_batch_newton_solve (status as lpg_newton_result.status). */
+typedef struct {
+    int status;
+    int iterations;
+    double energy;
+    double gradient_norm;
+    double gradient_norm0;
+    double seconds; /* from the start of the call to the iteration that ended this mesh */
+} lpg_batch_mesh_result;
+
+/*
+ * Batched newton_solve (no reference counterpart; the reference solves one energy per call):
+ * num_meshes independent meshes stored in one handle as contiguous vertex ranges
+ * [vertex_offsets[m], vertex_offsets[m+1]) and element ranges [element_offsets[m],
+ * element_offsets[m+1]) (every element inside its mesh's vertices). Assembly and SpMV run once
+ * over all meshes; every mesh has its own stop test, PCG scalars (one block-Jacobi PCG per mesh,
+ * in lockstep), feasible step and line search, as lpg_newton_solve has for one mesh. Where a
+ * mesh's PCG direction is not a descent direction, that iteration takes -g for the mesh instead
+ * of lpg_newton_solve's diagonal shifts. With exact_below the Exact Hessian is used once every
+ * unfinished mesh meets the threshold. fixed_dofs, f_ext, x0 and x_out are over the whole
+ * handle. per_mesh[num_meshes] receives the per-mesh outcomes; result (may be NULL) the totals
+ * (status = the worst mesh's, iterations = Newton iterations run, cg_iterations = lockstep PCG
+ * iterations, energy = the sum).
+ */
+int lpg_batch_newton_solve(lpg_fem_t h, int num_meshes, const int32_t* vertex_offsets, const int32_t* element_offsets,
+                           const int32_t* fixed_dofs, int num_fixed, const double* f_ext, const double* x0, int io_mem,
+                           const lpg_newton_options* options, double* x_out, lpg_batch_mesh_result* per_mesh,
+                           lpg_newton_result* result);
+
 /*
  * Adjoint of the static equilibrium: solves K_ff lambda = dLdu_free with the EXACT
  * Hessian at u_star and returns dtheta = -(dg/dtheta)^T lambda, per element

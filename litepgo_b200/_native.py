@@ -59,6 +59,17 @@ class NewtonResultC(ctypes.Structure):
     ]
 
 
+class BatchMeshResultC(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("energy", ctypes.c_double),
+        ("gradient_norm", ctypes.c_double),
+        ("gradient_norm0", ctypes.c_double),
+        ("seconds", ctypes.c_double),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 SIGNATURES = [
     ("lpg_last_error", ctypes.c_char_p, []),
@@ -83,6 +94,8 @@ SIGNATURES = [
     ("lpg_newton_default_options", None, [ctypes.POINTER(NewtonOptionsC)]),
     ("lpg_newton_solve", _int, [_vp, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC), _vp,
                                 ctypes.POINTER(NewtonResultC)]),
+    ("lpg_batch_newton_solve", _int, [_vp, _int, _ip, _ip, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC),
+                                      _vp, ctypes.POINTER(BatchMeshResultC), ctypes.POINTER(NewtonResultC)]),
     ("lpg_adjoint_theta", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _int, _vp, _vp]),
     ("lpg_fem_force_vjp_rest", _int, [_vp, _vp, _vp, _int, _vp]),
     ("lpg_adjoint_rest", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _vp, _vp]),

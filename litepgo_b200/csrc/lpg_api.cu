@@ -101,6 +101,7 @@ struct BusyGuard {
 
 lpg_fem::~lpg_fem() {
     if (pcg_graph) cudaGraphExecDestroy(pcg_graph);
+    if (batch_graph) cudaGraphExecDestroy(batch_graph);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -125,7 +126,8 @@ const double* lpg_fem::stage_in(const double* p, int mem, DeviceBuffer& buf, siz
 }
 
 void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int precision, int layout, void* dhess,
-                         double* delem, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+                         double* delem, cudaEvent_t ev_begin, cudaEvent_t ev_end, const int* emesh,
+                         const int* mesh_exact) {
     if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
         fail(LPG_EINVAL, "Energy: invalid Hessian kind");
     if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
@@ -145,7 +147,7 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.ev_end = ev_end;
     if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {
         void* proj = d_proj.ensure(project_bytes(dm, precision));
-        launch_project(dm, precision, hessian, du, proj, a.status, stream);
+        launch_project(dm, precision, hessian, du, proj, a.status, stream, emesh, mesh_exact);
         a.proj = proj;
     }
     launch_eval(dm, precision, hessian, a, stream);
@@ -600,6 +602,19 @@ int lpg_adjoint_rest(lpg_fem_t h, const double* u_star, const double* dLdu, cons
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         adjoint_rest(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, dX, lambda_out);
+    });
+}
+
+int lpg_batch_newton_solve(lpg_fem_t h, int num_meshes, const int32_t* vertex_offsets, const int32_t* element_offsets,
+                           const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
+                           const lpg_newton_options* o, double* x_out, lpg_batch_mesh_result* per_mesh,
+                           lpg_newton_result* result) {
+    return guarded([&] {
+        if (!h || !o || !x_out || (!x0 && h->dm.V > 0)) fail(LPG_EINVAL, "lpg_batch_newton_solve: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        batch_newton_solve(*h, num_meshes, vertex_offsets, element_offsets, fixed, nfixed, f_ext, x0, io_mem, *o, x_out,
+                           per_mesh, result);
     });
 }
 

@@ -664,7 +664,7 @@ __device__ double positive_det_step(const double* A, const double* dA, unsigned&
 
 __global__ void __launch_bounds__(256) feasible_kernel(const DevMesh m, const double* __restrict__ u,
                                                        const double* __restrict__ du, double* block_min,
-                                                       unsigned* status) {
+                                                       unsigned* status, double* per_elem) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double alpha = 1.0;
     unsigned st = 0;
@@ -712,6 +712,7 @@ __global__ void __launch_bounds__(256) feasible_kernel(const DevMesh m, const do
             st |= ST_NONFINITE_F;
         else if (st == 0)
             alpha = positive_det_step(F, dF, st);
+        if (per_elem) per_elem[e] = alpha;
     }
     // Block minimum (order-independent, hence deterministic).
     __shared__ double s[8];
@@ -847,7 +848,9 @@ template <> struct Eps<float> { static constexpr float v = 1.1920929e-7f; };
 
 template <typename R>
 __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, const double* __restrict__ u,
-                                                               R* __restrict__ proj, unsigned* status) {
+                                                               R* __restrict__ proj, unsigned* status,
+                                                               const int* __restrict__ emesh,
+                                                               const int* __restrict__ mesh_exact) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* A = reinterpret_cast<R*>(smem_raw) + kProjStride * threadIdx.x;
     R* V = A + 45;
@@ -890,9 +893,11 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
                         if (i == kk) v += k.mu * S[jp][lp];
                         A[sym9(r, c)] = k.vol * v;
                     }
+        // Elements of a mesh marked exact keep their tangent unclamped (the Exact Hessian).
+        const bool keep = emesh != nullptr && mesh_exact[emesh[e]] != 0;
         // LDL^T positive-definiteness test in the V area (row-major 9x9 scratch).
         bool pd = true;
-        for (int j = 0; j < 9 && pd; ++j) {
+        for (int j = 0; j < 9 && pd && !keep; ++j) {
             R d = A[sym9(j, j)];
             for (int t = 0; t < j; ++t) d -= V[9 * j + t] * V[9 * j + t] * V[9 * t + t];
             if (!(d > R(0))) {
@@ -907,7 +912,7 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
             }
         }
         R* out = proj + 45 * static_cast<size_t>(e);
-        if (pd) {
+        if (pd || keep) {
             for (int t = 0; t < 45; ++t) out[t] = A[t];
         } else {
             for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
@@ -1436,7 +1441,7 @@ size_t project_bytes(const DevMesh& m, int precision) {
 }
 
 void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
-                    cudaStream_t s) {
+                    cudaStream_t s, const int* emesh, const int* mesh_exact) {
     if (hessian != LPG_HESSIAN_PROJECTED) fail(LPG_EINVAL, "projected Hessian kind not available");
     const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
     if (blocks == 0) return;
@@ -1448,10 +1453,12 @@ void launch_project(const DevMesh& m, int precision, int hessian, const double* 
                                           static_cast<int>(sm)));
             configured = true;
         }
-        project_kernel<double><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<double*>(proj), status);
+        project_kernel<double><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<double*>(proj), status, emesh,
+                                                                mesh_exact);
     } else {
         const size_t sm = sizeof(float) * kProjStride * kProjThreads;
-        project_kernel<float><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<float*>(proj), status);
+        project_kernel<float><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<float*>(proj), status, emesh,
+                                                               mesh_exact);
     }
     LPG_CUDA(cudaGetLastError());
 }
@@ -1459,8 +1466,8 @@ void launch_project(const DevMesh& m, int precision, int hessian, const double* 
 int feasible_blocks(const DevMesh& m) { return (m.T + 255) / 256; }
 
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
-                     double* alpha, unsigned* status, cudaStream_t s) {
-    if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status);
+                     double* alpha, unsigned* status, cudaStream_t s, double* per_elem) {
+    if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status, per_elem);
     min_kernel<<<1, 1024, 0, s>>>(block_min, nblocks, alpha);
     LPG_CUDA(cudaGetLastError());
 }

@@ -146,11 +146,15 @@ struct EvalArgs {
 };
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s);
 // Per-element clamped tangents for the projected Hessians (45 values / element, upper triangle).
+// With emesh (element -> mesh) and mesh_exact (per mesh), the elements of the meshes marked
+// exact keep their tangent unclamped.
 void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
-                    cudaStream_t s);
+                    cudaStream_t s, const int* emesh = nullptr,
+                    const int* mesh_exact = nullptr);
 size_t project_bytes(const DevMesh& m, int precision);
+// per_elem (T doubles, optional) receives each element's step.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
-                     double* alpha, unsigned* status, cudaStream_t s);
+                     double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr);
 int feasible_blocks(const DevMesh& m);
 void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out_per_elem, unsigned* status,
                       cudaStream_t s);

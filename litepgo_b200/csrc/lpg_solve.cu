@@ -9,6 +9,7 @@
 // are two-stage with a fixed block -> index map, so results do not depend on scheduling.
 
 #include <algorithm>
+#include <chrono>
 #include <array>
 #include <cmath>
 #include <type_traits>
@@ -1023,6 +1024,737 @@ void adjoint_rest(lpg_fem& h, const double* u_star, const double* dLdu, const in
     if (io_mem == LPG_MEM_HOST && n > 0) LPG_CUDA(cudaMemcpyAsync(dX, out, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     copy_lambda(h, lam, io_mem, lambda_out);
     LPG_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------------------
+// Batched Newton: many independent meshes as one flat element / vertex stream. The meshes are
+// contiguous vertex and element ranges of one handle; assembly, SpMV and the vector kernels run
+// once over the union, while every per-mesh quantity (energy, gradient norms, PCG scalars,
+// feasible step, line search) is a segmented, fixed-order reduction over its mesh's range.
+// ---------------------------------------------------------------------------
+namespace {
+
+// One block per mesh over the DOFs [3 voff[m], 3 voff[m+1]): out[4m..] = {sum w a b, sum w a^2,
+// max w |a|, sum w b^2} with w = mask (1 where mask is null) and b = 0 where b is null.
+__global__ void __launch_bounds__(256) seg_stats(const double* __restrict__ a, const double* __restrict__ b,
+                                                 const double* __restrict__ mask, const int* __restrict__ voff,
+                                                 double* __restrict__ out) {
+    __shared__ double sh[4][8];
+    const int m = blockIdx.x;
+    const size_t lo = 3 * static_cast<size_t>(voff[m]), hi = 3 * static_cast<size_t>(voff[m + 1]);
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const double w = mask ? mask[i] : 1.0, av = a[i], bv = b ? b[i] : 0.0;
+        s0 += w * av * bv;
+        s1 += w * av * av;
+        s2 = fmax(s2, w * fabs(av));
+        s3 += w * bv * bv;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+        s2 = fmax(s2, __shfl_xor_sync(0xffffffffu, s2, off));
+        s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) sh[0][w] = s0, sh[1][w] = s1, sh[2][w] = s2, sh[3][w] = s3;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[4] = {0, 0, 0, 0};
+        for (int k = 0; k < (blockDim.x >> 5); ++k) {
+            r[0] += sh[0][k];
+            r[1] += sh[1][k];
+            r[2] = fmax(r[2], sh[2][k]);
+            r[3] += sh[3][k];
+        }
+        for (int k = 0; k < 4; ++k) out[4 * m + k] = r[k];
+    }
+}
+
+// One block per mesh over its elements [eoff[m], eoff[m+1]): sum (min_mode 0) or minimum
+// starting from 1 (min_mode 1) of a per-element value.
+__global__ void __launch_bounds__(256) seg_elem(const double* __restrict__ x, const int* __restrict__ eoff,
+                                                int min_mode, double* __restrict__ out) {
+    __shared__ double sh[8];
+    const int m = blockIdx.x;
+    double v = min_mode ? 1.0 : 0.0;
+    for (int e = eoff[m] + threadIdx.x; e < eoff[m + 1]; e += blockDim.x) v = min_mode ? fmin(v, x[e]) : v + x[e];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, v, off);
+        v = min_mode ? fmin(v, t) : v + t;
+    }
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = min_mode ? 1.0 : 0.0;
+        for (int k = 0; k < (blockDim.x >> 5); ++k) r = min_mode ? fmin(r, sh[k]) : r + sh[k];
+        out[m] = r;
+    }
+}
+
+// t = x + alpha[mesh] d and diff = t - x (the step actually taken) per DOF.
+__global__ void seg_axpy(const double* __restrict__ x, const double* __restrict__ alpha, const int* __restrict__ mov,
+                         const double* __restrict__ d, double* __restrict__ t, double* __restrict__ diff, size_t n) {
+    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const double v = x[i] + alpha[mov[i / 3]] * d[i];
+    t[i] = v;
+    diff[i] = v - x[i];
+}
+// x = src on the DOFs of the meshes with take[mesh] != 0.
+__global__ void seg_take(double* __restrict__ x, const double* __restrict__ src, const int* __restrict__ take,
+                         const int* __restrict__ mov, size_t n) {
+    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i < n && take[mov[i / 3]]) x[i] = src[i];
+}
+// b = -mask g on the active meshes, 0 elsewhere (an inactive mesh gets a zero direction).
+__global__ void seg_rhs(const double* __restrict__ g, const double* __restrict__ mask, const int* __restrict__ act,
+                        const int* __restrict__ mov, double* __restrict__ b, size_t n) {
+    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i < n) b[i] = act[mov[i / 3]] ? -mask[i] * g[i] : 0.0;
+}
+
+// Per-mesh PCG state (struct of arrays over the meshes).
+struct BatchPcg {
+    double *rz, *rr, *bb, *tol2, *alpha, *beta;
+    int *done, *iters, *brk;
+    int max_iters;
+};
+
+// r = b, x = 0, z = M^-1 r, p_old = 0 and the per-row r.z, r.r.
+template <typename R>
+__global__ void __launch_bounds__(kThreads) pcg_b_init(const R* __restrict__ b, const R* __restrict__ dinv, R* x, R* r,
+                                                       R* z, R* p_old, int V, double* __restrict__ rowdot2) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const size_t o = 4 * static_cast<size_t>(v);
+    R rv[4], zv[3];
+    ld4(b + o, rv);
+    apply_dinv(dinv + 12 * static_cast<size_t>(v), rv, zv);
+    st4(x + o, R(0), R(0), R(0));
+    st4(r + o, rv[0], rv[1], rv[2]);
+    st4(z + o, zv[0], zv[1], zv[2]);
+    st4(p_old + o, R(0), R(0), R(0));
+    double rz = 0, rr = 0;
+    for (int i = 0; i < 3; ++i) {
+        rz += static_cast<double>(rv[i]) * zv[i];
+        rr += static_cast<double>(rv[i]) * rv[i];
+    }
+    rowdot2[2 * static_cast<size_t>(v)] = rz;
+    rowdot2[2 * static_cast<size_t>(v) + 1] = rr;
+}
+
+// Sums per mesh of n interleaved per-row values (rows [voff[m], voff[m+1])), fixed order.
+template <int K>
+__device__ __forceinline__ void seg_rows(const double* __restrict__ rd, const int* __restrict__ voff, double* res) {
+    __shared__ double sh[K][8];
+    const int m = blockIdx.x;
+    double v[K];
+    for (int k = 0; k < K; ++k) v[k] = 0;
+    for (int r = voff[m] + threadIdx.x; r < voff[m + 1]; r += blockDim.x)
+        for (int k = 0; k < K; ++k) v[k] += rd[K * static_cast<size_t>(r) + k];
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+        if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < K; ++k) {
+            double t = 0;
+            for (int w = 0; w < (blockDim.x >> 5); ++w) t += sh[k][w];
+            res[k] = t;
+        }
+}
+
+__global__ void __launch_bounds__(256) pcg_b_start(BatchPcg st, const double* __restrict__ rowdot2,
+                                                   const int* __restrict__ voff, const double* __restrict__ tol,
+                                                   const int* __restrict__ act) {
+    double res[2];
+    seg_rows<2>(rowdot2, voff, res);
+    if (threadIdx.x != 0) return;
+    const int m = blockIdx.x;
+    st.rz[m] = res[0];
+    st.rr[m] = res[1];
+    st.bb[m] = res[1];
+    st.tol2[m] = tol[m] * tol[m] * res[1];
+    st.beta[m] = 0;
+    st.alpha[m] = 0;
+    st.iters[m] = 0;
+    st.brk[m] = 0;
+    st.done[m] = (!act[m] || res[1] == 0.0 || st.max_iters <= 0) ? 1 : 0;
+}
+
+// Ap = mask (K p) with p = z + beta[mesh] p_old formed on the fly (written to p_new), and the
+// per-row p.Ap; the sliced-ELL traversal of spmv_sell, one lane per row.
+template <typename R>
+__global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS)
+    spmv_sell_batch(const DevMesh m, const R* __restrict__ val, const R* __restrict__ z, const R* __restrict__ p_old,
+                    const R* __restrict__ mask, R* __restrict__ y, R* __restrict__ p_new, BatchPcg st,
+                    const int* __restrict__ mov, double* __restrict__ rowdot) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= m.n_sell) return;
+    const int row = __ldg(m.sell_row + 32 * static_cast<size_t>(c) + lane);
+    const int mesh = row >= 0 ? __ldg(mov + row) : 0;
+    const bool live = row >= 0 && !st.done[mesh];
+    const R beta = live ? static_cast<R>(st.beta[mesh]) : R(0);
+    const int s0 = __ldg(m.sell_ptr + c);
+    const int width = (__ldg(m.sell_ptr + c + 1) - s0) >> 5;
+    const int* cp = m.sell_col + s0 + lane;
+    const R* vp = val + 9 * static_cast<size_t>(s0) + lane;
+    R a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll 4
+    for (int q = 0; q < width; ++q) {
+        const size_t col = static_cast<size_t>(__ldg(cp + 32 * q));
+        R xz[3], xp[3];
+        ld3<4>(z, col, xz);
+        ld3<4>(p_old, col, xp);
+        const R xv[3] = {xz[0] + beta * xp[0], xz[1] + beta * xp[1], xz[2] + beta * xp[2]};
+        const R* vq = vp + 288 * static_cast<size_t>(q);
+        R kv[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) kv[e] = __ldg(vq + 32 * e);
+        a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
+        a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
+        a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
+    }
+    if (row < 0) return;
+    const size_t o = static_cast<size_t>(row);
+    R mv[3], xz[3], xp[3];
+    ld3<4>(mask, o, mv);
+    ld3<4>(z, o, xz);
+    ld3<4>(p_old, o, xp);
+    const R yv[3] = {mv[0] * a0, mv[1] * a1, mv[2] * a2};
+    st3<4, R>(y, o, yv[0], yv[1], yv[2]);
+    R pv[3];
+    double dot = 0;
+    for (int i = 0; i < 3; ++i) {
+        pv[i] = xz[i] + beta * xp[i];
+        dot += static_cast<double>(pv[i]) * static_cast<double>(yv[i]);
+    }
+    st3<4, R>(p_new, o, pv[0], pv[1], pv[2]);
+    rowdot[o] = live ? dot : 0.0;
+}
+
+__global__ void __launch_bounds__(256) pcg_b_alpha(BatchPcg st, const double* __restrict__ rowdot,
+                                                   const int* __restrict__ voff) {
+    const int m = blockIdx.x;
+    if (st.done[m]) return;
+    double res[1];
+    seg_rows<1>(rowdot, voff, res);
+    if (threadIdx.x != 0) return;
+    const double v = res[0];
+    if (!(v > 0.0) || !isfinite(v)) {
+        st.brk[m] = 1;
+        st.done[m] = 1;
+        st.alpha[m] = 0;
+    } else {
+        st.alpha[m] = st.rz[m] / v;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) pcg_b_update(BatchPcg st, const int* __restrict__ mov,
+                                                         const R* __restrict__ dinv, R* x, R* r, R* z,
+                                                         const R* __restrict__ p, const R* __restrict__ Ap, int V,
+                                                         double* __restrict__ rowdot2) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int mesh = __ldg(mov + v);
+    if (st.done[mesh]) {
+        rowdot2[2 * static_cast<size_t>(v)] = 0;
+        rowdot2[2 * static_cast<size_t>(v) + 1] = 0;
+        return;
+    }
+    const R alpha = static_cast<R>(st.alpha[mesh]);
+    const size_t o = 4 * static_cast<size_t>(v);
+    R xv[4], pv[4], rv[4], av[4], zv[3];
+    ld4c(x + o, xv);
+    ld4(p + o, pv);
+    ld4c(r + o, rv);
+    ld4(Ap + o, av);
+    for (int i = 0; i < 3; ++i) {
+        xv[i] += alpha * pv[i];
+        rv[i] = rv[i] - alpha * av[i];
+    }
+    apply_dinv(dinv + 12 * static_cast<size_t>(v), rv, zv);
+    st4(x + o, xv[0], xv[1], xv[2]);
+    st4(r + o, rv[0], rv[1], rv[2]);
+    st4(z + o, zv[0], zv[1], zv[2]);
+    double rz = 0, rr = 0;
+    for (int i = 0; i < 3; ++i) {
+        rz += static_cast<double>(rv[i]) * zv[i];
+        rr += static_cast<double>(rv[i]) * rv[i];
+    }
+    rowdot2[2 * static_cast<size_t>(v)] = rz;
+    rowdot2[2 * static_cast<size_t>(v) + 1] = rr;
+}
+
+__global__ void __launch_bounds__(256) pcg_b_beta(BatchPcg st, const double* __restrict__ rowdot2,
+                                                  const int* __restrict__ voff) {
+    const int m = blockIdx.x;
+    if (st.done[m]) return;
+    double res[2];
+    seg_rows<2>(rowdot2, voff, res);
+    if (threadIdx.x != 0) return;
+    const double a = res[0], b = res[1];
+    st.iters[m] += 1;
+    st.rr[m] = b;
+    if (b <= st.tol2[m] || st.iters[m] >= st.max_iters || !isfinite(b)) {
+        st.done[m] = 1;
+    } else {
+        st.beta[m] = a / st.rz[m];
+        st.rz[m] = a;
+    }
+}
+
+// Device arrays of one batched solve.
+struct BatchDev {
+    int M = 0;
+    int *voff = nullptr, *eoff = nullptr, *mov = nullptr, *emesh = nullptr;
+    int *act = nullptr, *take = nullptr, *exact = nullptr;
+    double *stats = nullptr, *esum = nullptr, *fdot = nullptr, *amin = nullptr, *alpha = nullptr, *tol = nullptr;
+    double *rowdot = nullptr, *rowdot2 = nullptr, *elem = nullptr;
+    BatchPcg pcg{};
+};
+
+struct BatchSolver {
+    lpg_fem& h;
+    BatchDev& d;
+    cudaStream_t s;
+    size_t n;
+    int V, M;
+    BatchSolver(lpg_fem& hh, BatchDev& dd)
+        : h(hh), d(dd), s(hh.stream), n(3 * static_cast<size_t>(hh.dm.V)), V(hh.dm.V), M(dd.M) {}
+
+    template <typename T> void down(std::vector<T>& v, const T* p, size_t count) {
+        v.resize(count);
+        if (count) LPG_CUDA(cudaMemcpyAsync(v.data(), p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+        LPG_CUDA(cudaStreamSynchronize(s));
+    }
+    template <typename T> void up(T* p, const std::vector<T>& v) {
+        if (!v.empty()) LPG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    // Per-mesh {sum w a b, sum w a^2, max w|a|, sum w b^2}.
+    std::vector<double> stats(const double* a, const double* b, const double* mask) {
+        seg_stats<<<M, 256, 0, s>>>(a, b, mask, d.voff, d.stats);
+        LPG_CUDA(cudaGetLastError());
+        std::vector<double> r;
+        down(r, d.stats, 4 * static_cast<size_t>(M));
+        return r;
+    }
+    // Per-mesh energy at x: element energies summed per mesh, minus f . x.
+    std::vector<double> energies(const double* x, const double* f, double* g, int hk, int precision, void* K) {
+        h.eval_async(x, g, hk, precision, kLayoutSell, K, d.elem, nullptr, nullptr, d.emesh, d.exact);
+        seg_elem<<<M, 256, 0, s>>>(d.elem, d.eoff, 0, d.esum);
+        LPG_CUDA(cudaGetLastError());
+        raise_status(h.take_status());
+        std::vector<double> e;
+        down(e, d.esum, M);
+        if (f) {
+            const auto fx = stats(x, f, nullptr);
+            for (int m = 0; m < M; ++m) e[m] -= fx[4 * m];
+        }
+        return e;
+    }
+
+    struct PcgOut {
+        int64_t iters = 0;
+        std::vector<int> breakdown;
+    };
+
+    template <typename R>
+    void enqueue(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA, R* pB, R* Ap,
+                 int pairs) {
+        const int sg = std::max(1, (h.dm.n_sell + 7) / 8), vg = grid(static_cast<size_t>(V));
+        for (int i = 0; i < pairs; ++i)
+            for (int half = 0; half < 2; ++half) {
+                R* po = half ? pB : pA;
+                R* pn = half ? pA : pB;
+                spmv_sell_batch<R><<<sg, kThreads, 0, gs>>>(h.dm, K, z, po, mask4, Ap, pn, d.pcg, d.mov, d.rowdot);
+                pcg_b_alpha<<<M, 256, 0, gs>>>(d.pcg, d.rowdot, d.voff);
+                pcg_b_update<R><<<vg, kThreads, 0, gs>>>(d.pcg, d.mov, dinv, x, r, z, pn, Ap, V, d.rowdot2);
+                pcg_b_beta<<<M, 256, 0, gs>>>(d.pcg, d.rowdot2, d.voff);
+            }
+    }
+
+    // Solves mask K x = mask b per active mesh (tolerance tol[m] relative to ||b_m||): inner PCG in
+    // precision R on Kin, FP64 refinement against Kres; the iterations replay a cached graph.
+    template <typename R>
+    PcgOut pcg(const void* Kin, const R* dinv, const void* Kres, bool res64, const double* mask, const double* b64,
+               double* x64, const std::vector<double>& tol, std::vector<int> act, int max_iters, int max_refine) {
+        PcgOut out;
+        out.breakdown.assign(M, 0);
+        const size_t n4 = 4 * static_cast<size_t>(V);
+        R* x = h.s_xcg.as<R>(n4);
+        R* r = h.s_r.as<R>(n4);
+        R* z = h.s_z.as<R>(n4);
+        R* pA = h.s_p.as<R>(n4);
+        R* pB = h.s_p2.as<R>(n4);
+        R* Ap = h.s_ap.as<R>(n4);
+        R* bR = h.s_trial.as<R>(n4);
+        R* mask4 = h.s_mask4.as<R>(n4);
+        double* r64 = h.s_r64.as<double>(n);
+        double* y64 = h.s_b64.as<double>(n);
+        LPG_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), s));
+        LPG_CUDA(cudaMemcpyAsync(r64, b64, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        const auto bs = stats(b64, nullptr, mask);
+        std::vector<double> bnorm(M), rnorm(M);
+        bool any = false;
+        for (int m = 0; m < M; ++m) {
+            bnorm[m] = rnorm[m] = std::sqrt(bs[4 * m + 1]);
+            act[m] = act[m] && bnorm[m] > 0;
+            any = any || act[m];
+        }
+        if (!any) return out;
+        pad_rhs<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(mask, mask, mask4, V);
+        constexpr int kPairs = 16;
+        const void* key[12] = {Kin, dinv, mask4, x, r, z, pA, pB, Ap, d.rowdot, d.pcg.rz,
+                               reinterpret_cast<const void*>((static_cast<size_t>(d.pcg.max_iters) << 40) ^
+                                                             (sizeof(R) * 1000003u + V + 7919u * static_cast<size_t>(M)))};
+        bool same = h.batch_graph != nullptr;
+        for (int i = 0; i < 12 && same; ++i) same = h.batch_graph_key[i] == key[i];
+        cudaStream_t gs = h.own_stream;
+        if (!same) {
+            if (h.batch_graph) {
+                cudaGraphExecDestroy(h.batch_graph);
+                h.batch_graph = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            LPG_CUDA(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+            enqueue<R>(gs, static_cast<const R*>(Kin), dinv, mask4, x, r, z, pA, pB, Ap, kPairs);
+            LPG_CUDA(cudaStreamEndCapture(gs, &g));
+            LPG_CUDA(cudaGraphInstantiate(&h.batch_graph, g, 0));
+            cudaGraphDestroy(g);
+            for (int i = 0; i < 12; ++i) h.batch_graph_key[i] = key[i];
+        }
+        cudaEvent_t ev;
+        LPG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        std::vector<double> itol(M);
+        std::vector<int> done, iters, brk;
+        int used = 0;
+        for (int ref = 0; ref <= max_refine; ++ref) {
+            for (int m = 0; m < M; ++m)
+                itol[m] = act[m] ? std::min(0.5, std::max(tol[m] * bnorm[m] / rnorm[m], sizeof(R) == 4 ? 1e-6 : 1e-14))
+                                 : 1.0;
+            up(d.tol, itol);
+            up(d.act, act);
+            pad_rhs<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(r64, mask, bR, V);
+            pcg_b_init<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(bR, dinv, x, r, z, pA, V, d.rowdot2);
+            pcg_b_start<<<M, 256, 0, s>>>(d.pcg, d.rowdot2, d.voff, d.tol, d.act);
+            LPG_CUDA(cudaGetLastError());
+            for (;;) {
+                LPG_CUDA(cudaEventRecord(ev, s));
+                LPG_CUDA(cudaStreamWaitEvent(gs, ev, 0));
+                LPG_CUDA(cudaGraphLaunch(h.batch_graph, gs));
+                LPG_CUDA(cudaEventRecord(ev, gs));
+                LPG_CUDA(cudaStreamWaitEvent(s, ev, 0));
+                down(done, d.pcg.done, M);
+                if (std::all_of(done.begin(), done.end(), [](int v) { return v != 0; })) break;
+            }
+            down(iters, d.pcg.iters, M);
+            down(brk, d.pcg.brk, M);
+            int mx = 0;
+            for (int m = 0; m < M; ++m) {
+                if (!act[m]) continue;
+                mx = std::max(mx, iters[m]);
+                if (brk[m]) out.breakdown[m] = 1;
+            }
+            used += mx;
+            out.iters += mx;
+            add_kernel<R><<<grid(n), kThreads, 0, s>>>(x64, x, n);
+            if (res64)
+                spmv_sell<double, double, double, false, false, 3>
+                    <<<std::max(1, (h.dm.n_sell + 7) / 8), kThreads, 0, s>>>(h.dm, static_cast<const double*>(Kres), x64,
+                                                                            nullptr, mask, y64, nullptr, nullptr, nullptr);
+            else
+                spmv_sell<float, double, double, false, false, 3>
+                    <<<std::max(1, (h.dm.n_sell + 7) / 8), kThreads, 0, s>>>(h.dm, static_cast<const float*>(Kres), x64,
+                                                                            nullptr, mask, y64, nullptr, nullptr, nullptr);
+            residual_kernel<<<grid(n), kThreads, 0, s>>>(b64, y64, mask, r64, n);
+            LPG_CUDA(cudaGetLastError());
+            const auto rs = stats(r64, nullptr, mask);
+            any = false;
+            for (int m = 0; m < M; ++m) {
+                rnorm[m] = std::sqrt(rs[4 * m + 1]);
+                act[m] = act[m] && !out.breakdown[m] && rnorm[m] > tol[m] * bnorm[m] && std::isfinite(rnorm[m]);
+                any = any || act[m];
+            }
+            if (!any || used >= max_iters) break;
+        }
+        cudaEventDestroy(ev);
+        return out;
+    }
+};
+
+} // namespace
+
+void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t* eoff_h, const int32_t* fixed,
+                        int nfixed, const double* f_ext, const double* x0, int io_mem, const lpg_newton_options& o,
+                        double* x_out, lpg_batch_mesh_result* per_mesh, lpg_newton_result* total) {
+    const int V = h.dm.V, T = h.dm.T;
+    if (M <= 0 || !voff_h || !eoff_h || !per_mesh) fail(LPG_EINVAL, "batch_newton_solve: invalid mesh offsets");
+    if (!(o.gradient_tolerance >= 0.0) || !std::isfinite(o.gradient_tolerance))
+        fail(LPG_EINVAL, "newton_solve: gradient_tolerance must be set to a finite non-negative value");
+    if (o.max_iterations < 0 || o.max_line_search_steps < 1)
+        fail(LPG_EINVAL, "newton_solve: max_iterations must be >= 0 and max_line_search_steps >= 1");
+    if (!(o.line_search_shrink > 0.0 && o.line_search_shrink < 1.0))
+        fail(LPG_EINVAL, "newton_solve: line_search_shrink must lie in (0, 1)");
+    if (o.hessian != LPG_HESSIAN_EXACT && o.hessian != LPG_HESSIAN_PROJECTED)
+        fail(LPG_EINVAL, "newton_solve: invalid Hessian kind");
+    if (o.precision != LPG_PRECISION_F64 && o.precision != LPG_PRECISION_MIXED)
+        fail(LPG_EINVAL, "newton_solve: invalid precision");
+    if (!(o.exact_below >= 0.0) || !std::isfinite(o.exact_below))
+        fail(LPG_EINVAL, "newton_solve: exact_below must be finite and non-negative");
+    // Meshes: contiguous vertex and element ranges; every element inside its mesh's vertices.
+    if (voff_h[0] != 0 || voff_h[M] != V || eoff_h[0] != 0 || eoff_h[M] != T)
+        fail(LPG_EINVAL, "batch_newton_solve: mesh offsets must start at 0 and end at the vertex / element counts");
+    for (int m = 0; m < M; ++m)
+        if (voff_h[m + 1] < voff_h[m] || eoff_h[m + 1] < eoff_h[m])
+            fail(LPG_EINVAL, "batch_newton_solve: mesh offsets must be non-decreasing");
+    cudaStream_t s = h.stream;
+    {
+        std::vector<int4> tv(static_cast<size_t>(T));
+        if (T) LPG_CUDA(cudaMemcpyAsync(tv.data(), h.dm.tets, T * sizeof(int4), cudaMemcpyDeviceToHost, s));
+        LPG_CUDA(cudaStreamSynchronize(s));
+        for (int m = 0; m < M; ++m)
+            for (int e = eoff_h[m]; e < eoff_h[m + 1]; ++e) {
+                const int vs[4] = {tv[e].x, tv[e].y, tv[e].z, tv[e].w};
+                for (int v : vs)
+                    if (v < voff_h[m] || v >= voff_h[m + 1])
+                        fail(LPG_EINVAL, "batch_newton_solve: element " + std::to_string(e) +
+                                             " references a vertex outside its mesh");
+            }
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    const size_t n = 3 * static_cast<size_t>(V);
+    BatchDev d;
+    d.M = M;
+    d.voff = h.bt_int[0].as<int>(M + 1);
+    d.eoff = h.bt_int[1].as<int>(M + 1);
+    d.mov = h.bt_int[2].as<int>(std::max(V, 1));
+    d.act = h.bt_int[3].as<int>(M);
+    d.take = h.bt_int[4].as<int>(M);
+    d.emesh = h.bt_int[6].as<int>(std::max(T, 1));
+    d.exact = h.bt_int[7].as<int>(M);
+    int* pcg_ints = h.bt_int[5].as<int>(3 * static_cast<size_t>(M) + 1);
+    d.pcg.done = pcg_ints;
+    d.pcg.iters = pcg_ints + M + 1;
+    d.pcg.brk = pcg_ints + 2 * M + 1;
+    double* dbl = h.bt_dbl[0].as<double>(16 * static_cast<size_t>(M));
+    d.stats = dbl;
+    d.esum = dbl + 4 * M;
+    d.fdot = dbl + 5 * M;
+    d.amin = dbl + 6 * M;
+    d.alpha = dbl + 7 * M;
+    d.tol = dbl + 8 * M;
+    d.pcg.rz = dbl + 9 * M;
+    d.pcg.rr = dbl + 10 * M;
+    d.pcg.bb = dbl + 11 * M;
+    d.pcg.tol2 = dbl + 12 * M;
+    d.pcg.alpha = dbl + 13 * M;
+    d.pcg.beta = dbl + 14 * M;
+    d.rowdot = h.bt_dbl[1].as<double>(std::max(V, 1));
+    d.rowdot2 = h.bt_dbl[2].as<double>(2 * static_cast<size_t>(std::max(V, 1)));
+    d.elem = h.bt_dbl[3].as<double>(std::max(T, 1));
+    d.pcg.max_iters = o.cg_max_iterations;
+    std::vector<int> mov_h(static_cast<size_t>(V));
+    for (int m = 0; m < M; ++m)
+        for (int v = voff_h[m]; v < voff_h[m + 1]; ++v) mov_h[v] = m;
+    BatchSolver B(h, d);
+    B.up(d.voff, std::vector<int>(voff_h, voff_h + M + 1));
+    B.up(d.eoff, std::vector<int>(eoff_h, eoff_h + M + 1));
+    B.up(d.mov, mov_h);
+    {
+        std::vector<int> em(static_cast<size_t>(T));
+        for (int m = 0; m < M; ++m)
+            for (int e = eoff_h[m]; e < eoff_h[m + 1]; ++e) em[e] = m;
+        B.up(d.emesh, em);
+    }
+    double* mask = h.s_mask.as<double>(std::max<size_t>(n, 1));
+    make_mask(h, fixed, nfixed, mask);
+    double* x = h.s_x.as<double>(std::max<size_t>(n, 1));
+    double* g = h.s_g.as<double>(2 * std::max<size_t>(n, 1));
+    double* rhs = g + std::max<size_t>(n, 1);
+    double* dir = h.s_d.as<double>(std::max<size_t>(n, 1));
+    double* trial = h.s_f.as<double>(3 * std::max<size_t>(n, 1));
+    double* diff = trial + std::max<size_t>(n, 1);
+    double* f = nullptr;
+    const double* fsrc = f_ext ? h.stage_in(f_ext, io_mem, h.d_u2, n) : nullptr;
+    if (fsrc) {
+        f = trial + 2 * std::max<size_t>(n, 1);
+        LPG_CUDA(cudaMemcpyAsync(f, fsrc, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    const double* x0d = h.stage_in(x0, io_mem, h.d_u, n);
+    LPG_CUDA(cudaMemcpyAsync(x, x0d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const bool f64 = o.precision == LPG_PRECISION_F64;
+    const size_t hbytes = 9 * static_cast<size_t>(h.plan.sell_ptr.back()) * (f64 ? 8 : 4);
+    void* K = h.s_hess.ensure(std::max<size_t>(hbytes, 8));
+    LPG_CUDA(cudaMemsetAsync(K, 0, hbytes, s));
+    void* dinv = h.s_dinv.ensure(12 * static_cast<size_t>(std::max(V, 1)) * (f64 ? 8 : 4));
+    const int nfeas = feasible_blocks(h.dm);
+    double* bm = h.d_block.as<double>(std::max(nfeas, 1));
+    double* al = h.d_alpha.as<double>(1);
+    // Per-mesh state on the host.
+    std::vector<int> status(M, -1), act(M, 1), iters(M, 0), take(M, 0), pending(M, 0);
+    std::vector<double> E(M, 0), g2(M, 0), gmax(M, 0), g0(M, -1), secs(M, 0), alpha(M, 0), gd(M, 0);
+    {
+        std::vector<double> mh;
+        B.down(mh, mask, n);
+        for (int m = 0; m < M; ++m) {
+            bool anyfree = false;
+            for (size_t i = 3 * static_cast<size_t>(voff_h[m]); i < 3 * static_cast<size_t>(voff_h[m + 1]); ++i)
+                anyfree = anyfree || mh[i] != 0;
+            if (!anyfree) act[m] = 0; // nothing to solve: converged at x0
+        }
+    }
+    lpg_newton_result R{};
+    // Per-mesh Hessian kind: a mesh whose gradient has fallen to exact_below of its first one
+    // switches to the Exact Hessian (its elements skip the projection's clamp).
+    std::vector<int> exact(M, o.hessian == LPG_HESSIAN_EXACT ? 1 : 0);
+    int it = 0;
+    for (;; ++it) {
+        B.up(d.exact, exact);
+        bool all_exact = true;
+        for (int m = 0; m < M; ++m) all_exact = all_exact && (exact[m] || !act[m]);
+        const int hk = all_exact ? LPG_HESSIAN_EXACT : LPG_HESSIAN_PROJECTED;
+        const std::vector<double> e = f64 ? B.energies(x, f, g, hk, LPG_PRECISION_F64, K)
+                                          : B.energies(x, f, g, LPG_HESSIAN_NONE, LPG_PRECISION_F64, nullptr);
+        if (f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
+        const auto gs = B.stats(g, nullptr, mask);
+        for (int m = 0; m < M; ++m) {
+            E[m] = e[m];
+            g2[m] = std::sqrt(gs[4 * m + 1]);
+            gmax[m] = gs[4 * m + 2];
+            if (g0[m] < 0) g0[m] = g2[m];
+            if (status[m] >= 0) continue;
+            if (!act[m]) {
+                status[m] = 0;
+                secs[m] = elapsed();
+                continue;
+            }
+            iters[m] = it;
+            const bool conv = o.stop_rule == 0 ? gmax[m] <= o.gradient_tolerance : g2[m] <= o.gradient_tolerance * g0[m];
+            if (conv || it == o.max_iterations) {
+                status[m] = conv ? 0 : 1;
+                act[m] = 0;
+                secs[m] = elapsed();
+            } else if (o.exact_below > 0 && g2[m] <= o.exact_below * g0[m]) {
+                exact[m] = 1;
+            }
+        }
+        if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
+        if (!f64) {
+            // The flags of this iteration's start (d.exact), as the FP64 path uses.
+            h.eval_async(x, nullptr, hk, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr, nullptr, nullptr, d.emesh,
+                         d.exact);
+            raise_status(h.take_status());
+        }
+        // Descent directions: per-mesh PCG on the block-diagonal system, forcing term per mesh.
+        B.up(d.act, act);
+        seg_rhs<<<grid(n), kThreads, 0, s>>>(g, mask, d.act, d.mov, rhs, n);
+        std::vector<double> tol(M, 1.0);
+        for (int m = 0; m < M; ++m)
+            if (act[m]) tol[m] = std::min(o.cg_tolerance, std::sqrt(g2[m] / g0[m]));
+        BatchSolver::PcgOut po;
+        if (f64) {
+            block_jacobi<double, double><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(
+                h.dm, static_cast<double*>(K), mask, static_cast<double*>(dinv), V);
+            po = B.pcg<double>(K, static_cast<double*>(dinv), K, true, mask, rhs, dir, tol, act, o.cg_max_iterations, 0);
+        } else {
+            block_jacobi<float, float><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(
+                h.dm, static_cast<float*>(K), mask, static_cast<float*>(dinv), V);
+            po = B.pcg<float>(K, static_cast<float*>(dinv), K, false, mask, rhs, dir, tol, act, o.cg_max_iterations, 3);
+        }
+        R.cg_iterations += po.iters;
+        // A mesh whose direction is not a descent direction (negative curvature at the first PCG
+        // step) takes the steepest-descent direction -g for this iteration.
+        auto gds = B.stats(g, dir, mask);
+        bool fallback = false;
+        for (int m = 0; m < M; ++m) {
+            take[m] = act[m] && !(gds[4 * m] < 0.0 && std::isfinite(gds[4 * m]));
+            fallback = fallback || take[m];
+        }
+        if (fallback) {
+            B.up(d.take, take);
+            seg_take<<<grid(n), kThreads, 0, s>>>(dir, rhs, d.take, d.mov, n);
+            gds = B.stats(g, dir, mask);
+        }
+        for (int m = 0; m < M; ++m) gd[m] = gds[4 * m];
+        // Line search per mesh from its feasible step.
+        launch_feasible(h.dm, x, dir, bm, nfeas, al, h.d_status.as<unsigned>(1), s, d.elem);
+        seg_elem<<<M, 256, 0, s>>>(d.elem, d.eoff, 1, d.amin);
+        raise_status(h.take_status());
+        std::vector<double> amin;
+        B.down(amin, d.amin, M);
+        for (int m = 0; m < M; ++m) {
+            pending[m] = act[m];
+            alpha[m] = act[m] ? amin[m] : 0.0;
+        }
+        for (int j = 0; j < o.max_line_search_steps; ++j) {
+            if (std::none_of(pending.begin(), pending.end(), [](int v) { return v != 0; })) break;
+            std::vector<double> a(M);
+            for (int m = 0; m < M; ++m) a[m] = pending[m] ? alpha[m] : 0.0;
+            B.up(d.alpha, a);
+            seg_axpy<<<grid(n), kThreads, 0, s>>>(x, d.alpha, d.mov, dir, trial, diff, n);
+            const auto mv = B.stats(diff, nullptr, nullptr);
+            for (int m = 0; m < M; ++m)
+                if (pending[m] && !(mv[4 * m + 2] > 0)) {
+                    pending[m] = 0;
+                    act[m] = 0;
+                    status[m] = 2;
+                    secs[m] = elapsed();
+                }
+            ++R.line_search_evaluations;
+            std::vector<double> Et = B.energies(trial, f, nullptr, LPG_HESSIAN_NONE, LPG_PRECISION_F64, nullptr);
+            for (int m = 0; m < M; ++m) {
+                take[m] = 0;
+                if (!pending[m]) continue;
+                const double noise = 16.0 * kEps * std::max(1.0, std::abs(E[m]));
+                const double armijo = o.accept_rule == 1 ? 1e-4 * alpha[m] * gd[m] : 0.0;
+                if (Et[m] <= E[m] + armijo + noise) {
+                    take[m] = 1;
+                    pending[m] = 0;
+                } else {
+                    alpha[m] *= o.line_search_shrink;
+                }
+            }
+            B.up(d.take, take);
+            seg_take<<<grid(n), kThreads, 0, s>>>(x, trial, d.take, d.mov, n);
+        }
+        for (int m = 0; m < M; ++m)
+            if (pending[m]) {
+                act[m] = 0;
+                status[m] = 2;
+                secs[m] = elapsed();
+            }
+    }
+    R.iterations = it;
+    R.seconds = elapsed();
+    int worst = 0;
+    double esum = 0;
+    for (int m = 0; m < M; ++m) {
+        per_mesh[m].status = status[m] < 0 ? 1 : status[m];
+        per_mesh[m].iterations = iters[m];
+        per_mesh[m].energy = E[m];
+        per_mesh[m].gradient_norm = o.stop_rule == 0 ? gmax[m] : g2[m];
+        per_mesh[m].gradient_norm0 = g0[m];
+        per_mesh[m].seconds = secs[m];
+        worst = std::max(worst, per_mesh[m].status);
+        esum += E[m];
+    }
+    R.status = worst;
+    R.energy = esum;
+    if (io_mem == LPG_MEM_DEVICE)
+        LPG_CUDA(cudaMemcpyAsync(x_out, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    else
+        LPG_CUDA(cudaMemcpyAsync(x_out, x, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    LPG_CUDA(cudaStreamSynchronize(s));
+    if (total) *total = R;
 }
 
 } // namespace lpg

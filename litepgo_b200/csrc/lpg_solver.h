@@ -36,6 +36,7 @@ struct lpg_fem {
         b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused;
     lpg::DeviceBuffer b_cl[10]; // assembly clusters
     lpg::DeviceBuffer b_sell[4]; // sliced-ELL pattern of the solvers
+    lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_status, d_tile_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
     // Solver state (Newton / PCG / adjoint).
@@ -44,13 +45,16 @@ struct lpg_fem {
     // CUDA graph of a chunk of PCG iterations, reused while its pointers stay the same.
     cudaGraphExec_t pcg_graph = nullptr;
     const void* pcg_graph_key[12] = {};
+    cudaGraphExec_t batch_graph = nullptr; // the batched (per-mesh) PCG iterations
+    const void* batch_graph_key[12] = {};
     ~lpg_fem();
     void sync();
     unsigned take_status();
     const double* stage_in(const double* p, int mem, lpg::DeviceBuffer& buf, size_t n);
     // Enqueues one evaluation on the handle's stream (no synchronisation).
     void eval_async(const double* du, double* dgrad, int hessian, int precision, int layout, void* dhess,
-                    double* delem, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr);
+                    double* delem, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
+                    const int* emesh = nullptr, const int* mesh_exact = nullptr);
 };
 
 namespace lpg {
@@ -58,6 +62,10 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
                   const lpg_newton_options& o, double* x_out, lpg_newton_result* res);
 void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                    int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out);
+void batch_newton_solve(lpg_fem& h, int num_meshes, const int32_t* vertex_offsets, const int32_t* element_offsets,
+                        const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
+                        const lpg_newton_options& o, double* x_out, lpg_batch_mesh_result* per_mesh,
+                        lpg_newton_result* total);
 void adjoint_rest(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                   int precision, double cg_tolerance, double* dX, double* lambda_out);
 } // namespace lpg

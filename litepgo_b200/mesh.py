@@ -117,3 +117,19 @@ def make_box(nx, ny=None, nz=None, size=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0))
     flip = det < 0
     tets[flip, 2], tets[flip, 3] = tets[flip, 3].copy(), tets[flip, 2].copy()
     return X, tets.astype(np.int32)
+
+
+def concatenate(meshes):
+    """Disjoint union of meshes [(X_m, tets_m), ...]: (X, tets, vertex_offsets,
+    element_offsets), each mesh a contiguous vertex and element range (the layout
+    solver.batch_newton_solve takes)."""
+    Xs, Ts, voff, eoff = [], [], [0], [0]
+    for X, tets in meshes:
+        X = np.asarray(X, dtype=np.float64).reshape(-1, 3)
+        tets = np.asarray(tets, dtype=np.int64)
+        Ts.append(tets + voff[-1])
+        Xs.append(X)
+        voff.append(voff[-1] + X.shape[0])
+        eoff.append(eoff[-1] + tets.shape[0])
+    return (np.concatenate(Xs), np.concatenate(Ts).astype(np.int32), np.array(voff, np.int32),
+            np.array(eoff, np.int32))

@@ -20,7 +20,8 @@ import numpy as np
 from . import _native as N
 from .energy import HessianKind, WeightedSumEnergy
 
-__all__ = ["NewtonOptions", "NewtonStatus", "NewtonResult", "newton_solve", "StaticEquilibriumResponse"]
+__all__ = ["NewtonOptions", "NewtonStatus", "NewtonResult", "newton_solve", "batch_newton_solve",
+           "StaticEquilibriumResponse"]
 
 
 class NewtonStatus(enum.IntEnum):
@@ -139,6 +140,60 @@ def newton_solve(energy, fixed, x0, options, solver=None, on_iteration=None):
                                    ctypes.byref(opts), ptrs[2], ctypes.byref(res)))
     return NewtonResult(res.status, xo, res.energy, res.gradient_norm, res.iterations, res.gradient_norm0,
                         res.cg_iterations, res.line_search_evaluations, res.seconds)
+
+
+def batch_newton_solve(energy, mesh_vertex_offsets, mesh_element_offsets, fixed, x0, options):
+    """newton_solve of many independent meshes held in one energy (no reference counterpart).
+
+    ``energy`` is one VolumetricFemEnergy (plus linear loads) over the meshes' disjoint union,
+    the meshes being contiguous vertex ranges ``mesh_vertex_offsets`` and element ranges
+    ``mesh_element_offsets`` (num_meshes + 1 entries each, see ``mesh.concatenate``). Every
+    mesh has its own stop test, PCG, feasible step and line search; the element and SpMV work
+    runs once over all of them. Returns (x, per_mesh, total): x over the union, per_mesh a list
+    of NewtonResult-like records (status, iterations, energy, gradient_norm, gradient_norm0,
+    seconds = time from the call's start to the iteration that ended the mesh), total the
+    whole call's NewtonResult.
+    """
+    fem, f = _split_energy(energy)
+    n = fem.num_dofs
+    voff = np.ascontiguousarray(mesh_vertex_offsets, dtype=np.int32)
+    eoff = np.ascontiguousarray(mesh_element_offsets, dtype=np.int32)
+    if voff.ndim != 1 or eoff.shape != voff.shape or voff.size < 2:
+        raise ValueError("batch_newton_solve: mesh offsets must be two arrays of num_meshes + 1 entries")
+    M = voff.size - 1
+    if fixed.num_dofs != n:
+        raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
+    is_dev = hasattr(x0, "is_cuda") and x0.is_cuda
+    if is_dev:
+        import torch
+
+        x0t = x0.detach().contiguous()
+        if x0t.dtype != torch.float64 or x0t.numel() != n:
+            raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
+        xo = torch.empty_like(x0t)
+        ft = None if f is None else torch.as_tensor(f, device=x0t.device)
+        N.check(N.lib.lpg_fem_set_stream(fem.handle, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        ptrs = (N.vptr(ft), N.vptr(x0t), N.vptr(xo), N.MEM_DEVICE)
+    else:
+        x0a = np.ascontiguousarray(x0, dtype=np.float64)
+        if x0a.size != n:
+            raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
+        xo = np.empty(n)
+        fa = None if f is None else np.ascontiguousarray(f)
+        N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
+        ptrs = (N.vptr(fa), N.vptr(x0a), N.vptr(xo), N.MEM_HOST)
+    fixed_arr = np.ascontiguousarray(fixed.fixed_dofs, dtype=np.int32)
+    per = (N.BatchMeshResultC * M)()
+    res = N.NewtonResultC()
+    opts = options.to_c()
+    N.check(N.lib.lpg_batch_newton_solve(fem.handle, M, N.iptr(voff), N.iptr(eoff), N.iptr(fixed_arr),
+                                         int(fixed_arr.size), ptrs[0], ptrs[1], ptrs[3], ctypes.byref(opts), ptrs[2],
+                                         per, ctypes.byref(res)))
+    meshes = [NewtonResult(p.status, None, p.energy, p.gradient_norm, p.iterations, p.gradient_norm0, 0, 0, p.seconds)
+              for p in per]
+    total = NewtonResult(res.status, xo, res.energy, res.gradient_norm, res.iterations, res.gradient_norm0,
+                         res.cg_iterations, res.line_search_evaluations, res.seconds)
+    return xo, meshes, total
 
 
 class StaticEquilibriumResponse:

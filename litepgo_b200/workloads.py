@@ -11,6 +11,10 @@ Every workload is generated from numpy.random.default_rng(seed); there is no dat
 - adjoint_box: n^3 cubes with per-element [lambda, mu] = [1.4e5, 3.4e4] (the parameters of
   an adjoint fit), bottom face fixed, gravity as above, and target parameters whose mu is
   perturbed to mu (1 + 0.2 N(0, 1)) (clipped below at 0.05 mu).
+- batch_boxes: independent boxes with cube counts per axis drawn from U{4..24} (spacing 1/16),
+  each with its own affine state A = I + 0.1 N(0, 1) (u0 = (A - I) X), uniform
+  [lambda, mu] = [1.4e5, 3.4e4], its bottom face fixed at u0 and gravity as above; returned as
+  one union (mesh.concatenate) with per-mesh offsets.
 - compressed_box: 0.6x axial compression along z plus per-vertex noise 0.05 h N(0, 1)
   (h = 1/n), resampled until every element has det F in [0.2, 3.0].
 """
@@ -19,7 +23,7 @@ import numpy as np
 
 from .mesh import make_box
 
-__all__ = ["deformed_box", "gravity_box", "adjoint_box", "compressed_box", "lame", "gravity_load", "det_F"]
+__all__ = ["deformed_box", "gravity_box", "adjoint_box", "batch_boxes", "compressed_box", "lame", "gravity_load", "det_F"]
 
 
 def lame(mu, nu):
@@ -89,6 +93,29 @@ def adjoint_box(n=32, seed=0, mu=3.4e4, lam=1.4e5, rho=1000.0):
     fixed = (3 * bottom[:, None] + np.arange(3)).ravel().astype(np.int32)
     return dict(X=X, tets=tets, theta=theta, target_theta=target, fixed=fixed, f=gravity_load(X, tets, rho),
                 u0=np.zeros(X.size), seed=seed, n=n)
+
+
+def batch_boxes(count=256, seed=0, lo=4, hi=24, mu=3.4e4, lam=1.4e5, rho=1000.0):
+    from .mesh import concatenate
+
+    rng = np.random.default_rng(seed)
+    meshes, u0, fixed, f, dims = [], [], [], [], []
+    base = 0
+    for _ in range(count):
+        nx, ny, nz = (int(v) for v in rng.integers(lo, hi + 1, 3))
+        X, tets = make_box(nx, ny, nz, size=(nx / 16, ny / 16, nz / 16))
+        A = np.eye(3) + 0.1 * rng.standard_normal((3, 3))
+        meshes.append((X, tets))
+        u0.append((X @ A.T - X).ravel())
+        bottom = np.flatnonzero(X[:, 2] == 0.0)
+        fixed.append(base * 3 + (3 * bottom[:, None] + np.arange(3)).ravel())
+        f.append(gravity_load(X, tets, rho))
+        dims.append((nx, ny, nz))
+        base += X.shape[0]
+    X, tets, voff, eoff = concatenate(meshes)
+    return dict(X=X, tets=tets, vertex_offsets=voff, element_offsets=eoff, u0=np.concatenate(u0),
+                fixed=np.concatenate(fixed).astype(np.int32), f=np.concatenate(f), theta=np.array([lam, mu]),
+                dims=dims, seed=seed)
 
 
 def compressed_box(n=128, seed=0, mu=3.4e4, lam=1.4e5):

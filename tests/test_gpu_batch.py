@@ -1,0 +1,63 @@
+"""Batched Newton (solver.batch_newton_solve): many independent meshes in one handle, each with
+its own stop test, PCG, feasible step and line search. Every mesh of a small uneven batch must
+reach the equilibrium that newton_solve finds for it alone."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from litepgo_b200 import dof, energy, fem, mesh, solver, workloads
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _opts(prec):
+    return solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", accept_rule="armijo",
+                                precision=prec, max_iterations=100, cg_tolerance=1e-2)
+
+
+def _total(X, tets, theta, f):
+    n = X.size
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta)
+    return energy.WeightedSumEnergy([(e, 1.0), (energy.QuadraticEnergy(sp.csc_matrix((n, n)), -f), 1.0)])
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+def test_batch_matches_single_mesh_solves(prec):
+    b = workloads.batch_boxes(count=6, seed=1, lo=2, hi=5)
+    X, tets, voff, eoff = b["X"], b["tets"], b["vertex_offsets"], b["element_offsets"]
+    n = X.size
+    x, per, total = solver.batch_newton_solve(_total(X, tets, b["theta"], b["f"]), voff, eoff,
+                                              dof.DofReduction(n, b["fixed"]), b["u0"], _opts(prec))
+    assert total.status == solver.NewtonStatus.Converged
+    assert all(p.status == solver.NewtonStatus.Converged for p in per)
+    assert all(0 < p.seconds <= total.seconds for p in per)
+    for m in range(len(per)):
+        v0, v1, e0, e1 = voff[m], voff[m + 1], eoff[m], eoff[m + 1]
+        Xm, tm = X[v0:v1], tets[e0:e1] - v0
+        fm = b["f"][3 * v0:3 * v1]
+        fixed_m = b["fixed"][(b["fixed"] >= 3 * v0) & (b["fixed"] < 3 * v1)] - 3 * v0
+        r = solver.newton_solve(_total(Xm, tm, b["theta"], fm), dof.DofReduction(Xm.size, fixed_m),
+                                b["u0"][3 * v0:3 * v1], _opts(prec))
+        assert r.status == solver.NewtonStatus.Converged
+        xm = x[3 * v0:3 * v1]
+        assert np.max(np.abs(xm - r.x)) <= 1e-7 * max(1.0, np.max(np.abs(r.x)))
+        assert abs(per[m].energy - r.energy) <= 1e-9 * max(1.0, abs(r.energy))
+
+
+def test_batch_device_inputs_and_offset_errors():
+    b = workloads.batch_boxes(count=3, seed=2, lo=2, hi=3)
+    X, tets, voff, eoff = b["X"], b["tets"], b["vertex_offsets"], b["element_offsets"]
+    total = _total(X, tets, b["theta"], b["f"])
+    fixed = dof.DofReduction(X.size, b["fixed"])
+    x_host, _, _ = solver.batch_newton_solve(total, voff, eoff, fixed, b["u0"], _opts("f64"))
+    x_dev, _, _ = solver.batch_newton_solve(total, voff, eoff, fixed, torch.as_tensor(b["u0"], device="cuda"),
+                                            _opts("f64"))
+    assert np.array_equal(x_dev.cpu().numpy(), x_host)
+    bad = voff.copy()
+    bad[1] -= 1  # the first mesh's last vertex now belongs to the second mesh
+    with pytest.raises(ValueError, match="outside its mesh"):
+        solver.batch_newton_solve(total, bad, eoff, fixed, b["u0"], _opts("f64"))
+    with pytest.raises(ValueError, match="offsets"):
+        solver.batch_newton_solve(total, voff[:-1], eoff[:-1], fixed, b["u0"], _opts("f64"))
