@@ -54,12 +54,11 @@ enum lpg_status {
     LPG_ELOGIC = 6
 };
 
-/* HessianKind (src/core/energy/scalar/energy.hpp:6-13) plus the analytic surrogate. */
+/* HessianKind (src/core/energy/scalar/energy.hpp:6-13); NONE = no Hessian. */
 enum lpg_hessian_kind {
     LPG_HESSIAN_NONE = 0,
     LPG_HESSIAN_EXACT = 1,
-    LPG_HESSIAN_PROJECTED = 2,          /* 12x12 eigenvalue clamp, mesh_energy.cpp:16-27 */
-    LPG_HESSIAN_PROJECTED_ANALYTIC = 3  /* clamp of the 9x9 material tangent (not in the reference) */
+    LPG_HESSIAN_PROJECTED = 2 /* 12x12 eigenvalue clamp, mesh_energy.cpp:16-27 */
 };
 
 enum lpg_precision {

@@ -13,7 +13,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_lib" / "liblpg_b200.so"
 
 LPG_OK, LPG_EINVAL, LPG_EDOMAIN, LPG_EBUSY, LPG_ENOCONV, LPG_ECUDA, LPG_ELOGIC = range(7)
-HESSIAN_NONE, HESSIAN_EXACT, HESSIAN_PROJECTED, HESSIAN_PROJECTED_ANALYTIC = range(4)
+HESSIAN_NONE, HESSIAN_EXACT, HESSIAN_PROJECTED = range(3)
 PRECISION_F64, PRECISION_MIXED = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
 LAYOUT_BSR, LAYOUT_CSC = 0, 1

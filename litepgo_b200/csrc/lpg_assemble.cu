@@ -981,7 +981,11 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
 #ifndef LPG_CLUSTER_MIN_BLOCKS_F32
 #define LPG_CLUSTER_MIN_BLOCKS_F32 6
 #endif
+#ifndef LPG_CLUSTER_UNROLL
+#define LPG_CLUSTER_UNROLL 4
+#endif
 constexpr int kClThreads = LPG_CLUSTER_THREADS;
+constexpr int kClUnroll = LPG_CLUSTER_UNROLL;
 template <typename R> struct ClMinBlocks;
 template <> struct ClMinBlocks<double> { static constexpr int value = LPG_CLUSTER_MIN_BLOCKS_F64; };
 template <> struct ClMinBlocks<float> { static constexpr int value = LPG_CLUSTER_MIN_BLOCKS_F32; };
@@ -1140,6 +1144,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
                 if (d >> 31) {
                     // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient.
                     R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
+#pragma unroll kClUnroll
                     for (int c = 0; c < cnt; ++c) {
                         const int w = en[c];
                         const int el = w >> 4, la = (w >> 2) & 3;
@@ -1182,6 +1187,7 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
                     // Off-diagonal block in the orientation of the lower vertex (a) -> higher (b):
                     //   C += vol lambda h_a h_b^T - vol p h_b h_a^T + vol mu (grad N_a . grad N_b) I.
                     R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll kClUnroll
                     for (int c = 0; c < cnt; ++c) {
                         const int w = en[c];
                         const int el = w >> 4, ra = (w >> 2) & 3, cb = w & 3;
