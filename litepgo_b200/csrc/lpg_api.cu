@@ -147,7 +147,9 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.ev_end = ev_end;
     if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {
         void* proj = d_proj.ensure(project_bytes(dm, precision));
-        launch_project(dm, precision, hessian, du, proj, a.status, stream, emesh, mesh_exact);
+        launch_project(dm, precision, hessian, du, proj, a.status, stream,
+                       d_plist.as<int>(std::max<size_t>(static_cast<size_t>(dm.T), 1)), d_pcount.as<unsigned>(1), emesh,
+                       mesh_exact);
         a.proj = proj;
     }
     launch_eval(dm, precision, hessian, a, stream);

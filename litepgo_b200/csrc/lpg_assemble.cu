@@ -850,7 +850,8 @@ template <typename R>
 __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, const double* __restrict__ u,
                                                                R* __restrict__ proj, unsigned* status,
                                                                const int* __restrict__ emesh,
-                                                               const int* __restrict__ mesh_exact) {
+                                                               const int* __restrict__ mesh_exact, int* list,
+                                                               unsigned* count) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* A = reinterpret_cast<R*>(smem_raw) + kProjStride * threadIdx.x;
     R* V = A + 45;
@@ -895,70 +896,110 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
                     }
         // Elements of a mesh marked exact keep their tangent unclamped (the Exact Hessian).
         const bool keep = emesh != nullptr && mesh_exact[emesh[e]] != 0;
-        // LDL^T positive-definiteness test in the V area (row-major 9x9 scratch).
+        // Positive semi-definiteness test: LDL^T with diagonal pivoting on a copy in the V area
+        // (row-major 9x9). Pivots above tol are eliminated; once none is left, M is semi-definite
+        // if the remaining Schur complement is below tol everywhere (tol = 64 eps max|diag M|:
+        // round-off of a singular semi-definite M, e.g. the rotation modes near rest). Such an M is
+        // its own clamp up to that round-off; any other goes to clamp_kernel.
         bool pd = true;
-        for (int j = 0; j < 9 && pd && !keep; ++j) {
-            R d = A[sym9(j, j)];
-            for (int t = 0; t < j; ++t) d -= V[9 * j + t] * V[9 * j + t] * V[9 * t + t];
-            if (!(d > R(0))) {
-                pd = false;
-                break;
+        if (!keep) {
+            R scale = 0;
+            for (int r = 0; r < 9; ++r) {
+                scale = fmax(scale, fabs(A[sym9(r, r)]));
+                for (int c = 0; c < 9; ++c) V[9 * r + c] = A[sym9(r, c)];
             }
-            V[9 * j + j] = d;
-            for (int i = j + 1; i < 9; ++i) {
-                R s = A[sym9(i, j)];
-                for (int t = 0; t < j; ++t) s -= V[9 * i + t] * V[9 * j + t] * V[9 * t + t];
-                V[9 * i + j] = s / d;
-            }
-        }
-        R* out = proj + 45 * static_cast<size_t>(e);
-        if (pd || keep) {
-            for (int t = 0; t < 45; ++t) out[t] = A[t];
-        } else {
-            for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
-            R total = 0;
-            for (int t = 0; t < 45; ++t) total += A[t] * A[t];
-            for (int sweep = 0; sweep < 20; ++sweep) {
-                R off = 0;
-                for (int r = 0; r < 9; ++r)
-                    for (int c = r + 1; c < 9; ++c) off += A[sym9(r, c)] * A[sym9(r, c)];
-                if (!(off > R(16) * Eps<R>::v * Eps<R>::v * total)) break;
-                for (int pp = 0; pp < 8; ++pp)
-                    for (int qq = pp + 1; qq < 9; ++qq) {
-                        const R apq = A[sym9(pp, qq)];
-                        if (apq == R(0)) continue;
-                        const R app = A[sym9(pp, pp)], aqq = A[sym9(qq, qq)];
-                        const R tau = (aqq - app) / (R(2) * apq);
-                        const R t = (tau >= R(0) ? R(1) : R(-1)) / (fabs(tau) + sqrt(R(1) + tau * tau));
-                        const R c = R(1) / sqrt(R(1) + t * t), sn = t * c;
-                        for (int kx = 0; kx < 9; ++kx) {
-                            if (kx == pp || kx == qq) continue;
-                            const R akp = A[sym9(kx, pp)], akq = A[sym9(kx, qq)];
-                            A[sym9(kx, pp)] = c * akp - sn * akq;
-                            A[sym9(kx, qq)] = sn * akp + c * akq;
-                        }
-                        A[sym9(pp, pp)] = app - t * apq;
-                        A[sym9(qq, qq)] = aqq + t * apq;
-                        A[sym9(pp, qq)] = R(0);
-                        for (int kx = 0; kx < 9; ++kx) {
-                            const R vkp = V[9 * kx + pp], vkq = V[9 * kx + qq];
-                            V[9 * kx + pp] = c * vkp - sn * vkq;
-                            V[9 * kx + qq] = sn * vkp + c * vkq;
-                        }
-                    }
-            }
-            R lam9[9];
-            for (int t = 0; t < 9; ++t) lam9[t] = fmax(A[sym9(t, t)], R(0));
-            for (int r = 0; r < 9; ++r)
-                for (int c = r; c < 9; ++c) {
-                    R s = 0;
-                    for (int t = 0; t < 9; ++t) s += V[9 * r + t] * lam9[t] * V[9 * c + t];
-                    out[sym9(r, c)] = s;
+            const R tol = R(64) * Eps<R>::v * scale;
+            unsigned left = 0x1ffu;
+            for (int k = 0; k < 9 && pd; ++k) {
+                int piv = -1;
+                R best = tol;
+                for (int i = 0; i < 9; ++i)
+                    if (((left >> i) & 1u) && V[9 * i + i] > best) best = V[9 * i + i], piv = i;
+                if (piv < 0) {
+                    for (int i = 0; i < 9 && pd; ++i)
+                        for (int j = 0; j < 9; ++j)
+                            if (((left >> i) & (left >> j) & 1u) && !(fabs(V[9 * i + j]) <= tol)) {
+                                pd = false;
+                                break;
+                            }
+                    break;
                 }
+                left &= ~(1u << piv);
+                const R inv = R(1) / best;
+                for (int i = 0; i < 9; ++i) {
+                    if (!((left >> i) & 1u)) continue;
+                    const R li = V[9 * i + piv] * inv;
+                    for (int j = 0; j < 9; ++j)
+                        if ((left >> j) & 1u) V[9 * i + j] -= li * V[9 * piv + j];
+                }
+            }
+            if (!(scale < R(INFINITY))) pd = false;
         }
+        // Semi-definite (or kept exact): final. Otherwise the unclamped tangent is stored and
+        // the element is listed for clamp_kernel, which runs the eigenvalue clamp on the listed
+        // elements only (a warp of pass 1 then never waits on another lane's Jacobi sweeps).
+        R* out = proj + 45 * static_cast<size_t>(e);
+        for (int t = 0; t < 45; ++t) out[t] = A[t];
+        if (!pd && !keep) list[atomicAdd(count, 1u)] = e;
     }
     st = __reduce_or_sync(0xffffffffu, st);
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// Eigenvalue clamp of the listed elements' 9x9 tangents (cyclic Jacobi, Golub & Van Loan 8.5.3):
+// M = V max(Lambda, 0) V^T, in place; grid-stride over the list whose length pass 1 counted.
+template <typename R>
+__global__ void __launch_bounds__(kProjThreads) clamp_kernel(R* __restrict__ proj, const int* __restrict__ list,
+                                                             const unsigned* __restrict__ count) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* A = reinterpret_cast<R*>(smem_raw) + kProjStride * threadIdx.x;
+    R* V = A + 45;
+    const unsigned n = *count;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        R* out = proj + 45 * static_cast<size_t>(list[i]);
+        for (int t = 0; t < 45; ++t) A[t] = out[t];
+        for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
+        R total = 0;
+        for (int t = 0; t < 45; ++t) total += A[t] * A[t];
+        for (int sweep = 0; sweep < 20; ++sweep) {
+            R off = 0;
+            for (int r = 0; r < 9; ++r)
+                for (int c = r + 1; c < 9; ++c) off += A[sym9(r, c)] * A[sym9(r, c)];
+            if (!(off > R(16) * Eps<R>::v * Eps<R>::v * total)) break;
+            for (int pp = 0; pp < 8; ++pp)
+                for (int qq = pp + 1; qq < 9; ++qq) {
+                    const R apq = A[sym9(pp, qq)];
+                    if (apq == R(0)) continue;
+                    const R app = A[sym9(pp, pp)], aqq = A[sym9(qq, qq)];
+                    const R tau = (aqq - app) / (R(2) * apq);
+                    const R t = (tau >= R(0) ? R(1) : R(-1)) / (fabs(tau) + sqrt(R(1) + tau * tau));
+                    const R c = R(1) / sqrt(R(1) + t * t), sn = t * c;
+                    for (int kx = 0; kx < 9; ++kx) {
+                        if (kx == pp || kx == qq) continue;
+                        const R akp = A[sym9(kx, pp)], akq = A[sym9(kx, qq)];
+                        A[sym9(kx, pp)] = c * akp - sn * akq;
+                        A[sym9(kx, qq)] = sn * akp + c * akq;
+                    }
+                    A[sym9(pp, pp)] = app - t * apq;
+                    A[sym9(qq, qq)] = aqq + t * apq;
+                    A[sym9(pp, qq)] = R(0);
+                    for (int kx = 0; kx < 9; ++kx) {
+                        const R vkp = V[9 * kx + pp], vkq = V[9 * kx + qq];
+                        V[9 * kx + pp] = c * vkp - sn * vkq;
+                        V[9 * kx + qq] = sn * vkp + c * vkq;
+                    }
+                }
+        }
+        R lam9[9];
+        for (int t = 0; t < 9; ++t) lam9[t] = fmax(A[sym9(t, t)], R(0));
+        for (int r = 0; r < 9; ++r)
+            for (int c = r; c < 9; ++c) {
+                R s = 0;
+                for (int t = 0; t < 9; ++t) s += V[9 * r + t] * lam9[t] * V[9 * c + t];
+                out[sym9(r, c)] = s;
+            }
+
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1446,26 +1487,36 @@ size_t project_bytes(const DevMesh& m, int precision) {
     return static_cast<size_t>(m.T) * 45 * (precision == LPG_PRECISION_F64 ? sizeof(double) : sizeof(float));
 }
 
-void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
-                    cudaStream_t s, const int* emesh, const int* mesh_exact) {
-    if (hessian != LPG_HESSIAN_PROJECTED) fail(LPG_EINVAL, "projected Hessian kind not available");
-    const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
-    if (blocks == 0) return;
-    if (precision == LPG_PRECISION_F64) {
-        const size_t sm = sizeof(double) * kProjStride * kProjThreads;
-        static bool configured = false;
-        if (!configured) {
-            LPG_CUDA(cudaFuncSetAttribute(project_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(sm)));
-            configured = true;
-        }
-        project_kernel<double><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<double*>(proj), status, emesh,
-                                                                mesh_exact);
-    } else {
-        const size_t sm = sizeof(float) * kProjStride * kProjThreads;
-        project_kernel<float><<<blocks, kProjThreads, sm, s>>>(m, u, static_cast<float*>(proj), status, emesh,
-                                                               mesh_exact);
+namespace {
+template <typename R>
+void launch_project_t(const DevMesh& m, const double* u, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
+                      const int* mesh_exact, int* list, unsigned* count) {
+    const size_t sm = sizeof(R) * kProjStride * kProjThreads;
+    thread_local int clamp_grid = 0;
+    if (clamp_grid == 0) {
+        LPG_CUDA(cudaFuncSetAttribute(project_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        LPG_CUDA(cudaFuncSetAttribute(clamp_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        int dev = 0, sms = 0, per = 0;
+        LPG_CUDA(cudaGetDevice(&dev));
+        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, clamp_kernel<R>, kProjThreads, sm));
+        clamp_grid = std::max(1, per) * std::max(1, sms);
     }
+    const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
+    LPG_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
+    project_kernel<R><<<blocks, kProjThreads, sm, s>>>(m, u, proj, status, emesh, mesh_exact, list, count);
+    clamp_kernel<R><<<std::min(clamp_grid, blocks), kProjThreads, sm, s>>>(proj, list, count);
+}
+} // namespace
+
+void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
+                    cudaStream_t s, int* list, unsigned* count, const int* emesh, const int* mesh_exact) {
+    if (hessian != LPG_HESSIAN_PROJECTED) fail(LPG_EINVAL, "projected Hessian kind not available");
+    if (m.T == 0) return;
+    if (precision == LPG_PRECISION_F64)
+        launch_project_t<double>(m, u, static_cast<double*>(proj), status, s, emesh, mesh_exact, list, count);
+    else
+        launch_project_t<float>(m, u, static_cast<float*>(proj), status, s, emesh, mesh_exact, list, count);
     LPG_CUDA(cudaGetLastError());
 }
 

@@ -146,10 +146,11 @@ struct EvalArgs {
 };
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s);
 // Per-element clamped tangents for the projected Hessians (45 values / element, upper triangle).
-// With emesh (element -> mesh) and mesh_exact (per mesh), the elements of the meshes marked
-// exact keep their tangent unclamped.
+// list (T ints) and count (1) are scratch: the elements whose tangent needs the eigenvalue
+// clamp. With emesh (element -> mesh) and mesh_exact (per mesh), the elements of the meshes
+// marked exact keep their tangent unclamped.
 void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
-                    cudaStream_t s, const int* emesh = nullptr,
+                    cudaStream_t s, int* list, unsigned* count, const int* emesh = nullptr,
                     const int* mesh_exact = nullptr);
 size_t project_bytes(const DevMesh& m, int precision);
 // per_elem (T doubles, optional) receives each element's step.

@@ -628,7 +628,7 @@ struct Solver {
     template <typename R>
     void enqueue_iterations(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA,
                             R* pB, R* Ap, PcgState* st, double* part, int pairs) {
-        const int sg = spmv_grid(spmv_sell<R, R, R, true, false, 4>), ug = vec_grid(pcg_update<R>);
+        const int sg = spmv_grid(spmv_sell<R, R, R, true, false, 4>), ug = std::max(1, grid(static_cast<size_t>(V)));
         for (int i = 0; i < pairs; ++i) {
             spmv_sell<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
             pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pB, Ap, V, part);
@@ -658,7 +658,7 @@ struct Solver {
         double* r64 = h.s_r64.as<double>(n);
         double* y64 = h.s_b64.as<double>(n);
         const int vg = vec_grid(pcg_init<R>);
-        const int pg = std::max(spmv_grid(spmv_sell<R, R, R, true, false, 4>), vec_grid(pcg_update<R>));
+        const int pg = std::max(spmv_grid(spmv_sell<R, R, R, true, false, 4>), std::max(1, grid(static_cast<size_t>(V))));
         double* part = h.s_part.as<double>(std::max(4 * 1024, 2 * std::max(pg, vg)));
         PcgState* st = reinterpret_cast<PcgState*>(h.s_scal.as<double>(64));
         LPG_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), s));
