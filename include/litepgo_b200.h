@@ -104,7 +104,10 @@ int lpg_mesh_plan_summary(int num_vertices, int num_tets, const int32_t* tets, i
  * evaluations per pass (sum over clusters), out[4] block contributor entries (16 per tet).
  * The plan's invariants are checked (LPG_ELOGIC if one fails): every referenced vertex is
  * owned by one cluster, every element's energy is counted once, and every block of every
- * owned row lists exactly the elements that share its two vertices, in ascending order.
+ * owned row lists exactly the elements that share its two vertices, in ascending order. The
+ * solvers' upper-triangle sliced-ELL layout (lpg_fem_solver_layout) is checked too: every row
+ * once, its blocks with column >= row stored (diagonal first), and every block left of the
+ * diagonal referencing the stored block of its transpose.
  */
 int lpg_mesh_cluster_summary(int num_vertices, int num_tets, const int32_t* tets, int64_t out[5]);
 
@@ -163,21 +166,24 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
  * mean duration of the assembly kernel alone (ms_assemble) and of one whole evaluation
  * including projection and the energy reduction (ms_eval). With flush_l2 != 0 a 512 MB
  * buffer is written before each launch, outside the measured intervals. Besides
- * LPG_LAYOUT_BSR and LPG_LAYOUT_CSC, layout 2 selects the solvers' sliced-ELL layout of
- * lpg_fem_solver_layout (hess then holds 9 * num_slots values; padding entries are not
- * written).
+ * LPG_LAYOUT_BSR and LPG_LAYOUT_CSC, layout 2 selects the solvers' upper-triangle sliced-ELL
+ * layout of lpg_fem_solver_layout (hess then holds 9 * num_slots values; padding entries are
+ * not written).
  */
 int lpg_fem_time_eval(lpg_fem_t h, const double* u, double* grad, int hessian, int precision, int layout, void* hess,
                       int launches, int flush_l2, double* ms_assemble, double* ms_eval);
 
 /*
  * The block layout the Newton and adjoint solvers keep the Hessian in (no reference
- * counterpart): sliced ELL with chunks of 32 rows, rows sorted by block count (descending,
- * stable) within windows of 128 rows. Chunk c holds rows sell_row[32 c + l] (l = 0..31, -1
- * past the last row) and slots [sell_ptr[c], sell_ptr[c + 1]), 32 per block column of its
- * longest row; block q of the row in lane l is slot sell_ptr[c] + 32 q + l, and entry t
- * (row-major) of that block is value 9 sell_ptr[c] + 32 (9 q + t) + l. Any output may be NULL;
- * sell_ptr has num_chunks + 1 entries, sell_row 32 * num_chunks.
+ * counterpart): the upper triangle of the symmetric block matrix (the blocks of row v with
+ * column >= v, the diagonal first) in sliced ELL with chunks of 32 rows, rows sorted by their
+ * BSR block count (descending, stable) within windows of 128 rows. Chunk c holds rows
+ * sell_row[32 c + l] (l = 0..31, -1 past the last row) and slots [sell_ptr[c], sell_ptr[c + 1]),
+ * 32 per stored block of its row with the most; stored block q of the row in lane l is slot
+ * sell_ptr[c] + 32 q + l, and entry t (row-major) of that block is value
+ * 9 sell_ptr[c] + 32 (9 q + t) + l. Blocks left of the diagonal are not stored (the solvers
+ * read them as transposes). Any output may be NULL; sell_ptr has num_chunks + 1 entries,
+ * sell_row 32 * num_chunks.
  */
 int lpg_fem_solver_layout(lpg_fem_t h, int64_t* num_slots, int* num_chunks, int32_t* sell_ptr, int32_t* sell_row);
 

@@ -203,6 +203,7 @@ int lpg_mesh_cluster_summary(int V, int T, const int32_t* tets, int64_t out[5]) 
         HostPlan p;
         build_plan(V, T, tets, p);
         check_clusters(p, tets);
+        check_solver_layout(p);
         const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
         int64_t max_rows = 0, max_els = 0;
         for (int c = 0; c < ncl; ++c) {
@@ -307,6 +308,8 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         m.sell_row = upload(h->b_sell[1], p.sell_row);
         m.sell_col = upload(h->b_sell[2], p.sell_col);
         m.sell_base = upload(h->b_sell[3], p.sell_base);
+        m.sell_bptr = upload(h->b_sell[4], p.sell_bptr);
+        m.sell_bref = reinterpret_cast<int2*>(upload(h->b_sell[5], p.sell_bref));
         m.n_sell = static_cast<int>(p.sell_ptr.size()) - 1;
         m.ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
         m.cl_row_ptr = upload(h->b_cl[0], p.cl_row_ptr);
@@ -319,6 +322,7 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         m.cl_slot_ent = upload(h->b_cl[7], p.cl_slot_ent);
         m.cl_ent_ptr = upload(h->b_cl[8], p.cl_ent_ptr);
         m.cl_ents = upload(h->b_cl[9], p.cl_ents);
+        m.cl_ntr = upload(h->b_cl[10], p.cl_ntr);
         m.cl_max_slots = m.cl_max_ents = 0;
         for (int c = 0; c < m.ncl; ++c) {
             m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);

@@ -227,7 +227,7 @@ struct TileMeta {
     int nb[32];
     int dq[32];   // position of the diagonal block within the row
     int ppre[33]; // the pairs of row j are [ppre[j], ppre[j + 1])
-    int sb[32];   // the row's sliced-ELL base (solver layout)
+    int sb[32];   // the row's sliced-ELL base less 288 x its diagonal position (solver layout)
 };
 
 // Position of entry t (row-major) of block q of tile row j in the output layout.
@@ -238,7 +238,7 @@ __device__ __forceinline__ size_t out_pos(int layout, const TileMeta* meta, int 
         const int i = t / 3, c = t - 3 * (t / 3);
         return 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * q + c;
     }
-    return static_cast<size_t>(meta->sb[j]) + 32 * static_cast<size_t>(9 * q + t);
+    return static_cast<size_t>(static_cast<int64_t>(meta->sb[j]) + 32 * static_cast<int64_t>(9 * q + t));
 }
 
 // Shared memory of one warp: off-diagonal blocks [9][3 cap + 1], slot descriptors [3 cap], metadata.
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
             meta->slot0[lane] = sb;
             meta->nb[lane] = m.row_ptr[r + 1] - sb;
             meta->dq[lane] = m.diag_slot[r] - sb;
-            if (a.layout == kLayoutSell) meta->sb[lane] = m.sell_base[r];
+            if (a.layout == kLayoutSell) meta->sb[lane] = m.sell_base[r] - 288 * (m.diag_slot[r] - sb);
             deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
         }
         int incl = deg;
@@ -512,7 +512,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) asse
                 R val = 0;
                 for (int c = c0; c < c1; ++c) val = X::add(val, col[c]);
                 if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                hout[out_pos(a.layout, meta, j, qs, kk)] = static_cast<HT>(val);
+                // The solver layout keeps the blocks right of the diagonal only.
+                if (a.layout != kLayoutSell || qs > meta->dq[j]) hout[out_pos(a.layout, meta, j, qs, kk)] = static_cast<HT>(val);
             }
         }
     #pragma unroll
@@ -946,59 +947,174 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
-// Eigenvalue clamp of the listed elements' 9x9 tangents (cyclic Jacobi, Golub & Van Loan 8.5.3):
+// One round of parallel-ordered Jacobi on a symmetric 9x9 (round-robin ordering: in round r
+// index r idles and the pairs (r+i, r-i) mod 9, i = 1..4, are disjoint, so a sweep of 9 rounds
+// meets each of the 36 pairs once; Golub & Van Loan 8.5.3 and 8.6 for the ordering). The four
+// rotations (Alg. 8.4.1 sym.schur2) are computed from the same A, i.e. four independent
+// dependency chains, and applied together as A <- J^T A J with J the block rotation, then
+// accumulated into V's columns.
+// A is kept relabelled by the round, A_cur(i, j) = A((i + r) mod 9, (j + r) mod 9), so every
+// round rotates the fixed pairs (1, 8), (2, 7), (3, 6), (4, 5) of A_cur with literal register
+// indices; after the round A_cur is shifted by one label. The loop over rounds therefore stays
+// a loop (a fully unrolled sweep of nine rounds overflows the instruction cache). V (register
+// array, VREG) is shifted with A; V in shared memory is addressed with the round's offset.
+template <typename R, bool VREG, typename VA>
+__device__ __forceinline__ void jacobi_round(R (&A)[45], VA& V, const int rd) {
+    R c[4], sn[4], t[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int P = k + 1, Q = 8 - k;
+        // t = sign(tau) / (|tau| + sqrt(1 + tau^2)), tau = d / a2, written with one square
+        // root and one division: t = +-|a2| / (|d| + sqrt(d^2 + a2^2)) (A is scaled to
+        // max |entry| <= 1, so the squares cannot overflow); c = 1 / sqrt(1 + t^2), s = t c.
+        const R apq = A[sym9(P, Q)];
+        const R d = A[sym9(Q, Q)] - A[sym9(P, P)], a2 = R(2) * apq;
+        const R num = d > R(0) ? a2 : (d < R(0) ? -a2 : fabs(a2));
+        const R tk = num / (fabs(d) + sqrt(d * d + a2 * a2));
+        t[k] = apq == R(0) ? R(0) : tk;
+        c[k] = rsqrt(R(1) + t[k] * t[k]);
+        sn[k] = t[k] * c[k];
+    }
+    // Off-diagonal 2x2 blocks between pairs k < l: R_k^T A_kl R_l, R = [[c, s], [-s, c]].
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int l = k + 1; l < 4; ++l) {
+            const int Pk = k + 1, Qk = 8 - k, Pl = l + 1, Ql = 8 - l;
+            const R a = A[sym9(Pk, Pl)], b = A[sym9(Pk, Ql)];
+            const R d = A[sym9(Qk, Pl)], e = A[sym9(Qk, Ql)];
+            const R a1 = c[l] * a - sn[l] * b, b1 = sn[l] * a + c[l] * b;
+            const R d1 = c[l] * d - sn[l] * e, e1 = sn[l] * d + c[l] * e;
+            A[sym9(Pk, Pl)] = c[k] * a1 - sn[k] * d1;
+            A[sym9(Pk, Ql)] = c[k] * b1 - sn[k] * e1;
+            A[sym9(Qk, Pl)] = sn[k] * a1 + c[k] * d1;
+            A[sym9(Qk, Ql)] = sn[k] * b1 + c[k] * e1;
+        }
+    // The idle index 0 against each pair, then each pair's own 2x2 block, then V.
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int P = k + 1, Q = 8 - k;
+        const R a = A[sym9(0, P)], b = A[sym9(0, Q)];
+        A[sym9(0, P)] = c[k] * a - sn[k] * b;
+        A[sym9(0, Q)] = sn[k] * a + c[k] * b;
+        const R apq = A[sym9(P, Q)];
+        A[sym9(P, P)] -= t[k] * apq;
+        A[sym9(Q, Q)] += t[k] * apq;
+        A[sym9(P, Q)] = R(0);
+        int vp_col = P, vq_col = Q;
+        if constexpr (!VREG) {
+            vp_col = P + rd >= 9 ? P + rd - 9 : P + rd;
+            vq_col = Q + rd >= 9 ? Q + rd - 9 : Q + rd;
+        }
+#pragma unroll
+        for (int x = 0; x < 9; ++x) {
+            const R vp = V[9 * x + vp_col], vq = V[9 * x + vq_col];
+            V[9 * x + vp_col] = c[k] * vp - sn[k] * vq;
+            V[9 * x + vq_col] = sn[k] * vp + c[k] * vq;
+        }
+    }
+    // Relabel for the next round: A_next(i, j) = A_cur(i + 1, j + 1) (indices mod 9).
+    R B[45];
+#pragma unroll
+    for (int u = 0; u < 45; ++u) B[u] = A[u];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int j = i; j < 9; ++j) A[sym9(i, j)] = B[sym9((i + 1) % 9, (j + 1) % 9)];
+    if constexpr (VREG) {
+#pragma unroll
+        for (int x = 0; x < 9; ++x) {
+            const R v0 = V[9 * x];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) V[9 * x + j] = V[9 * x + j + 1];
+            V[9 * x + 8] = v0;
+        }
+    }
+}
+
+// Eigenvalue clamp of the listed elements' 9x9 tangents (parallel-ordered cyclic Jacobi):
 // M = V max(Lambda, 0) V^T, in place; grid-stride over the list whose length pass 1 counted.
+// One thread per element with the packed matrix and the rotations in registers; in FP64 the
+// eigenvectors V live in shared memory (81 doubles per thread, an odd stride: conflict-free),
+// since A and V together would exceed the register file.
+template <typename R, bool VREG, typename VA>
+__device__ __forceinline__ void clamp9(R* __restrict__ out, VA& V) {
+    R A[45];
+    R amax = 0;
+#pragma unroll
+    for (int t = 0; t < 45; ++t) {
+        A[t] = out[t];
+        amax = fmax(amax, fabs(A[t]));
+    }
+    // Exact power-of-two scaling to max |entry| in [0.5, 1): no overflow in the rotations.
+    int ex = 0;
+    if (amax > R(0) && amax < R(INFINITY)) frexp(amax, &ex);
+    const R down = ldexp(R(1), -ex), up = ldexp(R(1), ex);
+    R total = 0;
+#pragma unroll
+    for (int t = 0; t < 45; ++t) {
+        A[t] *= down;
+        total += A[t] * A[t];
+    }
+#pragma unroll
+    for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
+    const R thr = R(16) * Eps<R>::v * Eps<R>::v * total;
+#pragma unroll 1
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        R off = 0;
+#pragma unroll
+        for (int r = 0; r < 9; ++r)
+#pragma unroll
+            for (int c = r + 1; c < 9; ++c) off += A[sym9(r, c)] * A[sym9(r, c)];
+        if (!(off > thr)) break;
+#pragma unroll 1
+        for (int rd = 0; rd < 9; ++rd) jacobi_round<R, VREG>(A, V, rd);
+    }
+    R lam[9];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) lam[t] = fmax(A[sym9(t, t)], R(0)) * up;
+#pragma unroll
+    for (int k = 0; k < 45; ++k) A[k] = R(0);
+    // M+ = sum_t lam_t v_t v_t^T, one eigenvector column at a time (A reused as the sum).
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+        R col[9];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) col[r] = V[9 * r + t];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            const R lr = lam[t] * col[r];
+#pragma unroll
+            for (int c = r; c < 9; ++c) A[sym9(r, c)] += lr * col[c];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 45; ++k) out[k] = A[k];
+}
+
+constexpr int kClampVStride = 81;
+// Resident 64-thread blocks per SM the FP32 clamp's register allocation must allow (6: at most
+// 170 registers, a few of them spilled; A, V and the relabelling copy need about 187).
+#ifndef LPG_CLAMP_MIN_BLOCKS_F32
+#define LPG_CLAMP_MIN_BLOCKS_F32 6
+#endif
+
 template <typename R>
-__global__ void __launch_bounds__(kProjThreads) clamp_kernel(R* __restrict__ proj, const int* __restrict__ list,
+__global__ void __launch_bounds__(kProjThreads, sizeof(R) == 4 ? LPG_CLAMP_MIN_BLOCKS_F32 : 1) clamp_kernel(R* __restrict__ proj, const int* __restrict__ list,
                                                              const unsigned* __restrict__ count) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* A = reinterpret_cast<R*>(smem_raw) + kProjStride * threadIdx.x;
-    R* V = A + 45;
     const unsigned n = *count;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         R* out = proj + 45 * static_cast<size_t>(list[i]);
-        for (int t = 0; t < 45; ++t) A[t] = out[t];
-        for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
-        R total = 0;
-        for (int t = 0; t < 45; ++t) total += A[t] * A[t];
-        for (int sweep = 0; sweep < 20; ++sweep) {
-            R off = 0;
-            for (int r = 0; r < 9; ++r)
-                for (int c = r + 1; c < 9; ++c) off += A[sym9(r, c)] * A[sym9(r, c)];
-            if (!(off > R(16) * Eps<R>::v * Eps<R>::v * total)) break;
-            for (int pp = 0; pp < 8; ++pp)
-                for (int qq = pp + 1; qq < 9; ++qq) {
-                    const R apq = A[sym9(pp, qq)];
-                    if (apq == R(0)) continue;
-                    const R app = A[sym9(pp, pp)], aqq = A[sym9(qq, qq)];
-                    const R tau = (aqq - app) / (R(2) * apq);
-                    const R t = (tau >= R(0) ? R(1) : R(-1)) / (fabs(tau) + sqrt(R(1) + tau * tau));
-                    const R c = R(1) / sqrt(R(1) + t * t), sn = t * c;
-                    for (int kx = 0; kx < 9; ++kx) {
-                        if (kx == pp || kx == qq) continue;
-                        const R akp = A[sym9(kx, pp)], akq = A[sym9(kx, qq)];
-                        A[sym9(kx, pp)] = c * akp - sn * akq;
-                        A[sym9(kx, qq)] = sn * akp + c * akq;
-                    }
-                    A[sym9(pp, pp)] = app - t * apq;
-                    A[sym9(qq, qq)] = aqq + t * apq;
-                    A[sym9(pp, qq)] = R(0);
-                    for (int kx = 0; kx < 9; ++kx) {
-                        const R vkp = V[9 * kx + pp], vkq = V[9 * kx + qq];
-                        V[9 * kx + pp] = c * vkp - sn * vkq;
-                        V[9 * kx + qq] = sn * vkp + c * vkq;
-                    }
-                }
+        if constexpr (sizeof(R) == 8) {
+            extern __shared__ __align__(16) unsigned char smem_raw[];
+            // volatile: every access goes to shared memory (cached copies would need the
+            // registers this layout is there to save).
+            volatile R* V = reinterpret_cast<R*>(smem_raw) + kClampVStride * threadIdx.x;
+            clamp9<R, false>(out, V);
+        } else {
+            R V[81];
+            clamp9<R, true>(out, V);
         }
-        R lam9[9];
-        for (int t = 0; t < 9; ++t) lam9[t] = fmax(A[sym9(t, t)], R(0));
-        for (int r = 0; r < 9; ++r)
-            for (int c = r; c < 9; ++c) {
-                R s = 0;
-                for (int t = 0; t < 9; ++t) s += V[9 * r + t] * lam9[t] * V[9 * c + t];
-                out[sym9(r, c)] = s;
-            }
-
     }
 }
 
@@ -1054,7 +1170,7 @@ __device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, 
         const int i = t / 3, c = t - 3 * (t / 3);
         return 9 * static_cast<size_t>(slot0) + static_cast<size_t>(i) * 3 * nb + 3 * q + c;
     }
-    return static_cast<size_t>(sb) + 32 * static_cast<size_t>(9 * q + t);
+    return static_cast<size_t>(static_cast<int64_t>(sb) + 32 * static_cast<int64_t>(9 * q + t));
 }
 
 template <typename R, bool WG, bool WH>
@@ -1159,7 +1275,8 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
             rt[j] = v;
             rt[kClusterRows + j] = sb;
             rt[2 * kClusterRows + j] = __ldg(m.row_ptr + v + 1) - sb;
-            if (a.layout == kLayoutSell) rt[3 * kClusterRows + j] = __ldg(m.sell_base + v);
+            // Solver layout: own block q - (diagonal position) of the row, so the base is shifted.
+            if (a.layout == kLayoutSell) rt[3 * kClusterRows + j] = __ldg(m.sell_base + v) - 288 * (__ldg(m.diag_slot + v) - sb);
         }
         prefetch(cl + gridDim.x);
         if (WG || WH) __pipeline_wait_prior(0);
@@ -1175,7 +1292,9 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
         if (WG || WH) {
             const int noff = __ldg(m.cl_noff + cl);
             HT* hout = reinterpret_cast<HT*>(a.hess);
-            for (int s = (WH ? 0 : noff) + tid; s < ns; s += bd) {
+            // The solver layout skips the slots left of the diagonal (the transposes it does not store).
+            const int first = WH ? (a.layout == kLayoutSell ? __ldg(m.cl_ntr + cl) : 0) : noff;
+            for (int s = first + tid; s < ns; s += bd) {
                 const uint32_t d = sslot[s], de = sslote[s];
                 const int j = d & 0xffu, q = (d >> 8) & 0x3fffffu;
                 const uint16_t* en = sent + (de & 0xfffffu);
@@ -1492,20 +1611,23 @@ template <typename R>
 void launch_project_t(const DevMesh& m, const double* u, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
                       const int* mesh_exact, int* list, unsigned* count) {
     const size_t sm = sizeof(R) * kProjStride * kProjThreads;
+    const size_t clamp_sm = sizeof(R) == 8 ? sizeof(R) * kClampVStride * kProjThreads : 0;
     thread_local int clamp_grid = 0;
     if (clamp_grid == 0) {
         LPG_CUDA(cudaFuncSetAttribute(project_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-        LPG_CUDA(cudaFuncSetAttribute(clamp_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
         int dev = 0, sms = 0, per = 0;
         LPG_CUDA(cudaGetDevice(&dev));
         LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, clamp_kernel<R>, kProjThreads, sm));
+        if (clamp_sm > 0)
+            LPG_CUDA(cudaFuncSetAttribute(clamp_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(clamp_sm)));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, clamp_kernel<R>, kProjThreads, clamp_sm));
         clamp_grid = std::max(1, per) * std::max(1, sms);
     }
     const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
     LPG_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
     project_kernel<R><<<blocks, kProjThreads, sm, s>>>(m, u, proj, status, emesh, mesh_exact, list, count);
-    clamp_kernel<R><<<std::min(clamp_grid, blocks), kProjThreads, sm, s>>>(proj, list, count);
+    clamp_kernel<R><<<std::min(clamp_grid, blocks), kProjThreads, clamp_sm, s>>>(proj, list, count);
 }
 } // namespace
 

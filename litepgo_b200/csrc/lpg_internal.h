@@ -55,17 +55,25 @@ struct HostPlan {
     std::vector<int32_t> diag_slot;          // V: block index of (v, v), -1 for an unused vertex
     std::vector<int32_t> unused_rows;        // vertices referenced by no element (not in any tile)
     std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
-    // Sliced-ELL copy of the pattern for the solvers (SELL-32 with rows sorted by block count
-    // within windows of kSellWindow rows): chunk c holds 32 rows (sell_row, -1 past the end)
-    // and sell_ptr[c + 1] - sell_ptr[c] = 32 x (its longest row) block slots; block slot q of
-    // the row in lane l is slot sell_ptr[c] + 32 q + l, its column sell_col (the row itself
-    // for a padding slot), and entry t of its 3x3 block is value 9 sell_ptr[c] + (9 q + t) 32 + l,
-    // i.e. sell_base[row] + 32 (9 q + t).
+    // Upper-triangle sliced ELL of the solvers (SELL-32 with rows sorted by block count within
+    // windows of kSellWindow rows). The matrix is symmetric, so each row stores only its blocks
+    // with column >= row ("own" blocks, the diagonal first) and reads its blocks left of the
+    // diagonal as the transposes of the owning rows' blocks ("borrowed" blocks).
+    //   Own: chunk c holds 32 rows (sell_row, -1 past the end) and sell_ptr[c + 1] - sell_ptr[c]
+    //   = 32 x (its most own blocks) slots; own block q of the row in lane l is slot
+    //   sell_ptr[c] + 32 q + l, its column sell_col (the row itself for padding), and entry t of
+    //   the 3x3 block is value 9 sell_ptr[c] + (9 q + t) 32 + l = sell_base[row] + 32 (9 q + t).
+    //   Borrowed: slots [sell_bptr[c], sell_bptr[c + 1]), 32 per borrowed block of the chunk's
+    //   longest such list; slot sell_bptr[c] + 32 q + l holds {value index of entry 0 of the
+    //   owning row's block, its column}; entry t is at that index + 32 t. Padding points at a
+    //   zero block stored after the own slots (sell_zero()).
     std::vector<int32_t> sell_ptr, sell_row, sell_col, sell_base;
+    std::vector<int32_t> sell_bptr, sell_bref;
     // Vertex clusters of the element-once assembly (one thread block per cluster): the rows a
     // cluster owns, the elements incident to them (ascending; bit 31 set on the elements whose
-    // energy the cluster counts, those whose first vertex it owns), and its block slots,
-    // off-diagonal first, then diagonal. Slot word: bits 0-7 the row within the cluster, bits
+    // energy the cluster counts, those whose first vertex it owns), and its block slots:
+    // off-diagonal slots left of the diagonal (cl_ntr of them), off-diagonal slots right of
+    // it, then the diagonal slots (cl_noff off-diagonal in all). Slot word: bits 0-7 the row within the cluster, bits
     // 8-29 the slot's position within its row, bit 30 "store the transpose", bit 31 diagonal.
     // Entry word of a slot: bits 0-19 first contributor (within the cluster), 20-31 count.
     // Contributors (uint16): element within the cluster << 4 | a << 2 | b, where (a, b) are
@@ -73,11 +81,14 @@ struct HostPlan {
     std::vector<int32_t> cl_row_ptr, cl_rows;
     std::vector<int32_t> cl_el_ptr;
     std::vector<uint32_t> cl_els;
-    std::vector<int32_t> cl_slot_ptr, cl_noff;
+    std::vector<int32_t> cl_slot_ptr, cl_noff, cl_ntr;
     std::vector<uint32_t> cl_slot, cl_slot_ent;
     std::vector<int32_t> cl_ent_ptr;
     std::vector<uint16_t> cl_ents;
     int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
+    // Value count of the solver layout: 9 per own slot, then the 9 x 32 zero block.
+    int64_t sell_zero() const { return 9 * static_cast<int64_t>(sell_ptr.back()); }
+    size_t sell_values() const { return static_cast<size_t>(sell_zero()) + 9 * 32; }
     int64_t nnzb() const { return static_cast<int64_t>(col_idx.size()); }
 };
 
@@ -98,6 +109,8 @@ constexpr int kClusterElems = LPG_CLUSTER_ELEMS;
 void build_plan(int V, int T, const int32_t* tets, HostPlan& plan);
 // Checks the cluster plan's invariants (throws LPG_ELOGIC on a violation).
 void check_clusters(const HostPlan& plan, const int32_t* tets);
+// Checks the solvers' upper-triangle sliced-ELL layout against the BSR pattern (LPG_ELOGIC).
+void check_solver_layout(const HostPlan& plan);
 
 // Device mirror of the plan and of the per-element records.
 struct DevMesh {
@@ -112,10 +125,12 @@ struct DevMesh {
     int num_unused = 0;
     int32_t* pair_elem = nullptr;
     int32_t *sell_ptr = nullptr, *sell_row = nullptr, *sell_col = nullptr, *sell_base = nullptr;
+    int32_t* sell_bptr = nullptr;
+    int2* sell_bref = nullptr; // {value index, column} per borrowed slot
     int n_sell = 0; // SELL chunks
     int ncl = 0, cl_max_slots = 0, cl_max_ents = 0;
     int32_t *cl_row_ptr = nullptr, *cl_rows = nullptr, *cl_el_ptr = nullptr, *cl_slot_ptr = nullptr, *cl_noff = nullptr,
-            *cl_ent_ptr = nullptr;
+            *cl_ntr = nullptr, *cl_ent_ptr = nullptr;
     uint32_t *cl_els = nullptr, *cl_slot = nullptr, *cl_slot_ent = nullptr;
     uint16_t* cl_ents = nullptr;
     int4* tets = nullptr;
@@ -128,7 +143,8 @@ struct DevMesh {
     float* fpinv32 = nullptr;
 };
 
-// Internal Hessian layout of the solvers: the sliced-ELL order of HostPlan::sell_*.
+// Internal Hessian layout of the solvers: the upper-triangle sliced ELL of HostPlan::sell_*
+// (blocks left of the diagonal are not stored).
 constexpr int kLayoutSell = 2;
 
 // ---- kernel launchers (lpg_assemble.cu) ----

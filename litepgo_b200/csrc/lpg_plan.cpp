@@ -12,6 +12,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <utility>
 
 #include "lpg_internal.h"
 
@@ -74,12 +75,14 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
     p.cl_ent_ptr.assign(1, 0);
     p.cl_els.clear();
     p.cl_noff.clear();
+    p.cl_ntr.clear();
     p.cl_slot.clear();
     p.cl_slot_ent.clear();
     p.cl_ents.clear();
     std::vector<int32_t> eloc(static_cast<size_t>(T), -1), els;
     std::vector<std::vector<uint16_t>> bucket;
     std::vector<std::vector<uint16_t>> diag;
+    std::vector<std::pair<uint32_t, uint32_t>> left, right; // (slot word, entry word)
     for (int c = 0; c < ncl; ++c) {
         const int r0 = p.cl_row_ptr[c], nr = p.cl_row_ptr[c + 1] - r0;
         els.clear();
@@ -98,6 +101,8 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
         p.cl_el_ptr.push_back(static_cast<int32_t>(p.cl_els.size()));
         const size_t ent0 = p.cl_ents.size();
         diag.assign(static_cast<size_t>(nr), {});
+        left.clear();
+        right.clear();
         int noff = 0;
         for (int j = 0; j < nr; ++j) {
             const int v = p.cl_rows[r0 + j];
@@ -120,13 +125,21 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
             for (int q = 0; q < nb; ++q) {
                 const int w = p.col_idx[rb + q];
                 if (w == v) continue;
-                p.cl_slot.push_back(static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (v > w ? 1u << 30 : 0u));
-                p.cl_slot_ent.push_back(static_cast<uint32_t>(p.cl_ents.size() - ent0) |
-                                        (static_cast<uint32_t>(bucket[q].size()) << 20));
+                const uint32_t word = static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (v > w ? 1u << 30 : 0u);
+                const uint32_t ent = static_cast<uint32_t>(p.cl_ents.size() - ent0) |
+                                     (static_cast<uint32_t>(bucket[q].size()) << 20);
+                (v > w ? left : right).emplace_back(word, ent);
                 p.cl_ents.insert(p.cl_ents.end(), bucket[q].begin(), bucket[q].end());
                 ++noff;
             }
         }
+        // Slots left of the diagonal first: the solver layout stores only the others.
+        for (const auto* side : {&left, &right})
+            for (const auto& we : *side) {
+                p.cl_slot.push_back(we.first);
+                p.cl_slot_ent.push_back(we.second);
+            }
+        p.cl_ntr.push_back(static_cast<int32_t>(left.size()));
         for (int j = 0; j < nr; ++j) {
             const int v = p.cl_rows[r0 + j];
             const int q = p.diag_slot[v] - p.row_ptr[v];
@@ -203,9 +216,15 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
         }
         p.col_idx.swap(cols);
     }
-    // Sliced ELL (SELL-32): rows sorted by block count (descending, then by index) within
-    // windows of kSellWindow rows, cut into chunks of 32; each chunk is as wide as its longest
-    // row and padding slots point at the row itself (their values stay zero).
+    p.diag_slot.assign(static_cast<size_t>(V), -1);
+    for (int v = 0; v < V; ++v)
+        for (int k = p.row_ptr[v]; k < p.row_ptr[v + 1]; ++k)
+            if (p.col_idx[k] == v) p.diag_slot[v] = k;
+    // Upper-triangle sliced ELL (SELL-32): rows sorted by block count (descending, then by
+    // index) within windows of kSellWindow rows, cut into chunks of 32. Own slots (columns >=
+    // row, diagonal first) are as wide as the chunk's longest own list, padding pointing at the
+    // row itself (values stay zero); borrowed slots (columns < row) reference the owning row's
+    // block, padding the zero block after the own slots.
     {
         const int nch = (V + 31) / 32;
         std::vector<int32_t> order(static_cast<size_t>(V));
@@ -216,32 +235,59 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
                 return p.row_ptr[a + 1] - p.row_ptr[a] > p.row_ptr[b + 1] - p.row_ptr[b];
             });
         }
+        // Own list of v: [diag, row end); borrowed: [row start, diag). A vertex in no element
+        // has neither.
+        auto own0 = [&](int v) { return p.diag_slot[v] >= 0 ? p.diag_slot[v] : p.row_ptr[v + 1]; };
         p.sell_ptr.assign(static_cast<size_t>(nch) + 1, 0);
+        p.sell_bptr.assign(static_cast<size_t>(nch) + 1, 0);
         p.sell_row.assign(32 * static_cast<size_t>(nch), -1);
         p.sell_base.assign(static_cast<size_t>(V), 0);
-        int64_t slots = 0;
+        int64_t slots = 0, bslots = 0;
         for (int c = 0; c < nch; ++c) {
-            int width = 0;
+            int width = 0, bwidth = 0;
             for (int l = 0; l < 32 && 32 * c + l < V; ++l) {
                 const int r = order[32 * c + l];
                 p.sell_row[32 * static_cast<size_t>(c) + l] = r;
-                width = std::max(width, p.row_ptr[r + 1] - p.row_ptr[r]);
+                width = std::max(width, p.row_ptr[r + 1] - own0(r));
+                bwidth = std::max(bwidth, own0(r) - p.row_ptr[r]);
                 p.sell_base[r] = static_cast<int32_t>(std::min<int64_t>(9 * slots + l, std::numeric_limits<int32_t>::max()));
             }
             slots += 32 * static_cast<int64_t>(width);
-            if (9 * slots + 9 * 32 >= std::numeric_limits<int32_t>::max())
+            bslots += 32 * static_cast<int64_t>(bwidth);
+            if (9 * slots + 9 * 32 >= std::numeric_limits<int32_t>::max() ||
+                bslots >= std::numeric_limits<int32_t>::max() / 2)
                 fail(LPG_EINVAL, "mesh too large for the solver's int32 Hessian offsets");
             p.sell_ptr[c + 1] = static_cast<int32_t>(slots);
+            p.sell_bptr[c + 1] = static_cast<int32_t>(bslots);
         }
+        const int32_t zero = static_cast<int32_t>(9 * slots);
         p.sell_col.assign(static_cast<size_t>(slots), 0);
+        p.sell_bref.assign(2 * static_cast<size_t>(bslots), 0);
         for (int c = 0; c < nch; ++c) {
             const int width = (p.sell_ptr[c + 1] - p.sell_ptr[c]) / 32;
+            const int bwidth = (p.sell_bptr[c + 1] - p.sell_bptr[c]) / 32;
             for (int l = 0; l < 32; ++l) {
                 const int r = p.sell_row[32 * static_cast<size_t>(c) + l];
-                const int nb = r < 0 ? 0 : p.row_ptr[r + 1] - p.row_ptr[r];
+                const int o0 = r < 0 ? 0 : own0(r);
+                const int no = r < 0 ? 0 : p.row_ptr[r + 1] - o0;
+                const int nbr = r < 0 ? 0 : o0 - p.row_ptr[r];
                 for (int q = 0; q < width; ++q)
-                    p.sell_col[p.sell_ptr[c] + 32 * static_cast<size_t>(q) + l] =
-                        q < nb ? p.col_idx[p.row_ptr[r] + q] : std::max(r, 0);
+                    p.sell_col[p.sell_ptr[c] + 32 * static_cast<size_t>(q) + l] = q < no ? p.col_idx[o0 + q] : std::max(r, 0);
+                for (int q = 0; q < bwidth; ++q) {
+                    int32_t idx = zero, col = std::max(r, 0);
+                    if (q < nbr) {
+                        col = p.col_idx[p.row_ptr[r] + q];
+                        // Block (col, r) is own block k - own0(col) of row col.
+                        const int32_t* beg = p.col_idx.data() + own0(col);
+                        const int32_t* end = p.col_idx.data() + p.row_ptr[col + 1];
+                        const int k = static_cast<int>(std::lower_bound(beg, end, r) - p.col_idx.data());
+                        if (k >= p.row_ptr[col + 1] || p.col_idx[k] != r) fail(LPG_ELOGIC, "Hessian pattern is not symmetric");
+                        idx = p.sell_base[col] + 32 * 9 * (k - own0(col));
+                    }
+                    const size_t at = 2 * (p.sell_bptr[c] + 32 * static_cast<size_t>(q) + l);
+                    p.sell_bref[at] = idx;
+                    p.sell_bref[at + 1] = col;
+                }
             }
         }
     }
@@ -291,10 +337,6 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
     p.contrib.assign(static_cast<size_t>(npairs) * 4, 0xff);
     p.slot_desc.clear();
     p.slot_desc.reserve(static_cast<size_t>(p.nnzb()));
-    p.diag_slot.assign(static_cast<size_t>(V), -1);
-    for (int v = 0; v < V; ++v)
-        for (int k = p.row_ptr[v]; k < p.row_ptr[v + 1]; ++k)
-            if (p.col_idx[k] == v) p.diag_slot[v] = k;
     std::vector<std::vector<int>> bucket;
     int64_t pair_cursor = 0;
     for (int t = 0; t < ntiles; ++t) {
@@ -386,6 +428,7 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
             const int j = d & 0xffu, q = (d >> 8) & 0x3fffffu;
             const bool diag = d >> 31, tr = (d >> 30) & 1u;
             if ((s >= p.cl_noff[c]) != diag) bad("slot order");
+            if (!diag && (s < p.cl_ntr[c]) != tr) bad("slot order (left of the diagonal first)");
             if (j >= static_cast<int>(first.size()) - 1) bad("slot row outside the cluster");
             const int v = p.cl_rows[p.cl_row_ptr[c] + j];
             if (q >= p.row_ptr[v + 1] - p.row_ptr[v]) bad("slot position outside its row");
@@ -420,6 +463,69 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
     if (contributors != 16 * static_cast<size_t>(T)) bad("contributor total differs from 16 per element");
     for (int c = 0; c < ncl; ++c)
         if (p.cl_ent_ptr[c] % 8 != 0) bad("contributor lists not 16-byte aligned");
+}
+
+void check_solver_layout(const HostPlan& p) {
+    auto bad = [](const char* what) { fail(LPG_ELOGIC, std::string("solver layout: ") + what); };
+    const int V = p.V;
+    const int nch = static_cast<int>(p.sell_ptr.size()) - 1;
+    if (nch != (V + 31) / 32 || p.sell_bptr.size() != p.sell_ptr.size()) bad("chunk count");
+    // (row, column) -> value index of entry 0, from the own slots as stored.
+    std::vector<std::vector<std::pair<int, int64_t>>> own(static_cast<size_t>(V));
+    std::vector<char> seen(static_cast<size_t>(V), 0);
+    for (int c = 0; c < nch; ++c) {
+        const int width = (p.sell_ptr[c + 1] - p.sell_ptr[c]) / 32;
+        if (p.sell_ptr[c + 1] - p.sell_ptr[c] != 32 * width || width < 0) bad("own slots not a multiple of 32");
+        for (int l = 0; l < 32; ++l) {
+            const int r = p.sell_row[32 * static_cast<size_t>(c) + l];
+            if (r < 0) continue;
+            if (r >= V || seen[r]++) bad("row listed twice or out of range");
+            if (p.sell_base[r] != 9 * p.sell_ptr[c] + l) bad("row base");
+            std::vector<int> upper;
+            for (int k = p.row_ptr[r]; k < p.row_ptr[r + 1]; ++k)
+                if (p.col_idx[k] >= r) upper.push_back(p.col_idx[k]);
+            if (static_cast<int>(upper.size()) > width) bad("chunk narrower than a row");
+            if (!upper.empty() && upper[0] != r) bad("diagonal is not the first own block");
+            for (int q = 0; q < width; ++q) {
+                const int col = p.sell_col[p.sell_ptr[c] + 32 * static_cast<size_t>(q) + l];
+                if (q < static_cast<int>(upper.size())) {
+                    if (col != upper[q]) bad("own column");
+                    own[r].emplace_back(col, static_cast<int64_t>(9) * p.sell_ptr[c] + 32 * 9 * static_cast<int64_t>(q) + l);
+                } else if (col != r) {
+                    bad("own padding column");
+                }
+            }
+        }
+    }
+    for (int v = 0; v < V; ++v)
+        if (!seen[v]) bad("row missing");
+    const int64_t zero = p.sell_zero();
+    for (int c = 0; c < nch; ++c) {
+        const int bwidth = (p.sell_bptr[c + 1] - p.sell_bptr[c]) / 32;
+        if (p.sell_bptr[c + 1] - p.sell_bptr[c] != 32 * bwidth || bwidth < 0) bad("borrowed slots not a multiple of 32");
+        for (int l = 0; l < 32; ++l) {
+            const int r = p.sell_row[32 * static_cast<size_t>(c) + l];
+            std::vector<int> lower;
+            if (r >= 0)
+                for (int k = p.row_ptr[r]; k < p.row_ptr[r + 1]; ++k)
+                    if (p.col_idx[k] < r) lower.push_back(p.col_idx[k]);
+            if (static_cast<int>(lower.size()) > bwidth) bad("chunk narrower than a borrowed list");
+            for (int q = 0; q < bwidth; ++q) {
+                const size_t at = 2 * (p.sell_bptr[c] + 32 * static_cast<size_t>(q) + l);
+                const int64_t idx = p.sell_bref[at];
+                const int col = p.sell_bref[at + 1];
+                if (q < static_cast<int>(lower.size())) {
+                    if (col != lower[q]) bad("borrowed column");
+                    int64_t want = -1;
+                    for (const auto& ce : own[col])
+                        if (ce.first == r) want = ce.second;
+                    if (want < 0 || idx != want) bad("borrowed block does not reference the owning row's block");
+                } else if (idx != zero || col < 0 || col >= std::max(V, 1)) {
+                    bad("borrowed padding");
+                }
+            }
+        }
+    }
 }
 
 } // namespace lpg

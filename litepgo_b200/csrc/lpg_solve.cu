@@ -194,29 +194,43 @@ template <int S, typename T> __device__ __forceinline__ void st3(T* p, size_t v,
     }
 }
 
-// Entry t (row-major) of the diagonal block of vertex v in the sliced-ELL layout, or -1.
+// Entry t (row-major) of the diagonal block of vertex v in the solver layout, or -1.
 __device__ __forceinline__ int64_t diag_entry(const DevMesh& m, int v, int t) {
-    const int k = m.diag_slot[v];
-    if (k < 0) return -1;
-    return static_cast<int64_t>(m.sell_base[v]) + 32 * static_cast<int64_t>(9 * (k - m.row_ptr[v]) + t);
+    if (m.diag_slot[v] < 0) return -1;
+    return static_cast<int64_t>(m.sell_base[v]) + 32 * t; // own block 0 is the diagonal
 }
 
-// y = mask (K x) on the 3x3 block matrix in the sliced-ELL layout (SELL-32): one warp per
-// chunk of 32 rows, one lane per row, block slot q of every lane read together, so each of the
-// nine value loads and the column load of a slot is one contiguous 128-byte (FP32) run, and a
-// lane's slots are independent (no cross-lane reduction). Vectors hold S values per vertex: 4
+// y = mask (K x) on the symmetric 3x3 block matrix in the upper-triangle sliced-ELL layout
+// (SELL-32): one warp per chunk of 32 rows, one lane per row. Own block slot q of every lane is
+// read together, so each of the nine value loads and the column load of a slot is one
+// contiguous 128-byte (FP32) run; a borrowed block (left of the diagonal) is the owning row's
+// block read transposed, nine 4- or 8-byte loads 32 entries apart (coalesced when the 32 rows'
+// owners sit in one chunk, as in a structured ordering). A lane's slots are independent (no
+// cross-lane reduction); half the blocks are stored, so the matrix stream is about halved. Vectors hold S values per vertex: 4
 // for the padded PCG vectors (4th value zero, one 16-byte load per gathered vertex in FP32),
 // 3 for plain FP64 vectors. With PCG the vector is z + beta p_old (beta from the state; each
 // row writes it to p_new), and the block of the grid that finishes last reduces the partial
 // p.Ap sums into alpha; otherwise, with DOT, part[block] = sum x.y. Both reductions use a
 // fixed order.
-// Resident blocks per SM the register allocation must allow (8 x 256 threads: 32 registers);
-// more resident warps hide the gathers' latency better than the registers they cost.
-#ifndef LPG_SPMV_MIN_BLOCKS
-#define LPG_SPMV_MIN_BLOCKS 8
+// Resident blocks per SM the register allocation must allow: 8 x 256 threads (32 registers)
+// for FP32 values, where more resident warps hide the gathers' latency better than the
+// registers they cost; 4 (64 registers) for FP64, whose nine 8-byte values per block spill at
+// 32. Slots unrolled by 2.
+#ifndef LPG_SPMV_MIN_BLOCKS_F32
+#define LPG_SPMV_MIN_BLOCKS_F32 8
 #endif
+#ifndef LPG_SPMV_MIN_BLOCKS_F64
+#define LPG_SPMV_MIN_BLOCKS_F64 4
+#endif
+#ifndef LPG_SPMV_UNROLL
+#define LPG_SPMV_UNROLL 2
+#endif
+constexpr int kSpmvUnroll = LPG_SPMV_UNROLL;
+template <typename TK> struct SpmvMinBlocks {
+    static constexpr int value = sizeof(TK) == 4 ? LPG_SPMV_MIN_BLOCKS_F32 : LPG_SPMV_MIN_BLOCKS_F64;
+};
 template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S>
-__global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS) spmv_sell(const DevMesh m, const TK* __restrict__ val,
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<TK>::value) spmv_sell(const DevMesh m, const TK* __restrict__ val,
                                                       const TV* __restrict__ x, const TV* __restrict__ p_old,
                                                       const TV* __restrict__ mask, TO* __restrict__ y,
                                                       TV* __restrict__ p_new, PcgState* st, double* part) {
@@ -235,9 +249,7 @@ __global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS) spmv_sell(const
         const int* cp = m.sell_col + s0 + lane;
         const TK* vp = val + 9 * static_cast<size_t>(s0) + lane;
         A a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll 4
-        for (int q = 0; q < width; ++q) {
-            const size_t col = static_cast<size_t>(__ldg(cp + 32 * q));
+        auto gather = [&](size_t col, A xv[3]) {
             TV xz[3];
             ld3<S>(x, col, xz);
             if (PCG) {
@@ -246,7 +258,14 @@ __global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS) spmv_sell(const
 #pragma unroll
                 for (int i = 0; i < 3; ++i) xz[i] = xz[i] + beta * xp[i];
             }
-            const A xv[3] = {static_cast<A>(xz[0]), static_cast<A>(xz[1]), static_cast<A>(xz[2])};
+#pragma unroll
+            for (int i = 0; i < 3; ++i) xv[i] = static_cast<A>(xz[i]);
+        };
+        // Own blocks (columns >= row): K_rc x_c.
+#pragma unroll kSpmvUnroll
+        for (int q = 0; q < width; ++q) {
+            A xv[3];
+            gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
             const TK* vq = vp + 288 * static_cast<size_t>(q);
             A kv[9];
 #pragma unroll
@@ -254,6 +273,23 @@ __global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS) spmv_sell(const
             a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
             a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
             a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
+        }
+        // Borrowed blocks (columns < row): K_cr^T x_c from the owning row's block.
+        const int b0 = __ldg(m.sell_bptr + c);
+        const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
+        const int2* bp = m.sell_bref + b0 + lane;
+#pragma unroll kSpmvUnroll
+        for (int q = 0; q < bwidth; ++q) {
+            const int2 ref = __ldg(bp + 32 * q);
+            A xv[3];
+            gather(static_cast<size_t>(ref.y), xv);
+            const TK* vq = val + static_cast<size_t>(ref.x);
+            A kv[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
+            a0 += kv[0] * xv[0] + kv[3] * xv[1] + kv[6] * xv[2];
+            a1 += kv[1] * xv[0] + kv[4] * xv[1] + kv[7] * xv[2];
+            a2 += kv[2] * xv[0] + kv[5] * xv[1] + kv[8] * xv[2];
         }
         if (row >= 0) {
             const size_t o = static_cast<size_t>(row);
@@ -779,7 +815,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
     LPG_CUDA(cudaMemcpyAsync(x, x0d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     const bool f64 = o.precision == LPG_PRECISION_F64;
     // Hessian in the sliced-ELL layout; its padding slots are zeroed once and never written.
-    const size_t hbytes = 9 * static_cast<size_t>(h.plan.sell_ptr.back()) * (f64 ? 8 : 4);
+    const size_t hbytes = h.plan.sell_values() * (f64 ? 8 : 4);
     void* K = h.s_hess.ensure(std::max<size_t>(hbytes, 8));
     LPG_CUDA(cudaMemsetAsync(K, 0, hbytes, s));
     void* dinv = h.s_dinv.ensure(12 * static_cast<size_t>(std::max(V, 1)) * (f64 ? 8 : 4));
@@ -942,7 +978,7 @@ void adjoint_solve(lpg_fem& h, const double* u_star, const double* dLdu, const i
     if (n == 0 || !(ws[1] > 0)) return;
     // Exact FP64 Hessian at u*: the residual matrix of the refinement (static_equilibrium_response.cpp:58).
     // Sliced-ELL Hessians; padding slots zeroed (never written by the assembly).
-    const size_t nv = 9 * static_cast<size_t>(h.plan.sell_ptr.back());
+    const size_t nv = h.plan.sell_values();
     double* K64 = h.s_hess64.as<double>(std::max<size_t>(nv, 1));
     LPG_CUDA(cudaMemsetAsync(K64, 0, nv * sizeof(double), s));
     h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutSell, K64, nullptr);
@@ -1190,7 +1226,7 @@ __global__ void __launch_bounds__(256) pcg_b_start(BatchPcg st, const double* __
 // Ap = mask (K p) with p = z + beta[mesh] p_old formed on the fly (written to p_new), and the
 // per-row p.Ap; the sliced-ELL traversal of spmv_sell, one lane per row.
 template <typename R>
-__global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<R>::value)
     spmv_sell_batch(const DevMesh m, const R* __restrict__ val, const R* __restrict__ z, const R* __restrict__ p_old,
                     const R* __restrict__ mask, R* __restrict__ y, R* __restrict__ p_new, BatchPcg st,
                     const int* __restrict__ mov, double* __restrict__ rowdot) {
@@ -1206,13 +1242,18 @@ __global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS)
     const int* cp = m.sell_col + s0 + lane;
     const R* vp = val + 9 * static_cast<size_t>(s0) + lane;
     R a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll 4
-    for (int q = 0; q < width; ++q) {
-        const size_t col = static_cast<size_t>(__ldg(cp + 32 * q));
+    // A block's rows and columns belong to one mesh, so the row's beta applies to its columns.
+    auto gather = [&](size_t col, R xv[3]) {
         R xz[3], xp[3];
         ld3<4>(z, col, xz);
         ld3<4>(p_old, col, xp);
-        const R xv[3] = {xz[0] + beta * xp[0], xz[1] + beta * xp[1], xz[2] + beta * xp[2]};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) xv[i] = xz[i] + beta * xp[i];
+    };
+#pragma unroll kSpmvUnroll
+    for (int q = 0; q < width; ++q) {
+        R xv[3];
+        gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
         const R* vq = vp + 288 * static_cast<size_t>(q);
         R kv[9];
 #pragma unroll
@@ -1220,6 +1261,22 @@ __global__ void __launch_bounds__(kThreads, LPG_SPMV_MIN_BLOCKS)
         a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
         a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
         a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
+    }
+    const int b0 = __ldg(m.sell_bptr + c);
+    const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
+    const int2* bp = m.sell_bref + b0 + lane;
+#pragma unroll kSpmvUnroll
+    for (int q = 0; q < bwidth; ++q) {
+        const int2 ref = __ldg(bp + 32 * q);
+        R xv[3];
+        gather(static_cast<size_t>(ref.y), xv);
+        const R* vq = val + static_cast<size_t>(ref.x);
+        R kv[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) kv[e] = __ldg(vq + 32 * e);
+        a0 += kv[0] * xv[0] + kv[3] * xv[1] + kv[6] * xv[2];
+        a1 += kv[1] * xv[0] + kv[4] * xv[1] + kv[7] * xv[2];
+        a2 += kv[2] * xv[0] + kv[5] * xv[1] + kv[8] * xv[2];
     }
     if (row < 0) return;
     const size_t o = static_cast<size_t>(row);
@@ -1592,7 +1649,7 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
     const double* x0d = h.stage_in(x0, io_mem, h.d_u, n);
     LPG_CUDA(cudaMemcpyAsync(x, x0d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     const bool f64 = o.precision == LPG_PRECISION_F64;
-    const size_t hbytes = 9 * static_cast<size_t>(h.plan.sell_ptr.back()) * (f64 ? 8 : 4);
+    const size_t hbytes = h.plan.sell_values() * (f64 ? 8 : 4);
     void* K = h.s_hess.ensure(std::max<size_t>(hbytes, 8));
     LPG_CUDA(cudaMemsetAsync(K, 0, hbytes, s));
     void* dinv = h.s_dinv.ensure(12 * static_cast<size_t>(std::max(V, 1)) * (f64 ? 8 : 4));

@@ -34,8 +34,8 @@ struct lpg_fem {
     // Plan and element data.
     lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tile_pair_ptr, b_tile_row_ptr, b_tile_rows, b_tile_slot_ptr,
         b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused;
-    lpg::DeviceBuffer b_cl[10]; // assembly clusters
-    lpg::DeviceBuffer b_sell[4]; // sliced-ELL pattern of the solvers
+    lpg::DeviceBuffer b_cl[11]; // assembly clusters
+    lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers
     lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_plist, d_pcount; // elements listed for the projection's eigenvalue clamp

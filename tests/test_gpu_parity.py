@@ -7,6 +7,7 @@ in each test; patterns bit-exact; repeated evaluations bitwise identical.
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 import oracle
 from conftest import TWO_TET_CELLS, TWO_TET_THETA, TWO_TET_X, rel_err, two_tet_states
@@ -305,9 +306,11 @@ def solver_values(e, u, hessian, precision, layout, nvalues):
 
 
 @pytest.mark.parametrize("case", ["box", "ragged", "valence"])
-def test_solver_sliced_ell_layout_is_a_permutation_of_bsr(case):
-    """The Newton / adjoint solvers keep the Hessian in sliced ELL (chunks of 32 rows sorted by
-    block count within 128-row windows, slot-major); it must hold the BSR values bit for bit."""
+def test_solver_sliced_ell_layout_holds_the_upper_bsr_blocks(case):
+    """The Newton / adjoint solvers keep the upper triangle of the Hessian (blocks with column >=
+    row, diagonal first) in sliced ELL (chunks of 32 rows sorted by block count within 128-row
+    windows, slot-major); it must hold those BSR values bit for bit, and the BSR Hessian must be
+    symmetric, so that the blocks it leaves out are the transposes of the ones it keeps."""
     from litepgo_b200 import _native as N
 
     rng = np.random.default_rng(12)
@@ -325,12 +328,16 @@ def test_solver_sliced_ell_layout_is_a_permutation_of_bsr(case):
         tets = np.array([[0, 2 + i, 2 + (i + 1) % k, 1] for i in range(k)], np.int32)
         theta, u = np.array([2.0, 3.0]), 0.01 * rng.standard_normal(X.size)
     e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta)
-    row_ptr, _ = e.pattern_bsr()
+    row_ptr, col_idx = e.pattern_bsr()
     nb = np.diff(row_ptr)
     V = X.shape[0]
+    rows_of = np.repeat(np.arange(V), nb)
+    upper = col_idx >= rows_of
+    own0 = np.array([row_ptr[v] + np.count_nonzero(col_idx[row_ptr[v]:row_ptr[v + 1]] < v) for v in range(V)])
+    no = row_ptr[1:] - own0
     nslots, ptr, rows = sell_layout(e)
     # The layout's own rules: every row once, sorted by block count within 128-row windows,
-    # each chunk as wide as its longest row.
+    # each chunk as wide as its row with the most stored blocks.
     order = rows[rows >= 0]
     assert np.array_equal(np.sort(order), np.arange(V)) and np.all(rows[V:] == -1)
     for w0 in range(0, V, 128):
@@ -340,20 +347,29 @@ def test_solver_sliced_ell_layout_is_a_permutation_of_bsr(case):
     for c in range(ptr.size - 1):
         rc = rows[32 * c:32 * c + 32]
         rc = rc[rc >= 0]
-        assert ptr[c + 1] - ptr[c] == 32 * nb[rc].max(initial=0)
+        assert ptr[c + 1] - ptr[c] == 32 * no[rc].max(initial=0)
     assert nslots == ptr[-1]
-    perm = np.empty(9 * e.nnzb, np.int64)  # perm[bsr position] = sliced-ELL position
+    bsr_at = []  # BSR entry positions of the stored blocks, and their sliced-ELL positions
+    sell_at = []
     for c in range(ptr.size - 1):
         for lane in range(32):
             r = rows[32 * c + lane]
             if r < 0:
                 continue
-            q = np.arange(nb[r])
+            q = np.arange(no[r])
             for t in range(9):
-                perm[9 * (row_ptr[r] + q) + t] = 9 * ptr[c] + 32 * (9 * q + t) + lane
-    assert np.unique(perm).size == perm.size and perm.max() < 9 * nslots
+                bsr_at.append(9 * (own0[r] + q) + t)
+                sell_at.append(9 * ptr[c] + 32 * (9 * q + t) + lane)
+    bsr_at, sell_at = np.concatenate(bsr_at), np.concatenate(sell_at)
+    assert np.unique(sell_at).size == sell_at.size and sell_at.max() < 9 * nslots
+    assert bsr_at.size == 9 * np.count_nonzero(upper)
     for hk in (Exact, Projected):
         for prec in (N.PRECISION_F64, N.PRECISION_MIXED):
             bsr = solver_values(e, u, hk, prec, N.LAYOUT_BSR, 9 * e.nnzb)
             sell = solver_values(e, u, hk, prec, 2, 9 * nslots)
-            assert np.array_equal(sell[perm], bsr)
+            assert np.array_equal(sell[sell_at], bsr[bsr_at])
+            Hb = sp.bsr_matrix((bsr.reshape(-1, 3, 3), col_idx, row_ptr), shape=(3 * V, 3 * V)).toarray()
+            if hk == Exact:
+                assert np.array_equal(Hb, Hb.T)  # bitwise symmetric by construction
+            else:
+                assert np.abs(Hb - Hb.T).max() <= 1e-5 * np.abs(Hb).max()
