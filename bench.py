@@ -232,6 +232,13 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def tuning_summary(fem_energy):
+    """The launch variants the handle's autotuner chose, with its timings (ms; null = not timed)."""
+    t = fem_energy.tuning()
+    return {"choice": t["choice"],
+            "ms": {k: [None if v != v else round(v, 4) for v in vals] for k, vals in t["ms"].items()}}
+
+
 def whole_job_rate(units_per_rank, seconds_max, world):
     """Whole-job throughput of `world` identical replicas: all ranks' units over the slowest
     rank's time (the max over ranks)."""
@@ -413,6 +420,7 @@ def run_ours(args):
             "config": dict(workload_config(), parallelism=f"replicas x{world}"),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
             "clocks": clocks.summary(), "mixed_precision_kernel": mixed, "newton_time_to_1e-8": newton,
+            "autotune": tuning_summary(e),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -334,6 +334,27 @@ int lpg_adjoint_rest(lpg_fem_t h, const double* u_star, const double* dLdu, cons
  */
 int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element);
 
+/*
+ * Autotuner (no reference counterpart). Three kernels come in launch variants that differ in
+ * register budget and loop unrolling only, so every variant computes bitwise the same
+ * results: the Exact-Hessian assembly (3 variants per precision), the PCG SpMV of the
+ * Newton and adjoint solvers (3 per precision) and the projected Hessian's eigenvalue clamp
+ * (2 in FP32, 1 in FP64). lpg_fem_create times every variant on the new handle's mesh (rest
+ * state; seeded 9x9 matrices for the clamp; mean of 3 launches after a warm-up) and keeps the
+ * fastest per precision, unless the environment variable LPG_AUTOTUNE is "0" (then variant 0
+ * everywhere). lpg_fem_autotune runs the timing again.
+ * lpg_fem_get_tuning: choice[6] = {assembly FP64, assembly FP32, SpMV FP64, SpMV FP32,
+ *   clamp FP64, clamp FP32}; ms[18] = mean ms per launch, ms[6 f + 3 p + v] for family f
+ *   (assembly, SpMV, clamp), precision p (FP64, FP32) and variant v; NaN where not timed
+ *   (variants a family does not have, and the FP64 clamp, which has one).
+ *   Either output may be NULL.
+ * lpg_fem_set_tuning: forces choices (same order; -1 keeps the current one); LPG_EINVAL
+ *   for an index outside the family's variants.
+ */
+int lpg_fem_autotune(lpg_fem_t h);
+int lpg_fem_get_tuning(lpg_fem_t h, int32_t choice[6], double ms[18]);
+int lpg_fem_set_tuning(lpg_fem_t h, const int32_t choice[6]);
+
 #ifdef __cplusplus
 }
 #endif

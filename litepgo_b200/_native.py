@@ -100,6 +100,9 @@ SIGNATURES = [
     ("lpg_fem_force_vjp_rest", _int, [_vp, _vp, _vp, _int, _vp]),
     ("lpg_adjoint_rest", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _vp, _vp]),
     ("lpg_fem_set_theta", _int, [_vp, _dp, _int]),
+    ("lpg_fem_autotune", _int, [_vp]),
+    ("lpg_fem_get_tuning", _int, [_vp, _ip, _dp]),
+    ("lpg_fem_set_tuning", _int, [_vp, _ip]),
 ]
 
 EXPORTED = [name for name, _, _ in SIGNATURES]

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -145,11 +146,13 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.status = d_status.as<unsigned>(1);
     a.ev_begin = ev_begin;
     a.ev_end = ev_end;
+    const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
+    a.cl_variant = tune.cl[pi];
     if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {
         void* proj = d_proj.ensure(project_bytes(dm, precision));
         launch_project(dm, precision, hessian, du, proj, a.status, stream,
                        d_plist.as<int>(std::max<size_t>(static_cast<size_t>(dm.T), 1)), d_pcount.as<unsigned>(1), emesh,
-                       mesh_exact);
+                       mesh_exact, tune.clamp[pi]);
         a.proj = proj;
     }
     launch_eval(dm, precision, hessian, a, stream);
@@ -339,6 +342,9 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         }
         LPG_CUDA(cudaMemset(h->d_status.as<unsigned>(1), 0, sizeof(unsigned)));
         LPG_CUDA(cudaDeviceSynchronize());
+        // Launch variants tuned on this mesh unless LPG_AUTOTUNE=0 (then the defaults stay).
+        const char* at = std::getenv("LPG_AUTOTUNE");
+        if (!(at && std::strcmp(at, "0") == 0)) autotune(*h);
         *out = h.release();
     });
 }
@@ -560,6 +566,44 @@ int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         newton_solve(*h, fixed, nfixed, f_ext, x0, io_mem, *o, x_out, res);
+    });
+}
+
+int lpg_fem_autotune(lpg_fem_t h) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        autotune(*h);
+    });
+}
+
+int lpg_fem_get_tuning(lpg_fem_t h, int32_t choice[6], double ms[18]) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        const Tuning& t = h->tune;
+        if (choice) {
+            const int32_t c[6] = {t.cl[0], t.cl[1], t.spmv[0], t.spmv[1], t.clamp[0], t.clamp[1]};
+            std::copy(c, c + 6, choice);
+        }
+        if (ms)
+            for (int f = 0; f < 3; ++f)
+                for (int p = 0; p < 2; ++p)
+                    for (int v = 0; v < 3; ++v) ms[6 * f + 3 * p + v] = t.tuned ? t.ms[f][p][v] : std::nan("");
+    });
+}
+
+int lpg_fem_set_tuning(lpg_fem_t h, const int32_t choice[6]) {
+    return guarded([&] {
+        if (!h || !choice) fail(LPG_EINVAL, "lpg_fem_set_tuning: null argument");
+        const int lim[6] = {kClVariants, kClVariants, kSpmvVariants, kSpmvVariants, 1, kClampVariants};
+        for (int i = 0; i < 6; ++i)
+            if (choice[i] < -1 || choice[i] >= lim[i]) fail(LPG_EINVAL, "lpg_fem_set_tuning: variant out of range");
+        BusyGuard busy(h->busy);
+        Tuning& t = h->tune;
+        int* dst[6] = {&t.cl[0], &t.cl[1], &t.spmv[0], &t.spmv[1], &t.clamp[0], &t.clamp[1]};
+        for (int i = 0; i < 6; ++i)
+            if (choice[i] >= 0) *dst[i] = choice[i];
     });
 }
 

@@ -1099,9 +1099,15 @@ constexpr int kClampVStride = 81;
 #define LPG_CLAMP_MIN_BLOCKS_F32 6
 #endif
 
-template <typename R>
-__global__ void __launch_bounds__(kProjThreads, sizeof(R) == 4 ? LPG_CLAMP_MIN_BLOCKS_F32 : 1) clamp_kernel(R* __restrict__ proj, const int* __restrict__ list,
-                                                             const unsigned* __restrict__ count) {
+// Register-budget variants of the clamp (autotuner): FP32 at LPG_CLAMP_MIN_BLOCKS_F32 resident
+// blocks or unconstrained (about 187 registers, no spill); FP64 has one.
+template <typename R> constexpr int clamp_minb(int v) {
+    return sizeof(R) == 8 ? 1 : (v == 0 ? LPG_CLAMP_MIN_BLOCKS_F32 : 1);
+}
+
+template <typename R, int MINB>
+__global__ void __launch_bounds__(kProjThreads, MINB) clamp_kernel(R* __restrict__ proj, const int* __restrict__ list,
+                                                                   const unsigned* __restrict__ count) {
     const unsigned n = *count;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         R* out = proj + 45 * static_cast<size_t>(list[i]);
@@ -1115,6 +1121,21 @@ __global__ void __launch_bounds__(kProjThreads, sizeof(R) == 4 ? LPG_CLAMP_MIN_B
             R V[81];
             clamp9<R, true>(out, V);
         }
+    }
+}
+
+// Seeded symmetric test matrices for timing the clamp: entry values in [-1, 1) from an integer
+// hash (SplitMix64 finaliser) of the element and entry index; list[i] = i.
+template <typename R> __global__ void clamp_sample_kernel(R* __restrict__ proj, int* __restrict__ list, int n) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    list[e] = e;
+    for (int t = 0; t < 45; ++t) {
+        unsigned long long z = 45ull * static_cast<unsigned long long>(e) + t + 0x9e3779b97f4a7c15ull;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        proj[45 * static_cast<size_t>(e) + t] = static_cast<R>(static_cast<double>(z >> 11) * 0x1.0p-52 - 1.0);
     }
 }
 
@@ -1143,9 +1164,13 @@ __global__ void __launch_bounds__(kProjThreads, sizeof(R) == 4 ? LPG_CLAMP_MIN_B
 #endif
 constexpr int kClThreads = LPG_CLUSTER_THREADS;
 constexpr int kClUnroll = LPG_CLUSTER_UNROLL;
-template <typename R> struct ClMinBlocks;
-template <> struct ClMinBlocks<double> { static constexpr int value = LPG_CLUSTER_MIN_BLOCKS_F64; };
-template <> struct ClMinBlocks<float> { static constexpr int value = LPG_CLUSTER_MIN_BLOCKS_F32; };
+// Register-budget variants of the Hessian-writing cluster kernel (resident blocks per SM the
+// allocation must allow), chosen per handle by the autotuner; variant 0 is the default. The
+// variants differ in register allocation only, so their results are bitwise identical.
+template <typename R> constexpr int cl_minb(int v) {
+    return sizeof(R) == 8 ? (v == 0 ? LPG_CLUSTER_MIN_BLOCKS_F64 : v == 1 ? 2 : 4)
+                          : (v == 0 ? LPG_CLUSTER_MIN_BLOCKS_F32 : v == 1 ? 4 : 8);
+}
 
 // Index of the unordered vertex pair (a, b) of a tet among its 10.
 __device__ __forceinline__ int pair10(int a, int b) {
@@ -1173,8 +1198,8 @@ __device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, 
     return static_cast<size_t>(static_cast<int64_t>(sb) + 32 * static_cast<int64_t>(9 * q + t));
 }
 
-template <typename R, bool WG, bool WH>
-__global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_kernel(const DevMesh m, const EvalArgs a) {
+template <typename R, bool WG, bool WH, int MINB>
+__global__ void __launch_bounds__(kClThreads, MINB) cluster_kernel(const DevMesh m, const EvalArgs a) {
     using X = M<R>;
     using HT = typename HOut<R>::T;
     constexpr int E = kClusterElems;
@@ -1389,7 +1414,8 @@ __global__ void __launch_bounds__(kClThreads, ClMinBlocks<R>::value) cluster_ker
     if ((tid & 31) == 0 && st) atomicOr(a.status, st);
 }
 
-template <typename R, bool WG, bool WH> void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+template <typename R, bool WG, bool WH, int MINB = cl_minb<R>(0)>
+void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = cl_smem_bytes<R, WG, WH>(m);
     // Resident blocks for this shared-memory size (cached for the last size seen).
     thread_local size_t cached_sm = 0;
@@ -1399,16 +1425,16 @@ template <typename R, bool WG, bool WH> void launch_cluster(const DevMesh& m, co
         LPG_CUDA(cudaGetDevice(&dev));
         LPG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         if (sm > static_cast<size_t>(optin)) fail(LPG_EINVAL, "mesh cluster needs more shared memory than the GPU has");
-        LPG_CUDA(cudaFuncSetAttribute(cluster_kernel<R, WG, WH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        LPG_CUDA(cudaFuncSetAttribute(cluster_kernel<R, WG, WH, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(sm)));
         LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_kernel<R, WG, WH>, kClThreads, sm));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_kernel<R, WG, WH, MINB>, kClThreads, sm));
         resident = std::max(1, sms * std::max(per_sm, 1));
         cached_sm = sm;
     }
     const int blocks = std::min(resident, m.ncl);
     if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-    if (blocks > 0) cluster_kernel<R, WG, WH><<<blocks, kClThreads, sm, s>>>(m, a);
+    if (blocks > 0) cluster_kernel<R, WG, WH, MINB><<<blocks, kClThreads, sm, s>>>(m, a);
     if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
     LPG_CUDA(cudaGetLastError());
 }
@@ -1558,6 +1584,15 @@ template <typename R, bool WG, int WH> void launch_chunks(const DevMesh& m, cons
         launch_assemble<R, WG, WH, 2>(m, a, s);
 }
 
+// The Hessian-writing cluster kernel in the register-budget variant a.cl_variant.
+template <typename R, bool WG> void launch_cluster_variant(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    switch (a.cl_variant) {
+    case 1: launch_cluster<R, WG, true, cl_minb<R>(1)>(m, a, s); break;
+    case 2: launch_cluster<R, WG, true, cl_minb<R>(2)>(m, a, s); break;
+    default: launch_cluster<R, WG, true>(m, a, s); break;
+    }
+}
+
 // Launches the element pass; returns the number of per-unit energies it wrote to tile_energy.
 // The Exact Hessian, gradient and energy use the element-once cluster kernel; the projected
 // Hessian uses the pair kernel over the per-element clamped tangents.
@@ -1565,9 +1600,9 @@ template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const Eva
     const bool wg = a.grad != nullptr;
     const int wh = a.hess == nullptr ? 0 : (hessian == LPG_HESSIAN_EXACT ? 1 : 2);
     int units = m.ncl;
-    if (wg && wh == 1) launch_cluster<R, true, true>(m, a, s);
+    if (wg && wh == 1) launch_cluster_variant<R, true>(m, a, s);
     else if (wg && wh == 2) launch_chunks<R, true, 2>(m, a, s), units = m.ntiles;
-    else if (!wg && wh == 1) launch_cluster<R, false, true>(m, a, s);
+    else if (!wg && wh == 1) launch_cluster_variant<R, false>(m, a, s);
     else if (!wg && wh == 2) launch_chunks<R, false, 2>(m, a, s), units = m.ntiles;
     else if (wg) launch_cluster<R, true, false>(m, a, s);
     else launch_cluster<R, false, false>(m, a, s);
@@ -1607,38 +1642,76 @@ size_t project_bytes(const DevMesh& m, int precision) {
 }
 
 namespace {
-template <typename R>
-void launch_project_t(const DevMesh& m, const double* u, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
-                      const int* mesh_exact, int* list, unsigned* count) {
-    const size_t sm = sizeof(R) * kProjStride * kProjThreads;
+template <typename R, int MINB>
+void launch_clamp_t(R* proj, const int* list, const unsigned* count, int max_count, cudaStream_t s) {
     const size_t clamp_sm = sizeof(R) == 8 ? sizeof(R) * kClampVStride * kProjThreads : 0;
-    thread_local int clamp_grid = 0;
+    thread_local int clamp_grid = 0; // one wave of this variant
     if (clamp_grid == 0) {
-        LPG_CUDA(cudaFuncSetAttribute(project_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
         int dev = 0, sms = 0, per = 0;
         LPG_CUDA(cudaGetDevice(&dev));
         LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if (clamp_sm > 0)
-            LPG_CUDA(cudaFuncSetAttribute(clamp_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            LPG_CUDA(cudaFuncSetAttribute(clamp_kernel<R, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(clamp_sm)));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, clamp_kernel<R>, kProjThreads, clamp_sm));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, clamp_kernel<R, MINB>, kProjThreads, clamp_sm));
         clamp_grid = std::max(1, per) * std::max(1, sms);
+    }
+    const int blocks = (max_count + kProjThreads - 1) / kProjThreads;
+    if (blocks > 0) clamp_kernel<R, MINB><<<std::min(clamp_grid, blocks), kProjThreads, clamp_sm, s>>>(proj, list, count);
+}
+template <typename R>
+void launch_clamp_v(R* proj, const int* list, const unsigned* count, int max_count, int variant, cudaStream_t s) {
+    if (variant == 1)
+        launch_clamp_t<R, clamp_minb<R>(1)>(proj, list, count, max_count, s);
+    else
+        launch_clamp_t<R, clamp_minb<R>(0)>(proj, list, count, max_count, s);
+}
+
+template <typename R>
+void launch_project_t(const DevMesh& m, const double* u, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
+                      const int* mesh_exact, int* list, unsigned* count, int clamp_variant) {
+    const size_t sm = sizeof(R) * kProjStride * kProjThreads;
+    thread_local bool ready = false;
+    if (!ready) {
+        LPG_CUDA(cudaFuncSetAttribute(project_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        ready = true;
     }
     const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
     LPG_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
     project_kernel<R><<<blocks, kProjThreads, sm, s>>>(m, u, proj, status, emesh, mesh_exact, list, count);
-    clamp_kernel<R><<<std::min(clamp_grid, blocks), kProjThreads, clamp_sm, s>>>(proj, list, count);
+    launch_clamp_v<R>(proj, list, count, m.T, clamp_variant, s);
 }
 } // namespace
 
 void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
-                    cudaStream_t s, int* list, unsigned* count, const int* emesh, const int* mesh_exact) {
+                    cudaStream_t s, int* list, unsigned* count, const int* emesh, const int* mesh_exact,
+                    int clamp_variant) {
     if (hessian != LPG_HESSIAN_PROJECTED) fail(LPG_EINVAL, "projected Hessian kind not available");
     if (m.T == 0) return;
     if (precision == LPG_PRECISION_F64)
-        launch_project_t<double>(m, u, static_cast<double*>(proj), status, s, emesh, mesh_exact, list, count);
+        launch_project_t<double>(m, u, static_cast<double*>(proj), status, s, emesh, mesh_exact, list, count,
+                                 clamp_variant);
     else
-        launch_project_t<float>(m, u, static_cast<float*>(proj), status, s, emesh, mesh_exact, list, count);
+        launch_project_t<float>(m, u, static_cast<float*>(proj), status, s, emesh, mesh_exact, list, count,
+                                clamp_variant);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_clamp(int precision, void* proj, const int* list, const unsigned* count, int max_count, int clamp_variant,
+                  cudaStream_t s) {
+    if (precision == LPG_PRECISION_F64)
+        launch_clamp_v<double>(static_cast<double*>(proj), list, count, max_count, clamp_variant, s);
+    else
+        launch_clamp_v<float>(static_cast<float*>(proj), list, count, max_count, clamp_variant, s);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_clamp_sample(int precision, void* proj, int* list, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    if (precision == LPG_PRECISION_F64)
+        clamp_sample_kernel<double><<<(n + 255) / 256, 256, 0, s>>>(static_cast<double*>(proj), list, n);
+    else
+        clamp_sample_kernel<float><<<(n + 255) / 256, 256, 0, s>>>(static_cast<float*>(proj), list, n);
     LPG_CUDA(cudaGetLastError());
 }
 

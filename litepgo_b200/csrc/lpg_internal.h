@@ -159,6 +159,21 @@ struct EvalArgs {
     const void* proj = nullptr;    // projected per-element 9x9 tangents (hessian PROJECTED*), or null
     unsigned* status = nullptr;    // device status word
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr; // optional: bracket the assembly kernel
+    int cl_variant = 0; // register-budget variant of the Exact-Hessian cluster kernel (autotuner)
+};
+
+// Autotuned launch variants (register budgets and unroll depths; every variant of a kernel
+// computes bitwise the same results). Index [0] FP64, [1] FP32 / mixed.
+constexpr int kClVariants = 3;    // cluster kernel, Exact Hessian
+constexpr int kSpmvVariants = 3;  // PCG sliced-ELL SpMV
+constexpr int kClampVariants = 2; // eigenvalue clamp (FP32 only; FP64 has one)
+struct Tuning {
+    int cl[2] = {0, 0};
+    int spmv[2] = {0, 0};
+    int clamp[2] = {0, 0};
+    // Mean ms per launch of each variant as measured ([family][precision][variant]); NaN if not run.
+    double ms[3][2][3];
+    bool tuned = false;
 };
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s);
 // Per-element clamped tangents for the projected Hessians (45 values / element, upper triangle).
@@ -167,7 +182,13 @@ void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a
 // marked exact keep their tangent unclamped.
 void launch_project(const DevMesh& m, int precision, int hessian, const double* u, void* proj, unsigned* status,
                     cudaStream_t s, int* list, unsigned* count, const int* emesh = nullptr,
-                    const int* mesh_exact = nullptr);
+                    const int* mesh_exact = nullptr, int clamp_variant = 0);
+// The eigenvalue clamp alone on `count` listed elements of proj (autotuner timing).
+void launch_clamp(int precision, void* proj, const int* list, const unsigned* count, int max_count, int clamp_variant,
+                  cudaStream_t s);
+// Fills n packed symmetric 9x9 matrices (45 values each) with seeded values in [-1, 1] and
+// list[i] = i (autotuner timing input for the clamp).
+void launch_clamp_sample(int precision, void* proj, int* list, int n, cudaStream_t s);
 size_t project_bytes(const DevMesh& m, int precision);
 // per_elem (T doubles, optional) receives each element's step.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,

@@ -225,12 +225,16 @@ __device__ __forceinline__ int64_t diag_entry(const DevMesh& m, int v, int t) {
 #ifndef LPG_SPMV_UNROLL
 #define LPG_SPMV_UNROLL 2
 #endif
-constexpr int kSpmvUnroll = LPG_SPMV_UNROLL;
-template <typename TK> struct SpmvMinBlocks {
-    static constexpr int value = sizeof(TK) == 4 ? LPG_SPMV_MIN_BLOCKS_F32 : LPG_SPMV_MIN_BLOCKS_F64;
+// Launch variants of the PCG SpMV (autotuner): {resident blocks, slot unroll}. Variant 0 is the
+// default; all variants sum each row in the same order, so their results are bitwise identical.
+template <typename TK, int VAR> struct SpmvCfg {
+    static constexpr bool f32 = sizeof(TK) == 4;
+    static constexpr int minb = VAR == 0 ? (f32 ? LPG_SPMV_MIN_BLOCKS_F32 : LPG_SPMV_MIN_BLOCKS_F64)
+                                         : VAR == 1 ? (f32 ? 8 : 4) : (f32 ? 6 : 3);
+    static constexpr int unroll = VAR == 0 ? LPG_SPMV_UNROLL : 4;
 };
-template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S>
-__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<TK>::value) spmv_sell(const DevMesh m, const TK* __restrict__ val,
+template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S, int VAR = 0>
+__global__ void __launch_bounds__(kThreads, (SpmvCfg<TK, VAR>::minb)) spmv_sell(const DevMesh m, const TK* __restrict__ val,
                                                       const TV* __restrict__ x, const TV* __restrict__ p_old,
                                                       const TV* __restrict__ mask, TO* __restrict__ y,
                                                       TV* __restrict__ p_new, PcgState* st, double* part) {
@@ -262,7 +266,7 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<TK>::value) spmv_sell(
             for (int i = 0; i < 3; ++i) xv[i] = static_cast<A>(xz[i]);
         };
         // Own blocks (columns >= row): K_rc x_c.
-#pragma unroll kSpmvUnroll
+#pragma unroll (SpmvCfg<TK, VAR>::unroll)
         for (int q = 0; q < width; ++q) {
             A xv[3];
             gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<TK>::value) spmv_sell(
         const int b0 = __ldg(m.sell_bptr + c);
         const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
         const int2* bp = m.sell_bref + b0 + lane;
-#pragma unroll kSpmvUnroll
+#pragma unroll (SpmvCfg<TK, VAR>::unroll)
         for (int q = 0; q < bwidth; ++q) {
             const int2 ref = __ldg(bp + 32 * q);
             A xv[3];
@@ -637,18 +641,18 @@ struct Solver {
     // One warp per sliced-ELL chunk (8 per block). Not persistent: with about one chunk per
     // resident warp, a grid-stride loop would leave a fifth of the warps with two chunks and the
     // rest idle; later blocks instead start as earlier ones finish.
-    template <typename Kern> int spmv_grid(Kern) const { return std::max(1, (h.dm.n_sell + 7) / 8); }
+    int spmv_grid(int = 0) const { return std::max(1, (h.dm.n_sell + 7) / 8); }
     template <typename Kern> int vec_grid(Kern k) const { return one_wave(k, grid(static_cast<size_t>(V))); }
 
     // y64 = mask (K x64) in FP64 with K stored as TK.
     void residual_spmv(const void* K, bool k64, const double* x64, const double* mask, double* y64) {
         if (k64)
             spmv_sell<double, double, double, false, false, 3>
-                <<<spmv_grid(spmv_sell<double, double, double, false, false, 3>), kThreads, 0, s>>>(
+                <<<spmv_grid(), kThreads, 0, s>>>(
                     h.dm, static_cast<const double*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
         else
             spmv_sell<float, double, double, false, false, 3>
-                <<<spmv_grid(spmv_sell<float, double, double, false, false, 3>), kThreads, 0, s>>>(
+                <<<spmv_grid(), kThreads, 0, s>>>(
                     h.dm, static_cast<const float*>(K), x64, nullptr, mask, y64, nullptr, nullptr, nullptr);
         LPG_CUDA(cudaGetLastError());
     }
@@ -661,15 +665,25 @@ struct Solver {
 
     // Enqueues `pairs` x 2 PCG iterations on stream gs (two launches per iteration; p_new and
     // p_old swap roles every iteration).
+    template <typename R, int VAR>
+    void enqueue_iterations_v(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA,
+                              R* pB, R* Ap, PcgState* st, double* part, int pairs) {
+        const int sg = spmv_grid(0), ug = std::max(1, grid(static_cast<size_t>(V)));
+        for (int i = 0; i < pairs; ++i) {
+            spmv_sell<R, R, R, true, false, 4, VAR><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
+            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pB, Ap, V, part);
+            spmv_sell<R, R, R, true, false, 4, VAR><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pB, mask4, Ap, pA, st, part);
+            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pA, Ap, V, part);
+        }
+    }
+    // The same with the handle's tuned SpMV variant for precision R.
     template <typename R>
     void enqueue_iterations(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA,
                             R* pB, R* Ap, PcgState* st, double* part, int pairs) {
-        const int sg = spmv_grid(spmv_sell<R, R, R, true, false, 4>), ug = std::max(1, grid(static_cast<size_t>(V)));
-        for (int i = 0; i < pairs; ++i) {
-            spmv_sell<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
-            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pB, Ap, V, part);
-            spmv_sell<R, R, R, true, false, 4><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pB, mask4, Ap, pA, st, part);
-            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pA, Ap, V, part);
+        switch (h.tune.spmv[sizeof(R) == 8 ? 0 : 1]) {
+        case 1: enqueue_iterations_v<R, 1>(gs, K, dinv, mask4, x, r, z, pA, pB, Ap, st, part, pairs); break;
+        case 2: enqueue_iterations_v<R, 2>(gs, K, dinv, mask4, x, r, z, pA, pB, Ap, st, part, pairs); break;
+        default: enqueue_iterations_v<R, 0>(gs, K, dinv, mask4, x, r, z, pA, pB, Ap, st, part, pairs); break;
         }
     }
 
@@ -694,7 +708,7 @@ struct Solver {
         double* r64 = h.s_r64.as<double>(n);
         double* y64 = h.s_b64.as<double>(n);
         const int vg = vec_grid(pcg_init<R>);
-        const int pg = std::max(spmv_grid(spmv_sell<R, R, R, true, false, 4>), std::max(1, grid(static_cast<size_t>(V))));
+        const int pg = std::max(spmv_grid(), std::max(1, grid(static_cast<size_t>(V))));
         double* part = h.s_part.as<double>(std::max(4 * 1024, 2 * std::max(pg, vg)));
         PcgState* st = reinterpret_cast<PcgState*>(h.s_scal.as<double>(64));
         LPG_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), s));
@@ -706,7 +720,8 @@ struct Solver {
         constexpr int kPairs = 16;
         constexpr int kKey = 12;
         const void* key[kKey] = {Kin, dinv, mask4, x, r, z, pA, pB, Ap, st, part,
-                                 reinterpret_cast<const void*>(sizeof(R) * 1000003u + V)};
+                                 reinterpret_cast<const void*>((sizeof(R) * 1000003u + V) * 4u +
+                                                               h.tune.spmv[sizeof(R) == 8 ? 0 : 1])};
         bool same = h.pcg_graph != nullptr;
         for (int i = 0; i < kKey && same; ++i) same = h.pcg_graph_key[i] == key[i];
         cudaStream_t gs = h.own_stream;
@@ -1226,7 +1241,7 @@ __global__ void __launch_bounds__(256) pcg_b_start(BatchPcg st, const double* __
 // Ap = mask (K p) with p = z + beta[mesh] p_old formed on the fly (written to p_new), and the
 // per-row p.Ap; the sliced-ELL traversal of spmv_sell, one lane per row.
 template <typename R>
-__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<R>::value)
+__global__ void __launch_bounds__(kThreads, (SpmvCfg<R, 0>::minb))
     spmv_sell_batch(const DevMesh m, const R* __restrict__ val, const R* __restrict__ z, const R* __restrict__ p_old,
                     const R* __restrict__ mask, R* __restrict__ y, R* __restrict__ p_new, BatchPcg st,
                     const int* __restrict__ mov, double* __restrict__ rowdot) {
@@ -1250,7 +1265,7 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<R>::value)
 #pragma unroll
         for (int i = 0; i < 3; ++i) xv[i] = xz[i] + beta * xp[i];
     };
-#pragma unroll kSpmvUnroll
+#pragma unroll (SpmvCfg<R, 0>::unroll)
     for (int q = 0; q < width; ++q) {
         R xv[3];
         gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
@@ -1265,7 +1280,7 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<R>::value)
     const int b0 = __ldg(m.sell_bptr + c);
     const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
     const int2* bp = m.sell_bref + b0 + lane;
-#pragma unroll kSpmvUnroll
+#pragma unroll (SpmvCfg<R, 0>::unroll)
     for (int q = 0; q < bwidth; ++q) {
         const int2 ref = __ldg(bp + 32 * q);
         R xv[3];
@@ -1812,6 +1827,142 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
         LPG_CUDA(cudaMemcpyAsync(x_out, x, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     LPG_CUDA(cudaStreamSynchronize(s));
     if (total) *total = R;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: times each launch variant of the cluster kernel (Exact Hessian + gradient, BSR),
+// the PCG SpMV (the solvers' layout) and the eigenvalue clamp on this handle's mesh and keeps
+// the fastest per precision. Inputs: the rest state u = 0 for the first two (their cost does
+// not depend on the values), seeded symmetric 9x9 matrices for the clamp. Each timing is the
+// mean of 3 launches after one warm-up, CUDA events on the handle's stream. Variants differ in
+// register budget and unroll depth only, so the choice never changes a result.
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneTimer {
+    cudaStream_t s;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    explicit TuneTimer(cudaStream_t st) : s(st) {
+        LPG_CUDA(cudaEventCreate(&e0));
+        LPG_CUDA(cudaEventCreate(&e1));
+    }
+    ~TuneTimer() {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    // Mean ms of `launch` over 3 runs after one warm-up; `prep` runs before each, untimed.
+    template <class Prep, class Launch> double time(Prep prep, Launch launch) {
+        double total = 0;
+        for (int rep = 0; rep < 4; ++rep) {
+            prep();
+            LPG_CUDA(cudaEventRecord(e0, s));
+            launch();
+            LPG_CUDA(cudaEventRecord(e1, s));
+            LPG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            LPG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) total += ms;
+        }
+        return total / 3;
+    }
+};
+int argmin(const double* ms, int n) {
+    int best = 0;
+    for (int v = 1; v < n; ++v)
+        if (ms[v] < ms[best]) best = v;
+    return best;
+}
+
+template <typename R> void tune_spmv(lpg_fem& h, TuneTimer& tt, const double* u0, double* ms) {
+    Solver S(h);
+    const int pi = sizeof(R) == 8 ? 0 : 1;
+    const int prec = sizeof(R) == 8 ? LPG_PRECISION_F64 : LPG_PRECISION_MIXED;
+    DeviceBuffer kb, vb, stb, pb;
+    const size_t nv = h.plan.sell_values();
+    R* K = kb.as<R>(nv);
+    LPG_CUDA(cudaMemsetAsync(K, 0, nv * sizeof(R), h.stream));
+    h.eval_async(u0, nullptr, LPG_HESSIAN_EXACT, prec, kLayoutSell, K, nullptr);
+    h.take_status(); // timing only: input problems (e.g. bad theta) surface at evaluation
+    const size_t n4 = 4 * static_cast<size_t>(std::max(h.dm.V, 1));
+    R* vec = vb.as<R>(5 * n4);
+    LPG_CUDA(cudaMemsetAsync(vec, 0, 5 * n4 * sizeof(R), h.stream));
+    R *z = vec, *pA = vec + n4, *pB = vec + 2 * n4, *mask4 = vec + 3 * n4, *Ap = vec + 4 * n4;
+    PcgState* st = stb.as<PcgState>(1);
+    const int sg = S.spmv_grid();
+    double* part = pb.as<double>(static_cast<size_t>(sg) + 64);
+    auto prep = [&] { LPG_CUDA(cudaMemsetAsync(st, 0, sizeof(PcgState), h.stream)); };
+    auto run = [&](auto kern) {
+        return tt.time(prep, [&] { kern<<<sg, kThreads, 0, h.stream>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part); });
+    };
+    ms[0] = run(spmv_sell<R, R, R, true, false, 4, 0>);
+    ms[1] = run(spmv_sell<R, R, R, true, false, 4, 1>);
+    ms[2] = run(spmv_sell<R, R, R, true, false, 4, 2>);
+    h.tune.spmv[pi] = argmin(ms, kSpmvVariants);
+}
+} // namespace
+
+void autotune(lpg_fem& h) {
+    Tuning& t = h.tune;
+    for (auto& a : t.ms)
+        for (auto& b : a)
+            for (double& c : b) c = std::nan("");
+    t.cl[0] = t.cl[1] = t.spmv[0] = t.spmv[1] = t.clamp[0] = t.clamp[1] = 0;
+    const DevMesh& m = h.dm;
+    if (m.T == 0) {
+        t.tuned = true;
+        return;
+    }
+    cudaStream_t s = h.stream;
+    TuneTimer tt(s);
+    DeviceBuffer ub, gb;
+    const size_t n = 3 * static_cast<size_t>(m.V);
+    double* u0 = ub.as<double>(n);
+    double* g = gb.as<double>(n);
+    LPG_CUDA(cudaMemsetAsync(u0, 0, n * sizeof(double), s));
+    const int precs[2] = {LPG_PRECISION_F64, LPG_PRECISION_MIXED};
+    for (int pi = 0; pi < 2; ++pi) {
+        const int prec = precs[pi];
+        // Cluster kernel: E + gradient + Exact Hessian into BSR (the evaluation entry point's work).
+        {
+            DeviceBuffer hb;
+            void* H = hb.ensure(9 * static_cast<size_t>(m.nnzb) * (pi == 0 ? 8 : 4));
+            for (int v = 0; v < kClVariants; ++v) {
+                t.cl[pi] = v;
+                cudaEvent_t b = tt.e0, e = tt.e1;
+                double total = 0;
+                for (int rep = 0; rep < 4; ++rep) {
+                    h.eval_async(u0, g, LPG_HESSIAN_EXACT, prec, LPG_LAYOUT_BSR, H, nullptr, b, e);
+                    LPG_CUDA(cudaEventSynchronize(e));
+                    float ms = 0;
+                    LPG_CUDA(cudaEventElapsedTime(&ms, b, e));
+                    if (rep > 0) total += ms;
+                }
+                t.ms[0][pi][v] = total / 3;
+            }
+            h.take_status(); // timing only: input problems (e.g. bad theta) surface at evaluation
+            t.cl[pi] = argmin(t.ms[0][pi], kClVariants);
+        }
+        // PCG SpMV.
+        if (pi == 0)
+            tune_spmv<double>(h, tt, u0, t.ms[1][0]);
+        else
+            tune_spmv<float>(h, tt, u0, t.ms[1][1]);
+        // Eigenvalue clamp (FP32 only has variants) on up to 2^17 seeded matrices.
+        if (pi == 1) {
+            const int ns = std::min(m.T, 1 << 17);
+            DeviceBuffer pb, lb, cb;
+            void* proj = pb.ensure(45 * static_cast<size_t>(ns) * sizeof(float));
+            int* list = lb.as<int>(static_cast<size_t>(ns));
+            unsigned* count = cb.as<unsigned>(1);
+            const unsigned cnt = static_cast<unsigned>(ns);
+            LPG_CUDA(cudaMemcpyAsync(count, &cnt, sizeof cnt, cudaMemcpyHostToDevice, s));
+            for (int v = 0; v < kClampVariants; ++v)
+                t.ms[2][1][v] = tt.time([&] { launch_clamp_sample(prec, proj, list, ns, s); },
+                                        [&] { launch_clamp(prec, proj, list, count, ns, v, s); });
+            t.clamp[1] = argmin(t.ms[2][1], kClampVariants);
+        }
+    }
+    LPG_CUDA(cudaStreamSynchronize(s));
+    t.tuned = true;
 }
 
 } // namespace lpg

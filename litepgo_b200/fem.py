@@ -281,6 +281,38 @@ class VolumetricFemEnergyTetP1(Energy):
         N.check(N.lib.lpg_fem_set_theta(self._h, N.dptr(th), 1 if th.ndim == 2 else 0))
         self._theta = th
 
+    # ---- autotuned launch variants (no reference counterpart) ----
+    TUNING_KEYS = ("assembly_f64", "assembly_f32", "spmv_f64", "spmv_f32", "clamp_f64", "clamp_f32")
+
+    def tuning(self):
+        """The launch variants the autotuner chose for this mesh and the mean ms per launch it
+        measured: {"choice": {key: variant}, "ms": {key: [ms per variant, NaN if not timed]}}.
+        Variants differ in register budget and unrolling only, never in results."""
+        choice = np.zeros(6, dtype=np.int32)
+        ms = np.zeros(18)
+        N.check(N.lib.lpg_fem_get_tuning(self._h, N.iptr(choice), N.dptr(ms)))
+        fam = {"assembly": 0, "spmv": 1, "clamp": 2}
+        out_ms = {}
+        for key in self.TUNING_KEYS:
+            f, p = key.rsplit("_", 1)
+            base = 6 * fam[f] + 3 * (0 if p == "f64" else 1)
+            out_ms[key] = [float(v) for v in ms[base:base + 3]]
+        return {"choice": dict(zip(self.TUNING_KEYS, (int(c) for c in choice))), "ms": out_ms}
+
+    def autotune(self):
+        """Times every launch variant on this mesh again and keeps the fastest."""
+        N.check(N.lib.lpg_fem_autotune(self._h))
+        return self.tuning()
+
+    def set_tuning(self, **choice):
+        """Forces variants by key (see TUNING_KEYS), e.g. set_tuning(spmv_f32=1)."""
+        vals = np.full(6, -1, dtype=np.int32)
+        for k, v in choice.items():
+            if k not in self.TUNING_KEYS:
+                raise ValueError(f"unknown tuning key {k!r}")
+            vals[self.TUNING_KEYS.index(k)] = int(v)
+        N.check(N.lib.lpg_fem_set_tuning(self._h, N.iptr(vals)))
+
     @property
     def handle(self):
         return self._h
