@@ -26,6 +26,7 @@
  *   LPG_ENOCONV <- a solve that did not converge
  *   LPG_ECUDA   <- a CUDA runtime failure
  *   LPG_ELOGIC  <- a broken contract (std::logic_error)
+ *   LPG_EIO     <- std::runtime_error of the mesh-file readers (missing file, bad format)
  *
  * Memory: the library owns its device buffers. Array arguments carry an
  * explicit LPG_MEM_HOST / LPG_MEM_DEVICE flag. Device pointers must be device
@@ -51,7 +52,8 @@ enum lpg_status {
     LPG_EBUSY = 3,
     LPG_ENOCONV = 4,
     LPG_ECUDA = 5,
-    LPG_ELOGIC = 6
+    LPG_ELOGIC = 6,
+    LPG_EIO = 7
 };
 
 /* HessianKind (src/core/energy/scalar/energy.hpp:6-13); NONE = no Hessian. */
@@ -352,6 +354,20 @@ int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element);
  *   for an index outside the family's variants.
  */
 int lpg_fem_autotune(lpg_fem_t h);
+
+/*
+ * VEG volume-mesh files: read_veg / write_veg (src/core/mesh/io/veg.cpp; Python
+ * mesh.read_veg / mesh.write_veg, src/binding/mesh/io/veg.cpp). lpg_read_veg parses the file
+ * (*VERTICES, one *ELEMENTS section of TET or CUBIC cells, *INCLUDE, '#' comments, 0- or
+ * 1-based ids) and reports num_vertices, num_cells and cell_width (4 or 8); positions (3 per
+ * vertex) and cells (cell_width per cell, 0-based) are filled when not NULL, so a caller
+ * asks for the sizes first. File and format errors are LPG_EIO, an invalid mesh LPG_EINVAL.
+ * lpg_write_veg writes 1-based ids and 17 significant digits (exact round trip).
+ */
+int lpg_read_veg(const char* path, int* num_vertices, int* num_cells, int* cell_width, double* positions,
+                 int32_t* cells);
+int lpg_write_veg(const char* path, int num_vertices, const double* positions, int num_cells, int cell_width,
+                  const int32_t* cells);
 int lpg_fem_get_tuning(lpg_fem_t h, int32_t choice[6], double ms[18]);
 int lpg_fem_set_tuning(lpg_fem_t h, const int32_t choice[6]);
 

@@ -12,7 +12,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_lib" / "liblpg_b200.so"
 
-LPG_OK, LPG_EINVAL, LPG_EDOMAIN, LPG_EBUSY, LPG_ENOCONV, LPG_ECUDA, LPG_ELOGIC = range(7)
+LPG_OK, LPG_EINVAL, LPG_EDOMAIN, LPG_EBUSY, LPG_ENOCONV, LPG_ECUDA, LPG_ELOGIC, LPG_EIO = range(8)
 HESSIAN_NONE, HESSIAN_EXACT, HESSIAN_PROJECTED = range(3)
 PRECISION_F64, PRECISION_MIXED = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -101,6 +101,8 @@ SIGNATURES = [
     ("lpg_adjoint_rest", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _vp, _vp]),
     ("lpg_fem_set_theta", _int, [_vp, _dp, _int]),
     ("lpg_fem_autotune", _int, [_vp]),
+    ("lpg_read_veg", _int, [ctypes.c_char_p, ctypes.POINTER(_int), ctypes.POINTER(_int), ctypes.POINTER(_int), _dp, _ip]),
+    ("lpg_write_veg", _int, [ctypes.c_char_p, _int, _dp, _int, _int, _ip]),
     ("lpg_fem_get_tuning", _int, [_vp, _ip, _dp]),
     ("lpg_fem_set_tuning", _int, [_vp, _ip]),
 ]

@@ -17,7 +17,7 @@ OUT_DIR = HERE / "_lib"
 LIB = OUT_DIR / "liblpg_b200.so"
 INCLUDE = HERE.parent / "include"
 
-SOURCES = ["lpg_plan.cpp", "lpg_assemble.cu", "lpg_solve.cu", "lpg_api.cu", "lpg_noalloc.cu"]
+SOURCES = ["lpg_plan.cpp", "lpg_veg.cpp", "lpg_assemble.cu", "lpg_solve.cu", "lpg_api.cu", "lpg_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr"]
 

@@ -569,6 +569,29 @@ int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double
     });
 }
 
+int lpg_read_veg(const char* path, int* num_vertices, int* num_cells, int* cell_width, double* positions,
+                 int32_t* cells) {
+    return guarded([&] {
+        if (!path) fail(LPG_EINVAL, "lpg_read_veg: null path");
+        VegMesh m;
+        read_veg(path, m);
+        if (num_vertices) *num_vertices = m.num_vertices;
+        if (num_cells) *num_cells = m.width ? static_cast<int>(m.cells.size() / m.width) : 0;
+        if (cell_width) *cell_width = m.width;
+        if (positions) std::copy(m.positions.begin(), m.positions.end(), positions);
+        if (cells) std::copy(m.cells.begin(), m.cells.end(), cells);
+    });
+}
+
+int lpg_write_veg(const char* path, int num_vertices, const double* positions, int num_cells, int cell_width,
+                  const int32_t* cells) {
+    return guarded([&] {
+        if (!path || (num_vertices > 0 && !positions) || (num_cells > 0 && !cells))
+            fail(LPG_EINVAL, "lpg_write_veg: null argument");
+        write_veg(path, num_vertices, positions, num_cells, cell_width, cells);
+    });
+}
+
 int lpg_fem_autotune(lpg_fem_t h) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");

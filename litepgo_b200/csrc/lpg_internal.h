@@ -105,6 +105,18 @@ constexpr int kSellWindow = 128;
 constexpr int kClusterRows = LPG_CLUSTER_ROWS;
 constexpr int kClusterElems = LPG_CLUSTER_ELEMS;
 
+// VEG volume-mesh files (lpg_veg.cpp; src/core/mesh/io/veg.cpp).
+struct VegMesh {
+    int num_vertices = 0;
+    int width = 0;                 // 4 (TET) or 8 (CUBIC)
+    std::vector<double> positions; // 3 per vertex
+    std::vector<int32_t> cells;    // width per cell, 0-based
+};
+void read_veg(const std::string& path, VegMesh& mesh);
+void write_veg(const std::string& path, int V, const double* positions, int T, int width, const int32_t* cells);
+// MeshData::validate + MeshTopology checks (LPG_EINVAL).
+void validate_volume_mesh(int V, const std::vector<double>& positions, int width, const std::vector<int32_t>& cells);
+
 // Validates connectivity (mesh_topology.hpp:25-44) and builds the plan.
 void build_plan(int V, int T, const int32_t* tets, HostPlan& plan);
 // Checks the cluster plan's invariants (throws LPG_ELOGIC on a violation).

@@ -14,7 +14,8 @@ every face diagonal. The reference ships a six-tet generator
 
 import numpy as np
 
-__all__ = ["TetTopology", "make_box", "box_counts"]
+__all__ = ["TetTopology", "HexTopology", "TetMesh", "HexMesh", "read_veg", "write_veg", "make_box", "box_counts",
+           "delaunay_ball"]
 
 
 class TetTopology:
@@ -23,15 +24,16 @@ class TetTopology:
     vertices_per_cell = 4
 
     def __init__(self, num_vertices, cells):
+        k = self.vertices_per_cell
         num_vertices = int(num_vertices)
-        cells = np.ascontiguousarray(np.asarray(cells, dtype=np.int64).reshape(-1, 4))
+        cells = np.ascontiguousarray(np.asarray(cells, dtype=np.int64).reshape(-1, k))
         if num_vertices < 0:
             raise ValueError("MeshTopology requires a non-negative vertex count")
         if cells.shape[0] > np.iinfo(np.int32).max:
             raise ValueError("MeshTopology cell count exceeds the int index range")
         if cells.size:
             s = np.sort(cells, axis=1)
-            bad = np.flatnonzero((s[:, 0] < 0) | (s[:, 3] >= num_vertices))
+            bad = np.flatnonzero((s[:, 0] < 0) | (s[:, -1] >= num_vertices))
             if bad.size:
                 raise ValueError(f"MeshTopology cell {int(bad[0])} has vertex indices outside [0, num_vertices)")
             dup = np.flatnonzero((s[:, 1:] == s[:, :-1]).any(axis=1))
@@ -56,6 +58,102 @@ class TetTopology:
         if cell < 0 or cell >= self.num_cells:
             raise IndexError(f"MeshTopology::cell_vertices: cell {cell} is out of range")
         return self._cells[cell].copy()
+
+
+class HexTopology(TetTopology):
+    """Hexahedral connectivity (8 vertices per cell); read from and written to VEG files. The
+    GPU energy path takes tets only."""
+
+    vertices_per_cell = 8
+
+
+class TetMesh:
+    """Vertex positions (V, 3) with their tet connectivity: mesh.TetMesh(positions, cells)
+    (src/core/mesh/mesh_data.hpp:10-21, src/binding/mesh/mesh_data.cpp). Coordinates must be
+    finite (ValueError otherwise, as MeshData::validate)."""
+
+    _topology_type = TetTopology
+
+    def __init__(self, positions, cells):
+        positions = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        topology = cells if isinstance(cells, TetTopology) else self._topology_type(positions.shape[0], cells)
+        if topology.num_vertices != positions.shape[0] or not np.all(np.isfinite(positions)):
+            raise ValueError("MeshData requires three finite coordinates per vertex")
+        self._positions = positions
+        self._topology = topology
+
+    @property
+    def positions(self):
+        return self._positions
+
+    @property
+    def cells(self):
+        return self._topology.cells
+
+    @property
+    def topology(self):
+        return self._topology
+
+
+class HexMesh(TetMesh):
+    """Vertex positions with hexahedral connectivity (mesh.HexMesh)."""
+
+    _topology_type = HexTopology
+
+
+def read_veg(path):
+    """Reads a VEG volume mesh (mesh.read_veg, src/core/mesh/io/veg.cpp): a TetMesh for TET
+    elements, a HexMesh for CUBIC ones. Parsed by the native library; file and format errors
+    raise RuntimeError, an invalid mesh ValueError."""
+    import ctypes
+
+    from . import _native as N
+
+    p = str(path).encode()
+    V, T, W = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    N.check(N.lib.lpg_read_veg(p, ctypes.byref(V), ctypes.byref(T), ctypes.byref(W), None, None))
+    pos = np.empty((V.value, 3), dtype=np.float64)
+    cells = np.empty((T.value, W.value), dtype=np.int32)
+    N.check(N.lib.lpg_read_veg(p, ctypes.byref(V), ctypes.byref(T), ctypes.byref(W), N.dptr(pos), N.iptr(cells)))
+    return (TetMesh if W.value == 4 else HexMesh)(pos, cells)
+
+
+def write_veg(path, mesh):
+    """Writes a TetMesh or HexMesh as VEG (mesh.write_veg): 1-based ids, 17 significant
+    digits, so read_veg(write_veg(m)) reproduces m exactly."""
+    from . import _native as N
+
+    pos = np.ascontiguousarray(mesh.positions, dtype=np.float64)
+    cells = np.ascontiguousarray(mesh.cells, dtype=np.int32)
+    N.check(N.lib.lpg_write_veg(str(path).encode(), pos.shape[0], N.dptr(pos), cells.shape[0], cells.shape[1],
+                                N.iptr(cells)))
+
+
+def delaunay_ball(n_points, seed=0, radius=1.0):
+    """An unstructured tet mesh: the Delaunay tetrahedralisation (scipy.spatial) of n_points
+    seeded points in a ball (a shell of surface points plus interior points), oriented so that
+    every tet has det[X1-X0, X2-X0, X3-X0] > 0, with slivers (volume below 1e-3 of the mean)
+    removed and unreferenced vertices dropped. Returns (X, tets)."""
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    n_shell = max(4, n_points // 4)
+    d = rng.standard_normal((n_shell, 3))
+    shell = radius * d / np.linalg.norm(d, axis=1, keepdims=True)
+    inner = rng.standard_normal((n_points - n_shell, 3))
+    inner = radius * 0.95 * inner / np.linalg.norm(inner, axis=1, keepdims=True) * rng.random((inner.shape[0], 1)) ** (1 / 3)
+    P = np.vstack([shell, inner])
+    tets = Delaunay(P).simplices.astype(np.int64)
+    D = P[tets[:, 1:]] - P[tets[:, :1]]
+    det = np.einsum("ij,ij->i", D[:, 0], np.cross(D[:, 1], D[:, 2]))
+    flip = det < 0
+    tets[flip, 2], tets[flip, 3] = tets[flip, 3].copy(), tets[flip, 2].copy()
+    vol = np.abs(det) / 6
+    tets = tets[vol > 1e-3 * vol.mean()]
+    used = np.unique(tets)
+    remap = np.full(P.shape[0], -1, np.int64)
+    remap[used] = np.arange(used.size)
+    return P[used], remap[tets].astype(np.int32)
 
 
 # Local cube corners (dx, dy, dz); the tets of a cube with parity 0. Corner tets list the
