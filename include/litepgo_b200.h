@@ -337,6 +337,32 @@ int lpg_adjoint_rest(lpg_fem_t h, const double* u_star, const double* dLdu, cons
 int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element);
 
 /*
+ * Plastic field of an existing handle: VolumetricFemForceFpResponse's input
+ * (src/core/fem/assembly/volumetric_fem_force_fp_response.hpp:8-10; the reference builds the
+ * response with a new Fp per evaluation). Fp: 9 column-major values per element
+ * (fp_per_element) or 9 shared ones, host; NULL removes the plastic field (Fp = I). Checked as
+ * MultiplicativeKinematics does (finite: LPG_EINVAL; det Fp > 0: LPG_EDOMAIN). The plan, rest
+ * geometry and [lambda, mu] are kept.
+ */
+int lpg_fem_set_fp(lpg_fem_t h, const double* Fp, int fp_per_element);
+
+/*
+ * (d g / d vec Fp)^T w of VolumetricFemForceFpResponse::eval_vjp (MeshResponse::product,
+ * mesh_response.cpp:70-98, with NeoHookean::eval_d2W_dF_dFp, neo_hookean.cpp:103-128) at
+ * displacement u: per element 9 values (column-major Fp index) when per_element, else their
+ * sum over elements (9). u, w: num_dofs values (io_mem); out likewise.
+ */
+int lpg_fem_force_vjp_fp(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out);
+
+/*
+ * StaticEquilibriumResponse VJP in the plastic field (static_equilibrium_response.cpp:43-88
+ * with the Fp force response): K lambda = dL/du on the free DOFs with the Exact FP64 Hessian
+ * at u_star (as lpg_adjoint_theta), then dFp = -(dg/dFp)^T lambda, 9 per element or 9 summed.
+ */
+int lpg_adjoint_fp(lpg_fem_t h, const double* u_star, const double* dLdu, const int32_t* fixed_dofs, int num_fixed,
+                   int io_mem, int precision, double cg_tolerance, int per_element, double* dFp, double* lambda_out);
+
+/*
  * Autotuner (no reference counterpart). Three kernels come in launch variants that differ in
  * register budget and loop unrolling only, so every variant computes bitwise the same
  * results: the Exact-Hessian assembly (3 variants per precision), the PCG SpMV of the

@@ -101,6 +101,9 @@ SIGNATURES = [
     ("lpg_adjoint_rest", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _vp, _vp]),
     ("lpg_fem_set_theta", _int, [_vp, _dp, _int]),
     ("lpg_fem_autotune", _int, [_vp]),
+    ("lpg_fem_set_fp", _int, [_vp, _dp, _int]),
+    ("lpg_fem_force_vjp_fp", _int, [_vp, _vp, _vp, _int, _int, _vp]),
+    ("lpg_adjoint_fp", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _int, _vp, _vp]),
     ("lpg_read_veg", _int, [ctypes.c_char_p, ctypes.POINTER(_int), ctypes.POINTER(_int), ctypes.POINTER(_int), _dp, _ip]),
     ("lpg_write_veg", _int, [ctypes.c_char_p, _int, _dp, _int, _int, _ip]),
     ("lpg_fem_get_tuning", _int, [_vp, _ip, _dp]),

@@ -240,6 +240,7 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         // sampled B of deformation_gradient_sampling_response.hpp:24-41).
         std::vector<double> rec(12 * static_cast<size_t>(T));
         std::vector<double> fpinv(Fp ? 9 * static_cast<size_t>(T) : 0);
+        h->geo_base.assign(10 * static_cast<size_t>(T), 0.0);
         for (int e = 0; e < T; ++e) {
             double Xc[4][3];
             for (int a = 0; a < 4; ++a)
@@ -261,6 +262,8 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
             for (double g : G)
                 if (!std::isfinite(g)) fail(LPG_EINVAL, "Deformation gradient sampling: non-finite physical gradient");
             double vol = w;
+            std::copy(G, G + 9, &h->geo_base[10 * static_cast<size_t>(e)]);
+            h->geo_base[10 * static_cast<size_t>(e) + 9] = w;
             if (Fp) {
                 double P[9]; // row-major from column-major input
                 for (int i = 0; i < 3; ++i)
@@ -566,6 +569,89 @@ int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         newton_solve(*h, fixed, nfixed, f_ext, x0, io_mem, *o, x_out, res);
+    });
+}
+
+int lpg_fem_set_fp(lpg_fem_t h, const double* Fp, int fp_per_element) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        DevMesh& m = h->dm;
+        const size_t T = static_cast<size_t>(m.T);
+        std::vector<double> geo(h->geo_base);
+        std::vector<double> fpinv(Fp ? 9 * T : 0);
+        for (size_t e = 0; e < T && Fp; ++e) {
+            const double* src = Fp + (fp_per_element ? 9 * e : 0);
+            double P[9]; // row-major from column-major input
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) P[3 * i + j] = src[i + 3 * j];
+            for (double v : P)
+                if (!std::isfinite(v)) fail(LPG_EINVAL, "MultiplicativeKinematics requires finite F and Fp");
+            const double dp = det3(P);
+            if (!std::isfinite(dp) || dp <= 0) fail(LPG_EDOMAIN, "MultiplicativeKinematics requires finite det(Fp) > 0");
+            double Pi[9];
+            inv3(P, Pi);
+            double* g = &geo[10 * e];
+            double G2[9];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) G2[3 * i + j] = g[3 * i] * Pi[j] + g[3 * i + 1] * Pi[3 + j] + g[3 * i + 2] * Pi[6 + j];
+            std::copy(G2, G2 + 9, g);
+            g[9] *= dp;
+            std::copy(Pi, Pi + 9, &fpinv[9 * e]);
+        }
+        if (T > 0) {
+            double* d = h->d_vjp.as<double>(10 * T);
+            LPG_CUDA(cudaMemcpyAsync(d, geo.data(), 10 * T * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            launch_set_geometry(m, d, h->stream);
+        }
+        if (Fp) {
+            std::vector<float> f32(fpinv.begin(), fpinv.end());
+            LPG_CUDA(cudaStreamSynchronize(h->stream));
+            m.fpinv64 = upload(h->b_fpinv64, fpinv);
+            m.fpinv32 = upload(h->b_fpinv32, f32);
+        } else {
+            m.fpinv64 = nullptr;
+            m.fpinv32 = nullptr;
+        }
+        LPG_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int lpg_fem_force_vjp_fp(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
+    return guarded([&] {
+        if (!h || !out) fail(LPG_EINVAL, "lpg_fem_force_vjp_fp: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        const double* d_u = h->stage_in(u, io_mem, h->d_u, n);
+        const double* d_w = h->stage_in(w, io_mem, h->d_u2, n);
+        const size_t T = static_cast<size_t>(h->dm.T);
+        double* pe = (per_element && io_mem == LPG_MEM_DEVICE) ? out : h->d_vjp.as<double>(std::max<size_t>(9 * T, 9));
+        launch_fp_vjp(h->dm, d_u, d_w, pe, h->d_status.as<unsigned>(1), h->stream);
+        if (per_element) {
+            if (io_mem == LPG_MEM_HOST && T > 0)
+                LPG_CUDA(cudaMemcpyAsync(out, pe, 9 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            const int nb = static_cast<int>(std::min<size_t>(1024, (T + 4095) / 4096));
+            double* part = h->d_block.as<double>(std::max(9 * nb, 9));
+            double* res = io_mem == LPG_MEM_DEVICE ? out : h->d_alpha.as<double>(9);
+            launch_sum_cols9(pe, static_cast<int>(T), part, nb, res, h->stream);
+            if (io_mem == LPG_MEM_HOST)
+                LPG_CUDA(cudaMemcpyAsync(out, res, 9 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        }
+        raise_status(h->take_status());
+    });
+}
+
+int lpg_adjoint_fp(lpg_fem_t h, const double* u_star, const double* dLdu, const int32_t* fixed_dofs, int num_fixed,
+                   int io_mem, int precision, double cg_tolerance, int per_element, double* dFp, double* lambda_out) {
+    return guarded([&] {
+        if (!h || !u_star || !dLdu || !dFp) fail(LPG_EINVAL, "lpg_adjoint_fp: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        adjoint_fp(*h, u_star, dLdu, fixed_dofs, num_fixed, io_mem, precision, cg_tolerance, per_element, dFp,
+                   lambda_out);
     });
 }
 

@@ -777,16 +777,159 @@ __global__ void __launch_bounds__(256) force_vjp_kernel(const DevMesh m, const d
                 sm += wi * (ff - hf);
             }
         }
+        // With a plastic field the record's G and vol already carry Fp^-1 and det Fp.
         double dl = k.vol * k.logJ * sl, dm = k.vol * sm;
-        if (m.fpinv64) {
-            // With a plastic field the record's G and vol already carry Fp^-1 and det Fp.
-        }
         if (!isfinite(dl) || !isfinite(dm)) st |= ST_NONFINITE_OUT;
         out[2 * static_cast<size_t>(e)] = dl;
         out[2 * static_cast<size_t>(e) + 1] = dm;
     }
     st = __reduce_or_sync(0xffffffffu, st);
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// ---------------------------------------------------------------------------
+// Plastic sensitivity of the elastic force (VolumetricFemForceFpResponse,
+// volumetric_fem_force_fp_response.hpp:8-10, with NeoHookean::eval_d2W_dF_dFp,
+// neo_hookean.cpp:103-128): per element the VJP out_c = w_dV <dP/dFp_c, grad w>, c = i + 3 j the
+// column-major index of Fp. With Fe = F Fp^-1, sigma = dpsi/dFe = mu Fe + p Fe^-T, the record's
+// rows n_a = grad N_a^T Fp^-1 (so H = grad w Fp^-1 = sum_a w_a n_a^T), Q = A : H (the
+// neo-Hookean tangent: mu H + lambda (Fe^-T : H) Fe^-T - p Fe^-T H^T Fe^-T) and the record's
+// vol = w_dV det Fp, the three terms of dP = tr(Fp^-1 dFp) P + det Fp (A : dFe) Fp^-T -
+// P dFp^T Fp^-T (dFe = -Fe dFp Fp^-1) contract with grad w to
+//   out_{i+3j} = vol [ (sigma : H) Fp^-1_{ji} - (Fe^T Q Fp^-T)_{ij} - (Fp^-1 sigma^T H)_{ji} ].
+// 9 values per element; FP64.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) fp_vjp_kernel(const DevMesh m, const double* __restrict__ u,
+                                                     const double* __restrict__ w, double* out, unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int4 tv = __ldg(m.tets + e);
+        Kin<double> k;
+        st |= kinematics<double>(m, e, tv, u, k);
+        const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
+        double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}; // row-major
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double wi = __ldg(w + 3 * static_cast<size_t>(vs[a]) + i);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) H[3 * i + j] = fma(wi, k.n[a][j], H[3 * i + j]);
+            }
+        double Pi[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}; // Fp^-1, row-major
+        if (m.fpinv64)
+#pragma unroll
+            for (int t = 0; t < 9; ++t) Pi[t] = __ldg(m.fpinv64 + 9 * static_cast<size_t>(e) + t);
+        const double p = k.lam * k.logJ - k.mu;
+        const double* Fe = k.F;
+        const double* G = k.FiT;
+        double sig[9], Q[9], fh = 0, sH = 0;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            sig[t] = k.mu * Fe[t] + p * G[t];
+            fh += G[t] * H[t];
+            sH += sig[t] * H[t];
+        }
+        // Q = mu H + lambda (G : H) G - p G H^T G.
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double ghg = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) ghg += G[3 * i + a] * H[3 * b + a] * G[3 * b + j];
+                Q[3 * i + j] = k.mu * H[3 * i + j] + k.lam * fh * G[3 * i + j] - p * ghg;
+            }
+        // A1 = Fe^T Q Fp^-T, A2 = Fp^-1 sigma^T H.
+        double A1[9], A2[9], T1[9], T2[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double a = 0, b = 0;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    a += Fe[3 * t + i] * Q[3 * t + j]; // (Fe^T Q)_ij
+                    b += Pi[3 * i + t] * sig[3 * j + t]; // (Fp^-1 sigma^T)_ij
+                }
+                T1[3 * i + j] = a;
+                T2[3 * i + j] = b;
+            }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double a = 0, b = 0;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    a += T1[3 * i + t] * Pi[3 * j + t]; // (Fe^T Q Fp^-T)_ij
+                    b += T2[3 * i + t] * H[3 * t + j];  // (Fp^-1 sigma^T H)_ij
+                }
+                A1[3 * i + j] = a;
+                A2[3 * i + j] = b;
+            }
+        double* o = out + 9 * static_cast<size_t>(e);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double v = k.vol * (sH * Pi[3 * j + i] - A1[3 * i + j] - A2[3 * j + i]);
+                if (!isfinite(v)) st |= ST_NONFINITE_OUT;
+                o[i + 3 * j] = v;
+            }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// Deterministic column sums of an (n x K) row-major array: fixed contiguous chunks per block,
+// a fixed warp tree, then one thread sums the partials in order.
+template <int K>
+__global__ void __launch_bounds__(256) sum_cols_partial(const double* __restrict__ x, int n, double* partial) {
+    __shared__ double s[K][8];
+    double a[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) a[c] = 0;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * per, hi = min(n, lo + per);
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < K; ++c) a[c] += x[K * static_cast<size_t>(i) + c];
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a[c] += __shfl_xor_sync(0xffffffffu, a[c], off);
+        if ((threadIdx.x & 31) == 0) s[c][threadIdx.x >> 5] = a[c];
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double t = 0;
+        for (int w = 0; w < (blockDim.x >> 5); ++w) t += s[threadIdx.x][w];
+        partial[K * blockIdx.x + threadIdx.x] = t;
+    }
+}
+template <int K> __global__ void sum_cols_final(const double* __restrict__ partial, int nb, double* out) {
+    if (threadIdx.x < K) {
+        double t = 0;
+        for (int i = 0; i < nb; ++i) t += partial[K * i + threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+}
+
+// Writes new geometry (G, vol: the first 10 values of each record) into both precisions'
+// records, keeping each element's [lambda, mu].
+__global__ void set_geometry_kernel(const DevMesh m, const double* __restrict__ geo) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+#pragma unroll
+    for (int t = 0; t < 10; ++t) {
+        const double v = geo[10 * static_cast<size_t>(e) + t];
+        m.rec64[12 * static_cast<size_t>(e) + t] = v;
+        m.rec32[12 * static_cast<size_t>(e) + t] = static_cast<float>(v);
+    }
 }
 
 // Deterministic column sums of an (n x 2) array: partial sums per block, then one block.
@@ -1727,6 +1870,22 @@ void launch_feasible(const DevMesh& m, const double* u, const double* du, double
 void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out, unsigned* status,
                       cudaStream_t s) {
     if (m.T > 0) force_vjp_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, u, w, out, status);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_fp_vjp(const DevMesh& m, const double* u, const double* w, double* out, unsigned* status, cudaStream_t s) {
+    if (m.T > 0) fp_vjp_kernel<<<(m.T + 127) / 128, 128, 0, s>>>(m, u, w, out, status);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_sum_cols9(const double* per_elem, int T, double* partial, int nblocks, double* out9, cudaStream_t s) {
+    if (nblocks > 0) sum_cols_partial<9><<<nblocks, 256, 0, s>>>(per_elem, T, partial);
+    sum_cols_final<9><<<1, 32, 0, s>>>(partial, nblocks, out9);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_set_geometry(const DevMesh& m, const double* geo, cudaStream_t s) {
+    if (m.T > 0) set_geometry_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, geo);
     LPG_CUDA(cudaGetLastError());
 }
 

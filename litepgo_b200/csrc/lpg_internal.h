@@ -213,5 +213,10 @@ void launch_rest_vjp(const DevMesh& m, const double* u, const double* w, double*
                      unsigned* status, cudaStream_t s);
 void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cudaStream_t s);
 void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s);
+// Plastic force VJP: out (9 T, column-major per element) = (d g_e / d vec Fp_e)^T w_e.
+void launch_fp_vjp(const DevMesh& m, const double* u, const double* w, double* out, unsigned* status, cudaStream_t s);
+void launch_sum_cols9(const double* per_elem, int T, double* partial, int nblocks, double* out9, cudaStream_t s);
+// geo: 10 doubles per element (G row-major, vol) written into rec64 / rec32 (theta kept).
+void launch_set_geometry(const DevMesh& m, const double* geo, cudaStream_t s);
 
 } // namespace lpg

@@ -1060,6 +1060,39 @@ void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const i
     LPG_CUDA(cudaStreamSynchronize(s));
 }
 
+void adjoint_fp(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                int precision, double cg_tolerance, int per_element, double* dFp, double* lambda_out) {
+    const double* u = nullptr;
+    double* lam = nullptr;
+    adjoint_solve(h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, &u, &lam);
+    cudaStream_t s = h.stream;
+    const size_t T = static_cast<size_t>(h.dm.T);
+    // dFp = -(dg/dFp)^T lambda.
+    double* pe = h.d_vjp.as<double>(std::max<size_t>(9 * T, 9));
+    launch_fp_vjp(h.dm, u, lam, pe, h.d_status.as<unsigned>(1), s);
+    std::vector<double> host;
+    if (per_element) {
+        host.resize(9 * T);
+        if (T) LPG_CUDA(cudaMemcpyAsync(host.data(), pe, 9 * T * sizeof(double), cudaMemcpyDeviceToHost, s));
+    } else {
+        const int nb = static_cast<int>(std::min<size_t>(1024, (T + 4095) / 4096));
+        double* part = h.d_block.as<double>(std::max(9 * nb, 9));
+        double* res = h.d_alpha.as<double>(9);
+        launch_sum_cols9(pe, static_cast<int>(T), part, nb, res, s);
+        host.resize(9);
+        LPG_CUDA(cudaMemcpyAsync(host.data(), res, 9 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    raise_status(h.take_status());
+    for (double& v : host) v = -v;
+    if (io_mem == LPG_MEM_DEVICE) {
+        if (!host.empty()) LPG_CUDA(cudaMemcpyAsync(dFp, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    } else {
+        std::copy(host.begin(), host.end(), dFp);
+    }
+    copy_lambda(h, lam, io_mem, lambda_out);
+    LPG_CUDA(cudaStreamSynchronize(s));
+}
+
 void adjoint_rest(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                   int precision, double cg_tolerance, double* dX, double* lambda_out) {
     const double* u = nullptr;

@@ -3,6 +3,7 @@
 
 #include <atomic>
 #include <cstddef>
+#include <vector>
 
 #include "lpg_internal.h"
 
@@ -43,6 +44,7 @@ struct lpg_fem {
     // Solver state (Newton / PCG / adjoint).
     lpg::DeviceBuffer s_x, s_g, s_f, s_d, s_trial, s_mask, s_hess, s_hess64, s_dinv, s_r, s_z, s_p, s_ap, s_xcg, s_r64,
         s_b64, s_scal, s_part, s_flag, d_flush, s_p2, s_mask4;
+    std::vector<double> geo_base; // per element: G = rows of Dm^-1 (9) and w_dV, before any Fp
     lpg::Tuning tune; // autotuned launch variants (lpg::autotune)
     // CUDA graph of a chunk of PCG iterations, reused while its pointers stay the same.
     cudaGraphExec_t pcg_graph = nullptr;
@@ -68,6 +70,8 @@ void batch_newton_solve(lpg_fem& h, int num_meshes, const int32_t* vertex_offset
                         const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
                         const lpg_newton_options& o, double* x_out, lpg_batch_mesh_result* per_mesh,
                         lpg_newton_result* total);
+void adjoint_fp(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
+                int precision, double cg_tolerance, int per_element, double* dFp, double* lambda_out);
 // Times every launch variant of the tuned kernels on this handle's mesh (rest state, seeded
 // clamp inputs) and keeps the fastest per precision in h.tune.
 void autotune(lpg_fem& h);

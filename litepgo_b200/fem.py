@@ -34,6 +34,8 @@ __all__ = [
     "VolumetricFemEnergyTetP1",
     "VolumetricFemForceMaterialResponseTetP1",
     "VolumetricFemForceRestPositionResponseTetP1",
+    "VolumetricFemForceFpResponse",
+    "VolumetricFemForceFpResponseTetP1",
 ]
 
 
@@ -280,6 +282,22 @@ class VolumetricFemEnergyTetP1(Energy):
             raise ValueError("VolumetricFemEnergy: theta must have shape (2,) or (num_elements, 2)")
         N.check(N.lib.lpg_fem_set_theta(self._h, N.dptr(th), 1 if th.ndim == 2 else 0))
         self._theta = th
+
+    def set_fp(self, Fp):
+        """Replaces the plastic field in place: (9,) shared or (num_elements, 9) per element,
+        column-major vec(Fp); None (or the identity) removes it. Plan, rest geometry and theta
+        are kept (no reference counterpart: the reference builds a new energy)."""
+        if Fp is None:
+            N.check(N.lib.lpg_fem_set_fp(self._h, None, 0))
+            return
+        fp = np.ascontiguousarray(Fp, dtype=np.float64)
+        if fp.shape not in ((9,), (self.num_elements, 9)):
+            raise ValueError("VolumetricFemEnergy: Fp must have shape (9,) or (num_elements, 9)")
+        eye = np.eye(3).ravel()
+        if np.all(fp.reshape(-1, 9) == eye):
+            N.check(N.lib.lpg_fem_set_fp(self._h, None, 0))
+            return
+        N.check(N.lib.lpg_fem_set_fp(self._h, N.dptr(fp), 1 if fp.ndim == 2 else 0))
 
     # ---- autotuned launch variants (no reference counterpart) ----
     TUNING_KEYS = ("assembly_f64", "assembly_f32", "spmv_f64", "spmv_f32", "clamp_f64", "clamp_f32")
@@ -542,11 +560,77 @@ class VolumetricFemForceRestPositionResponseTetP1:
         return out
 
 
+class VolumetricFemForceFpResponseTetP1:
+    """Force response Fp -> g(u; Fp) at a fixed displacement and theta, differentiated in the
+    plastic field.
+
+    Mirrors VolumetricFemForceFpResponse[NeoHookean, TetP1Basis, TetCentroidQuadrature]
+    (src/core/fem/assembly/volumetric_fem_force_fp_response.hpp:8-10; binding
+    src/binding/fem/assembly/volumetric_fem_force_fp_response.cpp): input column-major vec(Fp),
+    one block shared (ConstantDofMap, 9 inputs) or one per element (ElementDofMap, 9 per
+    element). ``eval_value(p)`` is the elastic force (the energy gradient) with Fp = p,
+    ``eval_vjp(p, w)`` is (dg/dFp)^T w.
+    """
+
+    def __init__(self, parameter_map, displacement_map, rest_position_fields, displacement, theta, batch_size=256):
+        if isinstance(batch_size, bool) or int(batch_size) <= 0:
+            raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
+        if not isinstance(parameter_map, (ConstantDofMap, ElementDofMap)):
+            raise TypeError("parameter_map must be a ConstantDofMap or an ElementDofMap")
+        width = parameter_map.num_dofs if isinstance(parameter_map, ConstantDofMap) else parameter_map.dofs_per_element
+        if parameter_map.num_elements != displacement_map.num_elements:
+            raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
+        if width != 9:
+            raise ValueError("VolumetricFemForceResponse: invalid parameter count")
+        self.per_element = isinstance(parameter_map, ElementDofMap)
+        self.parameter_map = parameter_map
+        u = np.ascontiguousarray(displacement, dtype=np.float64)
+        if u.size != displacement_map.num_dofs or not np.all(np.isfinite(u)):
+            raise ValueError("VolumetricFemForceResponse: incompatible map, displacement or responses")
+        self._energy = VolumetricFemEnergyTetP1(displacement_map, rest_position_fields, None, theta)
+        self.displacement = u
+        self.num_inputs = parameter_map.num_dofs
+        self.num_outputs = displacement_map.num_dofs
+        self._fp = None
+
+    def _set(self, p):
+        p = np.asarray(p, dtype=np.float64).ravel()
+        if p.size != self.num_inputs:
+            raise ValueError("Response: p must have num_inputs entries")
+        if not np.all(np.isfinite(p)):
+            raise ValueError("MultiplicativeKinematics requires finite F and Fp")
+        if self._fp is None or not np.array_equal(self._fp, p):
+            self._energy.set_fp(p.reshape(-1, 9) if self.per_element else p)
+            self._fp = p.copy()
+        return p
+
+    def eval_value(self, p):
+        """The elastic force g(u; Fp = p) (num_outputs values)."""
+        self._set(p)
+        return self._energy.eval_gradient(self.displacement)
+
+    def eval_vjp(self, p, w):
+        """(d g / d Fp)^T w: (9,) for a ConstantDofMap, (9 T,) for an ElementDofMap."""
+        self._set(p)
+        wv = np.ascontiguousarray(w, dtype=np.float64)
+        if wv.size != self.num_outputs:
+            raise ValueError("Response: weights must have num_outputs entries")
+        T = self._energy.num_elements
+        out = np.empty(9 * T if self.per_element else 9)
+        N.check(N.lib.lpg_fem_set_stream(self._energy.handle, None))
+        N.check(N.lib.lpg_fem_force_vjp_fp(self._energy.handle, N.vptr(self.displacement), N.vptr(wv), N.MEM_HOST,
+                                           1 if self.per_element else 0, N.vptr(out)))
+        return out
+
+
 VolumetricFemEnergy = Template("VolumetricFemEnergy",
                                {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyTetP1})
 VolumetricFemForceMaterialResponse = Template(
     "VolumetricFemForceMaterialResponse",
     {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceMaterialResponseTetP1})
+VolumetricFemForceFpResponse = Template(
+    "VolumetricFemForceFpResponse",
+    {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceFpResponseTetP1})
 
 # A constant field helper matching the reference tests' constant_fields(value, count).
 def constant_fields(value, count):

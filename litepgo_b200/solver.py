@@ -250,8 +250,16 @@ class StaticEquilibriumResponse:
         fem, _ = _split_energy(potential)
         fixed_arr = np.ascontiguousarray(self.fixed.fixed_dofs, dtype=np.int32)
         prec = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
-        from .fem import VolumetricFemForceRestPositionResponseTetP1
+        from .fem import VolumetricFemForceFpResponseTetP1, VolumetricFemForceRestPositionResponseTetP1
 
+        if isinstance(force, VolumetricFemForceFpResponseTetP1):
+            T = fem.num_elements
+            out = np.empty(9 * T if force.per_element else 9)
+            N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
+            N.check(N.lib.lpg_adjoint_fp(fem.handle, N.vptr(x), N.vptr(w), N.iptr(fixed_arr), int(fixed_arr.size),
+                                         N.MEM_HOST, prec, float(self.adjoint_tolerance),
+                                         1 if force.per_element else 0, N.vptr(out), None))
+            return out
         if isinstance(force, VolumetricFemForceRestPositionResponseTetP1):
             out = np.empty(self.num_inputs)
             N.check(N.lib.lpg_fem_set_stream(fem.handle, None))

@@ -753,6 +753,33 @@ void force_vjp_theta(orc_mesh& m, const double* u, const double* wvec, double* o
     });
 }
 
+// VolumetricFemForceFpResponse::eval_vjp (volumetric_fem_force_fp_response.hpp:8-10 through
+// detail/volumetric_fem_force_response.hpp:155-179 and MeshResponse::product,
+// mesh_response.cpp:70-98): per element J = w B^T dP/dFp (12 x 9, dP/dFp from
+// NeoHookean::eval_d2W_dF_dFp, neo_hookean.cpp:103-128) and out_c = sum_k J(k, c) w_e[k].
+void force_vjp_fp(orc_mesh& m, const double* u, const double* wvec, double* out) {
+    for_elements(m.T, [&](int e) {
+        double c[12], we[12];
+        gather_local(m, e, u, c);
+        gather_local(m, e, wvec, we);
+        const M3 F = element_F(m, e, c);
+        double mixed[81];
+        nh_P(F, elem_Fp(m, e), elem_theta(m, e)); // stress finite check as in eval_row
+        nh_dP_dFp(F, elem_Fp(m, e), elem_theta(m, e), mixed);
+        const double* B = m.B.data() + static_cast<size_t>(e) * 108;
+        const double w = m.w[e];
+        for (int p = 0; p < 9; ++p) {
+            double s = 0;
+            for (int k = 0; k < 12; ++k) {
+                double jk = 0;
+                for (int r = 0; r < 9; ++r) jk += B[r + 9 * k] * mixed[r + 9 * p];
+                s += (w * jk) * we[k];
+            }
+            out[9 * static_cast<size_t>(e) + p] = s;
+        }
+    });
+}
+
 // Rest-position sensitivity of the force (no reference counterpart; pinned by central finite
 // differences of the force in the rest positions). Per element s = w_e . g_e = vol P : grad w;
 // with H = F - I and Q = A : grad w (A the material tangent of nh_A),
@@ -1166,6 +1193,10 @@ int orc_mesh_feasible_step(orc_mesh* m, const double* u, const double* du, doubl
 
 int orc_mesh_force_vjp_theta(orc_mesh* m, const double* u, const double* w, double* out) {
     return guarded([&] { force_vjp_theta(*m, u, w, out); });
+}
+
+int orc_mesh_force_vjp_fp(orc_mesh* m, const double* u, const double* w, double* out) {
+    return guarded([&] { force_vjp_fp(*m, u, w, out); });
 }
 
 int orc_mesh_force_vjp_rest(orc_mesh* m, const double* u, const double* w, double* out) {

@@ -83,6 +83,8 @@ int orc_mesh_force_vjp_theta(orc_mesh* m, const double* u, const double* w, doub
 /* (d g / d X)^T w for the vertex rest positions X (3V), no plastic field; restated from the
  * shape derivative of the element force (the reference has no such derivative). */
 int orc_mesh_force_vjp_rest(orc_mesh* m, const double* u, const double* w, double* out);
+/* (d g / d vec Fp)^T w per element: 9 values each (column-major Fp index). */
+int orc_mesh_force_vjp_fp(orc_mesh* m, const double* u, const double* w, double* out);
 
 /* ---- Newton (newton.cpp) over E(u) = elastic(u) - f_ext . u ---- */
 typedef struct {

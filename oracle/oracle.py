@@ -83,6 +83,7 @@ def lib():
         L.orc_mesh_feasible_step.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_mesh_force_vjp_theta.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_mesh_force_vjp_rest.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
+        L.orc_mesh_force_vjp_fp.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_newton_solve.argtypes = [ctypes.c_void_p, _c_int_p, ctypes.c_int, _c_double_p, _c_double_p,
                                        ctypes.POINTER(NewtonOptions), _c_double_p, ctypes.POINTER(NewtonResult)]
         L.orc_adjoint_theta.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_int_p, ctypes.c_int, ctypes.c_int,
@@ -244,6 +245,13 @@ class OracleMesh:
         out = np.empty((self.num_tets, 2))
         _check(lib().orc_mesh_force_vjp_theta(self._h, _dp(np.ascontiguousarray(u, float)),
                                               _dp(np.ascontiguousarray(w, float)), _dp(out)))
+        return out
+
+    def force_vjp_fp(self, u, w):
+        """(d g / d vec Fp)^T w per element, (T, 9) column-major Fp index."""
+        out = np.empty((self.num_tets, 9))
+        _check(lib().orc_mesh_force_vjp_fp(self._h, _dp(np.ascontiguousarray(u, float)),
+                                           _dp(np.ascontiguousarray(w, float)), _dp(out)))
         return out
 
     def force_vjp_rest(self, u, w):
