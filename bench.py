@@ -602,6 +602,91 @@ def run_batch():
     return 0
 
 
+def run_rows():
+    """The widened rows on the bench mesh (64^3 gravity box): the plastic-field force VJP kernel
+    (per element, device arrays) with its algorithmic bytes, the equilibrium adjoint in Fp, and
+    VEG write / read of the mesh. Prints one JSON line."""
+    import tempfile
+
+    import scipy.sparse as sp
+    import torch
+
+    from litepgo_b200 import _native as N
+    from litepgo_b200 import dof, energy, fem, mesh, solver, workloads
+
+    torch.cuda.set_device(0)
+    g = workloads.gravity_box(N_CUBES, seed=0)
+    X, tets, theta = g["X"], g["tets"], g["theta"]
+    T, V, n = tets.shape[0], X.shape[0], X.size
+    rng = np.random.default_rng(21)
+    Fp = np.stack([(np.eye(3) + 0.02 * rng.standard_normal((3, 3))).T.ravel() for _ in range(T)])
+    e = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta, Fp=Fp)
+    dev = torch.device("cuda", 0)
+    u = torch.as_tensor(state(X), device=dev)
+    w = torch.as_tensor(rng.standard_normal(n), device=dev)
+    out = torch.empty(9 * T, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    N.check(N.lib.lpg_fem_set_stream(e.handle, ctypes.c_void_p(stream.cuda_stream)))
+
+    def vjp():
+        N.check(N.lib.lpg_fem_force_vjp_fp(e.handle, N.vptr(u), N.vptr(w), N.MEM_DEVICE, 1, N.vptr(out)))
+
+    for _ in range(3):
+        vjp()
+    k = 20
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(k):
+        vjp()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / k
+    # Per element: tet indices 16, FP64 record 96, Fp^-1 72, 9 outputs 72; per vertex u and w.
+    fp_bytes = T * (16 + 96 + 72 + 72) + V * 48
+    peak, _ = measured_peak()
+    fp_row = {"call_ms": ms, "tets_per_s": T / (ms * 1e-3), "algorithmic_bytes": fp_bytes,
+              "achieved_gbs": fp_bytes / (ms * 1e-3) / 1e9, "frac_of_measured_hbm": fp_bytes / (ms * 1e-3) / 1e9 / peak,
+              "timing": "CUDA events around 20 synchronous lpg_fem_force_vjp_fp calls (device arrays; each call "
+                        "ends with its status read-back); working set ~350 MB > L2"}
+    # Equilibrium adjoint in Fp at the gravity equilibrium of the plastic box.
+    N.check(N.lib.lpg_fem_set_stream(e.handle, None))
+    load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -g["f"])
+    total = energy.WeightedSumEnergy([(e, 1.0), (load, 1.0)])
+    fixed = dof.DofReduction(n, g["fixed"])
+    opts = solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", accept_rule="armijo",
+                                max_iterations=100, cg_tolerance=1e-2, exact_below=1e-3)
+    r = solver.newton_solve(total, fixed, np.zeros(n), opts)
+    x = np.asarray(r.x)
+    dLdx = rng.standard_normal(n)
+    fixed_arr = np.ascontiguousarray(g["fixed"], dtype=np.int32)
+    dFp = np.empty(9 * T)
+    adj = {}
+    for prec, name in ((N.PRECISION_F64, "f64"), (N.PRECISION_MIXED, "mixed")):
+        t0 = time.perf_counter()
+        N.check(N.lib.lpg_adjoint_fp(e.handle, N.vptr(x), N.vptr(dLdx), N.iptr(fixed_arr), int(fixed_arr.size),
+                                     N.MEM_HOST, prec, 1e-10, 1, N.vptr(dFp), None))
+        adj[name] = {"seconds": time.perf_counter() - t0, "norm": float(np.linalg.norm(dFp))}
+    # VEG write / read of the mesh.
+    with tempfile.TemporaryDirectory() as d:
+        path = Path(d) / "box64.veg"
+        t0 = time.perf_counter()
+        mesh.write_veg(path, mesh.TetMesh(X, tets))
+        tw = time.perf_counter() - t0
+        size = path.stat().st_size
+        t0 = time.perf_counter()
+        back = mesh.read_veg(path)
+        tr = time.perf_counter() - t0
+        exact = bool(np.array_equal(back.positions, X) and np.array_equal(back.cells, tets))
+    line = {"rows": "plastic-field force VJP, adjoint in Fp, VEG I/O", "config": workload_config(),
+            "fp_vjp": fp_row, "newton_with_fp": {"status": r.status.name, "iterations": r.iterations, "seconds": r.seconds},
+            "adjoint_fp": adj,
+            "veg": {"bytes": size, "write_s": tw, "read_s": tr, "read_mb_per_s": size / tr / 1e6,
+                    "write_mb_per_s": size / tw / 1e6, "round_trip_exact": exact}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -617,9 +702,13 @@ def main():
     ap.add_argument("--newton-iterations", type=int, default=2)
     ap.add_argument("--stress", action="store_true",
                     help="run the 128^3 compression stress case (errors, assembly GB/s, Newton) and exit")
+    ap.add_argument("--rows", action="store_true",
+                    help="time the plastic-field VJP, the adjoint in Fp and VEG I/O on the bench mesh and exit")
     ap.add_argument("--batch", action="store_true",
                     help="run the 256-mesh batched Newton (meshes/s, per-mesh p50/p99) and exit")
     args = ap.parse_args()
+    if args.rows:
+        return run_rows()
     if args.batch:
         return run_batch()
     if args.stress:

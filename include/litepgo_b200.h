@@ -387,7 +387,9 @@ int lpg_fem_autotune(lpg_fem_t h);
  * (*VERTICES, one *ELEMENTS section of TET or CUBIC cells, *INCLUDE, '#' comments, 0- or
  * 1-based ids) and reports num_vertices, num_cells and cell_width (4 or 8); positions (3 per
  * vertex) and cells (cell_width per cell, 0-based) are filled when not NULL, so a caller
- * asks for the sizes first. File and format errors are LPG_EIO, an invalid mesh LPG_EINVAL.
+ * asks for the sizes first (that call keeps the parsed mesh for the next call on the same
+ * thread with the same, unchanged file, which then does not parse it again). File and format
+ * errors are LPG_EIO, an invalid mesh LPG_EINVAL.
  * lpg_write_veg writes 1-based ids and 17 significant digits (exact round trip).
  */
 int lpg_read_veg(const char* path, int* num_vertices, int* num_cells, int* cell_width, double* positions,

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <memory>
 #include <string>
 #include <vector>
@@ -659,8 +660,26 @@ int lpg_read_veg(const char* path, int* num_vertices, int* num_cells, int* cell_
                  int32_t* cells) {
     return guarded([&] {
         if (!path) fail(LPG_EINVAL, "lpg_read_veg: null path");
+        // A sizes-only call keeps the parsed mesh for the next call on this thread with the same
+        // path (and unchanged file), so the usual two calls parse the file once.
+        thread_local std::string cached_key;
+        thread_local VegMesh cached;
+        std::error_code ec;
+        const auto stamp = std::filesystem::last_write_time(path, ec);
+        const auto bytes = std::filesystem::file_size(path, ec);
+        const std::string key = std::string(path) + '\n' + std::to_string(stamp.time_since_epoch().count()) + '\n' +
+                                std::to_string(ec ? 0 : bytes);
         VegMesh m;
-        read_veg(path, m);
+        if (!ec && key == cached_key) {
+            m = std::move(cached);
+            cached_key.clear();
+        } else {
+            read_veg(path, m);
+        }
+        if (!positions && !cells && !ec) {
+            cached = m;
+            cached_key = key;
+        }
         if (num_vertices) *num_vertices = m.num_vertices;
         if (num_cells) *num_cells = m.width ? static_cast<int>(m.cells.size() / m.width) : 0;
         if (cell_width) *cell_width = m.width;

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <filesystem>
 #include <fstream>
+#include <iterator>
 #include <limits>
 #include <string>
 #include <type_traits>
@@ -42,20 +43,27 @@ void load_lines(const fs::path& path, std::vector<fs::path>& chain, std::vector<
     const fs::path key = fs::weakly_canonical(path);
     for (const fs::path& p : chain)
         if (p == key) io_fail("veg *INCLUDE cycle through " + path.string());
-    std::ifstream in(path);
+    std::ifstream in(path, std::ios::binary);
     if (!in) io_fail("Failed to open veg file: " + path.string());
     chain.push_back(key);
-    std::string raw;
-    while (std::getline(in, raw)) {
-        const std::string line = strip(raw);
-        if (line.empty() || line[0] == '#') continue;
+    std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    if (in.bad()) io_fail("Failed reading VEG: " + path.string());
+    size_t pos = 0;
+    while (pos < text.size()) {
+        size_t eol = text.find('\n', pos);
+        if (eol == std::string::npos) eol = text.size();
+        size_t a = pos, b = eol;
+        while (a < b && (text[a] == ' ' || text[a] == '\t' || text[a] == '\r')) ++a;
+        while (b > a && (text[b - 1] == ' ' || text[b - 1] == '\t' || text[b - 1] == '\r')) --b;
+        pos = eol + 1;
+        if (a == b || text[a] == '#') continue;
+        std::string line(text, a, b - a);
         if (line.compare(0, 9, "*INCLUDE ") == 0) {
             load_lines(path.parent_path() / strip(line.substr(9)), chain, out);
             continue;
         }
-        out.push_back(line);
+        out.push_back(std::move(line));
     }
-    if (in.bad()) io_fail("Failed reading VEG: " + path.string());
     chain.pop_back();
 }
 
@@ -71,16 +79,16 @@ template <class T> bool fields(const std::string& line, std::vector<T>& out) {
         if (i >= n) break;
         size_t j = i;
         while (j < n && !sep(line[j])) ++j;
-        const std::string tok = line.substr(i, j - i);
+        // Parse in place; the number must end exactly where the field ends.
+        const char* beg = line.c_str() + i;
         char* end = nullptr;
         if constexpr (std::is_same<T, double>::value) {
-            const double v = std::strtod(tok.c_str(), &end);
-            if (end != tok.c_str() + tok.size()) return false;
+            const double v = std::strtod(beg, &end);
+            if (end != line.c_str() + j) return false;
             out.push_back(v);
         } else {
-            const long long v = std::strtoll(tok.c_str(), &end, 10);
-            if (end != tok.c_str() + tok.size() || v < std::numeric_limits<int>::min() ||
-                v > std::numeric_limits<int>::max())
+            const long long v = std::strtoll(beg, &end, 10);
+            if (end != line.c_str() + j || v < std::numeric_limits<int>::min() || v > std::numeric_limits<int>::max())
                 return false;
             out.push_back(static_cast<T>(v));
         }
