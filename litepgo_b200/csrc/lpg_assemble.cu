@@ -983,6 +983,45 @@ __global__ void sum_pairs_final(const double* __restrict__ partial, int nb, doub
 // positive definite, else by cyclic Jacobi (Golub & Van Loan, Alg. 8.5.3). The result is
 // stored packed (45 values per element) for the assembly kernel.
 // ---------------------------------------------------------------------------
+// Index of the unordered vertex pair (a, b) of a tet among its 10.
+__host__ __device__ constexpr int pair10(int a, int b) {
+    return (a < b ? a : b) * 4 - ((a < b ? a : b) * ((a < b ? a : b) - 1)) / 2 + ((a < b ? b : a) - (a < b ? a : b));
+}
+
+// The element's ten 3x3 blocks H_ab (a <= b, pair10 order, row-major) from its 9x9 tangent M in
+// the orthonormal basis q (packed upper triangle, index 3 j' + i):
+//   H_ab(i, k) = sum_{j', l'} q_a(j') q_b(l') M(3 j' + i, 3 l' + k),
+// as Y_a(i, c) = sum_j' q_a(j') M(3 j' + i, c), then H_ab(i, k) = sum_l' q_b(l') Y_a(i, 3 l' + k).
+// MA is any array-like of 45 values (registers or shared memory); out receives 90 values.
+template <typename R, typename MA> __device__ __forceinline__ void blocks_from_q(const MA& Mq, R* __restrict__ out) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        R Y[3][9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                R y = 0;
+#pragma unroll
+                for (int jp = 0; jp < 3; ++jp) y = fma(qbasis<R>(a, jp), static_cast<R>(Mq[sym9(3 * jp + i, c)]), y);
+                Y[i][c] = y;
+            }
+#pragma unroll
+        for (int b = a; b < 4; ++b) {
+            R* o = out + 9 * pair10(a, b);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                    R h = 0;
+#pragma unroll
+                    for (int lp = 0; lp < 3; ++lp) h = fma(qbasis<R>(b, lp), Y[i][3 * lp + kk], h);
+                    o[3 * i + kk] = h;
+                }
+        }
+    }
+}
+
 constexpr int kProjThreads = 64;
 constexpr int kProjStride = 127; // 45 (M) + 81 (V) + 1: odd stride, conflict-free 8-byte lanes
 
@@ -1082,9 +1121,13 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
         // Semi-definite (or kept exact): final. Otherwise the unclamped tangent is stored and
         // the element is listed for clamp_kernel, which runs the eigenvalue clamp on the listed
         // elements only (a warp of pass 1 then never waits on another lane's Jacobi sweeps).
-        R* out = proj + 45 * static_cast<size_t>(e);
-        for (int t = 0; t < 45; ++t) out[t] = A[t];
-        if (!pd && !keep) list[atomicAdd(count, 1u)] = e;
+        R* out = proj + kProjRecord * static_cast<size_t>(e);
+        if (pd || keep) {
+            blocks_from_q<R>(A, out);
+        } else {
+            for (int t = 0; t < 45; ++t) out[t] = A[t]; // the clamp reads M here and writes the blocks
+            list[atomicAdd(count, 1u)] = e;
+        }
     }
     st = __reduce_or_sync(0xffffffffu, st);
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
@@ -1231,8 +1274,7 @@ __device__ __forceinline__ void clamp9(R* __restrict__ out, VA& V) {
             for (int c = r; c < 9; ++c) A[sym9(r, c)] += lr * col[c];
         }
     }
-#pragma unroll
-    for (int k = 0; k < 45; ++k) out[k] = A[k];
+    blocks_from_q<R>(A, out); // the clamped M's ten blocks replace M in the element's record
 }
 
 constexpr int kClampVStride = 81;
@@ -1253,7 +1295,7 @@ __global__ void __launch_bounds__(kProjThreads, MINB) clamp_kernel(R* __restrict
                                                                    const unsigned* __restrict__ count) {
     const unsigned n = *count;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        R* out = proj + 45 * static_cast<size_t>(list[i]);
+        R* out = proj + kProjRecord * static_cast<size_t>(list[i]);
         if constexpr (sizeof(R) == 8) {
             extern __shared__ __align__(16) unsigned char smem_raw[];
             // volatile: every access goes to shared memory (cached copies would need the
@@ -1278,7 +1320,7 @@ template <typename R> __global__ void clamp_sample_kernel(R* __restrict__ proj, 
         z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
         z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
         z ^= z >> 31;
-        proj[45 * static_cast<size_t>(e) + t] = static_cast<R>(static_cast<double>(z >> 11) * 0x1.0p-52 - 1.0);
+        proj[kProjRecord * static_cast<size_t>(e) + t] = static_cast<R>(static_cast<double>(z >> 11) * 0x1.0p-52 - 1.0);
     }
 }
 
@@ -1315,17 +1357,16 @@ template <typename R> constexpr int cl_minb(int v) {
                           : (v == 0 ? LPG_CLUSTER_MIN_BLOCKS_F32 : v == 1 ? 4 : 8);
 }
 
-// Index of the unordered vertex pair (a, b) of a tet among its 10.
-__device__ __forceinline__ int pair10(int a, int b) {
-    const int lo = min(a, b), hi = max(a, b);
-    return lo * 4 - (lo * (lo - 1)) / 2 + (hi - lo);
-}
 
 // Shared memory of the cluster kernel: energy partials, per-element data, the row table, and
 // the cluster's slot words and contributor lists (sized by the mesh's largest cluster).
 template <typename R, bool WG, bool WH> constexpr size_t cl_smem_fixed() {
     return 32 * sizeof(double) + sizeof(R) * static_cast<size_t>(kClusterElems) * ((WH ? 24 : 0) + (WG ? 12 : 0)) +
            5 * kClusterRows * sizeof(int);
+}
+// Fixed shared memory of the block gather: element ids and a 4-column row table.
+constexpr size_t block_gather_fixed() {
+    return (static_cast<size_t>(kClusterElems) + 4 * kClusterRows) * sizeof(int);
 }
 template <typename R, bool WG, bool WH> size_t cl_smem_bytes(const DevMesh& m) {
     const size_t slots = (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16;
@@ -1583,6 +1624,110 @@ void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------
+// Hessian assembly from per-element blocks (the projected Hessian: each element's clamped
+// tangent as ten 3x3 blocks in a.proj, pair10 order). The cluster plan of the Exact path without
+// its element pass: one thread block per cluster stages the cluster's element ids, slot words and
+// contributor lists, then each thread sums one block slot's contributors in ascending element
+// order and stores the block once, in the lower vertex's orientation (transposed for the other),
+// so the result is bitwise symmetric and deterministic. Contributor (a, b) = local indices of the
+// lower- and higher-numbered vertex; the stored block is H_{min(a,b) max(a,b)}, read transposed
+// when a > b.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh m, const EvalArgs a) {
+    using HT = typename HOut<R>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int* sel = reinterpret_cast<int*>(smem_raw); // [kClusterElems] element ids
+    int* rt = sel + kClusterElems;               // [4][kClusterRows] row table
+    uint32_t* sslot = reinterpret_cast<uint32_t*>(rt + 4 * kClusterRows);
+    uint32_t* sslote = sslot + m.cl_max_slots;
+    uint16_t* sent = reinterpret_cast<uint16_t*>(smem_raw + block_gather_fixed() +
+                                                 (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16);
+    const R* blocks = reinterpret_cast<const R*>(a.proj);
+    HT* hout = reinterpret_cast<HT*>(a.hess);
+    const int tid = threadIdx.x, bd = blockDim.x;
+    unsigned st = 0;
+    for (int cl = blockIdx.x; cl < m.ncl; cl += gridDim.x) {
+        const int s0 = __ldg(m.cl_slot_ptr + cl), ns = __ldg(m.cl_slot_ptr + cl + 1) - s0;
+        const int eb = __ldg(m.cl_ent_ptr + cl), n16 = (__ldg(m.cl_ent_ptr + cl + 1) - eb) / 8;
+        for (int i = tid; i < ns; i += bd) {
+            __pipeline_memcpy_async(sslot + i, m.cl_slot + s0 + i, 4);
+            __pipeline_memcpy_async(sslote + i, m.cl_slot_ent + s0 + i, 4);
+        }
+        for (int i = tid; i < n16; i += bd)
+            __pipeline_memcpy_async(reinterpret_cast<uint4*>(sent) + i, reinterpret_cast<const uint4*>(m.cl_ents + eb) + i, 16);
+        __pipeline_commit();
+        const int e0 = __ldg(m.cl_el_ptr + cl), ne = __ldg(m.cl_el_ptr + cl + 1) - e0;
+        for (int el = tid; el < ne; el += bd) sel[el] = static_cast<int>(__ldg(m.cl_els + e0 + el) & 0x7fffffffu);
+        const int r0 = __ldg(m.cl_row_ptr + cl), nr = __ldg(m.cl_row_ptr + cl + 1) - r0;
+        for (int j = tid; j < nr; j += bd) {
+            const int v = __ldg(m.cl_rows + r0 + j);
+            const int sb = __ldg(m.row_ptr + v);
+            rt[j] = sb;
+            rt[kClusterRows + j] = __ldg(m.row_ptr + v + 1) - sb;
+            if (a.layout == kLayoutSell) rt[2 * kClusterRows + j] = __ldg(m.sell_base + v) - 288 * (__ldg(m.diag_slot + v) - sb);
+        }
+        __pipeline_wait_prior(0);
+        __syncthreads();
+        // The solver layout skips the slots left of the diagonal.
+        const int first = a.layout == kLayoutSell ? __ldg(m.cl_ntr + cl) : 0;
+        for (int s = first + tid; s < ns; s += bd) {
+            const uint32_t d = sslot[s], de = sslote[s];
+            const int j = d & 0xffu, q = (d >> 8) & 0x3fffffu;
+            const uint16_t* en = sent + (de & 0xfffffu);
+            const int cnt = static_cast<int>(de >> 20);
+            R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int c = 0; c < cnt; ++c) {
+                const int w = en[c];
+                const int el = w >> 4, la = (w >> 2) & 3, lb = w & 3;
+                const R* blk = blocks + kProjRecord * static_cast<size_t>(sel[el]) + 9 * pair10(la, lb);
+                R bv[9];
+#pragma unroll
+                for (int t = 0; t < 9; ++t) bv[t] = __ldg(blk + t);
+                if (la <= lb) {
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) acc[t] += bv[t];
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) acc[t] += bv[3 * (t % 3) + t / 3];
+                }
+            }
+            const bool tr = (d >> 30) & 1u;
+            const int slot0 = rt[j], nb = rt[kClusterRows + j], sb = rt[2 * kClusterRows + j];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const R val = tr ? acc[3 * (t % 3) + t / 3] : acc[t];
+                if (!(val == val) || val == R(INFINITY) || val == R(-INFINITY)) st |= ST_NONFINITE_OUT;
+                hout[cl_pos(a.layout, slot0, nb, sb, q, t)] = static_cast<HT>(val);
+            }
+        }
+        __syncthreads(); // the next cluster reuses the shared tables
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((tid & 31) == 0 && st) atomicOr(a.status, st);
+}
+
+template <typename R> void launch_block_gather(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    const size_t sm = block_gather_fixed() + (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16 +
+                      2 * static_cast<size_t>(m.cl_max_ents);
+    thread_local size_t cached_sm = 0;
+    thread_local int resident = 0;
+    if (cached_sm != sm) {
+        int dev = 0, sms = 0, per_sm = 0;
+        LPG_CUDA(cudaGetDevice(&dev));
+        LPG_CUDA(cudaFuncSetAttribute(block_gather_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sm)));
+        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, block_gather_kernel<R>, kClThreads, sm));
+        resident = std::max(1, sms * std::max(per_sm, 1));
+        cached_sm = sm;
+    }
+    const int blocks = std::min(resident, m.ncl);
+    if (blocks > 0) block_gather_kernel<R><<<blocks, kClThreads, sm, s>>>(m, a);
+    LPG_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
 // Rest-position sensitivity of the elastic force. For one element with s = w . g_e =
 // vol P : grad w (grad w = sum_a w_a grad N_a^T, H = F - I, Q = dP/dF [grad w] =
 // mu grad w + lambda (F^-T : grad w) F^-T - p F^-T grad w^T F^-T):
@@ -1743,12 +1888,26 @@ template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const Eva
     const bool wg = a.grad != nullptr;
     const int wh = a.hess == nullptr ? 0 : (hessian == LPG_HESSIAN_EXACT ? 1 : 2);
     int units = m.ncl;
-    if (wg && wh == 1) launch_cluster_variant<R, true>(m, a, s);
-    else if (wg && wh == 2) launch_chunks<R, true, 2>(m, a, s), units = m.ntiles;
-    else if (!wg && wh == 1) launch_cluster_variant<R, false>(m, a, s);
-    else if (!wg && wh == 2) launch_chunks<R, false, 2>(m, a, s), units = m.ntiles;
-    else if (wg) launch_cluster<R, true, false>(m, a, s);
-    else launch_cluster<R, false, false>(m, a, s);
+    if (wh == 2) {
+        // Projected: energy (and gradient) from the element pass, the Hessian gathered from the
+        // per-element clamped blocks; the optional events bracket both kernels.
+        EvalArgs ea = a;
+        ea.ev_end = nullptr;
+        if (wg)
+            launch_cluster<R, true, false>(m, ea, s);
+        else
+            launch_cluster<R, false, false>(m, ea, s);
+        launch_block_gather<R>(m, a, s);
+        if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
+    } else if (wg && wh == 1) {
+        launch_cluster_variant<R, true>(m, a, s);
+    } else if (!wg && wh == 1) {
+        launch_cluster_variant<R, false>(m, a, s);
+    } else if (wg) {
+        launch_cluster<R, true, false>(m, a, s);
+    } else {
+        launch_cluster<R, false, false>(m, a, s);
+    }
     if (wg && m.num_unused > 0)
         zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
     return units;
@@ -1781,7 +1940,7 @@ void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cu
 }
 
 size_t project_bytes(const DevMesh& m, int precision) {
-    return static_cast<size_t>(m.T) * 45 * (precision == LPG_PRECISION_F64 ? sizeof(double) : sizeof(float));
+    return static_cast<size_t>(m.T) * kProjRecord * (precision == LPG_PRECISION_F64 ? sizeof(double) : sizeof(float));
 }
 
 namespace {

@@ -202,6 +202,9 @@ void launch_clamp(int precision, void* proj, const int* list, const unsigned* co
 // list[i] = i (autotuner timing input for the clamp).
 void launch_clamp_sample(int precision, void* proj, int* list, int n, cudaStream_t s);
 size_t project_bytes(const DevMesh& m, int precision);
+// Values per element of the projected-Hessian scratch: the element's ten 3x3 blocks (pair10
+// order), or, for an element listed for the clamp until it is clamped, its 9x9 tangent (45).
+constexpr int kProjRecord = 90;
 // per_elem (T doubles, optional) receives each element's step.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
                      double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr);

@@ -1983,7 +1983,7 @@ void autotune(lpg_fem& h) {
         if (pi == 1) {
             const int ns = std::min(m.T, 1 << 17);
             DeviceBuffer pb, lb, cb;
-            void* proj = pb.ensure(45 * static_cast<size_t>(ns) * sizeof(float));
+            void* proj = pb.ensure(kProjRecord * static_cast<size_t>(ns) * sizeof(float));
             int* list = lb.as<int>(static_cast<size_t>(ns));
             unsigned* count = cb.as<unsigned>(1);
             const unsigned cnt = static_cast<unsigned>(ns);
