@@ -92,13 +92,6 @@ int lpg_mesh_pattern_bsr(int num_vertices, int num_tets, const int32_t* tets, in
                          int32_t* col_idx);
 
 /*
- * Host-only summary of the assembly plan: out[0] nnzb, out[1] (row, element) pairs,
- * out[2] warp tiles, out[3] pairs per tile capacity, out[4] most rows in one tile,
- * out[5] contributor entries (4 per pair).
- */
-int lpg_mesh_plan_summary(int num_vertices, int num_tets, const int32_t* tets, int64_t out[6]);
-
-/*
  * Host-only summary of the vertex clusters of the element-once assembly (no reference
  * counterpart; it replaces the per-column contribution lists of EnergyAssembler,
  * src/core/dof/energy_assembler.cpp:49-68, for the Exact Hessian): out[0] clusters,

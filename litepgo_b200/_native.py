@@ -76,7 +76,6 @@ SIGNATURES = [
     ("lpg_abi_version", _int, []),
     ("lpg_build_info", _int, [ctypes.c_char_p, ctypes.c_size_t]),
     ("lpg_mesh_pattern_bsr", _int, [_int, _int, _ip, _i64p, _ip, _ip]),
-    ("lpg_mesh_plan_summary", _int, [_int, _int, _ip, _i64p]),
     ("lpg_mesh_cluster_summary", _int, [_int, _int, _ip, _i64p]),
     ("lpg_fem_create", _int, [_int, _dp, _int, _ip, _dp, _dp, _int, _dp, _int, ctypes.POINTER(_vp)]),
     ("lpg_fem_destroy", _int, [_vp]),

@@ -140,8 +140,8 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.grad = dgrad;
     a.hess = hessian != LPG_HESSIAN_NONE ? dhess : nullptr;
     a.layout = layout;
-    // Per-tile (or per-cluster) energies, then partial sums.
-    a.tile_energy = d_tile_energy.as<double>(static_cast<size_t>(std::max(dm.ntiles, dm.ncl)) + 256);
+    // Per-cluster energies, then partial sums.
+    a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(dm.ncl) + 256);
     a.energy = d_energy.as<double>(1);
     a.elem_energy = delem;
     a.status = d_status.as<unsigned>(1);
@@ -182,22 +182,6 @@ int lpg_mesh_pattern_bsr(int V, int T, const int32_t* tets, int64_t* nnzb, int32
         if (nnzb) *nnzb = p.nnzb();
         if (row_ptr) std::copy(p.row_ptr.begin(), p.row_ptr.end(), row_ptr);
         if (col_idx) std::copy(p.col_idx.begin(), p.col_idx.end(), col_idx);
-    });
-}
-
-int lpg_mesh_plan_summary(int V, int T, const int32_t* tets, int64_t out[6]) {
-    return guarded([&] {
-        if (T > 0 && !tets) fail(LPG_EINVAL, "lpg_mesh_plan_summary: null tets");
-        HostPlan p;
-        build_plan(V, T, tets, p);
-        int max_rows = 0;
-        for (int t = 0; t < p.ntiles(); ++t) max_rows = std::max(max_rows, p.tile_row_ptr[t + 1] - p.tile_row_ptr[t]);
-        out[0] = p.nnzb();
-        out[1] = static_cast<int64_t>(p.pair_elem.size());
-        out[2] = p.ntiles();
-        out[3] = p.cap;
-        out[4] = max_rows;
-        out[5] = static_cast<int64_t>(p.contrib.size());
     });
 }
 
@@ -295,22 +279,13 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         DevMesh& m = h->dm;
         m.V = V;
         m.T = T;
-        m.ntiles = p.ntiles();
-        m.cap = p.cap;
         m.nnzb = p.nnzb();
         m.row_ptr = upload(h->b_row_ptr, p.row_ptr);
         m.col_idx = upload(h->b_col_idx, p.col_idx);
         m.inc_ptr = upload(h->b_inc_ptr, p.inc_ptr);
-        m.tile_pair_ptr = upload(h->b_tile_pair_ptr, p.tile_pair_ptr);
-        m.tile_row_ptr = upload(h->b_tile_row_ptr, p.tile_row_ptr);
-        m.tile_rows = upload(h->b_tile_rows, p.tile_rows);
-        m.tile_slot_ptr = upload(h->b_tile_slot_ptr, p.tile_slot_ptr);
-        m.slot_desc = upload(h->b_slot_desc, p.slot_desc);
         m.diag_slot = upload(h->b_diag_slot, p.diag_slot);
         m.unused_rows = upload(h->b_unused, p.unused_rows);
         m.num_unused = static_cast<int>(p.unused_rows.size());
-        m.contrib = upload(h->b_contrib, p.contrib);
-        m.pair_elem = upload(h->b_pair_elem, p.pair_elem);
         m.sell_ptr = upload(h->b_sell[0], p.sell_ptr);
         m.sell_row = upload(h->b_sell[1], p.sell_row);
         m.sell_col = upload(h->b_sell[2], p.sell_col);

@@ -11,12 +11,13 @@
 // which equals vol * B^T (d2W/dF2) B for B = kron(grad N^T, I3).
 //
 // Assembly (replacing EnergyAssembler::assemble, src/core/dof/energy_assembler.cpp:123-170)
-// is fused and atomic-free: one warp owns a tile of whole block rows; each lane evaluates one
-// (row vertex, incident element) pair and leaves its four 3x3 blocks in shared memory; the
-// warp then sums every block slot of its rows over the slot's contributor list, which is in
-// ascending element order (the reference's per-column order, energy_assembler.cpp:49-54).
-// Block entries are formed with explicit round-to-nearest products so that H_ba is the exact
-// transpose of H_ab; the assembled matrix is bitwise symmetric.
+// is atomic-free over vertex clusters: a thread block evaluates the elements incident to its
+// cluster of rows once, then sums every block slot of those rows over the slot's contributor
+// list, in ascending element order (the reference's per-column order,
+// energy_assembler.cpp:49-54). An off-diagonal block is summed in the orientation of its
+// lower-numbered vertex and stored transposed for the other, so the assembled matrix is
+// bitwise symmetric. The projected Hessian goes through per-element blocks (project_kernel,
+// clamp_kernel) gathered by the same cluster plan (block_gather_kernel).
 
 #include <algorithm>
 #include <cstdint>
@@ -28,23 +29,6 @@
 
 namespace lpg {
 namespace {
-
-constexpr int kWarpsPerBlock = 4;
-
-// Occupancy targets of the assembly kernel (resident blocks per SM the register allocation must
-// allow) and whether its warps persist over several tiles; tuned per precision on B200.
-#ifndef LPG_ASSEMBLE_MIN_BLOCKS_F64
-#define LPG_ASSEMBLE_MIN_BLOCKS_F64 6
-#endif
-#ifndef LPG_ASSEMBLE_MIN_BLOCKS_F32
-#define LPG_ASSEMBLE_MIN_BLOCKS_F32 8
-#endif
-#ifndef LPG_ASSEMBLE_PERSISTENT
-#define LPG_ASSEMBLE_PERSISTENT 1
-#endif
-template <typename R> struct MinBlocks;
-template <> struct MinBlocks<double> { static constexpr int value = LPG_ASSEMBLE_MIN_BLOCKS_F64; };
-template <> struct MinBlocks<float> { static constexpr int value = LPG_ASSEMBLE_MIN_BLOCKS_F32; };
 
 template <typename R> struct M;
 template <> struct M<double> {
@@ -219,313 +203,6 @@ __host__ __device__ constexpr int sym9(int r, int c) {
 template <typename R> __device__ __forceinline__ R qbasis(int a, int j) {
     const int sgn = (a == 0) ? 1 : ((a == j + 1) ? 1 : -1);
     return sgn > 0 ? R(0.5) : R(-0.5);
-}
-
-struct TileMeta {
-    int row[32];
-    int slot0[32];
-    int nb[32];
-    int dq[32];   // position of the diagonal block within the row
-    int ppre[33]; // the pairs of row j are [ppre[j], ppre[j + 1])
-    int sb[32];   // the row's sliced-ELL base less 288 x its diagonal position (solver layout)
-};
-
-// Position of entry t (row-major) of block q of tile row j in the output layout.
-__device__ __forceinline__ size_t out_pos(int layout, const TileMeta* meta, int j, int q, int t) {
-    const int64_t k = static_cast<int64_t>(meta->slot0[j]) + q;
-    if (layout == LPG_LAYOUT_BSR) return static_cast<size_t>(9 * k + t);
-    if (layout == LPG_LAYOUT_CSC) {
-        const int i = t / 3, c = t - 3 * (t / 3);
-        return 9 * static_cast<size_t>(meta->slot0[j]) + static_cast<size_t>(i) * 3 * meta->nb[j] + 3 * q + c;
-    }
-    return static_cast<size_t>(static_cast<int64_t>(meta->sb[j]) + 32 * static_cast<int64_t>(9 * q + t));
-}
-
-// Shared memory of one warp: off-diagonal blocks [9][3 cap + 1], slot descriptors [3 cap], metadata.
-template <typename R, int WH> __host__ __device__ constexpr size_t smem_per_warp(int cap) {
-    return ((WH ? (9 * static_cast<size_t>(3 * cap + 1) * sizeof(R) + 3 * static_cast<size_t>(cap) * 4) : 0) +
-            sizeof(TileMeta) + 15) / 16 * 16;
-}
-
-// Inclusive scan of the 12 per-pair values (gradient piece, diagonal block) over the lanes of
-// each row segment; segment heads are the set bits of `heads` (bit l = a row starts at lane l).
-// The fixed Hillis-Steele pattern makes the row sums deterministic.
-template <typename R> __device__ __forceinline__ void segmented_scan(R (&v)[12], unsigned heads, int lane) {
-    const unsigned upto = heads & (0xffffffffu >> (31 - lane));
-    const int seg = upto ? 31 - __clz(upto) : 0;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        R t[12];
-#pragma unroll
-        for (int k = 0; k < 12; ++k) t[k] = __shfl_up_sync(0xffffffffu, v[k], off);
-        if (lane - off >= seg)
-#pragma unroll
-            for (int k = 0; k < 12; ++k) v[k] = M<R>::add(t[k], v[k]);
-    }
-}
-
-// Evaluates pair q of the tile: returns E_e (a = 0 only), leaves g_a and the diagonal block
-// H_aa in v[0..2], v[3..11] and the three off-diagonal blocks at their slot-sorted positions.
-template <typename R, bool WG, int WH>
-__device__ __forceinline__ unsigned eval_pair(const DevMesh& m, const EvalArgs& a, int pe, unsigned pos4, int4 tv, R* sH,
-                                              int P, R (&v)[12], double& e_acc) {
-    using X = M<R>;
-    const int e = pe & ((1 << 30) - 1);
-    const int la = static_cast<unsigned>(pe) >> 30;
-    Kin<R> k;
-    const unsigned st = kinematics<R>(m, e, tv, a.u, k);
-    if (la == 0) {
-        const R Ee = k.vol * k.psi;
-        e_acc += static_cast<double>(Ee);
-        if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
-    }
-    R na[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) na[j] = la == 0 ? k.n[0][j] : la == 1 ? k.n[1][j] : la == 2 ? k.n[2][j] : k.n[3][j];
-    const R p = X::fma(k.lam, k.logJ, -k.mu);
-    if (WG) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            R s = 0;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) s = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), na[j], s);
-            v[i] = k.vol * s;
-        }
-    }
-    if (WH == 1) {
-        R h[4][3];
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-                h[b][i] = X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
-        R ha[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) ha[i] = la == 0 ? h[0][i] : la == 1 ? h[1][i] : la == 2 ? h[2][i] : h[3][i];
-        const R lv = X::mul(k.vol, k.lam);
-        const R pv = X::mul(k.vol, p);
-        const R mv = X::mul(k.vol, k.mu);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int pos = (pos4 >> (8 * b)) & 0xffu;
-            const R gg = X::fma(na[2], k.n[b][2], X::fma(na[1], k.n[b][1], X::mul(na[0], k.n[b][0])));
-            const R mg = X::mul(mv, gg);
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk) {
-                    const R x = X::mul(ha[i], h[b][kk]);
-                    const R y = X::mul(h[b][i], ha[kk]);
-                    R val = X::fma(lv, x, X::mul(-pv, y));
-                    if (i == kk) val = X::add(val, mg);
-                    if (b == la)
-                        v[3 + 3 * i + kk] = val;
-                    else
-                        sH[(3 * i + kk) * P + pos] = val;
-                }
-        }
-    } else if (WH == 2) {
-        // Projected: blocks from the clamped per-element tangent Mp (9x9 over (i, j') with
-        // index 3 j' + i, packed upper triangle) in the orthonormal basis q of {sum = 0}:
-        //   H_ab(i, k) = sum_{j', l'} q_a(j') q_b(l') Mp(3 j' + i, 3 l' + k).
-        const R* Mp = reinterpret_cast<const R*>(a.proj) + 45 * static_cast<size_t>(e);
-        R Y[3][9];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int c = 0; c < 9; ++c) {
-                R s = 0;
-#pragma unroll
-                for (int jp = 0; jp < 3; ++jp) s = X::fma(qbasis<R>(la, jp), __ldg(Mp + sym9(3 * jp + i, c)), s);
-                Y[i][c] = s;
-            }
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int pos = (pos4 >> (8 * b)) & 0xffu;
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk) {
-                    R s = 0;
-#pragma unroll
-                    for (int lp = 0; lp < 3; ++lp) s = X::fma(qbasis<R>(b, lp), Y[i][3 * lp + kk], s);
-                    if (b == la)
-                        v[3 + 3 * i + kk] = s;
-                    else
-                        sH[(3 * i + kk) * P + pos] = s;
-                }
-        }
-    }
-    return st;
-}
-
-// Fused element pass + assembly. WG: gradient, WH: Hessian (0 none, 1 exact, 2 from the
-// projected tangents in a.proj), energy always. CHUNKS = pairs per lane (1, or 2 for tiles of
-// up to 64 pairs).
-template <typename R, bool WG, int WH, int CHUNKS>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock, MinBlocks<R>::value) assemble_kernel(const DevMesh m,
-                                                                                            const EvalArgs a) {
-    using X = M<R>;
-    using HT = typename HOut<R>::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nw = gridDim.x * kWarpsPerBlock;
-    int tile = blockIdx.x * kWarpsPerBlock + warp;
-    if (tile >= m.ntiles) return;
-    const int cap = 32 * CHUNKS;
-    const int P = 3 * cap + 1;
-    unsigned char* base = smem_raw + smem_per_warp<R, WH>(cap) * warp;
-    R* sH = reinterpret_cast<R*>(base);
-    uint32_t* sdesc = reinterpret_cast<uint32_t*>(base + (WH ? 9 * static_cast<size_t>(P) * sizeof(R) : 0));
-    TileMeta* meta = reinterpret_cast<TileMeta*>(base + (WH ? 9 * static_cast<size_t>(P) * sizeof(R) + 12 * cap : 0));
-
-    unsigned st = 0;
-    // Index chain of the next tile: pair records first, then the vertex ids of their elements, so
-    // that a tile's element records and displacements are one dependent load away.
-    int np_n = 0;
-    int pe_n[CHUNKS];
-    unsigned pos_n[CHUNKS];
-    int4 tv_n[CHUNKS];
-    auto load_index = [&](int t) {
-        const int p0n = __ldg(m.tile_pair_ptr + t);
-        np_n = __ldg(m.tile_pair_ptr + t + 1) - p0n;
-#pragma unroll
-        for (int c = 0; c < CHUNKS; ++c) {
-            const int q = 32 * c + lane;
-            pe_n[c] = q < np_n ? __ldg(m.pair_elem + p0n + q) : 0;
-            pos_n[c] = q < np_n ? __ldg(reinterpret_cast<const unsigned*>(m.contrib) + p0n + q) : 0u;
-        }
-    };
-    auto load_tets = [&]() {
-#pragma unroll
-        for (int c = 0; c < CHUNKS; ++c)
-            tv_n[c] = 32 * c + lane < np_n ? __ldg(m.tets + (pe_n[c] & ((1 << 30) - 1))) : make_int4(0, 0, 0, 0);
-    };
-    load_index(tile);
-    load_tets();
-    for (; tile < m.ntiles; tile += nw) {
-        const int np = np_n;
-        int pe[CHUNKS];
-        unsigned pos[CHUNKS];
-        int4 tv[CHUNKS];
-    #pragma unroll
-        for (int c = 0; c < CHUNKS; ++c) {
-            pe[c] = pe_n[c];
-            pos[c] = pos_n[c];
-            tv[c] = tv_n[c];
-        }
-        const int tnext = tile + nw;
-        if (tnext < m.ntiles) load_index(tnext); // the next tile's pairs, ahead of this tile's work
-        const int r0 = m.tile_row_ptr[tile];
-        const int nr = m.tile_row_ptr[tile + 1] - r0;
-        const int s0 = m.tile_slot_ptr[tile];
-        const int ns = m.tile_slot_ptr[tile + 1] - s0;
-        // Row metadata and the pair prefix of the tile's rows (every row has at least one pair).
-        int deg = 0;
-        if (lane < nr) {
-            const int r = m.tile_rows[r0 + lane];
-            const int sb = m.row_ptr[r];
-            meta->row[lane] = r;
-            meta->slot0[lane] = sb;
-            meta->nb[lane] = m.row_ptr[r + 1] - sb;
-            meta->dq[lane] = m.diag_slot[r] - sb;
-            if (a.layout == kLayoutSell) meta->sb[lane] = m.sell_base[r] - 288 * (m.diag_slot[r] - sb);
-            deg = m.inc_ptr[r + 1] - m.inc_ptr[r];
-        }
-        int incl = deg;
-    #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl += t;
-        }
-        const int start = incl - deg; // first pair of row `lane`
-        meta->ppre[lane + 1] = incl;
-        if (lane == 0) meta->ppre[0] = 0;
-        if (WH)
-            for (int s = lane; s < ns; s += 32) sdesc[s] = __ldg(m.slot_desc + s0 + s);
-        const bool head = lane < nr;
-        const unsigned heads_lo = __reduce_or_sync(0xffffffffu, head && start < 32 ? 1u << start : 0u);
-        const unsigned heads_hi = __reduce_or_sync(0xffffffffu, head && start >= 32 ? 1u << (start - 32) : 0u);
-        __syncwarp();
-
-        double e_acc = 0.0;
-        R carry[12];
-    #pragma unroll
-        for (int c = 0; c < CHUNKS; ++c) {
-            const int q = 32 * c + lane;
-            R v[12];
-    #pragma unroll
-            for (int t = 0; t < 12; ++t) v[t] = R(0);
-            if (q < np) st |= eval_pair<R, WG, WH>(m, a, pe[c], pos[c], tv[c], sH, P, v, e_acc);
-            if (c == CHUNKS - 1 && tnext < m.ntiles) load_tets(); // vertex ids of the next tile's elements
-            const unsigned heads = c == 0 ? heads_lo : heads_hi;
-            segmented_scan<R>(v, heads, lane);
-            if (c == 1) {
-                // A row running on from chunk 0 adds chunk 0's partial (its last lane) once, at its end.
-                const bool cont = (heads & (0xffffffffu >> (31 - lane))) == 0;
-                if (cont)
-    #pragma unroll
-                    for (int t = 0; t < 12; ++t) v[t] = X::add(carry[t], v[t]);
-            }
-            if (CHUNKS == 2 && c == 0)
-    #pragma unroll
-                for (int t = 0; t < 12; ++t) carry[t] = __shfl_sync(0xffffffffu, v[t], 31);
-            // The last lane of each row segment in this chunk writes the row's gradient and diagonal block.
-            const unsigned next_heads = (lane == 31) ? (c == 0 ? (heads_hi & 1u) : 0u) : (heads >> (lane + 1)) & 1u;
-            const bool row_ends_here = q < np && (q == np - 1 || next_heads);
-            if (row_ends_here) {
-                const unsigned long long all = (static_cast<unsigned long long>(heads_hi) << 32) | heads_lo;
-                const unsigned long long upto = (q == 63) ? all : (all & ((2ull << q) - 1));
-                const int j = __popcll(upto) - 1;
-                const int r = meta->row[j];
-                if (WG) {
-    #pragma unroll
-                    for (int t = 0; t < 3; ++t) {
-                        if (!X::finite(v[t])) st |= ST_NONFINITE_OUT;
-                        a.grad[3 * static_cast<size_t>(r) + t] = static_cast<double>(v[t]);
-                    }
-                }
-                if (WH) {
-                    HT* hout = reinterpret_cast<HT*>(a.hess);
-                    const int dq = meta->dq[j];
-    #pragma unroll
-                    for (int t = 0; t < 9; ++t) {
-                        if (!X::finite(v[3 + t])) st |= ST_NONFINITE_OUT;
-                        hout[out_pos(a.layout, meta, j, dq, t)] = static_cast<HT>(v[3 + t]);
-                    }
-                }
-            }
-        }
-        __syncwarp();
-        // Off-diagonal slots: 27 lanes = 3 slots x 9 entries per pass; a slot's blocks are contiguous.
-        if (WH && lane < 27) {
-            HT* hout = reinterpret_cast<HT*>(a.hess);
-            const int sub = lane / 9, kk = lane - 9 * (lane / 9);
-            const int total = 3 * np;
-            const R* col = sH + kk * P;
-            for (int s = sub; s < ns; s += 3) {
-                const uint32_t d = sdesc[s];
-                const int c0 = d & 0xffu;
-                const int c1 = s + 1 < ns ? (sdesc[s + 1] & 0xffu) : total;
-                const int j = (d >> 8) & 31u;
-                const int qs = d >> 13;
-                R val = 0;
-                for (int c = c0; c < c1; ++c) val = X::add(val, col[c]);
-                if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                // The solver layout keeps the blocks right of the diagonal only.
-                if (a.layout != kLayoutSell || qs > meta->dq[j]) hout[out_pos(a.layout, meta, j, qs, kk)] = static_cast<HT>(val);
-            }
-        }
-    #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) e_acc += __shfl_xor_sync(0xffffffffu, e_acc, off);
-        if (lane == 0) {
-            a.tile_energy[tile] = e_acc;
-            if (!isfinite(e_acc)) st |= ST_NONFINITE_OUT;
-        }
-        __syncwarp();
-    }
-    st = __reduce_or_sync(0xffffffffu, st);
-    if (lane == 0 && st) atomicOr(a.status, st);
 }
 
 // Gradient rows of vertices that no element references are zero.
@@ -1493,7 +1170,7 @@ __global__ void __launch_bounds__(kClThreads, MINB) cluster_kernel(const DevMesh
         if (tid == 0) {
             double t = 0;
             for (int w = 0; w < (bd >> 5); ++w) t += red[w];
-            a.tile_energy[cl] = t;
+            a.cluster_energy[cl] = t;
             if (!isfinite(t)) st |= ST_NONFINITE_OUT;
         }
         // Phase 2: one thread per block slot (off-diagonal slots first, then diagonal slots,
@@ -1839,39 +1516,6 @@ __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __re
     rec32[12 * static_cast<size_t>(e) + 11] = static_cast<float>(mu);
 }
 
-template <typename R, bool WG, int WH, int CHUNKS> void launch_assemble(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
-    const size_t sm = kWarpsPerBlock * smem_per_warp<R, WH>(32 * CHUNKS);
-    static bool configured = false;
-    if (!configured) {
-        LPG_CUDA(cudaFuncSetAttribute(assemble_kernel<R, WG, WH, CHUNKS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sm)));
-        configured = true;
-    }
-    // Persistent warps: as many blocks as are resident at once, each warp looping over tiles.
-    static int resident = 0;
-    if (resident == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        LPG_CUDA(cudaGetDevice(&dev));
-        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, assemble_kernel<R, WG, WH, CHUNKS>,
-                                                               32 * kWarpsPerBlock, sm));
-        resident = std::max(1, sms * std::max(per_sm, 1));
-    }
-    const int all = (m.ntiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    const int blocks = LPG_ASSEMBLE_PERSISTENT ? std::min(resident, all) : all;
-    if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-    if (blocks > 0) assemble_kernel<R, WG, WH, CHUNKS><<<blocks, 32 * kWarpsPerBlock, sm, s>>>(m, a);
-    if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
-    LPG_CUDA(cudaGetLastError());
-}
-
-template <typename R, bool WG, int WH> void launch_chunks(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
-    if (m.cap <= 32)
-        launch_assemble<R, WG, WH, 1>(m, a, s);
-    else
-        launch_assemble<R, WG, WH, 2>(m, a, s);
-}
-
 // The Hessian-writing cluster kernel in the register-budget variant a.cl_variant.
 template <typename R, bool WG> void launch_cluster_variant(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     switch (a.cl_variant) {
@@ -1881,7 +1525,7 @@ template <typename R, bool WG> void launch_cluster_variant(const DevMesh& m, con
     }
 }
 
-// Launches the element pass; returns the number of per-unit energies it wrote to tile_energy.
+// Launches the element pass; returns the number of per-unit energies it wrote to cluster_energy.
 // The Exact Hessian, gradient and energy use the element-once cluster kernel; the projected
 // Hessian uses the pair kernel over the per-element clamped tangents.
 template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const EvalArgs& a, cudaStream_t s) {
@@ -1919,8 +1563,8 @@ void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a
     const int units = precision == LPG_PRECISION_F64 ? launch_eval_t<double>(m, hessian, a, s)
                                                       : launch_eval_t<float>(m, hessian, a, s);
     // Per-unit energies -> partials (stored after the units) -> total.
-    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(a.tile_energy, units, a.tile_energy + units);
-    sum_final_kernel<<<1, 256, 0, s>>>(a.tile_energy + units, kSumBlocks, a.energy);
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(a.cluster_energy, units, a.cluster_energy + units);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.cluster_energy + units, kSumBlocks, a.energy);
     LPG_CUDA(cudaGetLastError());
 }
 

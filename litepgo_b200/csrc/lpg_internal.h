@@ -28,33 +28,15 @@ struct Error {
 void check_cuda(cudaError_t e, const char* what);
 #define LPG_CUDA(call) ::lpg::check_cuda((call), #call)
 
-// Host-side assembly plan (built once per mesh, lpg_plan.cpp).
-//
-// Rows of the 3x3 block-CSR Hessian are vertices. A "pair" is (row vertex v, element e
-// incident to v, local index a of v in e); each pair produces the 4 blocks H_{a,b},
-// b = 0..3, of row v and the gradient piece g_a. Pairs are grouped into warp tiles of at
-// most `cap` pairs (whole rows only); a tile owns every block slot of its rows, so a warp
-// reduces its slots on chip in element order with no atomics.
+// Host-side assembly plan (built once per mesh, lpg_plan.cpp). Rows of the 3x3 block-CSR
+// Hessian are vertices; a "pair" is (row vertex v, element e incident to v, local index a of v
+// in e).
 struct HostPlan {
     int V = 0, T = 0;
-    int cap = 32;
     std::vector<int32_t> row_ptr, col_idx;   // BSR pattern (V+1, nnzb)
     std::vector<int32_t> inc_ptr;            // V+1: pairs per row, natural order
-    std::vector<int32_t> tile_pair_ptr;      // ntiles+1
-    std::vector<int32_t> tile_row_ptr;       // ntiles+1
-    std::vector<int32_t> tile_rows;          // rows of each tile, ascending
-    std::vector<int32_t> tile_slot_ptr;      // ntiles+1 (cumulative off-diagonal slot counts)
-    // One descriptor per off-diagonal slot, in tile order: bits 0-7 the slot's first block in the
-    // tile's slot-sorted block list, bits 8-12 the row within the tile, bits 13+ the slot's
-    // position within its row. A slot's blocks are contiguous in that list and ordered by
-    // element, the reference's summation order.
-    std::vector<uint32_t> slot_desc;
-    // 4 * npairs: position of off-diagonal block b of each pair in the slot-sorted list
-    // (0xff for the diagonal block b == a, which is reduced in registers).
-    std::vector<uint8_t> contrib;
     std::vector<int32_t> diag_slot;          // V: block index of (v, v), -1 for an unused vertex
-    std::vector<int32_t> unused_rows;        // vertices referenced by no element (not in any tile)
-    std::vector<int32_t> pair_elem;          // npairs: e | (a << 30), tile-major
+    std::vector<int32_t> unused_rows;        // vertices referenced by no element
     // Upper-triangle sliced ELL of the solvers (SELL-32 with rows sorted by block count within
     // windows of kSellWindow rows). The matrix is symmetric, so each row stores only its blocks
     // with column >= row ("own" blocks, the diagonal first) and reads its blocks left of the
@@ -85,7 +67,6 @@ struct HostPlan {
     std::vector<uint32_t> cl_slot, cl_slot_ent;
     std::vector<int32_t> cl_ent_ptr;
     std::vector<uint16_t> cl_ents;
-    int ntiles() const { return static_cast<int>(tile_pair_ptr.size()) - 1; }
     // Value count of the solver layout: 9 per own slot, then the 9 x 32 zero block.
     int64_t sell_zero() const { return 9 * static_cast<int64_t>(sell_ptr.back()); }
     size_t sell_values() const { return static_cast<size_t>(sell_zero()) + 9 * 32; }
@@ -126,16 +107,12 @@ void check_solver_layout(const HostPlan& plan);
 
 // Device mirror of the plan and of the per-element records.
 struct DevMesh {
-    int V = 0, T = 0, ntiles = 0, cap = 32;
+    int V = 0, T = 0;
     int64_t nnzb = 0;
     int32_t *row_ptr = nullptr, *col_idx = nullptr, *inc_ptr = nullptr;
-    int32_t *tile_pair_ptr = nullptr, *tile_row_ptr = nullptr, *tile_rows = nullptr, *tile_slot_ptr = nullptr;
-    uint32_t* slot_desc = nullptr;
-    uint8_t* contrib = nullptr;
     int32_t* diag_slot = nullptr;
     int32_t* unused_rows = nullptr;
     int num_unused = 0;
-    int32_t* pair_elem = nullptr;
     int32_t *sell_ptr = nullptr, *sell_row = nullptr, *sell_col = nullptr, *sell_base = nullptr;
     int32_t* sell_bptr = nullptr;
     int2* sell_bref = nullptr; // {value index, column} per borrowed slot
@@ -165,7 +142,7 @@ struct EvalArgs {
     double* grad = nullptr;     // device, 3V or null
     void* hess = nullptr;       // device values or null
     int layout = LPG_LAYOUT_BSR;
-    double* tile_energy = nullptr; // device, ntiles (always written)
+    double* cluster_energy = nullptr; // device, one per cluster (always written)
     double* energy = nullptr;      // device scalar (always written)
     double* elem_energy = nullptr; // device, T, or null
     const void* proj = nullptr;    // projected per-element 9x9 tangents (hessian PROJECTED*), or null

@@ -1,5 +1,5 @@
-// lpg_plan.cpp -- host-side assembly plan: block-CSR pattern, vertex incidence,
-// warp tiles and per-slot contributor lists.
+// lpg_plan.cpp -- host-side assembly plan: block-CSR pattern, vertex incidence, the
+// solvers' upper-triangle sliced ELL, and the vertex clusters with per-slot contributor lists.
 //
 // The scalar pattern of the reference is the union over elements of local x local DOF
 // pairs, both triangles (src/core/dof/energy_assembler.cpp:38-47). For 3 DOFs per vertex
@@ -192,9 +192,10 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
     }
     int maxdeg = 0;
     for (int v = 0; v < V; ++v) maxdeg = std::max(maxdeg, p.inc_ptr[v + 1] - p.inc_ptr[v]);
-    if (maxdeg > 64)
-        fail(LPG_EINVAL, "vertex valence " + std::to_string(maxdeg) + " exceeds the supported maximum of 64");
-    p.cap = maxdeg > 32 ? 64 : 32;
+    // A vertex's elements must fit in one assembly cluster.
+    if (maxdeg > kClusterElems)
+        fail(LPG_EINVAL, "vertex valence " + std::to_string(maxdeg) + " exceeds the supported maximum of " +
+                             std::to_string(kClusterElems));
     // Block-CSR pattern: sorted unique neighbours (including the vertex itself).
     p.row_ptr.assign(static_cast<size_t>(V) + 1, 0);
     {
@@ -291,88 +292,9 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
             }
         }
     }
-    // Warp tiles: whole rows, at most `cap` pairs and 32 rows per tile. First fit over a
-    // short window of open tiles keeps rows of one tile close in memory.
-    struct Open {
-        int tile, pairs, rows;
-    };
-    std::vector<std::vector<int32_t>> tiles;
-    std::vector<int> tile_pairs;
-    std::vector<Open> open;
-    constexpr int kWindow = 8;
     p.unused_rows.clear();
-    for (int v = 0; v < V; ++v) {
-        const int deg = p.inc_ptr[v + 1] - p.inc_ptr[v];
-        if (deg == 0) {
-            p.unused_rows.push_back(v); // no element references v: zero gradient, no Hessian slots
-            continue;
-        }
-        int chosen = -1;
-        for (size_t k = 0; k < open.size(); ++k)
-            if (open[k].pairs + deg <= p.cap && open[k].rows < 32) {
-                chosen = static_cast<int>(k);
-                break;
-            }
-        if (chosen < 0) {
-            tiles.emplace_back();
-            tile_pairs.push_back(0);
-            open.push_back({static_cast<int>(tiles.size()) - 1, 0, 0});
-            if (open.size() > kWindow) open.erase(open.begin());
-            chosen = static_cast<int>(open.size()) - 1;
-        }
-        Open& o = open[chosen];
-        tiles[o.tile].push_back(v);
-        o.pairs += deg;
-        o.rows += 1;
-        tile_pairs[o.tile] = o.pairs;
-        if (o.pairs == p.cap || o.rows == 32) open.erase(open.begin() + chosen);
-    }
-    const int ntiles = static_cast<int>(tiles.size());
-    p.tile_pair_ptr.assign(static_cast<size_t>(ntiles) + 1, 0);
-    p.tile_row_ptr.assign(static_cast<size_t>(ntiles) + 1, 0);
-    p.tile_slot_ptr.assign(static_cast<size_t>(ntiles) + 1, 0);
-    p.tile_rows.clear();
-    p.tile_rows.reserve(V);
-    p.pair_elem.resize(static_cast<size_t>(npairs));
-    p.contrib.assign(static_cast<size_t>(npairs) * 4, 0xff);
-    p.slot_desc.clear();
-    p.slot_desc.reserve(static_cast<size_t>(p.nnzb()));
-    std::vector<std::vector<int>> bucket;
-    int64_t pair_cursor = 0;
-    for (int t = 0; t < ntiles; ++t) {
-        const int64_t pair_base = pair_cursor;
-        int64_t slots = 0;
-        int count = 0; // off-diagonal blocks of the tile placed so far
-        for (int j = 0; j < static_cast<int>(tiles[t].size()); ++j) {
-            const int v = tiles[t][j];
-            p.tile_rows.push_back(v);
-            const int r0 = p.row_ptr[v], nb_v = p.row_ptr[v + 1] - p.row_ptr[v];
-            bucket.assign(static_cast<size_t>(nb_v), {});
-            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
-                const int local = static_cast<int>(pair_cursor - pair_base);
-                p.pair_elem[pair_cursor++] = inc[k];
-                const int e = inc[k] & ((1 << 30) - 1);
-                for (int b = 0; b < 4; ++b) {
-                    const int w = tets[4 * static_cast<size_t>(e) + b];
-                    if (w == v) continue; // the diagonal block is reduced in registers
-                    const int32_t* beg = p.col_idx.data() + r0;
-                    const int q = static_cast<int>(std::lower_bound(beg, beg + nb_v, w) - beg);
-                    bucket[q].push_back(4 * local + b);
-                }
-            }
-            // Off-diagonal slots in column order; each slot's blocks contiguous, in element order.
-            for (int q = 0; q < nb_v; ++q) {
-                if (p.col_idx[r0 + q] == v) continue;
-                p.slot_desc.push_back(static_cast<uint32_t>(count) | (static_cast<uint32_t>(j) << 8) |
-                                      (static_cast<uint32_t>(q) << 13));
-                for (int c : bucket[q]) p.contrib[4 * pair_base + c] = static_cast<uint8_t>(count++);
-                ++slots;
-            }
-        }
-        p.tile_pair_ptr[t + 1] = static_cast<int32_t>(pair_cursor);
-        p.tile_row_ptr[t + 1] = static_cast<int32_t>(p.tile_rows.size());
-        p.tile_slot_ptr[t + 1] = static_cast<int32_t>(p.tile_slot_ptr[t] + slots);
-    }
+    for (int v = 0; v < V; ++v)
+        if (p.inc_ptr[v + 1] == p.inc_ptr[v]) p.unused_rows.push_back(v); // no element: zero gradient, no blocks
     build_clusters(p, tets, inc);
 }
 

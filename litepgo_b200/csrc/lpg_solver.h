@@ -33,14 +33,14 @@ struct lpg_fem {
     lpg::DevMesh dm;
     std::atomic<bool> busy{false};
     // Plan and element data.
-    lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tile_pair_ptr, b_tile_row_ptr, b_tile_rows, b_tile_slot_ptr,
-        b_slot_desc, b_contrib, b_pair_elem, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot, b_unused;
+    lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot,
+        b_unused;
     lpg::DeviceBuffer b_cl[11]; // assembly clusters
     lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers
     lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_plist, d_pcount; // elements listed for the projection's eigenvalue clamp
-    lpg::DeviceBuffer d_status, d_tile_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
+    lpg::DeviceBuffer d_status, d_cluster_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
     // Solver state (Newton / PCG / adjoint).
     lpg::DeviceBuffer s_x, s_g, s_f, s_d, s_trial, s_mask, s_hess, s_hess64, s_dinv, s_r, s_z, s_p, s_ap, s_xcg, s_r64,
         s_b64, s_scal, s_part, s_flag, d_flush, s_p2, s_mask4;

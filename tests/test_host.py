@@ -39,12 +39,6 @@ def bsr_to_csc_pattern(row_ptr, col_idx):
     return np.array(outer, np.int32), (np.concatenate(inner).astype(np.int32) if inner else np.zeros(0, np.int32))
 
 
-def plan_summary(X, tets):
-    out = np.zeros(6, np.int64)
-    tets = np.ascontiguousarray(tets, dtype=np.int32)
-    N.check(N.lib.lpg_mesh_plan_summary(X.shape[0], tets.shape[0], N.iptr(tets), out.ctypes.data_as(N._i64p)))
-    return out
-
 
 @pytest.mark.parametrize("n", [1, 2, 3, 10, 64])
 def test_box_counts_and_orientation(n):
@@ -88,41 +82,28 @@ def test_bsr_pattern_expands_to_reference_csc_bit_exact(case):
     np.testing.assert_array_equal(inner, inner_ref)
 
 
-def test_plan_summary_invariants():
-    for n in (2, 10):
-        X, tets = mesh.make_box(n)
-        nnzb, pairs, tiles, cap, max_rows, contrib = plan_summary(X, tets)
-        assert pairs == 4 * tets.shape[0]
-        assert contrib == 4 * pairs
-        assert cap == 32  # vertex valence of the five-tet box is at most 32
-        assert max_rows <= 32
-        assert tiles * cap >= pairs
-    X, tets = mesh.make_box(10)
-    _, pairs, tiles, cap, _, _ = plan_summary(X, tets)
-    assert pairs == tiles * cap  # valences 32 and 8 pack warp tiles completely
-
-
 def test_plan_rejects_bad_connectivity():
     X, tets = mesh.make_box(2)
     bad = tets.copy()
     bad[3, 1] = bad[3, 0]
     with pytest.raises(ValueError, match="distinct"):
-        plan_summary(X, bad)
+        cluster_summary(X, bad)
     bad = tets.copy()
     bad[0, 2] = X.shape[0]
     with pytest.raises(ValueError, match="outside"):
-        plan_summary(X, bad)
+        cluster_summary(X, bad)
 
 
-def test_plan_valence_above_32_uses_64_pair_tiles():
-    # A fan of 40 tets around vertex 0 (valence 40).
-    k = 40
+def test_plan_rejects_valence_above_the_cluster_capacity():
+    # A fan of 230 tets around the axis (0, 1): both axis vertices have valence 230 > 224.
+    k = 230
     ang = np.linspace(0, 2 * np.pi, k, endpoint=False)
-    ring = np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1)
-    X = np.vstack([[0, 0, 0], [0, 0, 1], ring])
+    X = np.vstack([[0, 0, 0], [0, 0, 1], np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1)])
     tets = np.array([[0, 2 + i, 2 + (i + 1) % k, 1] for i in range(k)], np.int32)
-    nnzb, pairs, tiles, cap, _, _ = plan_summary(X, tets)
-    assert cap == 64 and pairs == 4 * k
+    with pytest.raises(ValueError, match="valence"):
+        cluster_summary(X, tets)
+    ok = tets[:200]
+    assert cluster_summary(X, ok)[4] == 16 * 200
 
 
 def cluster_summary(X, tets):
