@@ -356,6 +356,26 @@ int lpg_adjoint_fp(lpg_fem_t h, const double* u_star, const double* dLdu, const 
                    int io_mem, int precision, double cg_tolerance, int per_element, double* dFp, double* lambda_out);
 
 /*
+ * Materials evaluated by the caller (the reference's PyVolumetricMaterial and
+ * TorchVolumetricMaterial, src/python/fem.py:59-109, src/python/torch.py:72-94, bound through
+ * src/binding/fem/material/py_material.cpp), on a handle created without a plastic field (the
+ * caller's material receives Fp itself; LPG_EINVAL otherwise):
+ *   lpg_fem_deformation_gradients: F = I + grad u of every element at u (num_dofs values,
+ *     io_mem), 9 values per element, row-major F_ij at 3 i + j, into F (io_mem);
+ *   lpg_fem_eval_material: with the caller's W (num_tets, the density per reference volume),
+ *     P = dW/dF (9 per element, row-major) and, for a Hessian, A = d2W/dF2 (81 per element,
+ *     [3 i + j][3 k + l]) — host or device (in_mem) — writes E = sum vol W, the gradient
+ *     (sum vol P grad N_a per vertex; may be NULL) and the Hessian sum vol B^T A B (LPG_HESSIAN_
+ *     EXACT) or its per-element eigenvalue clamp (LPG_HESSIAN_PROJECTED) in BSR or CSC order, as
+ *     lpg_fem_eval does (grad and hess in out_mem). Each element's A is symmetrised,
+ *     (A + A^T) / 2, before use; non-finite material outputs give LPG_EDOMAIN. P may be NULL
+ *     when grad is NULL, A when hessian is LPG_HESSIAN_NONE.
+ */
+int lpg_fem_deformation_gradients(lpg_fem_t h, const double* u, int io_mem, double* F);
+int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const double* A, int in_mem, double* energy,
+                          double* grad, int hessian, int precision, int layout, void* hess, int out_mem);
+
+/*
  * Autotuner (no reference counterpart). Three kernels come in launch variants that differ in
  * register budget and loop unrolling only, so every variant computes bitwise the same
  * results: the Exact-Hessian assembly (3 variants per precision), the PCG SpMV of the

@@ -426,6 +426,75 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
     });
 }
 
+int lpg_fem_deformation_gradients(lpg_fem_t h, const double* u, int io_mem, double* F) {
+    return guarded([&] {
+        if (!h || !F) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: null argument");
+        if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: the handle has a plastic field");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        const size_t n = 3 * static_cast<size_t>(h->dm.V), T = static_cast<size_t>(h->dm.T);
+        const double* du = h->stage_in(u, io_mem, h->d_u, n);
+        double* dF = io_mem == LPG_MEM_DEVICE ? F : h->d_vjp.as<double>(std::max<size_t>(9 * T, 1));
+        launch_deformation_gradients(h->dm, du, dF, h->d_status.as<unsigned>(1), h->stream);
+        if (io_mem == LPG_MEM_HOST && T > 0)
+            LPG_CUDA(cudaMemcpyAsync(F, dF, 9 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        raise_status(h->take_status());
+    });
+}
+
+int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const double* A, int in_mem, double* energy,
+                          double* grad, int hessian, int precision, int layout, void* hess, int out_mem) {
+    return guarded([&] {
+        if (!h) fail(LPG_EINVAL, "null handle");
+        if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_eval_material: the handle has a plastic field");
+        const size_t T = static_cast<size_t>(h->dm.T), n = 3 * static_cast<size_t>(h->dm.V);
+        if (T > 0 && (!W || (grad && !P))) fail(LPG_EINVAL, "lpg_fem_eval_material: null material output");
+        if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
+            fail(LPG_EINVAL, "Energy: invalid Hessian kind");
+        if (hessian != LPG_HESSIAN_NONE && (!hess || (T > 0 && !A)))
+            fail(LPG_EINVAL, "lpg_fem_eval_material: a Hessian needs d2W/dF2 and an output");
+        if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
+        if (layout != LPG_LAYOUT_BSR && layout != LPG_LAYOUT_CSC) fail(LPG_EINVAL, "invalid Hessian layout");
+        if (out_mem != LPG_MEM_HOST && out_mem != LPG_MEM_DEVICE) fail(LPG_EINVAL, "invalid memory flag");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        cudaStream_t s = h->stream;
+        // Inputs on the device (staged through the handle's scratch when on the host).
+        auto stage = [&](const double* p, size_t count, DeviceBuffer& buf) -> const double* {
+            if (!p || count == 0 || in_mem == LPG_MEM_DEVICE) return p;
+            if (in_mem != LPG_MEM_HOST) fail(LPG_EINVAL, "invalid memory flag");
+            double* d = buf.as<double>(count);
+            LPG_CUDA(cudaMemcpyAsync(d, p, count * sizeof(double), cudaMemcpyHostToDevice, s));
+            return d;
+        };
+        const double* dW = stage(W, T, h->d_mat[0]);
+        const double* dP = grad ? stage(P, 9 * T, h->d_mat[1]) : nullptr;
+        const double* dA = hessian != LPG_HESSIAN_NONE ? stage(A, 81 * T, h->d_mat[2]) : nullptr;
+        EvalArgs a;
+        a.grad = grad ? (out_mem == LPG_MEM_DEVICE ? grad : h->d_grad.as<double>(std::max<size_t>(n, 1))) : nullptr;
+        const size_t hbytes = 9 * static_cast<size_t>(h->dm.nnzb) * (precision == LPG_PRECISION_F64 ? 8 : 4);
+        a.hess = hessian != LPG_HESSIAN_NONE ? (out_mem == LPG_MEM_DEVICE ? hess : h->d_hess.ensure(hbytes)) : nullptr;
+        a.layout = layout;
+        a.cluster_energy = h->d_cluster_energy.as<double>(static_cast<size_t>(h->dm.ncl) + 256);
+        a.energy = h->d_energy.as<double>(1);
+        a.status = h->d_status.as<unsigned>(1);
+        const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
+        void* proj = a.hess ? h->d_proj.ensure(project_bytes(h->dm, precision)) : nullptr;
+        launch_material_eval(h->dm, precision, hessian, dW, dP, dA, h->d_mat[3].as<double>(std::max<size_t>(T, 1)),
+                             h->d_vjp.as<double>(std::max<size_t>(12 * T, 1)), proj,
+                             h->d_plist.as<int>(std::max<size_t>(T, 1)), h->d_pcount.as<unsigned>(1), h->tune.clamp[pi],
+                             a, s);
+        double e = 0;
+        LPG_CUDA(cudaMemcpyAsync(&e, a.energy, sizeof e, cudaMemcpyDeviceToHost, s));
+        if (grad && out_mem == LPG_MEM_HOST && n > 0)
+            LPG_CUDA(cudaMemcpyAsync(grad, a.grad, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (a.hess && out_mem == LPG_MEM_HOST) LPG_CUDA(cudaMemcpyAsync(hess, a.hess, hbytes, cudaMemcpyDeviceToHost, s));
+        raise_status(h->take_status());
+        if (!std::isfinite(e)) fail(LPG_EDOMAIN, "MeshEnergy: non-finite energy sum");
+        if (energy) *energy = e;
+    });
+}
+
 int lpg_fem_time_eval(lpg_fem_t h, const double* u, double* grad, int hessian, int precision, int layout, void* hess,
                       int launches, int flush_l2, double* ms_assemble, double* ms_eval) {
     return guarded([&] {

@@ -706,8 +706,114 @@ template <typename R> struct Eps;
 template <> struct Eps<double> { static constexpr double v = 2.220446049250313e-16; };
 template <> struct Eps<float> { static constexpr float v = 1.1920929e-7f; };
 
+// Tangent sources of the projection pass: each forms the element's 9x9 tangent M in the q basis
+// (packed upper triangle into A; V is 81 values of per-thread scratch) and returns status bits.
+// NhTangent: the neo-Hookean closed form at displacement u.
+struct NhTangent {
+    const double* u;
+};
+__device__ __forceinline__ bool keeps_exact(const NhTangent&) { return false; }
+// MatTangent: a material's d2W/dF2 per element (81 FP64 values, [3 i + j][3 k + l] =
+// d2W / dF_ij dF_kl), M(3 j' + i, 3 l' + k) = vol sum_{j,l} Rq[j'][j] A[(i,j),(k,l)] Rq[l'][l],
+// symmetrised as (M + M^T) / 2; with exact set the tangent is kept as it is (the Exact Hessian).
+struct MatTangent {
+    const double* A;
+    bool exact;
+};
+__device__ __forceinline__ bool keeps_exact(const MatTangent& s) { return s.exact; }
+
 template <typename R>
-__global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, const double* __restrict__ u,
+__device__ __forceinline__ void rq_basis(const R (&n)[4][3], R (&Rq)[3][3]) {
+#pragma unroll
+    for (int jp = 0; jp < 3; ++jp)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            R s = 0;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) s += qbasis<R>(a, jp) * n[a][j];
+            Rq[jp][j] = s;
+        }
+}
+
+template <typename R>
+__device__ __forceinline__ unsigned form_tangent(const NhTangent& src, const DevMesh& m, int e, R* A, R* /*V*/) {
+    const int4 tv = __ldg(m.tets + e);
+    Kin<R> k;
+    const unsigned st = kinematics<R>(m, e, tv, src.u, k);
+    const R p = k.lam * k.logJ - k.mu;
+    R Rq[3][3];
+    rq_basis<R>(k.n, Rq);
+    R S[3][3], f[3][3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+#pragma unroll
+        for (int y = 0; y < 3; ++y) {
+            S[x][y] = Rq[x][0] * Rq[y][0] + Rq[x][1] * Rq[y][1] + Rq[x][2] * Rq[y][2];
+            f[x][y] = k.FiT[3 * x] * Rq[y][0] + k.FiT[3 * x + 1] * Rq[y][1] + k.FiT[3 * x + 2] * Rq[y][2];
+        }
+#pragma unroll
+    for (int jp = 0; jp < 3; ++jp)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int lp = 0; lp < 3; ++lp)
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                    const int r = 3 * jp + i, c = 3 * lp + kk;
+                    if (r > c) continue;
+                    R v = k.lam * f[i][jp] * f[kk][lp] - p * f[i][lp] * f[kk][jp];
+                    if (i == kk) v += k.mu * S[jp][lp];
+                    A[sym9(r, c)] = k.vol * v;
+                }
+    return st;
+}
+
+template <typename R>
+__device__ __forceinline__ unsigned form_tangent(const MatTangent& src, const DevMesh& m, int e, R* A, R* V) {
+    R rec[12];
+    load_rec<R>(rec_ptr<R>(m), e, rec);
+    R n[4][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) n[c + 1][j] = rec[3 * c + j];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) n[0][j] = -(n[1][j] + n[2][j] + n[3][j]);
+    R Rq[3][3];
+    rq_basis<R>(n, Rq);
+    const R vol = rec[9];
+    const double* Ae = src.A + 81 * static_cast<size_t>(e);
+    unsigned st = 0;
+    // Full M into V (row r = 3 j' + i, column c = 3 l' + k), then the symmetrised upper triangle.
+    for (int i = 0; i < 3; ++i)
+        for (int kk = 0; kk < 3; ++kk) {
+            R T[3][3]; // T[j][l'] = sum_l A[(i,j),(kk,l)] Rq[l'][l]
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                R a3[3];
+#pragma unroll
+                for (int l = 0; l < 3; ++l) a3[l] = static_cast<R>(__ldg(Ae + (3 * i + j) * 9 + 3 * kk + l));
+#pragma unroll
+                for (int lp = 0; lp < 3; ++lp) T[j][lp] = a3[0] * Rq[lp][0] + a3[1] * Rq[lp][1] + a3[2] * Rq[lp][2];
+            }
+#pragma unroll
+            for (int jp = 0; jp < 3; ++jp)
+#pragma unroll
+                for (int lp = 0; lp < 3; ++lp)
+                    V[9 * (3 * jp + i) + 3 * lp + kk] =
+                        vol * (Rq[jp][0] * T[0][lp] + Rq[jp][1] * T[1][lp] + Rq[jp][2] * T[2][lp]);
+        }
+    for (int r = 0; r < 9; ++r)
+        for (int c = r; c < 9; ++c) {
+            const R v = R(0.5) * (V[9 * r + c] + V[9 * c + r]);
+            if (!(v == v) || v == R(INFINITY) || v == R(-INFINITY)) st |= ST_NONFINITE_F;
+            A[sym9(r, c)] = v;
+        }
+    return st;
+}
+
+template <typename R, class Src>
+__global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, const Src src,
                                                                R* __restrict__ proj, unsigned* status,
                                                                const int* __restrict__ emesh,
                                                                const int* __restrict__ mesh_exact, int* list,
@@ -718,44 +824,9 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned st = 0;
     if (e < m.T) {
-        const int4 tv = __ldg(m.tets + e);
-        Kin<R> k;
-        st |= kinematics<R>(m, e, tv, u, k);
-        const R p = k.lam * k.logJ - k.mu;
-        R Rq[3][3];
-#pragma unroll
-        for (int jp = 0; jp < 3; ++jp)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                R s = 0;
-#pragma unroll
-                for (int a = 0; a < 4; ++a) s += qbasis<R>(a, jp) * k.n[a][j];
-                Rq[jp][j] = s;
-            }
-        R S[3][3], f[3][3];
-#pragma unroll
-        for (int x = 0; x < 3; ++x)
-#pragma unroll
-            for (int y = 0; y < 3; ++y) {
-                S[x][y] = Rq[x][0] * Rq[y][0] + Rq[x][1] * Rq[y][1] + Rq[x][2] * Rq[y][2];
-                f[x][y] = k.FiT[3 * x] * Rq[y][0] + k.FiT[3 * x + 1] * Rq[y][1] + k.FiT[3 * x + 2] * Rq[y][2];
-            }
-#pragma unroll
-        for (int jp = 0; jp < 3; ++jp)
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int lp = 0; lp < 3; ++lp)
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const int r = 3 * jp + i, c = 3 * lp + kk;
-                        if (r > c) continue;
-                        R v = k.lam * f[i][jp] * f[kk][lp] - p * f[i][lp] * f[kk][jp];
-                        if (i == kk) v += k.mu * S[jp][lp];
-                        A[sym9(r, c)] = k.vol * v;
-                    }
+        st |= form_tangent<R>(src, m, e, A, V);
         // Elements of a mesh marked exact keep their tangent unclamped (the Exact Hessian).
-        const bool keep = emesh != nullptr && mesh_exact[emesh[e]] != 0;
+        const bool keep = keeps_exact(src) || (emesh != nullptr && mesh_exact[emesh[e]] != 0);
         // Positive semi-definiteness test: LDL^T with diagonal pivoting on a copy in the V area
         // (row-major 9x9). Pivots above tol are eliminated; once none is left, M is semi-definite
         // if the remaining Schur complement is below tol everywhere (tol = 64 eps max|diag M|:
@@ -1504,6 +1575,85 @@ __global__ void __launch_bounds__(128) vertex_gather_kernel(const DevMesh m, con
     }
 }
 
+// ---------------------------------------------------------------------------
+// Materials evaluated outside the library (PyVolumetricMaterial, src/python/fem.py:59-109): the
+// library exports each element's deformation gradient, the caller evaluates W, dW/dF and
+// d2W/dF2 at those points, and the library integrates and assembles them.
+// ---------------------------------------------------------------------------
+// F = I + grad u per element (row-major, 9 per element), FP64; no plastic field on the handle.
+__global__ void __launch_bounds__(256) deformation_gradient_kernel(const DevMesh m, const double* __restrict__ u,
+                                                                   double* __restrict__ F, unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int4 tv = __ldg(m.tets + e);
+        const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
+        double uu[4][3];
+        bool ok = true;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                uu[c][i] = __ldg(u + 3 * static_cast<size_t>(vs[c]) + i);
+                ok = ok && isfinite(uu[c][i]);
+            }
+        if (!ok) st |= ST_BAD_INPUT;
+        const double* rec = m.rec64 + 12 * static_cast<size_t>(e);
+        double* o = F + 9 * static_cast<size_t>(e);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double h = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) h = fma(uu[c + 1][i] - uu[0][i], __ldg(rec + 3 * c + j), h);
+                o[3 * i + j] = h;
+            }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// Per element: vol W and the gradient pieces g_a = vol P grad N_a (12 values, vertex-major),
+// from the caller's W (T) and P = dW/dF (9 per element, row-major). Non-finite material outputs
+// reject the evaluation.
+__global__ void __launch_bounds__(256) material_pieces_kernel(const DevMesh m, const double* __restrict__ W,
+                                                              const double* __restrict__ P, double* __restrict__ elemE,
+                                                              double* __restrict__ per_elem, unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const double* rec = m.rec64 + 12 * static_cast<size_t>(e);
+        const double vol = rec[9];
+        double n[4][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) n[c + 1][j] = rec[3 * c + j];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) n[0][j] = -(n[1][j] + n[2][j] + n[3][j]);
+        const double w = __ldg(W + e);
+        const double Ee = vol * w;
+        if (!isfinite(Ee)) st |= ST_NONFINITE_OUT;
+        elemE[e] = Ee;
+        if (per_elem) {
+            double Pe[9];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) Pe[t] = __ldg(P + 9 * static_cast<size_t>(e) + t);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double g = vol * (Pe[3 * i] * n[a][0] + Pe[3 * i + 1] * n[a][1] + Pe[3 * i + 2] * n[a][2]);
+                    if (!isfinite(g)) st |= ST_NONFINITE_OUT;
+                    per_elem[12 * static_cast<size_t>(e) + 3 * a + i] = g;
+                }
+        }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
 // Lame parameters of every element record (FP64 and FP32 copies).
 __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __restrict__ theta, int per_element, int T) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1613,18 +1763,19 @@ void launch_clamp_v(R* proj, const int* list, const unsigned* count, int max_cou
         launch_clamp_t<R, clamp_minb<R>(0)>(proj, list, count, max_count, s);
 }
 
-template <typename R>
-void launch_project_t(const DevMesh& m, const double* u, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
+template <typename R, class Src>
+void launch_project_t(const DevMesh& m, const Src& src, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
                       const int* mesh_exact, int* list, unsigned* count, int clamp_variant) {
     const size_t sm = sizeof(R) * kProjStride * kProjThreads;
     thread_local bool ready = false;
     if (!ready) {
-        LPG_CUDA(cudaFuncSetAttribute(project_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        LPG_CUDA(cudaFuncSetAttribute(project_kernel<R, Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sm)));
         ready = true;
     }
     const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
     LPG_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
-    project_kernel<R><<<blocks, kProjThreads, sm, s>>>(m, u, proj, status, emesh, mesh_exact, list, count);
+    project_kernel<R, Src><<<blocks, kProjThreads, sm, s>>>(m, src, proj, status, emesh, mesh_exact, list, count);
     launch_clamp_v<R>(proj, list, count, m.T, clamp_variant, s);
 }
 } // namespace
@@ -1634,11 +1785,12 @@ void launch_project(const DevMesh& m, int precision, int hessian, const double* 
                     int clamp_variant) {
     if (hessian != LPG_HESSIAN_PROJECTED) fail(LPG_EINVAL, "projected Hessian kind not available");
     if (m.T == 0) return;
+    const NhTangent src{u};
     if (precision == LPG_PRECISION_F64)
-        launch_project_t<double>(m, u, static_cast<double*>(proj), status, s, emesh, mesh_exact, list, count,
+        launch_project_t<double>(m, src, static_cast<double*>(proj), status, s, emesh, mesh_exact, list, count,
                                  clamp_variant);
     else
-        launch_project_t<float>(m, u, static_cast<float*>(proj), status, s, emesh, mesh_exact, list, count,
+        launch_project_t<float>(m, src, static_cast<float*>(proj), status, s, emesh, mesh_exact, list, count,
                                 clamp_variant);
     LPG_CUDA(cudaGetLastError());
 }
@@ -1695,6 +1847,40 @@ void launch_set_geometry(const DevMesh& m, const double* geo, cudaStream_t s) {
 void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s) {
     if (nblocks > 0) sum_pairs_partial<<<nblocks, 256, 0, s>>>(per_elem, T, partial);
     sum_pairs_final<<<1, 32, 0, s>>>(partial, nblocks, out2);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_deformation_gradients(const DevMesh& m, const double* u, double* F, unsigned* status, cudaStream_t s) {
+    if (m.T > 0) deformation_gradient_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, u, F, status);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_material_eval(const DevMesh& m, int precision, int hessian, const double* W, const double* P,
+                          const double* A, double* elemE, double* per_elem, void* proj, int* list, unsigned* count,
+                          int clamp_variant, const EvalArgs& a, cudaStream_t s) {
+    if (m.T > 0) {
+        material_pieces_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, W, P, elemE, a.grad ? per_elem : nullptr, a.status);
+        if (a.grad) vertex_gather_kernel<<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
+    }
+    if (a.grad && m.num_unused > 0)
+        zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
+    // Energy: the per-element energies summed in a fixed order.
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(elemE, m.T, a.cluster_energy);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.cluster_energy, kSumBlocks, a.energy);
+    if (a.hess && m.T > 0) {
+        const MatTangent src{A, hessian == LPG_HESSIAN_EXACT};
+        EvalArgs ga = a;
+        ga.proj = proj;
+        if (precision == LPG_PRECISION_F64) {
+            launch_project_t<double>(m, src, static_cast<double*>(proj), a.status, s, nullptr, nullptr, list, count,
+                                     clamp_variant);
+            launch_block_gather<double>(m, ga, s);
+        } else {
+            launch_project_t<float>(m, src, static_cast<float*>(proj), a.status, s, nullptr, nullptr, list, count,
+                                    clamp_variant);
+            launch_block_gather<float>(m, ga, s);
+        }
+    }
     LPG_CUDA(cudaGetLastError());
 }
 

@@ -193,6 +193,15 @@ void launch_rest_vjp(const DevMesh& m, const double* u, const double* w, double*
                      unsigned* status, cudaStream_t s);
 void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cudaStream_t s);
 void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s);
+// Materials evaluated by the caller: F (9 T, row-major) at u, then integration and assembly of
+// the caller's W (T), P = dW/dF (9 T) and, for a Hessian, A = d2W/dF2 (81 T) — energy into
+// a.energy (a.cluster_energy is scratch of >= 256 values), gradient into a.grad if set, Hessian
+// (Exact, or projected: clamped) into a.hess in a.layout. elemE (T), per_elem (12 T), proj
+// (project_bytes), list (T) and count (1) are scratch.
+void launch_deformation_gradients(const DevMesh& m, const double* u, double* F, unsigned* status, cudaStream_t s);
+void launch_material_eval(const DevMesh& m, int precision, int hessian, const double* W, const double* P,
+                          const double* A, double* elemE, double* per_elem, void* proj, int* list, unsigned* count,
+                          int clamp_variant, const EvalArgs& a, cudaStream_t s);
 // Plastic force VJP: out (9 T, column-major per element) = (d g_e / d vec Fp_e)^T w_e.
 void launch_fp_vjp(const DevMesh& m, const double* u, const double* w, double* out, unsigned* status, cudaStream_t s);
 void launch_sum_cols9(const double* per_elem, int T, double* partial, int nblocks, double* out9, cudaStream_t s);

@@ -36,6 +36,8 @@ __all__ = [
     "VolumetricFemForceRestPositionResponseTetP1",
     "VolumetricFemForceFpResponse",
     "VolumetricFemForceFpResponseTetP1",
+    "PyVolumetricMaterial",
+    "VolumetricFemEnergyPyMaterialTetP1",
 ]
 
 
@@ -104,6 +106,10 @@ class Template:
 
     def __getitem__(self, args):
         key = args if isinstance(args, tuple) else (args,)
+        factory = getattr(self, "material_factory", None)
+        if (factory is not None and len(key) == 3 and isinstance(key[0], type) and
+                issubclass(key[0], PyVolumetricMaterial) and key[1:] == (TetP1Basis, TetCentroidQuadrature)):
+            return factory(key[0])
         try:
             return self._instances[key]
         except KeyError:
@@ -623,8 +629,188 @@ class VolumetricFemForceFpResponseTetP1:
         return out
 
 
+class PyVolumetricMaterial:
+    """Base class for volumetric materials written in Python (the reference's
+    PyVolumetricMaterial, src/python/fem.py:59-109): subclass it and put the subclass in the
+    Material slot of VolumetricFemEnergy[Material, TetP1Basis, TetCentroidQuadrature].
+
+    Required: ``num_parameters`` (the width k of theta) and
+    ``eval(F, Fp, theta, *, outputs) -> dict`` returning at least the requested entries of
+    ``W`` (N,), ``dW_dF`` (N,3,3) with [n,i,j] = dW/dF_ij and ``d2W_dF2`` (N,3,3,3,3) with
+    [n,i,j,k,l] = d2W/dF_ij dF_kl. Unlike the reference, whose batches are CPU NumPy arrays, F,
+    Fp and theta arrive here as CUDA float64 tensors of the whole mesh (one row per element), so
+    a torch material runs on the GPU; NumPy arrays are accepted as return values too. Energies
+    request ("W",), ("W", "dW_dF") or ("W", "dW_dF", "d2W_dF2"). Optional
+    ``eval_feasible_step(F, Fp, theta, dF) -> (N,)``: a bound in [0, 1] keeping each element
+    feasible along F + t dF; without it the step keeps det F > 0. Non-finite returned values
+    reject the evaluation (ValueError, as a native domain error)."""
+
+    num_parameters = None
+    eval_feasible_step = None
+
+    @staticmethod
+    def eval(F, Fp, theta, *, outputs):
+        raise NotImplementedError("PyVolumetricMaterial subclasses must implement eval")
+
+
+def _cuda_f64(a, shape, device):
+    import torch
+
+    t = torch.as_tensor(a, dtype=torch.float64, device=device)
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"PyVolumetricMaterial.eval returned shape {tuple(t.shape)}, expected {tuple(shape)}")
+    return t.contiguous()
+
+
+class VolumetricFemEnergyPyMaterialTetP1(Energy):
+    """VolumetricFemEnergy[Material, TetP1Basis, TetCentroidQuadrature] for a
+    PyVolumetricMaterial subclass ``material`` (set by the template), on one GPU: the library
+    exports every element's deformation gradient, the material evaluates W and its derivatives
+    on the device, and the library integrates (E = sum vol W, g_a = vol P grad N_a) and assembles
+    the Hessian (vol B^T A B, Exact or per-element eigenvalue clamp) as for the native material."""
+
+    material = None
+
+    def __init__(self, displacement_map, rest_position_fields, Fp, theta, batch_size=256):
+        import torch
+
+        mat = self.material
+        if mat is None or not isinstance(mat.num_parameters, int) or mat.num_parameters < 0:
+            raise ValueError("PyVolumetricMaterial: num_parameters must be a non-negative int")
+        if isinstance(batch_size, bool) or int(batch_size) <= 0:
+            raise ValueError("MeshEnergy: invalid batch size")
+        T = displacement_map.num_elements
+        k = mat.num_parameters
+        th = _sample_fields(theta, T, k, "theta") if k > 0 else np.zeros((T, 0))
+        if th is None:
+            raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
+        fp = _sample_fields(Fp, T, 9, "Fp")
+        fp = np.tile(np.eye(3).ravel(), (T, 1)) if fp is None else np.array(np.broadcast_to(fp, (T, 9)))
+        # The geometry handle: the native records carry only rest geometry here.
+        self._geo = VolumetricFemEnergyTetP1(displacement_map, rest_position_fields, None, np.array([1.0, 1.0]),
+                                             batch_size)
+        self.map = displacement_map
+        self.num_vertices, self.num_elements, self.num_dofs = (self._geo.num_vertices, self._geo.num_elements,
+                                                               self._geo.num_dofs)
+        self.nnzb, self.nnz = self._geo.nnzb, self._geo.nnz
+        self.device = torch.device("cuda", self._geo.device)
+        # Fp column-major vec -> (T, 3, 3) matrices.
+        self._Fp = torch.as_tensor(np.ascontiguousarray(fp, dtype=np.float64).reshape(T, 3, 3).transpose(0, 2, 1),
+                                   device=self.device).contiguous()
+        self._theta = torch.as_tensor(np.array(np.broadcast_to(th, (T, k)), dtype=np.float64),
+                                      device=self.device).contiguous()
+
+    @property
+    def handle(self):
+        return self._geo.handle
+
+    def pattern_csc(self):
+        return self._geo.pattern_csc()
+
+    def pattern_bsr(self):
+        return self._geo.pattern_bsr()
+
+    def _u(self, x):
+        import torch
+
+        if isinstance(x, torch.Tensor):
+            u = x.detach().to(device=self.device, dtype=torch.float64).contiguous()
+        else:
+            u = torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device=self.device)
+        if u.numel() != self.num_dofs:
+            raise ValueError("Energy: x must have num_dofs finite entries")
+        return u
+
+    def deformation_gradients(self, x):
+        """(T, 3, 3) CUDA tensor of F = I + grad u per element."""
+        import torch
+
+        u = self._u(x)
+        F = torch.empty((self.num_elements, 3, 3), dtype=torch.float64, device=self.device)
+        N.check(N.lib.lpg_fem_set_stream(self.handle, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
+        N.check(N.lib.lpg_fem_deformation_gradients(self.handle, N.vptr(u), N.MEM_DEVICE, N.vptr(F)))
+        return F
+
+    def _material(self, F, outputs):
+        out = self.material.eval(F, self._Fp, self._theta, outputs=outputs)
+        T = self.num_elements
+        shapes = {"W": (T,), "dW_dF": (T, 3, 3), "d2W_dF2": (T, 3, 3, 3, 3)}
+        return [_cuda_f64(out[name], shapes[name], self.device) for name in outputs]
+
+    def eval_device(self, x, gradient=True, hessian=None, precision="f64", layout="bsr"):
+        """Energy (float), gradient and Hessian values as CUDA tensors (block-CSR or CSC order)."""
+        import torch
+
+        kind = _hessian_kind(hessian)
+        prec = _precision(precision)
+        lay = N.LAYOUT_BSR if layout == "bsr" else N.LAYOUT_CSC
+        F = self.deformation_gradients(x)
+        outputs = ("W",) + (("dW_dF",) if gradient else ()) + (("d2W_dF2",) if kind else ())
+        vals = self._material(F, outputs)
+        W = vals[0]
+        P = vals[1] if gradient else None
+        A = vals[-1] if kind else None
+        g = torch.empty(self.num_dofs, dtype=torch.float64, device=self.device) if gradient else None
+        H = None
+        if kind:
+            dt = torch.float64 if prec == N.PRECISION_F64 else torch.float32
+            H = torch.empty(self.nnz, dtype=dt, device=self.device)
+        E = ctypes.c_double()
+        N.check(N.lib.lpg_fem_set_stream(self.handle, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
+        N.check(N.lib.lpg_fem_eval_material(self.handle, N.vptr(W), N.vptr(P), N.vptr(A), N.MEM_DEVICE,
+                                            ctypes.byref(E), N.vptr(g), kind, prec, lay, N.vptr(H), N.MEM_DEVICE))
+        return E.value, g, H
+
+    def eval(self, x, gradient=False, hessian=None, precision="f64"):
+        """(value, gradient or None, csc_matrix or None), like the native energy."""
+        import scipy.sparse as sp
+
+        E, g, H = self.eval_device(x, gradient=gradient, hessian=hessian, precision=precision, layout="csc")
+        gh = g.cpu().numpy() if g is not None else None
+        Hs = None
+        if H is not None:
+            outer, inner = self.pattern_csc()
+            Hs = sp.csc_matrix((H.double().cpu().numpy(), inner, outer), shape=(self.num_dofs,) * 2)
+        return E, gh, Hs
+
+    def eval_value(self, x):
+        return self.eval(x)[0]
+
+    def eval_gradient(self, x):
+        return self.eval(x, gradient=True)[1]
+
+    def eval_hessian(self, x, kind=HessianKind.Exact):
+        return self.eval(x, hessian=kind)[2]
+
+    def max_feasible_step(self, x, dx):
+        """The material's bound when it has eval_feasible_step (min over elements, in [0, 1]);
+        otherwise the largest step keeping det F > 0 (the native feasible step)."""
+        import torch
+
+        if self.material.eval_feasible_step is None:
+            u = self._u(x)
+            du = self._u(dx)
+            a = ctypes.c_double()
+            N.check(N.lib.lpg_fem_set_stream(self.handle, None))
+            N.check(N.lib.lpg_fem_feasible_step(self.handle, N.vptr(u), N.vptr(du), N.MEM_DEVICE, ctypes.byref(a)))
+            return a.value
+        F = self.deformation_gradients(x)
+        dF = self.deformation_gradients(dx) - torch.eye(3, dtype=torch.float64, device=self.device)
+        bound = _cuda_f64(self.material.eval_feasible_step(F, self._Fp, self._theta, dF), (self.num_elements,),
+                          self.device)
+        if not bool(torch.all(torch.isfinite(bound))):
+            raise ValueError("PyVolumetricMaterial.eval_feasible_step returned non-finite values")
+        return float(torch.clamp(bound, 0.0, 1.0).min()) if self.num_elements else 1.0
+
+
+def _py_energy_class(material):
+    return type(f"VolumetricFemEnergy[{material.__name__}]", (VolumetricFemEnergyPyMaterialTetP1,),
+                {"material": material})
+
+
 VolumetricFemEnergy = Template("VolumetricFemEnergy",
                                {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyTetP1})
+VolumetricFemEnergy.material_factory = _py_energy_class
 VolumetricFemForceMaterialResponse = Template(
     "VolumetricFemForceMaterialResponse",
     {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceMaterialResponseTetP1})

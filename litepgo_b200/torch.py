@@ -6,8 +6,10 @@ gradient in the forward pass, a response is differentiated through its VJP (reve
 or JVP (forward mode, where the model has one) at a saved copy of the input. The reference
 takes one-dimensional CPU float64 tensors; CUDA float64 tensors are accepted here too, and an
 energy of a CUDA tensor is evaluated and differentiated on that device without host copies.
-The torch-material classes of the reference (TorchVolumetricMaterial, TorchShellMaterial) are
-not part of this path.
+``TorchVolumetricMaterial`` (src/python/torch.py:72-94 of the reference) is a
+PyVolumetricMaterial whose density W(F, Fp, theta) is written in PyTorch: its derivatives come
+from autograd on whatever device F lives on, so with this package's energies they are computed
+on the GPU for the whole mesh at once. The shell material class is not part of this path.
 """
 
 import numpy as np
@@ -15,9 +17,55 @@ import torch
 from torch.autograd.function import once_differentiable
 
 from .energy import QuadraticEnergy, WeightedSumEnergy
-from .fem import VolumetricFemEnergyTetP1
+from .fem import PyVolumetricMaterial, VolumetricFemEnergyTetP1
 
-__all__ = ["energy", "response"]
+__all__ = ["energy", "response", "TorchVolumetricMaterial"]
+
+
+class TorchVolumetricMaterial(PyVolumetricMaterial):
+    """A PyVolumetricMaterial whose density is written in PyTorch.
+
+    Subclass it, set ``num_parameters`` and define ``W(F, Fp, theta)`` as a static or class
+    method taking float64 tensors (N,3,3), (N,3,3), (N,k) and returning the (N,) density per
+    reference volume; rows must be independent and W twice differentiable in F. ``eval`` takes
+    dW/dF by one backward pass and d2W/dF2 by nine more ([n,i,j,k,l] = d2W/dF_ij dF_kl), on the
+    device of F.
+    """
+
+    @classmethod
+    def W(cls, F, Fp, theta):
+        raise NotImplementedError("TorchVolumetricMaterial subclasses must define W(F, Fp, theta)")
+
+    @classmethod
+    def eval(cls, F, Fp, theta, *, outputs):
+        need2 = "d2W_dF2" in outputs
+        need1 = need2 or "dW_dF" in outputs
+        n = F.shape[0]
+        with torch.enable_grad():
+            Fv = F.detach().clone().requires_grad_(need1)
+            W = cls.W(Fv, Fp.detach(), theta.detach())
+            if tuple(W.shape) != (n,):
+                raise ValueError(f"TorchVolumetricMaterial.W must return shape ({n},)")
+            out = {"W": W.detach()}
+            if need1:
+                if not W.requires_grad:
+                    dW = torch.zeros_like(Fv)
+                else:
+                    (dW,) = torch.autograd.grad(W.sum(), Fv, create_graph=need2, allow_unused=True)
+                    dW = torch.zeros_like(Fv) if dW is None else dW
+                out["dW_dF"] = dW.detach()
+                if need2:
+                    rows = []
+                    for i in range(3):
+                        for j in range(3):
+                            if dW.requires_grad:
+                                (g,) = torch.autograd.grad(dW[:, i, j].sum(), Fv, retain_graph=True, allow_unused=True)
+                            else:
+                                g = None
+                            rows.append(torch.zeros_like(Fv) if g is None else g)
+                    # rows[3 i + j][n, k, l] = d2W / dF_ij dF_kl
+                    out["d2W_dF2"] = torch.stack(rows, 1).reshape(n, 3, 3, 3, 3).detach()
+        return out
 
 
 def _check(x):

@@ -1,0 +1,141 @@
+"""Python/Torch materials on the GPU path (the reference's PyVolumetricMaterial and
+TorchVolumetricMaterial): the library exports F per element, the material evaluates W and its
+derivatives on the device, the library integrates and assembles. A torch neo-Hookean must
+reproduce the native NeoHookean energy; a torch St. Venant-Kirchhoff material is checked against
+a dense NumPy assembly of vol B^T vec P and vol B^T A B from the same material on the CPU."""
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from litepgo_b200 import dof, energy, fem, mesh, workloads
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+from litepgo_b200.torch import TorchVolumetricMaterial  # noqa: E402
+
+Exact, Projected = energy.HessianKind.Exact, energy.HessianKind.Projected
+
+
+class TorchNeoHookean(TorchVolumetricMaterial):
+    num_parameters = 2
+
+    @staticmethod
+    def W(F, Fp, theta):
+        lam, mu = theta[:, 0], theta[:, 1]
+        L = torch.log(torch.linalg.det(F))
+        return 0.5 * mu * ((F * F).sum((1, 2)) - 3) - mu * L + 0.5 * lam * L * L
+
+
+class TorchStVK(TorchVolumetricMaterial):
+    num_parameters = 2
+
+    @staticmethod
+    def W(F, Fp, theta):
+        lam, mu = theta[:, 0], theta[:, 1]
+        I = torch.eye(3, dtype=F.dtype, device=F.device)
+        E = 0.5 * (F.transpose(1, 2) @ F - I)
+        tr = E.diagonal(dim1=1, dim2=2).sum(1)
+        return mu * (E * E).sum((1, 2)) + 0.5 * lam * tr * tr
+
+
+def build(material, w):
+    topo = mesh.TetTopology(w["X"].shape[0], w["tets"])
+    cls = fem.VolumetricFemEnergy[material, fem.TetP1Basis, fem.TetCentroidQuadrature]
+    return cls(dof.VertexDofMap(topo, 3), w["X"], None, w["theta"])
+
+
+def test_torch_neo_hookean_matches_the_native_energy():
+    w = workloads.deformed_box(6, seed=3)
+    native = fem.VolumetricFemEnergyTetP1.from_arrays(w["X"], w["tets"], w["theta"])
+    py = build(TorchNeoHookean, w)
+    u = w["u"]
+    H_exact = None
+    for hk, tol in ((Exact, 1e-12), (Projected, 1e-11)):
+        E0, g0, H0 = native.eval(u, gradient=True, hessian=hk)
+        E1, g1, H1 = py.eval(u, gradient=True, hessian=hk)
+        assert abs(E1 - E0) <= 1e-12 * abs(E0)
+        assert rel_err(g1, g0) <= 1e-12
+        assert rel_err(H1.data, H0.data) <= tol
+        if hk == Exact:
+            H_exact = H0
+    # Mixed precision: FP32 blocks from the same FP64 material outputs.
+    _, _, H32 = py.eval(u, hessian=Exact, precision="mixed")
+    assert rel_err(H32.data, H_exact.data) <= 1e-5
+    # The default feasible step is the native one (det F > 0).
+    du = 0.5 * np.random.default_rng(1).standard_normal(u.size)
+    assert py.max_feasible_step(u, du) == native.max_feasible_step(u, du)
+
+
+def dense_reference(material, X, tets, theta, u):
+    """E, g and dense H of sum_e vol [W, B^T vec P, B^T A B] with the material on the CPU."""
+    T, n = tets.shape[0], X.size
+    U = u.reshape(-1, 3)
+    Fs, vols, grads = [], [], []
+    for cell in tets:
+        Dm = np.stack([X[cell[k + 1]] - X[cell[0]] for k in range(3)], 1)
+        Dmi = np.linalg.inv(Dm)
+        gN = np.vstack([-Dmi.sum(0), Dmi])  # rows grad N_a
+        Fs.append(np.eye(3) + (U[cell[1:]] - U[cell[0]]).T @ Dmi)
+        vols.append(np.linalg.det(Dm) / 6)
+        grads.append(gN)
+    F = torch.tensor(np.array(Fs))
+    out = material.eval(F, torch.eye(3, dtype=torch.float64).expand(T, 3, 3),
+                        torch.tensor(np.broadcast_to(theta, (T, 2)).copy()), outputs=("W", "dW_dF", "d2W_dF2"))
+    W, P, A = out["W"].numpy(), out["dW_dF"].numpy(), out["d2W_dF2"].numpy()
+    E, g, H = 0.0, np.zeros(n), np.zeros((n, n))
+    for e, cell in enumerate(tets):
+        vol, gN = vols[e], grads[e]
+        E += vol * W[e]
+        dofs = (3 * cell[:, None] + np.arange(3)).ravel()
+        # dF_ij / du_(a,k) = delta_ik gN[a, j]
+        Bm = np.zeros((9, 12))
+        for a in range(4):
+            for i in range(3):
+                for j in range(3):
+                    Bm[3 * i + j, 3 * a + i] = gN[a, j]
+        g[dofs] += vol * Bm.T @ P[e].ravel()
+        H[np.ix_(dofs, dofs)] += vol * Bm.T @ A[e].reshape(9, 9) @ Bm
+    return E, g, H
+
+
+def test_torch_stvk_matches_a_dense_assembly():
+    w = workloads.deformed_box(3, seed=5)
+    X, tets = w["X"], w["tets"]
+    theta = np.array([1.4e5, 3.4e4])
+    w2 = dict(w, theta=theta)
+    py = build(TorchStVK, w2)
+    u = w["u"]
+    E, g, H = py.eval(u, gradient=True, hessian=Exact)
+    Er, gr, Hr = dense_reference(TorchStVK, X, tets, theta, u)
+    assert abs(E - Er) <= 1e-12 * abs(Er)
+    assert rel_err(g, gr) <= 1e-12
+    assert rel_err(H.toarray(), Hr) <= 1e-12
+    # Projected: positive semi-definite and equal to the Exact one where that already is.
+    _, _, Hp = py.eval(u, hessian=Projected)
+    x = np.random.default_rng(2).standard_normal(u.size)
+    assert x @ (Hp @ x) >= -1e-10 * np.abs(Hp.data).max() * (x @ x)
+
+
+def test_non_finite_material_outputs_are_rejected():
+    class Broken(TorchVolumetricMaterial):
+        num_parameters = 0
+
+        @staticmethod
+        def W(F, Fp, theta):
+            return torch.log(F[:, 0, 0] - 10.0)  # NaN at these states
+
+    w = workloads.deformed_box(2, seed=0)
+    topo = mesh.TetTopology(w["X"].shape[0], w["tets"])
+    e = fem.VolumetricFemEnergy[Broken, fem.TetP1Basis, fem.TetCentroidQuadrature](
+        dof.VertexDofMap(topo, 3), w["X"], None, None)
+    with pytest.raises(ValueError):
+        e.eval(w["u"], gradient=True)
+
+    class Bounded(TorchNeoHookean):
+        @staticmethod
+        def eval_feasible_step(F, Fp, theta, dF):
+            return torch.full((F.shape[0],), 0.5, dtype=F.dtype, device=F.device)
+
+    b = build(Bounded, w)
+    assert b.max_feasible_step(w["u"], np.ones(w["u"].size)) == 0.5

@@ -1,0 +1,69 @@
+"""TorchVolumetricMaterial (src/python/torch.py:72-94 of the reference): derivatives by autograd,
+checked on the CPU against the oracle's closed-form neo-Hookean W, dW/dF and d2W/dF2
+(NeoHookean, neo_hookean.cpp:33-86)."""
+
+import numpy as np
+import pytest
+
+import oracle
+
+torch = pytest.importorskip("torch")
+from litepgo_b200 import fem  # noqa: E402
+from litepgo_b200.torch import TorchVolumetricMaterial  # noqa: E402
+
+
+class TorchNeoHookean(TorchVolumetricMaterial):
+    num_parameters = 2
+
+    @staticmethod
+    def W(F, Fp, theta):
+        lam, mu = theta[:, 0], theta[:, 1]
+        L = torch.log(torch.linalg.det(F))
+        return 0.5 * mu * ((F * F).sum((1, 2)) - 3) - mu * L + 0.5 * lam * L * L
+
+
+def test_torch_neo_hookean_derivatives_match_the_oracle():
+    rng = np.random.default_rng(0)
+    n = 6
+    F = torch.tensor(np.eye(3) + 0.2 * rng.standard_normal((n, 3, 3)))
+    theta = torch.tensor(np.stack([rng.uniform(1e3, 1e5, n), rng.uniform(1e3, 1e5, n)], 1))
+    Fp = torch.eye(3, dtype=torch.float64).expand(n, 3, 3)
+    out = TorchNeoHookean.eval(F, Fp, theta, outputs=("W", "dW_dF", "d2W_dF2"))
+    assert out["W"].shape == (n,) and out["dW_dF"].shape == (n, 3, 3) and out["d2W_dF2"].shape == (n, 3, 3, 3, 3)
+    for k in range(n):
+        Fk, th = F[k].numpy(), theta[k].numpy()
+        W = oracle.nh_W(Fk, np.eye(3), th)
+        P = oracle.nh_dW_dF(Fk, np.eye(3), th)
+        D = oracle.nh_d2W_dF2(Fk, np.eye(3), th)  # column-major vec indices i + 3 j
+        A = out["d2W_dF2"][k].numpy()
+        Acol = np.empty((9, 9))
+        for i in range(3):
+            for j in range(3):
+                for kk in range(3):
+                    for ll in range(3):
+                        Acol[i + 3 * j, kk + 3 * ll] = A[i, j, kk, ll]
+        assert abs(out["W"][k].item() - W) <= 1e-12 * abs(W) + 1e-9
+        np.testing.assert_allclose(out["dW_dF"][k].numpy(), P, rtol=1e-12, atol=1e-12 * np.abs(P).max())
+        np.testing.assert_allclose(Acol, D, rtol=1e-12, atol=1e-12 * np.abs(D).max())
+
+
+def test_requested_outputs_only_and_shape_checks():
+    F = torch.eye(3, dtype=torch.float64).expand(2, 3, 3).clone()
+    th = torch.tensor([[1.0, 1.0], [1.0, 1.0]])
+    out = TorchNeoHookean.eval(F, F, th, outputs=("W",))
+    assert set(out) == {"W"} and torch.all(out["W"].abs() < 1e-12)
+
+    class Bad(TorchVolumetricMaterial):
+        num_parameters = 0
+
+        @staticmethod
+        def W(F, Fp, theta):
+            return F.sum()
+
+    with pytest.raises(ValueError):
+        Bad.eval(F, F, th[:, :0], outputs=("W",))
+    # The template accepts a Python material in the Material slot.
+    cls = fem.VolumetricFemEnergy[TorchNeoHookean, fem.TetP1Basis, fem.TetCentroidQuadrature]
+    assert issubclass(cls, fem.VolumetricFemEnergyPyMaterialTetP1) and cls.material is TorchNeoHookean
+    with pytest.raises(TypeError):
+        fem.VolumetricFemEnergy[int, fem.TetP1Basis, fem.TetCentroidQuadrature]
