@@ -33,6 +33,7 @@ void check_cuda(cudaError_t e, const char* what);
 // in e).
 struct HostPlan {
     int V = 0, T = 0;
+    int K = 4; // vertices per cell: 4 (tet) or 8 (hex)
     std::vector<int32_t> row_ptr, col_idx;   // BSR pattern (V+1, nnzb)
     std::vector<int32_t> inc_ptr;            // V+1: pairs per row, natural order
     std::vector<int32_t> diag_slot;          // V: block index of (v, v), -1 for an unused vertex
@@ -58,8 +59,9 @@ struct HostPlan {
     // it, then the diagonal slots (cl_noff off-diagonal in all). Slot word: bits 0-7 the row within the cluster, bits
     // 8-29 the slot's position within its row, bit 30 "store the transpose", bit 31 diagonal.
     // Entry word of a slot: bits 0-19 first contributor (within the cluster), 20-31 count.
-    // Contributors (uint16): element within the cluster << 4 | a << 2 | b, where (a, b) are
-    // the local indices of the lower- and higher-numbered vertex of the slot (a = b diagonal).
+    // Contributors (uint16): element within the cluster << 2s | a << s | b (s = 2 bits for tets,
+    // 3 for hexes), where (a, b) are the local indices of the lower- and higher-numbered vertex
+    // of the slot (a = b diagonal).
     std::vector<int32_t> cl_row_ptr, cl_rows;
     std::vector<int32_t> cl_el_ptr;
     std::vector<uint32_t> cl_els;
@@ -99,7 +101,7 @@ void write_veg(const std::string& path, int V, const double* positions, int T, i
 void validate_volume_mesh(int V, const std::vector<double>& positions, int width, const std::vector<int32_t>& cells);
 
 // Validates connectivity (mesh_topology.hpp:25-44) and builds the plan.
-void build_plan(int V, int T, const int32_t* tets, HostPlan& plan);
+void build_plan(int V, int T, const int32_t* cells, HostPlan& plan, int K = 4);
 // Checks the cluster plan's invariants (throws LPG_ELOGIC on a violation).
 void check_clusters(const HostPlan& plan, const int32_t* tets);
 // Checks the solvers' upper-triangle sliced-ELL layout against the BSR pattern (LPG_ELOGIC).

@@ -29,7 +29,8 @@ namespace {
 // are computed by the same operations and are exact transposes.
 void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>& inc) {
     const int V = p.V, T = p.T;
-    constexpr int kMaskE = (1 << 30) - 1;
+    constexpr int kMaskE = (1 << 29) - 1;
+    const int K = p.K, sh = K == 4 ? 2 : 3; // vertices per cell, bits per local index in a contributor
     std::vector<int32_t> cl_of(static_cast<size_t>(V), -1), qstamp(static_cast<size_t>(V), -1);
     std::vector<int32_t> estamp(static_cast<size_t>(T), -1);
     std::vector<int32_t> queue;
@@ -95,7 +96,7 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
         for (size_t i = 0; i < els.size(); ++i) {
             const int e = els[i];
             eloc[e] = static_cast<int32_t>(i);
-            const bool owner = cl_of[tets[4 * static_cast<size_t>(e)]] == c;
+            const bool owner = cl_of[tets[K * static_cast<size_t>(e)]] == c;
             p.cl_els.push_back(static_cast<uint32_t>(e) | (owner ? 0x80000000u : 0u));
         }
         p.cl_el_ptr.push_back(static_cast<int32_t>(p.cl_els.size()));
@@ -109,17 +110,17 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
             const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
             bucket.assign(static_cast<size_t>(nb), {});
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
-                const int e = inc[k] & kMaskE, a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> 30);
-                const uint16_t el = static_cast<uint16_t>(eloc[e] << 4);
-                for (int b = 0; b < 4; ++b) {
-                    const int w = tets[4 * static_cast<size_t>(e) + b];
+                const int e = inc[k] & kMaskE, a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> 29);
+                const uint16_t el = static_cast<uint16_t>(eloc[e] << (2 * sh));
+                for (int b = 0; b < K; ++b) {
+                    const int w = tets[K * static_cast<size_t>(e) + b];
                     if (w == v) {
-                        diag[j].push_back(static_cast<uint16_t>(el | (a << 2) | a));
+                        diag[j].push_back(static_cast<uint16_t>(el | (a << sh) | a));
                         continue;
                     }
                     const int32_t* beg = p.col_idx.data() + rb;
                     const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
-                    bucket[q].push_back(static_cast<uint16_t>(v < w ? (el | (a << 2) | b) : (el | (b << 2) | a)));
+                    bucket[q].push_back(static_cast<uint16_t>(v < w ? (el | (a << sh) | b) : (el | (b << sh) | a)));
                 }
             }
             for (int q = 0; q < nb; ++q) {
@@ -161,33 +162,36 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
 
 } // namespace
 
-void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
+void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
+    p.K = K;
     if (V < 0 || T < 0) fail(LPG_EINVAL, "MeshTopology requires a non-negative vertex count");
     if (V > std::numeric_limits<int>::max() / 3) fail(LPG_EINVAL, "VertexDofMap requires total DOFs fitting in int");
-    if (T >= (1 << 30)) fail(LPG_EINVAL, "mesh has too many elements for the assembly plan (limit 2^30)");
+    if (K != 4 && K != 8) fail(LPG_EINVAL, "cells must have 4 (tet) or 8 (hex) vertices");
+    if (T >= (1 << 29)) fail(LPG_EINVAL, "mesh has too many elements for the assembly plan (limit 2^29)");
     for (int e = 0; e < T; ++e) {
-        int s[4];
-        std::memcpy(s, tets + 4 * static_cast<size_t>(e), sizeof s);
-        std::sort(s, s + 4);
-        if (s[0] < 0 || s[3] >= V)
+        int s[8];
+        std::memcpy(s, tets + K * static_cast<size_t>(e), K * sizeof(int));
+        std::sort(s, s + K);
+        if (s[0] < 0 || s[K - 1] >= V)
             fail(LPG_EINVAL, "MeshTopology cell " + std::to_string(e) + " has vertex indices outside [0, num_vertices)");
-        if (s[0] == s[1] || s[1] == s[2] || s[2] == s[3])
-            fail(LPG_EINVAL, "MeshTopology cell " + std::to_string(e) + " must contain distinct vertices");
+        for (int a = 1; a < K; ++a)
+            if (s[a] == s[a - 1])
+                fail(LPG_EINVAL, "MeshTopology cell " + std::to_string(e) + " must contain distinct vertices");
     }
     p.V = V;
     p.T = T;
     // Incidence (row -> pairs in element order), by counting sort.
     p.inc_ptr.assign(static_cast<size_t>(V) + 1, 0);
-    for (int64_t k = 0; k < 4 * static_cast<int64_t>(T); ++k) ++p.inc_ptr[tets[k] + 1];
+    for (int64_t k = 0; k < K * static_cast<int64_t>(T); ++k) ++p.inc_ptr[tets[k] + 1];
     for (int v = 0; v < V; ++v) p.inc_ptr[v + 1] += p.inc_ptr[v];
     const int64_t npairs = p.inc_ptr[V];
     std::vector<int32_t> inc(static_cast<size_t>(npairs));
     {
         std::vector<int32_t> fill(p.inc_ptr.begin(), p.inc_ptr.end() - 1);
         for (int e = 0; e < T; ++e)
-            for (int a = 0; a < 4; ++a) {
-                const int v = tets[4 * static_cast<size_t>(e) + a];
-                inc[fill[v]++] = e | (a << 30);
+            for (int a = 0; a < K; ++a) {
+                const int v = tets[K * static_cast<size_t>(e) + a];
+                inc[fill[v]++] = e | (a << 29);
             }
     }
     int maxdeg = 0;
@@ -205,8 +209,8 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p) {
         for (int v = 0; v < V; ++v) {
             buf.clear();
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
-                const int e = inc[k] & ((1 << 30) - 1);
-                for (int b = 0; b < 4; ++b) buf.push_back(tets[4 * static_cast<size_t>(e) + b]);
+                const int e = inc[k] & ((1 << 29) - 1);
+                for (int b = 0; b < K; ++b) buf.push_back(tets[K * static_cast<size_t>(e) + b]);
             }
             std::sort(buf.begin(), buf.end());
             buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
@@ -302,15 +306,16 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
     const int V = p.V, T = p.T;
     const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
     auto bad = [](const char* what) { fail(LPG_ELOGIC, std::string("assembly cluster plan: ") + what); };
-    auto vert = [&](int e, int a) { return tets[4 * static_cast<size_t>(e) + a]; };
+    const int K = p.K, sh = K == 4 ? 2 : 3;
+    auto vert = [&](int e, int a) { return tets[K * static_cast<size_t>(e) + a]; };
     // Incidence (vertex -> elements, ascending), independent of the plan's own.
     std::vector<int32_t> ptr(static_cast<size_t>(V) + 1, 0), inc(4 * static_cast<size_t>(T));
-    for (size_t k = 0; k < 4 * static_cast<size_t>(T); ++k) ++ptr[tets[k] + 1];
+    for (size_t k = 0; k < K * static_cast<size_t>(T); ++k) ++ptr[tets[k] + 1];
     for (int v = 0; v < V; ++v) ptr[v + 1] += ptr[v];
     {
         std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
         for (int e = 0; e < T; ++e)
-            for (int a = 0; a < 4; ++a) inc[fill[vert(e, a)]++] = e;
+            for (int a = 0; a < K; ++a) inc[fill[vert(e, a)]++] = e;
     }
     std::vector<int> owner(static_cast<size_t>(V), -1), energy_count(static_cast<size_t>(T), 0);
     for (int c = 0; c < ncl; ++c)
@@ -327,7 +332,7 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
             const int e = static_cast<int>(p.cl_els[e0 + i] & 0x7fffffffu);
             if (i > 0 && e <= static_cast<int>(p.cl_els[e0 + i - 1] & 0x7fffffffu)) bad("elements not ascending");
             bool touches = false;
-            for (int a = 0; a < 4; ++a) touches = touches || owner[vert(e, a)] == c;
+            for (int a = 0; a < K; ++a) touches = touches || owner[vert(e, a)] == c;
             if (!touches) bad("element not incident to the cluster");
             if (p.cl_els[e0 + i] >> 31) {
                 if (owner[vert(e, 0)] != c) bad("energy counted by a non-owner");
@@ -363,14 +368,14 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
             for (int k = ptr[v]; k < ptr[v + 1]; ++k) {
                 const int e = inc[k];
                 bool has = false;
-                for (int a = 0; a < 4; ++a) has = has || vert(e, a) == w;
+                for (int a = 0; a < K; ++a) has = has || vert(e, a) == w;
                 if (has) expect.push_back(e);
             }
             if ((de >> 20) != expect.size()) bad("slot contributor count");
             const size_t off = p.cl_ent_ptr[c] + (de & 0xfffffu);
             for (size_t t = 0; t < expect.size(); ++t) {
                 const uint16_t en = p.cl_ents[off + t];
-                const int el = en >> 4, a = (en >> 2) & 3, b = en & 3;
+                const int el = en >> (2 * sh), a = (en >> sh) & (K - 1), b = en & (K - 1);
                 if (el >= ne) bad("contributor outside the cluster");
                 const int e = static_cast<int>(p.cl_els[e0 + el] & 0x7fffffffu);
                 if (e != expect[t]) bad("contributor list differs from the elements sharing the block");
