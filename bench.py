@@ -678,7 +678,22 @@ def run_rows():
         back = mesh.read_veg(path)
         tr = time.perf_counter() - t0
         exact = bool(np.array_equal(back.positions, X) and np.array_equal(back.cells, tets))
-    line = {"rows": "plastic-field force VJP, adjoint in Fp, VEG I/O", "config": workload_config(),
+    # Hex Q1 (GaussLegendre3D[2]) E + gradient + Exact Hessian on a 48^3 hex box.
+    Xh, ch = mesh.make_hex_box(48)
+    eh = fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexQ1Basis, fem.GaussLegendre3D[2]].from_arrays(
+        Xh, ch, np.array([1.4e5, 3.4e4]))
+    uh = torch.as_tensor(state(Xh), device=dev)
+    gh = torch.empty(Xh.size, dtype=torch.float64, device=dev)
+    Hh = torch.empty(eh.nnz, dtype=torch.float64, device=dev)
+    N.check(N.lib.lpg_fem_set_stream(eh.handle, ctypes.c_void_p(stream.cuda_stream)))
+    ma, me = ctypes.c_double(), ctypes.c_double()
+    N.check(N.lib.lpg_fem_time_eval(eh.handle, N.vptr(uh), N.vptr(gh), int(energy.HessianKind.Exact), N.PRECISION_F64,
+                                    N.LAYOUT_BSR, N.vptr(Hh), 10, 1, ctypes.byref(ma), ctypes.byref(me)))
+    hex_row = {"mesh": f"hex box 48^3 ({ch.shape[0]} hexes, {Xh.shape[0]} vertices, nnzb {eh.nnzb}), 8 points",
+               "element_pass_and_gather_ms": ma.value, "eval_ms": me.value, "hexes_per_s": ch.shape[0] / (me.value * 1e-3),
+               "timing": "lpg_fem_time_eval: CUDA events, L2 flushed between launches, FP64 E + gradient + Exact BSR"}
+    line = {"rows": "plastic-field force VJP, adjoint in Fp, VEG I/O, hex Q1", "config": workload_config(),
+            "hex_q1": hex_row,
             "fp_vjp": fp_row, "newton_with_fp": {"status": r.status.name, "iterations": r.iterations, "seconds": r.seconds},
             "adjoint_fp": adj,
             "veg": {"bytes": size, "write_s": tw, "read_s": tr, "read_mb_per_s": size / tr / 1e6,

@@ -126,6 +126,21 @@ int lpg_fem_create(int num_vertices, const double* X, int num_tets, const int32_
                    const double* theta, int theta_per_element, const double* Fp, int device, lpg_fem_t* out);
 int lpg_fem_destroy(lpg_fem_t h);
 
+/*
+ * Hex Q1 mesh: VolumetricFemEnergy<NeoHookean, HexQ1Basis, GaussLegendre3D<n>>
+ * (src/core/fem/assembly/volumetric_fem_energy.hpp:29-65 with fem/basis/3d/hex_q1_basis.hpp,
+ * fem/quadrature/3d/gauss_legendre_3d.hpp). cells: 8 per element in HexQ1Basis corner order
+ * ((0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1) of [0,1]^3); X: rest
+ * positions (3 per vertex); theta: [lambda, mu] (2, or 2 per element); points_per_axis: 2 or
+ * 4. Every quadrature point must have det J > 0 (LPG_EINVAL otherwise, as
+ * VolumetricElement3D). The handle answers lpg_fem_eval (Exact Hessian; the projected one is
+ * LPG_EINVAL), lpg_fem_feasible_step, lpg_fem_element_energies, the patterns, and
+ * lpg_newton_solve with the Exact Hessian; the sensitivity, plastic-field, material and batch
+ * entry points are for tet meshes only (LPG_EINVAL). No plastic field (Fp = I).
+ */
+int lpg_fem_create_hex(int num_vertices, const double* X, int num_cells, const int32_t* cells, const double* theta,
+                       int theta_per_element, int points_per_axis, int device, lpg_fem_t* out);
+
 /* Uses `stream` (a cudaStream_t) for all later work of this handle; NULL = the handle's own stream. */
 int lpg_fem_set_stream(lpg_fem_t h, void* stream);
 

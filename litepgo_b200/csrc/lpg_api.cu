@@ -61,6 +61,51 @@ template <class T> T* upload(DeviceBuffer& b, const std::vector<T>& v) {
     return p;
 }
 
+// Copies the host plan's arrays to the device mirror (every mesh kind).
+void upload_plan(lpg_fem& hh, int V, int T) {
+    lpg_fem* h = &hh;
+    const HostPlan& p = h->plan;
+    DevMesh& m = h->dm;
+    m.V = V;
+    m.T = T;
+    m.nnzb = p.nnzb();
+    m.row_ptr = upload(h->b_row_ptr, p.row_ptr);
+    m.col_idx = upload(h->b_col_idx, p.col_idx);
+    m.inc_ptr = upload(h->b_inc_ptr, p.inc_ptr);
+    m.diag_slot = upload(h->b_diag_slot, p.diag_slot);
+    m.unused_rows = upload(h->b_unused, p.unused_rows);
+    m.num_unused = static_cast<int>(p.unused_rows.size());
+    m.sell_ptr = upload(h->b_sell[0], p.sell_ptr);
+    m.sell_row = upload(h->b_sell[1], p.sell_row);
+    m.sell_col = upload(h->b_sell[2], p.sell_col);
+    m.sell_base = upload(h->b_sell[3], p.sell_base);
+    m.sell_bptr = upload(h->b_sell[4], p.sell_bptr);
+    m.sell_bref = reinterpret_cast<int2*>(upload(h->b_sell[5], p.sell_bref));
+    m.n_sell = static_cast<int>(p.sell_ptr.size()) - 1;
+    m.ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
+    m.cl_row_ptr = upload(h->b_cl[0], p.cl_row_ptr);
+    m.cl_rows = upload(h->b_cl[1], p.cl_rows);
+    m.cl_el_ptr = upload(h->b_cl[2], p.cl_el_ptr);
+    m.cl_els = upload(h->b_cl[3], p.cl_els);
+    m.cl_slot_ptr = upload(h->b_cl[4], p.cl_slot_ptr);
+    m.cl_noff = upload(h->b_cl[5], p.cl_noff);
+    m.cl_slot = upload(h->b_cl[6], p.cl_slot);
+    m.cl_slot_ent = upload(h->b_cl[7], p.cl_slot_ent);
+    m.cl_ent_ptr = upload(h->b_cl[8], p.cl_ent_ptr);
+    m.cl_ents = upload(h->b_cl[9], p.cl_ents);
+    m.cl_ntr = upload(h->b_cl[10], p.cl_ntr);
+    m.cl_max_slots = m.cl_max_ents = 0;
+    for (int c = 0; c < m.ncl; ++c) {
+        m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);
+        m.cl_max_ents = std::max(m.cl_max_ents, p.cl_ent_ptr[c + 1] - p.cl_ent_ptr[c]);
+    }
+}
+
+// Entry points whose kernels exist for tet meshes only.
+void tet_only(const lpg_fem& h, const char* what) {
+    if (h.dm.K != 4) fail(LPG_EINVAL, std::string(what) + " is available for tet meshes only");
+}
+
 // 3x3 row-major helpers for the element records.
 double det3(const double* a) {
     return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) + a[2] * (a[3] * a[7] - a[4] * a[6]);
@@ -149,6 +194,16 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.ev_end = ev_end;
     const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
     a.cl_variant = tune.cl[pi];
+    if (dm.K == 8) {
+        if (a.hess && hessian == LPG_HESSIAN_PROJECTED)
+            fail(LPG_EINVAL, "the projected Hessian is available for tet meshes only");
+        const size_t T = static_cast<size_t>(dm.T);
+        double* elemE = delem ? delem : d_mat[3].as<double>(std::max<size_t>(T, 1));
+        void* blocks = a.hess ? d_proj.ensure(T * kHexRecord * (precision == LPG_PRECISION_F64 ? 8 : 4)) : nullptr;
+        a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(dm.ncl) + 256);
+        launch_hex_eval(dm, precision, du, elemE, d_vjp.as<double>(std::max<size_t>(24 * T, 1)), blocks, a, stream);
+        return;
+    }
     if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {
         void* proj = d_proj.ensure(project_bytes(dm, precision));
         launch_project(dm, precision, hessian, du, proj, a.status, stream,
@@ -275,41 +330,8 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
             r[11] = theta_per_element ? theta[2 * static_cast<size_t>(e) + 1] : theta[1];
         }
         std::vector<float> rec32(rec.begin(), rec.end());
-        const HostPlan& p = h->plan;
+        upload_plan(*h, V, T);
         DevMesh& m = h->dm;
-        m.V = V;
-        m.T = T;
-        m.nnzb = p.nnzb();
-        m.row_ptr = upload(h->b_row_ptr, p.row_ptr);
-        m.col_idx = upload(h->b_col_idx, p.col_idx);
-        m.inc_ptr = upload(h->b_inc_ptr, p.inc_ptr);
-        m.diag_slot = upload(h->b_diag_slot, p.diag_slot);
-        m.unused_rows = upload(h->b_unused, p.unused_rows);
-        m.num_unused = static_cast<int>(p.unused_rows.size());
-        m.sell_ptr = upload(h->b_sell[0], p.sell_ptr);
-        m.sell_row = upload(h->b_sell[1], p.sell_row);
-        m.sell_col = upload(h->b_sell[2], p.sell_col);
-        m.sell_base = upload(h->b_sell[3], p.sell_base);
-        m.sell_bptr = upload(h->b_sell[4], p.sell_bptr);
-        m.sell_bref = reinterpret_cast<int2*>(upload(h->b_sell[5], p.sell_bref));
-        m.n_sell = static_cast<int>(p.sell_ptr.size()) - 1;
-        m.ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
-        m.cl_row_ptr = upload(h->b_cl[0], p.cl_row_ptr);
-        m.cl_rows = upload(h->b_cl[1], p.cl_rows);
-        m.cl_el_ptr = upload(h->b_cl[2], p.cl_el_ptr);
-        m.cl_els = upload(h->b_cl[3], p.cl_els);
-        m.cl_slot_ptr = upload(h->b_cl[4], p.cl_slot_ptr);
-        m.cl_noff = upload(h->b_cl[5], p.cl_noff);
-        m.cl_slot = upload(h->b_cl[6], p.cl_slot);
-        m.cl_slot_ent = upload(h->b_cl[7], p.cl_slot_ent);
-        m.cl_ent_ptr = upload(h->b_cl[8], p.cl_ent_ptr);
-        m.cl_ents = upload(h->b_cl[9], p.cl_ents);
-        m.cl_ntr = upload(h->b_cl[10], p.cl_ntr);
-        m.cl_max_slots = m.cl_max_ents = 0;
-        for (int c = 0; c < m.ncl; ++c) {
-            m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);
-            m.cl_max_ents = std::max(m.cl_max_ents, p.cl_ent_ptr[c + 1] - p.cl_ent_ptr[c]);
-        }
         std::vector<int32_t> tv(tets, tets + 4 * static_cast<size_t>(T));
         m.tets = reinterpret_cast<int4*>(upload(h->b_tets, tv));
         m.rec64 = upload(h->b_rec64, rec);
@@ -324,6 +346,89 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
         // Launch variants tuned on this mesh unless LPG_AUTOTUNE=0 (then the defaults stay).
         const char* at = std::getenv("LPG_AUTOTUNE");
         if (!(at && std::strcmp(at, "0") == 0)) autotune(*h);
+        *out = h.release();
+    });
+}
+
+int lpg_fem_create_hex(int V, const double* X, int T, const int32_t* cells, const double* theta,
+                       int theta_per_element, int points_per_axis, int device, lpg_fem_t* out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!out) fail(LPG_EINVAL, "lpg_fem_create_hex: null output handle");
+        if (T > 0 && (!cells || !theta || !X)) fail(LPG_EINVAL, "lpg_fem_create_hex: null input array");
+        if (points_per_axis != 2 && points_per_axis != 4)
+            fail(LPG_EINVAL, "GaussLegendre3D is instantiated for 2 or 4 points per axis");
+        auto h = std::make_unique<lpg_fem>();
+        h->device = device;
+        LPG_CUDA(cudaSetDevice(device));
+        LPG_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+        build_plan(V, T, cells, h->plan, 8);
+        // Gauss-Legendre points on [0,1]^3, last axis fastest (gauss_legendre_3d.hpp), and the
+        // trilinear basis derivatives at each (hex_q1_basis.hpp corner order).
+        const int n = points_per_axis, nq = n * n * n;
+        double t1[4], w1[4];
+        if (n == 2) {
+            t1[0] = 0.5 - 0.5 / std::sqrt(3.0);
+            t1[1] = 0.5 + 0.5 / std::sqrt(3.0);
+            w1[0] = w1[1] = 0.5;
+        } else {
+            const double outer = std::sqrt((3 + 2 * std::sqrt(6.0 / 5)) / 7), inner = std::sqrt((3 - 2 * std::sqrt(6.0 / 5)) / 7);
+            t1[0] = 0.5 * (1 - outer);
+            t1[1] = 0.5 * (1 - inner);
+            t1[2] = 0.5 * (1 + inner);
+            t1[3] = 0.5 * (1 + outer);
+            w1[0] = w1[3] = (18 - std::sqrt(30.0)) / 72;
+            w1[1] = w1[2] = (18 + std::sqrt(30.0)) / 72;
+        }
+        static const int corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                         {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+        std::vector<double> qt(25 * static_cast<size_t>(nq));
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                for (int k = 0; k < n; ++k) {
+                    const int q = (i * n + j) * n + k;
+                    const double xi[3] = {t1[i], t1[j], t1[k]};
+                    for (int a = 0; a < 8; ++a) {
+                        double f[3], df[3];
+                        for (int d = 0; d < 3; ++d) {
+                            f[d] = corner[a][d] ? xi[d] : 1 - xi[d];
+                            df[d] = corner[a][d] ? 1.0 : -1.0;
+                        }
+                        qt[25 * q + 3 * a] = df[0] * f[1] * f[2];
+                        qt[25 * q + 3 * a + 1] = f[0] * df[1] * f[2];
+                        qt[25 * q + 3 * a + 2] = f[0] * f[1] * df[2];
+                    }
+                    qt[25 * q + 24] = w1[i] * w1[j] * w1[k];
+                }
+        // Construction checks of VolumetricElement3D (volumetric_element.hpp:23-39) at every point.
+        for (size_t v = 0; v < 3 * static_cast<size_t>(V); ++v)
+            if (!std::isfinite(X[v])) fail(LPG_EINVAL, "VolumetricElement3D: invalid reference Jacobian");
+        for (int e = 0; e < T; ++e)
+            for (int q = 0; q < nq; ++q) {
+                double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                for (int a = 0; a < 8; ++a) {
+                    const double* Xa = X + 3 * static_cast<size_t>(cells[8 * static_cast<size_t>(e) + a]);
+                    for (int i = 0; i < 3; ++i)
+                        for (int d = 0; d < 3; ++d) J[3 * i + d] += Xa[i] * qt[25 * q + 3 * a + d];
+                }
+                const double det = det3(J), w = qt[25 * q + 24] * det;
+                if (!std::isfinite(det) || det <= 0 || !std::isfinite(w))
+                    fail(LPG_EINVAL, "VolumetricElement3D: invalid reference determinant or volume weight");
+            }
+        std::vector<double> th(2 * static_cast<size_t>(T));
+        for (int e = 0; e < T; ++e)
+            for (int c = 0; c < 2; ++c) th[2 * static_cast<size_t>(e) + c] = theta_per_element ? theta[2 * static_cast<size_t>(e) + c] : theta[c];
+        upload_plan(*h, V, T);
+        DevMesh& m = h->dm;
+        m.K = 8;
+        m.nq = nq;
+        m.hex_X = upload(h->b_hex[0], std::vector<double>(X, X + 3 * static_cast<size_t>(V)));
+        m.hex_cells = upload(h->b_hex[1], std::vector<int32_t>(cells, cells + 8 * static_cast<size_t>(T)));
+        m.hex_theta = upload(h->b_hex[2], th);
+        m.hex_q = upload(h->b_hex[3], qt);
+        LPG_CUDA(cudaMemset(h->d_status.as<unsigned>(1), 0, sizeof(unsigned)));
+        LPG_CUDA(cudaDeviceSynchronize());
         *out = h.release();
     });
 }
@@ -429,6 +534,7 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
 int lpg_fem_deformation_gradients(lpg_fem_t h, const double* u, int io_mem, double* F) {
     return guarded([&] {
         if (!h || !F) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: null argument");
+        tet_only(*h, "lpg_fem_deformation_gradients");
         if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: the handle has a plastic field");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
@@ -446,6 +552,7 @@ int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const d
                           double* grad, int hessian, int precision, int layout, void* hess, int out_mem) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
+        tet_only(*h, "lpg_fem_eval_material");
         if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_eval_material: the handle has a plastic field");
         const size_t T = static_cast<size_t>(h->dm.T), n = 3 * static_cast<size_t>(h->dm.V);
         if (T > 0 && (!W || (grad && !P))) fail(LPG_EINVAL, "lpg_fem_eval_material: null material output");
@@ -569,6 +676,7 @@ int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io
 int lpg_fem_force_vjp_theta(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
+        tet_only(*h, "lpg_fem_force_vjp_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         const size_t n = 3 * static_cast<size_t>(h->dm.V);
@@ -620,6 +728,7 @@ int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double
 int lpg_fem_set_fp(lpg_fem_t h, const double* Fp, int fp_per_element) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
+        tet_only(*h, "lpg_fem_set_fp");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         DevMesh& m = h->dm;
@@ -666,6 +775,7 @@ int lpg_fem_set_fp(lpg_fem_t h, const double* Fp, int fp_per_element) {
 int lpg_fem_force_vjp_fp(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
     return guarded([&] {
         if (!h || !out) fail(LPG_EINVAL, "lpg_fem_force_vjp_fp: null argument");
+        tet_only(*h, "lpg_fem_force_vjp_fp");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         const size_t n = 3 * static_cast<size_t>(h->dm.V);
@@ -693,6 +803,7 @@ int lpg_adjoint_fp(lpg_fem_t h, const double* u_star, const double* dLdu, const 
                    int io_mem, int precision, double cg_tolerance, int per_element, double* dFp, double* lambda_out) {
     return guarded([&] {
         if (!h || !u_star || !dLdu || !dFp) fail(LPG_EINVAL, "lpg_adjoint_fp: null argument");
+        tet_only(*h, "lpg_adjoint_fp");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         adjoint_fp(*h, u_star, dLdu, fixed_dofs, num_fixed, io_mem, precision, cg_tolerance, per_element, dFp,
@@ -782,6 +893,7 @@ int lpg_fem_set_tuning(lpg_fem_t h, const int32_t choice[6]) {
 int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
+        tet_only(*h, "lpg_fem_set_theta");
         if (!theta && h->dm.T > 0) fail(LPG_EINVAL, "lpg_fem_set_theta: null theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
@@ -799,6 +911,7 @@ int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element) {
 int lpg_fem_force_vjp_rest(lpg_fem_t h, const double* u, const double* w, int io_mem, double* out) {
     return guarded([&] {
         if (!h || !out) fail(LPG_EINVAL, "lpg_fem_force_vjp_rest: null argument");
+        tet_only(*h, "lpg_fem_force_vjp_rest");
         if (!h->from_vertices || h->dm.fpinv64)
             fail(LPG_EINVAL, "rest-position sensitivity needs vertex rest positions and no plastic field");
         BusyGuard busy(h->busy);
@@ -819,6 +932,7 @@ int lpg_adjoint_rest(lpg_fem_t h, const double* u_star, const double* dLdu, cons
                      int io_mem, int precision, double cg_tolerance, double* dX, double* lambda_out) {
     return guarded([&] {
         if (!h || !u_star || !dLdu || !dX) fail(LPG_EINVAL, "lpg_adjoint_rest: null argument");
+        tet_only(*h, "lpg_adjoint_rest");
         if (!h->from_vertices || h->dm.fpinv64)
             fail(LPG_EINVAL, "rest-position sensitivity needs vertex rest positions and no plastic field");
         BusyGuard busy(h->busy);
@@ -833,6 +947,7 @@ int lpg_batch_newton_solve(lpg_fem_t h, int num_meshes, const int32_t* vertex_of
                            lpg_newton_result* result) {
     return guarded([&] {
         if (!h || !o || !x_out || (!x0 && h->dm.V > 0)) fail(LPG_EINVAL, "lpg_batch_newton_solve: null argument");
+        tet_only(*h, "lpg_batch_newton_solve");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         batch_newton_solve(*h, num_meshes, vertex_offsets, element_offsets, fixed, nfixed, f_ext, x0, io_mem, *o, x_out,
@@ -845,6 +960,7 @@ int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, con
                       double* lambda_out) {
     return guarded([&] {
         if (!h || !u_star || !dLdu || !dtheta) fail(LPG_EINVAL, "lpg_adjoint_theta: null argument");
+        tet_only(*h, "lpg_adjoint_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         adjoint_theta(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, per_element, dtheta,

@@ -1381,8 +1381,24 @@ void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
 // lower- and higher-numbered vertex; the stored block is H_{min(a,b) max(a,b)}, read transposed
 // when a > b.
 // ---------------------------------------------------------------------------
-template <typename R>
+// Cell-size traits of the block gather: K vertices per cell, bits per local index in a
+// contributor, values per element in the block scratch, and the pair index of (a, b), a <= b.
+template <int K> struct CellBlocks;
+template <> struct CellBlocks<4> {
+    static constexpr int shift = 2, record = kProjRecord;
+    static __device__ __forceinline__ int pair(int a, int b) { return pair10(a, b); }
+};
+template <> struct CellBlocks<8> {
+    static constexpr int shift = 3, record = kHexRecord;
+    static __device__ __forceinline__ int pair(int a, int b) {
+        const int lo = min(a, b), hi = max(a, b);
+        return lo * 8 - (lo * (lo - 1)) / 2 + (hi - lo);
+    }
+};
+
+template <typename R, int K = 4>
 __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh m, const EvalArgs a) {
+    using CB = CellBlocks<K>;
     using HT = typename HOut<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     int* sel = reinterpret_cast<int*>(smem_raw); // [kClusterElems] element ids
@@ -1427,8 +1443,8 @@ __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh 
             R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             for (int c = 0; c < cnt; ++c) {
                 const int w = en[c];
-                const int el = w >> 4, la = (w >> 2) & 3, lb = w & 3;
-                const R* blk = blocks + kProjRecord * static_cast<size_t>(sel[el]) + 9 * pair10(la, lb);
+                const int el = w >> (2 * CB::shift), la = (w >> CB::shift) & (K - 1), lb = w & (K - 1);
+                const R* blk = blocks + CB::record * static_cast<size_t>(sel[el]) + 9 * CB::pair(la, lb);
                 R bv[9];
 #pragma unroll
                 for (int t = 0; t < 9; ++t) bv[t] = __ldg(blk + t);
@@ -1455,7 +1471,7 @@ __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh 
     if ((tid & 31) == 0 && st) atomicOr(a.status, st);
 }
 
-template <typename R> void launch_block_gather(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+template <typename R, int K = 4> void launch_block_gather(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = block_gather_fixed() + (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16 +
                       2 * static_cast<size_t>(m.cl_max_ents);
     thread_local size_t cached_sm = 0;
@@ -1463,15 +1479,15 @@ template <typename R> void launch_block_gather(const DevMesh& m, const EvalArgs&
     if (cached_sm != sm) {
         int dev = 0, sms = 0, per_sm = 0;
         LPG_CUDA(cudaGetDevice(&dev));
-        LPG_CUDA(cudaFuncSetAttribute(block_gather_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        LPG_CUDA(cudaFuncSetAttribute(block_gather_kernel<R, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(sm)));
         LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, block_gather_kernel<R>, kClThreads, sm));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, block_gather_kernel<R, K>, kClThreads, sm));
         resident = std::max(1, sms * std::max(per_sm, 1));
         cached_sm = sm;
     }
     const int blocks = std::min(resident, m.ncl);
-    if (blocks > 0) block_gather_kernel<R><<<blocks, kClThreads, sm, s>>>(m, a);
+    if (blocks > 0) block_gather_kernel<R, K><<<blocks, kClThreads, sm, s>>>(m, a);
     LPG_CUDA(cudaGetLastError());
 }
 
@@ -1551,6 +1567,7 @@ __global__ void __launch_bounds__(128) rest_vjp_kernel(const DevMesh m, const do
 
 // out[v] = sign * sum over the elements of v (ascending) of the per-element vertex values
 // (12 per element); vertices of no element are left to zero_rows_kernel.
+template <int K = 4>
 __global__ void __launch_bounds__(128) vertex_gather_kernel(const DevMesh m, const double* __restrict__ per_elem,
                                                             double sign, double* __restrict__ out) {
     for (int cl = blockIdx.x; cl < m.ncl; cl += gridDim.x) {
@@ -1564,10 +1581,11 @@ __global__ void __launch_bounds__(128) vertex_gather_kernel(const DevMesh m, con
             double acc[3] = {0, 0, 0};
             for (int c = 0; c < static_cast<int>(de >> 20); ++c) {
                 const int wd = __ldg(en + c);
-                const size_t e = __ldg(m.cl_els + e0 + (wd >> 4)) & 0x7fffffffu;
-                const int a = (wd >> 2) & 3;
+                constexpr int sh = K == 4 ? 2 : 3;
+                const size_t e = __ldg(m.cl_els + e0 + (wd >> (2 * sh))) & 0x7fffffffu;
+                const int a = (wd >> sh) & (K - 1);
 #pragma unroll
-                for (int i = 0; i < 3; ++i) acc[i] += __ldg(per_elem + 12 * e + 3 * a + i);
+                for (int i = 0; i < 3; ++i) acc[i] += __ldg(per_elem + 3 * K * e + 3 * a + i);
             }
 #pragma unroll
             for (int i = 0; i < 3; ++i) out[3 * static_cast<size_t>(v) + i] = sign * acc[i];
@@ -1654,6 +1672,244 @@ __global__ void __launch_bounds__(256) material_pieces_kernel(const DevMesh m, c
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
+// ---------------------------------------------------------------------------
+// Hex Q1 neo-Hookean element pass (VolumetricFemEnergy<NeoHookean, HexQ1Basis, GaussLegendre3D<n>>,
+// volumetric_fem_energy.hpp:78-123 with hex_q1_basis.hpp and gauss_legendre_3d.hpp). One thread
+// per (element, vertex pair a <= b): at every quadrature point it forms J = sum_c X_c dN_c^T,
+// w = weight det J, grad N = J^-T dN, F = I + (sum_c u_c dN_c^T) J^-1, and accumulates
+// H_ab += w [mu (grad N_a . grad N_b) I + lambda h_a h_b^T - p h_b h_a^T], h = F^-T grad N; the
+// pair (a, a) threads also accumulate g_a = sum w P grad N_a and the (0, 0) thread the energy.
+// FP64 throughout; the blocks are stored in the precision's type. The kinematics are recomputed
+// by each of an element's 36 threads (cheap next to reading a per-point cache).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void hex_pair(int pr, int& a, int& b) {
+    a = 0;
+    int base = 0;
+    while (pr >= base + (8 - a)) {
+        base += 8 - a;
+        ++a;
+    }
+    b = a + (pr - base);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) hex_element_kernel(const DevMesh m, const double* __restrict__ u,
+                                                          double* __restrict__ elemE, double* __restrict__ per_elem,
+                                                          R* __restrict__ blocks, unsigned* status) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    const int e = t / 36, pr = t - 36 * (t / 36);
+    if (e < m.T) {
+        int a, b;
+        hex_pair(pr, a, b);
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        const double lam = m.hex_theta[2 * static_cast<size_t>(e)], mu = m.hex_theta[2 * static_cast<size_t>(e) + 1];
+        if (!(lam >= 0 && mu > 0 && isfinite(lam) && isfinite(mu))) st |= ST_BAD_THETA;
+        double Hb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, ga[3] = {0, 0, 0}, E = 0;
+        for (int q = 0; q < m.nq; ++q) {
+            const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
+            double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            bool ok = true;
+            for (int c = 0; c < 8; ++c) {
+                const int v = __ldg(cell + c);
+                double dn[3], X[3], uu[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    dn[d] = __ldg(dq + 3 * c + d);
+                    X[d] = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + d);
+                    uu[d] = __ldg(u + 3 * static_cast<size_t>(v) + d);
+                    ok = ok && isfinite(uu[d]);
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        J[3 * i + d] = fma(X[i], dn[d], J[3 * i + d]);
+                        G[3 * i + d] = fma(uu[i], dn[d], G[3 * i + d]);
+                    }
+            }
+            if (!ok) st |= ST_BAD_INPUT;
+            // J^-1 by cofactors (det J > 0 was checked when the mesh was built).
+            double Ji[9];
+            const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                              J[2] * (J[3] * J[7] - J[4] * J[6]);
+            const double iJ = 1.0 / dJ;
+            Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
+            Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
+            Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
+            Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
+            Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
+            Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
+            Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
+            Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
+            Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+            const double w = __ldg(dq + 24) * dJ;
+            double F[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    F[3 * i + j] = (i == j ? 1.0 : 0.0) + G[3 * i] * Ji[j] + G[3 * i + 1] * Ji[3 + j] + G[3 * i + 2] * Ji[6 + j];
+            double C[9]; // cofactors: F^-T = C / det F
+            C[0] = F[4] * F[8] - F[5] * F[7];
+            C[1] = F[5] * F[6] - F[3] * F[8];
+            C[2] = F[3] * F[7] - F[4] * F[6];
+            C[3] = F[2] * F[7] - F[1] * F[8];
+            C[4] = F[0] * F[8] - F[2] * F[6];
+            C[5] = F[1] * F[6] - F[0] * F[7];
+            C[6] = F[1] * F[5] - F[2] * F[4];
+            C[7] = F[2] * F[3] - F[0] * F[5];
+            C[8] = F[0] * F[4] - F[1] * F[3];
+            const double detF = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+            if (!(detF > 0) || !isfinite(detF)) {
+                st |= isfinite(detF) ? ST_BAD_DET : ST_NONFINITE_F;
+                continue;
+            }
+            const double L = log(detF), p = lam * L - mu;
+            double FiT[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) FiT[k] = C[k] / detF;
+            // grad N of a and b: rows of dN J^-1.
+            double na[3], nb[3];
+            const double* dA = dq + 3 * a;
+            const double* dB = dq + 3 * b;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                na[j] = __ldg(dA) * Ji[j] + __ldg(dA + 1) * Ji[3 + j] + __ldg(dA + 2) * Ji[6 + j];
+                nb[j] = __ldg(dB) * Ji[j] + __ldg(dB + 1) * Ji[3 + j] + __ldg(dB + 2) * Ji[6 + j];
+            }
+            double ha[3], hb[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                ha[i] = FiT[3 * i] * na[0] + FiT[3 * i + 1] * na[1] + FiT[3 * i + 2] * na[2];
+                hb[i] = FiT[3 * i] * nb[0] + FiT[3 * i + 1] * nb[1] + FiT[3 * i + 2] * nb[2];
+            }
+            const double dn = na[0] * nb[0] + na[1] * nb[1] + na[2] * nb[2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    double v = lam * ha[i] * hb[k] - p * hb[i] * ha[k];
+                    if (i == k) v += mu * dn;
+                    Hb[3 * i + k] = fma(w, v, Hb[3 * i + k]);
+                }
+            if (a == b) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    double s = 0;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) s += (mu * F[3 * i + j] + p * FiT[3 * i + j]) * na[j];
+                    ga[i] = fma(w, s, ga[i]);
+                }
+                if (a == 0) {
+                    double ff = 0;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) ff += F[k] * F[k];
+                    E = fma(w, 0.5 * mu * (ff - 3.0) - mu * L + 0.5 * lam * L * L, E);
+                }
+            }
+        }
+        if (a == b) { // a diagonal block: mirror the upper triangle so the matrix is bitwise symmetric
+            Hb[3] = Hb[1];
+            Hb[6] = Hb[2];
+            Hb[7] = Hb[5];
+        }
+        if (blocks) {
+            R* o = blocks + kHexRecord * static_cast<size_t>(e) + 9 * pr;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                if (!isfinite(Hb[k])) st |= ST_NONFINITE_OUT;
+                o[k] = static_cast<R>(Hb[k]);
+            }
+        }
+        if (a == b && per_elem) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (!isfinite(ga[i])) st |= ST_NONFINITE_OUT;
+                per_elem[24 * static_cast<size_t>(e) + 3 * a + i] = ga[i];
+            }
+        }
+        if (pr == 0) {
+            if (!isfinite(E)) st |= ST_NONFINITE_OUT;
+            elemE[e] = E;
+        }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// Feasible step of a hex mesh: at every quadrature point F and dF (the increment's gradient),
+// the reference's positive-determinant step, minimum per block.
+__global__ void __launch_bounds__(256) hex_feasible_kernel(const DevMesh m, const double* __restrict__ u,
+                                                           const double* __restrict__ du, double* block_min,
+                                                           unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double alpha = 1.0;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        for (int q = 0; q < m.nq && st == 0; ++q) {
+            const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
+            double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, D[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            bool ok = true;
+            for (int c = 0; c < 8; ++c) {
+                const int v = __ldg(cell + c);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
+                    const double uu = u[3 * static_cast<size_t>(v) + i], dd = du[3 * static_cast<size_t>(v) + i];
+                    ok = ok && isfinite(uu) && isfinite(dd);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const double dn = __ldg(dq + 3 * c + d);
+                        J[3 * i + d] = fma(X, dn, J[3 * i + d]);
+                        G[3 * i + d] = fma(uu, dn, G[3 * i + d]);
+                        D[3 * i + d] = fma(dd, dn, D[3 * i + d]);
+                    }
+                }
+            }
+            if (!ok) {
+                st |= ST_BAD_INPUT;
+                break;
+            }
+            const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                              J[2] * (J[3] * J[7] - J[4] * J[6]);
+            const double iJ = 1.0 / dJ;
+            double Ji[9];
+            Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
+            Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
+            Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
+            Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
+            Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
+            Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
+            Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
+            Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
+            Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+            double F[9], dF[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    F[3 * i + j] = (i == j ? 1.0 : 0.0) + G[3 * i] * Ji[j] + G[3 * i + 1] * Ji[3 + j] + G[3 * i + 2] * Ji[6 + j];
+                    dF[3 * i + j] = D[3 * i] * Ji[j] + D[3 * i + 1] * Ji[3 + j] + D[3 * i + 2] * Ji[6 + j];
+                }
+            alpha = fmin(alpha, positive_det_step(F, dF, st));
+        }
+    }
+    __shared__ double sm[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) alpha = fmin(alpha, __shfl_xor_sync(0xffffffffu, alpha, off));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = alpha;
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = sm[0];
+        for (int w = 1; w < (blockDim.x >> 5); ++w) v = fmin(v, sm[w]);
+        block_min[blockIdx.x] = v;
+    }
+}
+
 // Lame parameters of every element record (FP64 and FP32 copies).
 __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __restrict__ theta, int per_element, int T) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1722,7 +1978,7 @@ void launch_rest_vjp(const DevMesh& m, const double* u, const double* w, double*
                      unsigned* status, cudaStream_t s) {
     if (m.T > 0) {
         rest_vjp_kernel<<<(m.T + 127) / 128, 128, 0, s>>>(m, u, w, per_elem, status);
-        vertex_gather_kernel<<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, sign, out);
+        vertex_gather_kernel<4><<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, sign, out);
     }
     if (m.num_unused > 0) zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(out, m.unused_rows, m.num_unused);
     LPG_CUDA(cudaGetLastError());
@@ -1817,6 +2073,11 @@ int feasible_blocks(const DevMesh& m) { return (m.T + 255) / 256; }
 
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
                      double* alpha, unsigned* status, cudaStream_t s, double* per_elem) {
+    if (m.K == 8) {
+        if (per_elem) fail(LPG_EINVAL, "per-element feasible steps are available for tet meshes only");
+        launch_hex_feasible(m, u, du, block_min, nblocks, alpha, status, s);
+        return;
+    }
     if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status, per_elem);
     min_kernel<<<1, 1024, 0, s>>>(block_min, nblocks, alpha);
     LPG_CUDA(cudaGetLastError());
@@ -1860,7 +2121,7 @@ void launch_material_eval(const DevMesh& m, int precision, int hessian, const do
                           int clamp_variant, const EvalArgs& a, cudaStream_t s) {
     if (m.T > 0) {
         material_pieces_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, W, P, elemE, a.grad ? per_elem : nullptr, a.status);
-        if (a.grad) vertex_gather_kernel<<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
+        if (a.grad) vertex_gather_kernel<4><<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
     }
     if (a.grad && m.num_unused > 0)
         zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
@@ -1881,6 +2142,45 @@ void launch_material_eval(const DevMesh& m, int precision, int hessian, const do
             launch_block_gather<float>(m, ga, s);
         }
     }
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_hex_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem, void* blocks,
+                     const EvalArgs& a, cudaStream_t s) {
+    if (m.T > 0) {
+        const size_t threads = 36 * static_cast<size_t>(m.T);
+        const int grid = static_cast<int>((threads + 127) / 128);
+        if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
+        if (precision == LPG_PRECISION_F64)
+            hex_element_kernel<double><<<grid, 128, 0, s>>>(m, u, elemE, a.grad ? per_elem : nullptr,
+                                                           a.hess ? static_cast<double*>(blocks) : nullptr, a.status);
+        else
+            hex_element_kernel<float><<<grid, 128, 0, s>>>(m, u, elemE, a.grad ? per_elem : nullptr,
+                                                          a.hess ? static_cast<float*>(blocks) : nullptr, a.status);
+        if (a.grad) vertex_gather_kernel<8><<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
+        if (a.hess) {
+            EvalArgs ga = a;
+            ga.proj = blocks;
+            if (precision == LPG_PRECISION_F64)
+                launch_block_gather<double, 8>(m, ga, s);
+            else
+                launch_block_gather<float, 8>(m, ga, s);
+        }
+        if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
+    }
+    if (a.grad && m.num_unused > 0)
+        zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(elemE, m.T, a.cluster_energy);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.cluster_energy, kSumBlocks, a.energy);
+    LPG_CUDA(cudaGetLastError());
+}
+
+int hex_feasible_blocks(const DevMesh& m) { return (m.T + 255) / 256; }
+
+void launch_hex_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
+                         double* alpha, unsigned* status, cudaStream_t s) {
+    if (nblocks > 0) hex_feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status);
+    min_kernel<<<1, 1024, 0, s>>>(block_min, nblocks, alpha);
     LPG_CUDA(cudaGetLastError());
 }
 

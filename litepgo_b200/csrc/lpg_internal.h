@@ -132,6 +132,14 @@ struct DevMesh {
     // Fp^-1 row-major (9 per element) when the mesh has a plastic field, else null.
     double* fpinv64 = nullptr;
     float* fpinv32 = nullptr;
+    // Hex Q1 meshes (K = 8): rest positions (3 per vertex), cells (8 per element), [lambda, mu]
+    // per element, and per quadrature point the 8 x 3 reference derivatives dN/dxi and the
+    // weight (25 values per point, nq points).
+    int K = 4, nq = 0;
+    double* hex_X = nullptr;
+    int32_t* hex_cells = nullptr;
+    double* hex_theta = nullptr;
+    double* hex_q = nullptr;
 };
 
 // Internal Hessian layout of the solvers: the upper-triangle sliced ELL of HostPlan::sell_*
@@ -184,6 +192,8 @@ size_t project_bytes(const DevMesh& m, int precision);
 // Values per element of the projected-Hessian scratch: the element's ten 3x3 blocks (pair10
 // order), or, for an element listed for the clamp until it is clamped, its 9x9 tangent (45).
 constexpr int kProjRecord = 90;
+// Values per element of the hex block scratch: 36 blocks (a <= b of 8 vertices) of 3x3.
+constexpr int kHexRecord = 324;
 // per_elem (T doubles, optional) receives each element's step.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
                      double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr);
@@ -195,6 +205,16 @@ void launch_rest_vjp(const DevMesh& m, const double* u, const double* w, double*
                      unsigned* status, cudaStream_t s);
 void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cudaStream_t s);
 void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s);
+// Hex Q1 element pass (K = 8): energy per element into elemE (T), gradient pieces (24 per element)
+// into per_elem when a.grad is set, the 36 blocks per element (precision's type) into blocks when
+// a.hess is set (Exact only), then the gradient gather, the energy sum and the block gather.
+void launch_hex_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem, void* blocks,
+                     const EvalArgs& a, cudaStream_t s);
+// Largest step along du keeping det F > 0 at every quadrature point of every hex (x 0.9 as the
+// reference), minimum over the mesh into *alpha (device).
+void launch_hex_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
+                         double* alpha, unsigned* status, cudaStream_t s);
+int hex_feasible_blocks(const DevMesh& m);
 // Materials evaluated by the caller: F (9 T, row-major) at u, then integration and assembly of
 // the caller's W (T), P = dW/dF (9 T) and, for a Hessian, A = d2W/dF2 (81 T) — energy into
 // a.energy (a.cluster_energy is scratch of >= 256 values), gradient into a.grad if set, Hessian

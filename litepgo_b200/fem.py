@@ -38,6 +38,9 @@ __all__ = [
     "VolumetricFemForceFpResponseTetP1",
     "PyVolumetricMaterial",
     "VolumetricFemEnergyPyMaterialTetP1",
+    "HexQ1Basis",
+    "GaussLegendre3D",
+    "VolumetricFemEnergyHexQ1",
 ]
 
 
@@ -60,6 +63,69 @@ class TetP1Basis:
     @staticmethod
     def eval_dN_dxi(xi):
         return np.array([[-1.0, -1, -1], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+
+
+class HexQ1Basis:
+    """Trilinear hex shape functions on [0,1]^3 (hex_q1_basis.hpp), corners in the order
+    (0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1)."""
+
+    num_basis_functions = 8
+    corners = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+
+    @classmethod
+    def eval_N(cls, xi):
+        xi = np.asarray(xi, dtype=np.float64)
+        f = np.stack([1 - xi, xi])  # f[c, d]
+        return np.array([f[i, 0] * f[j, 1] * f[k, 2] for i, j, k in cls.corners])
+
+    @classmethod
+    def eval_dN_dxi(cls, xi):
+        xi = np.asarray(xi, dtype=np.float64)
+        f = np.stack([1 - xi, xi])
+        df = np.array([-1.0, 1.0])
+        return np.array([[df[i] * f[j, 1] * f[k, 2], f[i, 0] * df[j] * f[k, 2], f[i, 0] * f[j, 1] * df[k]]
+                         for i, j, k in cls.corners])
+
+
+class _GaussLegendre3D:
+    """Gauss-Legendre points on [0,1]^3, last axis fastest (gauss_legendre_3d.hpp)."""
+
+    points_per_axis = None
+
+    @classmethod
+    def _rule(cls):
+        n = cls.points_per_axis
+        if n == 2:
+            return np.array([0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0)]), np.array([0.5, 0.5])
+        outer = np.sqrt((3 + 2 * np.sqrt(6.0 / 5)) / 7)
+        inner = np.sqrt((3 - 2 * np.sqrt(6.0 / 5)) / 7)
+        wo, wi = (18 - np.sqrt(30.0)) / 72, (18 + np.sqrt(30.0)) / 72
+        return (np.array([0.5 * (1 - outer), 0.5 * (1 - inner), 0.5 * (1 + inner), 0.5 * (1 + outer)]),
+                np.array([wo, wi, wi, wo]))
+
+    @classmethod
+    def points(cls):
+        t, _ = cls._rule()
+        return np.array([[a, b, c] for a in t for b in t for c in t])
+
+    @classmethod
+    def weights(cls):
+        _, w = cls._rule()
+        return np.array([a * b * c for a in w for b in w for c in w])
+
+
+class GaussLegendre3D_2(_GaussLegendre3D):
+    points_per_axis = 2
+    num_points = 8
+
+
+class GaussLegendre3D_4(_GaussLegendre3D):
+    points_per_axis = 4
+    num_points = 64
+
+
+GaussLegendre3D_2.__name__ = "GaussLegendre3D[2]"
+GaussLegendre3D_4.__name__ = "GaussLegendre3D[4]"
 
 
 class TetCentroidQuadrature:
@@ -115,7 +181,7 @@ class Template:
         except KeyError:
             names = ", ".join(getattr(a, "__name__", repr(a)) for a in key)
             avail = "; ".join(
-                f"{self.__name__}[{', '.join(a.__name__ for a in k)}]" for k in self._instances)
+                f"{self.__name__}[{', '.join(getattr(a, '__name__', repr(a)) for a in k)}]" for k in self._instances)
             raise TypeError(f"{self.__name__}[{names}] is not instantiated; available: {avail}") from None
 
     @property
@@ -629,6 +695,64 @@ class VolumetricFemForceFpResponseTetP1:
         return out
 
 
+class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
+    """VolumetricFemEnergy[NeoHookean, HexQ1Basis, GaussLegendre3D[n]] on one GPU (the class
+    variable ``points_per_axis`` is set by the template). The rest positions are vertex positions
+    (V, 3); no plastic field. The Energy interface is the tet energy's, with the Exact Hessian only
+    (a projected request raises ValueError); Newton runs with hessian=Exact."""
+
+    points_per_axis = 2
+
+    def __init__(self, displacement_map, rest_position_fields, Fp, theta, batch_size=256):
+        if isinstance(batch_size, bool) or int(batch_size) <= 0:
+            raise ValueError("MeshEnergy: invalid batch size")
+        if not isinstance(displacement_map, VertexDofMap) or displacement_map.dofs_per_vertex != 3:
+            raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
+        cells = np.ascontiguousarray(displacement_map.cells, dtype=np.int32)
+        if cells.ndim != 2 or cells.shape[1] != 8:
+            raise ValueError("VolumetricFemEnergy: HexQ1Basis needs 8 vertices per cell")
+        fp = _sample_fields(Fp, cells.shape[0], 9, "Fp")
+        if fp is not None and not np.all(np.asarray(fp).reshape(-1, 9) == np.eye(3).ravel()):
+            raise ValueError("VolumetricFemEnergy: hex meshes take no plastic field here")
+        X = np.ascontiguousarray(np.asarray(rest_position_fields, dtype=np.float64).reshape(-1, 3))
+        if X.shape[0] != displacement_map.num_vertices:
+            raise ValueError("VolumetricFemEnergy: rest positions must be (V, 3)")
+        th = _sample_fields(theta, cells.shape[0], 2, "theta")
+        if th is None:
+            raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
+        self.batch_size = int(batch_size)
+        self._h = None
+        th = np.ascontiguousarray(th, dtype=np.float64)
+        h = ctypes.c_void_p()
+        self.device = _device_index()
+        N.check(N.lib.lpg_fem_create_hex(X.shape[0], N.dptr(X), cells.shape[0], N.iptr(cells), N.dptr(th),
+                                         1 if th.ndim == 2 else 0, int(self.points_per_axis), self.device,
+                                         ctypes.byref(h)))
+        self._h = h
+        self._theta = th
+        V_, T_, n_ = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nnzb, nnz = ctypes.c_int64(), ctypes.c_int64()
+        N.check(N.lib.lpg_fem_sizes(h, ctypes.byref(V_), ctypes.byref(T_), ctypes.byref(n_), ctypes.byref(nnzb),
+                                    ctypes.byref(nnz)))
+        self.num_vertices, self.num_elements, self.num_dofs = V_.value, T_.value, n_.value
+        self.nnzb, self.nnz = nnzb.value, nnz.value
+        self._csc = None
+        self._bsr = None
+        self.map = displacement_map
+
+    @classmethod
+    def from_arrays(cls, X, cells, theta, Fp=None, batch_size=256):
+        from .mesh import HexTopology
+
+        X = np.asarray(X, dtype=np.float64).reshape(-1, 3)
+        topo = HexTopology(X.shape[0], cells)
+        return cls(VertexDofMap(topo, 3), X, Fp, theta, batch_size)
+
+
+class VolumetricFemEnergyHexQ1GL4(VolumetricFemEnergyHexQ1):
+    points_per_axis = 4
+
+
 class PyVolumetricMaterial:
     """Base class for volumetric materials written in Python (the reference's
     PyVolumetricMaterial, src/python/fem.py:59-109): subclass it and put the subclass in the
@@ -808,8 +932,11 @@ def _py_energy_class(material):
                 {"material": material})
 
 
+GaussLegendre3D = Template("GaussLegendre3D", {(2,): GaussLegendre3D_2, (4,): GaussLegendre3D_4})
 VolumetricFemEnergy = Template("VolumetricFemEnergy",
-                               {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyTetP1})
+                               {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyTetP1,
+                                (NeoHookean, HexQ1Basis, GaussLegendre3D_2): VolumetricFemEnergyHexQ1,
+                                (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemEnergyHexQ1GL4})
 VolumetricFemEnergy.material_factory = _py_energy_class
 VolumetricFemForceMaterialResponse = Template(
     "VolumetricFemForceMaterialResponse",

@@ -15,7 +15,7 @@ every face diagonal. The reference ships a six-tet generator
 import numpy as np
 
 __all__ = ["TetTopology", "HexTopology", "TetMesh", "HexMesh", "read_veg", "write_veg", "make_box", "box_counts",
-           "delaunay_ball"]
+           "delaunay_ball", "make_hex_box"]
 
 
 class TetTopology:
@@ -215,6 +215,23 @@ def make_box(nx, ny=None, nz=None, size=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0))
     flip = det < 0
     tets[flip, 2], tets[flip, 3] = tets[flip, 3].copy(), tets[flip, 2].copy()
     return X, tets.astype(np.int32)
+
+
+def make_hex_box(nx, ny=None, nz=None, size=(1.0, 1.0, 1.0)):
+    """Structured box of nx*ny*nz hexes on [0, size] (HexQ1Basis corner order, cells i fastest).
+    Returns (X, cells): X (V, 3) with vertex index i + (nx+1) (j + (ny+1) k), cells (T, 8) int32."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    if min(nx, ny, nz) < 1:
+        raise ValueError("make_hex_box requires at least one hex per axis")
+    xs, ys, zs = (size[d] * np.arange(m + 1) / m for d, m in enumerate((nx, ny, nz)))
+    Z, Y, Xg = np.meshgrid(zs, ys, xs, indexing="ij")
+    X = np.stack([Xg.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    corners = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    cells = np.stack([(i + dx) + (nx + 1) * ((j + dy) + (ny + 1) * (k + dz)) for dx, dy, dz in corners], axis=1)
+    return X, cells.astype(np.int32)
 
 
 def concatenate(meshes):

@@ -7,7 +7,12 @@ may import it. The product package (litepgo_b200) never does.
 """
 
 from .oracle import (  # noqa: F401
+    HEX_CORNERS,
     OracleError,
+    hex_box,
+    hex_dN_dxi,
+    hex_eval,
+    hex_points,
     OracleMesh,
     build,
     lib,

@@ -283,3 +283,101 @@ class OracleMesh:
                                        _dp(np.ascontiguousarray(dLdu, float)), _ip(fixed), len(fixed),
                                        int(linear_solver), float(cg_tolerance), _dp(out), _dp(lam)))
         return out, lam
+
+
+# ---------------------------------------------------------------------------
+# Hex Q1 elements (test infrastructure, NumPy): the reference's trilinear HexQ1Basis
+# (src/core/fem/basis/3d/hex_q1_basis.hpp: corners (0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1),
+# (1,0,1), (1,1,1), (0,1,1) of [0,1]^3) with Gauss-Legendre points on [0,1]^3, last axis fastest
+# (src/core/fem/quadrature/3d/gauss_legendre_3d.hpp; 1D rules of
+# quadrature/1d/gauss_legendre_1d.hpp), the point weight w_q det J_q
+# (fem/integration/volumetric_element.hpp:23-39, det J <= 0 rejected), F = I + sum_a u_a grad N_a^T
+# (deformation_gradient_sampling_response.hpp:15-45) and the element sums w B^T vec P,
+# w B^T A B (fem/assembly/dof_derivatives.cpp:22-51) with this oracle's NeoHookean W, P, A.
+# ---------------------------------------------------------------------------
+HEX_CORNERS = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+
+
+def gauss_legendre_01(n):
+    """Points and weights of the n-point Gauss-Legendre rule on [0, 1] (n = 2 or 4)."""
+    if n == 2:
+        return np.array([0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0)]), np.array([0.5, 0.5])
+    if n == 4:
+        outer = np.sqrt((3 + 2 * np.sqrt(6.0 / 5)) / 7)
+        inner = np.sqrt((3 - 2 * np.sqrt(6.0 / 5)) / 7)
+        wo, wi = (18 - np.sqrt(30.0)) / 72, (18 + np.sqrt(30.0)) / 72
+        return (np.array([0.5 * (1 - outer), 0.5 * (1 - inner), 0.5 * (1 + inner), 0.5 * (1 + outer)]),
+                np.array([wo, wi, wi, wo]))
+    raise ValueError("Gauss-Legendre rule with 2 or 4 points per axis")
+
+
+def hex_points(n):
+    t, w = gauss_legendre_01(n)
+    pts, wts = [], []
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                pts.append([t[i], t[j], t[k]])
+                wts.append(w[i] * w[j] * w[k])
+    return np.array(pts), np.array(wts)
+
+
+def hex_dN_dxi(xi):
+    """(8, 3) derivatives of the trilinear basis at xi in [0,1]^3."""
+    out = np.empty((8, 3))
+    for a, (i, j, k) in enumerate(HEX_CORNERS):
+        f = [(1 - xi[d], xi[d]) for d in range(3)]
+        df = [(-1.0, 1.0)] * 3
+        out[a] = [df[0][i] * f[1][j] * f[2][k], f[0][i] * df[1][j] * f[2][k], f[0][i] * f[1][j] * df[2][k]]
+    return out
+
+
+def hex_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
+    """E, gradient and dense Hessian (or None) of the hex Q1 neo-Hookean energy (Fp = I)."""
+    X = np.asarray(X, float).reshape(-1, 3)
+    cells = np.asarray(cells).reshape(-1, 8)
+    U = np.asarray(u, float).reshape(-1, 3)
+    T, n = cells.shape[0], X.size
+    th = np.broadcast_to(np.asarray(theta, float), (T, 2))
+    pts, wts = hex_points(points_per_axis)
+    E, g = 0.0, np.zeros(n)
+    H = np.zeros((n, n)) if hessian else None
+    for e, cell in enumerate(cells):
+        dofs = (3 * cell[:, None] + np.arange(3)).ravel()
+        ge, He = np.zeros(24), np.zeros((24, 24))
+        for xi, wq in zip(pts, wts):
+            dN = hex_dN_dxi(xi)
+            J = X[cell].T @ dN  # J[i, d] = dX_i / dxi_d
+            det = np.linalg.det(J)
+            if not det > 0:
+                raise ValueError("VolumetricElement3D: invalid reference determinant or volume weight")
+            gN = dN @ np.linalg.inv(J)  # rows grad_X N_a
+            F = np.eye(3) + U[cell].T @ gN
+            w = wq * det
+            E += w * nh_W(F, np.eye(3), th[e])
+            P = nh_dW_dF(F, np.eye(3), th[e])
+            B = np.zeros((9, 24))  # column-major vec(F): r = i + 3 j
+            for a in range(8):
+                for i in range(3):
+                    for j in range(3):
+                        B[i + 3 * j, 3 * a + i] = gN[a, j]
+            ge += w * B.T @ P.T.ravel()
+            if hessian:
+                He += w * B.T @ nh_d2W_dF2(F, np.eye(3), th[e]) @ B
+        g[dofs] += ge
+        if hessian:
+            H[np.ix_(dofs, dofs)] += He
+    return E, g, H
+
+
+def hex_box(nx, ny=None, nz=None):
+    """Structured box of nx*ny*nz unit-spacing-scaled hexes on [0,1]^3 (corner order above)."""
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    xs, ys, zs = (np.arange(m + 1) / m for m in (nx, ny, nz))
+    Z, Y, Xg = np.meshgrid(zs, ys, xs, indexing="ij")
+    P = np.stack([Xg.ravel(), Y.ravel(), Z.ravel()], 1)
+    idx = lambda i, j, k: i + (nx + 1) * (j + (ny + 1) * k)  # noqa: E731
+    cells = [[idx(i + c[0], j + c[1], k + c[2]) for c in HEX_CORNERS]
+             for k in range(nz) for j in range(ny) for i in range(nx)]
+    return P, np.array(cells, np.int32)

@@ -1,0 +1,114 @@
+"""Hex Q1 meshes on the GPU path (VolumetricFemEnergy[NeoHookean, HexQ1Basis, GaussLegendre3D[n]]):
+energy, gradient and Exact Hessian against the hex oracle (the reference's two-hex fixture and a
+hex box), the solvers' layout through Newton, the feasible step, and the construction checks."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle
+from conftest import rel_err
+from litepgo_b200 import dof, energy, fem, mesh, solver
+from test_oracle_hex import HEX_CELLS, HEX_THETA, HEX_X, hex_states
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+Exact, Projected = energy.HessianKind.Exact, energy.HessianKind.Projected
+
+
+def hex_energy(X, cells, theta, n=2):
+    cls = fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexQ1Basis, fem.GaussLegendre3D[n]]
+    return cls.from_arrays(X, cells, theta)
+
+
+@pytest.mark.parametrize("state", [0, 1, 2])
+def test_two_hex_fixture_matches_the_oracle(state):
+    x = hex_states()[state]
+    gpu = hex_energy(HEX_X, HEX_CELLS, HEX_THETA)
+    E, g, H = gpu.eval(x, gradient=True, hessian=Exact)
+    Er, gr, Hr = oracle.hex_eval(HEX_X, HEX_CELLS, HEX_THETA, x)
+    assert abs(E - Er) <= 1e-12 * max(abs(Er), 1e-300) + 1e-15
+    assert rel_err(g, gr) <= 1e-12 or np.abs(gr).max() == 0
+    assert rel_err(H.toarray(), Hr) <= 1e-12
+    D = (H - H.T).tocsc()
+    D.eliminate_zeros()
+    assert D.nnz == 0  # bitwise symmetric
+
+
+@pytest.mark.parametrize("n", [2, 4])
+def test_hex_box_matches_the_oracle(n):
+    X, cells = oracle.hex_box(3, 3, 2)
+    rng = np.random.default_rng(n)
+    T = cells.shape[0]
+    mu = np.exp(rng.uniform(np.log(1e3), np.log(1e5), T))
+    nu = rng.uniform(0.30, 0.45, T)
+    theta = np.stack([2 * mu * nu / (1 - 2 * nu), mu], 1)
+    A = np.eye(3) + 0.1 * rng.standard_normal((3, 3))
+    u = (X @ A.T - X + 1e-3 * rng.standard_normal(X.shape)).ravel()
+    gpu = hex_energy(X, cells, theta, n)
+    E, g, H = gpu.eval(u, gradient=True, hessian=Exact)
+    Er, gr, Hr = oracle.hex_eval(X, cells, theta, u, points_per_axis=n)
+    assert abs(E - Er) <= 1e-12 * abs(Er)
+    assert rel_err(g, gr) <= 1e-12
+    assert rel_err(H.toarray(), Hr) <= 1e-12
+    _, _, H32 = gpu.eval(u, hessian=Exact, precision="mixed")
+    assert rel_err(H32.toarray(), Hr) <= 1e-6
+    # The element energies sum to the energy; the feasible step is the minimum over every point.
+    assert abs(gpu.element_energies(u).sum() - E) <= 1e-12 * abs(E)
+    du = rng.standard_normal(u.size)
+    pts, _ = oracle.hex_points(n)
+    ref = 1.0
+    U, dU = u.reshape(-1, 3), du.reshape(-1, 3)
+    for cell in cells:
+        for xi in pts:
+            dN = oracle.hex_dN_dxi(xi)
+            gN = dN @ np.linalg.inv(X[cell].T @ dN)
+            F = np.eye(3) + U[cell].T @ gN
+            dF = dU[cell].T @ gN
+            ref = min(ref, oracle.positive_det_step(F, dF))
+    assert abs(gpu.max_feasible_step(u, du) - ref) <= 1e-12
+
+
+def test_projected_hessian_and_construction_errors():
+    gpu = hex_energy(HEX_X, HEX_CELLS, HEX_THETA)
+    with pytest.raises(ValueError, match="tet meshes only"):
+        gpu.eval(hex_states()[1], hessian=Projected)
+    for scale in (0.0, -1.0, 1e200):
+        with pytest.raises(ValueError):
+            hex_energy(scale * HEX_X, HEX_CELLS, HEX_THETA)
+    bad = HEX_X.copy()
+    bad[0, 0] = np.nan
+    with pytest.raises(ValueError):
+        hex_energy(bad, HEX_CELLS, HEX_THETA)
+    with pytest.raises(TypeError):
+        fem.GaussLegendre3D[3]
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_hex_newton_under_gravity(precision):
+    """A 4x4x4 hex box with its bottom face held under gravity (rho 1000): Newton with the Exact
+    Hessian reaches the relative tolerance and the oracle's free gradient vanishes there."""
+    X, cells = oracle.hex_box(4)
+    n = X.size
+    theta = np.array([1.4e5, 3.4e4])
+    gpu = hex_energy(X, cells, theta)
+    # Consistent load: f_a = -rho g sum_q w_q det J_q N_a(xi_q) (z component).
+    pts, wts = oracle.hex_points(2)
+    f = np.zeros(n)
+    for cell in cells:
+        for xi, wq in zip(pts, wts):
+            dN = oracle.hex_dN_dxi(xi)
+            det = np.linalg.det(X[cell].T @ dN)
+            Nq = fem.HexQ1Basis.eval_N(xi)
+            f[3 * cell + 2] += -9.8 * 1000 * wq * det * Nq
+    fixed = np.flatnonzero(np.repeat(X[:, 2] == 0, 3))
+    total = energy.WeightedSumEnergy([(gpu, 1.0), (energy.QuadraticEnergy(sp.csc_matrix((n, n)), -f), 1.0)])
+    opts = solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", accept_rule="armijo",
+                                precision=precision, max_iterations=50, cg_tolerance=1e-3, hessian=Exact)
+    r = solver.newton_solve(total, dof.DofReduction(n, fixed), np.zeros(n), opts)
+    assert r.status.name == "Converged"
+    x = np.asarray(r.x)
+    _, g, _ = oracle.hex_eval(X, cells, theta, x, hessian=False)
+    free = np.setdiff1d(np.arange(n), fixed)
+    assert np.abs((g - f)[free]).max() <= 1e-7 * np.abs(f).max()

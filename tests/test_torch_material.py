@@ -67,3 +67,15 @@ def test_requested_outputs_only_and_shape_checks():
     assert issubclass(cls, fem.VolumetricFemEnergyPyMaterialTetP1) and cls.material is TorchNeoHookean
     with pytest.raises(TypeError):
         fem.VolumetricFemEnergy[int, fem.TetP1Basis, fem.TetCentroidQuadrature]
+
+
+def test_quadrature_and_basis_templates():
+    """The hex templates as the reference's tests/python/test_fem.py:21-30 names them."""
+    cls = fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexQ1Basis, fem.GaussLegendre3D[2]]
+    assert cls.points_per_axis == 2
+    assert fem.GaussLegendre3D[4].num_points == 64
+    assert abs(fem.GaussLegendre3D[2].weights().sum() - 1.0) < 1e-15
+    with pytest.raises(TypeError, match=r"available: .*GaussLegendre3D\[2\]"):
+        fem.GaussLegendre3D[3]
+    with pytest.raises(TypeError):
+        fem.VolumetricFemEnergy[fem.NeoHookean, fem.TetP1Basis, fem.GaussLegendre3D[2]]
