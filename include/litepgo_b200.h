@@ -105,6 +105,10 @@ int lpg_mesh_pattern_bsr(int num_vertices, int num_tets, const int32_t* tets, in
  * diagonal referencing the stored block of its transpose.
  */
 int lpg_mesh_cluster_summary(int num_vertices, int num_tets, const int32_t* tets, int64_t out[5]);
+/* The same for cells of cell_width vertices: 4 (tets, as above) or 8 (hexes; out[4] counts
+ * 64 contributor entries per hex). */
+int lpg_mesh_cluster_summary_cells(int num_vertices, int num_cells, const int32_t* cells, int cell_width,
+                                   int64_t out[5]);
 
 /*
  * Creates the element data and assembly plan of one tet mesh on `device`.

@@ -241,10 +241,14 @@ int lpg_mesh_pattern_bsr(int V, int T, const int32_t* tets, int64_t* nnzb, int32
 }
 
 int lpg_mesh_cluster_summary(int V, int T, const int32_t* tets, int64_t out[5]) {
+    return lpg_mesh_cluster_summary_cells(V, T, tets, 4, out);
+}
+
+int lpg_mesh_cluster_summary_cells(int V, int T, const int32_t* tets, int cell_width, int64_t out[5]) {
     return guarded([&] {
-        if (T > 0 && !tets) fail(LPG_EINVAL, "lpg_mesh_cluster_summary: null tets");
+        if (T > 0 && !tets) fail(LPG_EINVAL, "lpg_mesh_cluster_summary: null cells");
         HostPlan p;
-        build_plan(V, T, tets, p);
+        build_plan(V, T, tets, p, cell_width);
         check_clusters(p, tets);
         check_solver_layout(p);
         const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;

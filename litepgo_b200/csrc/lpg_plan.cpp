@@ -309,7 +309,7 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
     const int K = p.K, sh = K == 4 ? 2 : 3;
     auto vert = [&](int e, int a) { return tets[K * static_cast<size_t>(e) + a]; };
     // Incidence (vertex -> elements, ascending), independent of the plan's own.
-    std::vector<int32_t> ptr(static_cast<size_t>(V) + 1, 0), inc(4 * static_cast<size_t>(T));
+    std::vector<int32_t> ptr(static_cast<size_t>(V) + 1, 0), inc(K * static_cast<size_t>(T));
     for (size_t k = 0; k < K * static_cast<size_t>(T); ++k) ++ptr[tets[k] + 1];
     for (int v = 0; v < V; ++v) ptr[v + 1] += ptr[v];
     {
@@ -387,7 +387,7 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
         if (energy_count[e] != 1) bad("element energy not counted exactly once");
     size_t contributors = 0;
     for (uint32_t de : p.cl_slot_ent) contributors += de >> 20;
-    if (contributors != 16 * static_cast<size_t>(T)) bad("contributor total differs from 16 per element");
+    if (contributors != static_cast<size_t>(K) * K * T) bad("contributor total differs from K^2 per element");
     for (int c = 0; c < ncl; ++c)
         if (p.cl_ent_ptr[c] % 8 != 0) bad("contributor lists not 16-byte aligned");
 }

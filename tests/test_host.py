@@ -221,3 +221,34 @@ def test_workloads_are_seeded_and_valid():
     c = workloads.compressed_box(6, seed=0)
     d = workloads.det_F(c["X"], c["tets"], c["u"])
     assert d.min() >= 0.2 and d.max() <= 3.0
+
+
+def cell_summary(X, cells, width):
+    out = np.zeros(5, np.int64)
+    cells = np.ascontiguousarray(cells, dtype=np.int32)
+    N.check(N.lib.lpg_mesh_cluster_summary_cells(X.shape[0], cells.shape[0], N.iptr(cells), width,
+                                                 out.ctypes.data_as(N._i64p)))
+    return out
+
+
+@pytest.mark.parametrize("case", ["hex4", "hex_ragged", "hex_shuffled"])
+def test_hex_cluster_plan_invariants(case):
+    """The assembly plan of 8-vertex cells: every invariant of the tet plan (ownership, energy once,
+    exact ordered contributor lists) and of the solvers' layout, checked by the library itself."""
+    rng = np.random.default_rng(9)
+    X, cells = mesh.make_hex_box(4, 3, 5)
+    if case == "hex_ragged":
+        cells = cells[rng.random(cells.shape[0]) < 0.6]
+    elif case == "hex_shuffled":
+        perm = rng.permutation(X.shape[0])
+        cells = perm[cells].astype(np.int32)
+    ncl, max_rows, max_els, evals, entries = cell_summary(X, cells, 8)
+    assert entries == 64 * cells.shape[0]
+    assert 1 <= max_rows <= 24 and max_els <= 224
+    assert cells.shape[0] <= evals <= 8 * cells.shape[0]
+    with pytest.raises(ValueError):
+        cell_summary(X, cells, 6)
+    bad = cells.copy()
+    bad[0, 3] = bad[0, 0]
+    with pytest.raises(ValueError, match="distinct"):
+        cell_summary(X, bad, 8)
