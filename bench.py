@@ -689,9 +689,15 @@ def run_rows():
     ma, me = ctypes.c_double(), ctypes.c_double()
     N.check(N.lib.lpg_fem_time_eval(eh.handle, N.vptr(uh), N.vptr(gh), int(energy.HessianKind.Exact), N.PRECISION_F64,
                                     N.LAYOUT_BSR, N.vptr(Hh), 10, 1, ctypes.byref(ma), ctypes.byref(me)))
+    pa, pe = ctypes.c_double(), ctypes.c_double()
+    N.check(N.lib.lpg_fem_time_eval(eh.handle, N.vptr(uh), N.vptr(gh), int(energy.HessianKind.Projected),
+                                    N.PRECISION_F64, N.LAYOUT_BSR, N.vptr(Hh), 10, 1, ctypes.byref(pa), ctypes.byref(pe)))
     hex_row = {"mesh": f"hex box 48^3 ({ch.shape[0]} hexes, {Xh.shape[0]} vertices, nnzb {eh.nnzb}), 8 points",
                "element_pass_and_gather_ms": ma.value, "eval_ms": me.value, "hexes_per_s": ch.shape[0] / (me.value * 1e-3),
-               "timing": "lpg_fem_time_eval: CUDA events, L2 flushed between launches, FP64 E + gradient + Exact BSR"}
+               "projected": {"element_pass_projection_and_gather_ms": pa.value, "eval_ms": pe.value,
+                             "hexes_per_s": ch.shape[0] / (pe.value * 1e-3)},
+               "timing": "lpg_fem_time_eval: CUDA events, L2 flushed between launches, FP64 E + gradient + BSR "
+                         "(Exact, and Projected: per-element 24x24 eigen-projection)"}
     line = {"rows": "plastic-field force VJP, adjoint in Fp, VEG I/O, hex Q1", "config": workload_config(),
             "hex_q1": hex_row,
             "fp_vjp": fp_row, "newton_with_fp": {"status": r.status.name, "iterations": r.iterations, "seconds": r.seconds},

@@ -195,13 +195,13 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
     a.cl_variant = tune.cl[pi];
     if (dm.K == 8) {
-        if (a.hess && hessian == LPG_HESSIAN_PROJECTED)
-            fail(LPG_EINVAL, "the projected Hessian is available for tet meshes only");
+        const bool projected = hessian == LPG_HESSIAN_PROJECTED;
         const size_t T = static_cast<size_t>(dm.T);
         double* elemE = delem ? delem : d_mat[3].as<double>(std::max<size_t>(T, 1));
-        void* blocks = a.hess ? d_proj.ensure(T * kHexRecord * (precision == LPG_PRECISION_F64 ? 8 : 4)) : nullptr;
+        void* blocks = a.hess ? d_proj.ensure(hex_blocks_bytes(dm, precision, projected)) : nullptr;
         a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(dm.ncl) + 256);
-        launch_hex_eval(dm, precision, du, elemE, d_vjp.as<double>(std::max<size_t>(24 * T, 1)), blocks, a, stream);
+        launch_hex_eval(dm, precision, projected, du, elemE, d_vjp.as<double>(std::max<size_t>(24 * T, 1)), blocks, a,
+                        stream);
         return;
     }
     if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {

@@ -26,6 +26,7 @@
 #include <cuda_pipeline.h>
 
 #include "lpg_internal.h"
+#include "lpg_psd.h"
 
 namespace lpg {
 namespace {
@@ -1838,6 +1839,65 @@ __global__ void __launch_bounds__(128) hex_element_kernel(const DevMesh m, const
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
+// Projected Hessian of hex meshes (HessianKind::Projected, mesh_energy.cpp:16-27): one warp per
+// element loads its record of 36 FP64 blocks (hex_element_kernel) as the 24x24 element Hessian
+// into shared memory, runs the parallel-ordered Jacobi iteration (lpg_psd.h) and writes
+// V max(L, 0) V^T back as 36 blocks in the precision's type: in place for FP64 (a warp reads its
+// whole record before it writes), into a separate FP32 record array for mixed precision. Each
+// entry is formed once from the upper triangle, so the diagonal blocks stay bitwise symmetric.
+struct WarpTeam {
+    int l;
+    __device__ int lane() const { return l; }
+    __device__ int size() const { return 32; }
+    __device__ void sync() const { __syncwarp(); }
+    __device__ double sum(double x) const {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        return __shfl_sync(0xffffffffu, x, 0);
+    }
+};
+
+constexpr int kHexPsdWarps = 4;
+
+template <typename R>
+__global__ void __launch_bounds__(32 * kHexPsdWarps) hex_psd_kernel(int T, const double* in, R* out, unsigned* status) {
+    using J = PsdJacobi<24>;
+    __shared__ double sA[kHexPsdWarps][24 * J::S], sV[kHexPsdWarps][24 * J::S];
+    __shared__ double sCS[kHexPsdWarps][24], sL[kHexPsdWarps][24];
+    __shared__ int sPQ[kHexPsdWarps][24];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int e = blockIdx.x * kHexPsdWarps + w; // uniform over the warp: a warp leaves whole
+    if (e >= T) return;
+    double* A = sA[w];
+    const double* rec = in + kHexRecord * static_cast<size_t>(e);
+    for (int t = lane; t < kHexRecord; t += 32) {
+        int a, b;
+        hex_pair(t / 9, a, b);
+        const int i = 3 * a + (t % 9) / 3, k = 3 * b + t % 3;
+        const double v = rec[t];
+        A[i * J::S + k] = v;
+        if (a != b) A[k * J::S + i] = v;
+    }
+    J::eigen(WarpTeam{lane}, A, sV[w], sCS[w], sPQ[w], sL[w]);
+    R* o = out + kHexRecord * static_cast<size_t>(e);
+    unsigned st = 0;
+    for (int t = lane; t < kHexRecord; t += 32) {
+        int a, b;
+        hex_pair(t / 9, a, b);
+        int i = 3 * a + (t % 9) / 3, k = 3 * b + t % 3;
+        if (i > k) {
+            const int x = i;
+            i = k;
+            k = x;
+        }
+        const double v = J::entry(sV[w], sL[w], i, k);
+        if (!isfinite(v)) st |= ST_NONFINITE_OUT;
+        o[t] = static_cast<R>(v);
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if (lane == 0 && st) atomicOr(status, st);
+}
+
 // Feasible step of a hex mesh: at every quadrature point F and dF (the increment's gradient),
 // the reference's positive-determinant step, minimum per block.
 __global__ void __launch_bounds__(256) hex_feasible_kernel(const DevMesh m, const double* __restrict__ u,
@@ -2145,18 +2205,38 @@ void launch_material_eval(const DevMesh& m, int precision, int hessian, const do
     LPG_CUDA(cudaGetLastError());
 }
 
-void launch_hex_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem, void* blocks,
-                     const EvalArgs& a, cudaStream_t s) {
+size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected) {
+    const size_t records = kHexRecord * static_cast<size_t>(m.T);
+    if (precision == LPG_PRECISION_F64) return records * sizeof(double);
+    return records * (projected ? sizeof(double) + sizeof(float) : sizeof(float));
+}
+
+void launch_hex_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
+                     double* per_elem, void* blocks, const EvalArgs& a, cudaStream_t s) {
     if (m.T > 0) {
         const size_t threads = 36 * static_cast<size_t>(m.T);
         const int grid = static_cast<int>((threads + 127) / 128);
         if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-        if (precision == LPG_PRECISION_F64)
-            hex_element_kernel<double><<<grid, 128, 0, s>>>(m, u, elemE, a.grad ? per_elem : nullptr,
+        double* per_grad = a.grad ? per_elem : nullptr;
+        if (a.hess && projected) {
+            // FP64 element Hessians, projected into the precision's records.
+            double* records = static_cast<double*>(blocks);
+            hex_element_kernel<double><<<grid, 128, 0, s>>>(m, u, elemE, per_grad, records, a.status);
+            const int pgrid = (m.T + kHexPsdWarps - 1) / kHexPsdWarps;
+            if (precision == LPG_PRECISION_F64) {
+                hex_psd_kernel<double><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, records, a.status);
+            } else {
+                float* out = reinterpret_cast<float*>(records + kHexRecord * static_cast<size_t>(m.T));
+                hex_psd_kernel<float><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, out, a.status);
+                blocks = out;
+            }
+        } else if (precision == LPG_PRECISION_F64) {
+            hex_element_kernel<double><<<grid, 128, 0, s>>>(m, u, elemE, per_grad,
                                                            a.hess ? static_cast<double*>(blocks) : nullptr, a.status);
-        else
-            hex_element_kernel<float><<<grid, 128, 0, s>>>(m, u, elemE, a.grad ? per_elem : nullptr,
+        } else {
+            hex_element_kernel<float><<<grid, 128, 0, s>>>(m, u, elemE, per_grad,
                                                           a.hess ? static_cast<float*>(blocks) : nullptr, a.status);
+        }
         if (a.grad) vertex_gather_kernel<8><<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
         if (a.hess) {
             EvalArgs ga = a;

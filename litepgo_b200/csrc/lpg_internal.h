@@ -207,9 +207,13 @@ void launch_set_theta(const DevMesh& m, const double* theta, int per_element, cu
 void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblocks, double* out2, cudaStream_t s);
 // Hex Q1 element pass (K = 8): energy per element into elemE (T), gradient pieces (24 per element)
 // into per_elem when a.grad is set, the 36 blocks per element (precision's type) into blocks when
-// a.hess is set (Exact only), then the gradient gather, the energy sum and the block gather.
-void launch_hex_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem, void* blocks,
-                     const EvalArgs& a, cudaStream_t s);
+// a.hess is set, then the gradient gather, the energy sum and the block gather. With projected,
+// every element's 24x24 Hessian is first projected to PSD; blocks then holds hex_blocks_bytes().
+void launch_hex_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
+                     double* per_elem, void* blocks, const EvalArgs& a, cudaStream_t s);
+// Bytes of the block records launch_hex_eval needs: FP64 records, plus FP32 ones for a
+// projected mixed-precision Hessian (the projection runs in FP64).
+size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected);
 // Largest step along du keeping det F > 0 at every quadrature point of every hex (x 0.9 as the
 // reference), minimum over the mesh into *alpha (device).
 void launch_hex_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,

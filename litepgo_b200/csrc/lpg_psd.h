@@ -1,0 +1,160 @@
+// Positive semi-definite projection of a dense symmetric N x N matrix, V max(L, 0) V^T, by the
+// cyclic Jacobi eigenvalue method in the round-robin parallel ordering (Brent and Luk, "The
+// solution of singular-value and symmetric eigenvalue problems on multiprocessor arrays", 1985):
+// a sweep is N - 1 rounds of N / 2 disjoint plane rotations, each round computed from one state
+// of the matrix, so the rotations of a round, their row updates and their column updates are
+// independent tasks. This is the projection HessianKind::Projected applies to every element's
+// local Hessian (mesh_energy.cpp:16-27, there by Eigen's SelfAdjointEigenSolver).
+//
+// The functions are the tasks of one round; a caller runs rotation() for k < N/2, then rows()
+// and cols() for t < N/2 * N, with a barrier between the three phases (one warp per matrix on
+// the GPU; plain loops on the host, where a test checks this code against an eigensolver).
+#pragma once
+#include <math.h>
+
+#ifdef __CUDACC__
+#define LPG_HD __host__ __device__ __forceinline__
+#else
+#define LPG_HD inline
+#endif
+
+namespace lpg {
+
+template <int N>
+struct PsdJacobi {
+    static_assert(N % 2 == 0 && N >= 2, "the round-robin ordering pairs an even number of indices");
+    static constexpr int S = N + 1;       // row stride (a padded row staggers column reads across banks)
+    static constexpr int kPairs = N / 2;  // rotations per round
+    static constexpr int kRounds = N - 1; // rounds per sweep: every index pair once
+    static constexpr int kTasks = kPairs * N;
+    static constexpr int kMaxSweeps = 30;
+    // A sweep ends the iteration once the off-diagonal Frobenius norm is below 1e-14 of the
+    // matrix's (the projection moves by at most that much: it is non-expansive).
+    static constexpr double kOffTol2 = 1e-28;
+
+    // Pair k of round r by the circle method: index N - 1 stays, the others rotate.
+    LPG_HD static void pair(int r, int k, int& p, int& q) {
+        int x, y;
+        if (k == 0) {
+            x = N - 1;
+            y = r;
+        } else {
+            x = (r + k) % (N - 1);
+            y = (r - k + (N - 1)) % (N - 1);
+        }
+        p = x < y ? x : y;
+        q = x < y ? y : x;
+    }
+
+    // The rotation zeroing A(p, q): A' = J^T A J with J_pp = J_qq = c, J_pq = s, J_qp = -s,
+    // t = tan phi the smaller root of t^2 + 2 t theta - 1 = 0, theta = (A_qq - A_pp) / (2 A_pq).
+    LPG_HD static void rotation(const double* A, int r, int k, double* cs, int* pq) {
+        int p, q;
+        pair(r, k, p, q);
+        const double apq = A[p * S + q];
+        double c = 1.0, s = 0.0;
+        if (apq != 0.0) {
+            const double th = (A[q * S + q] - A[p * S + p]) / (2.0 * apq);
+            const double at = fabs(th);
+            const double t = at > 1e150 ? 0.5 / th : copysign(1.0, th) / (at + sqrt(th * th + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            s = t * c;
+        }
+        cs[2 * k] = c;
+        cs[2 * k + 1] = s;
+        pq[2 * k] = p;
+        pq[2 * k + 1] = q;
+    }
+
+    // Rows p and q of J^T A at column j (task t = k N + j).
+    LPG_HD static void rows(double* A, const double* cs, const int* pq, int t) {
+        const int k = t / N, j = t - N * k;
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        double* ap = A + pq[2 * k] * S + j;
+        double* aq = A + pq[2 * k + 1] * S + j;
+        const double x = *ap, y = *aq;
+        *ap = c * x - s * y;
+        *aq = s * x + c * y;
+    }
+
+    // Columns p and q of A J and of V J at row i (task t = k N + i).
+    LPG_HD static void cols(double* A, double* V, const double* cs, const int* pq, int t) {
+        const int k = t / N, i = t - N * k;
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        const int p = pq[2 * k], q = pq[2 * k + 1];
+        double* a = A + i * S;
+        double* v = V + i * S;
+        const double x = a[p], y = a[q];
+        a[p] = c * x - s * y;
+        a[q] = s * x + c * y;
+        const double vx = v[p], vy = v[q];
+        v[p] = c * vx - s * vy;
+        v[q] = s * vx + c * vy;
+    }
+
+    // Entry (i, j), i <= j, of V diag(L) V^T for the clamped eigenvalues L (summed in index order).
+    LPG_HD static double entry(const double* V, const double* L, int i, int j) {
+        double sum = 0.0;
+        for (int m = 0; m < N; ++m) sum = fma(V[i * S + m] * L[m], V[j * S + m], sum);
+        return sum;
+    }
+
+    // The eigen-iteration by a team of lanes (lane(), size(), sync(), and sum(), which returns
+    // the same total to every lane). A holds the symmetric matrix (row stride S) on entry and its
+    // rotated diagonal form on exit; V (N S), cs (N), pq (N) and L (N) are scratch shared by the
+    // team, and on exit V holds the eigenvectors (columns) and L the eigenvalues clamped at zero.
+    // Returns the sweeps run; a non-finite A stops at once (its output is non-finite or zero,
+    // and the caller flags it).
+#ifdef __CUDACC__
+#pragma nv_exec_check_disable
+#endif
+    template <class Team>
+    LPG_HD static int eigen(const Team& team, double* A, double* V, double* cs, int* pq, double* L) {
+        const int lane = team.lane(), nl = team.size();
+        team.sync();
+        double tot = 0.0;
+        for (int t = lane; t < N * N; t += nl) {
+            const int i = t / N, j = t - N * i;
+            V[i * S + j] = i == j ? 1.0 : 0.0;
+            const double a = A[i * S + j];
+            tot = fma(a, a, tot);
+        }
+        tot = team.sum(tot);
+        team.sync();
+        int sweep = 0;
+        for (; sweep < kMaxSweeps; ++sweep) {
+            double off = 0.0;
+            for (int t = lane; t < N * N; t += nl) {
+                const int i = t / N, j = t - N * i;
+                const double a = A[i * S + j];
+                if (i != j) off = fma(a, a, off);
+            }
+            off = team.sum(off);
+            if (!(off > kOffTol2 * tot)) break;
+            for (int r = 0; r < kRounds; ++r) {
+                for (int k = lane; k < kPairs; k += nl) rotation(A, r, k, cs, pq);
+                team.sync();
+                for (int t = lane; t < kTasks; t += nl) rows(A, cs, pq, t);
+                team.sync();
+                for (int t = lane; t < kTasks; t += nl) cols(A, V, cs, pq, t);
+                team.sync();
+            }
+        }
+        for (int m = lane; m < N; m += nl) {
+            const double d = A[m * S + m];
+            L[m] = d > 0.0 ? d : 0.0;
+        }
+        team.sync();
+        return sweep;
+    }
+};
+
+// A team of one: the host form of the loops above.
+struct SerialTeam {
+    LPG_HD int lane() const { return 0; }
+    LPG_HD int size() const { return 1; }
+    LPG_HD void sync() const {}
+    LPG_HD double sum(double x) const { return x; }
+};
+
+} // namespace lpg

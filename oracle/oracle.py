@@ -332,8 +332,9 @@ def hex_dN_dxi(xi):
     return out
 
 
-def hex_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
-    """E, gradient and dense Hessian (or None) of the hex Q1 neo-Hookean energy (Fp = I)."""
+def hex_eval(X, cells, theta, u, points_per_axis=2, hessian=True, projected=False):
+    """E, gradient and dense Hessian (or None) of the hex Q1 neo-Hookean energy (Fp = I); with
+    projected, each element's 24x24 Hessian is projected (project_psd) before assembly."""
     X = np.asarray(X, float).reshape(-1, 3)
     cells = np.asarray(cells).reshape(-1, 8)
     U = np.asarray(u, float).reshape(-1, 3)
@@ -366,7 +367,7 @@ def hex_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
                 He += w * B.T @ nh_d2W_dF2(F, np.eye(3), th[e]) @ B
         g[dofs] += ge
         if hessian:
-            H[np.ix_(dofs, dofs)] += He
+            H[np.ix_(dofs, dofs)] += project_psd(He) if projected else He
     return E, g, H
 
 

@@ -1,0 +1,40 @@
+// Test harness: the GPU's element projection (litepgo_b200/csrc/lpg_psd.h) run on the host by a
+// team of one lane, for tests/test_psd_jacobi.py (built there with g++ into a temporary folder).
+#include <vector>
+
+#include "lpg_psd.h"
+
+namespace {
+
+template <int N>
+int project(const double* in, double* out, double* eig) {
+    using J = lpg::PsdJacobi<N>;
+    std::vector<double> A(N * J::S), V(N * J::S), cs(N), L(N);
+    std::vector<int> pq(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) A[i * J::S + j] = in[i * N + j];
+    const int sweeps = J::eigen(lpg::SerialTeam{}, A.data(), V.data(), cs.data(), pq.data(), L.data());
+    for (int i = 0; i < N; ++i) {
+        eig[i] = A[i * J::S + i];
+        for (int j = i; j < N; ++j) out[i * N + j] = out[j * N + i] = J::entry(V.data(), L.data(), i, j);
+    }
+    return sweeps;
+}
+
+} // namespace
+
+// Projects the row-major n x n matrix in (n = 2, 8 or 24) into out and writes the unclamped
+// eigenvalues (unsorted) to eig; returns the sweeps taken, or -1 for an unsupported n.
+extern "C" int psd_project(int n, const double* in, double* out, double* eig) {
+    switch (n) {
+    case 2: return project<2>(in, out, eig);
+    case 8: return project<8>(in, out, eig);
+    case 24: return project<24>(in, out, eig);
+    default: return -1;
+    }
+}
+
+// Pairs of round r of the n-index round-robin ordering (n = 24), 2 * n / 2 ints.
+extern "C" void psd_round_pairs(int r, int* out) {
+    for (int k = 0; k < 12; ++k) lpg::PsdJacobi<24>::pair(r, k, out[2 * k], out[2 * k + 1]);
+}

@@ -1,6 +1,7 @@
 """Hex Q1 meshes on the GPU path (VolumetricFemEnergy[NeoHookean, HexQ1Basis, GaussLegendre3D[n]]):
 energy, gradient and Exact Hessian against the hex oracle (the reference's two-hex fixture and a
-hex box), the solvers' layout through Newton, the feasible step, and the construction checks."""
+hex box), the Projected Hessian (per-element eigen-projection) against the oracle's, the solvers'
+layout through Newton, the feasible step, and the construction checks."""
 
 import numpy as np
 import pytest
@@ -70,10 +71,50 @@ def test_hex_box_matches_the_oracle(n):
     assert abs(gpu.max_feasible_step(u, du) - ref) <= 1e-12
 
 
-def test_projected_hessian_and_construction_errors():
+@pytest.mark.parametrize("state", [0, 1, 2])
+def test_two_hex_projected_hessian(state):
+    """HessianKind::Projected on the reference's two-hex fixture: elements already PSD keep
+    their Hessian up to the eigen-iteration's rounding."""
+    x = hex_states()[state]
     gpu = hex_energy(HEX_X, HEX_CELLS, HEX_THETA)
-    with pytest.raises(ValueError, match="tet meshes only"):
-        gpu.eval(hex_states()[1], hessian=Projected)
+    E, g, H = gpu.eval(x, gradient=True, hessian=Projected)
+    Er, gr, Hr = oracle.hex_eval(HEX_X, HEX_CELLS, HEX_THETA, x, projected=True)
+    assert abs(E - Er) <= 1e-12 * max(abs(Er), 1e-300) + 1e-15
+    assert rel_err(H.toarray(), Hr) <= 1e-11
+    D = (H - H.T).tocsc()
+    D.eliminate_zeros()
+    assert D.nnz == 0
+
+
+def test_compressed_hex_box_projected_hessian():
+    """A compressed hex box whose every element Hessian is indefinite (checked on the CPU):
+    the projected Hessian matches the oracle's per-element eigen-projection in FP64 and mixed
+    precision, is PSD, bitwise symmetric, and differs from the Exact one."""
+    X, cells = oracle.hex_box(3, 3, 2)
+    rng = np.random.default_rng(11)
+    T = cells.shape[0]
+    mu = np.exp(rng.uniform(np.log(1e3), np.log(1e5), T))
+    nu = rng.uniform(0.30, 0.45, T)
+    theta = np.stack([2 * mu * nu / (1 - 2 * nu), mu], 1)
+    A = np.diag([1.0, 1.0, 0.45]) + 0.05 * rng.standard_normal((3, 3))
+    u = (X @ A.T - X + 5e-3 * rng.standard_normal(X.shape)).ravel()
+    _, _, He = oracle.hex_eval(X, cells, theta, u)
+    _, _, Hr = oracle.hex_eval(X, cells, theta, u, projected=True)
+    assert rel_err(Hr, He) > 0.1
+    gpu = hex_energy(X, cells, theta)
+    _, _, H = gpu.eval(u, hessian=Projected)
+    assert rel_err(H.toarray(), Hr) <= 1e-11
+    D = (H - H.T).tocsc()
+    D.eliminate_zeros()
+    assert D.nnz == 0
+    assert np.linalg.eigvalsh(H.toarray()).min() >= -1e-10 * np.abs(Hr).max()
+    _, _, H32 = gpu.eval(u, hessian=Projected, precision="mixed")
+    assert rel_err(H32.toarray(), Hr) <= 1e-6
+
+
+def test_construction_errors():
+    gpu = hex_energy(HEX_X, HEX_CELLS, HEX_THETA)
+    assert gpu.eval(hex_states()[1])[0] > 0
     for scale in (0.0, -1.0, 1e200):
         with pytest.raises(ValueError):
             hex_energy(scale * HEX_X, HEX_CELLS, HEX_THETA)
@@ -85,10 +126,12 @@ def test_projected_hessian_and_construction_errors():
         fem.GaussLegendre3D[3]
 
 
-@pytest.mark.parametrize("precision", ["f64", "mixed"])
-def test_hex_newton_under_gravity(precision):
+@pytest.mark.parametrize("precision,hessian", [("f64", Exact), ("mixed", Exact), ("f64", Projected),
+                                               ("mixed", Projected)])
+def test_hex_newton_under_gravity(precision, hessian):
     """A 4x4x4 hex box with its bottom face held under gravity (rho 1000): Newton with the Exact
-    Hessian reaches the relative tolerance and the oracle's free gradient vanishes there."""
+    or the (default) Projected Hessian reaches the relative tolerance and the oracle's free
+    gradient vanishes there."""
     X, cells = oracle.hex_box(4)
     n = X.size
     theta = np.array([1.4e5, 3.4e4])
@@ -105,7 +148,7 @@ def test_hex_newton_under_gravity(precision):
     fixed = np.flatnonzero(np.repeat(X[:, 2] == 0, 3))
     total = energy.WeightedSumEnergy([(gpu, 1.0), (energy.QuadraticEnergy(sp.csc_matrix((n, n)), -f), 1.0)])
     opts = solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", accept_rule="armijo",
-                                precision=precision, max_iterations=50, cg_tolerance=1e-3, hessian=Exact)
+                                precision=precision, max_iterations=50, cg_tolerance=1e-3, hessian=hessian)
     r = solver.newton_solve(total, dof.DofReduction(n, fixed), np.zeros(n), opts)
     assert r.status.name == "Converged"
     x = np.asarray(r.x)
