@@ -200,8 +200,9 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
         double* elemE = delem ? delem : d_mat[3].as<double>(std::max<size_t>(T, 1));
         void* blocks = a.hess ? d_proj.ensure(hex_blocks_bytes(dm, precision, projected)) : nullptr;
         a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(dm.ncl) + 256);
-        launch_hex_eval(dm, precision, projected, du, elemE, d_vjp.as<double>(std::max<size_t>(24 * T, 1)), blocks, a,
-                        stream);
+        int* flags = projected && a.hess ? d_plist.as<int>(std::max<size_t>(T, 1)) : nullptr;
+        launch_hex_eval(dm, precision, projected, du, elemE, d_vjp.as<double>(std::max<size_t>(24 * T, 1)), blocks,
+                        flags, a, stream);
         return;
     }
     if (a.hess && hessian == LPG_HESSIAN_PROJECTED) {

@@ -840,31 +840,7 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
                 scale = fmax(scale, fabs(A[sym9(r, r)]));
                 for (int c = 0; c < 9; ++c) V[9 * r + c] = A[sym9(r, c)];
             }
-            const R tol = R(64) * Eps<R>::v * scale;
-            unsigned left = 0x1ffu;
-            for (int k = 0; k < 9 && pd; ++k) {
-                int piv = -1;
-                R best = tol;
-                for (int i = 0; i < 9; ++i)
-                    if (((left >> i) & 1u) && V[9 * i + i] > best) best = V[9 * i + i], piv = i;
-                if (piv < 0) {
-                    for (int i = 0; i < 9 && pd; ++i)
-                        for (int j = 0; j < 9; ++j)
-                            if (((left >> i) & (left >> j) & 1u) && !(fabs(V[9 * i + j]) <= tol)) {
-                                pd = false;
-                                break;
-                            }
-                    break;
-                }
-                left &= ~(1u << piv);
-                const R inv = R(1) / best;
-                for (int i = 0; i < 9; ++i) {
-                    if (!((left >> i) & 1u)) continue;
-                    const R li = V[9 * i + piv] * inv;
-                    for (int j = 0; j < 9; ++j)
-                        if ((left >> j) & 1u) V[9 * i + j] -= li * V[9 * piv + j];
-                }
-            }
+            pd = semidefinite_ldlt<9>(V, R(64) * Eps<R>::v * scale);
             if (!(scale < R(INFINITY))) pd = false;
         }
         // Semi-definite (or kept exact): final. Otherwise the unclamped tangent is stored and
@@ -1839,6 +1815,92 @@ __global__ void __launch_bounds__(128) hex_element_kernel(const DevMesh m, const
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
+// Pre-test of the hex projection: H = sum_q w_q B_q^T A_q B_q (w_q > 0) is semi-definite when
+// every quadrature point's tangent A_q = dP/dF is, and then H is its own projection. One thread
+// per (element, point) forms
+//   A(3 i + j, 3 k + l) = mu d_ik d_jl + lambda G_ij G_kl - p G_il G_kj,  G = F^-T, p = lambda log J - mu
+// (bitwise symmetric: each product is formed from the same two factors both ways) and runs the
+// LDL^T test with the tet pass's round-off allowance; an element with a point that fails is
+// marked in flags (zeroed before) for the eigen-projection. A failed point (det F <= 0 or
+// non-finite) marks its element too; the element pass reports it.
+__global__ void __launch_bounds__(128) hex_tangent_test_kernel(const DevMesh m, const double* __restrict__ u,
+                                                               int* __restrict__ flags) {
+    const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<size_t>(m.T) * m.nq) return;
+    const int e = static_cast<int>(t / m.nq), q = static_cast<int>(t - static_cast<size_t>(m.nq) * e);
+    const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+    const double lam = m.hex_theta[2 * static_cast<size_t>(e)], mu = m.hex_theta[2 * static_cast<size_t>(e) + 1];
+    const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < 8; ++c) {
+        const int v = __ldg(cell + c);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
+            const double uu = __ldg(u + 3 * static_cast<size_t>(v) + i);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double dn = __ldg(dq + 3 * c + d);
+                J[3 * i + d] = fma(X, dn, J[3 * i + d]);
+                G[3 * i + d] = fma(uu, dn, G[3 * i + d]);
+            }
+        }
+    }
+    const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                      J[2] * (J[3] * J[7] - J[4] * J[6]);
+    const double iJ = 1.0 / dJ;
+    double Ji[9];
+    Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
+    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
+    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
+    Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
+    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
+    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
+    Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
+    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
+    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+    double F[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            F[3 * i + j] = (i == j ? 1.0 : 0.0) + G[3 * i] * Ji[j] + G[3 * i + 1] * Ji[3 + j] + G[3 * i + 2] * Ji[6 + j];
+    double C[9];
+    C[0] = F[4] * F[8] - F[5] * F[7];
+    C[1] = F[5] * F[6] - F[3] * F[8];
+    C[2] = F[3] * F[7] - F[4] * F[6];
+    C[3] = F[2] * F[7] - F[1] * F[8];
+    C[4] = F[0] * F[8] - F[2] * F[6];
+    C[5] = F[1] * F[6] - F[0] * F[7];
+    C[6] = F[1] * F[5] - F[2] * F[4];
+    C[7] = F[2] * F[3] - F[0] * F[5];
+    C[8] = F[0] * F[4] - F[1] * F[3];
+    const double detF = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+    if (!(detF > 0) || !isfinite(detF)) {
+        flags[e] = 1;
+        return;
+    }
+    double Gt[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Gt[k] = C[k] / detF;
+    const double p = lam * log(detF) - mu;
+    double A[81];
+    double scale = 0;
+#pragma unroll
+    for (int r = 0; r < 9; ++r)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const int i = r / 3, j = r % 3, k = c / 3, l = c % 3;
+            double v = lam * (Gt[r] * Gt[c]) - p * (Gt[3 * i + l] * Gt[3 * k + j]);
+            if (r == c) {
+                v += mu;
+                scale = fmax(scale, fabs(v));
+            }
+            A[9 * r + c] = v;
+        }
+    if (!(scale < INFINITY) || !semidefinite_ldlt<9>(A, 64 * Eps<double>::v * scale)) flags[e] = 1;
+}
+
 // Projected Hessian of hex meshes (HessianKind::Projected, mesh_energy.cpp:16-27): one warp per
 // element loads its record of 36 FP64 blocks (hex_element_kernel) as the 24x24 element Hessian
 // into shared memory, runs the parallel-ordered Jacobi iteration (lpg_psd.h) and writes
@@ -1860,16 +1922,23 @@ struct WarpTeam {
 constexpr int kHexPsdWarps = 4;
 
 template <typename R>
-__global__ void __launch_bounds__(32 * kHexPsdWarps) hex_psd_kernel(int T, const double* in, R* out, unsigned* status) {
+__global__ void __launch_bounds__(32 * kHexPsdWarps) hex_psd_kernel(int T, const double* in, R* out,
+                                                                   const int* __restrict__ flags, unsigned* status) {
     using J = PsdJacobi<24>;
     __shared__ double sA[kHexPsdWarps][24 * J::S], sV[kHexPsdWarps][24 * J::S];
-    __shared__ double sCS[kHexPsdWarps][24], sL[kHexPsdWarps][24];
+    __shared__ double sCS[kHexPsdWarps][J::kCs], sL[kHexPsdWarps][24];
     __shared__ int sPQ[kHexPsdWarps][24];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int e = blockIdx.x * kHexPsdWarps + w; // uniform over the warp: a warp leaves whole
     if (e >= T) return;
-    double* A = sA[w];
     const double* rec = in + kHexRecord * static_cast<size_t>(e);
+    R* o = out + kHexRecord * static_cast<size_t>(e);
+    if (flags[e] == 0) { // semi-definite (hex_tangent_test_kernel): the Hessian as it is
+        if (static_cast<const void*>(rec) != static_cast<const void*>(o))
+            for (int t = lane; t < kHexRecord; t += 32) o[t] = static_cast<R>(rec[t]);
+        return;
+    }
+    double* A = sA[w];
     for (int t = lane; t < kHexRecord; t += 32) {
         int a, b;
         hex_pair(t / 9, a, b);
@@ -1879,7 +1948,6 @@ __global__ void __launch_bounds__(32 * kHexPsdWarps) hex_psd_kernel(int T, const
         if (a != b) A[k * J::S + i] = v;
     }
     J::eigen(WarpTeam{lane}, A, sV[w], sCS[w], sPQ[w], sL[w]);
-    R* o = out + kHexRecord * static_cast<size_t>(e);
     unsigned st = 0;
     for (int t = lane; t < kHexRecord; t += 32) {
         int a, b;
@@ -2212,7 +2280,7 @@ size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected) {
 }
 
 void launch_hex_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
-                     double* per_elem, void* blocks, const EvalArgs& a, cudaStream_t s) {
+                     double* per_elem, void* blocks, int* flags, const EvalArgs& a, cudaStream_t s) {
     if (m.T > 0) {
         const size_t threads = 36 * static_cast<size_t>(m.T);
         const int grid = static_cast<int>((threads + 127) / 128);
@@ -2222,12 +2290,15 @@ void launch_hex_eval(const DevMesh& m, int precision, bool projected, const doub
             // FP64 element Hessians, projected into the precision's records.
             double* records = static_cast<double*>(blocks);
             hex_element_kernel<double><<<grid, 128, 0, s>>>(m, u, elemE, per_grad, records, a.status);
+            LPG_CUDA(cudaMemsetAsync(flags, 0, static_cast<size_t>(m.T) * sizeof(int), s));
+            const size_t points = static_cast<size_t>(m.T) * m.nq;
+            hex_tangent_test_kernel<<<static_cast<int>((points + 127) / 128), 128, 0, s>>>(m, u, flags);
             const int pgrid = (m.T + kHexPsdWarps - 1) / kHexPsdWarps;
             if (precision == LPG_PRECISION_F64) {
-                hex_psd_kernel<double><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, records, a.status);
+                hex_psd_kernel<double><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, records, flags, a.status);
             } else {
                 float* out = reinterpret_cast<float*>(records + kHexRecord * static_cast<size_t>(m.T));
-                hex_psd_kernel<float><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, out, a.status);
+                hex_psd_kernel<float><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, out, flags, a.status);
                 blocks = out;
             }
         } else if (precision == LPG_PRECISION_F64) {

@@ -208,9 +208,10 @@ void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblock
 // Hex Q1 element pass (K = 8): energy per element into elemE (T), gradient pieces (24 per element)
 // into per_elem when a.grad is set, the 36 blocks per element (precision's type) into blocks when
 // a.hess is set, then the gradient gather, the energy sum and the block gather. With projected,
-// every element's 24x24 Hessian is first projected to PSD; blocks then holds hex_blocks_bytes().
+// every element's 24x24 Hessian is first projected to PSD (flags: T ints of scratch marking the
+// elements that need the eigen-projection); blocks then holds hex_blocks_bytes().
 void launch_hex_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
-                     double* per_elem, void* blocks, const EvalArgs& a, cudaStream_t s);
+                     double* per_elem, void* blocks, int* flags, const EvalArgs& a, cudaStream_t s);
 // Bytes of the block records launch_hex_eval needs: FP64 records, plus FP32 ones for a
 // projected mixed-precision Hessian (the projection runs in FP64).
 size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected);

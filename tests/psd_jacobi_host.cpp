@@ -9,7 +9,7 @@ namespace {
 template <int N>
 int project(const double* in, double* out, double* eig) {
     using J = lpg::PsdJacobi<N>;
-    std::vector<double> A(N * J::S), V(N * J::S), cs(N), L(N);
+    std::vector<double> A(N * J::S), V(N * J::S), cs(J::kCs), L(N);
     std::vector<int> pq(N);
     for (int i = 0; i < N; ++i)
         for (int j = 0; j < N; ++j) A[i * J::S + j] = in[i * N + j];
@@ -37,4 +37,11 @@ extern "C" int psd_project(int n, const double* in, double* out, double* eig) {
 // Pairs of round r of the n-index round-robin ordering (n = 24), 2 * n / 2 ints.
 extern "C" void psd_round_pairs(int r, int* out) {
     for (int k = 0; k < 12; ++k) lpg::PsdJacobi<24>::pair(r, k, out[2 * k], out[2 * k + 1]);
+}
+
+// The semi-definiteness test of the projection passes on a row-major 9 x 9 copy of V.
+extern "C" int psd_semidefinite9(const double* V, double tol) {
+    double W[81];
+    for (int i = 0; i < 81; ++i) W[i] = V[i];
+    return lpg::semidefinite_ldlt<9>(W, tol) ? 1 : 0;
 }

@@ -112,6 +112,24 @@ def test_compressed_hex_box_projected_hessian():
     assert rel_err(H32.toarray(), Hr) <= 1e-6
 
 
+def test_projected_hessian_half_at_rest():
+    """The lower layer of a hex box compressed to half its height, the upper layer at rest: the
+    upper elements pass the per-point semi-definiteness pre-test (their Hessian is kept), the
+    lower ones are indefinite and eigen-projected, in one launch."""
+    X, cells = oracle.hex_box(3, 3, 2)
+    theta = np.array([1.4e5, 3.4e4])
+    u = np.zeros_like(X)
+    u[:, 2] = -0.5 * np.minimum(X[:, 2], 0.5)
+    u = u.ravel()
+    _, _, He = oracle.hex_eval(X, cells, theta, u)
+    _, _, Hr = oracle.hex_eval(X, cells, theta, u, projected=True)
+    assert rel_err(Hr, He) > 0.05
+    gpu = hex_energy(X, cells, theta)
+    for precision, tol in (("f64", 1e-11), ("mixed", 1e-6)):
+        _, _, H = gpu.eval(u, hessian=Projected, precision=precision)
+        assert rel_err(H.toarray(), Hr) <= tol
+
+
 def test_construction_errors():
     gpu = hex_energy(HEX_X, HEX_CELLS, HEX_THETA)
     assert gpu.eval(hex_states()[1])[0] > 0

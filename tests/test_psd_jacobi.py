@@ -26,6 +26,7 @@ def psd(tmp_path_factory):
     lib = ctypes.CDLL(str(out))
     lib.psd_project.argtypes = [ctypes.c_int, _dp, _dp, _dp]
     lib.psd_round_pairs.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.psd_semidefinite9.argtypes = [_dp, ctypes.c_double]
 
     def run(H):
         H = np.ascontiguousarray(H, dtype=np.float64)
@@ -88,7 +89,8 @@ def test_degenerate_spectra(psd):
     rng = np.random.default_rng(7)
     Q, _ = np.linalg.qr(rng.standard_normal((24, 24)))
     lam = np.repeat([-2.0, 0.0, 1.0, 3.0], 6)  # repeated eigenvalues, a zero block
-    check(psd, (Q * lam) @ Q.T)
+    M = (Q * lam) @ Q.T
+    check(psd, 0.5 * (M + M.T))  # exactly symmetric, as the element records are
     P, sweeps = check(psd, np.zeros((24, 24)))
     assert sweeps == 0 and not P.any()
     D = np.diag(np.linspace(-1, 1, 24))
@@ -96,3 +98,51 @@ def test_degenerate_spectra(psd):
     assert sweeps == 0 and np.array_equal(P, np.maximum(D, 0))
     low = rng.standard_normal((24, 3))
     check(psd, low @ low.T)  # rank 3, PSD
+
+
+def nh_tangent_rowmajor(F, lam, mu):
+    """A(3i+j, 3k+l) = mu d_ik d_jl + lam G_ij G_kl - p G_il G_kj, G = F^-T, p = lam log J - mu:
+    the closed form the hex pre-test forms at each quadrature point."""
+    G = np.linalg.inv(F).T
+    p = lam * np.log(np.linalg.det(F)) - mu
+    A = mu * np.eye(9) + lam * np.outer(G.ravel(), G.ravel())
+    A -= p * np.einsum("il,kj->ijkl", G, G).reshape(9, 9)
+    return A
+
+
+@pytest.mark.parametrize("stretch", [1.0, 1.1, 0.9, 0.6, 1.6])
+def test_tangent_closed_form_and_semidefinite_test(psd, stretch):
+    """The closed-form tangent equals the oracle's d2W/dF2 (column-major vec there), and the LDL^T
+    test (tol 64 eps max|diag|, the tet projection pass's) agrees with the eigenvalues' sign:
+    at rest the tangent is singular semi-definite (rotation modes) and passes."""
+    lam, mu = 1.4e5, 3.4e4
+    rng = np.random.default_rng(int(stretch * 10))
+    F = np.diag([1.0, 1.0, stretch]) + (0.0 if stretch == 1.0 else 0.03) * rng.standard_normal((3, 3))
+    A = nh_tangent_rowmajor(F, lam, mu)
+    perm = np.array([i + 3 * j for i in range(3) for j in range(3)])  # row-major r -> column-major index
+    Ao = oracle.nh_d2W_dF2(F, np.eye(3), [lam, mu])[np.ix_(perm, perm)]
+    assert np.abs(A - Ao).max() <= 1e-12 * np.abs(Ao).max()
+    A = np.ascontiguousarray(A)
+    tol = 64 * np.finfo(float).eps * np.abs(np.diag(A)).max()
+    ev = np.linalg.eigvalsh(A)
+    got = psd.lib.psd_semidefinite9(A.ctypes.data_as(_dp), ctypes.c_double(tol))
+    if ev.min() >= 0 or ev.min() > -tol:
+        assert got == 1
+    elif ev.min() < -1e3 * tol:
+        assert got == 0
+
+
+def test_semidefinite_test_edge_cases(psd):
+    lib = psd.lib
+    rng = np.random.default_rng(3)
+    Q, _ = np.linalg.qr(rng.standard_normal((9, 9)))
+
+    def run(lam):
+        A = np.ascontiguousarray((Q * lam) @ Q.T)
+        return lib.psd_semidefinite9(A.ctypes.data_as(_dp), 64 * np.finfo(float).eps * np.abs(np.diag(A)).max())
+
+    assert run(np.linspace(0.1, 2, 9)) == 1
+    assert run(np.r_[np.zeros(3), np.linspace(0.1, 2, 6)]) == 1       # singular semi-definite
+    assert run(np.r_[-1e-6, np.linspace(0.1, 2, 8)]) == 0              # a small negative eigenvalue
+    assert run(np.r_[-1.0, np.zeros(2), np.linspace(0.1, 2, 6)]) == 0
+    assert run(np.zeros(9)) == 1
