@@ -2,13 +2,14 @@
 // cyclic Jacobi eigenvalue method in the round-robin parallel ordering (Brent and Luk, "The
 // solution of singular-value and symmetric eigenvalue problems on multiprocessor arrays", 1985):
 // a sweep is N - 1 rounds of N / 2 disjoint plane rotations, each round computed from one state
-// of the matrix, so the rotations of a round, their row updates and their column updates are
-// independent tasks. This is the projection HessianKind::Projected applies to every element's
-// local Hessian (mesh_energy.cpp:16-27, there by Eigen's SelfAdjointEigenSolver).
+// of the matrix, so a round is three data-parallel phases: the rotations, then every row of
+// A J and V J (one row per lane), then every column of J^T (A J) (one column per lane). This is
+// the projection HessianKind::Projected applies to every element's local Hessian
+// (mesh_energy.cpp:16-27, there by Eigen's SelfAdjointEigenSolver).
 //
-// The functions are the tasks of one round; a caller runs rotation() for k < N/2, then
-// update() for t < kUpdateTasks, with a barrier after each phase (one warp per matrix on the
-// GPU; plain loops on the host, where a test checks this code against an eigensolver).
+// The functions are the tasks of one round; eigen() runs them for a team of lanes with a
+// barrier after each phase (one warp per matrix on the GPU; plain loops on the host, where a
+// test checks this code against an eigensolver).
 #pragma once
 #include <math.h>
 
@@ -20,15 +21,21 @@
 
 namespace lpg {
 
+LPG_HD double inv_sqrt(double x) {
+#ifdef __CUDA_ARCH__
+    return rsqrt(x);
+#else
+    return 1.0 / sqrt(x);
+#endif
+}
+
 template <int N>
 struct PsdJacobi {
     static_assert(N % 2 == 0 && N >= 2, "the round-robin ordering pairs an even number of indices");
     static constexpr int S = N + 1;       // row stride (a padded row staggers column reads across banks)
     static constexpr int kPairs = N / 2;  // rotations per round
     static constexpr int kRounds = N - 1; // rounds per sweep: every index pair once
-    static constexpr int kCs = 3 * kPairs; // c, s, t per rotation
-    static constexpr int kBlockTasks = kPairs * (kPairs + 1) / 2; // 2x2 blocks (k, l), k <= l
-    static constexpr int kUpdateTasks = kBlockTasks + kPairs * N;  // ... then V's rows
+    static constexpr int kCs = 2 * kPairs; // c, s per rotation
     static constexpr int kMaxSweeps = 30;
     // A sweep ends the iteration once the off-diagonal Frobenius norm is below 1e-14 of the
     // matrix's (the projection moves by at most that much: it is non-expansive).
@@ -54,67 +61,46 @@ struct PsdJacobi {
         int p, q;
         pair(r, k, p, q);
         const double apq = A[p * S + q];
-        double c = 1.0, s = 0.0, t = 0.0;
+        double c = 1.0, s = 0.0;
         if (apq != 0.0) {
             const double th = (A[q * S + q] - A[p * S + p]) / (2.0 * apq);
             const double at = fabs(th);
-            t = at > 1e150 ? 0.5 / th : copysign(1.0, th) / (at + sqrt(th * th + 1.0));
-            c = 1.0 / sqrt(t * t + 1.0);
+            const double t = at > 1e150 ? 0.5 / th : copysign(1.0, th) / (at + sqrt(th * th + 1.0));
+            c = inv_sqrt(t * t + 1.0);
             s = t * c;
         }
-        cs[3 * k] = c;
-        cs[3 * k + 1] = s;
-        cs[3 * k + 2] = t;
+        cs[2 * k] = c;
+        cs[2 * k + 1] = s;
         pq[2 * k] = p;
         pq[2 * k + 1] = q;
     }
 
-    // Task t of a round's update. t < kBlockTasks: the 2x2 block of A at rows (p_k, q_k) and
-    // columns (p_l, q_l), k <= l, becomes J_k^T X J_l and is mirrored to (l, k); on a diagonal
-    // block (k = l) the rotation's own entry is annihilated exactly, a'_pp = a_pp - t a_pq,
-    // a'_qq = a_qq + t a_pq, a'_pq = 0, so A stays bitwise symmetric. Otherwise: columns p_k
-    // and q_k of V J at row i (t - kBlockTasks = k N + i).
-    LPG_HD static void update(double* A, double* V, const double* cs, const int* pq, int t) {
-        if (t >= kBlockTasks) {
-            const int u = t - kBlockTasks, k = u / N, i = u - N * k;
-            const double c = cs[3 * k], s = cs[3 * k + 1];
-            double* v = V + i * S;
+    // Row i of A J and of V J: columns p_k and q_k of every pair k.
+    LPG_HD static void right(double* A, double* V, const double* cs, const int* pq, int i) {
+        double* a = A + i * S;
+        double* v = V + i * S;
+        for (int k = 0; k < kPairs; ++k) {
             const int p = pq[2 * k], q = pq[2 * k + 1];
-            const double x = v[p], y = v[q];
-            v[p] = c * x - s * y;
-            v[q] = s * x + c * y;
-            return;
+            const double c = cs[2 * k], s = cs[2 * k + 1];
+            const double x = a[p], y = a[q];
+            a[p] = c * x - s * y;
+            a[q] = s * x + c * y;
+            const double vx = v[p], vy = v[q];
+            v[p] = c * vx - s * vy;
+            v[q] = s * vx + c * vy;
         }
-        int k = 0, l = t;
-        while (l >= kPairs - k) {
-            l -= kPairs - k;
-            ++k;
+    }
+
+    // Column j of J^T (A J): rows p_k and q_k of every pair k; the entries the rotations
+    // annihilate, (p_k, q_k) and (q_k, p_k), are set to zero.
+    LPG_HD static void left(double* A, const double* cs, const int* pq, int j) {
+        for (int k = 0; k < kPairs; ++k) {
+            const int p = pq[2 * k], q = pq[2 * k + 1];
+            const double c = cs[2 * k], s = cs[2 * k + 1];
+            const double x = A[p * S + j], y = A[q * S + j];
+            A[p * S + j] = j == q ? 0.0 : c * x - s * y;
+            A[q * S + j] = j == p ? 0.0 : s * x + c * y;
         }
-        l += k;
-        const int p = pq[2 * k], q = pq[2 * k + 1];
-        if (l == k) {
-            const double apq = A[p * S + q], tk = cs[3 * k + 2];
-            A[p * S + p] -= tk * apq;
-            A[q * S + q] += tk * apq;
-            A[p * S + q] = 0.0;
-            A[q * S + p] = 0.0;
-            return;
-        }
-        const int pl = pq[2 * l], ql = pq[2 * l + 1];
-        const double ck = cs[3 * k], sk = cs[3 * k + 1], cl = cs[3 * l], sl = cs[3 * l + 1];
-        const double x00 = A[p * S + pl], x01 = A[p * S + ql], x10 = A[q * S + pl], x11 = A[q * S + ql];
-        const double y00 = ck * x00 - sk * x10, y01 = ck * x01 - sk * x11; // rows: J_k^T X
-        const double y10 = sk * x00 + ck * x10, y11 = sk * x01 + ck * x11;
-        const double z00 = cl * y00 - sl * y01, z01 = sl * y00 + cl * y01; // columns: (J_k^T X) J_l
-        const double z10 = cl * y10 - sl * y11, z11 = sl * y10 + cl * y11;
-        A[p * S + pl] = z00;
-        A[p * S + ql] = z01;
-        A[q * S + pl] = z10;
-        A[q * S + ql] = z11;
-        A[pl * S + p] = z00;
-        A[ql * S + p] = z01;
-        A[pl * S + q] = z10;
-        A[ql * S + q] = z11;
     }
 
     // Entry (i, j), i <= j, of V diag(L) V^T for the clamped eigenvalues L (summed in index order).
@@ -159,7 +145,9 @@ struct PsdJacobi {
             for (int r = 0; r < kRounds; ++r) {
                 for (int k = lane; k < kPairs; k += nl) rotation(A, r, k, cs, pq);
                 team.sync();
-                for (int t = lane; t < kUpdateTasks; t += nl) update(A, V, cs, pq, t);
+                for (int i = lane; i < N; i += nl) right(A, V, cs, pq, i);
+                team.sync();
+                for (int j = lane; j < N; j += nl) left(A, cs, pq, j);
                 team.sync();
             }
         }
