@@ -75,32 +75,52 @@ struct PsdJacobi {
         pq[2 * k + 1] = q;
     }
 
+    // One row (or column) of the round's rotations applied from the right (or left): the round's
+    // pairs partition the indices, so the row's 2 kPairs entries are distinct and all of them are
+    // loaded before any is stored (one load latency per row instead of one per pair).
+    // x(m) addresses entry m of the row; zero_p / zero_q: set entries (row, q_k) / (row, p_k) of
+    // the pair whose p_k / q_k is the row itself to zero (the entries the rotations annihilate).
+    template <class Addr>
+    LPG_HD static void rotate_line(const double* cs, const int* pq, Addr x, int row, bool zero) {
+        double a[kPairs], b[kPairs], c[kPairs], s[kPairs];
+        int p[kPairs], q[kPairs];
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+        for (int k = 0; k < kPairs; ++k) {
+            p[k] = pq[2 * k];
+            q[k] = pq[2 * k + 1];
+            c[k] = cs[2 * k];
+            s[k] = cs[2 * k + 1];
+        }
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+        for (int k = 0; k < kPairs; ++k) {
+            a[k] = *x(p[k]);
+            b[k] = *x(q[k]);
+        }
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+        for (int k = 0; k < kPairs; ++k) {
+            *x(p[k]) = zero && row == q[k] ? 0.0 : c[k] * a[k] - s[k] * b[k];
+            *x(q[k]) = zero && row == p[k] ? 0.0 : s[k] * a[k] + c[k] * b[k];
+        }
+    }
+
     // Row i of A J and of V J: columns p_k and q_k of every pair k.
     LPG_HD static void right(double* A, double* V, const double* cs, const int* pq, int i) {
         double* a = A + i * S;
         double* v = V + i * S;
-        for (int k = 0; k < kPairs; ++k) {
-            const int p = pq[2 * k], q = pq[2 * k + 1];
-            const double c = cs[2 * k], s = cs[2 * k + 1];
-            const double x = a[p], y = a[q];
-            a[p] = c * x - s * y;
-            a[q] = s * x + c * y;
-            const double vx = v[p], vy = v[q];
-            v[p] = c * vx - s * vy;
-            v[q] = s * vx + c * vy;
-        }
+        rotate_line(cs, pq, [a](int m) { return a + m; }, i, false);
+        rotate_line(cs, pq, [v](int m) { return v + m; }, i, false);
     }
 
     // Column j of J^T (A J): rows p_k and q_k of every pair k; the entries the rotations
     // annihilate, (p_k, q_k) and (q_k, p_k), are set to zero.
     LPG_HD static void left(double* A, const double* cs, const int* pq, int j) {
-        for (int k = 0; k < kPairs; ++k) {
-            const int p = pq[2 * k], q = pq[2 * k + 1];
-            const double c = cs[2 * k], s = cs[2 * k + 1];
-            const double x = A[p * S + j], y = A[q * S + j];
-            A[p * S + j] = j == q ? 0.0 : c * x - s * y;
-            A[q * S + j] = j == p ? 0.0 : s * x + c * y;
-        }
+        rotate_line(cs, pq, [A, j](int m) { return A + m * S + j; }, j, true);
     }
 
     // Entry (i, j), i <= j, of V diag(L) V^T for the clamped eigenvalues L (summed in index order).
