@@ -681,7 +681,6 @@ int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io
 int lpg_fem_force_vjp_theta(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
-        tet_only(*h, "lpg_fem_force_vjp_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         const size_t n = 3 * static_cast<size_t>(h->dm.V);
@@ -898,7 +897,6 @@ int lpg_fem_set_tuning(lpg_fem_t h, const int32_t choice[6]) {
 int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
-        tet_only(*h, "lpg_fem_set_theta");
         if (!theta && h->dm.T > 0) fail(LPG_EINVAL, "lpg_fem_set_theta: null theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
@@ -906,6 +904,16 @@ int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element) {
         for (size_t k = 0; k < n && h->dm.T > 0; ++k)
             if (!std::isfinite(theta[k])) fail(LPG_EINVAL, "VolumetricFemEnergy: theta must be finite");
         if (h->dm.T == 0) return;
+        if (h->dm.K == 8) { // hexes keep theta per element, read at every evaluation
+            const size_t T = static_cast<size_t>(h->dm.T);
+            std::vector<double> th(2 * T);
+            for (size_t e = 0; e < T; ++e)
+                for (int c = 0; c < 2; ++c) th[2 * e + c] = theta_per_element ? theta[2 * e + c] : theta[c];
+            LPG_CUDA(cudaMemcpyAsync(h->dm.hex_theta, th.data(), 2 * T * sizeof(double),
+                                     cudaMemcpyHostToDevice, h->stream));
+            LPG_CUDA(cudaStreamSynchronize(h->stream));
+            return;
+        }
         double* d = h->d_u2.as<double>(n);
         LPG_CUDA(cudaMemcpyAsync(d, theta, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         launch_set_theta(h->dm, d, theta_per_element, h->stream);
@@ -965,7 +973,6 @@ int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, con
                       double* lambda_out) {
     return guarded([&] {
         if (!h || !u_star || !dLdu || !dtheta) fail(LPG_EINVAL, "lpg_adjoint_theta: null argument");
-        tet_only(*h, "lpg_adjoint_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         adjoint_theta(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, per_element, dtheta,

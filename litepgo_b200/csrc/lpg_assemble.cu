@@ -1815,6 +1815,93 @@ __global__ void __launch_bounds__(128) hex_element_kernel(const DevMesh m, const
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
+// Force-response parameter VJP of hex meshes (the tet pass's force_vjp_kernel at every
+// quadrature point): per element, with grad w = (sum_c w_c dN_c^T) J^-1 at each point,
+//   d/dlambda = sum_q w_q log J_q (F_q^-T : grad w_q),   d/dmu = sum_q w_q ((F_q - F_q^-T) : grad w_q),
+// w_q = weight det J. One thread per element, points in order; FP64.
+__global__ void __launch_bounds__(128) hex_force_vjp_kernel(const DevMesh m, const double* __restrict__ u,
+                                                            const double* __restrict__ w, double* out,
+                                                            unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        double dl = 0, dm = 0;
+        for (int q = 0; q < m.nq; ++q) {
+            const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
+            double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double Wr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int c = 0; c < 8; ++c) {
+                const int v = __ldg(cell + c);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
+                    const double uu = __ldg(u + 3 * static_cast<size_t>(v) + i);
+                    const double ww = __ldg(w + 3 * static_cast<size_t>(v) + i);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const double dn = __ldg(dq + 3 * c + d);
+                        J[3 * i + d] = fma(X, dn, J[3 * i + d]);
+                        G[3 * i + d] = fma(uu, dn, G[3 * i + d]);
+                        Wr[3 * i + d] = fma(ww, dn, Wr[3 * i + d]);
+                    }
+                }
+            }
+            const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                              J[2] * (J[3] * J[7] - J[4] * J[6]);
+            const double iJ = 1.0 / dJ;
+            double Ji[9];
+            Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
+            Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
+            Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
+            Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
+            Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
+            Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
+            Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
+            Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
+            Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+            double F[9], Wg[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    F[3 * i + j] = (i == j ? 1.0 : 0.0) + G[3 * i] * Ji[j] + G[3 * i + 1] * Ji[3 + j] +
+                                   G[3 * i + 2] * Ji[6 + j];
+                    Wg[3 * i + j] = Wr[3 * i] * Ji[j] + Wr[3 * i + 1] * Ji[3 + j] + Wr[3 * i + 2] * Ji[6 + j];
+                }
+            double C[9];
+            C[0] = F[4] * F[8] - F[5] * F[7];
+            C[1] = F[5] * F[6] - F[3] * F[8];
+            C[2] = F[3] * F[7] - F[4] * F[6];
+            C[3] = F[2] * F[7] - F[1] * F[8];
+            C[4] = F[0] * F[8] - F[2] * F[6];
+            C[5] = F[1] * F[6] - F[0] * F[7];
+            C[6] = F[1] * F[5] - F[2] * F[4];
+            C[7] = F[2] * F[3] - F[0] * F[5];
+            C[8] = F[0] * F[4] - F[1] * F[3];
+            const double detF = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+            if (!(detF > 0) || !isfinite(detF)) {
+                st |= isfinite(detF) ? ST_BAD_DET : ST_NONFINITE_F;
+                continue;
+            }
+            double hf = 0, ff = 0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                hf = fma(C[k] / detF, Wg[k], hf);
+                ff = fma(F[k], Wg[k], ff);
+            }
+            const double wq = __ldg(dq + 24) * dJ;
+            dl = fma(wq * log(detF), hf, dl);
+            dm = fma(wq, ff - hf, dm);
+        }
+        if (!isfinite(dl) || !isfinite(dm)) st |= ST_NONFINITE_OUT;
+        out[2 * static_cast<size_t>(e)] = dl;
+        out[2 * static_cast<size_t>(e) + 1] = dm;
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
 // Pre-test of the hex projection: H = sum_q w_q B_q^T A_q B_q (w_q > 0) is semi-definite when
 // every quadrature point's tangent A_q = dP/dF is, and then H is its own projection. One thread
 // per (element, point) forms
@@ -2213,7 +2300,10 @@ void launch_feasible(const DevMesh& m, const double* u, const double* du, double
 
 void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out, unsigned* status,
                       cudaStream_t s) {
-    if (m.T > 0) force_vjp_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, u, w, out, status);
+    if (m.T > 0 && m.K == 8)
+        hex_force_vjp_kernel<<<(m.T + 127) / 128, 128, 0, s>>>(m, u, w, out, status);
+    else if (m.T > 0)
+        force_vjp_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, u, w, out, status);
     LPG_CUDA(cudaGetLastError());
 }
 

@@ -33,6 +33,7 @@ __all__ = [
     "VolumetricFemForceMaterialResponse",
     "VolumetricFemEnergyTetP1",
     "VolumetricFemForceMaterialResponseTetP1",
+    "VolumetricFemForceMaterialResponseHexQ1",
     "VolumetricFemForceRestPositionResponseTetP1",
     "VolumetricFemForceFpResponse",
     "VolumetricFemForceFpResponseTetP1",
@@ -545,6 +546,8 @@ class VolumetricFemForceMaterialResponseTetP1:
     ElementDofMap gives each element its own block.
     """
 
+    _energy_cls = VolumetricFemEnergyTetP1
+
     def __init__(self, parameter_map, displacement_map, rest_position_fields, displacement, Fp, batch_size=256):
         if isinstance(batch_size, bool) or int(batch_size) <= 0:
             raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
@@ -561,7 +564,7 @@ class VolumetricFemForceMaterialResponseTetP1:
         if u.size != displacement_map.num_dofs or not np.all(np.isfinite(u)):
             raise ValueError("VolumetricFemForceResponse: incompatible map, displacement or responses")
         # theta does not enter d g / d theta (P is linear in theta); any valid value builds the mesh.
-        self._energy = VolumetricFemEnergyTetP1(displacement_map, rest_position_fields, Fp, np.array([1.0, 1.0]))
+        self._energy = self._energy_cls(displacement_map, rest_position_fields, Fp, np.array([1.0, 1.0]))
         self.displacement = u
         self.num_inputs = parameter_map.num_dofs
         self.num_outputs = displacement_map.num_dofs
@@ -698,8 +701,9 @@ class VolumetricFemForceFpResponseTetP1:
 class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
     """VolumetricFemEnergy[NeoHookean, HexQ1Basis, GaussLegendre3D[n]] on one GPU (the class
     variable ``points_per_axis`` is set by the template). The rest positions are vertex positions
-    (V, 3); no plastic field. The Energy interface is the tet energy's, with the Exact Hessian only
-    (a projected request raises ValueError); Newton runs with hessian=Exact."""
+    (V, 3); no plastic field. The Energy interface is the tet energy's, with the Exact and the
+    Projected Hessian (each element's 24x24 Hessian projected to PSD); set_theta, the theta force
+    response and the theta adjoint work as for tets."""
 
     points_per_axis = 2
 
@@ -751,6 +755,18 @@ class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
 
 class VolumetricFemEnergyHexQ1GL4(VolumetricFemEnergyHexQ1):
     points_per_axis = 4
+
+
+class VolumetricFemForceMaterialResponseHexQ1(VolumetricFemForceMaterialResponseTetP1):
+    """VolumetricFemForceMaterialResponse[NeoHookean, HexQ1Basis, GaussLegendre3D[2]]: the
+    force's VJP in theta summed over the quadrature points of each hex (vertex rest positions
+    (V, 3), no plastic field); usable as the make_response of a StaticEquilibriumResponse."""
+
+    _energy_cls = VolumetricFemEnergyHexQ1
+
+
+class VolumetricFemForceMaterialResponseHexQ1GL4(VolumetricFemForceMaterialResponseTetP1):
+    _energy_cls = VolumetricFemEnergyHexQ1GL4
 
 
 class PyVolumetricMaterial:
@@ -940,7 +956,9 @@ VolumetricFemEnergy = Template("VolumetricFemEnergy",
 VolumetricFemEnergy.material_factory = _py_energy_class
 VolumetricFemForceMaterialResponse = Template(
     "VolumetricFemForceMaterialResponse",
-    {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceMaterialResponseTetP1})
+    {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceMaterialResponseTetP1,
+     (NeoHookean, HexQ1Basis, GaussLegendre3D_2): VolumetricFemForceMaterialResponseHexQ1,
+     (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemForceMaterialResponseHexQ1GL4})
 VolumetricFemForceFpResponse = Template(
     "VolumetricFemForceFpResponse",
     {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceFpResponseTetP1})

@@ -12,6 +12,7 @@ from .oracle import (  # noqa: F401
     hex_box,
     hex_dN_dxi,
     hex_eval,
+    hex_force_vjp_theta,
     hex_points,
     OracleMesh,
     build,

@@ -371,6 +371,29 @@ def hex_eval(X, cells, theta, u, points_per_axis=2, hessian=True, projected=Fals
     return E, g, H
 
 
+def hex_force_vjp_theta(X, cells, theta, u, w, points_per_axis=2):
+    """(d g / d theta)^T w per hex (T, 2) for the hex Q1 neo-Hookean force g (Fp = I): at every
+    point w_q d2W/dF dtheta : grad w (VolumetricFemForceMaterialResponse over the hex basis)."""
+    X = np.asarray(X, float).reshape(-1, 3)
+    cells = np.asarray(cells).reshape(-1, 8)
+    U = np.asarray(u, float).reshape(-1, 3)
+    Wv = np.asarray(w, float).reshape(-1, 3)
+    T = cells.shape[0]
+    th = np.broadcast_to(np.asarray(theta, float), (T, 2))
+    pts, wts = hex_points(points_per_axis)
+    out = np.zeros((T, 2))
+    for e, cell in enumerate(cells):
+        for xi, wq in zip(pts, wts):
+            dN = hex_dN_dxi(xi)
+            J = X[cell].T @ dN
+            gN = dN @ np.linalg.inv(J)
+            F = np.eye(3) + U[cell].T @ gN
+            Gw = Wv[cell].T @ gN  # grad w, [i, j]
+            D = nh_d2W_dF_dtheta(F, np.eye(3), th[e])  # (9, 2), rows column-major vec(F)
+            out[e] += wq * np.linalg.det(J) * (D.T @ Gw.T.ravel())
+    return out
+
+
 def hex_box(nx, ny=None, nz=None):
     """Structured box of nx*ny*nz unit-spacing-scaled hexes on [0,1]^3 (corner order above)."""
     ny = nx if ny is None else ny

@@ -173,3 +173,86 @@ def test_hex_newton_under_gravity(precision, hessian):
     _, g, _ = oracle.hex_eval(X, cells, theta, x, hessian=False)
     free = np.setdiff1d(np.arange(n), fixed)
     assert np.abs((g - f)[free]).max() <= 1e-7 * np.abs(f).max()
+
+
+def test_hex_theta_vjp_and_set_theta():
+    """The hex force's theta VJP (VolumetricFemForceMaterialResponse over HexQ1Basis) against
+    the oracle per element and summed; set_theta against a freshly built energy (bitwise)."""
+    from litepgo_b200 import dof
+
+    X, cells = oracle.hex_box(3, 3, 2)
+    rng = np.random.default_rng(5)
+    T = cells.shape[0]
+    A = np.eye(3) + 0.1 * rng.standard_normal((3, 3))
+    u = (X @ A.T - X + 1e-3 * rng.standard_normal(X.shape)).ravel()
+    w = rng.standard_normal(u.size)
+    topo = mesh.HexTopology(X.shape[0], cells)
+    ref = oracle.hex_force_vjp_theta(X, cells, np.array([1.0, 1.0]), u, w)
+    for cls, n in ((fem.VolumetricFemForceMaterialResponse[fem.NeoHookean, fem.HexQ1Basis, fem.GaussLegendre3D[2]], 2),
+                   (fem.VolumetricFemForceMaterialResponse[fem.NeoHookean, fem.HexQ1Basis, fem.GaussLegendre3D[4]], 4)):
+        r = oracle.hex_force_vjp_theta(X, cells, np.array([1.0, 1.0]), u, w, points_per_axis=n) if n == 4 else ref
+        per = cls(dof.ElementDofMap(topo, 2), dof.VertexDofMap(topo, 3), X, u, None)
+        got = per.eval_vjp(np.tile([1e5, 3e4], T), w).reshape(T, 2)
+        assert rel_err(got, r) <= 1e-12
+        shared = cls(dof.ConstantDofMap(topo, 2), dof.VertexDofMap(topo, 3), X, u, None)
+        assert rel_err(shared.eval_vjp(np.array([1e5, 3e4]), w), r.sum(0)) <= 1e-12
+    th = np.column_stack([np.full(T, 1.2e5), 3e4 * (1 + 0.3 * rng.random(T))])
+    e = hex_energy(X, cells, np.array([1.4e5, 3.4e4]))
+    e.set_theta(th)
+    E1, g1, H1 = e.eval(u, gradient=True, hessian=Exact)
+    E2, g2, H2 = hex_energy(X, cells, th).eval(u, gradient=True, hessian=Exact)
+    assert E1 == E2 and np.array_equal(g1, g2) and np.array_equal(H1.data, H2.data)
+
+
+def test_hex_theta_adjoint_matches_finite_differences():
+    """Per-element [lambda, mu] of a 5x5x5 hex box under gravity (bottom face held) as a torch
+    leaf, loss |x*(theta) - x_t|^2: the adjoint gradient against five-point differences of the
+    loss (step 1e-4 relative to theta) along 8 seeded directions, to 1e-6."""
+    from litepgo_b200 import dof
+    from litepgo_b200 import torch as bridge
+
+    X, cells = oracle.hex_box(5)
+    n, T = X.size, cells.shape[0]
+    rng = np.random.default_rng(3)
+    mu = 3e4 * (1 + 0.5 * rng.random(T))
+    theta0 = np.column_stack([4 * mu, mu])
+    pts, wts = oracle.hex_points(2)
+    f = np.zeros(n)
+    for cell in cells:
+        for xi, wq in zip(pts, wts):
+            dN = oracle.hex_dN_dxi(xi)
+            f[3 * cell + 2] += -9.8 * 1000 * wq * np.linalg.det(X[cell].T @ dN) * fem.HexQ1Basis.eval_N(xi)
+    fixed = np.flatnonzero(np.repeat(X[:, 2] == 0, 3))
+    load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -f)
+    shared = hex_energy(X, cells, theta0)
+    topo = mesh.HexTopology(X.shape[0], cells)
+    Resp = fem.VolumetricFemForceMaterialResponse[fem.NeoHookean, fem.HexQ1Basis, fem.GaussLegendre3D[2]]
+
+    def make_energy(p):
+        shared.set_theta(p.reshape(T, 2))
+        return energy.WeightedSumEnergy([(shared, 1.0), (load, 1.0)])
+
+    def make_response(u):
+        return Resp(dof.ElementDofMap(topo, 2), dof.VertexDofMap(topo, 3), X, u, None)
+
+    opts = solver.NewtonOptions(gradient_tolerance=1e-12 * np.abs(f).max(), stop_rule="max_abs", accept_rule="noise",
+                                max_iterations=100, cg_tolerance=1e-3)
+    model = solver.StaticEquilibriumResponse(2 * T, dof.DofReduction(n, fixed), np.zeros(n), opts, make_energy,
+                                             make_response)
+    x_target = model.eval_value((theta0 * (1 + 0.2 * rng.standard_normal(theta0.shape))).ravel())
+    theta = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+    loss = ((bridge.response(model, theta.reshape(-1)) - torch.as_tensor(x_target)) ** 2).sum()
+    loss.backward()
+    grad = theta.grad.numpy().ravel()
+    th0 = theta0.ravel()
+    warm = solver.StaticEquilibriumResponse(2 * T, dof.DofReduction(n, fixed), model.eval_value(th0), opts,
+                                            make_energy, make_response)
+
+    def L(q):
+        return float(np.sum((warm.eval_value(q) - x_target) ** 2))
+
+    h = 1e-4
+    for _ in range(8):
+        d = rng.standard_normal(2 * T) * th0
+        fd = (8 * (L(th0 + h * d) - L(th0 - h * d)) - (L(th0 + 2 * h * d) - L(th0 - 2 * h * d))) / (12 * h)
+        assert abs(grad @ d - fd) <= 1e-6 * abs(fd)

@@ -64,3 +64,24 @@ def test_patch_test_and_quadrature(n):
 def test_invalid_geometry_is_rejected(scale):
     with pytest.raises(ValueError):
         oracle.hex_eval(scale * HEX_X, HEX_CELLS, HEX_THETA, np.zeros(HEX_X.size))
+
+
+@pytest.mark.parametrize("state", [1, 2])
+def test_hex_theta_vjp_matches_finite_differences(state):
+    """The oracle's hex theta VJP (per element) against central differences of w . g(u; theta)
+    in each element's own [lambda, mu] (g is linear in theta, so the difference is exact up to
+    rounding)."""
+    x = hex_states()[state]
+    w = np.cos(np.arange(x.size) + 0.7)
+    theta = np.array([[2.0, 3.0], [5.0, 1.5]])
+    vjp = oracle.hex_force_vjp_theta(HEX_X, HEX_CELLS, theta, x, w)
+    h = 1e-3
+    for e in range(2):
+        for c in range(2):
+            tp, tm = theta.copy(), theta.copy()
+            tp[e, c] += h
+            tm[e, c] -= h
+            gp = oracle.hex_eval(HEX_X, HEX_CELLS, tp, x, hessian=False)[1]
+            gm = oracle.hex_eval(HEX_X, HEX_CELLS, tm, x, hessian=False)[1]
+            fd = w @ (gp - gm) / (2 * h)
+            assert abs(vjp[e, c] - fd) <= 1e-9 * (1 + abs(fd))
