@@ -137,10 +137,11 @@ int lpg_fem_destroy(lpg_fem_t h);
  * ((0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1), (1,0,1), (1,1,1), (0,1,1) of [0,1]^3); X: rest
  * positions (3 per vertex); theta: [lambda, mu] (2, or 2 per element); points_per_axis: 2 or
  * 4. Every quadrature point must have det J > 0 (LPG_EINVAL otherwise, as
- * VolumetricElement3D). The handle answers lpg_fem_eval (Exact Hessian; the projected one is
- * LPG_EINVAL), lpg_fem_feasible_step, lpg_fem_element_energies, the patterns, and
- * lpg_newton_solve with the Exact Hessian; the sensitivity, plastic-field, material and batch
- * entry points are for tet meshes only (LPG_EINVAL). No plastic field (Fp = I).
+ * VolumetricElement3D). The handle answers lpg_fem_eval (Exact, and Projected: each element's
+ * 24x24 Hessian projected to PSD), lpg_fem_feasible_step, lpg_fem_element_energies, the
+ * patterns, lpg_newton_solve, lpg_fem_set_theta, lpg_fem_force_vjp_theta and lpg_adjoint_theta;
+ * the rest-position, plastic-field, material and batch entry points are for tet meshes only
+ * (LPG_EINVAL). No plastic field (Fp = I).
  */
 int lpg_fem_create_hex(int num_vertices, const double* X, int num_cells, const int32_t* cells, const double* theta,
                        int theta_per_element, int points_per_axis, int device, lpg_fem_t* out);
