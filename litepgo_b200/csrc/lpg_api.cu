@@ -539,16 +539,20 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
 int lpg_fem_deformation_gradients(lpg_fem_t h, const double* u, int io_mem, double* F) {
     return guarded([&] {
         if (!h || !F) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: null argument");
-        tet_only(*h, "lpg_fem_deformation_gradients");
         if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: the handle has a plastic field");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
-        const size_t n = 3 * static_cast<size_t>(h->dm.V), T = static_cast<size_t>(h->dm.T);
+        const bool hex = h->dm.K == 8;
+        const size_t n = 3 * static_cast<size_t>(h->dm.V);
+        const size_t rows = static_cast<size_t>(h->dm.T) * (hex ? h->dm.nq : 1); // one F per quadrature point
         const double* du = h->stage_in(u, io_mem, h->d_u, n);
-        double* dF = io_mem == LPG_MEM_DEVICE ? F : h->d_vjp.as<double>(std::max<size_t>(9 * T, 1));
-        launch_deformation_gradients(h->dm, du, dF, h->d_status.as<unsigned>(1), h->stream);
-        if (io_mem == LPG_MEM_HOST && T > 0)
-            LPG_CUDA(cudaMemcpyAsync(F, dF, 9 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        double* dF = io_mem == LPG_MEM_DEVICE ? F : h->d_vjp.as<double>(std::max<size_t>(9 * rows, 1));
+        if (hex)
+            launch_hex_deformation_gradients(h->dm, du, dF, h->d_status.as<unsigned>(1), h->stream);
+        else
+            launch_deformation_gradients(h->dm, du, dF, h->d_status.as<unsigned>(1), h->stream);
+        if (io_mem == LPG_MEM_HOST && rows > 0)
+            LPG_CUDA(cudaMemcpyAsync(F, dF, 9 * rows * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         raise_status(h->take_status());
     });
 }
@@ -557,9 +561,10 @@ int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const d
                           double* grad, int hessian, int precision, int layout, void* hess, int out_mem) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
-        tet_only(*h, "lpg_fem_eval_material");
         if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_eval_material: the handle has a plastic field");
-        const size_t T = static_cast<size_t>(h->dm.T), n = 3 * static_cast<size_t>(h->dm.V);
+        const bool hex = h->dm.K == 8;
+        // Material rows: one per element (tets) or per quadrature point (hexes).
+        const size_t T = static_cast<size_t>(h->dm.T) * (hex ? h->dm.nq : 1), n = 3 * static_cast<size_t>(h->dm.V);
         if (T > 0 && (!W || (grad && !P))) fail(LPG_EINVAL, "lpg_fem_eval_material: null material output");
         if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
             fail(LPG_EINVAL, "Energy: invalid Hessian kind");
@@ -591,11 +596,19 @@ int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const d
         a.energy = h->d_energy.as<double>(1);
         a.status = h->d_status.as<unsigned>(1);
         const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
-        void* proj = a.hess ? h->d_proj.ensure(project_bytes(h->dm, precision)) : nullptr;
-        launch_material_eval(h->dm, precision, hessian, dW, dP, dA, h->d_mat[3].as<double>(std::max<size_t>(T, 1)),
-                             h->d_vjp.as<double>(std::max<size_t>(12 * T, 1)), proj,
-                             h->d_plist.as<int>(std::max<size_t>(T, 1)), h->d_pcount.as<unsigned>(1), h->tune.clamp[pi],
-                             a, s);
+        const size_t nel = std::max<size_t>(static_cast<size_t>(h->dm.T), 1);
+        if (hex) {
+            const bool projected = hessian == LPG_HESSIAN_PROJECTED;
+            void* blocks = a.hess ? h->d_proj.ensure(hex_blocks_bytes(h->dm, precision, projected)) : nullptr;
+            launch_hex_material_eval(h->dm, precision, hessian, dW, dP, dA, h->d_mat[3].as<double>(nel),
+                                     h->d_vjp.as<double>(24 * nel), blocks,
+                                     projected && a.hess ? h->d_plist.as<int>(nel) : nullptr, a, s);
+        } else {
+            void* proj = a.hess ? h->d_proj.ensure(project_bytes(h->dm, precision)) : nullptr;
+            launch_material_eval(h->dm, precision, hessian, dW, dP, dA, h->d_mat[3].as<double>(nel),
+                                 h->d_vjp.as<double>(12 * nel), proj, h->d_plist.as<int>(nel),
+                                 h->d_pcount.as<unsigned>(1), h->tune.clamp[pi], a, s);
+        }
         double e = 0;
         LPG_CUDA(cudaMemcpyAsync(&e, a.energy, sizeof e, cudaMemcpyDeviceToHost, s));
         if (grad && out_mem == LPG_MEM_HOST && n > 0)

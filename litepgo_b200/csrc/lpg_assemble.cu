@@ -1902,6 +1902,174 @@ __global__ void __launch_bounds__(128) hex_force_vjp_kernel(const DevMesh m, con
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
+// Materials evaluated outside the library on hex meshes (PyVolumetricMaterial over HexQ1Basis):
+// F at every quadrature point (row-major, 9 per point, points of an element consecutive), then
+// the caller's W, P = dW/dF and A = d2W/dF2 per point integrated and assembled per hex.
+__device__ __forceinline__ void hex_point_geometry(const DevMesh& m, const int32_t* cell, const double* dq,
+                                                   double (&Ji)[9], double& dJ) {
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < 8; ++c) {
+        const int v = __ldg(cell + c);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) J[3 * i + d] = fma(X, __ldg(dq + 3 * c + d), J[3 * i + d]);
+        }
+    }
+    dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+    const double iJ = 1.0 / dJ;
+    Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
+    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
+    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
+    Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
+    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
+    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
+    Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
+    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
+    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+}
+
+__global__ void __launch_bounds__(128) hex_deformation_gradient_kernel(const DevMesh m, const double* __restrict__ u,
+                                                                       double* __restrict__ F, unsigned* status) {
+    const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (t < static_cast<size_t>(m.T) * m.nq) {
+        const int e = static_cast<int>(t / m.nq), q = static_cast<int>(t - static_cast<size_t>(m.nq) * e);
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
+        double Ji[9], dJ;
+        hex_point_geometry(m, cell, dq, Ji, dJ);
+        double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        bool ok = true;
+        for (int c = 0; c < 8; ++c) {
+            const int v = __ldg(cell + c);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double uu = __ldg(u + 3 * static_cast<size_t>(v) + i);
+                ok = ok && isfinite(uu);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) G[3 * i + d] = fma(uu, __ldg(dq + 3 * c + d), G[3 * i + d]);
+            }
+        }
+        if (!ok) st |= ST_BAD_INPUT;
+        double* o = F + 9 * t;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                o[3 * i + j] = (i == j ? 1.0 : 0.0) + G[3 * i] * Ji[j] + G[3 * i + 1] * Ji[3 + j] + G[3 * i + 2] * Ji[6 + j];
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// One thread per (element, vertex pair a <= b), 36 per hex, points in order: with grad N = J^-T dN
+// and w_q = weight det J,
+//   H_ab(i, k) += w_q sum_{j, l} grad N_a[j] As(3 i + j, 3 k + l) grad N_b[l],  As = (A + A^T) / 2,
+//   g_a += w_q P grad N_a (pairs (a, a)),  E += w_q W (pair (0, 0)).
+// Diagonal blocks are mirrored (bitwise symmetric); A may be null when no Hessian is asked for.
+template <typename R>
+__global__ void __launch_bounds__(128) hex_material_kernel(const DevMesh m, const double* __restrict__ W,
+                                                           const double* __restrict__ P, const double* __restrict__ A,
+                                                           double* __restrict__ elemE, double* __restrict__ per_elem,
+                                                           R* __restrict__ blocks, unsigned* status) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    const int e = t / 36, pr = t - 36 * (t / 36);
+    if (e < m.T) {
+        int a, b;
+        hex_pair(pr, a, b);
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        double Hb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, ga[3] = {0, 0, 0}, E = 0;
+        for (int q = 0; q < m.nq; ++q) {
+            const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
+            double Ji[9], dJ;
+            hex_point_geometry(m, cell, dq, Ji, dJ);
+            const double w = __ldg(dq + 24) * dJ;
+            const size_t pt = static_cast<size_t>(e) * m.nq + q;
+            double na[3], nb[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                na[j] = __ldg(dq + 3 * a) * Ji[j] + __ldg(dq + 3 * a + 1) * Ji[3 + j] + __ldg(dq + 3 * a + 2) * Ji[6 + j];
+                nb[j] = __ldg(dq + 3 * b) * Ji[j] + __ldg(dq + 3 * b + 1) * Ji[3 + j] + __ldg(dq + 3 * b + 2) * Ji[6 + j];
+            }
+            if (blocks) {
+                const double* Aq = A + 81 * pt;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        double v = 0;
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+#pragma unroll
+                            for (int l = 0; l < 3; ++l) {
+                                const double as = 0.5 * (__ldg(Aq + 9 * (3 * i + j) + 3 * k + l) +
+                                                         __ldg(Aq + 9 * (3 * k + l) + 3 * i + j));
+                                v = fma(na[j] * as, nb[l], v);
+                            }
+                        Hb[3 * i + k] = fma(w, v, Hb[3 * i + k]);
+                    }
+            }
+            if (a == b && per_elem) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double* Pq = P + 9 * pt + 3 * i;
+                    ga[i] = fma(w, __ldg(Pq) * na[0] + __ldg(Pq + 1) * na[1] + __ldg(Pq + 2) * na[2], ga[i]);
+                }
+            }
+            if (pr == 0) E = fma(w, __ldg(W + pt), E);
+        }
+        if (a == b) {
+            Hb[3] = Hb[1];
+            Hb[6] = Hb[2];
+            Hb[7] = Hb[5];
+        }
+        if (blocks) {
+            R* o = blocks + kHexRecord * static_cast<size_t>(e) + 9 * pr;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                if (!isfinite(Hb[k])) st |= ST_NONFINITE_OUT;
+                o[k] = static_cast<R>(Hb[k]);
+            }
+        }
+        if (a == b && per_elem) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (!isfinite(ga[i])) st |= ST_NONFINITE_OUT;
+                per_elem[24 * static_cast<size_t>(e) + 3 * a + i] = ga[i];
+            }
+        }
+        if (pr == 0) {
+            if (!isfinite(E)) st |= ST_NONFINITE_OUT;
+            elemE[e] = E;
+        }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
+// The projection pre-test on a material's own tangents: one thread per (element, point), the
+// symmetrised As = (A + A^T) / 2 through the LDL^T test; an element with a point that fails is
+// marked in flags (zeroed before).
+__global__ void __launch_bounds__(128) hex_material_tangent_test_kernel(const DevMesh m, const double* __restrict__ A,
+                                                                        int* __restrict__ flags) {
+    const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<size_t>(m.T) * m.nq) return;
+    const int e = static_cast<int>(t / m.nq);
+    const double* Aq = A + 81 * t;
+    double V[81];
+    double scale = 0;
+    for (int r = 0; r < 9; ++r)
+        for (int c = 0; c < 9; ++c) {
+            const double v = 0.5 * (__ldg(Aq + 9 * r + c) + __ldg(Aq + 9 * c + r));
+            V[9 * r + c] = v;
+            if (r == c) scale = fmax(scale, fabs(v));
+        }
+    if (!(scale < INFINITY) || !semidefinite_ldlt<9>(V, 64 * Eps<double>::v * scale)) flags[e] = 1;
+}
+
 // Pre-test of the hex projection: H = sum_q w_q B_q^T A_q B_q (w_q > 0) is semi-definite when
 // every quadrature point's tangent A_q = dP/dF is, and then H is its own projection. One thread
 // per (element, point) forms
@@ -2360,6 +2528,58 @@ void launch_material_eval(const DevMesh& m, int precision, int hessian, const do
             launch_block_gather<float>(m, ga, s);
         }
     }
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_hex_deformation_gradients(const DevMesh& m, const double* u, double* F, unsigned* status, cudaStream_t s) {
+    const size_t points = static_cast<size_t>(m.T) * m.nq;
+    if (points > 0) hex_deformation_gradient_kernel<<<static_cast<int>((points + 127) / 128), 128, 0, s>>>(m, u, F, status);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_hex_material_eval(const DevMesh& m, int precision, int hessian, const double* W, const double* P,
+                              const double* A, double* elemE, double* per_elem, void* blocks, int* flags,
+                              const EvalArgs& a, cudaStream_t s) {
+    const bool projected = hessian == LPG_HESSIAN_PROJECTED;
+    if (m.T > 0) {
+        const size_t threads = 36 * static_cast<size_t>(m.T);
+        const int grid = static_cast<int>((threads + 127) / 128);
+        double* per_grad = a.grad ? per_elem : nullptr;
+        if (a.hess && projected) {
+            double* records = static_cast<double*>(blocks);
+            hex_material_kernel<double><<<grid, 128, 0, s>>>(m, W, P, A, elemE, per_grad, records, a.status);
+            LPG_CUDA(cudaMemsetAsync(flags, 0, static_cast<size_t>(m.T) * sizeof(int), s));
+            const size_t points = static_cast<size_t>(m.T) * m.nq;
+            hex_material_tangent_test_kernel<<<static_cast<int>((points + 127) / 128), 128, 0, s>>>(m, A, flags);
+            const int pgrid = (m.T + kHexPsdWarps - 1) / kHexPsdWarps;
+            if (precision == LPG_PRECISION_F64) {
+                hex_psd_kernel<double><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, records, flags, a.status);
+            } else {
+                float* out = reinterpret_cast<float*>(records + kHexRecord * static_cast<size_t>(m.T));
+                hex_psd_kernel<float><<<pgrid, 32 * kHexPsdWarps, 0, s>>>(m.T, records, out, flags, a.status);
+                blocks = out;
+            }
+        } else if (precision == LPG_PRECISION_F64 || !a.hess) {
+            hex_material_kernel<double><<<grid, 128, 0, s>>>(m, W, P, A, elemE, per_grad,
+                                                             a.hess ? static_cast<double*>(blocks) : nullptr, a.status);
+        } else {
+            hex_material_kernel<float><<<grid, 128, 0, s>>>(m, W, P, A, elemE, per_grad, static_cast<float*>(blocks),
+                                                            a.status);
+        }
+        if (a.grad) vertex_gather_kernel<8><<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
+        if (a.hess) {
+            EvalArgs ga = a;
+            ga.proj = blocks;
+            if (precision == LPG_PRECISION_F64)
+                launch_block_gather<double, 8>(m, ga, s);
+            else
+                launch_block_gather<float, 8>(m, ga, s);
+        }
+    }
+    if (a.grad && m.num_unused > 0)
+        zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(elemE, m.T, a.cluster_energy);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.cluster_energy, kSumBlocks, a.energy);
     LPG_CUDA(cudaGetLastError());
 }
 

@@ -212,6 +212,13 @@ void launch_sum_pairs(const double* per_elem, int T, double* partial, int nblock
 // elements that need the eigen-projection); blocks then holds hex_blocks_bytes().
 void launch_hex_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
                      double* per_elem, void* blocks, int* flags, const EvalArgs& a, cudaStream_t s);
+// Python/Torch materials on hex meshes: F at every quadrature point (9 per point, T * nq rows,
+// element-major), and the caller's W (T nq), P (9 T nq) and A (81 T nq, or null without a
+// Hessian) integrated per hex and assembled (blocks and flags as for launch_hex_eval).
+void launch_hex_deformation_gradients(const DevMesh& m, const double* u, double* F, unsigned* status, cudaStream_t s);
+void launch_hex_material_eval(const DevMesh& m, int precision, int hessian, const double* W, const double* P,
+                              const double* A, double* elemE, double* per_elem, void* blocks, int* flags,
+                              const EvalArgs& a, cudaStream_t s);
 // Bytes of the block records launch_hex_eval needs: FP64 records, plus FP32 ones for a
 // projected mixed-precision Hessian (the projection runs in FP64).
 size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected);

@@ -42,6 +42,7 @@ __all__ = [
     "HexQ1Basis",
     "GaussLegendre3D",
     "VolumetricFemEnergyHexQ1",
+    "VolumetricFemEnergyPyMaterialHexQ1",
 ]
 
 
@@ -175,8 +176,8 @@ class Template:
         key = args if isinstance(args, tuple) else (args,)
         factory = getattr(self, "material_factory", None)
         if (factory is not None and len(key) == 3 and isinstance(key[0], type) and
-                issubclass(key[0], PyVolumetricMaterial) and key[1:] == (TetP1Basis, TetCentroidQuadrature)):
-            return factory(key[0])
+                issubclass(key[0], PyVolumetricMaterial) and key[1:] in _PY_ENERGY_BASES):
+            return factory(*key)
         try:
             return self._instances[key]
         except KeyError:
@@ -810,6 +811,7 @@ class VolumetricFemEnergyPyMaterialTetP1(Energy):
     the Hessian (vol B^T A B, Exact or per-element eigenvalue clamp) as for the native material."""
 
     material = None
+    _geometry_cls = VolumetricFemEnergyTetP1  # the native handle carrying the rest geometry
 
     def __init__(self, displacement_map, rest_position_fields, Fp, theta, batch_size=256):
         import torch
@@ -827,18 +829,23 @@ class VolumetricFemEnergyPyMaterialTetP1(Energy):
         fp = _sample_fields(Fp, T, 9, "Fp")
         fp = np.tile(np.eye(3).ravel(), (T, 1)) if fp is None else np.array(np.broadcast_to(fp, (T, 9)))
         # The geometry handle: the native records carry only rest geometry here.
-        self._geo = VolumetricFemEnergyTetP1(displacement_map, rest_position_fields, None, np.array([1.0, 1.0]),
-                                             batch_size)
+        self._geo = self._geometry_cls(displacement_map, rest_position_fields, None, np.array([1.0, 1.0]),
+                                       batch_size)
         self.map = displacement_map
         self.num_vertices, self.num_elements, self.num_dofs = (self._geo.num_vertices, self._geo.num_elements,
                                                                self._geo.num_dofs)
         self.nnzb, self.nnz = self._geo.nnzb, self._geo.nnz
         self.device = torch.device("cuda", self._geo.device)
+        # Material rows: one per element (tets) or per quadrature point (hexes, element-major);
+        # Fp and theta are per element, the same at each of its points.
+        per = getattr(self._geo, "points_per_axis", None)
+        self._points = 1 if per is None else per ** 3
+        self._rows = T * self._points
         # Fp column-major vec -> (T, 3, 3) matrices.
         self._Fp = torch.as_tensor(np.ascontiguousarray(fp, dtype=np.float64).reshape(T, 3, 3).transpose(0, 2, 1),
-                                   device=self.device).contiguous()
+                                   device=self.device).repeat_interleave(self._points, dim=0).contiguous()
         self._theta = torch.as_tensor(np.array(np.broadcast_to(th, (T, k)), dtype=np.float64),
-                                      device=self.device).contiguous()
+                                      device=self.device).repeat_interleave(self._points, dim=0).contiguous()
 
     @property
     def handle(self):
@@ -862,18 +869,19 @@ class VolumetricFemEnergyPyMaterialTetP1(Energy):
         return u
 
     def deformation_gradients(self, x):
-        """(T, 3, 3) CUDA tensor of F = I + grad u per element."""
+        """CUDA tensor of F = I + grad u: (T, 3, 3) per element for tets, (T n^3, 3, 3) per
+        quadrature point (element-major) for hexes."""
         import torch
 
         u = self._u(x)
-        F = torch.empty((self.num_elements, 3, 3), dtype=torch.float64, device=self.device)
+        F = torch.empty((self._rows, 3, 3), dtype=torch.float64, device=self.device)
         N.check(N.lib.lpg_fem_set_stream(self.handle, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
         N.check(N.lib.lpg_fem_deformation_gradients(self.handle, N.vptr(u), N.MEM_DEVICE, N.vptr(F)))
         return F
 
     def _material(self, F, outputs):
         out = self.material.eval(F, self._Fp, self._theta, outputs=outputs)
-        T = self.num_elements
+        T = self._rows
         shapes = {"W": (T,), "dW_dF": (T, 3, 3), "d2W_dF2": (T, 3, 3, 3, 3)}
         return [_cuda_f64(out[name], shapes[name], self.device) for name in outputs]
 
@@ -936,15 +944,36 @@ class VolumetricFemEnergyPyMaterialTetP1(Energy):
             return a.value
         F = self.deformation_gradients(x)
         dF = self.deformation_gradients(dx) - torch.eye(3, dtype=torch.float64, device=self.device)
-        bound = _cuda_f64(self.material.eval_feasible_step(F, self._Fp, self._theta, dF), (self.num_elements,),
+        bound = _cuda_f64(self.material.eval_feasible_step(F, self._Fp, self._theta, dF), (self._rows,),
                           self.device)
         if not bool(torch.all(torch.isfinite(bound))):
             raise ValueError("PyVolumetricMaterial.eval_feasible_step returned non-finite values")
         return float(torch.clamp(bound, 0.0, 1.0).min()) if self.num_elements else 1.0
 
 
-def _py_energy_class(material):
-    return type(f"VolumetricFemEnergy[{material.__name__}]", (VolumetricFemEnergyPyMaterialTetP1,),
+class VolumetricFemEnergyPyMaterialHexQ1(VolumetricFemEnergyPyMaterialTetP1):
+    """VolumetricFemEnergy[Material, HexQ1Basis, GaussLegendre3D[2]] for a PyVolumetricMaterial:
+    the library exports F at every quadrature point, the material evaluates W, dW/dF and
+    d2W/dF2 there (one row per point, element-major; theta and Fp per element, repeated over its
+    points), and the library integrates E = sum_q w_q W, g_a = sum_q w_q P grad N_a and
+    H = sum_q w_q B_q^T A_q B_q per hex and assembles them as the native hex energy (Exact, or
+    each element's 24x24 Hessian projected to PSD)."""
+
+    _geometry_cls = VolumetricFemEnergyHexQ1
+
+
+class VolumetricFemEnergyPyMaterialHexQ1GL4(VolumetricFemEnergyPyMaterialHexQ1):
+    _geometry_cls = VolumetricFemEnergyHexQ1GL4
+
+
+_PY_ENERGY_BASES = {(TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyPyMaterialTetP1,
+                    (HexQ1Basis, GaussLegendre3D_2): VolumetricFemEnergyPyMaterialHexQ1,
+                    (HexQ1Basis, GaussLegendre3D_4): VolumetricFemEnergyPyMaterialHexQ1GL4}
+
+
+def _py_energy_class(material, basis=TetP1Basis, quadrature=TetCentroidQuadrature):
+    base = _PY_ENERGY_BASES[(basis, quadrature)]
+    return type(f"VolumetricFemEnergy[{material.__name__}, {basis.__name__}, {quadrature.__name__}]", (base,),
                 {"material": material})
 
 
