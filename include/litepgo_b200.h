@@ -139,8 +139,9 @@ int lpg_fem_destroy(lpg_fem_t h);
  * 4. Every quadrature point must have det J > 0 (LPG_EINVAL otherwise, as
  * VolumetricElement3D). The handle answers lpg_fem_eval (Exact, and Projected: each element's
  * 24x24 Hessian projected to PSD), lpg_fem_feasible_step, lpg_fem_element_energies, the
- * patterns, lpg_newton_solve, lpg_fem_set_theta, lpg_fem_force_vjp_theta and lpg_adjoint_theta;
- * the rest-position, plastic-field, material and batch entry points are for tet meshes only
+ * patterns, lpg_newton_solve, lpg_fem_set_theta, lpg_fem_force_vjp_theta, lpg_adjoint_theta,
+ * lpg_fem_deformation_gradients and lpg_fem_eval_material (one material row per quadrature
+ * point); the rest-position, plastic-field and batch entry points are for tet meshes only
  * (LPG_EINVAL). No plastic field (Fp = I).
  */
 int lpg_fem_create_hex(int num_vertices, const double* X, int num_cells, const int32_t* cells, const double* theta,
@@ -390,6 +391,11 @@ int lpg_adjoint_fp(lpg_fem_t h, const double* u_star, const double* dLdu, const 
  *     lpg_fem_eval does (grad and hess in out_mem). Each element's A is symmetrised,
  *     (A + A^T) / 2, before use; non-finite material outputs give LPG_EDOMAIN. P may be NULL
  *     when grad is NULL, A when hessian is LPG_HESSIAN_NONE.
+ * On a hex handle (lpg_fem_create_hex with n points per axis) a material row is a quadrature
+ * point instead of an element: F, W, P and A have num_cells * n^3 rows, the points of an element
+ * consecutive in the quadrature order, and the sums run over the points with weight
+ * w_q = weight_q det J_q (E = sum w_q W, g_a = sum w_q P grad N_a, H = sum w_q B_q^T A_q B_q).
+ * LPG_HESSIAN_PROJECTED then projects each hex's 24x24 Hessian as lpg_fem_eval does.
  */
 int lpg_fem_deformation_gradients(lpg_fem_t h, const double* u, int io_mem, double* F);
 int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const double* A, int in_mem, double* energy,
