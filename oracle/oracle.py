@@ -394,6 +394,88 @@ def hex_force_vjp_theta(X, cells, theta, u, w, points_per_axis=2):
     return out
 
 
+# Tricubic Hermite hexes (hex_hermite_basis.hpp, cubic_hermite_basis.hpp): 64 functions, index
+# 8 * corner + slot, slot derivative orders below; per vertex 24 physical DOFs (slot-major, 3 per
+# slot: u, u_X, u_Y, u_Z, u_XY, u_XZ, u_YZ, u_XYZ), scaled to reference coefficients by
+# 1, hx, hy, hz, hx hy, hx hz, hy hz, hx hy hz on an axis-aligned box (basis_dof_transform.hpp:59-148).
+HERMITE_ORDERS = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0], [1, 0, 1], [0, 1, 1], [1, 1, 1]])
+
+
+def cubic_hermite(t):
+    """1D cubic Hermite values and t-derivatives ordered u(0), u'(0), u(1), u'(1)."""
+    t2, t3 = t * t, t * t * t
+    N = np.array([2 * t3 - 3 * t2 + 1, t3 - 2 * t2 + t, -2 * t3 + 3 * t2, t3 - t2])
+    dN = np.array([6 * t2 - 6 * t, 3 * t2 - 4 * t + 1, -6 * t2 + 6 * t, 3 * t2 - 2 * t])
+    return N, dN
+
+
+def hex_hermite_N_dN(xi):
+    """(64,) values and (64, 3) reference gradients of the tricubic Hermite functions at xi."""
+    (x, dx), (y, dy), (z, dz) = (cubic_hermite(c) for c in xi)
+    N, dN = np.empty(64), np.empty((64, 3))
+    for row in range(64):
+        corner, order = HEX_CORNERS[row // 8], HERMITE_ORDERS[row % 8]
+        i, j, k = 2 * corner + order
+        N[row] = x[i] * y[j] * z[k]
+        dN[row] = [dx[i] * y[j] * z[k], x[i] * dy[j] * z[k], x[i] * y[j] * dz[k]]
+    return N, dN
+
+
+def hermite_box(Xc):
+    """Edge lengths of an axis-aligned box in corner order (the reference's check: positive lengths,
+    normalized corners equal to the unit corners within 1e-12); ValueError otherwise."""
+    origin = Xc[0]
+    h = np.array([Xc[1, 0] - origin[0], Xc[3, 1] - origin[1], Xc[4, 2] - origin[2]])
+    if not np.all(np.isfinite(h)) or np.any(h <= 0):
+        raise ValueError("Hermite DOF transform requires positive axis-aligned box dimensions")
+    if np.abs((Xc - origin) / h - HEX_CORNERS).max() > 1e-12:
+        raise ValueError("Hermite DOF transform requires axis-aligned boxes in Hex corner order")
+    return h
+
+
+def hermite_slot_scales(h):
+    return np.array([1, h[0], h[1], h[2], h[0] * h[1], h[0] * h[2], h[1] * h[2], h[0] * h[1] * h[2]])
+
+
+def hex_hermite_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
+    """E, gradient and dense Hessian (or None) over the physical DOFs (24 per vertex) of the
+    tricubic Hermite neo-Hookean energy on axis-aligned box hexes (Fp = I): reference coefficients
+    c = s * d, F = I + sum_b c_b (J^-T dN_b), J = diag(h), and the element gradient and Hessian
+    pulled back by the same scales (s g, S H S)."""
+    X = np.asarray(X, float).reshape(-1, 3)
+    cells = np.asarray(cells).reshape(-1, 8)
+    D = np.asarray(u, float).reshape(-1, 24)
+    T, n = cells.shape[0], D.size
+    th = np.broadcast_to(np.asarray(theta, float), (T, 2))
+    pts, wts = hex_points(points_per_axis)
+    tables = [hex_hermite_N_dN(xi)[1] for xi in pts]
+    E, g = 0.0, np.zeros(n)
+    H = np.zeros((n, n)) if hessian else None
+    for e, cell in enumerate(cells):
+        h = hermite_box(X[cell])
+        s = np.repeat(np.tile(hermite_slot_scales(h), 8), 3)  # per local DOF, 192
+        dofs = (24 * cell[:, None] + np.arange(24)).ravel()
+        C = (D[cell].ravel() * s).reshape(64, 3)
+        ge, He = np.zeros(192), np.zeros((192, 192))
+        for dN, wq in zip(tables, wts):
+            gN = dN / h  # rows grad_X N_b (J^-T = diag(1 / h))
+            F = np.eye(3) + C.T @ gN
+            w = wq * np.prod(h)
+            E += w * nh_W(F, np.eye(3), th[e])
+            B = np.zeros((9, 192))  # column-major vec(F): r = i + 3 j
+            for b in range(64):
+                for i in range(3):
+                    for j in range(3):
+                        B[i + 3 * j, 3 * b + i] = gN[b, j]
+            ge += w * B.T @ nh_dW_dF(F, np.eye(3), th[e]).T.ravel()
+            if hessian:
+                He += w * B.T @ nh_d2W_dF2(F, np.eye(3), th[e]) @ B
+        g[dofs] += s * ge
+        if hessian:
+            H[np.ix_(dofs, dofs)] += s[:, None] * He * s[None, :]
+    return E, g, H
+
+
 def hex_box(nx, ny=None, nz=None):
     """Structured box of nx*ny*nz unit-spacing-scaled hexes on [0,1]^3 (corner order above)."""
     ny = nx if ny is None else ny
