@@ -147,6 +147,23 @@ int lpg_fem_destroy(lpg_fem_t h);
 int lpg_fem_create_hex(int num_vertices, const double* X, int num_cells, const int32_t* cells, const double* theta,
                        int theta_per_element, int points_per_axis, int device, lpg_fem_t* out);
 
+/*
+ * Tricubic Hermite hex mesh: VolumetricFemEnergy<NeoHookean, HexHermiteBasis, GaussLegendre3D<n>>
+ * with BasisDofTransform<HexHermiteBasis> (fem/basis/3d/hex_hermite_basis.hpp,
+ * fem/assembly/basis_dof_transform.hpp:59-148). Arguments as lpg_fem_create_hex; every cell must
+ * be a positive axis-aligned box in corner order (LPG_EINVAL otherwise). The unknowns are 24
+ * physical DOFs per vertex (num_dofs = 24 num_vertices): slots u, u_X, u_Y, u_Z, u_XY, u_XZ,
+ * u_YZ, u_XYZ of 3 components each, DOF 24 v + 3 slot + c. Block patterns and Hessians are over
+ * 3x3 blocks of (vertex, slot) rows, 8 per vertex (lpg_fem_sizes reports 8 num_vertices block
+ * rows). The handle answers lpg_fem_eval (Exact Hessian; Projected is LPG_EINVAL),
+ * lpg_fem_feasible_step, lpg_fem_element_energies, lpg_fem_set_theta, the patterns and
+ * lpg_newton_solve with the Exact Hessian; the sensitivity, material and batch entry points are
+ * LPG_EINVAL. No plastic field (Fp = I).
+ */
+int lpg_fem_create_hex_hermite(int num_vertices, const double* X, int num_cells, const int32_t* cells,
+                               const double* theta, int theta_per_element, int points_per_axis, int device,
+                               lpg_fem_t* out);
+
 /* Uses `stream` (a cudaStream_t) for all later work of this handle; NULL = the handle's own stream. */
 int lpg_fem_set_stream(lpg_fem_t h, void* stream);
 

@@ -102,6 +102,7 @@ SIGNATURES = [
     ("lpg_fem_autotune", _int, [_vp]),
     ("lpg_mesh_cluster_summary_cells", _int, [_int, _int, _ip, _int, _i64p]),
     ("lpg_fem_create_hex", _int, [_int, _dp, _int, _ip, _dp, _int, _int, _int, ctypes.POINTER(_vp)]),
+    ("lpg_fem_create_hex_hermite", _int, [_int, _dp, _int, _ip, _dp, _int, _int, _int, ctypes.POINTER(_vp)]),
     ("lpg_fem_deformation_gradients", _int, [_vp, _vp, _int, _vp]),
     ("lpg_fem_eval_material", _int, [_vp, _vp, _vp, _vp, _int, _dp, _vp, _int, _int, _int, _vp, _int]),
     ("lpg_fem_set_fp", _int, [_vp, _dp, _int]),

@@ -102,6 +102,31 @@ void upload_plan(lpg_fem& hh, int V, int T) {
 }
 
 // Entry points whose kernels exist for tet meshes only.
+// Gauss-Legendre points and weights on [0, 1] for 2 or 4 points (gauss_legendre_3d.hpp).
+void gauss_legendre_01(int n, double* t1, double* w1) {
+    if (n == 2) {
+        t1[0] = 0.5 - 0.5 / std::sqrt(3.0);
+        t1[1] = 0.5 + 0.5 / std::sqrt(3.0);
+        w1[0] = w1[1] = 0.5;
+    } else {
+        const double outer = std::sqrt((3 + 2 * std::sqrt(6.0 / 5)) / 7), inner = std::sqrt((3 - 2 * std::sqrt(6.0 / 5)) / 7);
+        t1[0] = 0.5 * (1 - outer);
+        t1[1] = 0.5 * (1 - inner);
+        t1[2] = 0.5 * (1 + inner);
+        t1[3] = 0.5 * (1 + outer);
+        w1[0] = w1[3] = (18 - std::sqrt(30.0)) / 72;
+        w1[1] = w1[2] = (18 + std::sqrt(30.0)) / 72;
+    }
+}
+
+// HexQ1Basis / HexHermiteBasis corner order on [0,1]^3.
+constexpr int kHexCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+
+// Entry points whose kernels do not exist for tricubic Hermite hexes.
+void not_hermite(const lpg_fem& h, const char* what) {
+    if (h.dm.K == 64) fail(LPG_EINVAL, std::string(what) + " is not available for Hermite hex meshes");
+}
+
 void tet_only(const lpg_fem& h, const char* what) {
     if (h.dm.K != 4) fail(LPG_EINVAL, std::string(what) + " is available for tet meshes only");
 }
@@ -194,6 +219,15 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.ev_end = ev_end;
     const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
     a.cl_variant = tune.cl[pi];
+    if (dm.K == 64) {
+        if (a.hess && hessian == LPG_HESSIAN_PROJECTED)
+            fail(LPG_EINVAL, "the projected Hessian is not available for Hermite hex meshes");
+        const size_t T = static_cast<size_t>(dm.T);
+        double* elemE = delem ? delem : d_mat[3].as<double>(std::max<size_t>(T, 1));
+        void* blocks = a.hess ? d_proj.ensure(T * kHermiteRecord * (precision == LPG_PRECISION_F64 ? 8 : 4)) : nullptr;
+        launch_hermite_eval(dm, precision, du, elemE, d_vjp.as<double>(std::max<size_t>(192 * T, 1)), blocks, a, stream);
+        return;
+    }
     if (dm.K == 8) {
         const bool projected = hessian == LPG_HESSIAN_PROJECTED;
         const size_t T = static_cast<size_t>(dm.T);
@@ -355,6 +389,100 @@ int lpg_fem_create(int V, const double* X, int T, const int32_t* tets, const dou
     });
 }
 
+int lpg_fem_create_hex_hermite(int V, const double* X, int T, const int32_t* cells, const double* theta,
+                               int theta_per_element, int points_per_axis, int device, lpg_fem_t* out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!out) fail(LPG_EINVAL, "lpg_fem_create_hex_hermite: null output handle");
+        if (T > 0 && (!cells || !theta || !X)) fail(LPG_EINVAL, "lpg_fem_create_hex_hermite: null input array");
+        if (points_per_axis != 2 && points_per_axis != 4)
+            fail(LPG_EINVAL, "GaussLegendre3D is instantiated for 2 or 4 points per axis");
+        if (V < 0 || T < 0 || V > std::numeric_limits<int>::max() / 24)
+            fail(LPG_EINVAL, "VertexDofMap requires total DOFs fitting in int");
+        for (size_t k = 0; k < 8 * static_cast<size_t>(T); ++k)
+            if (cells[k] < 0 || cells[k] >= V)
+                fail(LPG_EINVAL, "MeshTopology cell " + std::to_string(k / 8) + " has vertex indices outside [0, num_vertices)");
+        auto h = std::make_unique<lpg_fem>();
+        h->device = device;
+        LPG_CUDA(cudaSetDevice(device));
+        LPG_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+        // Plan rows: node 8 v + slot (3 DOFs each, so DOF 24 v + 3 slot + c); cell nodes in basis
+        // order 8 corner + slot.
+        std::vector<int32_t> nodes(64 * static_cast<size_t>(T));
+        for (size_t e = 0; e < static_cast<size_t>(T); ++e)
+            for (int b = 0; b < 64; ++b) nodes[64 * e + b] = 8 * cells[8 * e + b / 8] + b % 8;
+        build_plan(8 * V, T, nodes.data(), h->plan, 64);
+        // BasisDofTransform<HexHermiteBasis> (basis_dof_transform.hpp:59-92): every element a
+        // positive axis-aligned box in corner order; its edge lengths scale the DOF slots.
+        std::vector<double> hb(3 * static_cast<size_t>(T));
+        for (size_t e = 0; e < static_cast<size_t>(T); ++e) {
+            const double* o = X + 3 * static_cast<size_t>(cells[8 * e]);
+            const double len[3] = {X[3 * static_cast<size_t>(cells[8 * e + 1])] - o[0],
+                                   X[3 * static_cast<size_t>(cells[8 * e + 3]) + 1] - o[1],
+                                   X[3 * static_cast<size_t>(cells[8 * e + 4]) + 2] - o[2]};
+            for (int d = 0; d < 3; ++d)
+                if (!std::isfinite(len[d]) || !(len[d] > 0))
+                    fail(LPG_EINVAL, "Hermite DOF transform requires positive axis-aligned box dimensions");
+            for (int c = 0; c < 8; ++c)
+                for (int d = 0; d < 3; ++d) {
+                    const double r = (X[3 * static_cast<size_t>(cells[8 * e + c]) + d] - o[d]) / len[d];
+                    if (!std::isfinite(r) || std::fabs(r - kHexCorner[c][d]) > 1e-12)
+                        fail(LPG_EINVAL, "Hermite DOF transform requires axis-aligned boxes in Hex corner order");
+                }
+            for (int d = 0; d < 3; ++d) hb[3 * e + d] = len[d];
+        }
+        // Per point the tricubic Hermite reference derivatives (hex_hermite_basis.hpp: function
+        // 8 corner + slot is the product of 1D cubic Hermite factors 2 corner_d + order_d, ordered
+        // u(0), u'(0), u(1), u'(1), cubic_hermite_basis.hpp) and the weight.
+        static const int order[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                        {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+        const int n = points_per_axis, nq = n * n * n;
+        double t1[4], w1[4];
+        gauss_legendre_01(n, t1, w1);
+        std::vector<double> qt(193 * static_cast<size_t>(nq));
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                for (int k = 0; k < n; ++k) {
+                    const int q = (i * n + j) * n + k;
+                    const double xi[3] = {t1[i], t1[j], t1[k]};
+                    double f[3][4], df[3][4];
+                    for (int d = 0; d < 3; ++d) {
+                        const double t = xi[d], t2 = t * t, t3 = t2 * t;
+                        const double fv[4] = {2 * t3 - 3 * t2 + 1, t3 - 2 * t2 + t, -2 * t3 + 3 * t2, t3 - t2};
+                        const double dv[4] = {6 * t2 - 6 * t, 3 * t2 - 4 * t + 1, -6 * t2 + 6 * t, 3 * t2 - 2 * t};
+                        for (int r = 0; r < 4; ++r) {
+                            f[d][r] = fv[r];
+                            df[d][r] = dv[r];
+                        }
+                    }
+                    for (int b = 0; b < 64; ++b) {
+                        int ix[3];
+                        for (int d = 0; d < 3; ++d) ix[d] = 2 * kHexCorner[b / 8][d] + order[b % 8][d];
+                        qt[193 * q + 3 * b] = df[0][ix[0]] * f[1][ix[1]] * f[2][ix[2]];
+                        qt[193 * q + 3 * b + 1] = f[0][ix[0]] * df[1][ix[1]] * f[2][ix[2]];
+                        qt[193 * q + 3 * b + 2] = f[0][ix[0]] * f[1][ix[1]] * df[2][ix[2]];
+                    }
+                    qt[193 * q + 192] = w1[i] * w1[j] * w1[k];
+                }
+        std::vector<double> th(2 * static_cast<size_t>(T));
+        for (int e = 0; e < T; ++e)
+            for (int c = 0; c < 2; ++c) th[2 * static_cast<size_t>(e) + c] = theta_per_element ? theta[2 * static_cast<size_t>(e) + c] : theta[c];
+        upload_plan(*h, 8 * V, T);
+        DevMesh& m = h->dm;
+        m.K = 64;
+        m.nq = nq;
+        m.hex_X = upload(h->b_hex[0], std::vector<double>(X, X + 3 * static_cast<size_t>(V)));
+        m.hex_cells = upload(h->b_hex[1], std::vector<int32_t>(cells, cells + 8 * static_cast<size_t>(T)));
+        m.hex_theta = upload(h->b_hex[2], th);
+        m.herm_q = upload(h->b_hex[3], qt);
+        m.herm_h = upload(h->b_herm, hb);
+        LPG_CUDA(cudaMemset(h->d_status.as<unsigned>(1), 0, sizeof(unsigned)));
+        LPG_CUDA(cudaDeviceSynchronize());
+        *out = h.release();
+    });
+}
+
 int lpg_fem_create_hex(int V, const double* X, int T, const int32_t* cells, const double* theta,
                        int theta_per_element, int points_per_axis, int device, lpg_fem_t* out) {
     if (out) *out = nullptr;
@@ -373,21 +501,7 @@ int lpg_fem_create_hex(int V, const double* X, int T, const int32_t* cells, cons
         // trilinear basis derivatives at each (hex_q1_basis.hpp corner order).
         const int n = points_per_axis, nq = n * n * n;
         double t1[4], w1[4];
-        if (n == 2) {
-            t1[0] = 0.5 - 0.5 / std::sqrt(3.0);
-            t1[1] = 0.5 + 0.5 / std::sqrt(3.0);
-            w1[0] = w1[1] = 0.5;
-        } else {
-            const double outer = std::sqrt((3 + 2 * std::sqrt(6.0 / 5)) / 7), inner = std::sqrt((3 - 2 * std::sqrt(6.0 / 5)) / 7);
-            t1[0] = 0.5 * (1 - outer);
-            t1[1] = 0.5 * (1 - inner);
-            t1[2] = 0.5 * (1 + inner);
-            t1[3] = 0.5 * (1 + outer);
-            w1[0] = w1[3] = (18 - std::sqrt(30.0)) / 72;
-            w1[1] = w1[2] = (18 + std::sqrt(30.0)) / 72;
-        }
-        static const int corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
-                                         {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+        gauss_legendre_01(n, t1, w1);
         std::vector<double> qt(25 * static_cast<size_t>(nq));
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j)
@@ -397,8 +511,8 @@ int lpg_fem_create_hex(int V, const double* X, int T, const int32_t* cells, cons
                     for (int a = 0; a < 8; ++a) {
                         double f[3], df[3];
                         for (int d = 0; d < 3; ++d) {
-                            f[d] = corner[a][d] ? xi[d] : 1 - xi[d];
-                            df[d] = corner[a][d] ? 1.0 : -1.0;
+                            f[d] = kHexCorner[a][d] ? xi[d] : 1 - xi[d];
+                            df[d] = kHexCorner[a][d] ? 1.0 : -1.0;
                         }
                         qt[25 * q + 3 * a] = df[0] * f[1] * f[2];
                         qt[25 * q + 3 * a + 1] = f[0] * df[1] * f[2];
@@ -539,6 +653,7 @@ int lpg_fem_eval(lpg_fem_t h, const double* u, int io_mem, double* energy, doubl
 int lpg_fem_deformation_gradients(lpg_fem_t h, const double* u, int io_mem, double* F) {
     return guarded([&] {
         if (!h || !F) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: null argument");
+        not_hermite(*h, "lpg_fem_deformation_gradients");
         if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_deformation_gradients: the handle has a plastic field");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
@@ -561,6 +676,7 @@ int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const d
                           double* grad, int hessian, int precision, int layout, void* hess, int out_mem) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
+        not_hermite(*h, "lpg_fem_eval_material");
         if (h->dm.fpinv64) fail(LPG_EINVAL, "lpg_fem_eval_material: the handle has a plastic field");
         const bool hex = h->dm.K == 8;
         // Material rows: one per element (tets) or per quadrature point (hexes).
@@ -694,6 +810,7 @@ int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io
 int lpg_fem_force_vjp_theta(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
+        not_hermite(*h, "lpg_fem_force_vjp_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         const size_t n = 3 * static_cast<size_t>(h->dm.V);
@@ -917,7 +1034,7 @@ int lpg_fem_set_theta(lpg_fem_t h, const double* theta, int theta_per_element) {
         for (size_t k = 0; k < n && h->dm.T > 0; ++k)
             if (!std::isfinite(theta[k])) fail(LPG_EINVAL, "VolumetricFemEnergy: theta must be finite");
         if (h->dm.T == 0) return;
-        if (h->dm.K == 8) { // hexes keep theta per element, read at every evaluation
+        if (h->dm.K != 4) { // hexes keep theta per element, read at every evaluation
             const size_t T = static_cast<size_t>(h->dm.T);
             std::vector<double> th(2 * T);
             for (size_t e = 0; e < T; ++e)
@@ -986,6 +1103,7 @@ int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, con
                       double* lambda_out) {
     return guarded([&] {
         if (!h || !u_star || !dLdu || !dtheta) fail(LPG_EINVAL, "lpg_adjoint_theta: null argument");
+        not_hermite(*h, "lpg_adjoint_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         adjoint_theta(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, per_element, dtheta,

@@ -1372,6 +1372,19 @@ template <> struct CellBlocks<8> {
         return lo * 8 - (lo * (lo - 1)) / 2 + (hi - lo);
     }
 };
+template <> struct CellBlocks<64> {
+    static constexpr int shift = 6, record = kHermiteRecord;
+    static __device__ __forceinline__ int pair(int a, int b) {
+        const int lo = min(a, b), hi = max(a, b);
+        return lo * 64 - (lo * (lo - 1)) / 2 + (hi - lo);
+    }
+};
+
+// Contributor word c of a list: one 16-bit word, or two (low half first) for 64-node cells.
+template <int K> __device__ __forceinline__ uint32_t contributor(const uint16_t* en, int c) {
+    if (K == 64) return static_cast<uint32_t>(en[2 * c]) | (static_cast<uint32_t>(en[2 * c + 1]) << 16);
+    return en[c];
+}
 
 template <typename R, int K = 4>
 __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh m, const EvalArgs a) {
@@ -1419,8 +1432,8 @@ __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh 
             const int cnt = static_cast<int>(de >> 20);
             R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             for (int c = 0; c < cnt; ++c) {
-                const int w = en[c];
-                const int el = w >> (2 * CB::shift), la = (w >> CB::shift) & (K - 1), lb = w & (K - 1);
+                const uint32_t w = contributor<K>(en, c);
+                const int el = static_cast<int>(w >> (2 * CB::shift)), la = (w >> CB::shift) & (K - 1), lb = w & (K - 1);
                 const R* blk = blocks + CB::record * static_cast<size_t>(sel[el]) + 9 * CB::pair(la, lb);
                 R bv[9];
 #pragma unroll
@@ -1557,8 +1570,9 @@ __global__ void __launch_bounds__(128) vertex_gather_kernel(const DevMesh m, con
             const uint16_t* en = ents + (de & 0xfffffu);
             double acc[3] = {0, 0, 0};
             for (int c = 0; c < static_cast<int>(de >> 20); ++c) {
-                const int wd = __ldg(en + c);
-                constexpr int sh = K == 4 ? 2 : 3;
+                const uint32_t wd = K == 64 ? static_cast<uint32_t>(__ldg(en + 2 * c)) | (static_cast<uint32_t>(__ldg(en + 2 * c + 1)) << 16)
+                                            : __ldg(en + c);
+                constexpr int sh = cell_bits(K);
                 const size_t e = __ldg(m.cl_els + e0 + (wd >> (2 * sh))) & 0x7fffffffu;
                 const int a = (wd >> sh) & (K - 1);
 #pragma unroll
@@ -2293,6 +2307,248 @@ __global__ void __launch_bounds__(256) hex_feasible_kernel(const DevMesh m, cons
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tricubic Hermite hexes (VolumetricFemEnergy<NeoHookean, HexHermiteBasis, GaussLegendre3D<n>>,
+// hex_hermite_basis.hpp, with the physical DOFs of BasisDofTransform<HexHermiteBasis>,
+// basis_dof_transform.hpp:59-148). Elements are axis-aligned boxes of edge lengths h; a vertex
+// carries 24 physical DOFs, slots u, u_X, u_Y, u_Z, u_XY, u_XZ, u_YZ, u_XYZ of 3 components, and
+// node b = 8 corner + slot of an element is the plan's row 8 v + slot. With the slot scale s_b
+// (1, hx, hy, hz, hx hy, hx hz, hy hz, hx hy hz) and G_b = s_b (dN_b / dxi) / h at a point,
+// F = I + sum_b d_b G_b^T on the physical DOFs d, so the element's gradient and Hessian come out
+// pulled back to physical DOFs (s g, S H S) as in the reference, with w = weight hx hy hz and
+//   g_b = sum_q w P G_b,   H_ab = sum_q w [mu (G_a . G_b) I + lambda h_a h_b^T - p h_b h_a^T], h = F^-T G.
+// The point table holds, per point, the 64 x 3 reference derivatives and the weight (193 values).
+// ---------------------------------------------------------------------------
+constexpr int kHermiteTable = 193;
+
+__device__ __forceinline__ double hermite_slot_scale(int slot, double hx, double hy, double hz) {
+    switch (slot) {
+    case 0: return 1.0;
+    case 1: return hx;
+    case 2: return hy;
+    case 3: return hz;
+    case 4: return hx * hy;
+    case 5: return hx * hz;
+    case 6: return hy * hz;
+    default: return hx * hy * hz;
+    }
+}
+
+// G_b at a point (tq: the point's table row).
+__device__ __forceinline__ void hermite_G(const double* tq, int b, const double (&h)[3], double (&G)[3]) {
+    const double sb = hermite_slot_scale(b & 7, h[0], h[1], h[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) G[d] = sb * __ldg(tq + 3 * b + d) / h[d];
+}
+
+__device__ __forceinline__ void hermite_pair(int pr, int& a, int& b) {
+    a = 0;
+    int base = 0;
+    while (pr >= base + (64 - a)) {
+        base += 64 - a;
+        ++a;
+    }
+    b = a + (pr - base);
+}
+
+// One CTA per element: the element's 192 DOFs and each point's w, p, F^-T and P in shared
+// memory (points by thread), then the energy (thread 0, points in order), the gradient (a thread
+// per node) and the 2080 blocks H_ab, a <= b (strided over the CTA; diagonal blocks mirrored so
+// the matrix is bitwise symmetric).
+constexpr int kHermiteThreads = 128;
+
+template <typename R>
+__global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const DevMesh m, const double* __restrict__ u,
+                                                                          double* __restrict__ elemE,
+                                                                          double* __restrict__ per_elem,
+                                                                          R* __restrict__ blocks, unsigned* status) {
+    __shared__ double sD[192];
+    __shared__ double sK[64 * 20]; // per point: w, p, F^-T (9), P (9)
+    __shared__ double sE[64];
+    __shared__ int sOk[64];
+    const int e = blockIdx.x, tid = threadIdx.x;
+    unsigned st = 0;
+    const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+    const double lam = m.hex_theta[2 * static_cast<size_t>(e)], mu = m.hex_theta[2 * static_cast<size_t>(e) + 1];
+    if (!(lam >= 0 && mu > 0 && isfinite(lam) && isfinite(mu))) st |= ST_BAD_THETA;
+    const double h[3] = {m.herm_h[3 * static_cast<size_t>(e)], m.herm_h[3 * static_cast<size_t>(e) + 1],
+                         m.herm_h[3 * static_cast<size_t>(e) + 2]};
+    for (int t = tid; t < 192; t += blockDim.x) {
+        const double d = __ldg(u + 24 * static_cast<size_t>(__ldg(cell + t / 24)) + t % 24);
+        if (!isfinite(d)) st |= ST_BAD_INPUT;
+        sD[t] = d;
+    }
+    __syncthreads();
+    for (int q = tid; q < m.nq; q += blockDim.x) {
+        const double* tq = m.herm_q + kHermiteTable * static_cast<size_t>(q);
+        double Gu[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < 64; ++b) {
+            double G[3];
+            hermite_G(tq, b, h, G);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Gu[3 * i + d] = fma(sD[3 * b + i], G[d], Gu[3 * i + d]);
+        }
+        double F[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F[k] = Gu[k] + (k % 4 == 0 ? 1.0 : 0.0);
+        double C[9];
+        C[0] = F[4] * F[8] - F[5] * F[7];
+        C[1] = F[5] * F[6] - F[3] * F[8];
+        C[2] = F[3] * F[7] - F[4] * F[6];
+        C[3] = F[2] * F[7] - F[1] * F[8];
+        C[4] = F[0] * F[8] - F[2] * F[6];
+        C[5] = F[1] * F[6] - F[0] * F[7];
+        C[6] = F[1] * F[5] - F[2] * F[4];
+        C[7] = F[2] * F[3] - F[0] * F[5];
+        C[8] = F[0] * F[4] - F[1] * F[3];
+        const double detF = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+        double* k = sK + 20 * q;
+        if (!(detF > 0) || !isfinite(detF)) {
+            st |= isfinite(detF) ? ST_BAD_DET : ST_NONFINITE_F;
+            sOk[q] = 0;
+            sE[q] = 0;
+            continue;
+        }
+        sOk[q] = 1;
+        const double L = log(detF), p = lam * L - mu, w = __ldg(tq + 192) * h[0] * h[1] * h[2];
+        k[0] = w;
+        k[1] = p;
+        double ff = 0;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const double fit = C[t] / detF;
+            k[2 + t] = fit;
+            k[11 + t] = mu * F[t] + p * fit;
+            ff += F[t] * F[t];
+        }
+        sE[q] = w * (0.5 * mu * (ff - 3.0) - mu * L + 0.5 * lam * L * L);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double E = 0;
+        for (int q = 0; q < m.nq; ++q) E += sE[q];
+        if (!isfinite(E)) st |= ST_NONFINITE_OUT;
+        elemE[e] = E;
+    }
+    if (per_elem) {
+        for (int b = tid; b < 64; b += blockDim.x) {
+            double ga[3] = {0, 0, 0};
+            for (int q = 0; q < m.nq; ++q) {
+                if (!sOk[q]) continue;
+                double G[3];
+                hermite_G(m.herm_q + kHermiteTable * static_cast<size_t>(q), b, h, G);
+                const double* k = sK + 20 * q;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    ga[i] = fma(k[0], k[11 + 3 * i] * G[0] + k[12 + 3 * i] * G[1] + k[13 + 3 * i] * G[2], ga[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (!isfinite(ga[i])) st |= ST_NONFINITE_OUT;
+                per_elem[192 * static_cast<size_t>(e) + 3 * b + i] = ga[i];
+            }
+        }
+    }
+    if (blocks) {
+        for (int pr = tid; pr < 2080; pr += blockDim.x) {
+            int a, b;
+            hermite_pair(pr, a, b);
+            double Hb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int q = 0; q < m.nq; ++q) {
+                if (!sOk[q]) continue;
+                const double* tq = m.herm_q + kHermiteTable * static_cast<size_t>(q);
+                double Ga[3], Gb[3];
+                hermite_G(tq, a, h, Ga);
+                hermite_G(tq, b, h, Gb);
+                const double* k = sK + 20 * q;
+                const double w = k[0], p = k[1];
+                double ha[3], hb[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    ha[i] = k[2 + 3 * i] * Ga[0] + k[3 + 3 * i] * Ga[1] + k[4 + 3 * i] * Ga[2];
+                    hb[i] = k[2 + 3 * i] * Gb[0] + k[3 + 3 * i] * Gb[1] + k[4 + 3 * i] * Gb[2];
+                }
+                const double dn = Ga[0] * Gb[0] + Ga[1] * Gb[1] + Ga[2] * Gb[2];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        double v = lam * ha[i] * hb[c] - p * hb[i] * ha[c];
+                        if (i == c) v += mu * dn;
+                        Hb[3 * i + c] = fma(w, v, Hb[3 * i + c]);
+                    }
+            }
+            if (a == b) {
+                Hb[3] = Hb[1];
+                Hb[6] = Hb[2];
+                Hb[7] = Hb[5];
+            }
+            R* o = blocks + kHermiteRecord * static_cast<size_t>(e) + 9 * pr;
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                if (!isfinite(Hb[t])) st |= ST_NONFINITE_OUT;
+                o[t] = static_cast<R>(Hb[t]);
+            }
+        }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((tid & 31) == 0 && st) atomicOr(status, st);
+}
+
+// Feasible step of a Hermite hex mesh: F and dF at every point, the positive-determinant step,
+// minimum per block (as hex_feasible_kernel).
+__global__ void __launch_bounds__(256) hermite_feasible_kernel(const DevMesh m, const double* __restrict__ u,
+                                                               const double* __restrict__ du, double* block_min,
+                                                               unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double alpha = 1.0;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        const double h[3] = {m.herm_h[3 * static_cast<size_t>(e)], m.herm_h[3 * static_cast<size_t>(e) + 1],
+                             m.herm_h[3 * static_cast<size_t>(e) + 2]};
+        for (int q = 0; q < m.nq && st == 0; ++q) {
+            const double* tq = m.herm_q + kHermiteTable * static_cast<size_t>(q);
+            double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, dF[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            bool ok = true;
+            for (int b = 0; b < 64; ++b) {
+                double G[3];
+                hermite_G(tq, b, h, G);
+                const size_t base = 24 * static_cast<size_t>(__ldg(cell + (b >> 3))) + 3 * (b & 7);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double uu = u[base + i], dd = du[base + i];
+                    ok = ok && isfinite(uu) && isfinite(dd);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        F[3 * i + d] = fma(uu, G[d], F[3 * i + d]);
+                        dF[3 * i + d] = fma(dd, G[d], dF[3 * i + d]);
+                    }
+                }
+            }
+            if (!ok) {
+                st |= ST_BAD_INPUT;
+                break;
+            }
+            alpha = fmin(alpha, positive_det_step(F, dF, st));
+        }
+    }
+    __shared__ double sm[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) alpha = fmin(alpha, __shfl_xor_sync(0xffffffffu, alpha, off));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = alpha;
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = sm[0];
+        for (int w = 1; w < (blockDim.x >> 5); ++w) v = fmin(v, sm[w]);
+        block_min[blockIdx.x] = v;
+    }
+}
+
 // Lame parameters of every element record (FP64 and FP32 copies).
 __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __restrict__ theta, int per_element, int T) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2456,9 +2712,15 @@ int feasible_blocks(const DevMesh& m) { return (m.T + 255) / 256; }
 
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
                      double* alpha, unsigned* status, cudaStream_t s, double* per_elem) {
+    if (m.K != 4 && per_elem) fail(LPG_EINVAL, "per-element feasible steps are available for tet meshes only");
     if (m.K == 8) {
-        if (per_elem) fail(LPG_EINVAL, "per-element feasible steps are available for tet meshes only");
         launch_hex_feasible(m, u, du, block_min, nblocks, alpha, status, s);
+        return;
+    }
+    if (m.K == 64) {
+        if (nblocks > 0) hermite_feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status);
+        min_kernel<<<1, 1024, 0, s>>>(block_min, nblocks, alpha);
+        LPG_CUDA(cudaGetLastError());
         return;
     }
     if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status, per_elem);
@@ -2575,6 +2837,35 @@ void launch_hex_material_eval(const DevMesh& m, int precision, int hessian, cons
             else
                 launch_block_gather<float, 8>(m, ga, s);
         }
+    }
+    if (a.grad && m.num_unused > 0)
+        zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
+    sum_partial_kernel<<<kSumBlocks, 256, 0, s>>>(elemE, m.T, a.cluster_energy);
+    sum_final_kernel<<<1, 256, 0, s>>>(a.cluster_energy, kSumBlocks, a.energy);
+    LPG_CUDA(cudaGetLastError());
+}
+
+void launch_hermite_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem,
+                         void* blocks, const EvalArgs& a, cudaStream_t s) {
+    if (m.T > 0) {
+        if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
+        double* per_grad = a.grad ? per_elem : nullptr;
+        if (precision == LPG_PRECISION_F64 || !a.hess)
+            hermite_element_kernel<double><<<m.T, kHermiteThreads, 0, s>>>(
+                m, u, elemE, per_grad, a.hess ? static_cast<double*>(blocks) : nullptr, a.status);
+        else
+            hermite_element_kernel<float><<<m.T, kHermiteThreads, 0, s>>>(m, u, elemE, per_grad,
+                                                                          static_cast<float*>(blocks), a.status);
+        if (a.grad) vertex_gather_kernel<64><<<std::min(m.ncl, 148 * 8), 128, 0, s>>>(m, per_elem, 1.0, a.grad);
+        if (a.hess) {
+            EvalArgs ga = a;
+            ga.proj = blocks;
+            if (precision == LPG_PRECISION_F64)
+                launch_block_gather<double, 64>(m, ga, s);
+            else
+                launch_block_gather<float, 64>(m, ga, s);
+        }
+        if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
     }
     if (a.grad && m.num_unused > 0)
         zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);

@@ -87,6 +87,13 @@ constexpr int kSellWindow = 128;
 #endif
 constexpr int kClusterRows = LPG_CLUSTER_ROWS;
 constexpr int kClusterElems = LPG_CLUSTER_ELEMS;
+// Clusters of 64-node cells (Hermite hexes: 8 slot rows per vertex, ~216 blocks per row) hold at
+// most one vertex's rows, so a cluster's slot and contributor tables fit in shared memory.
+constexpr int kClusterRowsWide = 8;
+// Bits of a node index inside a contributor word (2, 3 or 6), and the bit where the plan's
+// incidence words keep a node's local index above its element id.
+constexpr int cell_bits(int K) { return K == 4 ? 2 : K == 8 ? 3 : 6; }
+constexpr int inc_shift(int K) { return K == 64 ? 26 : 29; }
 
 // VEG volume-mesh files (lpg_veg.cpp; src/core/mesh/io/veg.cpp).
 struct VegMesh {
@@ -140,6 +147,11 @@ struct DevMesh {
     int32_t* hex_cells = nullptr;
     double* hex_theta = nullptr;
     double* hex_q = nullptr;
+    // Tricubic Hermite hexes (K = 64 plan nodes, 8 per vertex; hex_cells and hex_theta as
+    // above): per point the 64 x 3 reference derivatives and the weight (193 values), and each
+    // element's box edge lengths (3 per element).
+    double* herm_q = nullptr;
+    double* herm_h = nullptr;
 };
 
 // Internal Hessian layout of the solvers: the upper-triangle sliced ELL of HostPlan::sell_*
@@ -194,6 +206,7 @@ size_t project_bytes(const DevMesh& m, int precision);
 constexpr int kProjRecord = 90;
 // Values per element of the hex block scratch: 36 blocks (a <= b of 8 vertices) of 3x3.
 constexpr int kHexRecord = 324;
+constexpr int kHermiteRecord = 2080 * 9; // tricubic Hermite hex: 64 nodes, 2080 blocks (a <= b)
 // per_elem (T doubles, optional) receives each element's step.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
                      double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr);
@@ -219,6 +232,11 @@ void launch_hex_deformation_gradients(const DevMesh& m, const double* u, double*
 void launch_hex_material_eval(const DevMesh& m, int precision, int hessian, const double* W, const double* P,
                               const double* A, double* elemE, double* per_elem, void* blocks, int* flags,
                               const EvalArgs& a, cudaStream_t s);
+// Tricubic Hermite hex element pass (Exact Hessian): energy per element into elemE, gradient
+// pieces (192 per element) into per_elem when a.grad is set, the 2080 blocks per element
+// (precision's type, kHermiteRecord values) into blocks when a.hess is set, then the gathers.
+void launch_hermite_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem,
+                         void* blocks, const EvalArgs& a, cudaStream_t s);
 // Bytes of the block records launch_hex_eval needs: FP64 records, plus FP32 ones for a
 // projected mixed-precision Hessian (the projection runs in FP64).
 size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected);

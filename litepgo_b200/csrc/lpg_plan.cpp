@@ -29,8 +29,10 @@ namespace {
 // are computed by the same operations and are exact transposes.
 void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>& inc) {
     const int V = p.V, T = p.T;
-    constexpr int kMaskE = (1 << 29) - 1;
-    const int K = p.K, sh = K == 4 ? 2 : 3; // vertices per cell, bits per local index in a contributor
+    const int ishift = inc_shift(p.K), kMaskE = (1 << ishift) - 1;
+    const int K = p.K, sh = cell_bits(K); // vertices per cell, bits per local index in a contributor
+    const bool wide = K == 64;             // 32-bit contributors, stored as two 16-bit halves (low first)
+    const int max_rows = wide ? kClusterRowsWide : kClusterRows;
     std::vector<int32_t> cl_of(static_cast<size_t>(V), -1), qstamp(static_cast<size_t>(V), -1);
     std::vector<int32_t> estamp(static_cast<size_t>(T), -1);
     std::vector<int32_t> queue;
@@ -41,7 +43,7 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
         queue.assign(1, seed);
         qstamp[seed] = c;
         int nr = 0, ne = 0;
-        for (size_t qi = 0; qi < queue.size() && nr < kClusterRows; ++qi) {
+        for (size_t qi = 0; qi < queue.size() && nr < max_rows; ++qi) {
             const int v = queue[qi];
             if (cl_of[v] >= 0) continue;
             int add = 0;
@@ -81,8 +83,15 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
     p.cl_slot_ent.clear();
     p.cl_ents.clear();
     std::vector<int32_t> eloc(static_cast<size_t>(T), -1), els;
-    std::vector<std::vector<uint16_t>> bucket;
-    std::vector<std::vector<uint16_t>> diag;
+    std::vector<std::vector<uint32_t>> bucket;
+    std::vector<std::vector<uint32_t>> diag;
+    // Appends a contributor list to cl_ents: one 16-bit word each, or two for wide cells.
+    auto append = [&](const std::vector<uint32_t>& list) {
+        for (uint32_t w : list) {
+            p.cl_ents.push_back(static_cast<uint16_t>(w & 0xffffu));
+            if (wide) p.cl_ents.push_back(static_cast<uint16_t>(w >> 16));
+        }
+    };
     std::vector<std::pair<uint32_t, uint32_t>> left, right; // (slot word, entry word)
     for (int c = 0; c < ncl; ++c) {
         const int r0 = p.cl_row_ptr[c], nr = p.cl_row_ptr[c + 1] - r0;
@@ -110,17 +119,17 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
             const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
             bucket.assign(static_cast<size_t>(nb), {});
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
-                const int e = inc[k] & kMaskE, a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> 29);
-                const uint16_t el = static_cast<uint16_t>(eloc[e] << (2 * sh));
+                const int e = inc[k] & kMaskE, a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> ishift);
+                const uint32_t el = static_cast<uint32_t>(eloc[e]) << (2 * sh);
                 for (int b = 0; b < K; ++b) {
                     const int w = tets[K * static_cast<size_t>(e) + b];
                     if (w == v) {
-                        diag[j].push_back(static_cast<uint16_t>(el | (a << sh) | a));
+                        diag[j].push_back(el | static_cast<uint32_t>((a << sh) | a));
                         continue;
                     }
                     const int32_t* beg = p.col_idx.data() + rb;
                     const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
-                    bucket[q].push_back(static_cast<uint16_t>(v < w ? (el | (a << sh) | b) : (el | (b << sh) | a)));
+                    bucket[q].push_back(el | static_cast<uint32_t>(v < w ? ((a << sh) | b) : ((b << sh) | a)));
                 }
             }
             for (int q = 0; q < nb; ++q) {
@@ -130,7 +139,7 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
                 const uint32_t ent = static_cast<uint32_t>(p.cl_ents.size() - ent0) |
                                      (static_cast<uint32_t>(bucket[q].size()) << 20);
                 (v > w ? left : right).emplace_back(word, ent);
-                p.cl_ents.insert(p.cl_ents.end(), bucket[q].begin(), bucket[q].end());
+                append(bucket[q]);
                 ++noff;
             }
         }
@@ -147,7 +156,7 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
             p.cl_slot.push_back(static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (1u << 31));
             p.cl_slot_ent.push_back(static_cast<uint32_t>(p.cl_ents.size() - ent0) |
                                     (static_cast<uint32_t>(diag[j].size()) << 20));
-            p.cl_ents.insert(p.cl_ents.end(), diag[j].begin(), diag[j].end());
+            append(diag[j]);
         }
         if (p.cl_ents.size() - ent0 >= (1u << 20) ||
             p.cl_ents.size() >= static_cast<size_t>(std::numeric_limits<int32_t>::max()))
@@ -166,10 +175,12 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
     p.K = K;
     if (V < 0 || T < 0) fail(LPG_EINVAL, "MeshTopology requires a non-negative vertex count");
     if (V > std::numeric_limits<int>::max() / 3) fail(LPG_EINVAL, "VertexDofMap requires total DOFs fitting in int");
-    if (K != 4 && K != 8) fail(LPG_EINVAL, "cells must have 4 (tet) or 8 (hex) vertices");
-    if (T >= (1 << 29)) fail(LPG_EINVAL, "mesh has too many elements for the assembly plan (limit 2^29)");
+    if (K != 4 && K != 8 && K != 64) fail(LPG_EINVAL, "cells must have 4 (tet), 8 (hex) or 64 (Hermite hex) nodes");
+    const int ishift = inc_shift(K);
+    if (T >= (1 << ishift))
+        fail(LPG_EINVAL, "mesh has too many elements for the assembly plan (limit 2^" + std::to_string(ishift) + ")");
     for (int e = 0; e < T; ++e) {
-        int s[8];
+        int s[64];
         std::memcpy(s, tets + K * static_cast<size_t>(e), K * sizeof(int));
         std::sort(s, s + K);
         if (s[0] < 0 || s[K - 1] >= V)
@@ -191,7 +202,7 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
         for (int e = 0; e < T; ++e)
             for (int a = 0; a < K; ++a) {
                 const int v = tets[K * static_cast<size_t>(e) + a];
-                inc[fill[v]++] = e | (a << 29);
+                inc[fill[v]++] = e | (a << ishift);
             }
     }
     int maxdeg = 0;
@@ -209,7 +220,7 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
         for (int v = 0; v < V; ++v) {
             buf.clear();
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
-                const int e = inc[k] & ((1 << 29) - 1);
+                const int e = inc[k] & ((1 << ishift) - 1);
                 for (int b = 0; b < K; ++b) buf.push_back(tets[K * static_cast<size_t>(e) + b]);
             }
             std::sort(buf.begin(), buf.end());
@@ -306,7 +317,8 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
     const int V = p.V, T = p.T;
     const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
     auto bad = [](const char* what) { fail(LPG_ELOGIC, std::string("assembly cluster plan: ") + what); };
-    const int K = p.K, sh = K == 4 ? 2 : 3;
+    const int K = p.K, sh = cell_bits(K);
+    const bool wide = K == 64;
     auto vert = [&](int e, int a) { return tets[K * static_cast<size_t>(e) + a]; };
     // Incidence (vertex -> elements, ascending), independent of the plan's own.
     std::vector<int32_t> ptr(static_cast<size_t>(V) + 1, 0), inc(K * static_cast<size_t>(T));
@@ -327,7 +339,8 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
         if ((owner[v] >= 0) != (ptr[v + 1] > ptr[v])) bad("referenced vertex without a cluster");
     for (int c = 0; c < ncl; ++c) {
         const int e0 = p.cl_el_ptr[c], ne = p.cl_el_ptr[c + 1] - e0;
-        if (p.cl_row_ptr[c + 1] - p.cl_row_ptr[c] > kClusterRows || ne > kClusterElems) bad("cluster over its limits");
+        if (p.cl_row_ptr[c + 1] - p.cl_row_ptr[c] > (wide ? kClusterRowsWide : kClusterRows) || ne > kClusterElems)
+            bad("cluster over its limits");
         for (int i = 0; i < ne; ++i) {
             const int e = static_cast<int>(p.cl_els[e0 + i] & 0x7fffffffu);
             if (i > 0 && e <= static_cast<int>(p.cl_els[e0 + i - 1] & 0x7fffffffu)) bad("elements not ascending");
@@ -374,7 +387,8 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
             if ((de >> 20) != expect.size()) bad("slot contributor count");
             const size_t off = p.cl_ent_ptr[c] + (de & 0xfffffu);
             for (size_t t = 0; t < expect.size(); ++t) {
-                const uint16_t en = p.cl_ents[off + t];
+                const uint32_t en = wide ? p.cl_ents[off + 2 * t] | (static_cast<uint32_t>(p.cl_ents[off + 2 * t + 1]) << 16)
+                                         : p.cl_ents[off + t];
                 const int el = en >> (2 * sh), a = (en >> sh) & (K - 1), b = en & (K - 1);
                 if (el >= ne) bad("contributor outside the cluster");
                 const int e = static_cast<int>(p.cl_els[e0 + el] & 0x7fffffffu);

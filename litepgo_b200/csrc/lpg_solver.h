@@ -36,6 +36,7 @@ struct lpg_fem {
     lpg::DeviceBuffer b_row_ptr, b_col_idx, b_inc_ptr, b_tets, b_rec64, b_rec32, b_fpinv64, b_fpinv32, b_diag_slot,
         b_unused;
     lpg::DeviceBuffer b_hex[4]; // hex meshes: rest positions, cells, [lambda, mu], quadrature table
+    lpg::DeviceBuffer b_herm;   // Hermite hex meshes: box edge lengths per element
     lpg::DeviceBuffer b_cl[11]; // assembly clusters
     lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers
     lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton

@@ -40,8 +40,10 @@ __all__ = [
     "PyVolumetricMaterial",
     "VolumetricFemEnergyPyMaterialTetP1",
     "HexQ1Basis",
+    "HexHermiteBasis",
     "GaussLegendre3D",
     "VolumetricFemEnergyHexQ1",
+    "VolumetricFemEnergyHexHermite",
     "VolumetricFemEnergyPyMaterialHexQ1",
 ]
 
@@ -87,6 +89,40 @@ class HexQ1Basis:
         df = np.array([-1.0, 1.0])
         return np.array([[df[i] * f[j, 1] * f[k, 2], f[i, 0] * df[j] * f[k, 2], f[i, 0] * f[j, 1] * df[k]]
                          for i, j, k in cls.corners])
+
+
+class HexHermiteBasis:
+    """Tricubic Hermite functions on [0,1]^3 (hex_hermite_basis.hpp): function 8 corner + slot is
+    the product of 1D cubic Hermite factors (u(0), u'(0), u(1), u'(1), cubic_hermite_basis.hpp)
+    with index 2 corner_d + order_d per axis; slot derivative orders (0,0,0), (1,0,0), (0,1,0),
+    (0,0,1), (1,1,0), (1,0,1), (0,1,1), (1,1,1). A vertex carries 24 physical DOFs (slots u, u_X,
+    u_Y, u_Z, u_XY, u_XZ, u_YZ, u_XYZ of 3 components)."""
+
+    num_basis_functions = 64
+    dofs_per_vertex = 24
+    corners = HexQ1Basis.corners
+    orders = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0], [1, 0, 1], [0, 1, 1], [1, 1, 1]])
+
+    @staticmethod
+    def _cubic(t):
+        t2, t3 = t * t, t * t * t
+        return (np.array([2 * t3 - 3 * t2 + 1, t3 - 2 * t2 + t, -2 * t3 + 3 * t2, t3 - t2]),
+                np.array([6 * t2 - 6 * t, 3 * t2 - 4 * t + 1, -6 * t2 + 6 * t, 3 * t2 - 2 * t]))
+
+    @classmethod
+    def _index(cls, row):
+        return 2 * cls.corners[row // 8] + cls.orders[row % 8]
+
+    @classmethod
+    def eval_N(cls, xi):
+        (x, _), (y, _), (z, _) = (cls._cubic(float(c)) for c in xi)
+        return np.array([x[i] * y[j] * z[k] for i, j, k in (cls._index(r) for r in range(64))])
+
+    @classmethod
+    def eval_dN_dxi(cls, xi):
+        (x, dx), (y, dy), (z, dz) = (cls._cubic(float(c)) for c in xi)
+        return np.array([[dx[i] * y[j] * z[k], x[i] * dy[j] * z[k], x[i] * y[j] * dz[k]]
+                         for i, j, k in (cls._index(r) for r in range(64))])
 
 
 class _GaussLegendre3D:
@@ -420,7 +456,7 @@ class VolumetricFemEnergyTetP1(Energy):
 
     def pattern_bsr(self):
         if self._bsr is None:
-            row_ptr = np.empty(self.num_vertices + 1, dtype=np.int32)
+            row_ptr = np.empty(self.num_dofs // 3 + 1, dtype=np.int32)  # one block row per 3 DOFs
             col_idx = np.empty(self.nnzb, dtype=np.int32)
             N.check(N.lib.lpg_fem_pattern_bsr(self._h, N.iptr(row_ptr), N.iptr(col_idx)))
             self._bsr = (row_ptr, col_idx)
@@ -707,11 +743,13 @@ class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
     response and the theta adjoint work as for tets."""
 
     points_per_axis = 2
+    _dofs_per_vertex = 3  # DOFs per mesh vertex (24 for Hermite)
+    _create = "lpg_fem_create_hex"
 
     def __init__(self, displacement_map, rest_position_fields, Fp, theta, batch_size=256):
         if isinstance(batch_size, bool) or int(batch_size) <= 0:
             raise ValueError("MeshEnergy: invalid batch size")
-        if not isinstance(displacement_map, VertexDofMap) or displacement_map.dofs_per_vertex != 3:
+        if not isinstance(displacement_map, VertexDofMap) or displacement_map.dofs_per_vertex != self._dofs_per_vertex:
             raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
         cells = np.ascontiguousarray(displacement_map.cells, dtype=np.int32)
         if cells.ndim != 2 or cells.shape[1] != 8:
@@ -730,16 +768,17 @@ class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
         th = np.ascontiguousarray(th, dtype=np.float64)
         h = ctypes.c_void_p()
         self.device = _device_index()
-        N.check(N.lib.lpg_fem_create_hex(X.shape[0], N.dptr(X), cells.shape[0], N.iptr(cells), N.dptr(th),
-                                         1 if th.ndim == 2 else 0, int(self.points_per_axis), self.device,
-                                         ctypes.byref(h)))
+        N.check(getattr(N.lib, self._create)(X.shape[0], N.dptr(X), cells.shape[0], N.iptr(cells), N.dptr(th),
+                                             1 if th.ndim == 2 else 0, int(self.points_per_axis), self.device,
+                                             ctypes.byref(h)))
         self._h = h
         self._theta = th
         V_, T_, n_ = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         nnzb, nnz = ctypes.c_int64(), ctypes.c_int64()
         N.check(N.lib.lpg_fem_sizes(h, ctypes.byref(V_), ctypes.byref(T_), ctypes.byref(n_), ctypes.byref(nnzb),
                                     ctypes.byref(nnz)))
-        self.num_vertices, self.num_elements, self.num_dofs = V_.value, T_.value, n_.value
+        # The plan's block rows are (vertex, 3-DOF group): one per vertex, 8 per Hermite vertex.
+        self.num_vertices, self.num_elements, self.num_dofs = X.shape[0], T_.value, n_.value
         self.nnzb, self.nnz = nnzb.value, nnz.value
         self._csc = None
         self._bsr = None
@@ -751,10 +790,25 @@ class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
 
         X = np.asarray(X, dtype=np.float64).reshape(-1, 3)
         topo = HexTopology(X.shape[0], cells)
-        return cls(VertexDofMap(topo, 3), X, Fp, theta, batch_size)
+        return cls(VertexDofMap(topo, cls._dofs_per_vertex), X, Fp, theta, batch_size)
 
 
 class VolumetricFemEnergyHexQ1GL4(VolumetricFemEnergyHexQ1):
+    points_per_axis = 4
+
+
+class VolumetricFemEnergyHexHermite(VolumetricFemEnergyHexQ1):
+    """VolumetricFemEnergy[NeoHookean, HexHermiteBasis, GaussLegendre3D[n]] on one GPU: rest
+    positions (V, 3) of axis-aligned box cells in corner order (ValueError otherwise), 24 physical
+    DOFs per vertex (VertexDofMap(topology, 24)), the reference's DOF scaling by the box edges.
+    The Exact Hessian only (a projected request raises ValueError): run Newton with
+    hessian=Exact. set_theta works; the sensitivities and Python materials are tet/Q1 only."""
+
+    _dofs_per_vertex = 24
+    _create = "lpg_fem_create_hex_hermite"
+
+
+class VolumetricFemEnergyHexHermiteGL4(VolumetricFemEnergyHexHermite):
     points_per_axis = 4
 
 
@@ -981,7 +1035,9 @@ GaussLegendre3D = Template("GaussLegendre3D", {(2,): GaussLegendre3D_2, (4,): Ga
 VolumetricFemEnergy = Template("VolumetricFemEnergy",
                                {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyTetP1,
                                 (NeoHookean, HexQ1Basis, GaussLegendre3D_2): VolumetricFemEnergyHexQ1,
-                                (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemEnergyHexQ1GL4})
+                                (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemEnergyHexQ1GL4,
+                                (NeoHookean, HexHermiteBasis, GaussLegendre3D_2): VolumetricFemEnergyHexHermite,
+                                (NeoHookean, HexHermiteBasis, GaussLegendre3D_4): VolumetricFemEnergyHexHermiteGL4})
 VolumetricFemEnergy.material_factory = _py_energy_class
 VolumetricFemForceMaterialResponse = Template(
     "VolumetricFemForceMaterialResponse",

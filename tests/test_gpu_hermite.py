@@ -1,0 +1,119 @@
+"""Tricubic Hermite hexes on the GPU path (VolumetricFemEnergy[NeoHookean, HexHermiteBasis,
+GaussLegendre3D[n]]): energy, gradient and Exact Hessian over the 24 physical DOFs per vertex
+against the Hermite oracle (the two-box fixture of the reference's hex force test and a
+structured box), the feasible step, the construction checks, and Newton with the Exact Hessian."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle
+from conftest import rel_err
+from litepgo_b200 import dof, energy, fem, mesh, solver
+from test_oracle_hermite import HERMITE_CELLS, HERMITE_THETA, HERMITE_X, hermite_state
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+Exact, Projected = energy.HessianKind.Exact, energy.HessianKind.Projected
+
+
+def hermite_energy(X, cells, theta, n=2):
+    cls = fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[n]]
+    return cls.from_arrays(X, cells, theta)
+
+
+@pytest.mark.parametrize("n", [2, 4])
+def test_two_box_fixture_matches_the_oracle(n):
+    x = hermite_state()
+    gpu = hermite_energy(HERMITE_X, HERMITE_CELLS, HERMITE_THETA, n)
+    assert gpu.num_dofs == 24 * 12
+    E, g, H = gpu.eval(x, gradient=True, hessian=Exact)
+    Er, gr, Hr = oracle.hex_hermite_eval(HERMITE_X, HERMITE_CELLS, HERMITE_THETA, x, points_per_axis=n)
+    assert abs(E - Er) <= 1e-12 * abs(Er)
+    assert rel_err(g, gr) <= 1e-12
+    assert rel_err(H.toarray(), Hr) <= 1e-12
+    D = (H - H.T).tocsc()
+    D.eliminate_zeros()
+    assert D.nnz == 0  # bitwise symmetric
+    _, _, H32 = gpu.eval(x, hessian=Exact, precision="mixed")
+    assert rel_err(H32.toarray(), Hr) <= 1e-6
+    assert abs(gpu.element_energies(x).sum() - E) <= 1e-12 * abs(E)
+
+
+def test_structured_box_and_feasible_step():
+    X, cells = mesh.make_hex_box(3, 2, 2)
+    rng = np.random.default_rng(4)
+    T = cells.shape[0]
+    mu = np.exp(rng.uniform(np.log(1e3), np.log(1e5), T))
+    theta = np.column_stack([3 * mu, mu])
+    u = 1e-3 * rng.standard_normal(24 * X.shape[0])
+    gpu = hermite_energy(X, cells, theta)
+    E, g, H = gpu.eval(u, gradient=True, hessian=Exact)
+    Er, gr, Hr = oracle.hex_hermite_eval(X, cells, theta, u)
+    assert abs(E - Er) <= 1e-12 * abs(Er)
+    assert rel_err(g, gr) <= 1e-12
+    assert rel_err(H.toarray(), Hr) <= 1e-12
+    # The feasible step: the reference's positive-determinant step at every point, minimum.
+    du = 0.3 * rng.standard_normal(u.size)
+    pts, _ = oracle.hex_points(2)
+    U, dU = u.reshape(-1, 24), du.reshape(-1, 24)
+    ref = 1.0
+    for cell in cells:
+        h = oracle.hermite_box(X[cell])
+        s = np.repeat(np.tile([1, h[0], h[1], h[2], h[0] * h[1], h[0] * h[2], h[1] * h[2], np.prod(h)], 8), 3)
+        C, dC = (U[cell].ravel() * s).reshape(64, 3), (dU[cell].ravel() * s).reshape(64, 3)
+        for xi in pts:
+            gN = oracle.hex_hermite_N_dN(xi)[1] / h
+            ref = min(ref, oracle.positive_det_step(np.eye(3) + C.T @ gN, dC.T @ gN))
+    assert ref < 1.0
+    assert abs(gpu.max_feasible_step(u, du) - ref) <= 1e-12
+
+
+def test_construction_and_unsupported_requests():
+    gpu = hermite_energy(HERMITE_X, HERMITE_CELLS, HERMITE_THETA)
+    with pytest.raises(ValueError, match="Hermite"):
+        gpu.eval(hermite_state(), hessian=Projected)
+    corners = oracle.HEX_CORNERS.astype(float)
+    cell = np.arange(8, dtype=np.int32)[None]
+    hermite_energy(corners, cell, HERMITE_THETA)
+    sheared = corners.copy()
+    sheared[:, 0] += 0.2 * sheared[:, 1]
+    with pytest.raises(ValueError, match="axis-aligned"):
+        hermite_energy(sheared, cell, HERMITE_THETA)
+    with pytest.raises(ValueError):
+        hermite_energy(corners, np.array([[1, 0, 3, 2, 5, 4, 7, 6]], dtype=np.int32), HERMITE_THETA)
+    topo = mesh.HexTopology(12, HERMITE_CELLS)
+    with pytest.raises(ValueError):  # the Q1 map width
+        fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[2]](
+            dof.VertexDofMap(topo, 3), HERMITE_X, None, HERMITE_THETA)
+    Resp = fem.VolumetricFemForceMaterialResponseHexQ1
+    with pytest.raises(ValueError):
+        Resp(dof.ConstantDofMap(topo, 2), dof.VertexDofMap(topo, 24), HERMITE_X, hermite_state(), None)
+    th = np.tile([3.0, 4.0], (2, 1))
+    gpu.set_theta(th)
+    assert gpu.eval(hermite_state())[0] == hermite_energy(HERMITE_X, HERMITE_CELLS, th).eval(hermite_state())[0]
+
+
+def test_hermite_newton_exact_hessian():
+    """A 3x2x2 Hermite box (4 points per axis: 2 leave zero-energy modes in the tricubic field)
+    with its x = 0 vertices held (all 24 DOFs) and a load on the value slots: Newton with the
+    Exact Hessian converges, and the oracle's free gradient equals the load."""
+    X, cells = mesh.make_hex_box(3, 2, 2)
+    n = 24 * X.shape[0]
+    theta = np.array([1.4e5, 3.4e4])
+    gpu = hermite_energy(X, cells, theta, 4)
+    rng = np.random.default_rng(8)
+    f = np.zeros(n)
+    value = (24 * np.arange(X.shape[0])[:, None] + np.arange(3)).ravel()
+    f[value] = 50.0 * rng.standard_normal(value.size)
+    fixed = (24 * np.flatnonzero(X[:, 0] == 0)[:, None] + np.arange(24)).ravel()
+    f[fixed] = 0
+    total = energy.WeightedSumEnergy([(gpu, 1.0), (energy.QuadraticEnergy(sp.csc_matrix((n, n)), -f), 1.0)])
+    opts = solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", accept_rule="armijo",
+                                precision="f64", max_iterations=50, cg_tolerance=1e-4, hessian=Exact)
+    r = solver.newton_solve(total, dof.DofReduction(n, fixed), np.zeros(n), opts)
+    assert r.status.name == "Converged"
+    _, g, _ = oracle.hex_hermite_eval(X, cells, theta, np.asarray(r.x), points_per_axis=4, hessian=False)
+    free = np.setdiff1d(np.arange(n), fixed)
+    assert np.abs((g - f)[free]).max() <= 1e-7 * np.abs(f).max()

@@ -252,3 +252,24 @@ def test_hex_cluster_plan_invariants(case):
     bad[0, 3] = bad[0, 0]
     with pytest.raises(ValueError, match="distinct"):
         cell_summary(X, bad, 8)
+
+
+def hermite_cells(cells):
+    """The 64 nodes of each tricubic Hermite hex: node 8 v + slot for basis function
+    8 corner + slot (v = cells[corner]), each node a 3-DOF row of the assembly plan."""
+    cells = np.asarray(cells, dtype=np.int64)
+    return (8 * cells[:, :, None] + np.arange(8)).reshape(-1, 64).astype(np.int32)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 2, 2), (4, 3, 2)])
+def test_hermite_cluster_plan_invariants(shape):
+    """The assembly plan of 64-node cells (two 16-bit words per contributor, clusters of at most
+    one vertex's eight rows): every invariant the library checks, and 64^2 contributors per cell."""
+    X, cells = mesh.make_hex_box(*shape)
+    nodes = hermite_cells(cells)
+    ncl, max_rows, max_els, evals, entries = cell_summary(np.zeros((8 * X.shape[0], 3)), nodes, 64)
+    assert entries == 64 * 64 * cells.shape[0]
+    assert 1 <= max_rows <= 8 and max_els <= 224
+    rng = np.random.default_rng(1)
+    perm = rng.permutation(8 * X.shape[0])
+    assert cell_summary(np.zeros((8 * X.shape[0], 3)), perm[nodes].astype(np.int32), 64)[4] == entries
