@@ -24,13 +24,17 @@ def hermite_energy(X, cells, theta, n=2):
 
 
 @pytest.mark.parametrize("n", [2, 4])
-def test_two_box_fixture_matches_the_oracle(n):
-    x = hermite_state()
+@pytest.mark.parametrize("scale,e_tol", [(0.05, 1e-12), (0.002, 1e-10)])
+def test_two_box_fixture_matches_the_oracle(n, scale, e_tol):
+    """At the reference test's scale (0.002) W is second order in strains whose terms are first
+    order, so the energy carries ~1/strain times the round-off of F (different summation orders
+    of the 64 nodes): its tolerance is wider there; gradient and Hessian keep 1e-12."""
+    x = hermite_state(scale)
     gpu = hermite_energy(HERMITE_X, HERMITE_CELLS, HERMITE_THETA, n)
     assert gpu.num_dofs == 24 * 12
     E, g, H = gpu.eval(x, gradient=True, hessian=Exact)
     Er, gr, Hr = oracle.hex_hermite_eval(HERMITE_X, HERMITE_CELLS, HERMITE_THETA, x, points_per_axis=n)
-    assert abs(E - Er) <= 1e-12 * abs(Er)
+    assert abs(E - Er) <= e_tol * abs(Er)
     assert rel_err(g, gr) <= 1e-12
     assert rel_err(H.toarray(), Hr) <= 1e-12
     D = (H - H.T).tocsc()
@@ -38,7 +42,7 @@ def test_two_box_fixture_matches_the_oracle(n):
     assert D.nnz == 0  # bitwise symmetric
     _, _, H32 = gpu.eval(x, hessian=Exact, precision="mixed")
     assert rel_err(H32.toarray(), Hr) <= 1e-6
-    assert abs(gpu.element_energies(x).sum() - E) <= 1e-12 * abs(E)
+    assert abs(gpu.element_energies(x).sum() - E) <= e_tol * abs(E)
 
 
 def test_structured_box_and_feasible_step():
@@ -47,7 +51,7 @@ def test_structured_box_and_feasible_step():
     T = cells.shape[0]
     mu = np.exp(rng.uniform(np.log(1e3), np.log(1e5), T))
     theta = np.column_stack([3 * mu, mu])
-    u = 1e-3 * rng.standard_normal(24 * X.shape[0])
+    u = 0.02 * rng.standard_normal(24 * X.shape[0])  # det F >= 0.78 at every point
     gpu = hermite_energy(X, cells, theta)
     E, g, H = gpu.eval(u, gradient=True, hessian=Exact)
     Er, gr, Hr = oracle.hex_hermite_eval(X, cells, theta, u)
