@@ -702,8 +702,23 @@ def run_rows():
                              "at_rest_eval_ms": re.value, "at_rest_hexes_per_s": ch.shape[0] / (re.value * 1e-3)},
                "timing": "lpg_fem_time_eval: CUDA events, L2 flushed between launches, FP64 E + gradient + BSR "
                          "(Exact, and Projected: per-element 24x24 eigen-projection)"}
-    line = {"rows": "plastic-field force VJP, adjoint in Fp, VEG I/O, hex Q1", "config": workload_config(),
-            "hex_q1": hex_row,
+    # Tricubic Hermite hexes (GaussLegendre3D[2]) E + gradient + Exact Hessian on a 12^3 box.
+    Xm, cm = mesh.make_hex_box(12)
+    em = fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[2]].from_arrays(
+        Xm, cm, np.array([1.4e5, 3.4e4]))
+    um = torch.as_tensor(0.005 * np.random.default_rng(3).standard_normal(em.num_dofs), device=dev)
+    gm = torch.empty(em.num_dofs, dtype=torch.float64, device=dev)
+    Hm = torch.empty(em.nnz, dtype=torch.float64, device=dev)
+    N.check(N.lib.lpg_fem_set_stream(em.handle, ctypes.c_void_p(stream.cuda_stream)))
+    ha, he = ctypes.c_double(), ctypes.c_double()
+    N.check(N.lib.lpg_fem_time_eval(em.handle, N.vptr(um), N.vptr(gm), int(energy.HessianKind.Exact), N.PRECISION_F64,
+                                    N.LAYOUT_BSR, N.vptr(Hm), 10, 1, ctypes.byref(ha), ctypes.byref(he)))
+    hermite_row = {"mesh": f"Hermite hex box 12^3 ({cm.shape[0]} hexes, {em.num_dofs} DOFs, nnzb {em.nnzb}), 8 points",
+                   "element_pass_and_gather_ms": ha.value, "eval_ms": he.value,
+                   "hexes_per_s": cm.shape[0] / (he.value * 1e-3),
+                   "timing": "lpg_fem_time_eval: CUDA events, L2 flushed between launches, FP64 E + gradient + Exact BSR"}
+    line = {"rows": "plastic-field force VJP, adjoint in Fp, VEG I/O, hex Q1, Hermite hex", "config": workload_config(),
+            "hex_q1": hex_row, "hex_hermite": hermite_row,
             "fp_vjp": fp_row, "newton_with_fp": {"status": r.status.name, "iterations": r.iterations, "seconds": r.seconds},
             "adjoint_fp": adj,
             "veg": {"bytes": size, "write_s": tw, "read_s": tr, "read_mb_per_s": size / tr / 1e6,
