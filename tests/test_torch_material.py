@@ -79,3 +79,29 @@ def test_quadrature_and_basis_templates():
         fem.GaussLegendre3D[3]
     with pytest.raises(TypeError):
         fem.VolumetricFemEnergy[fem.NeoHookean, fem.TetP1Basis, fem.GaussLegendre3D[2]]
+
+
+def test_hermite_and_hex_templates():
+    """Every (material, basis, quadrature) the hex rows instantiate, as the reference binds them
+    (src/binding/detail/fem_helpers.hpp:112-118), and the Hermite basis mirror."""
+    import oracle
+
+    for n in (2, 4):
+        Q = fem.GaussLegendre3D[n]
+        herm = fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexHermiteBasis, Q]
+        assert herm.points_per_axis == n and herm._dofs_per_vertex == 24
+        resp = fem.VolumetricFemForceMaterialResponse[fem.NeoHookean, fem.HexQ1Basis, Q]
+        assert resp._energy_cls.points_per_axis == n
+        mat = fem.VolumetricFemEnergy[TorchNeoHookean, fem.HexQ1Basis, Q]
+        assert mat.material is TorchNeoHookean and mat._geometry_cls.points_per_axis == n
+    with pytest.raises(TypeError):
+        fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexHermiteBasis, fem.TetCentroidQuadrature]
+    with pytest.raises(TypeError):  # no Python materials over the Hermite basis
+        fem.VolumetricFemEnergy[TorchNeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[2]]
+    rng = np.random.default_rng(0)
+    for xi in rng.random((5, 3)):
+        N0, dN0 = oracle.hex_hermite_N_dN(xi)
+        np.testing.assert_allclose(fem.HexHermiteBasis.eval_N(xi), N0, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(fem.HexHermiteBasis.eval_dN_dxi(xi), dN0, rtol=0, atol=1e-14)
+        # The value functions alone sum to one (the reference's tests/python/test_fem.py:43).
+        assert abs(fem.HexHermiteBasis.eval_N(xi)[0::8].sum() - 1.0) < 1e-14
