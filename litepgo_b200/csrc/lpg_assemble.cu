@@ -1673,6 +1673,33 @@ __global__ void __launch_bounds__(256) material_pieces_kernel(const DevMesh m, c
 // FP64 throughout; the blocks are stored in the precision's type. The kinematics are recomputed
 // by each of an element's 36 threads (cheap next to reading a per-point cache).
 // ---------------------------------------------------------------------------
+// The rest geometry at one quadrature point of a hex (dq: the point's table row): J = sum_c X_c
+// dN_c^T (corners in order, fma per entry), its determinant and its inverse by cofactors.
+__device__ __forceinline__ void hex_point_geometry(const DevMesh& m, const int32_t* cell, const double* dq,
+                                                   double (&Ji)[9], double& dJ) {
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < 8; ++c) {
+        const int v = __ldg(cell + c);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) J[3 * i + d] = fma(X, __ldg(dq + 3 * c + d), J[3 * i + d]);
+        }
+    }
+    dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+    const double iJ = 1.0 / dJ;
+    Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
+    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
+    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
+    Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
+    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
+    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
+    Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
+    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
+    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+}
+
 __device__ __forceinline__ void hex_pair(int pr, int& a, int& b) {
     a = 0;
     int base = 0;
@@ -1699,41 +1726,22 @@ __global__ void __launch_bounds__(128) hex_element_kernel(const DevMesh m, const
         double Hb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, ga[3] = {0, 0, 0}, E = 0;
         for (int q = 0; q < m.nq; ++q) {
             const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
-            double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            // J^-1 (det J > 0 was checked when the mesh was built) and grad u in reference coordinates.
+            double Ji[9], dJ;
+            hex_point_geometry(m, cell, dq, Ji, dJ);
+            double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             bool ok = true;
             for (int c = 0; c < 8; ++c) {
                 const int v = __ldg(cell + c);
-                double dn[3], X[3], uu[3];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    dn[d] = __ldg(dq + 3 * c + d);
-                    X[d] = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + d);
-                    uu[d] = __ldg(u + 3 * static_cast<size_t>(v) + d);
-                    ok = ok && isfinite(uu[d]);
+                for (int i = 0; i < 3; ++i) {
+                    const double uu = __ldg(u + 3 * static_cast<size_t>(v) + i);
+                    ok = ok && isfinite(uu);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) G[3 * i + d] = fma(uu, __ldg(dq + 3 * c + d), G[3 * i + d]);
                 }
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        J[3 * i + d] = fma(X[i], dn[d], J[3 * i + d]);
-                        G[3 * i + d] = fma(uu[i], dn[d], G[3 * i + d]);
-                    }
             }
             if (!ok) st |= ST_BAD_INPUT;
-            // J^-1 by cofactors (det J > 0 was checked when the mesh was built).
-            double Ji[9];
-            const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
-                              J[2] * (J[3] * J[7] - J[4] * J[6]);
-            const double iJ = 1.0 / dJ;
-            Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
-            Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
-            Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
-            Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
-            Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
-            Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
-            Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
-            Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
-            Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
             const double w = __ldg(dq + 24) * dJ;
             double F[9];
 #pragma unroll
@@ -1843,37 +1851,23 @@ __global__ void __launch_bounds__(128) hex_force_vjp_kernel(const DevMesh m, con
         double dl = 0, dm = 0;
         for (int q = 0; q < m.nq; ++q) {
             const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
-            double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            double Wr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double Ji[9], dJ;
+            hex_point_geometry(m, cell, dq, Ji, dJ);
+            double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Wr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             for (int c = 0; c < 8; ++c) {
                 const int v = __ldg(cell + c);
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
                     const double uu = __ldg(u + 3 * static_cast<size_t>(v) + i);
                     const double ww = __ldg(w + 3 * static_cast<size_t>(v) + i);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         const double dn = __ldg(dq + 3 * c + d);
-                        J[3 * i + d] = fma(X, dn, J[3 * i + d]);
                         G[3 * i + d] = fma(uu, dn, G[3 * i + d]);
                         Wr[3 * i + d] = fma(ww, dn, Wr[3 * i + d]);
                     }
                 }
             }
-            const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
-                              J[2] * (J[3] * J[7] - J[4] * J[6]);
-            const double iJ = 1.0 / dJ;
-            double Ji[9];
-            Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
-            Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
-            Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
-            Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
-            Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
-            Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
-            Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
-            Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
-            Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
             double F[9], Wg[9];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
@@ -1919,31 +1913,6 @@ __global__ void __launch_bounds__(128) hex_force_vjp_kernel(const DevMesh m, con
 // Materials evaluated outside the library on hex meshes (PyVolumetricMaterial over HexQ1Basis):
 // F at every quadrature point (row-major, 9 per point, points of an element consecutive), then
 // the caller's W, P = dW/dF and A = d2W/dF2 per point integrated and assembled per hex.
-__device__ __forceinline__ void hex_point_geometry(const DevMesh& m, const int32_t* cell, const double* dq,
-                                                   double (&Ji)[9], double& dJ) {
-    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int c = 0; c < 8; ++c) {
-        const int v = __ldg(cell + c);
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) J[3 * i + d] = fma(X, __ldg(dq + 3 * c + d), J[3 * i + d]);
-        }
-    }
-    dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
-    const double iJ = 1.0 / dJ;
-    Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
-    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
-    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
-    Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
-    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
-    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
-    Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
-    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
-    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
-}
-
 __global__ void __launch_bounds__(128) hex_deformation_gradient_kernel(const DevMesh m, const double* __restrict__ u,
                                                                        double* __restrict__ F, unsigned* status) {
     const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -2100,34 +2069,18 @@ __global__ void __launch_bounds__(128) hex_tangent_test_kernel(const DevMesh m, 
     const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
     const double lam = m.hex_theta[2 * static_cast<size_t>(e)], mu = m.hex_theta[2 * static_cast<size_t>(e) + 1];
     const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
-    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double Ji[9], dJ;
+    hex_point_geometry(m, cell, dq, Ji, dJ);
+    double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int c = 0; c < 8; ++c) {
         const int v = __ldg(cell + c);
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
             const double uu = __ldg(u + 3 * static_cast<size_t>(v) + i);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double dn = __ldg(dq + 3 * c + d);
-                J[3 * i + d] = fma(X, dn, J[3 * i + d]);
-                G[3 * i + d] = fma(uu, dn, G[3 * i + d]);
-            }
+            for (int d = 0; d < 3; ++d) G[3 * i + d] = fma(uu, __ldg(dq + 3 * c + d), G[3 * i + d]);
         }
     }
-    const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
-                      J[2] * (J[3] * J[7] - J[4] * J[6]);
-    const double iJ = 1.0 / dJ;
-    double Ji[9];
-    Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
-    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
-    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
-    Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
-    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
-    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
-    Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
-    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
-    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
     double F[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -2247,19 +2200,17 @@ __global__ void __launch_bounds__(256) hex_feasible_kernel(const DevMesh m, cons
         const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
         for (int q = 0; q < m.nq && st == 0; ++q) {
             const double* dq = m.hex_q + 25 * static_cast<size_t>(q);
-            double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, D[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, D[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             bool ok = true;
             for (int c = 0; c < 8; ++c) {
                 const int v = __ldg(cell + c);
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    const double X = __ldg(m.hex_X + 3 * static_cast<size_t>(v) + i);
                     const double uu = u[3 * static_cast<size_t>(v) + i], dd = du[3 * static_cast<size_t>(v) + i];
                     ok = ok && isfinite(uu) && isfinite(dd);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         const double dn = __ldg(dq + 3 * c + d);
-                        J[3 * i + d] = fma(X, dn, J[3 * i + d]);
                         G[3 * i + d] = fma(uu, dn, G[3 * i + d]);
                         D[3 * i + d] = fma(dd, dn, D[3 * i + d]);
                     }
@@ -2269,19 +2220,8 @@ __global__ void __launch_bounds__(256) hex_feasible_kernel(const DevMesh m, cons
                 st |= ST_BAD_INPUT;
                 break;
             }
-            const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
-                              J[2] * (J[3] * J[7] - J[4] * J[6]);
-            const double iJ = 1.0 / dJ;
-            double Ji[9];
-            Ji[0] = (J[4] * J[8] - J[5] * J[7]) * iJ;
-            Ji[1] = (J[2] * J[7] - J[1] * J[8]) * iJ;
-            Ji[2] = (J[1] * J[5] - J[2] * J[4]) * iJ;
-            Ji[3] = (J[5] * J[6] - J[3] * J[8]) * iJ;
-            Ji[4] = (J[0] * J[8] - J[2] * J[6]) * iJ;
-            Ji[5] = (J[2] * J[3] - J[0] * J[5]) * iJ;
-            Ji[6] = (J[3] * J[7] - J[4] * J[6]) * iJ;
-            Ji[7] = (J[1] * J[6] - J[0] * J[7]) * iJ;
-            Ji[8] = (J[0] * J[4] - J[1] * J[3]) * iJ;
+            double Ji[9], dJ;
+            hex_point_geometry(m, cell, dq, Ji, dJ);
             double F[9], dF[9];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
