@@ -156,8 +156,9 @@ int lpg_fem_create_hex(int num_vertices, const double* X, int num_cells, const i
  * u_YZ, u_XYZ of 3 components each, DOF 24 v + 3 slot + c. Block patterns and Hessians are over
  * 3x3 blocks of (vertex, slot) rows, 8 per vertex (lpg_fem_sizes reports 8 num_vertices block
  * rows). The handle answers lpg_fem_eval (Exact Hessian; Projected is LPG_EINVAL),
- * lpg_fem_feasible_step, lpg_fem_element_energies, lpg_fem_set_theta, the patterns and
- * lpg_newton_solve with the Exact Hessian; the sensitivity, material and batch entry points are
+ * lpg_fem_feasible_step, lpg_fem_element_energies, lpg_fem_set_theta, the patterns,
+ * lpg_newton_solve with the Exact Hessian, lpg_fem_force_vjp_theta and lpg_adjoint_theta (over
+ * the physical DOFs); the rest-position, plastic-field, material and batch entry points are
  * LPG_EINVAL. No plastic field (Fp = I).
  */
 int lpg_fem_create_hex_hermite(int num_vertices, const double* X, int num_cells, const int32_t* cells,

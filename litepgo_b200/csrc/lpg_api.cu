@@ -810,7 +810,6 @@ int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io
 int lpg_fem_force_vjp_theta(lpg_fem_t h, const double* u, const double* w, int io_mem, int per_element, double* out) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");
-        not_hermite(*h, "lpg_fem_force_vjp_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         const size_t n = 3 * static_cast<size_t>(h->dm.V);
@@ -1103,7 +1102,6 @@ int lpg_adjoint_theta(lpg_fem_t h, const double* u_star, const double* dLdu, con
                       double* lambda_out) {
     return guarded([&] {
         if (!h || !u_star || !dLdu || !dtheta) fail(LPG_EINVAL, "lpg_adjoint_theta: null argument");
-        not_hermite(*h, "lpg_adjoint_theta");
         BusyGuard busy(h->busy);
         LPG_CUDA(cudaSetDevice(h->device));
         adjoint_theta(*h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, per_element, dtheta,

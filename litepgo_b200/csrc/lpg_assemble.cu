@@ -2437,6 +2437,69 @@ __global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const 
     if ((tid & 31) == 0 && st) atomicOr(status, st);
 }
 
+// Force-response parameter VJP of Hermite hexes (the hex pass's, over the 64 nodes): per element
+//   d/dlambda = sum_q w_q log J_q (F_q^-T : grad w_q),   d/dmu = sum_q w_q ((F_q - F_q^-T) : grad w_q),
+// grad w = sum_b w_b G_b^T on the weight's physical DOFs. One thread per element; FP64.
+__global__ void __launch_bounds__(128) hermite_force_vjp_kernel(const DevMesh m, const double* __restrict__ u,
+                                                                const double* __restrict__ w, double* out,
+                                                                unsigned* status) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned st = 0;
+    if (e < m.T) {
+        const int32_t* cell = m.hex_cells + 8 * static_cast<size_t>(e);
+        const double h[3] = {m.herm_h[3 * static_cast<size_t>(e)], m.herm_h[3 * static_cast<size_t>(e) + 1],
+                             m.herm_h[3 * static_cast<size_t>(e) + 2]};
+        double dl = 0, dm = 0;
+        for (int q = 0; q < m.nq; ++q) {
+            const double* tq = m.herm_q + kHermiteTable * static_cast<size_t>(q);
+            double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, Gw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int b = 0; b < 64; ++b) {
+                double G[3];
+                hermite_G(tq, b, h, G);
+                const size_t base = 24 * static_cast<size_t>(__ldg(cell + (b >> 3))) + 3 * (b & 7);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const double uu = __ldg(u + base + i), ww = __ldg(w + base + i);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        F[3 * i + d] = fma(uu, G[d], F[3 * i + d]);
+                        Gw[3 * i + d] = fma(ww, G[d], Gw[3 * i + d]);
+                    }
+                }
+            }
+            double C[9];
+            C[0] = F[4] * F[8] - F[5] * F[7];
+            C[1] = F[5] * F[6] - F[3] * F[8];
+            C[2] = F[3] * F[7] - F[4] * F[6];
+            C[3] = F[2] * F[7] - F[1] * F[8];
+            C[4] = F[0] * F[8] - F[2] * F[6];
+            C[5] = F[1] * F[6] - F[0] * F[7];
+            C[6] = F[1] * F[5] - F[2] * F[4];
+            C[7] = F[2] * F[3] - F[0] * F[5];
+            C[8] = F[0] * F[4] - F[1] * F[3];
+            const double detF = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+            if (!(detF > 0) || !isfinite(detF)) {
+                st |= isfinite(detF) ? ST_BAD_DET : ST_NONFINITE_F;
+                continue;
+            }
+            double hf = 0, ff = 0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                hf = fma(C[k] / detF, Gw[k], hf);
+                ff = fma(F[k], Gw[k], ff);
+            }
+            const double wq = __ldg(tq + 192) * h[0] * h[1] * h[2];
+            dl = fma(wq * log(detF), hf, dl);
+            dm = fma(wq, ff - hf, dm);
+        }
+        if (!isfinite(dl) || !isfinite(dm)) st |= ST_NONFINITE_OUT;
+        out[2 * static_cast<size_t>(e)] = dl;
+        out[2 * static_cast<size_t>(e) + 1] = dm;
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
+}
+
 // Feasible step of a Hermite hex mesh: F and dF at every point, the positive-determinant step,
 // minimum per block (as hex_feasible_kernel).
 __global__ void __launch_bounds__(256) hermite_feasible_kernel(const DevMesh m, const double* __restrict__ u,
@@ -2672,6 +2735,8 @@ void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double
                       cudaStream_t s) {
     if (m.T > 0 && m.K == 8)
         hex_force_vjp_kernel<<<(m.T + 127) / 128, 128, 0, s>>>(m, u, w, out, status);
+    else if (m.T > 0 && m.K == 64)
+        hermite_force_vjp_kernel<<<(m.T + 127) / 128, 128, 0, s>>>(m, u, w, out, status);
     else if (m.T > 0)
         force_vjp_kernel<<<(m.T + 255) / 256, 256, 0, s>>>(m, u, w, out, status);
     LPG_CUDA(cudaGetLastError());

@@ -802,7 +802,8 @@ class VolumetricFemEnergyHexHermite(VolumetricFemEnergyHexQ1):
     positions (V, 3) of axis-aligned box cells in corner order (ValueError otherwise), 24 physical
     DOFs per vertex (VertexDofMap(topology, 24)), the reference's DOF scaling by the box edges.
     The Exact Hessian only (a projected request raises ValueError): run Newton with
-    hessian=Exact. set_theta works; the sensitivities and Python materials are tet/Q1 only."""
+    hessian=Exact. set_theta, the theta force response and the theta adjoint work; Python
+    materials are tet/Q1 only."""
 
     _dofs_per_vertex = 24
     _create = "lpg_fem_create_hex_hermite"
@@ -810,6 +811,18 @@ class VolumetricFemEnergyHexHermite(VolumetricFemEnergyHexQ1):
 
 class VolumetricFemEnergyHexHermiteGL4(VolumetricFemEnergyHexHermite):
     points_per_axis = 4
+
+
+class VolumetricFemForceMaterialResponseHexHermite(VolumetricFemForceMaterialResponseTetP1):
+    """VolumetricFemForceMaterialResponse[NeoHookean, HexHermiteBasis, GaussLegendre3D[2]]: the
+    force's VJP in theta over the 24 physical DOFs per vertex (VertexDofMap(topology, 24));
+    usable as the make_response of a StaticEquilibriumResponse."""
+
+    _energy_cls = VolumetricFemEnergyHexHermite
+
+
+class VolumetricFemForceMaterialResponseHexHermiteGL4(VolumetricFemForceMaterialResponseTetP1):
+    _energy_cls = VolumetricFemEnergyHexHermiteGL4
 
 
 class VolumetricFemForceMaterialResponseHexQ1(VolumetricFemForceMaterialResponseTetP1):
@@ -1043,7 +1056,9 @@ VolumetricFemForceMaterialResponse = Template(
     "VolumetricFemForceMaterialResponse",
     {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceMaterialResponseTetP1,
      (NeoHookean, HexQ1Basis, GaussLegendre3D_2): VolumetricFemForceMaterialResponseHexQ1,
-     (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemForceMaterialResponseHexQ1GL4})
+     (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemForceMaterialResponseHexQ1GL4,
+     (NeoHookean, HexHermiteBasis, GaussLegendre3D_2): VolumetricFemForceMaterialResponseHexHermite,
+     (NeoHookean, HexHermiteBasis, GaussLegendre3D_4): VolumetricFemForceMaterialResponseHexHermiteGL4})
 VolumetricFemForceFpResponse = Template(
     "VolumetricFemForceFpResponse",
     {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceFpResponseTetP1})

@@ -14,6 +14,7 @@ from .oracle import (  # noqa: F401
     hex_eval,
     hex_force_vjp_theta,
     hex_hermite_eval,
+    hex_hermite_force_vjp_theta,
     hex_hermite_N_dN,
     hermite_box,
     hex_points,

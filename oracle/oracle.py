@@ -476,6 +476,31 @@ def hex_hermite_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
     return E, g, H
 
 
+def hex_hermite_force_vjp_theta(X, cells, theta, u, w, points_per_axis=2):
+    """(d g / d theta)^T w per Hermite hex (T, 2) over physical DOFs u, w (24 per vertex): at every
+    point w_q d2W/dF dtheta : grad w, with grad w = sum_b (s_b w_b) (J^-T dN_b)."""
+    X = np.asarray(X, float).reshape(-1, 3)
+    cells = np.asarray(cells).reshape(-1, 8)
+    D = np.asarray(u, float).reshape(-1, 24)
+    Wv = np.asarray(w, float).reshape(-1, 24)
+    T = cells.shape[0]
+    th = np.broadcast_to(np.asarray(theta, float), (T, 2))
+    pts, wts = hex_points(points_per_axis)
+    out = np.zeros((T, 2))
+    for e, cell in enumerate(cells):
+        h = hermite_box(X[cell])
+        s = np.repeat(np.tile(hermite_slot_scales(h), 8), 3)
+        C = (D[cell].ravel() * s).reshape(64, 3)
+        Cw = (Wv[cell].ravel() * s).reshape(64, 3)
+        for xi, wq in zip(pts, wts):
+            gN = hex_hermite_N_dN(xi)[1] / h
+            F = np.eye(3) + C.T @ gN
+            Gw = Cw.T @ gN
+            Dth = nh_d2W_dF_dtheta(F, np.eye(3), th[e])  # (9, 2), rows column-major vec(F)
+            out[e] += wq * np.prod(h) * (Dth.T @ Gw.T.ravel())
+    return out
+
+
 def hex_box(nx, ny=None, nz=None):
     """Structured box of nx*ny*nz unit-spacing-scaled hexes on [0,1]^3 (corner order above)."""
     ny = nx if ny is None else ny

@@ -1,7 +1,8 @@
 """Tricubic Hermite hexes on the GPU path (VolumetricFemEnergy[NeoHookean, HexHermiteBasis,
 GaussLegendre3D[n]]): energy, gradient and Exact Hessian over the 24 physical DOFs per vertex
 against the Hermite oracle (the two-box fixture of the reference's hex force test and a
-structured box), the feasible step, the construction checks, and Newton with the Exact Hessian."""
+structured box), the feasible step, the construction checks, Newton with the Exact Hessian, and
+the theta force response and adjoint."""
 
 import numpy as np
 import pytest
@@ -91,7 +92,7 @@ def test_construction_and_unsupported_requests():
     with pytest.raises(ValueError):  # the Q1 map width
         fem.VolumetricFemEnergy[fem.NeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[2]](
             dof.VertexDofMap(topo, 3), HERMITE_X, None, HERMITE_THETA)
-    Resp = fem.VolumetricFemForceMaterialResponseHexQ1
+    Resp = fem.VolumetricFemForceMaterialResponseHexQ1  # the Q1 response rejects the Hermite map width
     with pytest.raises(ValueError):
         Resp(dof.ConstantDofMap(topo, 2), dof.VertexDofMap(topo, 24), HERMITE_X, hermite_state(), None)
     th = np.tile([3.0, 4.0], (2, 1))
@@ -121,3 +122,73 @@ def test_hermite_newton_exact_hessian():
     _, g, _ = oracle.hex_hermite_eval(X, cells, theta, np.asarray(r.x), points_per_axis=4, hessian=False)
     free = np.setdiff1d(np.arange(n), fixed)
     assert np.abs((g - f)[free]).max() <= 1e-7 * np.abs(f).max()
+
+
+@pytest.mark.parametrize("n", [2, 4])
+def test_hermite_theta_vjp(n):
+    """The Hermite force's theta VJP over physical DOFs against the oracle, per element and summed."""
+    x = hermite_state(0.05)
+    w = np.cos(np.arange(x.size) + 0.7)
+    topo = mesh.HexTopology(12, HERMITE_CELLS)
+    Resp = fem.VolumetricFemForceMaterialResponse[fem.NeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[n]]
+    ref = oracle.hex_hermite_force_vjp_theta(HERMITE_X, HERMITE_CELLS, [1.0, 1.0], x, w, points_per_axis=n)
+    per = Resp(dof.ElementDofMap(topo, 2), dof.VertexDofMap(topo, 24), HERMITE_X, x, None)
+    assert rel_err(per.eval_vjp(np.tile(HERMITE_THETA, 2), w).reshape(2, 2), ref) <= 1e-12
+    shared = Resp(dof.ConstantDofMap(topo, 2), dof.VertexDofMap(topo, 24), HERMITE_X, x, None)
+    assert rel_err(shared.eval_vjp(HERMITE_THETA, w), ref.sum(0)) <= 1e-12
+
+
+def test_hermite_theta_adjoint_matches_finite_differences():
+    """Per-element [lambda, mu] of a 2x2x1 box of unit Hermite cells (4 points per axis) as a torch
+    leaf, loss |x*(theta) - x_t|^2, with the bottom vertices and every vertex's mixed-derivative
+    slots held (the free Hessian's condition is then ~1e3, not ~1e7) and a downward load on the
+    value slots: the adjoint gradient against five-point differences (step 1e-4 relative to
+    theta) along 6 seeded directions, to 1e-6."""
+    from litepgo_b200 import torch as bridge
+
+    X, cells = mesh.make_hex_box(2, 2, 1)
+    X = X * np.array([2.0, 2.0, 1.0])
+    n, T = 24 * X.shape[0], cells.shape[0]
+    rng = np.random.default_rng(3)
+    mu = 3e4 * (1 + 0.5 * rng.random(T))
+    theta0 = np.column_stack([4 * mu, mu])
+    f = np.zeros(n)
+    value = (24 * np.arange(X.shape[0])[:, None] + np.arange(3)).ravel()
+    f[value] = -2e3 * (value % 3 == 2)
+    base = (24 * np.flatnonzero(X[:, 2] == 0)[:, None] + np.arange(24)).ravel()
+    mixed = (24 * np.arange(X.shape[0])[:, None] + np.arange(12, 24)).ravel()
+    fixed = np.union1d(base, mixed)
+    f[fixed] = 0
+    load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -f)
+    shared = hermite_energy(X, cells, theta0, 4)
+    topo = mesh.HexTopology(X.shape[0], cells)
+    Resp = fem.VolumetricFemForceMaterialResponse[fem.NeoHookean, fem.HexHermiteBasis, fem.GaussLegendre3D[4]]
+
+    def make_energy(p):
+        shared.set_theta(p.reshape(T, 2))
+        return energy.WeightedSumEnergy([(shared, 1.0), (load, 1.0)])
+
+    def make_response(u):
+        return Resp(dof.ElementDofMap(topo, 2), dof.VertexDofMap(topo, 24), X, u, None)
+
+    opts = solver.NewtonOptions(gradient_tolerance=1e-12 * np.abs(f).max(), stop_rule="max_abs", accept_rule="noise",
+                                max_iterations=100, cg_tolerance=1e-3, hessian=Exact)
+    model = solver.StaticEquilibriumResponse(2 * T, dof.DofReduction(n, fixed), np.zeros(n), opts, make_energy,
+                                             make_response)
+    x_target = model.eval_value((theta0 * (1 + 0.2 * rng.standard_normal(theta0.shape))).ravel())
+    theta = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+    loss = ((bridge.response(model, theta.reshape(-1)) - torch.as_tensor(x_target)) ** 2).sum()
+    loss.backward()
+    grad = theta.grad.numpy().ravel()
+    th0 = theta0.ravel()
+    warm = solver.StaticEquilibriumResponse(2 * T, dof.DofReduction(n, fixed), model.eval_value(th0), opts,
+                                            make_energy, make_response)
+
+    def L(q):
+        return float(np.sum((warm.eval_value(q) - x_target) ** 2))
+
+    h = 1e-4
+    for _ in range(6):
+        d = rng.standard_normal(2 * T) * th0
+        fd = (8 * (L(th0 + h * d) - L(th0 - h * d)) - (L(th0 + 2 * h * d) - L(th0 - 2 * h * d))) / (12 * h)
+        assert abs(grad @ d - fd) <= 1e-6 * abs(fd)

@@ -73,3 +73,22 @@ def test_sheared_geometry_is_rejected():
         oracle.hermite_box(sheared)
     with pytest.raises(ValueError):
         oracle.hermite_box(X[[1, 0, 3, 2, 5, 4, 7, 6]])
+
+
+def test_theta_vjp_matches_finite_differences():
+    """The oracle's Hermite theta VJP per element against central differences of w . g(u; theta)
+    in each element's [lambda, mu] (g is linear in theta)."""
+    x = hermite_state(0.05)
+    w = np.cos(np.arange(x.size) + 0.7)
+    theta = np.array([[2.0, 3.0], [5.0, 1.5]])
+    vjp = oracle.hex_hermite_force_vjp_theta(HERMITE_X, HERMITE_CELLS, theta, x, w)
+    h = 1e-3
+    for e in range(2):
+        for c in range(2):
+            tp, tm = theta.copy(), theta.copy()
+            tp[e, c] += h
+            tm[e, c] -= h
+            gp = oracle.hex_hermite_eval(HERMITE_X, HERMITE_CELLS, tp, x, hessian=False)[1]
+            gm = oracle.hex_hermite_eval(HERMITE_X, HERMITE_CELLS, tm, x, hessian=False)[1]
+            fd = w @ (gp - gm) / (2 * h)
+            assert abs(vjp[e, c] - fd) <= 1e-9 * (1 + abs(fd))
