@@ -45,3 +45,10 @@ extern "C" int psd_semidefinite9(const double* V, double tol) {
     for (int i = 0; i < 81; ++i) W[i] = V[i];
     return lpg::semidefinite_ldlt<9>(W, tol) ? 1 : 0;
 }
+
+// The same test in FP32 (the mixed-precision tet projection's instantiation).
+extern "C" int psd_semidefinite9f(const float* V, float tol) {
+    float W[81];
+    for (int i = 0; i < 81; ++i) W[i] = V[i];
+    return lpg::semidefinite_ldlt<9>(W, tol) ? 1 : 0;
+}

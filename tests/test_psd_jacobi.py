@@ -27,6 +27,7 @@ def psd(tmp_path_factory):
     lib.psd_project.argtypes = [ctypes.c_int, _dp, _dp, _dp]
     lib.psd_round_pairs.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.psd_semidefinite9.argtypes = [_dp, ctypes.c_double]
+    lib.psd_semidefinite9f.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_float]
 
     def run(H):
         H = np.ascontiguousarray(H, dtype=np.float64)
@@ -146,3 +147,23 @@ def test_semidefinite_test_edge_cases(psd):
     assert run(np.r_[-1e-6, np.linspace(0.1, 2, 8)]) == 0              # a small negative eigenvalue
     assert run(np.r_[-1.0, np.zeros(2), np.linspace(0.1, 2, 6)]) == 0
     assert run(np.zeros(9)) == 1
+
+
+def test_semidefinite_test_in_fp32(psd):
+    """The FP32 instantiation (tol 64 eps_f max|diag|): semi-definite and singular semi-definite
+    matrices pass, a clearly negative eigenvalue fails."""
+    lib = psd.lib
+    fp = ctypes.POINTER(ctypes.c_float)
+    rng = np.random.default_rng(5)
+    Q, _ = np.linalg.qr(rng.standard_normal((9, 9)))
+
+    def run(lam):
+        A = np.ascontiguousarray(((Q * lam) @ Q.T).astype(np.float32))
+        A = np.ascontiguousarray(0.5 * (A + A.T))
+        tol = np.float32(64 * np.finfo(np.float32).eps * np.abs(np.diag(A)).max())
+        return lib.psd_semidefinite9f(A.ctypes.data_as(fp), tol)
+
+    assert run(np.linspace(0.1, 2, 9)) == 1
+    assert run(np.r_[np.zeros(3), np.linspace(0.1, 2, 6)]) == 1
+    assert run(np.r_[-1e-2, np.linspace(0.1, 2, 8)]) == 0
+
