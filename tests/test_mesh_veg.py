@@ -143,3 +143,19 @@ def test_unstructured_mesh_round_trip_and_plan(tmp_path):
     np.testing.assert_array_equal(data.cells, tets)
     ncl, max_rows, max_els, evals, entries = test_host.cluster_summary(data.positions, data.cells)
     assert entries == 16 * tets.shape[0] and ncl >= 1 and max_rows <= 24 and max_els <= 224
+
+
+def test_cubic_veg_feeds_the_hex_and_hermite_plans(tmp_path):
+    """A CUBIC VEG file read back gives cells the Q1 (8-node) and tricubic Hermite (64-node)
+    assembly plans accept with all their invariants (the reference's Hermite examples read
+    assets/box-hex.veg the same way)."""
+    import test_host
+
+    X, cells = hex_grid(3)
+    path = tmp_path / "grid.veg"
+    mesh.write_veg(path, mesh.HexMesh(X, cells))
+    data = mesh.read_veg(path)
+    T = data.cells.shape[0]
+    assert test_host.cell_summary(data.positions, data.cells, 8)[4] == 64 * T
+    nodes = test_host.hermite_cells(data.cells)
+    assert test_host.cell_summary(np.zeros((8 * data.positions.shape[0], 3)), nodes, 64)[4] == 64 * 64 * T
