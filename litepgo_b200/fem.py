@@ -201,6 +201,19 @@ class _InterpolatedResponseTetP1:
         return self.coefficients.T @ TetP1Basis.eval_N(xi)
 
 
+class _InterpolatedResponseHexQ1(_InterpolatedResponseTetP1):
+    """xi -> coefficients^T N(xi) over the trilinear hex basis (8 corner coefficients)."""
+
+    def __init__(self, coefficients):
+        c = np.asarray(coefficients, dtype=np.float64)
+        if c.ndim != 2 or c.shape[0] != 8:
+            raise ValueError("InterpolatedResponse[HexQ1Basis] requires (8, k) coefficients")
+        self.coefficients = c.copy()
+
+    def eval_value(self, xi):
+        return self.coefficients.T @ HexQ1Basis.eval_N(xi)
+
+
 class Template:
     """A template of the reference indexed by argument tuple, e.g. VolumetricFemEnergy[M, B, Q]."""
 
@@ -230,7 +243,8 @@ class Template:
         return f"<template litepgo_b200.fem.{self.__name__}>"
 
 
-InterpolatedResponse = Template("InterpolatedResponse", {(TetP1Basis,): _InterpolatedResponseTetP1})
+InterpolatedResponse = Template("InterpolatedResponse", {(TetP1Basis,): _InterpolatedResponseTetP1,
+                                                          (HexQ1Basis,): _InterpolatedResponseHexQ1})
 
 _CENTROID = np.full(3, 0.25)
 
@@ -259,6 +273,61 @@ def _sample_fields(fields, count, width, what):
         if key not in cache:
             cache[key] = np.asarray(f.eval_value(_CENTROID), dtype=np.float64)
         out[e] = cache[key]
+    if len(cache) == 1:
+        return out[0].copy()
+    return out
+
+
+def _hex_rest_positions(fields, cells, num_vertices):
+    """Vertex rest positions (V, 3) of a hex mesh from a (V, 3) array or from per-element fields
+    with (8, 3) corner coefficients (InterpolatedResponse[HexQ1Basis]); per-element corners must
+    agree at shared vertices (the hex path keeps one position per vertex)."""
+    if isinstance(fields, np.ndarray) or (isinstance(fields, (list, tuple)) and fields and
+                                          not hasattr(fields[0], "coefficients")):
+        X = np.asarray(fields, dtype=np.float64)
+        if X.size != 3 * num_vertices:
+            raise ValueError("VolumetricFemEnergy: rest positions must be (V, 3)")
+        return np.ascontiguousarray(X.reshape(-1, 3))
+    fields = list(fields)
+    if len(fields) != cells.shape[0]:
+        raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
+    X = np.full((num_vertices, 3), np.nan)
+    for e, f in enumerate(fields):
+        c = np.asarray(getattr(f, "coefficients", None), dtype=np.float64)
+        if c.shape != (8, 3):
+            raise ValueError("VolumetricFemEnergy: hex rest fields need (8, 3) corner coefficients")
+        for a in range(8):
+            v = cells[e, a]
+            if np.all(np.isnan(X[v])):
+                X[v] = c[a]
+            elif not np.array_equal(X[v], c[a]):
+                raise ValueError("VolumetricFemEnergy: per-element hex rest fields must agree at shared vertices")
+    if np.any(np.isnan(X)):
+        raise ValueError("VolumetricFemEnergy: a vertex of no element has no rest position")
+    return X
+
+
+def _sample_fields_hex(fields, count, width, what, points):
+    """Per-element values of fields that must be constant over each hex: arrays as in
+    _sample_fields; spatial responses are evaluated at every quadrature point and must agree to
+    1e-12 (the hex path keeps theta and Fp per element)."""
+    if fields is None or isinstance(fields, np.ndarray) or (isinstance(fields, (list, tuple)) and fields and
+                                                            isinstance(fields[0], (int, float, np.floating))):
+        return _sample_fields(fields, count, width, what)
+    fields = list(fields)
+    if len(fields) != count:
+        raise ValueError("VolumetricFemEnergy: incompatible map or response counts")
+    out = np.empty((count, width))
+    cache = {}
+    for e, f in enumerate(fields):
+        if f is None or getattr(f, "num_inputs", 3) != 3 or getattr(f, "num_outputs", width) != width:
+            raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
+        if id(f) not in cache:
+            vals = np.array([np.asarray(f.eval_value(xi), dtype=np.float64) for xi in points])
+            if np.abs(vals - vals[0]).max() > 1e-12 * max(1.0, np.abs(vals).max()):
+                raise ValueError(f"VolumetricFemEnergy: hex meshes take element-constant {what} fields")
+            cache[id(f)] = vals[0]
+        out[e] = cache[id(f)]
     if len(cache) == 1:
         return out[0].copy()
     return out
@@ -754,13 +823,12 @@ class VolumetricFemEnergyHexQ1(VolumetricFemEnergyTetP1):
         cells = np.ascontiguousarray(displacement_map.cells, dtype=np.int32)
         if cells.ndim != 2 or cells.shape[1] != 8:
             raise ValueError("VolumetricFemEnergy: HexQ1Basis needs 8 vertices per cell")
-        fp = _sample_fields(Fp, cells.shape[0], 9, "Fp")
+        points = (GaussLegendre3D_2 if self.points_per_axis == 2 else GaussLegendre3D_4).points()
+        fp = _sample_fields_hex(Fp, cells.shape[0], 9, "Fp", points)
         if fp is not None and not np.all(np.asarray(fp).reshape(-1, 9) == np.eye(3).ravel()):
             raise ValueError("VolumetricFemEnergy: hex meshes take no plastic field here")
-        X = np.ascontiguousarray(np.asarray(rest_position_fields, dtype=np.float64).reshape(-1, 3))
-        if X.shape[0] != displacement_map.num_vertices:
-            raise ValueError("VolumetricFemEnergy: rest positions must be (V, 3)")
-        th = _sample_fields(theta, cells.shape[0], 2, "theta")
+        X = _hex_rest_positions(rest_position_fields, cells, displacement_map.num_vertices)
+        th = _sample_fields_hex(theta, cells.shape[0], 2, "theta", points)
         if th is None:
             raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
         self.batch_size = int(batch_size)
@@ -890,10 +958,16 @@ class VolumetricFemEnergyPyMaterialTetP1(Energy):
             raise ValueError("MeshEnergy: invalid batch size")
         T = displacement_map.num_elements
         k = mat.num_parameters
-        th = _sample_fields(theta, T, k, "theta") if k > 0 else np.zeros((T, 0))
+        per = getattr(self._geometry_cls, "points_per_axis", None)
+        if per is None:
+            sample = _sample_fields
+        else:  # hexes: element-constant fields, checked at every quadrature point
+            points = (GaussLegendre3D_2 if per == 2 else GaussLegendre3D_4).points()
+            sample = lambda f, c, w, what: _sample_fields_hex(f, c, w, what, points)  # noqa: E731
+        th = sample(theta, T, k, "theta") if k > 0 else np.zeros((T, 0))
         if th is None:
             raise ValueError("VolumetricFemEnergy: incompatible spatial responses")
-        fp = _sample_fields(Fp, T, 9, "Fp")
+        fp = sample(Fp, T, 9, "Fp")
         fp = np.tile(np.eye(3).ravel(), (T, 1)) if fp is None else np.array(np.broadcast_to(fp, (T, 9)))
         # The geometry handle: the native records carry only rest geometry here.
         self._geo = self._geometry_cls(displacement_map, rest_position_fields, None, np.array([1.0, 1.0]),

@@ -105,3 +105,29 @@ def test_hermite_and_hex_templates():
         np.testing.assert_allclose(fem.HexHermiteBasis.eval_dN_dxi(xi), dN0, rtol=0, atol=1e-14)
         # The value functions alone sum to one (the reference's tests/python/test_fem.py:43).
         assert abs(fem.HexHermiteBasis.eval_N(xi)[0::8].sum() - 1.0) < 1e-14
+
+
+def test_hex_fields_as_the_reference_builds_them():
+    """Reference-style hex inputs (its examples/fem/equilibrium/hex_hermite_corner_pull.py): per-element
+    InterpolatedResponse[HexQ1Basis] rest fields become vertex positions, constant AffineResponse
+    theta and Fp fields become per-element values; inconsistent corners and varying fields raise."""
+    from litepgo_b200 import mesh
+    from litepgo_b200.energy import AffineResponse
+
+    X, cells = mesh.make_hex_box(2, 1, 1)
+    Field = fem.InterpolatedResponse[fem.HexQ1Basis]
+    fields = [Field(X[c]) for c in cells]
+    np.testing.assert_allclose(fields[0].eval_value(np.full(3, 0.5)), X[cells[0]].mean(0), atol=1e-15)
+    np.testing.assert_array_equal(fem._hex_rest_positions(fields, cells, X.shape[0]), X)
+    bad = [Field(X[cells[0]]), Field(X[cells[1]] + [0, 0, 1e-9])]
+    with pytest.raises(ValueError, match="agree"):
+        fem._hex_rest_positions(bad, cells, X.shape[0])
+    pts = fem.GaussLegendre3D[2].points()
+    theta_field = AffineResponse(np.zeros((2, 3)), np.array([2.0, 3.0]))
+    np.testing.assert_array_equal(fem._sample_fields_hex([theta_field] * 2, 2, 2, "theta", pts), [2.0, 3.0])
+    varying = AffineResponse(np.array([[1.0, 0, 0], [0, 0, 0]]), np.array([2.0, 3.0]))
+    with pytest.raises(ValueError, match="element-constant"):
+        fem._sample_fields_hex([varying] * 2, 2, 2, "theta", pts)
+    # Interpolated theta from equal nodal values is constant (the reference's test_fem.py:247-257).
+    q1 = Field(np.tile([2.0, 3.0], (8, 1)))
+    np.testing.assert_allclose(fem._sample_fields_hex([q1] * 2, 2, 2, "theta", pts), [2.0, 3.0], atol=1e-15)
