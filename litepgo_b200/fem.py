@@ -41,6 +41,9 @@ __all__ = [
     "VolumetricFemEnergyPyMaterialTetP1",
     "HexQ1Basis",
     "HexHermiteBasis",
+    "BasisDofTransform",
+    "CoefficientInfo",
+    "DeformationGradientResponse",
     "GaussLegendre3D",
     "VolumetricFemEnergyHexQ1",
     "VolumetricFemEnergyHexHermite",
@@ -54,10 +57,33 @@ class NeoHookean:
     num_parameters = 2
 
 
+class CoefficientInfo:
+    """Where a basis coefficient lives (basis.hpp's CoefficientInfo): the reference point and the
+    derivative order per axis of the functional it interpolates."""
+
+    def __init__(self, point, derivative_orders):
+        self.point = np.asarray(point, dtype=np.float64)
+        self.derivative_orders = tuple(int(o) for o in derivative_orders)
+
+    def __repr__(self):
+        return f"CoefficientInfo(point={self.point.tolist()}, derivative_orders={self.derivative_orders})"
+
+
+def _check_index(cls, i):
+    if not 0 <= int(i) < cls.num_basis_functions:
+        raise IndexError(f"{cls.__name__}::coefficient_info: index out of range")
+    return int(i)
+
+
 class TetP1Basis:
     """Linear tetrahedron shape functions (tet_p1_basis.cpp:7-15)."""
 
     num_basis_functions = 4
+    _points = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.float64)
+
+    @classmethod
+    def coefficient_info(cls, i):
+        return CoefficientInfo(cls._points[_check_index(cls, i)], (0, 0, 0))
 
     @staticmethod
     def eval_N(xi):
@@ -75,6 +101,10 @@ class HexQ1Basis:
 
     num_basis_functions = 8
     corners = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+
+    @classmethod
+    def coefficient_info(cls, i):
+        return CoefficientInfo(cls.corners[_check_index(cls, i)], (0, 0, 0))
 
     @classmethod
     def eval_N(cls, xi):
@@ -112,6 +142,11 @@ class HexHermiteBasis:
     @classmethod
     def _index(cls, row):
         return 2 * cls.corners[row // 8] + cls.orders[row % 8]
+
+    @classmethod
+    def coefficient_info(cls, i):
+        i = _check_index(cls, i)
+        return CoefficientInfo(cls.corners[i // 8], cls.orders[i % 8])
 
     @classmethod
     def eval_N(cls, xi):
@@ -197,12 +232,20 @@ class _InterpolatedResponseTetP1:
     def num_outputs(self):
         return self.coefficients.shape[1]
 
+    basis = TetP1Basis
+
     def eval_value(self, xi):
-        return self.coefficients.T @ TetP1Basis.eval_N(xi)
+        return self.coefficients.T @ self.basis.eval_N(xi)
+
+    def eval_jacobian(self, xi):
+        """(k, 3): d value / d xi."""
+        return self.coefficients.T @ self.basis.eval_dN_dxi(xi)
 
 
 class _InterpolatedResponseHexQ1(_InterpolatedResponseTetP1):
     """xi -> coefficients^T N(xi) over the trilinear hex basis (8 corner coefficients)."""
+
+    basis = HexQ1Basis
 
     def __init__(self, coefficients):
         c = np.asarray(coefficients, dtype=np.float64)
@@ -210,8 +253,101 @@ class _InterpolatedResponseHexQ1(_InterpolatedResponseTetP1):
             raise ValueError("InterpolatedResponse[HexQ1Basis] requires (8, k) coefficients")
         self.coefficients = c.copy()
 
+
+class _InterpolatedResponseHexHermite(_InterpolatedResponseTetP1):
+    """xi -> coefficients^T N(xi) over the tricubic Hermite basis (64 reference coefficients,
+    index 8 corner + slot)."""
+
+    basis = HexHermiteBasis
+
+    def __init__(self, coefficients):
+        c = np.asarray(coefficients, dtype=np.float64)
+        if c.ndim != 2 or c.shape[0] != 64:
+            raise ValueError("InterpolatedResponse[HexHermiteBasis] requires (64, k) coefficients")
+        self.coefficients = c.copy()
+
+
+class DeformationGradientResponse:
+    """xi -> vec(F) (column-major) with F = I + (du/dxi)(dX/dxi)^-1 for a displacement field u and a
+    rest-position field X over the reference cell (deformation_gradient_response.hpp)."""
+
+    def __init__(self, displacement, rest_position):
+        if displacement.num_outputs != 3 or rest_position.num_outputs != 3:
+            raise ValueError("DeformationGradientResponse requires three-component fields")
+        self.displacement, self.rest_position = displacement, rest_position
+        self.num_inputs, self.num_outputs = 3, 9
+
     def eval_value(self, xi):
-        return self.coefficients.T @ HexQ1Basis.eval_N(xi)
+        J = self.rest_position.eval_jacobian(xi)
+        F = np.eye(3) + self.displacement.eval_jacobian(xi) @ np.linalg.inv(J)
+        return F.ravel(order="F")
+
+
+class _NodalDofTransform:
+    """BasisDofTransform for nodal bases (basis_dof_transform.hpp:15-57): 3 DOFs per vertex, the
+    coefficients are the DOFs, and the pullback is the identity."""
+
+    dofs_per_vertex = 3
+    nodes = None
+
+    def __init__(self, geometry):
+        if getattr(geometry, "num_inputs", 3) != 3 or getattr(geometry, "num_outputs", 3) != 3:
+            raise ValueError("BasisDofTransform: geometry must map R3 to R3")
+
+    def to_coefficients(self, local):
+        a = np.asarray(local, dtype=np.float64)
+        if a.shape != (self.nodes, 3) or not np.all(np.isfinite(a)):
+            raise ValueError("BasisDofTransform: invalid nodal DOFs")
+        return a.copy()
+
+    def pullback(self, gradient=None, hessian=None):
+        return (None if gradient is None else np.asarray(gradient, dtype=np.float64).copy(),
+                None if hessian is None else np.asarray(hessian, dtype=np.float64).copy())
+
+
+class _TetP1DofTransform(_NodalDofTransform):
+    nodes = 4
+
+
+class _HexQ1DofTransform(_NodalDofTransform):
+    nodes = 8
+
+
+class _HexHermiteDofTransform:
+    """BasisDofTransform<HexHermiteBasis> (basis_dof_transform.hpp:59-148): the geometry must be a
+    positive axis-aligned box in corner order (its corners checked to 1e-12); per vertex 24
+    physical DOFs (slots u, u_X, u_Y, u_Z, u_XY, u_XZ, u_YZ, u_XYZ) scaled to reference
+    coefficients by 1, hx, hy, hz, hx hy, hx hz, hy hz, hx hy hz; the pullback scales a gradient
+    (s g) and a Hessian (S H S) by the same factors."""
+
+    dofs_per_vertex = 24
+
+    def __init__(self, geometry):
+        if getattr(geometry, "num_inputs", 3) != 3 or getattr(geometry, "num_outputs", 3) != 3:
+            raise ValueError("Hermite DOFs require three reference components")
+        nodes = np.array([np.asarray(geometry.eval_value(HexQ1Basis.corners[v]), dtype=np.float64)
+                          for v in range(8)])
+        if nodes.shape != (8, 3) or not np.all(np.isfinite(nodes)):
+            raise ValueError("Hermite DOFs require finite three-component reference values")
+        origin = nodes[0]
+        h = np.array([nodes[1, 0] - origin[0], nodes[3, 1] - origin[1], nodes[4, 2] - origin[2]])
+        if not np.all(np.isfinite(h)) or np.any(h <= 0):
+            raise ValueError("Hermite DOF transform requires positive axis-aligned box dimensions")
+        if np.abs((nodes - origin) / h - HexQ1Basis.corners).max() > 1e-12:
+            raise ValueError("Hermite DOF transform requires axis-aligned boxes in Hex corner order")
+        slots = np.array([1, h[0], h[1], h[2], h[0] * h[1], h[0] * h[2], h[1] * h[2], h[0] * h[1] * h[2]])
+        self.scales = np.tile(np.repeat(slots, 3), 8)
+
+    def to_coefficients(self, local):
+        a = np.asarray(local, dtype=np.float64)
+        if a.shape != (8, 24) or not np.all(np.isfinite(a)):
+            raise ValueError("Hex Hermite requires finite 8x24 physical DOFs")
+        return (a.ravel() * self.scales).reshape(64, 3)
+
+    def pullback(self, gradient=None, hessian=None):
+        g = None if gradient is None else np.asarray(gradient, dtype=np.float64) * self.scales
+        H = None if hessian is None else self.scales[:, None] * np.asarray(hessian, dtype=np.float64) * self.scales
+        return g, H
 
 
 class Template:
@@ -244,7 +380,11 @@ class Template:
 
 
 InterpolatedResponse = Template("InterpolatedResponse", {(TetP1Basis,): _InterpolatedResponseTetP1,
-                                                          (HexQ1Basis,): _InterpolatedResponseHexQ1})
+                                                          (HexQ1Basis,): _InterpolatedResponseHexQ1,
+                                                          (HexHermiteBasis,): _InterpolatedResponseHexHermite})
+BasisDofTransform = Template("BasisDofTransform", {(TetP1Basis,): _TetP1DofTransform,
+                                                    (HexQ1Basis,): _HexQ1DofTransform,
+                                                    (HexHermiteBasis,): _HexHermiteDofTransform})
 
 _CENTROID = np.full(3, 0.25)
 

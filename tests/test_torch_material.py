@@ -131,3 +131,39 @@ def test_hex_fields_as_the_reference_builds_them():
     # Interpolated theta from equal nodal values is constant (the reference's test_fem.py:247-257).
     q1 = Field(np.tile([2.0, 3.0], (8, 1)))
     np.testing.assert_allclose(fem._sample_fields_hex([q1] * 2, 2, 2, "theta", pts), [2.0, 3.0], atol=1e-15)
+
+
+def test_basis_dof_transform_and_deformation_gradient():
+    """The Hermite DOF convention through the basis utilities (the reference's
+    tests/python/test_fem.py:472-496 scenario): on an axis-aligned box, an affine displacement's
+    physical slots (u, u_X, u_Y, u_Z, zero mixed derivatives) interpolate to F = I + A at interior
+    points, and the pullback scales by 1, hx, hy, hz, hx hy, hx hz, hy hz, hx hy hz."""
+    size, origin = np.array([2.0, 1.0, 3.0]), np.array([0.5, -1.0, 2.0])
+    X_nodes = origin + size * np.array([fem.HexQ1Basis.coefficient_info(v).point for v in range(8)])
+    X_field = fem.InterpolatedResponse[fem.HexQ1Basis](X_nodes)
+    transform = fem.BasisDofTransform[fem.HexHermiteBasis](X_field)
+    assert transform.dofs_per_vertex == 24
+    A = np.array([[0.1, -0.2, 0.05], [0.3, 0.0, -0.1], [0.02, 0.15, 0.2]])
+    local = np.hstack([X_nodes @ A.T, np.tile(A.T.ravel(), (8, 1)), np.zeros((8, 12))])
+    u_field = fem.InterpolatedResponse[fem.HexHermiteBasis](transform.to_coefficients(local))
+    F = fem.DeformationGradientResponse(u_field, X_field)
+    for xi in ([0.2, 0.7, 0.4], [0.9, 0.1, 0.5]):
+        np.testing.assert_allclose(F.eval_value(np.array(xi)), (np.eye(3) + A).ravel(order="F"), atol=1e-13)
+    gradient, hessian = transform.pullback(gradient=np.ones(192))
+    assert hessian is None
+    hx, hy, hz = size
+    slots = np.array([1, hx, hy, hz, hx * hy, hx * hz, hy * hz, hx * hy * hz])
+    np.testing.assert_allclose(gradient, np.tile(np.repeat(slots, 3), 8))
+    _, H = transform.pullback(hessian=np.ones((192, 192)))
+    np.testing.assert_allclose(H, np.outer(np.tile(np.repeat(slots, 3), 8), np.tile(np.repeat(slots, 3), 8)))
+    nodal = fem.BasisDofTransform[fem.HexQ1Basis](X_field)
+    assert nodal.dofs_per_vertex == 3
+    np.testing.assert_array_equal(nodal.to_coefficients(X_nodes), X_nodes)
+    sheared = X_nodes.copy()
+    sheared[:, 0] += 0.2 * sheared[:, 1]
+    with pytest.raises(ValueError):
+        fem.BasisDofTransform[fem.HexHermiteBasis](fem.InterpolatedResponse[fem.HexQ1Basis](sheared))
+    info = fem.HexHermiteBasis.coefficient_info(8 * 6 + 7)
+    assert info.point.tolist() == [1, 1, 1] and info.derivative_orders == (1, 1, 1)
+    with pytest.raises(IndexError):
+        fem.HexHermiteBasis.coefficient_info(64)
