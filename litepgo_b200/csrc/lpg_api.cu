@@ -99,6 +99,18 @@ void upload_plan(lpg_fem& hh, int V, int T) {
         m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);
         m.cl_max_ents = std::max(m.cl_max_ents, p.cl_ent_ptr[c + 1] - p.cl_ent_ptr[c]);
     }
+    // The block gather stages a cluster's element ids, row table, slot words and contributor
+    // lists in shared memory: a mesh whose largest cluster would not fit is rejected here rather
+    // than at its first evaluation.
+    const size_t gather_bytes = (static_cast<size_t>(kClusterElems) + 4 * kClusterRows) * sizeof(int) +
+                                (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16 +
+                                2 * static_cast<size_t>(m.cl_max_ents);
+    int optin = 0;
+    LPG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    if (gather_bytes > static_cast<size_t>(optin))
+        fail(LPG_EINVAL, "mesh valence too high for the assembly plan: a cluster needs " +
+                             std::to_string(gather_bytes / 1024) + " KB of shared memory (device limit " +
+                             std::to_string(optin / 1024) + " KB)");
 }
 
 // Entry points whose kernels exist for tet meshes only.
