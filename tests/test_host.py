@@ -261,11 +261,15 @@ def hermite_cells(cells):
     return (8 * cells[:, :, None] + np.arange(8)).reshape(-1, 64).astype(np.int32)
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 2, 2), (4, 3, 2)])
-def test_hermite_cluster_plan_invariants(shape):
+@pytest.mark.parametrize("shape,ragged", [((1, 1, 1), False), ((3, 2, 2), False), ((4, 3, 2), False),
+                                          ((5, 4, 3), True)])
+def test_hermite_cluster_plan_invariants(shape, ragged):
     """The assembly plan of 64-node cells (two 16-bit words per contributor, clusters of at most
-    one vertex's eight rows): every invariant the library checks, and 64^2 contributors per cell."""
+    one vertex's eight rows): every invariant the library checks, and 64^2 contributors per cell;
+    ragged: 40 % of the hexes removed (irregular valence, vertices of no cell)."""
     X, cells = mesh.make_hex_box(*shape)
+    if ragged:
+        cells = cells[np.random.default_rng(2).random(cells.shape[0]) < 0.6]
     nodes = hermite_cells(cells)
     ncl, max_rows, max_els, evals, entries = cell_summary(np.zeros((8 * X.shape[0], 3)), nodes, 64)
     assert entries == 64 * 64 * cells.shape[0]
