@@ -452,7 +452,7 @@ int lpg_fem_create_hex_hermite(int V, const double* X, int T, const int32_t* cel
         const int n = points_per_axis, nq = n * n * n;
         double t1[4], w1[4];
         gauss_legendre_01(n, t1, w1);
-        std::vector<double> qt(193 * static_cast<size_t>(nq));
+        std::vector<double> qt(kHermiteTable * static_cast<size_t>(nq));
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j)
                 for (int k = 0; k < n; ++k) {
@@ -471,11 +471,11 @@ int lpg_fem_create_hex_hermite(int V, const double* X, int T, const int32_t* cel
                     for (int b = 0; b < 64; ++b) {
                         int ix[3];
                         for (int d = 0; d < 3; ++d) ix[d] = 2 * kHexCorner[b / 8][d] + order[b % 8][d];
-                        qt[193 * q + 3 * b] = df[0][ix[0]] * f[1][ix[1]] * f[2][ix[2]];
-                        qt[193 * q + 3 * b + 1] = f[0][ix[0]] * df[1][ix[1]] * f[2][ix[2]];
-                        qt[193 * q + 3 * b + 2] = f[0][ix[0]] * f[1][ix[1]] * df[2][ix[2]];
+                        qt[kHermiteTable * q + 3 * b] = df[0][ix[0]] * f[1][ix[1]] * f[2][ix[2]];
+                        qt[kHermiteTable * q + 3 * b + 1] = f[0][ix[0]] * df[1][ix[1]] * f[2][ix[2]];
+                        qt[kHermiteTable * q + 3 * b + 2] = f[0][ix[0]] * f[1][ix[1]] * df[2][ix[2]];
                     }
-                    qt[193 * q + 192] = w1[i] * w1[j] * w1[k];
+                    qt[kHermiteTable * q + 192] = w1[i] * w1[j] * w1[k];
                 }
         std::vector<double> th(2 * static_cast<size_t>(T));
         for (int e = 0; e < T; ++e)

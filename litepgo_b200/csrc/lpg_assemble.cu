@@ -2259,8 +2259,6 @@ __global__ void __launch_bounds__(256) hex_feasible_kernel(const DevMesh m, cons
 //   g_b = sum_q w P G_b,   H_ab = sum_q w [mu (G_a . G_b) I + lambda h_a h_b^T - p h_b h_a^T], h = F^-T G.
 // The point table holds, per point, the 64 x 3 reference derivatives and the weight (193 values).
 // ---------------------------------------------------------------------------
-constexpr int kHermiteTable = 193;
-
 __device__ __forceinline__ double hermite_slot_scale(int slot, double hx, double hy, double hz) {
     switch (slot) {
     case 0: return 1.0;

@@ -207,6 +207,7 @@ constexpr int kProjRecord = 90;
 // Values per element of the hex block scratch: 36 blocks (a <= b of 8 vertices) of 3x3.
 constexpr int kHexRecord = 324;
 constexpr int kHermiteRecord = 2080 * 9; // tricubic Hermite hex: 64 nodes, 2080 blocks (a <= b)
+constexpr int kHermiteTable = 193;       // per quadrature point: 64 x 3 reference derivatives, weight
 // per_elem (T doubles, optional) receives each element's step.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
                      double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr);
