@@ -92,3 +92,21 @@ def test_theta_vjp_matches_finite_differences():
             gm = oracle.hex_hermite_eval(HERMITE_X, HERMITE_CELLS, tm, x, hessian=False)[1]
             fd = w @ (gp - gm) / (2 * h)
             assert abs(vjp[e, c] - fd) <= 1e-9 * (1 + abs(fd))
+
+
+@pytest.mark.parametrize("kind", ["q1", "hermite"])
+def test_theta_vjp_reproduces_the_force(kind):
+    """g is linear in theta, so w . g(u; theta) = sum_e theta_e . vjp_e(w) (the reference's
+    tests/python/test_material_force_response.py: the force response equals the energy gradient)."""
+    theta = np.array([[2.0, 3.0], [5.0, 1.5]])
+    if kind == "q1":
+        from test_oracle_hex import HEX_CELLS, HEX_X, hex_states
+
+        X, cells, x = HEX_X, HEX_CELLS, hex_states()[2]
+        g = oracle.hex_eval(X, cells, theta, x, hessian=False)[1]
+        vjp = oracle.hex_force_vjp_theta(X, cells, theta, x, g)
+    else:
+        X, cells, x = HERMITE_X, HERMITE_CELLS, hermite_state(0.05)
+        g = oracle.hex_hermite_eval(X, cells, theta, x, hessian=False)[1]
+        vjp = oracle.hex_hermite_force_vjp_theta(X, cells, theta, x, g)
+    assert abs((vjp * theta).sum() - g @ g) <= 1e-12 * (g @ g)
