@@ -80,7 +80,8 @@ typedef struct lpg_fem* lpg_fem_t;
 /* Message of the last failed call on this thread ("" if none). */
 const char* lpg_last_error(void);
 int lpg_abi_version(void);
-/* Writes a short build description (CUDA version, arch) into buf. */
+/* Writes a short build description (CUDA version, arch, and the number of device allocations
+ * the library has made in this process so far) into buf. */
 int lpg_build_info(char* buf, size_t size);
 
 /*
@@ -233,13 +234,17 @@ int lpg_fem_element_energies(lpg_fem_t h, const double* u, int io_mem, double* e
 int lpg_fem_feasible_step(lpg_fem_t h, const double* u, const double* du, int io_mem, double* alpha);
 
 /*
- * The feasible step of lpg_fem_feasible_step, for callers that cannot allocate device memory
- * when they call it (inside a CUDA stream capture, or under a framework that owns the device
- * memory pool). This entry point has no counterpart in the reference: it is the same
- * computation with its scratch in a fixed ~512 KB array inside the library image instead of
- * a cudaMalloc'd buffer, so it calls no cudaMalloc / cudaFree. u and du are DEVICE arrays of
- * num_dofs doubles; *alpha is written on the host. Limits and rules:
- *   - meshes of at most 16,777,216 tets; larger ones fail with LPG_EINVAL;
+ * The feasible step of lpg_fem_feasible_step, for callers that must not allocate device
+ * memory when they call it: a solver embedded in a framework that owns the device memory pool
+ * (a training loop on a caching allocator, an application with a fixed memory budget), where
+ * a library cudaMalloc mid-step fragments or exceeds that budget. This entry point has no
+ * counterpart in the reference: it is the same computation on tet, hex and Hermite handles,
+ * with its scratch in a fixed ~512 KB array inside the library image instead of a
+ * cudaMalloc'd buffer, so it calls no cudaMalloc / cudaFree. It is synchronous: it returns
+ * once the step is on the host. u and du are DEVICE arrays (device or managed memory on the
+ * handle's GPU) of num_dofs doubles; other pointers fail with LPG_EINVAL. *alpha is written on
+ * the host. Limits and rules:
+ *   - meshes of at most 16,777,216 elements; larger ones fail with LPG_EINVAL;
  *   - the array is shared by every call on a device and keeps the last call's contents
  *     (each call clears what it needs), so calls that overlap on the GPU race: order them;
  *   - the first call on a device looks the array's device address up (cudaGetSymbolAddress

@@ -40,6 +40,9 @@ template <class F> int guarded(F&& f) {
     }
 }
 
+// Device allocations made by the library since the process started (reported by lpg_build_info).
+std::atomic<long long> g_device_allocations{0};
+
 DeviceBuffer::~DeviceBuffer() {
     if (ptr) cudaFree(ptr);
 }
@@ -49,6 +52,7 @@ void* DeviceBuffer::ensure(size_t n) {
     ptr = nullptr;
     bytes = 0;
     LPG_CUDA(cudaMalloc(&ptr, n > 0 ? n : 1));
+    g_device_allocations.fetch_add(1);
     bytes = n;
     return ptr;
 }
@@ -99,17 +103,15 @@ void upload_plan(lpg_fem& hh, int V, int T) {
         m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);
         m.cl_max_ents = std::max(m.cl_max_ents, p.cl_ent_ptr[c + 1] - p.cl_ent_ptr[c]);
     }
-    // The block gather stages a cluster's element ids, row table, slot words and contributor
+    // The assembly kernels stage a cluster's element data, row table, slot words and contributor
     // lists in shared memory: a mesh whose largest cluster would not fit is rejected here rather
     // than at its first evaluation.
-    const size_t gather_bytes = (static_cast<size_t>(kClusterElems) + 4 * kClusterRows) * sizeof(int) +
-                                (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16 +
-                                2 * static_cast<size_t>(m.cl_max_ents);
+    const size_t need = assembly_smem_bytes(m);
     int optin = 0;
     LPG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    if (gather_bytes > static_cast<size_t>(optin))
+    if (need > static_cast<size_t>(optin))
         fail(LPG_EINVAL, "mesh valence too high for the assembly plan: a cluster needs " +
-                             std::to_string(gather_bytes / 1024) + " KB of shared memory (device limit " +
+                             std::to_string(need / 1024) + " KB of shared memory (device limit " +
                              std::to_string(optin / 1024) + " KB)");
 }
 
@@ -271,8 +273,8 @@ int lpg_build_info(char* buf, size_t size) {
         int rt = 0, drv = 0;
         cudaRuntimeGetVersion(&rt);
         cudaDriverGetVersion(&drv);
-        std::snprintf(buf, size, "litepgo_b200 abi %d; CUDA runtime %d, driver %d; built for sm_100a", LPG_ABI_VERSION,
-                      rt, drv);
+        std::snprintf(buf, size, "litepgo_b200 abi %d; CUDA runtime %d, driver %d; built for sm_100a; device allocations %lld",
+                      LPG_ABI_VERSION, rt, drv, g_device_allocations.load());
     });
 }
 

@@ -1049,6 +1049,41 @@ template <typename R> __global__ void clamp_sample_kernel(R* __restrict__ proj, 
     }
 }
 
+// Resident-grid facts of one kernel at one dynamic shared-memory size, cached per device: the
+// shared-memory opt-in (cudaFuncAttributeMaxDynamicSharedMemorySize) is a per-device attribute
+// and the occupancy can differ between devices, so a host thread that drives handles on several
+// GPUs sets the attribute and sizes the grid on each of them.
+constexpr int kMaxDevices = 64;
+struct LaunchCache {
+    size_t smem[kMaxDevices];
+    int resident[kMaxDevices];
+    LaunchCache() {
+        for (int d = 0; d < kMaxDevices; ++d) {
+            smem[d] = ~size_t(0);
+            resident[d] = 0;
+        }
+    }
+};
+// Blocks of `kernel` (threads per block, dynamic shared memory smem) that fit on all SMs of the
+// current device at once; sets the kernel's shared-memory opt-in there first when smem > 0.
+template <typename Kern> int resident_grid(Kern kernel, int threads, size_t smem, LaunchCache& c) {
+    int dev = 0;
+    LPG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) fail(LPG_EINVAL, "device index out of range");
+    if (c.smem[dev] != smem) {
+        int sms = 0, per_sm = 0, optin = 0;
+        LPG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (smem > static_cast<size_t>(optin)) fail(LPG_EINVAL, "mesh cluster needs more shared memory than the GPU has");
+        if (smem > 0)
+            LPG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+        c.resident[dev] = std::max(1, sms * std::max(per_sm, 1));
+        c.smem[dev] = smem;
+    }
+    return c.resident[dev];
+}
+
 // ---------------------------------------------------------------------------
 // Element-once assembly over vertex clusters (Exact Hessian, gradient, energy).
 //
@@ -1326,21 +1361,8 @@ __global__ void __launch_bounds__(kClThreads, MINB) cluster_kernel(const DevMesh
 template <typename R, bool WG, bool WH, int MINB = cl_minb<R>(0)>
 void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = cl_smem_bytes<R, WG, WH>(m);
-    // Resident blocks for this shared-memory size (cached for the last size seen).
-    thread_local size_t cached_sm = 0;
-    thread_local int resident = 0;
-    if (cached_sm != sm) {
-        int dev = 0, sms = 0, per_sm = 0, optin = 0;
-        LPG_CUDA(cudaGetDevice(&dev));
-        LPG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        if (sm > static_cast<size_t>(optin)) fail(LPG_EINVAL, "mesh cluster needs more shared memory than the GPU has");
-        LPG_CUDA(cudaFuncSetAttribute(cluster_kernel<R, WG, WH, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sm)));
-        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_kernel<R, WG, WH, MINB>, kClThreads, sm));
-        resident = std::max(1, sms * std::max(per_sm, 1));
-        cached_sm = sm;
-    }
+    thread_local LaunchCache cache;
+    const int resident = resident_grid(cluster_kernel<R, WG, WH, MINB>, kClThreads, sm, cache);
     const int blocks = std::min(resident, m.ncl);
     if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
     if (blocks > 0) cluster_kernel<R, WG, WH, MINB><<<blocks, kClThreads, sm, s>>>(m, a);
@@ -1461,21 +1483,15 @@ __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh 
     if ((tid & 31) == 0 && st) atomicOr(a.status, st);
 }
 
+size_t block_gather_bytes(const DevMesh& m) {
+    return block_gather_fixed() + (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16 +
+           2 * static_cast<size_t>(m.cl_max_ents);
+}
+
 template <typename R, int K = 4> void launch_block_gather(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
-    const size_t sm = block_gather_fixed() + (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16 +
-                      2 * static_cast<size_t>(m.cl_max_ents);
-    thread_local size_t cached_sm = 0;
-    thread_local int resident = 0;
-    if (cached_sm != sm) {
-        int dev = 0, sms = 0, per_sm = 0;
-        LPG_CUDA(cudaGetDevice(&dev));
-        LPG_CUDA(cudaFuncSetAttribute(block_gather_kernel<R, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sm)));
-        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, block_gather_kernel<R, K>, kClThreads, sm));
-        resident = std::max(1, sms * std::max(per_sm, 1));
-        cached_sm = sm;
-    }
+    const size_t sm = block_gather_bytes(m);
+    thread_local LaunchCache cache;
+    const int resident = resident_grid(block_gather_kernel<R, K>, kClThreads, sm, cache);
     const int blocks = std::min(resident, m.ncl);
     if (blocks > 0) block_gather_kernel<R, K><<<blocks, kClThreads, sm, s>>>(m, a);
     LPG_CUDA(cudaGetLastError());
@@ -2605,6 +2621,12 @@ template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const Eva
 
 } // namespace
 
+size_t assembly_smem_bytes(const DevMesh& m) {
+    const size_t gather = block_gather_bytes(m);
+    if (m.K != 4) return gather;
+    return std::max(gather, std::max(cl_smem_bytes<double, true, true>(m), cl_smem_bytes<float, true, true>(m)));
+}
+
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s) {
     const int units = precision == LPG_PRECISION_F64 ? launch_eval_t<double>(m, hessian, a, s)
                                                       : launch_eval_t<float>(m, hessian, a, s);
@@ -2637,17 +2659,8 @@ namespace {
 template <typename R, int MINB>
 void launch_clamp_t(R* proj, const int* list, const unsigned* count, int max_count, cudaStream_t s) {
     const size_t clamp_sm = sizeof(R) == 8 ? sizeof(R) * kClampVStride * kProjThreads : 0;
-    thread_local int clamp_grid = 0; // one wave of this variant
-    if (clamp_grid == 0) {
-        int dev = 0, sms = 0, per = 0;
-        LPG_CUDA(cudaGetDevice(&dev));
-        LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        if (clamp_sm > 0)
-            LPG_CUDA(cudaFuncSetAttribute(clamp_kernel<R, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(clamp_sm)));
-        LPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, clamp_kernel<R, MINB>, kProjThreads, clamp_sm));
-        clamp_grid = std::max(1, per) * std::max(1, sms);
-    }
+    thread_local LaunchCache cache; // one wave of this variant
+    const int clamp_grid = resident_grid(clamp_kernel<R, MINB>, kProjThreads, clamp_sm, cache);
     const int blocks = (max_count + kProjThreads - 1) / kProjThreads;
     if (blocks > 0) clamp_kernel<R, MINB><<<std::min(clamp_grid, blocks), kProjThreads, clamp_sm, s>>>(proj, list, count);
 }
@@ -2663,12 +2676,8 @@ template <typename R, class Src>
 void launch_project_t(const DevMesh& m, const Src& src, R* proj, unsigned* status, cudaStream_t s, const int* emesh,
                       const int* mesh_exact, int* list, unsigned* count, int clamp_variant) {
     const size_t sm = sizeof(R) * kProjStride * kProjThreads;
-    thread_local bool ready = false;
-    if (!ready) {
-        LPG_CUDA(cudaFuncSetAttribute(project_kernel<R, Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sm)));
-        ready = true;
-    }
+    thread_local LaunchCache cache;
+    resident_grid(project_kernel<R, Src>, kProjThreads, sm, cache);
     const int blocks = (m.T + kProjThreads - 1) / kProjThreads;
     LPG_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
     project_kernel<R, Src><<<blocks, kProjThreads, sm, s>>>(m, src, proj, status, emesh, mesh_exact, list, count);

@@ -187,6 +187,9 @@ struct Tuning {
     bool tuned = false;
 };
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s);
+// Largest dynamic shared memory any assembly kernel of this mesh's cell type needs for its
+// largest cluster (the same formulas the launches use).
+size_t assembly_smem_bytes(const DevMesh& m);
 // Per-element clamped tangents for the projected Hessians (45 values / element, upper triangle).
 // list (T ints) and count (1) are scratch: the elements whose tangent needs the eigenvalue
 // clamp. With emesh (element -> mesh) and mesh_exact (per mesh), the elements of the meshes

@@ -1,12 +1,12 @@
 // lpg_noalloc.cu -- the feasible step without any device allocation.
 //
-// Some callers cannot call cudaMalloc at the moment they need a feasible step: code that is
-// recording a CUDA stream capture (a device allocation is not a legal operation there), and
-// solvers embedded in a framework whose device memory is owned by its own pool (a training
-// loop on PyTorch's caching allocator, a renderer with a fixed budget), where a library
+// Some callers must not call cudaMalloc at the moment they need a feasible step: solvers
+// embedded in a framework whose device memory is owned by its own pool (a training loop on
+// PyTorch's caching allocator, an application with a fixed memory budget), where a library
 // allocation mid-step fragments or exceeds that budget. lpg_fem_feasible_step may allocate
 // its per-block scratch on first use; this variant takes that scratch from a fixed array in
-// the library image instead.
+// the library image instead. It serves tet, hex and Hermite handles (one thread per element
+// in every case) and returns synchronously.
 //
 // The scratch is one file-scope __device__ array of kMaxBlocks + 4 doubles (about 512 KB):
 // the per-block minima of the feasible-step reduction, the result and the status word. Every
@@ -27,7 +27,7 @@ extern thread_local std::string g_last_error;
 
 namespace {
 
-// 65,536 blocks of 256 elements: meshes of up to 16,777,216 tets.
+// 65,536 blocks of 256 elements: meshes of up to 16,777,216 elements.
 constexpr int kMaxBlocks = 65536;
 constexpr int kMaxDevices = 64;
 
@@ -50,6 +50,21 @@ double* scratch_address(int device) {
     return g_scratch_address[device];
 }
 
+// u and du must be device (or managed) memory on the handle's GPU: a host pointer given to the
+// kernel would fault, so it is rejected here.
+void check_device_array(const void* p, int device, const char* name) {
+    cudaPointerAttributes at{};
+    const cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(LPG_EINVAL, std::string("lpg_fem_feasible_step_noalloc: ") + name + " is not a device pointer");
+    }
+    const bool ok = at.type == cudaMemoryTypeManaged || (at.type == cudaMemoryTypeDevice && at.device == device);
+    if (!ok)
+        fail(LPG_EINVAL, std::string("lpg_fem_feasible_step_noalloc: ") + name +
+                             " must be device memory on the handle's GPU");
+}
+
 } // namespace
 } // namespace lpg
 
@@ -63,10 +78,12 @@ extern "C" int lpg_fem_feasible_step_noalloc(lpg_fem_t h, const double* u, const
             ~Release() { b.store(false); }
         } release{h->busy};
         LPG_CUDA(cudaSetDevice(h->device));
+        check_device_array(u, h->device, "u");
+        check_device_array(du, h->device, "du");
         const int nb = feasible_blocks(h->dm);
         if (nb > kMaxBlocks)
-            fail(LPG_EINVAL, "lpg_fem_feasible_step_noalloc: at most 16,777,216 tets (" + std::to_string(h->dm.T) +
-                                 " given); use lpg_fem_feasible_step");
+            fail(LPG_EINVAL, "lpg_fem_feasible_step_noalloc: at most 16,777,216 elements (" +
+                                 std::to_string(h->dm.T) + " given); use lpg_fem_feasible_step");
         double* scratch = scratch_address(h->device);
         double* block_min = scratch;
         double* result = scratch + kMaxBlocks;

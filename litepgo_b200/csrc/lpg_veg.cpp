@@ -1,24 +1,33 @@
-// lpg_veg.cpp -- VEG volume-mesh files (the reference's src/core/mesh/io/veg.cpp, read_veg and
-// write_veg): the text format of libpgo/Vega with a *VERTICES section ("n 3 ..." then one
-// "id x y z" line per vertex, ids consecutive from 0 or 1) and one *ELEMENTS section (a type
-// line, TET or CUBIC, then "m width ..." and one "id v1 .. v_width" line per element, vertex ids
-// in the vertices' base). Blank lines and lines starting with '#' are skipped, "*INCLUDE name"
-// splices another file (relative to the including one; cycles are an error) and every other
-// record is ignored. Fields may be separated by spaces, tabs or commas.
+// lpg_veg.cpp -- VEG volume-mesh files: read_veg and write_veg of the reference's mesh I/O
+// (src/core/mesh/io/veg.cpp), written here from the format's grammar.
 //
-// File and format problems raise LPG_EIO (the reference's std::runtime_error); a mesh that
-// parses but is not a valid mesh (non-finite coordinates, repeated vertices in a cell) raises
-// LPG_EINVAL (its std::invalid_argument).
+// Grammar (one record per line; fields separated by spaces, tabs or commas):
+//
+//   file       := { blank | comment | directive | record }
+//   comment    := '#' anything
+//   directive  := '*' keyword { field }
+//   *INCLUDE p    the lines of file p (relative to the including file) in place; a file that
+//                 includes itself, directly or through others, is an error
+//   *VERTICES     header "count 3 ..." then `count` records "id x y z ..."; ids start at 0 or 1
+//                 and increase by one (the first id fixes the base of every vertex reference)
+//   *ELEMENTS     a type record (TET or CUBIC, blanks inside ignored), header "count width ...",
+//                 then `count` records "id v_1 .. v_width ..." of vertex references
+//   *other        material, set and region directives: their records are skipped
+//
+// A file holds one *VERTICES section and, after it, one *ELEMENTS section. Problems with the
+// file or its format raise LPG_EIO (the reference's std::runtime_error), with the file and line
+// where they were found; a file that parses into an invalid mesh (non-finite coordinates,
+// repeated vertices in a cell) raises LPG_EINVAL (its std::invalid_argument).
 
+#include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <filesystem>
 #include <fstream>
-#include <iterator>
-#include <limits>
+#include <memory>
 #include <string>
-#include <type_traits>
+#include <string_view>
 #include <vector>
 
 #include "lpg_internal.h"
@@ -28,87 +37,206 @@ namespace fs = std::filesystem;
 
 namespace {
 
-[[noreturn]] void io_fail(const std::string& what) { fail(LPG_EIO, what); }
+bool blank(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n'; }
+bool separator(char c) { return blank(c) || c == ','; }
 
-std::string strip(const std::string& s) {
-    const char* ws = " \t\r\n";
-    const size_t a = s.find_first_not_of(ws);
-    if (a == std::string::npos) return {};
-    return s.substr(a, s.find_last_not_of(ws) - a + 1);
+std::string_view trim(std::string_view s) {
+    while (!s.empty() && blank(s.front())) s.remove_prefix(1);
+    while (!s.empty() && blank(s.back())) s.remove_suffix(1);
+    return s;
 }
 
-// The meaningful lines of a file, *INCLUDE files spliced in place. `chain` holds the files being
-// read around this one.
-void load_lines(const fs::path& path, std::vector<fs::path>& chain, std::vector<std::string>& out) {
-    const fs::path key = fs::weakly_canonical(path);
-    for (const fs::path& p : chain)
-        if (p == key) io_fail("veg *INCLUDE cycle through " + path.string());
-    std::ifstream in(path, std::ios::binary);
-    if (!in) io_fail("Failed to open veg file: " + path.string());
-    chain.push_back(key);
-    std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
-    if (in.bad()) io_fail("Failed reading VEG: " + path.string());
-    size_t pos = 0;
-    while (pos < text.size()) {
-        size_t eol = text.find('\n', pos);
-        if (eol == std::string::npos) eol = text.size();
-        size_t a = pos, b = eol;
-        while (a < b && (text[a] == ' ' || text[a] == '\t' || text[a] == '\r')) ++a;
-        while (b > a && (text[b - 1] == ' ' || text[b - 1] == '\t' || text[b - 1] == '\r')) --b;
-        pos = eol + 1;
-        if (a == b || text[a] == '#') continue;
-        std::string line(text, a, b - a);
-        if (line.compare(0, 9, "*INCLUDE ") == 0) {
-            load_lines(path.parent_path() / strip(line.substr(9)), chain, out);
-            continue;
-        }
-        out.push_back(std::move(line));
+// A meaningful line and the place it was read from.
+struct Line {
+    std::string text;
+    std::string where; // "file:line"
+    bool directive() const { return !text.empty() && text[0] == '*'; }
+    // The directive's keyword: the letters after '*' up to the first separator.
+    std::string_view keyword() const {
+        std::string_view t(text);
+        t.remove_prefix(1);
+        size_t n = 0;
+        while (n < t.size() && !separator(t[n])) ++n;
+        return t.substr(0, n);
     }
-    chain.pop_back();
-}
+};
 
-// Splits a record into fields (space, tab or comma separated) and parses each completely as a
-// number; false if a field is not one.
-template <class T> bool fields(const std::string& line, std::vector<T>& out) {
-    out.clear();
-    size_t i = 0;
-    const size_t n = line.size();
-    auto sep = [](char c) { return c == ' ' || c == '\t' || c == ',' || c == '\r' || c == '\n'; };
-    while (i < n) {
-        while (i < n && sep(line[i])) ++i;
-        if (i >= n) break;
-        size_t j = i;
-        while (j < n && !sep(line[j])) ++j;
-        // Parse in place; the number must end exactly where the field ends.
-        const char* beg = line.c_str() + i;
-        char* end = nullptr;
-        if constexpr (std::is_same<T, double>::value) {
-            const double v = std::strtod(beg, &end);
-            if (end != line.c_str() + j) return false;
-            out.push_back(v);
-        } else {
-            const long long v = std::strtoll(beg, &end, 10);
-            if (end != line.c_str() + j || v < std::numeric_limits<int>::min() || v > std::numeric_limits<int>::max())
-                return false;
-            out.push_back(static_cast<T>(v));
+// Lines of a VEG file with *INCLUDE directives followed in place. Blank and comment lines are
+// dropped. The open files form a stack; a file already on it may not be opened again.
+class LineSource {
+public:
+    explicit LineSource(const fs::path& root) { open(root, ""); }
+
+    // The next meaningful line; false once the root file is exhausted.
+    bool next(Line& out) {
+        while (!files_.empty()) {
+            File& f = *files_.back();
+            std::string raw;
+            if (!std::getline(f.in, raw)) {
+                if (f.in.bad()) fail(LPG_EIO, "VEG: read error in " + f.path.string());
+                files_.pop_back();
+                continue;
+            }
+            ++f.line;
+            const std::string_view t = trim(raw);
+            if (t.empty() || t[0] == '#') continue;
+            const std::string where = f.path.string() + ":" + std::to_string(f.line);
+            if (t.substr(0, 8) == "*INCLUDE" && (t.size() == 8 || blank(t[8]))) {
+                const std::string_view target = trim(t.substr(8));
+                if (target.empty()) fail(LPG_EIO, "VEG " + where + ": *INCLUDE names no file");
+                open(f.path.parent_path() / std::string(target), where);
+                continue;
+            }
+            out.text.assign(t);
+            out.where = where;
+            return true;
         }
-        i = j;
+        return false;
     }
-    return true;
+
+private:
+    struct File {
+        std::ifstream in;
+        fs::path path, key;
+        long line = 0;
+    };
+    std::vector<std::unique_ptr<File>> files_;
+
+    void open(const fs::path& path, const std::string& from) {
+        std::error_code ec;
+        fs::path key = fs::weakly_canonical(path, ec);
+        if (ec) key = path;
+        for (const auto& f : files_)
+            if (f->key == key) fail(LPG_EIO, "VEG " + from + ": include cycle: " + path.string() + " is already being read");
+        auto f = std::make_unique<File>();
+        f->in.open(path, std::ios::binary);
+        if (!f->in) fail(LPG_EIO, "VEG: cannot open " + path.string() + (from.empty() ? "" : " (included at " + from + ")"));
+        f->path = path;
+        f->key = key;
+        files_.push_back(std::move(f));
+    }
+};
+
+// The numeric fields of a record, each parsed in full (std::from_chars).
+template <class T> std::vector<T> numbers(const Line& line) {
+    std::vector<T> out;
+    const char* p = line.text.data();
+    const char* end = p + line.text.size();
+    while (true) {
+        while (p < end && separator(*p)) ++p;
+        if (p == end) break;
+        const char* q = p;
+        while (q < end && !separator(*q)) ++q;
+        T v{};
+        const char* s = (*p == '+' && q - p > 1) ? p + 1 : p; // from_chars takes no leading '+'
+        const auto r = std::from_chars(s, q, v);
+        if (r.ec != std::errc() || r.ptr != q)
+            fail(LPG_EIO, "VEG " + line.where + ": '" + std::string(p, q) + "' is not a number (record '" + line.text + "')");
+        out.push_back(v);
+        p = q;
+    }
+    return out;
 }
 
-template <class T> std::vector<T> record(const std::string& line) {
-    std::vector<T> v;
-    if (!fields(line, v)) io_fail("Malformed VEG numeric record: " + line);
-    return v;
-}
+// Reads a VEG mesh from a line source: a small state machine over the directives.
+class VegParser {
+public:
+    VegParser(const fs::path& root, VegMesh& mesh) : src_(root), mesh_(mesh), root_(root.string()) {}
 
-std::string no_space(const std::string& s) {
-    std::string r;
-    for (char c : s)
-        if (c != ' ' && c != '\t' && c != '\r' && c != '\n') r.push_back(c);
-    return r;
-}
+    void run() {
+        mesh_ = VegMesh{};
+        Line line;
+        bool have = src_.next(line);
+        while (have) {
+            if (!line.directive()) { // a record of a skipped section
+                have = src_.next(line);
+                continue;
+            }
+            const std::string_view kw = line.keyword();
+            if (kw == "VERTICES")
+                vertices(line);
+            else if (kw == "ELEMENTS")
+                elements(line);
+            have = src_.next(line);
+        }
+        if (!seen_vertices_) fail(LPG_EIO, "VEG " + root_ + ": the file has no *VERTICES section");
+        if (mesh_.width == 0) fail(LPG_EIO, "VEG " + root_ + ": the file has no *ELEMENTS section");
+    }
+
+private:
+    LineSource src_;
+    VegMesh& mesh_;
+    std::string root_;
+    bool seen_vertices_ = false;
+    long base_ = 1;
+
+    // The next line, which must be a record of the section `what` opened at `at`.
+    Line record(const Line& at, const char* what) {
+        Line r;
+        if (!src_.next(r)) fail(LPG_EIO, "VEG " + at.where + ": the file ends inside the " + what);
+        if (r.directive()) fail(LPG_EIO, "VEG " + r.where + ": expected the " + std::string(what) + ", found '" + r.text + "'");
+        return r;
+    }
+
+    void vertices(const Line& at) {
+        if (seen_vertices_) fail(LPG_EIO, "VEG " + at.where + ": a second *VERTICES section");
+        seen_vertices_ = true;
+        const Line h = record(at, "vertex header");
+        const std::vector<long> head = numbers<long>(h);
+        if (head.size() < 2 || head[0] < 0 || head[0] > (1L << 31) - 1 || head[1] != 3)
+            fail(LPG_EIO, "VEG " + h.where + ": the vertex header must read '<count> 3 ...', got '" + h.text + "'");
+        const long n = head[0];
+        mesh_.positions.reserve(3 * static_cast<size_t>(std::min(n, 1L << 20))); // the count is not trusted
+        for (long k = 0; k < n; ++k) {
+            const Line r = record(at, "vertex records");
+            const std::vector<double> v = numbers<double>(r);
+            if (v.size() < 4) fail(LPG_EIO, "VEG " + r.where + ": a vertex record needs an id and three coordinates");
+            if (k == 0) base_ = v[0] == 0.0 ? 0 : 1;
+            if (v[0] != static_cast<double>(k + base_))
+                fail(LPG_EIO, "VEG " + r.where + ": vertex id " + std::to_string(v[0]) + " where " +
+                                  std::to_string(k + base_) + " was expected (ids run consecutively)");
+            mesh_.positions.push_back(v[1]);
+            mesh_.positions.push_back(v[2]);
+            mesh_.positions.push_back(v[3]);
+        }
+        mesh_.num_vertices = static_cast<int>(n);
+    }
+
+    void elements(const Line& at) {
+        if (!seen_vertices_) fail(LPG_EIO, "VEG " + at.where + ": *ELEMENTS before any *VERTICES section");
+        if (mesh_.width != 0) fail(LPG_EIO, "VEG " + at.where + ": a second *ELEMENTS section");
+        const Line t = record(at, "element type");
+        std::string type;
+        for (char c : t.text)
+            if (!blank(c)) type.push_back(c);
+        const int width = type == "TET" ? 4 : type == "CUBIC" ? 8 : 0;
+        if (width == 0) fail(LPG_EIO, "VEG " + t.where + ": element type '" + type + "' is neither TET nor CUBIC");
+        const Line h = record(at, "element header");
+        const std::vector<long> head = numbers<long>(h);
+        if (head.empty() || head[0] < 0 || head[0] > (1L << 31) - 1)
+            fail(LPG_EIO, "VEG " + h.where + ": the element header must start with a non-negative count");
+        if (head.size() < 2 || head[1] != width)
+            fail(LPG_EIO, "VEG " + h.where + ": " + type + " elements have " + std::to_string(width) +
+                              " vertices, the header says '" + h.text + "'");
+        const long m = head[0];
+        mesh_.cells.reserve(static_cast<size_t>(std::min(m, 1L << 20)) * width);
+        for (long k = 0; k < m; ++k) {
+            const Line r = record(at, "element records");
+            const std::vector<long> v = numbers<long>(r);
+            if (static_cast<long>(v.size()) < width + 1)
+                fail(LPG_EIO, "VEG " + r.where + ": an element record needs an id and " + std::to_string(width) +
+                                  " vertex references");
+            for (int a = 1; a <= width; ++a) {
+                const long id = v[a] - base_;
+                if (id < 0 || id >= mesh_.num_vertices)
+                    fail(LPG_EIO, "VEG " + r.where + ": vertex reference " + std::to_string(v[a]) +
+                                      " is not one of the file's vertices");
+                mesh_.cells.push_back(static_cast<int32_t>(id));
+            }
+        }
+        mesh_.width = width;
+    }
+};
 
 } // namespace
 
@@ -129,68 +257,7 @@ void validate_volume_mesh(int V, const std::vector<double>& positions, int width
 }
 
 void read_veg(const std::string& file, VegMesh& mesh) {
-    const fs::path path(file);
-    std::vector<std::string> lines;
-    std::vector<fs::path> chain;
-    load_lines(path, chain, lines);
-    mesh = VegMesh{};
-    const std::string where = " in " + path.string();
-    int base = 1; // 1-based vertex ids unless the first one is 0
-    bool have_vertices = false;
-    size_t i = 0;
-    while (i < lines.size()) {
-        const std::string& line = lines[i];
-        if (line.compare(0, 9, "*VERTICES") == 0) {
-            if (have_vertices) io_fail("Duplicate *VERTICES section" + where);
-            have_vertices = true;
-            if (++i >= lines.size()) io_fail("Missing *VERTICES header" + where);
-            const std::vector<int> head = record<int>(lines[i++]);
-            if (head.size() < 2 || head[0] < 0 || head[1] != 3) io_fail("Invalid 3D vertex header" + where);
-            const size_t n = static_cast<size_t>(head[0]);
-            if (n > lines.size() - i) io_fail("Truncated vertex data" + where);
-            mesh.positions.reserve(3 * n);
-            for (size_t row = 0; row < n; ++row, ++i) {
-                const std::vector<double> v = record<double>(lines[i]);
-                if (v.size() < 4) io_fail("Malformed vertex line" + where + ": " + lines[i]);
-                if (row == 0 && v[0] == 0) base = 0;
-                if (v[0] != static_cast<double>(row) + base) io_fail("Vertex IDs must be consecutive" + where);
-                mesh.positions.insert(mesh.positions.end(), {v[1], v[2], v[3]});
-            }
-            mesh.num_vertices = static_cast<int>(n);
-            continue;
-        }
-        if (line.compare(0, 9, "*ELEMENTS") == 0) {
-            if (!have_vertices || mesh.width != 0)
-                io_fail("Expected one *VERTICES section followed by one *ELEMENTS section" + where);
-            if (++i >= lines.size()) io_fail("Missing element type" + where);
-            const std::string type = no_space(lines[i++]);
-            if (type == "TET")
-                mesh.width = 4;
-            else if (type == "CUBIC")
-                mesh.width = 8;
-            else
-                io_fail("Unsupported element type" + where + ": " + type);
-            if (i >= lines.size()) io_fail("Missing element count" + where);
-            const std::vector<int> head = record<int>(lines[i++]);
-            if (head.empty() || head[0] < 0) io_fail("Invalid element count" + where);
-            const size_t m = static_cast<size_t>(head[0]);
-            if (m > lines.size() - i) io_fail("Truncated element data" + where);
-            if (head.size() < 2 || head[1] != mesh.width) io_fail("Element width does not match its type" + where);
-            mesh.cells.reserve(m * static_cast<size_t>(mesh.width));
-            for (size_t row = 0; row < m; ++row, ++i) {
-                const std::vector<int> v = record<int>(lines[i]);
-                if (static_cast<int>(v.size()) < mesh.width + 1) io_fail("Malformed element line" + where + ": " + lines[i]);
-                for (int a = 1; a <= mesh.width; ++a) {
-                    const long long id = static_cast<long long>(v[a]) - base;
-                    if (id < 0 || id >= mesh.num_vertices) io_fail("Element vertex index out of range" + where);
-                    mesh.cells.push_back(static_cast<int32_t>(id));
-                }
-            }
-            continue;
-        }
-        ++i; // materials, sets, regions and other records carry no geometry
-    }
-    if (mesh.width == 0) io_fail("No *ELEMENTS section found" + where);
+    VegParser(fs::path(file), mesh).run();
     validate_volume_mesh(mesh.num_vertices, mesh.positions, mesh.width, mesh.cells);
 }
 
@@ -200,7 +267,7 @@ void write_veg(const std::string& file, int V, const double* positions, int T, i
     std::vector<int32_t> cl(cells, cells + static_cast<size_t>(width) * T);
     validate_volume_mesh(V, pos, width, cl);
     std::FILE* f = std::fopen(file.c_str(), "w");
-    if (!f) io_fail("Cannot write VEG: " + file);
+    if (!f) fail(LPG_EIO, "VEG: cannot open " + file + " for writing");
     bool ok = std::fprintf(f, "*VERTICES\n%d 3 0 0\n", V) > 0;
     for (int v = 0; v < V && ok; ++v)
         ok = std::fprintf(f, "%d %.17g %.17g %.17g\n", v + 1, pos[3 * size_t(v)], pos[3 * size_t(v) + 1],
@@ -212,7 +279,7 @@ void write_veg(const std::string& file, int V, const double* positions, int T, i
         ok = ok && std::fputc('\n', f) != EOF;
     }
     if (std::fclose(f) != 0) ok = false;
-    if (!ok) io_fail("Failed writing VEG: " + file);
+    if (!ok) fail(LPG_EIO, "VEG: writing " + file + " failed");
 }
 
 } // namespace lpg

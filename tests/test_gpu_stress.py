@@ -1,10 +1,13 @@
 """Large mixed-precision stress case: 128^3 cubes x 5 tets (10,485,760 tets), 0.6x axial
 compression plus per-vertex noise 0.05 h N(0, 1) with every det F in [0.2, 3.0].
 
-Per-result error of the mixed path (FP32 element arithmetic and Hessian, FP64 energy sum and
-gradient output) against the FP64 path, with bounds written below; the FP64 path itself against
-the oracle on the element energies of 2,000 sampled elements (1e-12 relative), since the
-oracle's full assembly does not fit this size.
+- Per-result error of the mixed path (FP32 element arithmetic and Hessian, FP64 energy sum and
+  gradient output) against the FP64 path, with bounds written below.
+- The FP64 path against the oracle on the whole mesh, in overlapping z-slabs: a slab of cube
+  layers holds every element incident to the vertex levels strictly inside it, so those rows of
+  the slab's oracle assembly are the full mesh's rows. The slabs cover every vertex level, so
+  the whole gradient and every column of the Exact CSC Hessian (pattern bit for bit, values
+  1e-12 max-norm relative per slab) are compared, plus the energy of every element.
 """
 
 import numpy as np
@@ -16,10 +19,12 @@ from litepgo_b200 import energy, fem, mesh, workloads
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
+N = 128
+
 
 @pytest.fixture(scope="module")
 def stress():
-    w = workloads.compressed_box(128, seed=0)
+    w = workloads.compressed_box(N, seed=0)
     d = workloads.det_F(w["X"], w["tets"], w["u"])
     assert d.min() >= 0.2 and d.max() <= 3.0
     e = fem.VolumetricFemEnergyTetP1.from_arrays(w["X"], w["tets"], w["theta"])
@@ -32,7 +37,7 @@ def rel_max(a, b):
 
 def test_stress_counts(stress):
     w, e = stress
-    assert (e.num_vertices, e.num_elements, e.nnzb) == mesh.box_counts(128) == (2146689, 10485760, 27608193)
+    assert (e.num_vertices, e.num_elements, e.nnzb) == mesh.box_counts(N) == (2146689, 10485760, 27608193)
 
 
 def test_stress_mixed_against_f64(stress):
@@ -46,14 +51,53 @@ def test_stress_mixed_against_f64(stress):
     assert errs["energy"] <= 1e-6 and errs["gradient"] <= 1e-5 and errs["hessian"] <= 1e-5
 
 
-def test_stress_f64_element_energies_against_oracle(stress):
+def slabs(n, width=16):
+    """Cube-layer ranges [k0, k1) and the vertex levels [l0, l1] whose rows they hold in full."""
+    # Vertex level l touches cube layers l - 1 and l.
+    return [(max(s - 1, 0), min(s + width + 1, n), s, min(s + width, n)) for s in range(0, n, width)]
+
+
+def test_slab_cover():
+    """Every vertex level lies in a slab that holds both of its cube layers."""
+    cover = set()
+    for k0, k1, l0, l1 in slabs(N):
+        for lev in range(l0, l1 + 1):
+            assert all(k0 <= c < k1 for c in (lev - 1, lev) if 0 <= c < N)
+            cover.add(lev)
+    assert cover == set(range(N + 1))
+
+
+def test_stress_f64_against_oracle_by_slabs(stress):
     w, e = stress
-    u = torch.as_tensor(w["u"], device="cuda")
-    got = e.element_energies(u).cpu().numpy()
-    pick = np.sort(np.random.default_rng(0).choice(w["tets"].shape[0], 2000, replace=False))
-    sub = w["tets"][pick]
-    verts, local = np.unique(sub, return_inverse=True)
-    orc = oracle.OracleMesh(w["X"][verts], local.reshape(-1, 4).astype(np.int32), w["theta"])
-    uu = w["u"].reshape(-1, 3)[verts].ravel()
-    _, _, _, (ref, _, _) = orc.eval(uu, False, 0, elements=True)
-    assert np.max(np.abs(got[pick] - ref)) <= 1e-12 * np.max(np.abs(ref))
+    X, tets, u, theta = w["X"], w["tets"], w["u"], w["theta"]
+    sy = (N + 1) * (N + 1)  # vertices per level
+    per_layer = 5 * N * N   # elements per cube layer
+    ut = torch.as_tensor(u, device="cuda")
+    E, g, Hc = e.eval_device(ut, gradient=True, hessian=energy.HessianKind.Exact, layout="csc")
+    g = g.cpu().numpy()
+    Hc = Hc.cpu().numpy()
+    eE = e.element_energies(ut).cpu().numpy()
+    outer, inner = e.pattern_csc()
+    worst = {"gradient": 0.0, "hessian": 0.0, "elements": 0.0}
+    for k0, k1, l0, l1 in slabs(N):
+        v0, v1 = sy * k0, sy * (k1 + 1)
+        sub = tets[per_layer * k0:per_layer * k1] - v0
+        orc = oracle.OracleMesh(X[v0:v1], sub, theta)
+        _, gs, vs, (eEs, _, _) = orc.eval(u[3 * v0:3 * v1], True, 1, elements=True)
+        so, si = orc.pattern()
+        d0, d1 = 3 * sy * l0, 3 * sy * (l1 + 1)  # complete DOF columns, full numbering
+        s0, s1 = d0 - 3 * v0, d1 - 3 * v0         # the same columns in the slab's numbering
+        # Pattern: the slab's columns are the full mesh's, shifted by the slab's first DOF.
+        assert np.array_equal(np.diff(outer[d0:d1 + 1]), np.diff(so[s0:s1 + 1]))
+        a, b = outer[d0], outer[d1]
+        assert np.array_equal(inner[a:b] - 3 * v0, si[so[s0]:so[s1]])
+        gr = gs[s0:s1]
+        worst["gradient"] = max(worst["gradient"], float(np.max(np.abs(g[d0:d1] - gr)) / np.max(np.abs(gr))))
+        hr = vs[so[s0]:so[s1]]
+        worst["hessian"] = max(worst["hessian"], float(np.max(np.abs(Hc[a:b] - hr)) / np.max(np.abs(hr))))
+        er = eEs
+        got = eE[per_layer * k0:per_layer * k1]
+        worst["elements"] = max(worst["elements"], float(np.max(np.abs(got - er)) / np.max(np.abs(er))))
+        del orc
+    print("FP64 vs oracle at 128^3 (worst slab):", worst)
+    assert worst["gradient"] <= 1e-12 and worst["hessian"] <= 1e-12 and worst["elements"] <= 1e-12
