@@ -98,6 +98,27 @@ void upload_plan(lpg_fem& hh, int V, int T) {
     m.cl_ent_ptr = upload(h->b_cl[8], p.cl_ent_ptr);
     m.cl_ents = upload(h->b_cl[9], p.cl_ents);
     m.cl_ntr = upload(h->b_cl[10], p.cl_ntr);
+    m.tc_ncl = p.tc_row_ptr.empty() ? 0 : static_cast<int>(p.tc_row_ptr.size()) - 1;
+    if (m.tc_ncl > 0) {
+        m.tc_row_ptr = upload(h->b_tc[0], p.tc_row_ptr);
+        m.tc_rows = upload(h->b_tc[1], p.tc_rows);
+        m.tc_row_so = upload(h->b_tc[2], p.tc_row_so);
+        m.tc_el_ptr = upload(h->b_tc[3], p.tc_el_ptr);
+        m.tc_vert_ptr = upload(h->b_tc[4], p.tc_vert_ptr);
+        m.tc_verts = upload(h->b_tc[5], p.tc_verts);
+        m.tc_item_ptr = upload(h->b_tc[6], p.tc_item_ptr);
+        m.tc_ndiag = upload(h->b_tc[7], p.tc_ndiag);
+        m.tc_ent_ptr = upload(h->b_tc[8], p.tc_ent_ptr);
+        m.tc_els = upload(h->b_tc[9], p.tc_els);
+        m.tc_loc = upload(h->b_tc[10], p.tc_loc);
+        m.tc_items = reinterpret_cast<uint4*>(upload(h->b_tc[11], p.tc_items));
+        m.tc_ents = upload(h->b_tc[12], p.tc_ents);
+        m.tc_max_els = m.tc_max_verts = m.tc_max_vals = 0;
+        for (int c = 0; c < m.tc_ncl; ++c) {
+            m.tc_max_els = std::max(m.tc_max_els, p.tc_el_ptr[c + 1] - p.tc_el_ptr[c]);
+            m.tc_max_verts = std::max(m.tc_max_verts, p.tc_vert_ptr[c + 1] - p.tc_vert_ptr[c]);
+        }
+    }
     m.cl_max_slots = m.cl_max_ents = 0;
     for (int c = 0; c < m.ncl; ++c) {
         m.cl_max_slots = std::max(m.cl_max_slots, p.cl_slot_ptr[c + 1] - p.cl_slot_ptr[c]);
@@ -225,7 +246,7 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.hess = hessian != LPG_HESSIAN_NONE ? dhess : nullptr;
     a.layout = layout;
     // Per-cluster energies, then partial sums.
-    a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(dm.ncl) + 256);
+    a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(std::max(dm.ncl, dm.tc_ncl)) + 256);
     a.energy = d_energy.as<double>(1);
     a.elem_energy = delem;
     a.status = d_status.as<unsigned>(1);
@@ -247,7 +268,7 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
         const size_t T = static_cast<size_t>(dm.T);
         double* elemE = delem ? delem : d_mat[3].as<double>(std::max<size_t>(T, 1));
         void* blocks = a.hess ? d_proj.ensure(hex_blocks_bytes(dm, precision, projected)) : nullptr;
-        a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(dm.ncl) + 256);
+        a.cluster_energy = d_cluster_energy.as<double>(static_cast<size_t>(std::max(dm.ncl, dm.tc_ncl)) + 256);
         int* flags = projected && a.hess ? d_plist.as<int>(std::max<size_t>(T, 1)) : nullptr;
         launch_hex_eval(dm, precision, projected, du, elemE, d_vjp.as<double>(std::max<size_t>(24 * T, 1)), blocks,
                         flags, a, stream);
@@ -299,6 +320,7 @@ int lpg_mesh_cluster_summary_cells(int V, int T, const int32_t* tets, int cell_w
         HostPlan p;
         build_plan(V, T, tets, p, cell_width);
         check_clusters(p, tets);
+        check_tet_clusters(p, tets);
         check_solver_layout(p);
         const int ncl = static_cast<int>(p.cl_row_ptr.size()) - 1;
         int64_t max_rows = 0, max_els = 0;
@@ -722,7 +744,7 @@ int lpg_fem_eval_material(lpg_fem_t h, const double* W, const double* P, const d
         const size_t hbytes = 9 * static_cast<size_t>(h->dm.nnzb) * (precision == LPG_PRECISION_F64 ? 8 : 4);
         a.hess = hessian != LPG_HESSIAN_NONE ? (out_mem == LPG_MEM_DEVICE ? hess : h->d_hess.ensure(hbytes)) : nullptr;
         a.layout = layout;
-        a.cluster_energy = h->d_cluster_energy.as<double>(static_cast<size_t>(h->dm.ncl) + 256);
+        a.cluster_energy = h->d_cluster_energy.as<double>(static_cast<size_t>(std::max(h->dm.ncl, h->dm.tc_ncl)) + 256);
         a.energy = h->d_energy.as<double>(1);
         a.status = h->d_status.as<unsigned>(1);
         const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;

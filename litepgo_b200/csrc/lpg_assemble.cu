@@ -93,10 +93,12 @@ template <typename R> struct Kin {
 // accurate near the rest state. Validity is checked once on J; the rare failure path then
 // tells a non-finite input from a non-finite F and from det F <= 0.
 template <typename R>
+__device__ __forceinline__ unsigned kinematics_of(const DevMesh& m, int e, const R (&rec)[12], const double (&uu)[4][3],
+                                                  Kin<R>& k);
+
+template <typename R>
 __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const int4 tv, const double* __restrict__ u,
                                                Kin<R>& k) {
-    using X = M<R>;
-    unsigned st = 0;
     R rec[12];
     load_rec<R>(rec_ptr<R>(m), e, rec);
     const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
@@ -105,6 +107,15 @@ __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const in
     for (int c = 0; c < 4; ++c)
 #pragma unroll
         for (int i = 0; i < 3; ++i) uu[c][i] = __ldg(u + 3 * static_cast<size_t>(vs[c]) + i);
+    return kinematics_of<R>(m, e, rec, uu, k);
+}
+
+// The element's kinematics from its record (rec) and its vertices' displacements (uu).
+template <typename R>
+__device__ __forceinline__ unsigned kinematics_of(const DevMesh& m, int e, const R (&rec)[12], const double (&uu)[4][3],
+                                                  Kin<R>& k) {
+    using X = M<R>;
+    unsigned st = 0;
     R Ds[3][3]; // Ds[i][c] = u_{c+1,i} - u_{0,i}
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -1370,6 +1381,290 @@ void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     LPG_CUDA(cudaGetLastError());
 }
 
+
+// ---------------------------------------------------------------------------
+// Tet assembly over the tet clusters (E, gradient and Exact Hessian in the BSR, CSC or solver
+// layout). One thread block per cluster (persistent over clusters), four passes:
+//   stage:   the cluster's vertex displacements and element records are copied into shared
+//            memory by consecutive threads (runs of consecutive ids read coalesced);
+//   element: one thread per element evaluates it once (kinematics as the reference computes
+//            it) and keeps h_a = F^-T grad N_a, vol mu grad N_a . grad N_b, vol lambda, vol p
+//            and the gradient pieces g_a = vol P grad N_a in shared memory;
+//   items:   one thread per diagonal block (with the row's gradient) or edge block sums the
+//            block's contributors in ascending element order into registers and writes it into
+//            the cluster's output staging (an edge between two owned rows once, at both
+//            positions; the staging reuses the memory of the staged inputs);
+//   copy:    one warp per owned row copies the row's staged values to the output: the row's
+//            9 nb values are contiguous in the BSR and CSC layouts, so the stores are
+//            coalesced.
+// ---------------------------------------------------------------------------
+#ifndef LPG_TC_THREADS
+#define LPG_TC_THREADS 256
+#endif
+constexpr int kTcThreads = LPG_TC_THREADS;
+// Per-element data in shared memory, one component per kTcElems-long array: h_a (3 a + i),
+// vol mu grad N_a . grad N_b (pair order), vol lambda, vol p, g_a (3 a + i).
+constexpr int kTcH = 0, kTcCC = 12, kTcL = 22, kTcP = 23, kTcG = 24, kTcComp = 36;
+template <typename R> constexpr int tc_minb(int v) {
+    return sizeof(R) == 8 ? (v == 0 ? 2 : v == 1 ? 1 : 2) : (v == 0 ? 3 : v == 1 ? 2 : 4);
+}
+template <typename R> constexpr size_t tc_records_bytes() { return static_cast<size_t>(kTcElems) * 12 * sizeof(R); }
+template <typename R> constexpr size_t tc_region_bytes() {
+    return tc_records_bytes<R>() + static_cast<size_t>(kTcVerts) * 3 * sizeof(double) >
+                   static_cast<size_t>(kTcVals) * sizeof(R)
+               ? tc_records_bytes<R>() + static_cast<size_t>(kTcVerts) * 3 * sizeof(double)
+               : static_cast<size_t>(kTcVals) * sizeof(R);
+}
+template <typename R> constexpr size_t tc_smem_bytes() {
+    return 32 * sizeof(double) + static_cast<size_t>(kTcComp) * kTcElems * sizeof(R) + tc_region_bytes<R>();
+}
+
+// Staging index of entry (i, c) of the block at packed position pos (row offset so, block q,
+// row length nb): BSR and solver layouts keep blocks row-major one after the other, CSC keeps
+// the row's three scalar rows one after the other.
+__device__ __forceinline__ int tc_stage(uint32_t pos, bool csc, int i, int c) {
+    const int so = static_cast<int>(pos & 0xffffu), q = static_cast<int>((pos >> 16) & 0xffu),
+              nb = static_cast<int>(pos >> 24);
+    return csc ? so + 3 * nb * i + 3 * q + c : so + 9 * q + 3 * i + c;
+}
+
+template <typename R, bool WG, bool WH, int MINB>
+__global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const DevMesh m, const EvalArgs a) {
+    using X = M<R>;
+    using HT = typename HOut<R>::T;
+    constexpr int E = kTcElems;
+    constexpr int CH = 12 * static_cast<int>(sizeof(R)) / 16; // 16-byte chunks per element record
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* red = reinterpret_cast<double*>(smem_raw);
+    R* ed = reinterpret_cast<R*>(smem_raw + 32 * sizeof(double));
+    unsigned char* region = smem_raw + 32 * sizeof(double) + static_cast<size_t>(kTcComp) * E * sizeof(R);
+    R* srec = reinterpret_cast<R*>(region);                                        // [ne][12]
+    double* su = reinterpret_cast<double*>(region + tc_records_bytes<R>());       // [nv][3]
+    R* stage = reinterpret_cast<R*>(region);                                       // output staging
+    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+    const R* rec = rec_ptr<R>(m);
+    HT* hout = reinterpret_cast<HT*>(a.hess);
+    const bool csc = a.layout == LPG_LAYOUT_CSC, sell = a.layout == kLayoutSell;
+    unsigned st = 0;
+    for (int cl = blockIdx.x; cl < m.tc_ncl; cl += gridDim.x) {
+        const int e0 = __ldg(m.tc_el_ptr + cl), ne = __ldg(m.tc_el_ptr + cl + 1) - e0;
+        const int v0 = __ldg(m.tc_vert_ptr + cl), nv = __ldg(m.tc_vert_ptr + cl + 1) - v0;
+        // Stage: displacements of the cluster's vertices, then its element records.
+        for (int k = tid; k < 3 * nv; k += bd) {
+            const int j = k / 3;
+            su[k] = __ldg(a.u + 3 * static_cast<size_t>(__ldg(m.tc_verts + v0 + j)) + (k - 3 * j));
+        }
+        for (int k = tid; k < CH * ne; k += bd) {
+            const int j = k / CH;
+            const size_t e = __ldg(m.tc_els + e0 + j) & 0x7fffffffu;
+            reinterpret_cast<uint4*>(srec)[k] = __ldg(reinterpret_cast<const uint4*>(rec) + CH * e + (k - CH * j));
+        }
+        __syncthreads();
+        // Element pass: every element of the cluster once.
+        double eacc = 0;
+        for (int el = tid; el < ne; el += bd) {
+            const uint32_t ew = __ldg(m.tc_els + e0 + el);
+            const int e = static_cast<int>(ew & 0x7fffffffu);
+            const uint32_t loc = __ldg(m.tc_loc + e0 + el);
+            R r12[12];
+#pragma unroll
+            for (int t = 0; t < 12; ++t) r12[t] = srec[12 * el + t];
+            double uu[4][3];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int lv = static_cast<int>((loc >> (8 * c)) & 0xffu);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) uu[c][i] = su[3 * lv + i];
+            }
+            Kin<R> k;
+            st |= kinematics_of<R>(m, e, r12, uu, k);
+            if (ew >> 31) {
+                const R Ee = k.vol * k.psi;
+                eacc += static_cast<double>(Ee);
+                if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
+            }
+            const R p = X::fma(k.lam, k.logJ, -k.mu);
+            if (WG) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        R sum = 0;
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+                            sum = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[b][j], sum);
+                        ed[(kTcG + 3 * b + i) * E + el] = k.vol * sum;
+                    }
+            }
+            if (WH) {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        ed[(kTcH + 3 * b + i) * E + el] =
+                            X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
+                ed[kTcL * E + el] = X::mul(k.vol, k.lam);
+                ed[kTcP * E + el] = X::mul(k.vol, p);
+                const R mv = X::mul(k.vol, k.mu);
+#pragma unroll
+                for (int x = 0; x < 4; ++x)
+#pragma unroll
+                    for (int y = x; y < 4; ++y)
+                        ed[(kTcCC + pair10(x, y)) * E + el] =
+                            X::mul(mv, X::fma(k.n[x][2], k.n[y][2], X::fma(k.n[x][1], k.n[y][1], X::mul(k.n[x][0], k.n[y][0]))));
+            }
+        }
+        // Energy of the cluster's own elements: fixed thread order, fixed tree.
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, off);
+        if (lane == 0) red[warp] = eacc;
+        __syncthreads(); // element data complete; the staged inputs are dead
+        if (tid == 0) {
+            double t = 0;
+            for (int w = 0; w < nw; ++w) t += red[w];
+            a.cluster_energy[cl] = t;
+            if (!isfinite(t)) st |= ST_NONFINITE_OUT;
+        }
+        if (WG || WH) {
+            // Item pass: diagonal blocks (and gradient rows) first, then edge blocks.
+            const int i0 = __ldg(m.tc_item_ptr + cl), nd = __ldg(m.tc_ndiag + cl);
+            const int ni = WH ? __ldg(m.tc_item_ptr + cl + 1) - i0 : nd;
+            const uint16_t* ents = m.tc_ents + __ldg(m.tc_ent_ptr + cl);
+            const int r0 = __ldg(m.tc_row_ptr + cl);
+            for (int k = tid; k < ni; k += bd) {
+                const uint4 it = __ldg(m.tc_items + i0 + k);
+                const uint16_t* en = ents + (it.z & 0xfffffu);
+                const int cnt = static_cast<int>(it.z >> 20);
+                if (it.w >> 31) {
+                    // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient:
+                    //   H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
+                    R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
+                    for (int c = 0; c < cnt; ++c) {
+                        const int w = __ldg(en + c);
+                        const int el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
+                        if (WG) {
+#pragma unroll
+                            for (int i = 0; i < 3; ++i) gs[i] = X::add(gs[i], ed[(kTcG + 3 * la + i) * E + el]);
+                        }
+                        if (WH) {
+                            const R hh[3] = {ed[(kTcH + 3 * la) * E + el], ed[(kTcH + 3 * la + 1) * E + el],
+                                             ed[(kTcH + 3 * la + 2) * E + el]};
+                            const R dv = X::add(ed[kTcL * E + el], -ed[kTcP * E + el]), mg = ed[(kTcCC + pr) * E + el];
+                            int u = 0;
+#pragma unroll
+                            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                                for (int kk = i; kk < 3; ++kk, ++u) {
+                                    acc[u] = X::fma(dv, X::mul(hh[i], hh[kk]), acc[u]);
+                                    if (i == kk) acc[u] = X::add(acc[u], mg);
+                                }
+                        }
+                    }
+                    if (WG) {
+                        const int v = __ldg(m.tc_rows + r0 + static_cast<int>(it.w & 0xffu));
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            if (!X::finite(gs[i])) st |= ST_NONFINITE_OUT;
+                            a.grad[3 * static_cast<size_t>(v) + i] = static_cast<double>(gs[i]);
+                        }
+                    }
+                    if (WH) {
+                        constexpr int sym3[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) stage[tc_stage(it.x, csc, i, c)] = acc[sym3[3 * i + c]];
+                    }
+                } else if (WH) {
+                    // The solver layout keeps only blocks right of the diagonal: an edge to a
+                    // lower-numbered row of another cluster is not needed there.
+                    if (sell && ((it.w >> 30) & 1u)) continue;
+                    // Off-diagonal block in the orientation of the lower vertex (a) -> higher (b):
+                    //   C += vol lambda h_a h_b^T - vol p h_b h_a^T + vol mu (grad N_a . grad N_b) I.
+                    R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                    for (int c = 0; c < cnt; ++c) {
+                        const int w = __ldg(en + c);
+                        const int el = w >> 8, pr = (w >> 4) & 15, ra = (w >> 2) & 3, cb = w & 3;
+                        R ha[3], hb[3];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            ha[i] = ed[(kTcH + 3 * ra + i) * E + el];
+                            hb[i] = ed[(kTcH + 3 * cb + i) * E + el];
+                        }
+                        const R lv = ed[kTcL * E + el], pv = ed[kTcP * E + el], mg = ed[(kTcCC + pr) * E + el];
+                        R A[3], B[3];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            A[i] = X::mul(lv, ha[i]);
+                            B[i] = X::mul(-pv, ha[i]);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int kk = 0; kk < 3; ++kk) {
+                                acc[3 * i + kk] = X::fma(B[kk], hb[i], X::fma(A[i], hb[kk], acc[3 * i + kk]));
+                                if (i == kk) acc[3 * i + kk] = X::add(acc[3 * i + kk], mg);
+                            }
+                    }
+                    const bool tr = (it.w >> 30) & 1u;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) stage[tc_stage(it.x, csc, i, c)] = tr ? acc[3 * c + i] : acc[3 * i + c];
+                    if (it.y != 0xffffffffu) {
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) stage[tc_stage(it.y, csc, i, c)] = acc[3 * c + i];
+                    }
+                }
+            }
+        }
+        if (WH) {
+            __syncthreads(); // staging complete
+            // Copy pass: one warp per owned row.
+            const int r0 = __ldg(m.tc_row_ptr + cl), nr = __ldg(m.tc_row_ptr + cl + 1) - r0;
+            for (int j = warp; j < nr; j += nw) {
+                const int v = __ldg(m.tc_rows + r0 + j), so = __ldg(m.tc_row_so + r0 + j);
+                const int base = __ldg(m.row_ptr + v), nb = __ldg(m.row_ptr + v + 1) - base;
+                bool ok = true;
+                if (!sell) {
+                    HT* dst = hout + 9 * static_cast<size_t>(base);
+                    for (int t = lane; t < 9 * nb; t += 32) {
+                        const R val = stage[so + t];
+                        ok = ok && X::finite(val);
+                        dst[t] = static_cast<HT>(val);
+                    }
+                } else {
+                    const int qd = __ldg(m.diag_slot + v) - base, sb = __ldg(m.sell_base + v);
+                    for (int t = lane; t < 9 * (nb - qd); t += 32) {
+                        const int qq = t / 9, tt = t - 9 * qq;
+                        const R val = stage[so + 9 * qd + t];
+                        ok = ok && X::finite(val);
+                        hout[static_cast<int64_t>(sb) + 32 * static_cast<int64_t>(9 * qq + tt)] = static_cast<HT>(val);
+                    }
+                }
+                if (!ok) st |= ST_NONFINITE_OUT;
+            }
+        }
+        __syncthreads(); // the next cluster reuses the shared memory
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if (lane == 0 && st) atomicOr(a.status, st);
+}
+
+template <typename R, bool WG, bool WH, int MINB = tc_minb<R>(0)>
+void launch_tet_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+    const size_t sm = tc_smem_bytes<R>();
+    thread_local LaunchCache cache;
+    const int resident = resident_grid(tet_cluster_kernel<R, WG, WH, MINB>, kTcThreads, sm, cache);
+    const int blocks = std::min(resident, m.tc_ncl);
+    if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
+    if (blocks > 0) tet_cluster_kernel<R, WG, WH, MINB><<<blocks, kTcThreads, sm, s>>>(m, a);
+    if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
+    LPG_CUDA(cudaGetLastError());
+}
+
 // ---------------------------------------------------------------------------
 // Hessian assembly from per-element blocks (the projected Hessian: each element's clamped
 // tangent as ten 3x3 blocks in a.proj, pair10 order). The cluster plan of the Exact path without
@@ -2578,41 +2873,42 @@ __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __re
     rec32[12 * static_cast<size_t>(e) + 11] = static_cast<float>(mu);
 }
 
-// The Hessian-writing cluster kernel in the register-budget variant a.cl_variant.
-template <typename R, bool WG> void launch_cluster_variant(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
+// The Hessian-writing tet cluster kernel in the register-budget variant a.cl_variant.
+template <typename R, bool WG> void launch_tet_variant(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     switch (a.cl_variant) {
-    case 1: launch_cluster<R, WG, true, cl_minb<R>(1)>(m, a, s); break;
-    case 2: launch_cluster<R, WG, true, cl_minb<R>(2)>(m, a, s); break;
-    default: launch_cluster<R, WG, true>(m, a, s); break;
+    case 1: launch_tet_cluster<R, WG, true, tc_minb<R>(1)>(m, a, s); break;
+    case 2: launch_tet_cluster<R, WG, true, tc_minb<R>(2)>(m, a, s); break;
+    default: launch_tet_cluster<R, WG, true>(m, a, s); break;
     }
 }
 
 // Launches the element pass; returns the number of per-unit energies it wrote to cluster_energy.
-// The Exact Hessian, gradient and energy use the element-once cluster kernel; the projected
-// Hessian uses the pair kernel over the per-element clamped tangents.
+// Energy, gradient and the Exact Hessian come from the tet cluster kernel; the projected Hessian
+// is gathered from the per-element clamped blocks by the block gather.
 template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const EvalArgs& a, cudaStream_t s) {
     const bool wg = a.grad != nullptr;
     const int wh = a.hess == nullptr ? 0 : (hessian == LPG_HESSIAN_EXACT ? 1 : 2);
-    int units = m.ncl;
+    const int units = m.tc_ncl;
     if (wh == 2) {
         // Projected: energy (and gradient) from the element pass, the Hessian gathered from the
         // per-element clamped blocks; the optional events bracket both kernels.
         EvalArgs ea = a;
         ea.ev_end = nullptr;
+        ea.hess = nullptr;
         if (wg)
-            launch_cluster<R, true, false>(m, ea, s);
+            launch_tet_cluster<R, true, false>(m, ea, s);
         else
-            launch_cluster<R, false, false>(m, ea, s);
+            launch_tet_cluster<R, false, false>(m, ea, s);
         launch_block_gather<R>(m, a, s);
         if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
     } else if (wg && wh == 1) {
-        launch_cluster_variant<R, true>(m, a, s);
+        launch_tet_variant<R, true>(m, a, s);
     } else if (!wg && wh == 1) {
-        launch_cluster_variant<R, false>(m, a, s);
+        launch_tet_variant<R, false>(m, a, s);
     } else if (wg) {
-        launch_cluster<R, true, false>(m, a, s);
+        launch_tet_cluster<R, true, false>(m, a, s);
     } else {
-        launch_cluster<R, false, false>(m, a, s);
+        launch_tet_cluster<R, false, false>(m, a, s);
     }
     if (wg && m.num_unused > 0)
         zero_rows_kernel<<<(m.num_unused + 255) / 256, 256, 0, s>>>(a.grad, m.unused_rows, m.num_unused);
@@ -2624,7 +2920,7 @@ template <typename R> int launch_eval_t(const DevMesh& m, int hessian, const Eva
 size_t assembly_smem_bytes(const DevMesh& m) {
     const size_t gather = block_gather_bytes(m);
     if (m.K != 4) return gather;
-    return std::max(gather, std::max(cl_smem_bytes<double, true, true>(m), cl_smem_bytes<float, true, true>(m)));
+    return std::max(gather, std::max(tc_smem_bytes<double>(), tc_smem_bytes<float>()));
 }
 
 void launch_eval(const DevMesh& m, int precision, int hessian, const EvalArgs& a, cudaStream_t s) {

@@ -69,6 +69,31 @@ struct HostPlan {
     std::vector<uint32_t> cl_slot, cl_slot_ent;
     std::vector<int32_t> cl_ent_ptr;
     std::vector<uint16_t> cl_ents;
+    // Tet assembly clusters (cluster_kernel of tet meshes; empty for other cells). A cluster owns
+    // up to kTcRows rows; its elements (those incident to the rows, ascending, at most kTcElems;
+    // bit 31 on the ones whose energy it counts: those whose first vertex it owns) touch at most
+    // kTcVerts vertices (tc_verts, ascending); tc_loc packs each element's four local vertex
+    // indices (one byte each, vertex order). Output staging: row j of the cluster (tc_rows) keeps
+    // its 9 nb_j values at offset tc_row_so[j] (values), so_j = 9 sum_{i<j} nb_i.
+    // Items (4 words each): the cluster's diagonal blocks first (tc_ndiag of them), then its
+    // edge blocks, each group sorted by contributor count (descending):
+    //   w0: primary staging position (so 16 bits | block position q in the row << 16 | nb << 24)
+    //   w1: second position (same packing; the transposed block of an edge between two owned
+    //       rows) or 0xffffffff
+    //   w2: first contributor (within the cluster's list, 20 bits) | count << 20
+    //   w3: bit 31 diagonal, bit 30 the primary position stores the transpose; bits 0-7 the row
+    //       j of a diagonal block (its gradient row)
+    // An edge between two owned rows is summed once and stored at both positions; an edge to a
+    // row of another cluster is summed by each of the two clusters for its own row, in the same
+    // orientation (lower-numbered vertex first) and order, so both blocks are exact transposes.
+    // Contributors (uint16): element within the cluster << 8 | its block pair index (pair10 of
+    // the two local indices) << 4 | a << 2 | b, (a, b) the local indices of the lower- and
+    // higher-numbered vertex (a = b for a diagonal block), ascending by element (the
+    // reference's per-column order).
+    std::vector<int32_t> tc_row_ptr, tc_rows, tc_row_so;
+    std::vector<int32_t> tc_el_ptr, tc_vert_ptr, tc_verts, tc_item_ptr, tc_ndiag, tc_ent_ptr;
+    std::vector<uint32_t> tc_els, tc_loc, tc_items;
+    std::vector<uint16_t> tc_ents;
     // Value count of the solver layout: 9 per own slot, then the 9 x 32 zero block.
     int64_t sell_zero() const { return 9 * static_cast<int64_t>(sell_ptr.back()); }
     size_t sell_values() const { return static_cast<size_t>(sell_zero()) + 9 * 32; }
@@ -87,6 +112,22 @@ constexpr int kSellWindow = 128;
 #endif
 constexpr int kClusterRows = LPG_CLUSTER_ROWS;
 constexpr int kClusterElems = LPG_CLUSTER_ELEMS;
+// Limits of a tet assembly cluster (HostPlan::tc_*): owned rows, distinct incident elements
+// (their data is held in shared memory) and distinct vertices of those elements.
+#ifndef LPG_TC_ROWS
+#define LPG_TC_ROWS 64
+#endif
+#ifndef LPG_TC_ELEMS
+#define LPG_TC_ELEMS 256
+#endif
+#ifndef LPG_TC_VALS
+#define LPG_TC_VALS 4608
+#endif
+constexpr int kTcRows = LPG_TC_ROWS;
+constexpr int kTcElems = LPG_TC_ELEMS;
+constexpr int kTcVerts = 256;
+constexpr int kTcVals = LPG_TC_VALS; // output staging values of a cluster (its rows' 9 nb)
+static_assert(kTcElems <= 256 && kTcRows <= 256, "tet cluster indices are 8-bit");
 // Clusters of 64-node cells (Hermite hexes: 8 slot rows per vertex, ~216 blocks per row) hold at
 // most one vertex's rows, so a cluster's slot and contributor tables fit in shared memory.
 constexpr int kClusterRowsWide = 8;
@@ -111,6 +152,8 @@ void validate_volume_mesh(int V, const std::vector<double>& positions, int width
 void build_plan(int V, int T, const int32_t* cells, HostPlan& plan, int K = 4);
 // Checks the cluster plan's invariants (throws LPG_ELOGIC on a violation).
 void check_clusters(const HostPlan& plan, const int32_t* tets);
+// Checks the tet assembly clusters (HostPlan::tc_*) against the mesh (throws LPG_ELOGIC).
+void check_tet_clusters(const HostPlan& plan, const int32_t* tets);
 // Checks the solvers' upper-triangle sliced-ELL layout against the BSR pattern (LPG_ELOGIC).
 void check_solver_layout(const HostPlan& plan);
 
@@ -131,6 +174,15 @@ struct DevMesh {
             *cl_ntr = nullptr, *cl_ent_ptr = nullptr;
     uint32_t *cl_els = nullptr, *cl_slot = nullptr, *cl_slot_ent = nullptr;
     uint16_t* cl_ents = nullptr;
+    // Tet assembly clusters (HostPlan::tc_*), and their largest element, vertex, row and staging
+    // counts.
+    int tc_ncl = 0, tc_max_els = 0, tc_max_verts = 0, tc_max_vals = 0;
+    int32_t *tc_row_ptr = nullptr, *tc_rows = nullptr, *tc_row_so = nullptr, *tc_el_ptr = nullptr,
+            *tc_vert_ptr = nullptr, *tc_verts = nullptr, *tc_item_ptr = nullptr, *tc_ndiag = nullptr,
+            *tc_ent_ptr = nullptr;
+    uint32_t *tc_els = nullptr, *tc_loc = nullptr;
+    uint4* tc_items = nullptr;
+    uint16_t* tc_ents = nullptr;
     int4* tets = nullptr;
     // Per-element record: G (3x3 row-major, rows = grad N_1..3 in rest coordinates, times Fp^-1),
     // vol (= det(Dm)/6 * det Fp), lambda, mu. 12 values, 16-byte aligned.

@@ -169,6 +169,199 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
     }
 }
 
+// Tet assembly clusters (HostPlan::tc_*). Growth as build_clusters (breadth-first from the lowest
+// unassigned vertex), under the tet limits: a row joins while the cluster's distinct elements
+// stay within kTcElems and their distinct vertices within kTcVerts.
+void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>& inc) {
+    const int V = p.V, T = p.T;
+    const int kMaskE = (1 << inc_shift(4)) - 1;
+    auto vert = [&](int e, int a) { return tets[4 * static_cast<size_t>(e) + a]; };
+    std::vector<int32_t> cl_of(static_cast<size_t>(V), -1), qstamp(static_cast<size_t>(V), -1);
+    std::vector<int32_t> estamp(static_cast<size_t>(T), -1), vstamp(static_cast<size_t>(V), -1);
+    std::vector<int32_t> queue;
+    int ncl = 0;
+    for (int seed = 0; seed < V; ++seed) {
+        if (cl_of[seed] >= 0 || p.inc_ptr[seed + 1] == p.inc_ptr[seed]) continue;
+        const int c = ncl++;
+        queue.assign(1, seed);
+        qstamp[seed] = c;
+        int nr = 0, ne = 0, nv = 0, nvals = 0;
+        for (size_t qi = 0; qi < queue.size() && nr < kTcRows; ++qi) {
+            const int v = queue[qi];
+            if (cl_of[v] >= 0) continue;
+            int add_e = 0, add_v = 0;
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
+                const int e = inc[k] & kMaskE;
+                if (estamp[e] == c) continue;
+                ++add_e;
+                for (int a = 0; a < 4; ++a) {
+                    const int w = vert(e, a);
+                    if (vstamp[w] != c && vstamp[w] != -2 - c) {
+                        vstamp[w] = -2 - c; // counted once while sizing this row
+                        ++add_v;
+                    }
+                }
+            }
+            // Undo the provisional vertex marks.
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k)
+                for (int a = 0; a < 4; ++a)
+                    if (vstamp[vert(inc[k] & kMaskE, a)] == -2 - c) vstamp[vert(inc[k] & kMaskE, a)] = -1;
+            const int add_vals = 9 * (p.row_ptr[v + 1] - p.row_ptr[v]);
+            if (ne + add_e > kTcElems || nv + add_v > kTcVerts || nvals + add_vals > kTcVals) {
+                if (nr == 0) fail(LPG_EINVAL, "vertex neighbourhood exceeds the assembly cluster limits");
+                continue;
+            }
+            cl_of[v] = c;
+            ++nr;
+            ne += add_e;
+            nv += add_v;
+            nvals += add_vals;
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
+                const int e = inc[k] & kMaskE;
+                estamp[e] = c;
+                for (int a = 0; a < 4; ++a) vstamp[vert(e, a)] = c;
+            }
+            for (int k = p.row_ptr[v]; k < p.row_ptr[v + 1]; ++k) {
+                const int w = p.col_idx[k];
+                if (cl_of[w] < 0 && qstamp[w] != c && p.inc_ptr[w + 1] > p.inc_ptr[w]) {
+                    qstamp[w] = c;
+                    queue.push_back(w);
+                }
+            }
+        }
+    }
+    p.tc_row_ptr.assign(static_cast<size_t>(ncl) + 1, 0);
+    for (int v = 0; v < V; ++v)
+        if (cl_of[v] >= 0) ++p.tc_row_ptr[cl_of[v] + 1];
+    for (int c = 0; c < ncl; ++c) p.tc_row_ptr[c + 1] += p.tc_row_ptr[c];
+    p.tc_rows.assign(static_cast<size_t>(p.tc_row_ptr[ncl]), 0);
+    {
+        std::vector<int32_t> fill(p.tc_row_ptr.begin(), p.tc_row_ptr.end() - 1);
+        for (int v = 0; v < V; ++v)
+            if (cl_of[v] >= 0) p.tc_rows[fill[cl_of[v]]++] = v;
+    }
+    p.tc_row_so.assign(p.tc_rows.size(), 0);
+    p.tc_el_ptr.assign(1, 0);
+    p.tc_vert_ptr.assign(1, 0);
+    p.tc_item_ptr.assign(1, 0);
+    p.tc_ent_ptr.assign(1, 0);
+    p.tc_els.clear();
+    p.tc_loc.clear();
+    p.tc_verts.clear();
+    p.tc_items.clear();
+    p.tc_ndiag.clear();
+    p.tc_ents.clear();
+    std::vector<int32_t> eloc(static_cast<size_t>(T), -1), vloc(static_cast<size_t>(V), -1), rloc(static_cast<size_t>(V), -1);
+    std::vector<int32_t> els, verts;
+    struct Item {
+        uint32_t w0, w1, w3;
+        std::vector<uint16_t> ents;
+    };
+    std::vector<Item> diag, edge;
+    auto pack = [](int so, int q, int nb) {
+        return static_cast<uint32_t>(so) | (static_cast<uint32_t>(q) << 16) | (static_cast<uint32_t>(nb) << 24);
+    };
+    for (int c = 0; c < ncl; ++c) {
+        const int r0 = p.tc_row_ptr[c], nr = p.tc_row_ptr[c + 1] - r0;
+        els.clear();
+        verts.clear();
+        int so = 0;
+        for (int j = 0; j < nr; ++j) {
+            const int v = p.tc_rows[r0 + j];
+            rloc[v] = j;
+            p.tc_row_so[r0 + j] = so;
+            const int nb = p.row_ptr[v + 1] - p.row_ptr[v];
+            if (nb > 255) fail(LPG_EINVAL, "vertex has more than 254 neighbours (assembly plan limit)");
+            so += 9 * nb;
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) els.push_back(inc[k] & kMaskE);
+        }
+        if (so > 65535) fail(LPG_EINVAL, "assembly cluster output exceeds its staging index range");
+        std::sort(els.begin(), els.end());
+        els.erase(std::unique(els.begin(), els.end()), els.end());
+        for (int e : els)
+            for (int a = 0; a < 4; ++a) verts.push_back(vert(e, a));
+        std::sort(verts.begin(), verts.end());
+        verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
+        for (size_t i = 0; i < verts.size(); ++i) {
+            vloc[verts[i]] = static_cast<int32_t>(i);
+            p.tc_verts.push_back(verts[i]);
+        }
+        for (size_t i = 0; i < els.size(); ++i) {
+            const int e = els[i];
+            eloc[e] = static_cast<int32_t>(i);
+            const bool owner = cl_of[vert(e, 0)] == c;
+            p.tc_els.push_back(static_cast<uint32_t>(e) | (owner ? 0x80000000u : 0u));
+            uint32_t loc = 0;
+            for (int a = 0; a < 4; ++a) loc |= static_cast<uint32_t>(vloc[vert(e, a)]) << (8 * a);
+            p.tc_loc.push_back(loc);
+        }
+        diag.clear();
+        edge.clear();
+        for (int j = 0; j < nr; ++j) {
+            const int v = p.tc_rows[r0 + j];
+            const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
+            // Contributors of every block of row v, in element order (the incidence is ascending).
+            std::vector<std::vector<uint16_t>> bucket(static_cast<size_t>(nb));
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
+                const int e = inc[k] & kMaskE;
+                const int a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> inc_shift(4));
+                const uint32_t el = static_cast<uint32_t>(eloc[e]) << 8;
+                for (int b = 0; b < 4; ++b) {
+                    const int w = vert(e, b);
+                    const int32_t* beg = p.col_idx.data() + rb;
+                    const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
+                    const int lo = v <= w ? a : b, hi = v <= w ? b : a;
+                    const int x = std::min(a, b), y = std::max(a, b);
+                    const int pr = x * 4 - (x * (x - 1)) / 2 + (y - x); // element block pair index (a <= b order)
+                    bucket[q].push_back(static_cast<uint16_t>(el | static_cast<uint32_t>((pr << 4) | (lo << 2) | hi)));
+                }
+            }
+            for (int q = 0; q < nb; ++q) {
+                const int w = p.col_idx[rb + q];
+                if (w == v) {
+                    diag.push_back({pack(p.tc_row_so[r0 + j], q, nb), 0xffffffffu, 0x80000000u | static_cast<uint32_t>(j),
+                                    std::move(bucket[q])});
+                } else if (cl_of[w] == c) {
+                    if (v > w) continue; // summed with the lower row's item
+                    const int k = rloc[w];
+                    const int wb = p.row_ptr[w], wn = p.row_ptr[w + 1] - wb;
+                    const int qw = static_cast<int>(std::lower_bound(p.col_idx.data() + wb, p.col_idx.data() + wb + wn, v) -
+                                                    (p.col_idx.data() + wb));
+                    edge.push_back({pack(p.tc_row_so[r0 + j], q, nb), pack(p.tc_row_so[r0 + k], qw, wn), 0u,
+                                    std::move(bucket[q])});
+                } else {
+                    edge.push_back({pack(p.tc_row_so[r0 + j], q, nb), 0xffffffffu, v > w ? 0x40000000u : 0u,
+                                    std::move(bucket[q])});
+                }
+            }
+        }
+        auto by_count = [](const Item& x, const Item& y) { return x.ents.size() > y.ents.size(); };
+        std::stable_sort(diag.begin(), diag.end(), by_count);
+        std::stable_sort(edge.begin(), edge.end(), by_count);
+        const size_t ent0 = p.tc_ents.size();
+        for (const auto* group : {&diag, &edge})
+            for (const Item& it : *group) {
+                const size_t first = p.tc_ents.size() - ent0;
+                if (first >= (1u << 20) || it.ents.size() >= (1u << 12))
+                    fail(LPG_EINVAL, "mesh too large for the assembly plan's index ranges");
+                p.tc_items.insert(p.tc_items.end(),
+                                  {it.w0, it.w1, static_cast<uint32_t>(first) | (static_cast<uint32_t>(it.ents.size()) << 20), it.w3});
+                p.tc_ents.insert(p.tc_ents.end(), it.ents.begin(), it.ents.end());
+            }
+        while (p.tc_ents.size() % 8 != 0) p.tc_ents.push_back(0); // 16-byte aligned per cluster
+        p.tc_ndiag.push_back(static_cast<int32_t>(diag.size()));
+        p.tc_el_ptr.push_back(static_cast<int32_t>(p.tc_els.size()));
+        p.tc_vert_ptr.push_back(static_cast<int32_t>(p.tc_verts.size()));
+        p.tc_item_ptr.push_back(static_cast<int32_t>(p.tc_items.size() / 4));
+        p.tc_ent_ptr.push_back(static_cast<int32_t>(p.tc_ents.size()));
+        if (p.tc_ents.size() >= static_cast<size_t>(std::numeric_limits<int32_t>::max()))
+            fail(LPG_EINVAL, "mesh too large for the assembly plan's index ranges");
+        for (int e : els) eloc[e] = -1;
+        for (int w : verts) vloc[w] = -1;
+        for (int j = 0; j < nr; ++j) rloc[p.tc_rows[r0 + j]] = -1;
+    }
+}
+
 } // namespace
 
 void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
@@ -311,6 +504,7 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
     for (int v = 0; v < V; ++v)
         if (p.inc_ptr[v + 1] == p.inc_ptr[v]) p.unused_rows.push_back(v); // no element: zero gradient, no blocks
     build_clusters(p, tets, inc);
+    if (K == 4) build_tet_clusters(p, tets, inc);
 }
 
 void check_clusters(const HostPlan& p, const int32_t* tets) {
@@ -404,6 +598,136 @@ void check_clusters(const HostPlan& p, const int32_t* tets) {
     if (contributors != static_cast<size_t>(K) * K * T) bad("contributor total differs from K^2 per element");
     for (int c = 0; c < ncl; ++c)
         if (p.cl_ent_ptr[c] % 8 != 0) bad("contributor lists not 16-byte aligned");
+}
+
+void check_tet_clusters(const HostPlan& p, const int32_t* tets) {
+    auto bad = [](const char* what) { fail(LPG_ELOGIC, std::string("tet assembly plan: ") + what); };
+    if (p.K != 4) {
+        if (!p.tc_items.empty()) bad("tet clusters on a non-tet mesh");
+        return;
+    }
+    const int V = p.V, T = p.T;
+    auto vert = [&](int e, int a) { return tets[4 * static_cast<size_t>(e) + a]; };
+    const int ncl = static_cast<int>(p.tc_row_ptr.size()) - 1;
+    std::vector<int> owner(static_cast<size_t>(V), -1), energy_count(static_cast<size_t>(T), 0);
+    for (int c = 0; c < ncl; ++c)
+        for (int k = p.tc_row_ptr[c]; k < p.tc_row_ptr[c + 1]; ++k) {
+            if (owner[p.tc_rows[k]] >= 0) bad("vertex owned twice");
+            owner[p.tc_rows[k]] = c;
+        }
+    for (int v = 0; v < V; ++v)
+        if ((owner[v] >= 0) != (p.inc_ptr[v + 1] > p.inc_ptr[v])) bad("referenced vertex without a cluster");
+    // Every block of every row must be written exactly once, with the right contributors.
+    std::vector<char> written(static_cast<size_t>(p.nnzb()), 0);
+    std::vector<int> incident;
+    for (int c = 0; c < ncl; ++c) {
+        const int r0 = p.tc_row_ptr[c], nr = p.tc_row_ptr[c + 1] - r0;
+        const int e0 = p.tc_el_ptr[c], ne = p.tc_el_ptr[c + 1] - e0;
+        const int v0 = p.tc_vert_ptr[c], nv = p.tc_vert_ptr[c + 1] - v0;
+        if (nr > kTcRows || ne > kTcElems || nv > kTcVerts) bad("cluster over its limits");
+        if (nr == 0) bad("cluster without rows");
+        {
+            const int vl = p.tc_rows[r0 + nr - 1];
+            if (p.tc_row_so[r0 + nr - 1] + 9 * (p.row_ptr[vl + 1] - p.row_ptr[vl]) > kTcVals)
+                bad("cluster staging over its limit");
+        }
+        for (int i = 0; i < nv; ++i)
+            if (i > 0 && p.tc_verts[v0 + i] <= p.tc_verts[v0 + i - 1]) bad("vertices not ascending");
+        for (int i = 0; i < ne; ++i) {
+            const int e = static_cast<int>(p.tc_els[e0 + i] & 0x7fffffffu);
+            if (e >= T || (i > 0 && e <= static_cast<int>(p.tc_els[e0 + i - 1] & 0x7fffffffu))) bad("elements not ascending");
+            bool touches = false;
+            for (int a = 0; a < 4; ++a) {
+                const int lv = static_cast<int>((p.tc_loc[e0 + i] >> (8 * a)) & 0xffu);
+                if (lv >= nv || p.tc_verts[v0 + lv] != vert(e, a)) bad("local vertex index");
+                touches = touches || owner[vert(e, a)] == c;
+            }
+            if (!touches) bad("element not incident to the cluster");
+            if (p.tc_els[e0 + i] >> 31) {
+                if (owner[vert(e, 0)] != c) bad("energy counted by a non-owner");
+                ++energy_count[e];
+            }
+        }
+        // Staging offsets: rows back to back.
+        int so = 0;
+        for (int j = 0; j < nr; ++j) {
+            const int v = p.tc_rows[r0 + j];
+            if (j > 0 && v <= p.tc_rows[r0 + j - 1]) bad("rows not ascending");
+            if (p.tc_row_so[r0 + j] != so) bad("row staging offset");
+            so += 9 * (p.row_ptr[v + 1] - p.row_ptr[v]);
+        }
+        const int i0 = p.tc_item_ptr[c], ni = p.tc_item_ptr[c + 1] - i0;
+        const int nd = p.tc_ndiag[c];
+        if (nd != nr) bad("one diagonal item per row");
+        size_t prev = ~size_t(0);
+        for (int it = 0; it < ni; ++it) {
+            const uint32_t* w = p.tc_items.data() + 4 * static_cast<size_t>(i0 + it);
+            const bool dg = w[3] >> 31, tr = (w[3] >> 30) & 1u;
+            if ((it < nd) != dg) bad("diagonal items first");
+            const size_t cnt = w[2] >> 20;
+            if (it == nd) prev = ~size_t(0);
+            if (cnt > prev) bad("items not sorted by contributor count");
+            prev = cnt;
+            // Decode a staging position into (row j, block q) and check its packing.
+            auto locate = [&](uint32_t pos, int& j, int& q) {
+                const int s0 = static_cast<int>(pos & 0xffffu), qq = static_cast<int>((pos >> 16) & 0xffu),
+                          nb = static_cast<int>(pos >> 24);
+                j = -1;
+                for (int r = 0; r < nr; ++r)
+                    if (p.tc_row_so[r0 + r] == s0) j = r;
+                if (j < 0) bad("staging position is not a row start");
+                const int v = p.tc_rows[r0 + j];
+                if (nb != p.row_ptr[v + 1] - p.row_ptr[v] || qq >= nb) bad("staging position row length");
+                q = qq;
+            };
+            int j1, q1;
+            locate(w[0], j1, q1);
+            const int v = p.tc_rows[r0 + j1];
+            const int x = p.col_idx[p.row_ptr[v] + q1];
+            if (dg != (x == v)) bad("diagonal flag");
+            if (dg && static_cast<int>(w[3] & 0xffu) != j1) bad("diagonal row index");
+            if (written[p.row_ptr[v] + q1]++) bad("block written twice");
+            if (w[1] != 0xffffffffu) {
+                int j2, q2;
+                locate(w[1], j2, q2);
+                const int xv = p.tc_rows[r0 + j2];
+                if (dg || owner[x] != c || xv != x || p.col_idx[p.row_ptr[x] + q2] != v || v > x || tr)
+                    bad("second position of an owned edge");
+                if (written[p.row_ptr[x] + q2]++) bad("block written twice");
+            } else if (!dg) {
+                if (owner[x] == c) bad("owned edge without its transpose");
+                if (tr != (v > x)) bad("transpose flag");
+            }
+            const int lo = std::min(v, x), hi = std::max(v, x);
+            // Expected contributors: the elements holding both vertices, ascending.
+            incident.clear();
+            for (int e = 0; e < ne; ++e) {
+                const int ge = static_cast<int>(p.tc_els[e0 + e] & 0x7fffffffu);
+                bool hv = false, hx = false;
+                for (int a = 0; a < 4; ++a) {
+                    hv = hv || vert(ge, a) == v;
+                    hx = hx || vert(ge, a) == x;
+                }
+                if (hv && hx) incident.push_back(e);
+            }
+            if (cnt != incident.size()) bad("item contributor count");
+            const size_t off = static_cast<size_t>(p.tc_ent_ptr[c]) + (w[2] & 0xfffffu);
+            for (size_t t = 0; t < cnt; ++t) {
+                const uint16_t en = p.tc_ents[off + t];
+                const int el = en >> 8, pr = (en >> 4) & 15, a = (en >> 2) & 3, b = en & 3;
+                if (el != incident[t]) bad("contributor list differs from the elements sharing the block");
+                const int ge = static_cast<int>(p.tc_els[e0 + el] & 0x7fffffffu);
+                if (vert(ge, a) != lo || vert(ge, b) != hi) bad("contributor local indices");
+                const int x = std::min(a, b), y = std::max(a, b);
+                if (pr != x * 4 - (x * (x - 1)) / 2 + (y - x)) bad("contributor pair index");
+            }
+        }
+        if (p.tc_ent_ptr[c] % 8 != 0) bad("contributor lists not 16-byte aligned");
+    }
+    for (int64_t k = 0; k < p.nnzb(); ++k)
+        if (!written[k]) bad("block not written");
+    for (int e = 0; e < T; ++e)
+        if (energy_count[e] != 1) bad("element energy not counted exactly once");
 }
 
 void check_solver_layout(const HostPlan& p) {

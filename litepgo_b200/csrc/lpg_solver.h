@@ -38,6 +38,7 @@ struct lpg_fem {
     lpg::DeviceBuffer b_hex[4]; // hex meshes: rest positions, cells, [lambda, mu], quadrature table
     lpg::DeviceBuffer b_herm;   // Hermite hex meshes: box edge lengths per element
     lpg::DeviceBuffer b_cl[11]; // assembly clusters
+    lpg::DeviceBuffer b_tc[13]; // tet assembly clusters
     lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers
     lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton
     // Scratch of the evaluation entry points.
