@@ -27,6 +27,7 @@
  *   LPG_ECUDA   <- a CUDA runtime failure
  *   LPG_ELOGIC  <- a broken contract (std::logic_error)
  *   LPG_EIO     <- std::runtime_error of the mesh-file readers (missing file, bad format)
+ *   LPG_ESTOPPED <- an exception raised by a caller's per-iteration callback (the solve stops)
  *
  * Memory: the library owns its device buffers. Array arguments carry an
  * explicit LPG_MEM_HOST / LPG_MEM_DEVICE flag. Device pointers must be device
@@ -53,7 +54,8 @@ enum lpg_status {
     LPG_ENOCONV = 4,
     LPG_ECUDA = 5,
     LPG_ELOGIC = 6,
-    LPG_EIO = 7
+    LPG_EIO = 7,
+    LPG_ESTOPPED = 8 /* a caller's per-iteration callback asked the solve to stop */
 };
 
 /* HessianKind (src/core/energy/scalar/energy.hpp:6-13); NONE = no Hessian. */
@@ -306,6 +308,59 @@ void lpg_newton_default_options(lpg_newton_options* options);
  */
 int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed_dofs, int num_fixed, const double* f_ext, const double* x0,
                      int io_mem, const lpg_newton_options* options, double* x_out, lpg_newton_result* result);
+
+/*
+ * What one Newton iteration did: the reference's NewtonStep (src/core/solver/newton.hpp:34-44),
+ * reported at the same points (after each accepted step, and once for the iteration that ends
+ * the solve; newton.cpp:123-181), plus two fields it does not have.
+ */
+typedef struct {
+    int iteration;
+    double energy;
+    double gradient_norm;        /* max |g| over the free DOFs (the reference's norm) */
+    int pattern_changed;         /* 1 on the first evaluation (the Hessian pattern is fixed after it) */
+    int diagonal_shifts;         /* diagonal shifts of the descent-direction search (10 when none worked) */
+    double feasible_step;        /* max_feasible_step's bound on the step; 0 when no search ran */
+    double step;                 /* the accepted step length; 0 when none was */
+    int line_search_evaluations;
+    double gradient_norm_2;      /* ||g_free||_2 (not in the reference) */
+    int64_t cg_iterations;       /* PCG iterations of this iteration (not in the reference) */
+} lpg_newton_step;
+
+/* Per-iteration callback: return 0 to continue; any other value stops the solve, which then
+ * returns LPG_ESTOPPED (for a binding's callback that raised). */
+typedef int (*lpg_newton_callback)(const lpg_newton_step* step, void* user);
+
+/*
+ * The terms of a weighted-sum potential around the handle's elastic energy, for
+ * lpg_newton_solve_terms (the reference's WeightedSumEnergy, weighted_sum_energy.hpp:16-47, of
+ * one VolumetricFemEnergy and QuadraticEnergy terms, quadratic_energy.hpp:10-20, summed
+ * beforehand into one A; f_ext carries the linear part):
+ *   E(x) = elastic_weight elastic(x) + 1/2 x^T A x - f_ext . x + constant.
+ * A is a scalar CSR matrix on the host (num_dofs rows, a_indptr[num_dofs + 1], a_indices and
+ * a_values of a_indptr[num_dofs] entries; duplicates are summed) or a_indptr = NULL for none. It
+ * must be symmetric and lie inside the elastic Hessian's pattern (vertex pairs sharing an
+ * element), else LPG_EINVAL. on_iteration (may be NULL) is called with user at every step.
+ */
+typedef struct {
+    double elastic_weight; /* finite and non-zero; 1 for the elastic energy alone */
+    const int32_t* a_indptr;
+    const int32_t* a_indices;
+    const double* a_values;
+    double constant;
+    lpg_newton_callback on_iteration;
+    void* user;
+} lpg_newton_terms;
+
+/*
+ * lpg_newton_solve over the weighted-sum potential of terms (NULL: the elastic energy and the
+ * load alone, as lpg_newton_solve). Replaces newton_solve(energy, fixed, x0, options, solver,
+ * on_iteration) (src/core/solver/newton.hpp:67-69; binding src/binding/solver/newton.cpp:62-82)
+ * for such an energy, with its on_iteration callback.
+ */
+int lpg_newton_solve_terms(lpg_fem_t h, const lpg_newton_terms* terms, const int32_t* fixed_dofs, int num_fixed,
+                           const double* f_ext, const double* x0, int io_mem, const lpg_newton_options* options,
+                           double* x_out, lpg_newton_result* result);
 
 /* Per-mesh outcome of lpg_batch_newton_solve (status as lpg_newton_result.status). */
 typedef struct {

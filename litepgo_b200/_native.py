@@ -12,7 +12,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_lib" / "liblpg_b200.so"
 
-LPG_OK, LPG_EINVAL, LPG_EDOMAIN, LPG_EBUSY, LPG_ENOCONV, LPG_ECUDA, LPG_ELOGIC, LPG_EIO = range(8)
+LPG_OK, LPG_EINVAL, LPG_EDOMAIN, LPG_EBUSY, LPG_ENOCONV, LPG_ECUDA, LPG_ELOGIC, LPG_EIO, LPG_ESTOPPED = range(9)
 HESSIAN_NONE, HESSIAN_EXACT, HESSIAN_PROJECTED = range(3)
 PRECISION_F64, PRECISION_MIXED = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -70,6 +70,36 @@ class BatchMeshResultC(ctypes.Structure):
     ]
 
 
+class NewtonStepC(ctypes.Structure):
+    _fields_ = [
+        ("iteration", ctypes.c_int),
+        ("energy", ctypes.c_double),
+        ("gradient_norm", ctypes.c_double),
+        ("pattern_changed", ctypes.c_int),
+        ("diagonal_shifts", ctypes.c_int),
+        ("feasible_step", ctypes.c_double),
+        ("step", ctypes.c_double),
+        ("line_search_evaluations", ctypes.c_int),
+        ("gradient_norm_2", ctypes.c_double),
+        ("cg_iterations", ctypes.c_int64),
+    ]
+
+
+NEWTON_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(NewtonStepC), ctypes.c_void_p)
+
+
+class NewtonTermsC(ctypes.Structure):
+    _fields_ = [
+        ("elastic_weight", ctypes.c_double),
+        ("a_indptr", _ip),
+        ("a_indices", _ip),
+        ("a_values", _dp),
+        ("constant", ctypes.c_double),
+        ("on_iteration", NEWTON_CALLBACK),
+        ("user", ctypes.c_void_p),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 SIGNATURES = [
     ("lpg_last_error", ctypes.c_char_p, []),
@@ -93,6 +123,8 @@ SIGNATURES = [
     ("lpg_newton_default_options", None, [ctypes.POINTER(NewtonOptionsC)]),
     ("lpg_newton_solve", _int, [_vp, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC), _vp,
                                 ctypes.POINTER(NewtonResultC)]),
+    ("lpg_newton_solve_terms", _int, [_vp, ctypes.POINTER(NewtonTermsC), _ip, _int, _vp, _vp, _int,
+                                      ctypes.POINTER(NewtonOptionsC), _vp, ctypes.POINTER(NewtonResultC)]),
     ("lpg_batch_newton_solve", _int, [_vp, _int, _ip, _ip, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC),
                                       _vp, ctypes.POINTER(BatchMeshResultC), ctypes.POINTER(NewtonResultC)]),
     ("lpg_adjoint_theta", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _int, _vp, _vp]),

@@ -894,6 +894,17 @@ int lpg_newton_solve(lpg_fem_t h, const int32_t* fixed, int nfixed, const double
     });
 }
 
+int lpg_newton_solve_terms(lpg_fem_t h, const lpg_newton_terms* terms, const int32_t* fixed, int nfixed,
+                           const double* f_ext, const double* x0, int io_mem, const lpg_newton_options* o,
+                           double* x_out, lpg_newton_result* res) {
+    return guarded([&] {
+        if (!h || !o || !x0 || !x_out) fail(LPG_EINVAL, "lpg_newton_solve_terms: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        newton_solve(*h, fixed, nfixed, f_ext, x0, io_mem, *o, x_out, res, terms);
+    });
+}
+
 int lpg_fem_set_fp(lpg_fem_t h, const double* Fp, int fp_per_element) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");

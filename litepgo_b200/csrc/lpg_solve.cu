@@ -535,6 +535,35 @@ __global__ void residual_kernel(const double* __restrict__ b, const double* __re
     if (i < n) r[i] = mask[i] * (b[i] - y[i]);
 }
 // g = g_el - f ; out = -g masked (the Newton right-hand side).
+// y = A x for a scalar CSR matrix (one thread per row, entries in stored order).
+__global__ void csr_apply_kernel(const int32_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                                 const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                                 int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = 0;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) acc = fma(val[k], x[col[k]], acc);
+    y[i] = acc;
+}
+// g = w g (+ y when y is given).
+__global__ void scale_add_kernel(double* __restrict__ g, double w, const double* __restrict__ y, size_t n) {
+    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    double v = g[i] * w;
+    if (y) v += y[i];
+    g[i] = v;
+}
+template <typename R> __global__ void scale_values_kernel(R* __restrict__ v, size_t n, double w) {
+    const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i < n) v[i] = static_cast<R>(static_cast<double>(v[i]) * w);
+}
+// Adds the quadratic term's entries at their solver-layout positions (distinct positions).
+template <typename R>
+__global__ void add_at_kernel(R* __restrict__ K, const int64_t* __restrict__ pos, const double* __restrict__ val, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) K[pos[i]] = static_cast<R>(static_cast<double>(K[pos[i]]) + val[i]);
+}
+
 __global__ void load_gradient(double* __restrict__ g, const double* __restrict__ f, size_t n) {
     const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
     if (i < n && f) g[i] -= f[i];
@@ -602,12 +631,27 @@ template <typename Kern> int one_wave(Kern kernel, size_t work) {
 // ---------------------------------------------------------------------------
 // Host-side helpers bound to one handle.
 // ---------------------------------------------------------------------------
+// A weighted-sum potential around the elastic energy (lpg_newton_terms) on the device:
+//   E = w elastic + 1/2 x^T A x + c (the linear load is handled as f_ext).
+struct Potential {
+    double w = 1.0, c = 0.0;
+    int n = 0;                                    // rows of A (0: no quadratic term)
+    int32_t *ptr = nullptr, *col = nullptr;       // A, CSR (duplicates merged)
+    double* val = nullptr;
+    int nk = 0;                                   // A's entries in the solver layout's upper blocks
+    int64_t* kpos = nullptr;
+    double* kval = nullptr;
+    double* Ax = nullptr;                         // scratch, n values
+};
+
 struct Solver {
     lpg_fem& h;
     cudaStream_t s;
     size_t n;
     int V;
-    explicit Solver(lpg_fem& hh) : h(hh), s(hh.stream), n(3 * static_cast<size_t>(hh.dm.V)), V(hh.dm.V) {}
+    const Potential* P = nullptr;
+    explicit Solver(lpg_fem& hh, const Potential* p = nullptr)
+        : h(hh), s(hh.stream), n(3 * static_cast<size_t>(hh.dm.V)), V(hh.dm.V), P(p) {}
 
     // {sum m a b, sum m a^2, max m|a|, sum m b^2}
     template <typename TA, typename TB> std::array<double, 4> stats(const TA* a, const TB* b, const double* mask) {
@@ -631,11 +675,36 @@ struct Solver {
     // E(x) (FP64) with optional gradient g (FP64, load included); throws on bad status.
     double energy(const double* x, const double* f, double* g) {
         h.eval_async(x, g, LPG_HESSIAN_NONE, LPG_PRECISION_F64, LPG_LAYOUT_BSR, nullptr, nullptr);
+        return compose(x, f, g);
+    }
+    // The potential from the elastic evaluation just enqueued (energy in h.d_energy, gradient
+    // in g if given): weight, quadratic term, load and constant.
+    double compose(const double* x, const double* f, double* g) {
+        double aq = 0;
+        if (P && (P->w != 1.0 || P->n > 0)) {
+            if (P->n > 0)
+                csr_apply_kernel<<<grid(static_cast<size_t>(P->n)), kThreads, 0, s>>>(P->ptr, P->col, P->val, x, P->Ax,
+                                                                                    P->n);
+            if (g) scale_add_kernel<<<grid(n), kThreads, 0, s>>>(g, P->w, P->n > 0 ? P->Ax : nullptr, n);
+            LPG_CUDA(cudaGetLastError());
+        }
         if (g && f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
         double e = 0;
         LPG_CUDA(cudaMemcpyAsync(&e, h.d_energy.ptr, sizeof e, cudaMemcpyDeviceToHost, s));
         raise_status(h.take_status());
+        if (P && P->n > 0) aq = 0.5 * stats<double, double>(x, P->Ax, nullptr)[0];
+        if (P) e = P->w * e + aq + P->c;
         return e - energy_dot_f(x, f);
+    }
+    // The quadratic term and weight applied to a solver-layout Hessian of precision R.
+    template <typename R> void compose_hessian(R* K) {
+        if (!P) return;
+        if (P->w != 1.0) {
+            const size_t nv = h.plan.sell_values();
+            scale_values_kernel<R><<<grid(nv), kThreads, 0, s>>>(K, nv, P->w);
+        }
+        if (P->nk > 0) add_at_kernel<R><<<grid(static_cast<size_t>(P->nk)), kThreads, 0, s>>>(K, P->kpos, P->kval, P->nk);
+        LPG_CUDA(cudaGetLastError());
     }
 
     // One warp per sliced-ELL chunk (8 per block). Not persistent: with about one chunk per
@@ -791,8 +860,98 @@ void make_mask(lpg_fem& h, const int32_t* fixed, int nfixed, double* mask) {
 
 } // namespace
 
+namespace {
+
+// The quadratic term of a weighted-sum potential on the device: A merged and checked on the host
+// (symmetric, inside the elastic pattern), its CSR for A x, and its entries of the solver
+// layout's upper blocks (row vertex <= column vertex) for the Hessian.
+void build_potential(lpg_fem& h, const lpg_newton_terms* t, Potential& P) {
+    if (!t) return;
+    if (!std::isfinite(t->elastic_weight) || t->elastic_weight == 0.0)
+        fail(LPG_EINVAL, "WeightedSumEnergy weights must be finite and nonzero");
+    if (!std::isfinite(t->constant)) fail(LPG_EINVAL, "newton_solve: the potential's constant must be finite");
+    P.w = t->elastic_weight;
+    P.c = t->constant;
+    if (!t->a_indptr) return;
+    const HostPlan& p = h.plan;
+    const int n = 3 * p.V;
+    if (!t->a_indices || !t->a_values) fail(LPG_EINVAL, "QuadraticEnergy: null CSR arrays");
+    if (t->a_indptr[0] != 0) fail(LPG_EINVAL, "QuadraticEnergy: CSR row pointers must start at 0");
+    struct Ent {
+        int r, c;
+        double v;
+    };
+    std::vector<Ent> ents;
+    for (int r = 0; r < n; ++r) {
+        if (t->a_indptr[r + 1] < t->a_indptr[r]) fail(LPG_EINVAL, "QuadraticEnergy: CSR row pointers must not decrease");
+        for (int k = t->a_indptr[r]; k < t->a_indptr[r + 1]; ++k) {
+            const int c = t->a_indices[k];
+            const double v = t->a_values[k];
+            if (c < 0 || c >= n) fail(LPG_EINVAL, "QuadraticEnergy: column index out of range");
+            if (!std::isfinite(v)) fail(LPG_EINVAL, "QuadraticEnergy: A must be finite");
+            ents.push_back({r, c, v});
+        }
+    }
+    std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
+    std::vector<Ent> m;
+    for (const Ent& e : ents) {
+        if (!m.empty() && m.back().r == e.r && m.back().c == e.c)
+            m.back().v += e.v;
+        else
+            m.push_back(e);
+    }
+    // Symmetry: entry (c, r) equals entry (r, c).
+    auto find = [&](int r, int c) -> const Ent* {
+        auto it = std::lower_bound(m.begin(), m.end(), Ent{r, c, 0},
+                                   [](const Ent& a, const Ent& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
+        return it != m.end() && it->r == r && it->c == c ? &*it : nullptr;
+    };
+    std::vector<int32_t> ptr(static_cast<size_t>(n) + 1, 0), col;
+    std::vector<double> val;
+    std::vector<int64_t> kpos;
+    std::vector<double> kval;
+    for (const Ent& e : m) {
+        const Ent* tr = find(e.c, e.r);
+        if (!tr || tr->v != e.v) fail(LPG_EINVAL, "QuadraticEnergy: A must be symmetric on the GPU Newton path");
+        ++ptr[e.r + 1];
+        col.push_back(e.c);
+        val.push_back(e.v);
+        const int vr = e.r / 3, vc = e.c / 3;
+        const int32_t* beg = p.col_idx.data() + p.row_ptr[vr];
+        const int32_t* end = p.col_idx.data() + p.row_ptr[vr + 1];
+        const int32_t* at = std::lower_bound(beg, end, vc);
+        if (at == end || *at != vc)
+            fail(LPG_EINVAL, "QuadraticEnergy: A couples DOFs of vertices that share no element (outside the elastic "
+                             "Hessian's pattern), which the GPU Newton path does not support");
+        if (vr <= vc && e.v != 0.0) {
+            const int k = static_cast<int>(at - p.col_idx.data());
+            kpos.push_back(static_cast<int64_t>(p.sell_base[vr]) +
+                           32 * static_cast<int64_t>(9 * (k - p.diag_slot[vr]) + 3 * (e.r % 3) + (e.c % 3)));
+            kval.push_back(e.v);
+        }
+    }
+    for (int r = 0; r < n; ++r) ptr[r + 1] += ptr[r];
+    auto up = [&](lpg::DeviceBuffer& b, const auto& v) {
+        using T = typename std::decay_t<decltype(v)>::value_type;
+        T* d = b.as<T>(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) LPG_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h.stream));
+        return d;
+    };
+    P.n = n;
+    P.ptr = up(h.s_q[0], ptr);
+    P.col = up(h.s_q[1], col);
+    P.val = up(h.s_q[2], val);
+    P.nk = static_cast<int>(kpos.size());
+    P.kpos = up(h.s_q[3], kpos);
+    P.kval = up(h.s_q[4], kval);
+    P.Ax = h.s_q[5].as<double>(std::max<size_t>(n, 1));
+    LPG_CUDA(cudaStreamSynchronize(h.stream)); // the host vectors go out of scope
+}
+
+} // namespace
+
 void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
-                  const lpg_newton_options& o, double* x_out, lpg_newton_result* res) {
+                  const lpg_newton_options& o, double* x_out, lpg_newton_result* res, const lpg_newton_terms* terms) {
     if (!(o.gradient_tolerance >= 0.0) || !std::isfinite(o.gradient_tolerance))
         fail(LPG_EINVAL, "newton_solve: gradient_tolerance must be set to a finite non-negative value");
     if (o.max_iterations < 0 || o.max_line_search_steps < 1)
@@ -805,12 +964,20 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         fail(LPG_EINVAL, "newton_solve: invalid Hessian kind");
     if (o.precision != LPG_PRECISION_F64 && o.precision != LPG_PRECISION_MIXED)
         fail(LPG_EINVAL, "newton_solve: invalid precision");
-    Solver S(h);
+    Potential pot;
+    build_potential(h, terms, pot);
+    Solver S(h, &pot);
     const size_t n = S.n;
     const int V = S.V;
     cudaStream_t s = h.stream;
     double* mask = h.s_mask.as<double>(std::max<size_t>(n, 1));
     make_mask(h, fixed, nfixed, mask);
+    // Per-iteration records for the caller's callback (NewtonStep, newton.hpp:34-44).
+    lpg_newton_step step{};
+    auto report = [&]() {
+        if (terms && terms->on_iteration && terms->on_iteration(&step, terms->user) != 0)
+            fail(LPG_ESTOPPED, "newton_solve: the on_iteration callback stopped the solve");
+    };
     cudaEvent_t ev0, ev1;
     LPG_CUDA(cudaEventCreate(&ev0));
     LPG_CUDA(cudaEventCreate(&ev1));
@@ -867,15 +1034,16 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
     bool exact = false; // the exact_below switch, decided on the previous iteration's gradient
     for (int it = 0;; ++it) {
         const int hk = exact ? LPG_HESSIAN_EXACT : o.hessian;
+        const int64_t cg0 = R.cg_iterations;
+        step = lpg_newton_step{};
+        step.iteration = it;
+        step.pattern_changed = it == 0;
         // Energy and FP64 gradient (the Newton residual).
         double E;
         if (f64) {
             h.eval_async(x, g, hk, LPG_PRECISION_F64, kLayoutSell, K, nullptr);
-            if (f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
-            double e = 0;
-            LPG_CUDA(cudaMemcpyAsync(&e, h.d_energy.ptr, sizeof e, cudaMemcpyDeviceToHost, s));
-            raise_status(h.take_status());
-            E = e - S.energy_dot_f(x, f);
+            E = S.compose(x, f, g);
+            S.compose_hessian(static_cast<double*>(K));
         } else {
             E = S.energy(x, f, g);
         }
@@ -887,12 +1055,22 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         R.gradient_norm = o.stop_rule == 0 ? gmax : g2;
         R.gradient_norm0 = gnorm0;
         R.iterations = it;
+        step.energy = E;
+        step.gradient_norm = gmax;
+        step.gradient_norm_2 = g2;
         const bool converged = o.stop_rule == 0 ? gmax <= o.gradient_tolerance : g2 <= o.gradient_tolerance * gnorm0;
-        if (converged) return finish(0);
-        if (it == o.max_iterations) return finish(1);
+        if (converged) {
+            report();
+            return finish(0);
+        }
+        if (it == o.max_iterations) {
+            report();
+            return finish(1);
+        }
         if (!f64) {
             h.eval_async(x, nullptr, hk, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr);
             raise_status(h.take_status());
+            S.compose_hessian(static_cast<float*>(K));
         }
         // Descent direction with diagonal shifts (newton.cpp:55-72).
         neg_mask<<<grid(n), kThreads, 0, s>>>(g, mask, rhs, n);
@@ -926,6 +1104,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
             }
             R.cg_iterations += po.iters;
             gd = S.stats<double, double>(g, d, mask)[0];
+            step.diagonal_shifts = shifts;
             if (gd < 0.0 && std::isfinite(gd)) {
                 found = true;
                 break;
@@ -935,7 +1114,11 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
                                                                        f64 ? nullptr : static_cast<float*>(K), shift);
             shift *= 10.0;
         }
-        if (!found) return finish(3);
+        step.cg_iterations = R.cg_iterations - cg0;
+        if (!found) {
+            report();
+            return finish(3);
+        }
         // Line search (newton.cpp:92-108) from the feasible step.
         const int nb = feasible_blocks(h.dm);
         double* bm = h.d_block.as<double>(std::max(nb, 1));
@@ -944,6 +1127,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         double alpha = 1;
         LPG_CUDA(cudaMemcpyAsync(&alpha, al, sizeof alpha, cudaMemcpyDeviceToHost, s));
         raise_status(h.take_status());
+        step.feasible_step = alpha;
         bool accepted = false;
         for (int j = 0; j < o.max_line_search_steps; ++j) {
             LPG_CUDA(cudaMemsetAsync(moved, 0, sizeof(int), s));
@@ -953,6 +1137,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
             LPG_CUDA(cudaStreamSynchronize(s));
             if (!mv) break;
             ++R.line_search_evaluations;
+            ++step.line_search_evaluations;
             const double Et = S.energy(trial, f, nullptr);
             const double noise = 16.0 * kEps * std::max(1.0, std::abs(E));
             const double armijo = o.accept_rule == 1 ? 1e-4 * alpha * gd : 0.0;
@@ -962,7 +1147,12 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
             }
             alpha *= o.line_search_shrink;
         }
-        if (!accepted) return finish(2);
+        if (!accepted) {
+            report();
+            return finish(2);
+        }
+        step.step = alpha;
+        report();
         LPG_CUDA(cudaMemcpyAsync(x, trial, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
 }

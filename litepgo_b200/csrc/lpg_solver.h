@@ -48,6 +48,7 @@ struct lpg_fem {
     // Solver state (Newton / PCG / adjoint).
     lpg::DeviceBuffer s_x, s_g, s_f, s_d, s_trial, s_mask, s_hess, s_hess64, s_dinv, s_r, s_z, s_p, s_ap, s_xcg, s_r64,
         s_b64, s_scal, s_part, s_flag, d_flush, s_p2, s_mask4;
+    lpg::DeviceBuffer s_q[6]; // quadratic term of a weighted-sum potential (CSR, solver-layout entries, A x)
     std::vector<double> geo_base; // per element: G = rows of Dm^-1 (9) and w_dV, before any Fp
     lpg::Tuning tune; // autotuned launch variants (lpg::autotune)
     // CUDA graph of a chunk of PCG iterations, reused while its pointers stay the same.
@@ -66,8 +67,10 @@ struct lpg_fem {
 };
 
 namespace lpg {
+// terms (may be null): elastic weight, quadratic term, constant and per-iteration callback.
 void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
-                  const lpg_newton_options& o, double* x_out, lpg_newton_result* res);
+                  const lpg_newton_options& o, double* x_out, lpg_newton_result* res,
+                  const lpg_newton_terms* terms = nullptr);
 void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                    int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out);
 void batch_newton_solve(lpg_fem& h, int num_meshes, const int32_t* vertex_offsets, const int32_t* element_offsets,

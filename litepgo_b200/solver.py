@@ -20,7 +20,7 @@ import numpy as np
 from . import _native as N
 from .energy import HessianKind, WeightedSumEnergy
 
-__all__ = ["NewtonOptions", "NewtonStatus", "NewtonResult", "newton_solve", "batch_newton_solve",
+__all__ = ["NewtonOptions", "NewtonStatus", "NewtonResult", "NewtonStep", "newton_solve", "batch_newton_solve",
            "StaticEquilibriumResponse"]
 
 
@@ -93,24 +93,87 @@ class NewtonResult:
                 f"gradient_norm={self.gradient_norm:.3e}, cg_iterations={self.cg_iterations})")
 
 
+class NewtonStep:
+    """What one iteration did (newton.hpp:34-44; binding src/binding/solver/newton.cpp:42-50),
+    passed to newton_solve's on_iteration: iteration, energy, gradient_norm (max-norm over the
+    free DOFs), pattern_changed, diagonal_shifts, feasible_step, step, line_search_evaluations;
+    plus gradient_norm_2 (2-norm) and cg_iterations (PCG iterations of the step), which the
+    reference does not report."""
+
+    __slots__ = ("iteration", "energy", "gradient_norm", "pattern_changed", "diagonal_shifts", "feasible_step", "step",
+                 "line_search_evaluations", "gradient_norm_2", "cg_iterations")
+
+    def __init__(self, c):
+        self.iteration = int(c.iteration)
+        self.energy = float(c.energy)
+        self.gradient_norm = float(c.gradient_norm)
+        self.pattern_changed = bool(c.pattern_changed)
+        self.diagonal_shifts = int(c.diagonal_shifts)
+        self.feasible_step = float(c.feasible_step)
+        self.step = float(c.step)
+        self.line_search_evaluations = int(c.line_search_evaluations)
+        self.gradient_norm_2 = float(c.gradient_norm_2)
+        self.cg_iterations = int(c.cg_iterations)
+
+    def __repr__(self):
+        return (f"NewtonStep(iteration={self.iteration}, energy={self.energy:.6e}, gradient_norm={self.gradient_norm:.3e}, "
+                f"diagonal_shifts={self.diagonal_shifts}, step={self.step:.3g}, "
+                f"line_search_evaluations={self.line_search_evaluations})")
+
+
 def _split_energy(energy):
+    """(fem, elastic weight, A or None, f_ext or None, constant) of a potential."""
     from .fem import VolumetricFemEnergyTetP1
 
     if isinstance(energy, VolumetricFemEnergyTetP1):
-        return energy, None
+        return energy, 1.0, None, None, 0.0
     if isinstance(energy, WeightedSumEnergy):
-        fem, f = energy.split()
-        return fem, (f if np.any(f) else None)
-    raise TypeError("newton_solve: energy must be a VolumetricFemEnergy or a WeightedSumEnergy of one plus loads")
+        fem, w, A, f, c = energy.potential()
+        return fem, w, A, (f if np.any(f) else None), c
+    raise TypeError("newton_solve: energy must be a VolumetricFemEnergy or a WeightedSumEnergy of one plus quadratic "
+                    "terms")
+
+
+def _terms(w, A, c, on_iteration):
+    """lpg_newton_terms for a weighted sum and an optional callback (None when neither is needed).
+    Returns (terms, keep-alive list, error box): an exception raised by the callback stops the
+    solve (LPG_ESTOPPED) and is re-raised by the caller from the box."""
+    if w == 1.0 and A is None and c == 0.0 and on_iteration is None:
+        return None, [], None
+    keep, box = [], []
+    t = N.NewtonTermsC()
+    t.elastic_weight = float(w)
+    t.constant = float(c)
+    if A is not None:
+        A = A.tocsr()
+        A.sum_duplicates()
+        ptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
+        idx = np.ascontiguousarray(A.indices, dtype=np.int32)
+        val = np.ascontiguousarray(A.data, dtype=np.float64)
+        keep += [ptr, idx, val]
+        t.a_indptr, t.a_indices, t.a_values = N.iptr(ptr), N.iptr(idx), N.dptr(val)
+    if on_iteration is not None:
+        def trampoline(step_ptr, _user):
+            try:
+                on_iteration(NewtonStep(step_ptr.contents))
+                return 0
+            except BaseException as exc:  # re-raised after the solve returns
+                box.append(exc)
+                return 1
+
+        cb = N.NEWTON_CALLBACK(trampoline)
+        keep.append(cb)
+        t.on_iteration = cb
+    return t, keep, box
 
 
 def newton_solve(energy, fixed, x0, options, solver=None, on_iteration=None):
-    """Minimises energy over the free DOFs of ``fixed`` from x0 on the GPU."""
+    """Minimises energy over the free DOFs of ``fixed`` from x0 on the GPU. ``energy`` is a
+    VolumetricFemEnergy or a WeightedSumEnergy of one plus QuadraticEnergy /
+    VertexPullingEnergy terms; on_iteration(NewtonStep) is called as the reference calls it."""
     if solver is not None:
         raise ValueError("newton_solve: the GPU path solves with block-Jacobi PCG; pass solver=None")
-    if on_iteration is not None:
-        raise ValueError("newton_solve: per-iteration callbacks are not available on the GPU path")
-    fem, f = _split_energy(energy)
+    fem, w, A, f, c = _split_energy(energy)
     n = fem.num_dofs
     if fixed.num_dofs != n:
         raise ValueError("newton_solve: energy, fixed DOFs, and x0 must have the same DOF count")
@@ -136,8 +199,17 @@ def newton_solve(energy, fixed, x0, options, solver=None, on_iteration=None):
     fixed_arr = np.ascontiguousarray(fixed.fixed_dofs, dtype=np.int32)
     res = N.NewtonResultC()
     opts = options.to_c()
-    N.check(N.lib.lpg_newton_solve(fem.handle, N.iptr(fixed_arr), int(fixed_arr.size), ptrs[0], ptrs[1], ptrs[3],
-                                   ctypes.byref(opts), ptrs[2], ctypes.byref(res)))
+    terms, keep, box = _terms(w, A, c, on_iteration)
+    if terms is None:
+        N.check(N.lib.lpg_newton_solve(fem.handle, N.iptr(fixed_arr), int(fixed_arr.size), ptrs[0], ptrs[1], ptrs[3],
+                                       ctypes.byref(opts), ptrs[2], ctypes.byref(res)))
+    else:
+        code = N.lib.lpg_newton_solve_terms(fem.handle, ctypes.byref(terms), N.iptr(fixed_arr), int(fixed_arr.size),
+                                            ptrs[0], ptrs[1], ptrs[3], ctypes.byref(opts), ptrs[2], ctypes.byref(res))
+        if code == N.LPG_ESTOPPED and box:
+            raise box[0]
+        N.check(code)
+    del keep
     return NewtonResult(res.status, xo, res.energy, res.gradient_norm, res.iterations, res.gradient_norm0,
                         res.cg_iterations, res.line_search_evaluations, res.seconds)
 
@@ -154,7 +226,9 @@ def batch_newton_solve(energy, mesh_vertex_offsets, mesh_element_offsets, fixed,
     seconds = time from the call's start to the iteration that ended the mesh), total the
     whole call's NewtonResult.
     """
-    fem, f = _split_energy(energy)
+    fem, w, A, f, c = _split_energy(energy)
+    if w != 1.0 or A is not None or c != 0.0:
+        raise ValueError("batch_newton_solve: the energy must be the elastic term plus linear loads")
     n = fem.num_dofs
     voff = np.ascontiguousarray(mesh_vertex_offsets, dtype=np.int32)
     eoff = np.ascontiguousarray(mesh_element_offsets, dtype=np.int32)
@@ -247,7 +321,9 @@ class StaticEquilibriumResponse:
         force = self.make_response(x)
         if force is None or force.num_inputs != self.num_inputs or force.num_outputs != self.num_outputs:
             raise ValueError("StaticEquilibriumResponse: incompatible force response")
-        fem, _ = _split_energy(potential)
+        fem, w, A, _, _ = _split_energy(potential)
+        if w != 1.0 or A is not None:
+            raise ValueError("StaticEquilibriumResponse: the adjoint needs the elastic term plus linear loads")
         fixed_arr = np.ascontiguousarray(self.fixed.fixed_dofs, dtype=np.int32)
         prec = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
         from .fem import VolumetricFemForceFpResponseTetP1, VolumetricFemForceRestPositionResponseTetP1

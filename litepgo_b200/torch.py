@@ -85,11 +85,23 @@ def _on_device(potential, x, need_gradient):
         value, g, _ = potential.eval_device(x.detach(), gradient=need_gradient)
         return value, g
     if isinstance(potential, WeightedSumEnergy):
-        fem, f = potential.split()
-        value, g, _ = fem.eval_device(x.detach(), gradient=need_gradient)
+        fem, w, A, f, c = potential.potential()
+        xd = x.detach()
+        value, g, _ = fem.eval_device(xd, gradient=need_gradient)
         ft = torch.as_tensor(f, device=x.device)
-        value -= float(torch.dot(ft, x.detach()))
-        return value, (g - ft if g is not None else None)
+        value = w * value - float(torch.dot(ft, xd)) + c
+        if g is not None:
+            g = w * g - ft
+        if A is not None:
+            A = A.tocsr()
+            At = torch.sparse_csr_tensor(torch.as_tensor(A.indptr, dtype=torch.int64),
+                                         torch.as_tensor(A.indices, dtype=torch.int64),
+                                         torch.as_tensor(A.data, dtype=torch.float64), size=A.shape).to(x.device)
+            Ax = torch.mv(At, xd)
+            value += 0.5 * float(torch.dot(xd, Ax))
+            if g is not None:
+                g = g + Ax
+        return value, g
     if isinstance(potential, QuadraticEnergy) and potential.is_linear:
         b = torch.as_tensor(potential.b, device=x.device)
         return float(torch.dot(b, x.detach())), (b.clone() if need_gradient else None)

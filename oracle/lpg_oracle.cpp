@@ -1207,8 +1207,47 @@ int orc_mesh_force_vjp_rest(orc_mesh* m, const double* u, const double* w, doubl
 // relative-2-norm / Armijo variant and a PCG linear solver option.
 int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_ext, const double* x0,
                      const orc_newton_options* o, double* x_out, orc_newton_result* res) {
+    return orc_newton_solve_ex(m, nullptr, fixed, nfixed, f_ext, x0, o, x_out, res, nullptr, 0, nullptr);
+}
+
+// The same over a weighted-sum potential (WeightedSumEnergy of the elastic energy and
+// QuadraticEnergy terms) with the NewtonStep trace.
+int orc_newton_solve_ex(orc_mesh* m, const orc_terms* terms, const int* fixed, int nfixed, const double* f_ext,
+                        const double* x0, const orc_newton_options* o, double* x_out, orc_newton_result* res,
+                        double* trace, int trace_cap, int* trace_len) {
     return guarded([&] {
         const int n = m->n;
+        const double w = terms ? terms->elastic_weight : 1.0, cst = terms ? terms->constant : 0.0;
+        const bool has_a = terms && terms->a_indptr;
+        // A's entries at their positions in the elastic CSC values (A symmetric: CSR row r is column r).
+        std::vector<std::pair<int, double>> apos;
+        if (has_a) {
+            for (int r = 0; r < n; ++r)
+                for (int k = terms->a_indptr[r]; k < terms->a_indptr[r + 1]; ++k) {
+                    const int c = terms->a_indices[k];
+                    const int* beg = m->inner.data() + m->outer[r];
+                    const int* end = m->inner.data() + m->outer[r + 1];
+                    const int* at = std::lower_bound(beg, end, c);
+                    if (at == end || *at != c) fail(ORC_EINVAL, "QuadraticEnergy: A outside the elastic pattern");
+                    apos.emplace_back(static_cast<int>(at - m->inner.data()), terms->a_values[k]);
+                }
+        }
+        int nsteps = 0;
+        if (trace_len) *trace_len = 0;
+        auto report = [&](int it, double E, double gmax, int shifts, double feas, double step, int lse) {
+            if (trace && nsteps < trace_cap) {
+                double* t = trace + 7 * static_cast<size_t>(nsteps);
+                t[0] = it;
+                t[1] = E;
+                t[2] = gmax;
+                t[3] = shifts;
+                t[4] = feas;
+                t[5] = step;
+                t[6] = lse;
+            }
+            ++nsteps;
+            if (trace_len) *trace_len = std::min(nsteps, trace_cap);
+        };
         if (!(o->gradient_tolerance >= 0) || !std::isfinite(o->gradient_tolerance))
             fail(ORC_EINVAL, "newton_solve: gradient_tolerance must be set to a finite non-negative value");
         if (o->max_iterations < 0 || o->max_line_search_steps < 1)
@@ -1221,6 +1260,27 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
         auto energy = [&](const std::vector<double>& y, std::vector<double>* g, std::vector<double>* vals) {
             double E = mesh_eval(*m, y.data(), g ? g->data() : nullptr, vals ? o->hessian : 0,
                                  vals ? vals->data() : nullptr, nullptr, nullptr, nullptr);
+            if (terms) {
+                E *= w;
+                if (g)
+                    for (double& v : *g) v *= w;
+                if (vals)
+                    for (double& v : *vals) v *= w;
+                if (has_a) {
+                    double q = 0;
+                    for (int r = 0; r < n; ++r) {
+                        double ax = 0;
+                        for (int k = terms->a_indptr[r]; k < terms->a_indptr[r + 1]; ++k)
+                            ax += terms->a_values[k] * y[terms->a_indices[k]];
+                        q += y[r] * ax;
+                        if (g) (*g)[r] += ax;
+                    }
+                    E += 0.5 * q;
+                    if (vals)
+                        for (const auto& pa : apos) (*vals)[pa.first] += pa.second;
+                }
+                E += cst;
+            }
             for (int k = 0; k < n; ++k) E -= f[k] * y[k];
             if (g)
                 for (int k = 0; k < n; ++k) (*g)[k] -= f[k];
@@ -1254,10 +1314,12 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
             const bool converged = o->stop_rule == 0 ? gn <= o->gradient_tolerance : g2 <= o->gradient_tolerance * gnorm0;
             if (converged) {
                 res->status = 0;
+                report(it, E, gmax, 0, 0.0, 0.0, 0);
                 break;
             }
             if (it == o->max_iterations) {
                 res->status = 1;
+                report(it, E, gmax, 0, 0.0, 0.0, 0);
                 break;
             }
             Csc K = reduce_matrix(red, m->outer, m->inner, vals);
@@ -1274,7 +1336,9 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
                     }
             double shift = 1e-8 * dscale;
             bool found = false;
+            int nshift = 0;
             for (int shifts = 0;; ++shifts) {
+                nshift = shifts;
                 bool ok = false;
                 if (o->linear_solver == 0) {
                     Ldlt fct;
@@ -1302,6 +1366,7 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
             }
             if (!found) {
                 res->status = 3;
+                report(it, E, gmax, 10, 0.0, 0.0, 0);
                 break;
             }
             std::fill(dir.begin(), dir.end(), 0.0);
@@ -1310,6 +1375,8 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
             for (int i = 0; i < nf; ++i) gd += gf[i] * df[i];
             // line_search (newton.cpp:92-108)
             double alpha = mesh_feasible_step(*m, x.data(), dir.data());
+            const double feas = alpha;
+            int lse = 0;
             bool accepted = false;
             for (int j = 0; j < o->max_line_search_steps; ++j) {
                 bool moved = false;
@@ -1319,6 +1386,7 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
                 }
                 if (!moved) break;
                 ++res->line_search_evaluations;
+                ++lse;
                 const double Et = energy(trial, nullptr, nullptr);
                 const double noise = 16.0 * kEps * std::max(1.0, std::abs(E));
                 const double armijo = o->accept_rule == 1 ? 1e-4 * alpha * gd : 0.0;
@@ -1330,8 +1398,10 @@ int orc_newton_solve(orc_mesh* m, const int* fixed, int nfixed, const double* f_
             }
             if (!accepted) {
                 res->status = 2;
+                report(it, E, gmax, nshift, feas, 0.0, lse);
                 break;
             }
+            report(it, E, gmax, nshift, feas, alpha, lse);
             x = trial;
         }
         std::copy(x.begin(), x.end(), x_out);

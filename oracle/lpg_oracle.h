@@ -113,6 +113,25 @@ typedef struct {
 int orc_newton_solve(orc_mesh* m, const int* fixed_dofs, int num_fixed, const double* f_ext, const double* x0,
                      const orc_newton_options* options, double* x_out, orc_newton_result* result);
 
+/* A weighted-sum potential around the elastic energy (weighted_sum_energy.hpp:16-47 with
+ * QuadraticEnergy terms, quadratic_energy.hpp:10-20): E = w elastic + 1/2 x^T A x - f_ext . x + c,
+ * A a symmetric scalar CSR matrix inside the elastic pattern (a_indptr NULL: none). */
+typedef struct {
+    double elastic_weight;
+    const int* a_indptr;
+    const int* a_indices;
+    const double* a_values;
+    double constant;
+} orc_terms;
+
+/* orc_newton_solve over terms (NULL: elastic and load only) with the reference's NewtonStep trace
+ * (newton.hpp:34-44, reported where newton.cpp:123-181 reports it): 7 doubles per step
+ * {iteration, energy, max|g_free|, diagonal_shifts, feasible_step, step, line_search_evaluations},
+ * at most trace_cap steps; *trace_len receives the count (trace may be NULL). */
+int orc_newton_solve_ex(orc_mesh* m, const orc_terms* terms, const int* fixed_dofs, int num_fixed, const double* f_ext,
+                        const double* x0, const orc_newton_options* options, double* x_out, orc_newton_result* result,
+                        double* trace, int trace_cap, int* trace_len);
+
 /* Adjoint of the static equilibrium (static_equilibrium_response.cpp:43-88, transpose branch):
  * solves K_ff lambda = dLdu_free with the exact Hessian at u_star and returns
  * dtheta = -(d g / d theta)^T expand(lambda) per element (T*2). linear_solver as above. */

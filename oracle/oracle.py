@@ -62,6 +62,20 @@ class NewtonResult(ctypes.Structure):
     ]
 
 
+class Terms(ctypes.Structure):
+    _fields_ = [
+        ("elastic_weight", ctypes.c_double),
+        ("a_indptr", _c_int_p),
+        ("a_indices", _c_int_p),
+        ("a_values", _c_double_p),
+        ("constant", ctypes.c_double),
+    ]
+
+
+# Fields of one NewtonStep trace record (orc_newton_solve_ex).
+TRACE_FIELDS = ("iteration", "energy", "gradient_norm", "diagonal_shifts", "feasible_step", "step",
+                "line_search_evaluations")
+
 _lib = None
 
 
@@ -86,6 +100,9 @@ def lib():
         L.orc_mesh_force_vjp_fp.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_newton_solve.argtypes = [ctypes.c_void_p, _c_int_p, ctypes.c_int, _c_double_p, _c_double_p,
                                        ctypes.POINTER(NewtonOptions), _c_double_p, ctypes.POINTER(NewtonResult)]
+        L.orc_newton_solve_ex.argtypes = [ctypes.c_void_p, ctypes.POINTER(Terms), _c_int_p, ctypes.c_int, _c_double_p,
+                                          _c_double_p, ctypes.POINTER(NewtonOptions), _c_double_p,
+                                          ctypes.POINTER(NewtonResult), _c_double_p, ctypes.c_int, _c_int_p]
         L.orc_adjoint_theta.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p, _c_int_p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_double, _c_double_p, _c_double_p]
         L.orc_set_threads.argtypes = [ctypes.c_int]
@@ -262,7 +279,10 @@ class OracleMesh:
         return out
 
     def newton(self, fixed, x0, f_ext=None, tol=1e-9, max_iterations=50, hessian=2, max_line_search_steps=30,
-               shrink=0.5, stop_rule=0, accept_rule=0, linear_solver=0, cg_tolerance=1e-2, cg_max_iterations=10000):
+               shrink=0.5, stop_rule=0, accept_rule=0, linear_solver=0, cg_tolerance=1e-2, cg_max_iterations=10000,
+               elastic_weight=1.0, A=None, constant=0.0, trace=False):
+        """Newton over E = w elastic + 1/2 x^T A x - f_ext . x + constant (A a symmetric scipy
+        matrix or None). With trace, info["trace"] lists one dict per NewtonStep."""
         fixed = np.ascontiguousarray(fixed, dtype=np.int32)
         x0 = np.ascontiguousarray(x0, dtype=np.float64)
         f = None if f_ext is None else np.ascontiguousarray(f_ext, dtype=np.float64)
@@ -270,9 +290,29 @@ class OracleMesh:
                              linear_solver, cg_tolerance, cg_max_iterations)
         x = np.empty(self.num_dofs)
         res = NewtonResult()
-        _check(lib().orc_newton_solve(self._h, _ip(fixed), len(fixed), _dp(f), _dp(x0), ctypes.byref(opts), _dp(x),
-                                      ctypes.byref(res)))
+        keep = []
+        terms = None
+        if elastic_weight != 1.0 or A is not None or constant != 0.0:
+            terms = Terms(float(elastic_weight), None, None, None, float(constant))
+            if A is not None:
+                import scipy.sparse as sp
+
+                Ac = sp.csr_matrix(A)
+                Ac.sum_duplicates()
+                Ac.sort_indices()
+                keep = [np.ascontiguousarray(Ac.indptr, dtype=np.int32), np.ascontiguousarray(Ac.indices, dtype=np.int32),
+                        np.ascontiguousarray(Ac.data, dtype=np.float64)]
+                terms.a_indptr, terms.a_indices, terms.a_values = _ip(keep[0]), _ip(keep[1]), _dp(keep[2])
+        cap = max_iterations + 2
+        buf = np.zeros((cap, 7))
+        count = ctypes.c_int(0)
+        _check(lib().orc_newton_solve_ex(self._h, ctypes.byref(terms) if terms is not None else None, _ip(fixed),
+                                         len(fixed), _dp(f), _dp(x0), ctypes.byref(opts), _dp(x), ctypes.byref(res),
+                                         _dp(buf), cap, ctypes.byref(count)))
+        del keep
         info = {name: getattr(res, name) for name, _ in NewtonResult._fields_}
+        if trace:
+            info["trace"] = [dict(zip(TRACE_FIELDS, row)) for row in buf[:count.value]]
         return x, info
 
     def adjoint_theta(self, u_star, dLdu, fixed, linear_solver=0, cg_tolerance=1e-12):
