@@ -18,6 +18,7 @@ import argparse
 import ctypes
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -174,25 +175,59 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(X, tets, theta, u_full, seconds=12.0):
-    """The oracle (the reference's CPU algorithm restated in C++/OpenMP) on the host cores:
-    E + gradient + exact CSC Hessian, repeated for about `seconds` on the full mesh."""
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
+def _median_eval_seconds(m, u, runs=5, warm=2):
+    """The reference benchmark's method (benchmarks/torch_material.py:50-59, 207-219): one cold
+    call, `warm` warm-up calls, then the median of `runs` timed calls of E + gradient + exact
+    CSC Hessian."""
+    m.eval(u, True, 1)
+    for _ in range(warm):
+        m.eval(u, True, 1)
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        m.eval(u, True, 1)
+        times.append(time.perf_counter() - t0)
+    return float(np.median(times))
+
+
+def cpu_baseline(X, tets, theta, u_full):
+    """The oracle (the reference's CPU algorithm restated in C++/OpenMP) on the host cores: E +
+    gradient + exact CSC Hessian, median of 5 after a cold call and 2 warm-ups, on the full mesh
+    with every host thread, and with one thread on a slab of the mesh (its first eighth of cube
+    layers, the same elements' evaluation per tet)."""
     import oracle
 
     oracle.set_threads(0)
     threads = oracle.get_threads()
+    T = tets.shape[0]
     m = oracle.OracleMesh(X, tets, theta)
-    m.eval(u_full, True, 1)  # cold call
-    n, t0 = 0, time.perf_counter()
-    while True:
-        m.eval(u_full, True, 1)
-        n += 1
-        el = time.perf_counter() - t0
-        if el >= seconds or n >= 20:
-            break
-    return {"value": n * tets.shape[0] / el, "unit": "tets/s", "cores": threads, "kind": "port",
-            "sample": f"{n} full evaluations (E+grad+exact CSC Hessian) of the {tets.shape[0]}-tet mesh, "
-                      f"{el:.1f} s wall, OpenMP {threads} threads, median-free mean"}
+    med = _median_eval_seconds(m, u_full)
+    del m
+    # One thread on a slab: elements [0, T/8) of the cube-ordered box and their vertices.
+    Ts = max(T // 8, 1)
+    sub = tets[:Ts]
+    verts, local = np.unique(sub, return_inverse=True)
+    ms = oracle.OracleMesh(X[verts], local.reshape(-1, 4).astype(np.int32), theta[:Ts] if theta.ndim == 2 else theta)
+    oracle.set_threads(1)
+    med1 = _median_eval_seconds(ms, u_full.reshape(-1, 3)[verts].ravel())
+    oracle.set_threads(0)
+    return {"value": T / med, "unit": "tets/s", "cores": threads, "kind": "port",
+            "sample": f"E+grad+exact CSC Hessian of the {T}-tet mesh: 1 cold call, 2 warm-ups, median of 5 "
+                      f"({med:.3f} s) with {threads} OpenMP threads",
+            "one_thread": {"value": Ts / med1, "unit": "tets/s", "cores": 1,
+                           "sample": f"the same on the first {Ts} tets (their {verts.size} vertices), median of 5 "
+                                     f"({med1:.3f} s) on one thread"},
+            "cpu_model": cpu_model()}
 
 
 def dist_setup(n_gpus):
@@ -259,20 +294,26 @@ def run_reference(args):
     threads = oracle.get_threads()
     m = oracle.OracleMesh(g["X"], g["tets"], g["theta"])
     T = g["tets"].shape[0]
+    m.eval(u, True, 1)  # cold call
     for _ in range(max(args.warmup, 0)):
         m.eval(u, True, 1)
-    t0 = time.perf_counter()
+    times = []
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         m.eval(u, True, 1)
-    el = time.perf_counter() - t0
-    value = args.steps * T / el
+        times.append(time.perf_counter() - t0)
+    el = float(np.sum(times))
+    med = float(np.median(times))
+    value = T / med
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": "tets/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full evaluations (E+grad+exact CSC Hessian) of the {T}-tet mesh "
-                                   f"by the C++/OpenMP restatement of the reference CPU path, {threads} threads"},
+                         "sample": f"median of {args.steps} full evaluations (E+grad+exact CSC Hessian) of the {T}-tet "
+                                   f"mesh after a cold call and {args.warmup} warm-ups, by the C++/OpenMP restatement "
+                                   f"of the reference CPU path, {threads} threads",
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "tets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference itself cannot be built here (Eigen 5 / oneTBB / nanobind fetched at configure time, "
                 "no network); this arm times its algorithm restated in oracle/",

@@ -332,6 +332,23 @@ typedef struct {
 typedef int (*lpg_newton_callback)(const lpg_newton_step* step, void* user);
 
 /*
+ * A caller's volumetric material (the reference's PyVolumetricMaterial / TorchVolumetricMaterial
+ * in the Material slot of VolumetricFemEnergy, src/python/fem.py:59-109, src/python/torch.py:72-94):
+ * given F at every material row (rows 3x3 row-major matrices on the device: one row per tet,
+ * or per quadrature point of a hex, element-major), it writes W (rows), and with want >= 1
+ * P = dW/dF (9 rows, row-major 3x3), with want = 2 A = d2W/dF2 (81 rows, A[9 (3 i + j) + 3 k + l]
+ * = d2W / dF_ij dF_kl) into the library's device buffers, on the handle's stream. Returns 0, or
+ * non-zero to stop the solve (LPG_ESTOPPED).
+ */
+typedef int (*lpg_material_fn)(const double* F, int rows, int want, double* W, double* P, double* A, void* user);
+
+/* A caller's material bound on the step from x along dx (PyVolumetricMaterial.eval_feasible_step):
+ * F = I + grad x and G = I + grad dx at every material row (device, as for lpg_material_fn; the
+ * increment is dF = G - I); writes a value in [0, 1] to *alpha and returns 0, or non-zero to
+ * stop the solve (LPG_ESTOPPED). */
+typedef int (*lpg_feasible_fn)(const double* F, const double* G, int rows, double* alpha, void* user);
+
+/*
  * The terms of a weighted-sum potential around the handle's elastic energy, for
  * lpg_newton_solve_terms (the reference's WeightedSumEnergy, weighted_sum_energy.hpp:16-47, of
  * one VolumetricFemEnergy and QuadraticEnergy terms, quadratic_energy.hpp:10-20, summed
@@ -341,6 +358,8 @@ typedef int (*lpg_newton_callback)(const lpg_newton_step* step, void* user);
  * a_values of a_indptr[num_dofs] entries; duplicates are summed) or a_indptr = NULL for none. It
  * must be symmetric and lie inside the elastic Hessian's pattern (vertex pairs sharing an
  * element), else LPG_EINVAL. on_iteration (may be NULL) is called with user at every step.
+ * With material set, every evaluation of the elastic term exports F, calls material and
+ * integrates its W, P and A (as lpg_fem_eval_material); feasible, if set, bounds each line search.
  */
 typedef struct {
     double elastic_weight; /* finite and non-zero; 1 for the elastic energy alone */
@@ -350,6 +369,10 @@ typedef struct {
     double constant;
     lpg_newton_callback on_iteration;
     void* user;
+    lpg_material_fn material;   /* NULL: the handle's neo-Hookean records; else the caller's material
+                                   (the handle then carries rest geometry only) */
+    lpg_feasible_fn feasible;   /* NULL: the positive-determinant step of lpg_fem_feasible_step */
+    void* material_user;
 } lpg_newton_terms;
 
 /*

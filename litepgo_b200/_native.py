@@ -86,6 +86,11 @@ class NewtonStepC(ctypes.Structure):
 
 
 NEWTON_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(NewtonStepC), ctypes.c_void_p)
+# (F, rows, want, W, P, A, user) and (F, G, rows, alpha, user): device pointers as integers.
+MATERIAL_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+FEASIBLE_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
 
 
 class NewtonTermsC(ctypes.Structure):
@@ -97,6 +102,9 @@ class NewtonTermsC(ctypes.Structure):
         ("constant", ctypes.c_double),
         ("on_iteration", NEWTON_CALLBACK),
         ("user", ctypes.c_void_p),
+        ("material", MATERIAL_CALLBACK),
+        ("feasible", FEASIBLE_CALLBACK),
+        ("material_user", ctypes.c_void_p),
     ]
 
 

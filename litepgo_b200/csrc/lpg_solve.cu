@@ -634,6 +634,7 @@ template <typename Kern> int one_wave(Kern kernel, size_t work) {
 // A weighted-sum potential around the elastic energy (lpg_newton_terms) on the device:
 //   E = w elastic + 1/2 x^T A x + c (the linear load is handled as f_ext).
 struct Potential {
+    const lpg_newton_terms* t = nullptr;          // the caller's terms (material and feasible callbacks)
     double w = 1.0, c = 0.0;
     int n = 0;                                    // rows of A (0: no quadratic term)
     int32_t *ptr = nullptr, *col = nullptr;       // A, CSR (duplicates merged)
@@ -643,6 +644,55 @@ struct Potential {
     double* kval = nullptr;
     double* Ax = nullptr;                         // scratch, n values
 };
+
+// One evaluation of the elastic term at x (gradient into g if given, Hessian of kind hk into K
+// in layout): the handle's own element pass, or with a caller's material the exported F, the
+// material's W / P / A and their integration (lpg_fem_eval_material's path). Enqueued on the
+// handle's stream; the material callback runs on the host in between.
+void eval_elastic_async(lpg_fem& h, const lpg_newton_terms* t, const double* x, double* g, int hk, int prec,
+                        int layout, void* K) {
+    if (!t || !t->material) {
+        h.eval_async(x, g, hk, prec, layout, K, nullptr);
+        return;
+    }
+    const DevMesh& m = h.dm;
+    if (m.K == 64) fail(LPG_EINVAL, "newton_solve: materials are not available for Hermite hex meshes");
+    if (m.fpinv64) fail(LPG_EINVAL, "newton_solve: a material handle has no plastic field");
+    cudaStream_t s = h.stream;
+    const bool hex = m.K == 8;
+    const size_t rows = static_cast<size_t>(m.T) * (hex ? m.nq : 1), nel = std::max<size_t>(m.T, 1);
+    double* F = h.d_mat[4].as<double>(std::max<size_t>(9 * rows, 1));
+    double* W = h.d_mat[0].as<double>(std::max<size_t>(rows, 1));
+    double* P = h.d_mat[1].as<double>(std::max<size_t>(9 * rows, 1));
+    double* A = hk != LPG_HESSIAN_NONE ? h.d_mat[2].as<double>(std::max<size_t>(81 * rows, 1)) : nullptr;
+    unsigned* status = h.d_status.as<unsigned>(1);
+    if (hex)
+        launch_hex_deformation_gradients(m, x, F, status, s);
+    else
+        launch_deformation_gradients(m, x, F, status, s);
+    raise_status(h.take_status());
+    const int want = hk != LPG_HESSIAN_NONE ? 2 : g ? 1 : 0;
+    if (t->material(F, static_cast<int>(rows), want, W, want >= 1 ? P : nullptr, A, t->material_user) != 0)
+        fail(LPG_ESTOPPED, "newton_solve: the material callback stopped the solve");
+    EvalArgs a;
+    a.grad = g;
+    a.hess = hk != LPG_HESSIAN_NONE ? K : nullptr;
+    a.layout = layout;
+    a.cluster_energy = h.d_cluster_energy.as<double>(static_cast<size_t>(std::max(m.ncl, m.tc_ncl)) + 256);
+    a.energy = h.d_energy.as<double>(1);
+    a.status = status;
+    const int pi = prec == LPG_PRECISION_F64 ? 0 : 1;
+    if (hex) {
+        const bool projected = hk == LPG_HESSIAN_PROJECTED;
+        void* blocks = a.hess ? h.d_proj.ensure(hex_blocks_bytes(m, prec, projected)) : nullptr;
+        launch_hex_material_eval(m, prec, hk, W, g ? P : nullptr, A, h.d_mat[3].as<double>(nel), h.d_vjp.as<double>(24 * nel),
+                                 blocks, projected && a.hess ? h.d_plist.as<int>(nel) : nullptr, a, s);
+    } else {
+        void* proj = a.hess ? h.d_proj.ensure(project_bytes(m, prec)) : nullptr;
+        launch_material_eval(m, prec, hk, W, g ? P : nullptr, A, h.d_mat[3].as<double>(nel), h.d_vjp.as<double>(12 * nel),
+                             proj, h.d_plist.as<int>(nel), h.d_pcount.as<unsigned>(1), h.tune.clamp[pi], a, s);
+    }
+}
 
 struct Solver {
     lpg_fem& h;
@@ -674,7 +724,7 @@ struct Solver {
 
     // E(x) (FP64) with optional gradient g (FP64, load included); throws on bad status.
     double energy(const double* x, const double* f, double* g) {
-        h.eval_async(x, g, LPG_HESSIAN_NONE, LPG_PRECISION_F64, LPG_LAYOUT_BSR, nullptr, nullptr);
+        eval_elastic_async(h, P ? P->t : nullptr, x, g, LPG_HESSIAN_NONE, LPG_PRECISION_F64, LPG_LAYOUT_BSR, nullptr);
         return compose(x, f, g);
     }
     // The potential from the elastic evaluation just enqueued (energy in h.d_energy, gradient
@@ -870,6 +920,7 @@ void build_potential(lpg_fem& h, const lpg_newton_terms* t, Potential& P) {
     if (!std::isfinite(t->elastic_weight) || t->elastic_weight == 0.0)
         fail(LPG_EINVAL, "WeightedSumEnergy weights must be finite and nonzero");
     if (!std::isfinite(t->constant)) fail(LPG_EINVAL, "newton_solve: the potential's constant must be finite");
+    P.t = t;
     P.w = t->elastic_weight;
     P.c = t->constant;
     if (!t->a_indptr) return;
@@ -1041,7 +1092,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         // Energy and FP64 gradient (the Newton residual).
         double E;
         if (f64) {
-            h.eval_async(x, g, hk, LPG_PRECISION_F64, kLayoutSell, K, nullptr);
+            eval_elastic_async(h, terms, x, g, hk, LPG_PRECISION_F64, kLayoutSell, K);
             E = S.compose(x, f, g);
             S.compose_hessian(static_cast<double*>(K));
         } else {
@@ -1068,7 +1119,7 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
             return finish(1);
         }
         if (!f64) {
-            h.eval_async(x, nullptr, hk, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr);
+            eval_elastic_async(h, terms, x, nullptr, hk, LPG_PRECISION_MIXED, kLayoutSell, K);
             raise_status(h.take_status());
             S.compose_hessian(static_cast<float*>(K));
         }
@@ -1123,10 +1174,30 @@ void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_
         const int nb = feasible_blocks(h.dm);
         double* bm = h.d_block.as<double>(std::max(nb, 1));
         double* al = h.d_alpha.as<double>(1);
-        launch_feasible(h.dm, x, d, bm, nb, al, h.d_status.as<unsigned>(1), s);
         double alpha = 1;
-        LPG_CUDA(cudaMemcpyAsync(&alpha, al, sizeof alpha, cudaMemcpyDeviceToHost, s));
-        raise_status(h.take_status());
+        if (terms && terms->feasible) {
+            const bool hex = h.dm.K == 8;
+            const size_t rows = static_cast<size_t>(h.dm.T) * (hex ? h.dm.nq : 1);
+            double* Fx = h.d_mat[4].as<double>(std::max<size_t>(9 * rows, 1));
+            double* Gd = h.d_mat[5].as<double>(std::max<size_t>(9 * rows, 1));
+            unsigned* stw = h.d_status.as<unsigned>(1);
+            if (hex) {
+                launch_hex_deformation_gradients(h.dm, x, Fx, stw, s);
+                launch_hex_deformation_gradients(h.dm, d, Gd, stw, s);
+            } else {
+                launch_deformation_gradients(h.dm, x, Fx, stw, s);
+                launch_deformation_gradients(h.dm, d, Gd, stw, s);
+            }
+            raise_status(h.take_status());
+            if (terms->feasible(Fx, Gd, static_cast<int>(rows), &alpha, terms->material_user) != 0)
+                fail(LPG_ESTOPPED, "newton_solve: the feasible-step callback stopped the solve");
+            if (!(alpha >= 0.0 && alpha <= 1.0))
+                fail(LPG_ELOGIC, "Energy::max_feasible_step: the energy returned a value outside [0, 1]");
+        } else {
+            launch_feasible(h.dm, x, d, bm, nb, al, h.d_status.as<unsigned>(1), s);
+            LPG_CUDA(cudaMemcpyAsync(&alpha, al, sizeof alpha, cudaMemcpyDeviceToHost, s));
+            raise_status(h.take_status());
+        }
         step.feasible_step = alpha;
         bool accepted = false;
         for (int j = 0; j < o.max_line_search_steps; ++j) {

@@ -43,7 +43,7 @@ struct lpg_fem {
     lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_plist, d_pcount; // elements listed for the projection's eigenvalue clamp
-    lpg::DeviceBuffer d_mat[4];          // staged material outputs (W, P, A) and per-element energies
+    lpg::DeviceBuffer d_mat[6];          // material outputs (W, P, A), per-element energies, F and G
     lpg::DeviceBuffer d_status, d_cluster_energy, d_energy, d_block, d_alpha, d_u, d_u2, d_grad, d_hess, d_proj, d_vjp;
     // Solver state (Newton / PCG / adjoint).
     lpg::DeviceBuffer s_x, s_g, s_f, s_d, s_trial, s_mask, s_hess, s_hess64, s_dinv, s_r, s_z, s_p, s_ap, s_xcg, s_r64,

@@ -191,11 +191,11 @@ class WeightedSumEnergy(Energy):
         summed). Raises ValueError for other terms."""
         import scipy.sparse as sp
 
-        from .fem import VolumetricFemEnergyTetP1
+        from .fem import VolumetricFemEnergyPyMaterialTetP1, VolumetricFemEnergyTetP1
 
         fem, wf, A, b, c = None, 1.0, None, np.zeros(self.num_dofs), 0.0
         for e, w in self.terms:
-            if isinstance(e, VolumetricFemEnergyTetP1):
+            if isinstance(e, (VolumetricFemEnergyTetP1, VolumetricFemEnergyPyMaterialTetP1)):
                 if fem is not None:
                     raise ValueError("WeightedSumEnergy: one elastic term is supported on the GPU path")
                 fem, wf = e, w

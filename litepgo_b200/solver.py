@@ -122,10 +122,11 @@ class NewtonStep:
 
 
 def _split_energy(energy):
-    """(fem, elastic weight, A or None, f_ext or None, constant) of a potential."""
-    from .fem import VolumetricFemEnergyTetP1
+    """(fem, elastic weight, A or None, f_ext or None, constant) of a potential; fem is a native
+    or a Python-material VolumetricFemEnergy."""
+    from .fem import VolumetricFemEnergyPyMaterialTetP1, VolumetricFemEnergyTetP1
 
-    if isinstance(energy, VolumetricFemEnergyTetP1):
+    if isinstance(energy, (VolumetricFemEnergyTetP1, VolumetricFemEnergyPyMaterialTetP1)):
         return energy, 1.0, None, None, 0.0
     if isinstance(energy, WeightedSumEnergy):
         fem, w, A, f, c = energy.potential()
@@ -134,11 +135,75 @@ def _split_energy(energy):
                     "terms")
 
 
-def _terms(w, A, c, on_iteration):
-    """lpg_newton_terms for a weighted sum and an optional callback (None when neither is needed).
-    Returns (terms, keep-alive list, error box): an exception raised by the callback stops the
-    solve (LPG_ESTOPPED) and is re-raised by the caller from the box."""
-    if w == 1.0 and A is None and c == 0.0 and on_iteration is None:
+class _DeviceArray:
+    """A float64 device buffer of the library as a torch-importable array (zero copy)."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def _view(ptr, shape, device):
+    import torch
+
+    return torch.as_tensor(_DeviceArray(ptr, shape), device=device)
+
+
+def _material_callbacks(fem, t, keep, box):
+    """The material and feasible-step callbacks of a Python-material energy (PyVolumetricMaterial
+    or TorchVolumetricMaterial): the library hands over F at every material row and takes W, P
+    and A back in its own device buffers."""
+    import torch
+
+    dev = fem.device
+
+    def material(Fp, rows, want, Wp, Pp, Ap, _user):
+        try:
+            F = _view(Fp, (rows, 3, 3), dev)
+            outputs = ("W",) + (("dW_dF",) if want >= 1 else ()) + (("d2W_dF2",) if want >= 2 else ())
+            vals = fem._material(F, outputs)
+            _view(Wp, (rows,), dev).copy_(vals[0])
+            if want >= 1:
+                _view(Pp, (rows, 3, 3), dev).copy_(vals[1])
+            if want >= 2:
+                _view(Ap, (rows, 3, 3, 3, 3), dev).copy_(vals[2])
+            return 0
+        except BaseException as exc:  # re-raised after the solve returns
+            box.append(exc)
+            return 1
+
+    cb = N.MATERIAL_CALLBACK(material)
+    keep.append(cb)
+    t.material = cb
+    if fem.material.eval_feasible_step is not None:
+        from .fem import _cuda_f64
+
+        def feasible(Fp, Gp, rows, alpha, _user):
+            try:
+                F = _view(Fp, (rows, 3, 3), dev)
+                dF = _view(Gp, (rows, 3, 3), dev) - torch.eye(3, dtype=torch.float64, device=dev)
+                bound = _cuda_f64(fem.material.eval_feasible_step(F, fem._Fp, fem._theta, dF), (rows,), dev)
+                if not bool(torch.all(torch.isfinite(bound))):
+                    raise ValueError("PyVolumetricMaterial.eval_feasible_step returned non-finite values")
+                alpha[0] = float(torch.clamp(bound, 0.0, 1.0).min()) if rows else 1.0
+                return 0
+            except BaseException as exc:
+                box.append(exc)
+                return 1
+
+        fcb = N.FEASIBLE_CALLBACK(feasible)
+        keep.append(fcb)
+        t.feasible = fcb
+
+
+def _terms(w, A, c, on_iteration, fem=None):
+    """lpg_newton_terms for a weighted sum, an optional callback and a Python material (None when
+    none is needed). Returns (terms, keep-alive list, error box): an exception raised by a
+    callback stops the solve (LPG_ESTOPPED) and is re-raised by the caller from the box."""
+    from .fem import VolumetricFemEnergyPyMaterialTetP1
+
+    is_material = isinstance(fem, VolumetricFemEnergyPyMaterialTetP1)
+    if w == 1.0 and A is None and c == 0.0 and on_iteration is None and not is_material:
         return None, [], None
     keep, box = [], []
     t = N.NewtonTermsC()
@@ -164,6 +229,8 @@ def _terms(w, A, c, on_iteration):
         cb = N.NEWTON_CALLBACK(trampoline)
         keep.append(cb)
         t.on_iteration = cb
+    if is_material:
+        _material_callbacks(fem, t, keep, box)
     return t, keep, box
 
 
@@ -199,7 +266,12 @@ def newton_solve(energy, fixed, x0, options, solver=None, on_iteration=None):
     fixed_arr = np.ascontiguousarray(fixed.fixed_dofs, dtype=np.int32)
     res = N.NewtonResultC()
     opts = options.to_c()
-    terms, keep, box = _terms(w, A, c, on_iteration)
+    terms, keep, box = _terms(w, A, c, on_iteration, fem)
+    if terms is not None and terms.material:
+        # The material runs on torch's current stream: the library's work goes on the same one.
+        import torch
+
+        N.check(N.lib.lpg_fem_set_stream(fem.handle, ctypes.c_void_p(torch.cuda.current_stream(fem.device).cuda_stream)))
     if terms is None:
         N.check(N.lib.lpg_newton_solve(fem.handle, N.iptr(fixed_arr), int(fixed_arr.size), ptrs[0], ptrs[1], ptrs[3],
                                        ctypes.byref(opts), ptrs[2], ctypes.byref(res)))

@@ -6,7 +6,8 @@
   adjoint against central finite differences;
 - the per-element Lame adjoint of a 32^3 box through torch.autograd against central finite
   differences along 20 seeded directions (steps relative to theta): 1e-6 relative at step
-  1e-4, and within the solves' round-off noise at step 1e-6.
+  1e-4, and within the solves' round-off noise at step 1e-6; and against the oracle's
+  equilibrium gradient at the same equilibrium (1e-7 max-norm relative).
 """
 
 import numpy as np
@@ -177,3 +178,13 @@ def test_theta_adjoint_32cube_matches_finite_differences():
     print("adjoint vs central differences, max relative error per step:", {h: max(v) for h, v in errs.items()})
     assert max(errs[1e-4]) <= 1e-6, errs
     assert max(errs[1e-6]) <= 2e-4, errs
+    # The reference's own equilibrium gradient (StaticEquilibriumResponse's adjoint,
+    # static_equilibrium_response.cpp:43-88, restated by the oracle) at the same equilibrium
+    # x*(theta0) with dL/du = 2 (x* - x_target): per-element [d/dlambda, d/dmu]. The oracle solves
+    # K lambda = dL/du with its block-Jacobi PCG to 1e-12 (its envelope LDL^T does not fit 32^3).
+    x_star = model.eval_value(th0)
+    orc = oracle.OracleMesh(X, tets, g["theta"])
+    dtheta, _ = orc.adjoint_theta(x_star, 2.0 * (x_star - x_target), fixed, linear_solver=1, cg_tolerance=1e-12)
+    err = float(np.max(np.abs(grad - dtheta.ravel())) / np.max(np.abs(dtheta)))
+    print("adjoint vs the oracle's equilibrium gradient at 32^3:", err)
+    assert err <= 1e-7

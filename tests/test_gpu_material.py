@@ -227,3 +227,44 @@ def test_torch_stvk_on_hexes_matches_a_dense_assembly():
     assert abs(E - Er) <= 1e-12 * abs(Er)
     assert rel_err(g, gr) <= 1e-12
     assert rel_err(H.toarray(), Hr) <= 1e-12
+
+
+def test_newton_over_a_torch_material_matches_the_native_solve():
+    """The reference runs newton_solve on a TorchVolumetricMaterial energy
+    (examples/fem/fitting/torch_neohookean.py:112-113): a torch neo-Hookean gravity equilibrium
+    (projected Hessian, Exact near the end) matches the native one, with the same step records;
+    an exception in the material stops the solve and propagates."""
+    import scipy.sparse as sp
+
+    from litepgo_b200 import solver
+
+    g = workloads.gravity_box(4, seed=0)
+    n = g["X"].size
+    load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -g["f"])
+    native = fem.VolumetricFemEnergyTetP1.from_arrays(g["X"], g["tets"], g["theta"])
+    py = build(TorchNeoHookean, {"X": g["X"], "tets": g["tets"], "theta": g["theta"]})
+    opts = solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", cg_tolerance=1e-8)
+    fixed = dof.DofReduction(n, g["fixed"])
+    steps_n, steps_p = [], []
+    rn = solver.newton_solve(energy.WeightedSumEnergy([(native, 1.0), (load, 1.0)]), fixed, np.zeros(n), opts,
+                             on_iteration=steps_n.append)
+    rp = solver.newton_solve(energy.WeightedSumEnergy([(py, 1.0), (load, 1.0)]), fixed, np.zeros(n), opts,
+                             on_iteration=steps_p.append)
+    assert rn.status == rp.status == solver.NewtonStatus.Converged
+    assert rel_err(rp.x, rn.x) <= 1e-8
+    assert rp.iterations == rn.iterations and len(steps_p) == len(steps_n)
+    for a, b in zip(steps_p, steps_n):
+        assert abs(a.energy - b.energy) <= 1e-9 * abs(b.energy) + 1e-300
+    # A device start works too; a failing material stops the solve with its own exception.
+    rd = solver.newton_solve(energy.WeightedSumEnergy([(py, 1.0), (load, 1.0)]), fixed,
+                             torch.zeros(n, dtype=torch.float64, device="cuda"), opts)
+    assert rel_err(rd.x.cpu().numpy(), rn.x) <= 1e-8
+
+    class Broken(TorchNeoHookean):
+        @staticmethod
+        def W(F, Fp, theta):
+            raise RuntimeError("material failed")
+
+    bad = build(Broken, {"X": g["X"], "tets": g["tets"], "theta": g["theta"]})
+    with pytest.raises(RuntimeError, match="material failed"):
+        solver.newton_solve(bad, fixed, np.zeros(n), opts)
