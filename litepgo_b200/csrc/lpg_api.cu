@@ -255,12 +255,16 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
     a.cl_variant = tune.cl[pi];
     if (dm.K == 64) {
-        if (a.hess && hessian == LPG_HESSIAN_PROJECTED)
-            fail(LPG_EINVAL, "the projected Hessian is not available for Hermite hex meshes");
+        const bool projected = hessian == LPG_HESSIAN_PROJECTED;
         const size_t T = static_cast<size_t>(dm.T);
         double* elemE = delem ? delem : d_mat[3].as<double>(std::max<size_t>(T, 1));
-        void* blocks = a.hess ? d_proj.ensure(T * kHermiteRecord * (precision == LPG_PRECISION_F64 ? 8 : 4)) : nullptr;
-        launch_hermite_eval(dm, precision, du, elemE, d_vjp.as<double>(std::max<size_t>(192 * T, 1)), blocks, a, stream);
+        void* blocks = a.hess ? d_proj.ensure(hermite_blocks_bytes(dm, precision, projected)) : nullptr;
+        int* flags = projected && a.hess ? d_plist.as<int>(std::max<size_t>(T, 1)) : nullptr;
+        double* qbuf = projected && a.hess && T > 0
+                           ? d_herm_q.as<double>(static_cast<size_t>(hermite_psd_grid(dm)) * 192 * 192)
+                           : nullptr;
+        launch_hermite_eval(dm, precision, projected, du, elemE, d_vjp.as<double>(std::max<size_t>(192 * T, 1)), blocks,
+                            flags, qbuf, a, stream);
         return;
     }
     if (dm.K == 8) {

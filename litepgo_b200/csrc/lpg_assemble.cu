@@ -2606,11 +2606,16 @@ __device__ __forceinline__ void hermite_pair(int pr, int& a, int& b) {
 // the matrix is bitwise symmetric).
 constexpr int kHermiteThreads = 128;
 
+// With flags (projected Hessian), flags[e] is set when the tangent d2W/dF2 of some point is not
+// positive semi-definite (the element's Hessian then needs the eigenvalue clamp), and cleared
+// otherwise: a sum of w B^T A B with semi-definite A is semi-definite.
 template <typename R>
 __global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const DevMesh m, const double* __restrict__ u,
                                                                           double* __restrict__ elemE,
                                                                           double* __restrict__ per_elem,
-                                                                          R* __restrict__ blocks, unsigned* status) {
+                                                                          R* __restrict__ blocks, unsigned* status,
+                                                                          int* __restrict__ flags = nullptr) {
+    __shared__ int sFlag;
     __shared__ double sD[192];
     __shared__ double sK[64 * 20]; // per point: w, p, F^-T (9), P (9)
     __shared__ double sE[64];
@@ -2627,6 +2632,7 @@ __global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const 
         if (!isfinite(d)) st |= ST_BAD_INPUT;
         sD[t] = d;
     }
+    if (tid == 0) sFlag = 0;
     __syncthreads();
     for (int q = tid; q < m.nq; q += blockDim.x) {
         const double* tq = m.herm_q + kHermiteTable * static_cast<size_t>(q);
@@ -2664,6 +2670,23 @@ __global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const 
         const double L = log(detF), p = lam * L - mu, w = __ldg(tq + 192) * h[0] * h[1] * h[2];
         k[0] = w;
         k[1] = p;
+        if (flags) {
+            // The point's tangent A[(3i+j)(3k+l)] = mu d_ik d_jl + lambda H_ij H_kl - p H_il H_kj (H = F^-T).
+            double Gt[9], A[81], scale = 0;
+#pragma unroll
+            for (int t = 0; t < 9; ++t) Gt[t] = C[t] / detF;
+            for (int r = 0; r < 9; ++r)
+                for (int c = 0; c < 9; ++c) {
+                    const int i = r / 3, j = r % 3, kk = c / 3, l = c % 3;
+                    double v = lam * (Gt[r] * Gt[c]) - p * (Gt[3 * i + l] * Gt[3 * kk + j]);
+                    if (r == c) {
+                        v += mu;
+                        scale = fmax(scale, fabs(v));
+                    }
+                    A[9 * r + c] = v;
+                }
+            if (!(scale < INFINITY) || !semidefinite_ldlt<9>(A, 64 * Eps<double>::v * scale)) sFlag = 1;
+        }
         double ff = 0;
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
@@ -2680,6 +2703,7 @@ __global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const 
         for (int q = 0; q < m.nq; ++q) E += sE[q];
         if (!isfinite(E)) st |= ST_NONFINITE_OUT;
         elemE[e] = E;
+        if (flags) flags[e] = sFlag;
     }
     if (per_elem) {
         for (int b = tid; b < 64; b += blockDim.x) {
@@ -2741,6 +2765,277 @@ __global__ void __launch_bounds__(kHermiteThreads) hermite_element_kernel(const 
                 o[t] = static_cast<R>(Hb[t]);
             }
         }
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if ((tid & 31) == 0 && st) atomicOr(status, st);
+}
+
+
+// ---------------------------------------------------------------------------
+// Projected Hessian of tricubic Hermite hexes: V max(L, 0) V^T of each flagged element's 192 x 192
+// Hessian (mesh_energy.cpp:16-27, there Eigen's SelfAdjointEigenSolver). One CTA per element:
+// the lower triangle, packed, in shared memory is reduced to tridiagonal form by Householder
+// reflections (Golub & Van Loan, Matrix Computations, 8.3.1), the reflections are accumulated
+// into Q (column-major, in the CTA's global scratch), and the implicit QL iteration with
+// Wilkinson shifts (Golub & Van Loan 8.3.3, in the form of the EISPACK tql2 routine) diagonalises
+// the tridiagonal matrix, one thread generating each sweep's plane rotations and every thread
+// applying them to its row of Q. The projection is then H - sum_{L_m < 0} L_m v_m v_m^T (or the
+// sum over the positive eigenpairs when they are fewer), written back as the element's blocks.
+// ---------------------------------------------------------------------------
+constexpr int kHermN = 192;
+constexpr int kHermPacked = kHermN * (kHermN + 1) / 2;
+constexpr int kHermPsdThreads = 256;
+constexpr int kHermQlSweeps = 60; // per eigenvalue, far above the few the iteration takes
+constexpr size_t kHermPsdSmem = sizeof(double) * (kHermPacked + 6 * kHermN + 32);
+
+__device__ __forceinline__ int hpk(int r, int c) { return r * (r + 1) / 2 + c; } // r >= c
+__device__ __forceinline__ double hsym(const double* Ap, int r, int c) { return r >= c ? Ap[hpk(r, c)] : Ap[hpk(c, r)]; }
+
+// Block-wide sum (every thread receives it); red holds 32 doubles.
+__device__ __forceinline__ double herm_sum(double v, double* red) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+    __syncthreads();
+    return t;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kHermPsdThreads) hermite_psd_kernel(int T, double* in, R* out,
+                                                                      const int* __restrict__ flags,
+                                                                      double* __restrict__ qbuf, unsigned* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* Ap = reinterpret_cast<double*>(smem_raw); // packed lower triangle
+    double* d = Ap + kHermPacked;                     // diagonal, then eigenvalues
+    double* ev = d + kHermN;                          // off-diagonal
+    double* beta = ev + kHermN;                       // reflector coefficients
+    double* vp = beta + kHermN;                       // p, then w, of the current reflection
+    double* rc = vp + kHermN;                         // a sweep's rotations: c, s (2 per index)
+    double* red = rc + 2 * kHermN;
+    __shared__ int s_hi, s_count, s_bad;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    constexpr int n = kHermN;
+    double* Q = qbuf + static_cast<size_t>(blockIdx.x) * n * n; // Q(r, c) at c n + r
+    unsigned st = 0;
+    for (int e = blockIdx.x; e < T; e += gridDim.x) {
+        const double* rec = in + kHermiteRecord * static_cast<size_t>(e);
+        R* o = out + kHermiteRecord * static_cast<size_t>(e);
+        if (!flags[e]) { // semi-definite at every point: its own projection
+            if (static_cast<const void*>(o) != static_cast<const void*>(rec))
+                for (int t = tid; t < kHermiteRecord; t += bd) o[t] = static_cast<R>(rec[t]);
+            continue;
+        }
+        // The element matrix: block (a, b), a <= b, entry (i, c) is H(3a + i, 3b + c).
+        for (int t = tid; t < kHermiteRecord; t += bd) {
+            const int pr = t / 9, ic = t - 9 * (t / 9);
+            int a, b;
+            hermite_pair(pr, a, b);
+            const int r = 3 * a + ic / 3, c = 3 * b + ic % 3;
+            if (r >= c) Ap[hpk(r, c)] = rec[t];
+            else if (a != b) Ap[hpk(c, r)] = rec[t];
+        }
+        __syncthreads();
+        // Householder tridiagonalisation: column k's reflection P = I - beta v v^T maps
+        // A[k+1:, k] to (alpha, 0, ...); v is kept in place of the column below the subdiagonal.
+        for (int k = 0; k < n - 2; ++k) {
+            const int m = n - k - 1;
+            double x2 = 0;
+            for (int j = tid + 1; j < m; j += bd) {
+                const double x = Ap[hpk(k + 1 + j, k)];
+                x2 = fma(x, x, x2);
+            }
+            x2 = herm_sum(x2, red);
+            const double x0 = Ap[hpk(k + 1, k)];
+            if (x2 == 0.0) { // already tridiagonal in this column
+                if (tid == 0) {
+                    beta[k] = 0.0;
+                    ev[k] = x0;
+                }
+                __syncthreads();
+                continue;
+            }
+            const double alpha = -copysign(sqrt(fma(x0, x0, x2)), x0);
+            const double v0 = x0 - alpha, bk = 1.0 / (alpha * (alpha - x0)); // 2 / v^T v
+            __syncthreads();
+            if (tid == 0) {
+                Ap[hpk(k + 1, k)] = v0;
+                beta[k] = bk;
+                ev[k] = alpha;
+            }
+            __syncthreads();
+            // p = beta A22 v (row i of the trailing block), then K = beta / 2 p^T v, w = p - K v.
+            double pv = 0;
+            for (int i = tid; i < m; i += bd) {
+                double acc = 0;
+                for (int j = 0; j < m; ++j) acc = fma(hsym(Ap, k + 1 + i, k + 1 + j), Ap[hpk(k + 1 + j, k)], acc);
+                const double p = bk * acc;
+                vp[i] = p;
+                pv = fma(p, Ap[hpk(k + 1 + i, k)], pv);
+            }
+            const double K = 0.5 * bk * herm_sum(pv, red);
+            for (int i = tid; i < m; i += bd) vp[i] = fma(-K, Ap[hpk(k + 1 + i, k)], vp[i]);
+            __syncthreads();
+            // A22 -= v w^T + w v^T on the lower triangle (rows paired for balance).
+            for (int t = tid; t < m; t += bd) {
+                const int i = t;
+                const double vi = Ap[hpk(k + 1 + i, k)], wi = vp[i];
+                for (int j = 0; j <= i; ++j) {
+                    const double vj = Ap[hpk(k + 1 + j, k)], wj = vp[j];
+                    Ap[hpk(k + 1 + i, k + 1 + j)] -= fma(vi, wj, wi * vj);
+                }
+            }
+            __syncthreads();
+        }
+        for (int i = tid; i < n; i += bd) d[i] = Ap[hpk(i, i)];
+        if (tid == 0) {
+            ev[n - 2] = Ap[hpk(n - 1, n - 2)];
+            beta[n - 2] = 0.0;
+            ev[n - 1] = 0.0;
+        }
+        // Q = P_0 P_1 ... P_{n-3}, accumulated from the last reflection (Q = I to begin with).
+        for (int t = tid; t < n * n; t += bd) Q[t] = (t % n == t / n) ? 1.0 : 0.0;
+        __syncthreads();
+        for (int k = n - 3; k >= 0; --k) {
+            const double bk = beta[k];
+            if (bk == 0.0) continue;
+            const int m = n - k - 1;
+            // Columns c of Q with c > k: Q[k+1:, c] -= bk v (v^T Q[k+1:, c]); a warp per column.
+            const int warp = tid >> 5, lane = tid & 31;
+            for (int c = k + 1 + warp; c < n; c += bd >> 5) {
+                double* qc = Q + static_cast<size_t>(c) * n + k + 1;
+                double acc = 0;
+                for (int j = lane; j < m; j += 32) acc = fma(Ap[hpk(k + 1 + j, k)], qc[j], acc);
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+                const double f = bk * acc;
+                for (int j = lane; j < m; j += 32) qc[j] = fma(-f, Ap[hpk(k + 1 + j, k)], qc[j]);
+            }
+            __syncthreads();
+        }
+        // Implicit QL with Wilkinson shifts on (d, ev); rotations applied to the rows of Q.
+        if (tid == 0) s_bad = 0;
+        __syncthreads();
+        for (int l = 0; l < n; ++l) {
+            for (int iter = 0;; ++iter) {
+                if (tid == 0) {
+                    int m = l;
+                    for (; m < n - 1; ++m) {
+                        const double dd = fabs(d[m]) + fabs(d[m + 1]);
+                        if (fabs(ev[m]) <= 2.220446049250313e-16 * dd) break;
+                    }
+                    s_hi = m;
+                    s_count = 0;
+                    if (m != l) {
+                        if (iter >= kHermQlSweeps) {
+                            s_bad = 1;
+                            s_hi = l;
+                        } else {
+                            double g = (d[l + 1] - d[l]) / (2.0 * ev[l]);
+                            double r = hypot(g, 1.0);
+                            g = d[m] - d[l] + ev[l] / (g + copysign(r, g));
+                            double sn = 1.0, cs = 1.0, p = 0.0;
+                            int i = m - 1;
+                            bool split = false;
+                            for (; i >= l; --i) {
+                                const double f = sn * ev[i], b = cs * ev[i];
+                                r = hypot(f, g);
+                                ev[i + 1] = r;
+                                if (r == 0.0) {
+                                    d[i + 1] -= p;
+                                    ev[m] = 0.0;
+                                    split = true;
+                                    break;
+                                }
+                                sn = f / r;
+                                cs = g / r;
+                                g = d[i + 1] - p;
+                                r = (d[i] - g) * sn + 2.0 * cs * b;
+                                p = sn * r;
+                                d[i + 1] = g + p;
+                                g = cs * r - b;
+                                rc[2 * i] = cs;
+                                rc[2 * i + 1] = sn;
+                                ++s_count;
+                            }
+                            if (!split) {
+                                d[l] -= p;
+                                ev[l] = g;
+                                ev[m] = 0.0;
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                const int m = s_hi, cnt = s_count;
+                if (m == l) break;
+                // Apply rotations i = m-1 .. m-cnt to row r of Q: columns i and i+1.
+                for (int r = tid; r < n; r += bd) {
+                    double hi = Q[static_cast<size_t>(m) * n + r];
+                    for (int i = m - 1; i >= m - cnt; --i) {
+                        const double cs = rc[2 * i], sn = rc[2 * i + 1];
+                        const double lo = Q[static_cast<size_t>(i) * n + r];
+                        Q[static_cast<size_t>(i + 1) * n + r] = fma(sn, lo, cs * hi);
+                        hi = fma(cs, lo, -sn * hi);
+                    }
+                    Q[static_cast<size_t>(m - cnt) * n + r] = hi;
+                }
+                __syncthreads();
+            }
+        }
+        if (s_bad) st |= ST_NONFINITE_OUT;
+        // Reconstruction from the fewer of the negative and positive eigenpairs, staged in the
+        // (now free) shared matrix 96 vectors at a time.
+        int nneg = 0;
+        for (int i = 0; i < n; ++i) nneg += d[i] < 0.0;
+        const bool from_neg = nneg <= n / 2;
+        constexpr int kStage = 96;
+        // Each thread keeps its entries' partial sums in the FP64 record itself (`in` is scratch:
+        // it is read and rewritten by the same thread, entry by entry).
+        double* acc_rec = in + kHermiteRecord * static_cast<size_t>(e);
+        for (int base = 0; base < n; base += kStage) {
+            // Stage eigenvectors base .. base + kStage - 1 that take part, scaled by their eigenvalue.
+            __syncthreads();
+            for (int t = tid; t < kStage * n; t += bd) {
+                const int mm = base + t / n, r = t % n;
+                double v = 0.0;
+                if (mm < n) {
+                    const double lm = d[mm];
+                    const bool use = from_neg ? lm < 0.0 : lm > 0.0;
+                    v = use ? Q[static_cast<size_t>(mm) * n + r] : 0.0;
+                }
+                Ap[t] = v;
+            }
+            __syncthreads();
+            for (int t = tid; t < kHermiteRecord; t += bd) {
+                const int pr = t / 9, ic = t - 9 * (t / 9);
+                int a, b;
+                hermite_pair(pr, a, b);
+                int r = 3 * a + ic / 3, c = 3 * b + ic % 3;
+                if (a == b && r > c) { // diagonal blocks: the lower entry mirrors the upper one
+                    const int tmp = r;
+                    r = c;
+                    c = tmp;
+                }
+                double sum = 0.0;
+                for (int k2 = 0; k2 < kStage && base + k2 < n; ++k2)
+                    sum = fma(d[base + k2] * Ap[k2 * n + r], Ap[k2 * n + c], sum);
+                // The element pass stores diagonal blocks bitwise symmetric, so entry t itself holds
+                // the mirrored value.
+                const double prev = base == 0 ? (from_neg ? acc_rec[t] : 0.0) : acc_rec[t];
+                acc_rec[t] = from_neg ? prev - sum : prev + sum;
+            }
+        }
+        __syncthreads();
+        for (int t = tid; t < kHermiteRecord; t += bd) {
+            const double v = acc_rec[t];
+            if (!isfinite(v)) st |= ST_NONFINITE_OUT;
+            o[t] = static_cast<R>(v);
+        }
+        __syncthreads();
     }
     st = __reduce_or_sync(0xffffffffu, st);
     if ((tid & 31) == 0 && st) atomicOr(status, st);
@@ -3153,12 +3448,45 @@ void launch_hex_material_eval(const DevMesh& m, int precision, int hessian, cons
     LPG_CUDA(cudaGetLastError());
 }
 
-void launch_hermite_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem,
-                         void* blocks, const EvalArgs& a, cudaStream_t s) {
+size_t hermite_blocks_bytes(const DevMesh& m, int precision, bool projected) {
+    const size_t records = kHermiteRecord * static_cast<size_t>(m.T);
+    if (precision == LPG_PRECISION_F64) return records * sizeof(double);
+    return records * (projected ? sizeof(double) + sizeof(float) : sizeof(float));
+}
+
+int hermite_psd_grid(const DevMesh& m) {
+    int dev = 0, sms = 0;
+    LPG_CUDA(cudaGetDevice(&dev));
+    LPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return std::max(1, std::min(m.T, sms));
+}
+
+void launch_hermite_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
+                         double* per_elem, void* blocks, int* flags, double* qbuf, const EvalArgs& a, cudaStream_t s) {
     if (m.T > 0) {
         if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
         double* per_grad = a.grad ? per_elem : nullptr;
-        if (precision == LPG_PRECISION_F64 || !a.hess)
+        if (a.hess && projected) {
+            // FP64 element Hessians with the per-point pre-test, then the clamp of the flagged
+            // elements into the precision's records.
+            double* records = static_cast<double*>(blocks);
+            hermite_element_kernel<double><<<m.T, kHermiteThreads, 0, s>>>(m, u, elemE, per_grad, records, a.status,
+                                                                            flags);
+            const int grid = hermite_psd_grid(m);
+            if (precision == LPG_PRECISION_F64) {
+                thread_local LaunchCache cache;
+                resident_grid(hermite_psd_kernel<double>, kHermPsdThreads, kHermPsdSmem, cache);
+                hermite_psd_kernel<double><<<grid, kHermPsdThreads, kHermPsdSmem, s>>>(m.T, records, records, flags,
+                                                                                      qbuf, a.status);
+            } else {
+                float* out = reinterpret_cast<float*>(records + kHermiteRecord * static_cast<size_t>(m.T));
+                thread_local LaunchCache cache;
+                resident_grid(hermite_psd_kernel<float>, kHermPsdThreads, kHermPsdSmem, cache);
+                hermite_psd_kernel<float><<<grid, kHermPsdThreads, kHermPsdSmem, s>>>(m.T, records, out, flags, qbuf,
+                                                                                     a.status);
+                blocks = out;
+            }
+        } else if (precision == LPG_PRECISION_F64 || !a.hess)
             hermite_element_kernel<double><<<m.T, kHermiteThreads, 0, s>>>(
                 m, u, elemE, per_grad, a.hess ? static_cast<double*>(blocks) : nullptr, a.status);
         else

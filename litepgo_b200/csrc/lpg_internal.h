@@ -291,8 +291,13 @@ void launch_hex_material_eval(const DevMesh& m, int precision, int hessian, cons
 // Tricubic Hermite hex element pass (Exact Hessian): energy per element into elemE, gradient
 // pieces (192 per element) into per_elem when a.grad is set, the 2080 blocks per element
 // (precision's type, kHermiteRecord values) into blocks when a.hess is set, then the gathers.
-void launch_hermite_eval(const DevMesh& m, int precision, const double* u, double* elemE, double* per_elem,
-                         void* blocks, const EvalArgs& a, cudaStream_t s);
+// With projected, each element's 192 x 192 Hessian is first projected to PSD where its per-point
+// pre-test fails (flags: T ints of scratch; qbuf: hermite_psd_grid() x 192^2 doubles of scratch);
+// blocks then holds hermite_blocks_bytes().
+void launch_hermite_eval(const DevMesh& m, int precision, bool projected, const double* u, double* elemE,
+                         double* per_elem, void* blocks, int* flags, double* qbuf, const EvalArgs& a, cudaStream_t s);
+size_t hermite_blocks_bytes(const DevMesh& m, int precision, bool projected);
+int hermite_psd_grid(const DevMesh& m);
 // Bytes of the block records launch_hex_eval needs: FP64 records, plus FP32 ones for a
 // projected mixed-precision Hessian (the projection runs in FP64).
 size_t hex_blocks_bytes(const DevMesh& m, int precision, bool projected);

@@ -37,6 +37,7 @@ struct lpg_fem {
         b_unused;
     lpg::DeviceBuffer b_hex[4]; // hex meshes: rest positions, cells, [lambda, mu], quadrature table
     lpg::DeviceBuffer b_herm;   // Hermite hex meshes: box edge lengths per element
+    lpg::DeviceBuffer d_herm_q; // Hermite projected Hessian: eigenvector scratch, 192^2 doubles per CTA
     lpg::DeviceBuffer b_cl[11]; // assembly clusters
     lpg::DeviceBuffer b_tc[13]; // tet assembly clusters
     lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers

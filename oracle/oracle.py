@@ -477,11 +477,13 @@ def hermite_slot_scales(h):
     return np.array([1, h[0], h[1], h[2], h[0] * h[1], h[0] * h[2], h[1] * h[2], h[0] * h[1] * h[2]])
 
 
-def hex_hermite_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
+def hex_hermite_eval(X, cells, theta, u, points_per_axis=2, hessian=True, projected=False):
     """E, gradient and dense Hessian (or None) over the physical DOFs (24 per vertex) of the
     tricubic Hermite neo-Hookean energy on axis-aligned box hexes (Fp = I): reference coefficients
     c = s * d, F = I + sum_b c_b (J^-T dN_b), J = diag(h), and the element gradient and Hessian
-    pulled back by the same scales (s g, S H S)."""
+    pulled back by the same scales (s g, S H S). With projected, each element's 192 x 192
+    Hessian (over its physical DOFs) is projected (project_psd) before assembly, as
+    MeshEnergy does for HessianKind::Projected (mesh_energy.cpp:16-27)."""
     X = np.asarray(X, float).reshape(-1, 3)
     cells = np.asarray(cells).reshape(-1, 8)
     D = np.asarray(u, float).reshape(-1, 24)
@@ -512,7 +514,8 @@ def hex_hermite_eval(X, cells, theta, u, points_per_axis=2, hessian=True):
                 He += w * B.T @ nh_d2W_dF2(F, np.eye(3), th[e]) @ B
         g[dofs] += s * ge
         if hessian:
-            H[np.ix_(dofs, dofs)] += s[:, None] * He * s[None, :]
+            Hp = s[:, None] * He * s[None, :]
+            H[np.ix_(dofs, dofs)] += project_psd(Hp) if projected else Hp
     return E, g, H
 
 

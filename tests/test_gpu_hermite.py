@@ -77,8 +77,6 @@ def test_structured_box_and_feasible_step():
 
 def test_construction_and_unsupported_requests():
     gpu = hermite_energy(HERMITE_X, HERMITE_CELLS, HERMITE_THETA)
-    with pytest.raises(ValueError, match="Hermite"):
-        gpu.eval(hermite_state(), hessian=Projected)
     corners = oracle.HEX_CORNERS.astype(float)
     cell = np.arange(8, dtype=np.int32)[None]
     hermite_energy(corners, cell, HERMITE_THETA)
@@ -192,3 +190,66 @@ def test_hermite_theta_adjoint_matches_finite_differences():
         d = rng.standard_normal(2 * T) * th0
         fd = (8 * (L(th0 + h * d) - L(th0 - h * d)) - (L(th0 + 2 * h * d) - L(th0 - 2 * h * d))) / (12 * h)
         assert abs(grad @ d - fd) <= 1e-6 * abs(fd)
+
+
+def expanded_hermite_state(X, scale, noise, seed):
+    """The affine field u = scale X in physical Hermite DOFs (value slot scale X, u_X, u_Y, u_Z the
+    columns of scale I, mixed slots zero) plus seeded noise on every DOF."""
+    V = X.shape[0]
+    D = np.zeros((V, 8, 3))
+    D[:, 0] = scale * X
+    for k in range(3):
+        D[:, 1 + k, k] = scale
+    return D.ravel() + noise * np.random.default_rng(seed).standard_normal(24 * V)
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-11), ("mixed", 1e-6)])
+def test_projected_hessian_matches_the_oracle(precision, tol):
+    """HessianKind.Projected on Hermite hexes: every element's 192 x 192 Hessian clamped to PSD
+    (the reference's per-element eigenvalue clamp) where its tangents are indefinite; here a
+    uniform expansion with lambda / mu = 10 makes them so."""
+    X, cells = mesh.make_hex_box(3, 2, 2)
+    theta = np.array([10.0, 1.0])
+    u = expanded_hermite_state(X, 0.5, 1e-3, 3)
+    gpu = hermite_energy(X, cells, theta)
+    _, _, Hp = gpu.eval(u, hessian=Projected, precision=precision)
+    _, _, He = gpu.eval(u, hessian=Exact)
+    _, _, Hr = oracle.hex_hermite_eval(X, cells, theta, u, projected=True)
+    assert rel_err(Hp.toarray(), Hr) <= tol
+    assert rel_err(He.toarray(), Hr) > 1e-3  # the clamp changed the matrix
+    assert np.linalg.eigvalsh(Hp.toarray()).min() >= -1e-10 * np.abs(Hr).max()
+    D = (Hp - Hp.T).tocsc()
+    D.eliminate_zeros()
+    assert D.nnz == 0  # bitwise symmetric
+
+
+def test_hermite_corner_pull_example():
+    """The reference's examples/fem/equilibrium/hex_hermite_corner_pull.py on its own box-hex.veg:
+    tricubic Hermite hexes with GaussLegendre3D[4], theta = [2, 3], springs pulling the value
+    slots of the eight bounding-box corners to a copy of the box stretched by 0.3, no fixed DOF,
+    default NewtonOptions (Projected Hessian) with gradient_tolerance 1e-8. The oracle's gradient
+    of the same potential at the result meets the tolerance."""
+    from pathlib import Path
+
+    assets = np.load(Path(__file__).resolve().parent / "golden" / "assets.npz")
+    X, cells = assets["box_hex_X"], assets["box_hex_cells"]
+    theta = np.array([2.0, 3.0])
+    elastic = hermite_energy(X, cells, theta, 4)
+    n = elastic.num_dofs
+    lower, upper = X.min(axis=0), X.max(axis=0)
+    tol = (upper - lower).max() * 1e-8
+    near = (np.abs(X - lower) <= tol) | (np.abs(X - upper) <= tol)
+    corners = np.flatnonzero(near.all(axis=1))
+    assert corners.size == 8
+    pulled = (24 * corners[:, None] + np.arange(3)).astype(np.int32)
+    targets = 0.3 * (X[corners] - lower)
+    pulling = energy.VertexPullingEnergy(n, pulled, targets, 1.0)
+    potential = energy.WeightedSumEnergy([(elastic, 1.0), (pulling, 1.0)])
+    steps = []
+    r = solver.newton_solve(potential, dof.DofReduction(n, []), np.zeros(n),
+                            solver.NewtonOptions(gradient_tolerance=1e-8), on_iteration=steps.append)
+    assert r.status == solver.NewtonStatus.Converged, r
+    assert any(s.diagonal_shifts == 0 for s in steps) and steps[-1].gradient_norm <= 1e-8
+    _, g, _ = oracle.hex_hermite_eval(X, cells, theta, np.asarray(r.x), points_per_axis=4, hessian=False)
+    g = g + pulling.eval_gradient(r.x)
+    assert np.abs(g).max() <= 1e-8 + 1e-12 * np.abs(pulling.eval_gradient(np.zeros(n))).max()
