@@ -227,11 +227,17 @@ __device__ __forceinline__ int64_t diag_entry(const DevMesh& m, int v, int t) {
 #endif
 // Launch variants of the PCG SpMV (autotuner): {resident blocks, slot unroll}. Variant 0 is the
 // default; all variants sum each row in the same order, so their results are bitwise identical.
+// Variant 2 reads a lane's slots in batches of four: their column indices first,
+// then all their vector gathers, then the block values and products, so that a batch of gathers
+// per lane is in flight instead of the loop's dependent column -> gather chain of one or two
+// slots; the products are summed in the same slot order as the other variants.
 template <typename TK, int VAR> struct SpmvCfg {
     static constexpr bool f32 = sizeof(TK) == 4;
     static constexpr int minb = VAR == 0 ? (f32 ? LPG_SPMV_MIN_BLOCKS_F32 : LPG_SPMV_MIN_BLOCKS_F64)
-                                         : VAR == 1 ? (f32 ? 8 : 4) : (f32 ? 6 : 3);
+                                         : VAR == 1 ? (f32 ? 8 : 4) : (f32 ? 3 : 2);
     static constexpr int unroll = VAR == 0 ? LPG_SPMV_UNROLL : 4;
+    static constexpr bool batched = VAR == 2;
+    static constexpr int batch = 4;
 };
 template <typename TK, typename TV, typename TO, bool PCG, bool DOT, int S, int VAR = 0>
 __global__ void __launch_bounds__(kThreads, (SpmvCfg<TK, VAR>::minb)) spmv_sell(const DevMesh m, const TK* __restrict__ val,
@@ -265,35 +271,80 @@ __global__ void __launch_bounds__(kThreads, (SpmvCfg<TK, VAR>::minb)) spmv_sell(
 #pragma unroll
             for (int i = 0; i < 3; ++i) xv[i] = static_cast<A>(xz[i]);
         };
-        // Own blocks (columns >= row): K_rc x_c.
-#pragma unroll (SpmvCfg<TK, VAR>::unroll)
-        for (int q = 0; q < width; ++q) {
-            A xv[3];
-            gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
-            const TK* vq = vp + 288 * static_cast<size_t>(q);
-            A kv[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
-            a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
-            a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
-            a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
-        }
-        // Borrowed blocks (columns < row): K_cr^T x_c from the owning row's block.
         const int b0 = __ldg(m.sell_bptr + c);
         const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
         const int2* bp = m.sell_bref + b0 + lane;
-#pragma unroll (SpmvCfg<TK, VAR>::unroll)
-        for (int q = 0; q < bwidth; ++q) {
-            const int2 ref = __ldg(bp + 32 * q);
-            A xv[3];
-            gather(static_cast<size_t>(ref.y), xv);
-            const TK* vq = val + static_cast<size_t>(ref.x);
-            A kv[9];
+        if constexpr (SpmvCfg<TK, VAR>::batched) {
+            constexpr int kSpmvBatch = SpmvCfg<TK, VAR>::batch;
+            // Own blocks (columns >= row), then borrowed blocks, each in batches of kSpmvBatch slots.
+            for (int q0 = 0; q0 < width; q0 += kSpmvBatch) {
+                int col[kSpmvBatch];
 #pragma unroll
-            for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
-            a0 += kv[0] * xv[0] + kv[3] * xv[1] + kv[6] * xv[2];
-            a1 += kv[1] * xv[0] + kv[4] * xv[1] + kv[7] * xv[2];
-            a2 += kv[2] * xv[0] + kv[5] * xv[1] + kv[8] * xv[2];
+                for (int j = 0; j < kSpmvBatch; ++j) col[j] = q0 + j < width ? __ldg(cp + 32 * (q0 + j)) : 0;
+                A xv[kSpmvBatch][3];
+#pragma unroll
+                for (int j = 0; j < kSpmvBatch; ++j)
+                    if (q0 + j < width) gather(static_cast<size_t>(col[j]), xv[j]);
+#pragma unroll
+                for (int j = 0; j < kSpmvBatch; ++j) {
+                    if (q0 + j >= width) break;
+                    const TK* vq = vp + 288 * static_cast<size_t>(q0 + j);
+                    A kv[9];
+#pragma unroll
+                    for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
+                    a0 += kv[0] * xv[j][0] + kv[1] * xv[j][1] + kv[2] * xv[j][2];
+                    a1 += kv[3] * xv[j][0] + kv[4] * xv[j][1] + kv[5] * xv[j][2];
+                    a2 += kv[6] * xv[j][0] + kv[7] * xv[j][1] + kv[8] * xv[j][2];
+                }
+            }
+            for (int q0 = 0; q0 < bwidth; q0 += kSpmvBatch) {
+                int2 ref[kSpmvBatch];
+#pragma unroll
+                for (int j = 0; j < kSpmvBatch; ++j) ref[j] = q0 + j < bwidth ? __ldg(bp + 32 * (q0 + j)) : make_int2(0, 0);
+                A xv[kSpmvBatch][3];
+#pragma unroll
+                for (int j = 0; j < kSpmvBatch; ++j)
+                    if (q0 + j < bwidth) gather(static_cast<size_t>(ref[j].y), xv[j]);
+#pragma unroll
+                for (int j = 0; j < kSpmvBatch; ++j) {
+                    if (q0 + j >= bwidth) break;
+                    const TK* vq = val + static_cast<size_t>(ref[j].x);
+                    A kv[9];
+#pragma unroll
+                    for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
+                    a0 += kv[0] * xv[j][0] + kv[3] * xv[j][1] + kv[6] * xv[j][2];
+                    a1 += kv[1] * xv[j][0] + kv[4] * xv[j][1] + kv[7] * xv[j][2];
+                    a2 += kv[2] * xv[j][0] + kv[5] * xv[j][1] + kv[8] * xv[j][2];
+                }
+            }
+        } else {
+            // Own blocks (columns >= row): K_rc x_c.
+#pragma unroll (SpmvCfg<TK, VAR>::unroll)
+            for (int q = 0; q < width; ++q) {
+                A xv[3];
+                gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
+                const TK* vq = vp + 288 * static_cast<size_t>(q);
+                A kv[9];
+#pragma unroll
+                for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
+                a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
+                a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
+                a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
+            }
+            // Borrowed blocks (columns < row): K_cr^T x_c from the owning row's block.
+#pragma unroll (SpmvCfg<TK, VAR>::unroll)
+            for (int q = 0; q < bwidth; ++q) {
+                const int2 ref = __ldg(bp + 32 * q);
+                A xv[3];
+                gather(static_cast<size_t>(ref.y), xv);
+                const TK* vq = val + static_cast<size_t>(ref.x);
+                A kv[9];
+#pragma unroll
+                for (int e = 0; e < 9; ++e) kv[e] = static_cast<A>(__ldg(vq + 32 * e));
+                a0 += kv[0] * xv[0] + kv[3] * xv[1] + kv[6] * xv[2];
+                a1 += kv[1] * xv[0] + kv[4] * xv[1] + kv[7] * xv[2];
+                a2 += kv[2] * xv[0] + kv[5] * xv[1] + kv[8] * xv[2];
+            }
         }
         if (row >= 0) {
             const size_t o = static_cast<size_t>(row);
