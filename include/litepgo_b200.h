@@ -385,6 +385,18 @@ int lpg_newton_solve_terms(lpg_fem_t h, const lpg_newton_terms* terms, const int
                            const double* f_ext, const double* x0, int io_mem, const lpg_newton_options* options,
                            double* x_out, lpg_newton_result* result);
 
+/*
+ * The adjoint solve of StaticEquilibriumResponse over a weighted-sum potential
+ * (static_equilibrium_response.cpp:43-68): lambda (num_dofs, io_mem; fixed entries zero) of
+ * K_ff lambda = dLdu_free, K the Exact Hessian of the potential of terms (NULL: the handle's
+ * elastic energy) at u_star, by PCG with FP64 refinement and the reference's residual check. A
+ * caller then forms the parameter gradient -(dg/dtheta)^T lambda with its own force response
+ * (for a Python material, through the material's d2W/dF dtheta).
+ */
+int lpg_adjoint_solve_terms(lpg_fem_t h, const lpg_newton_terms* terms, const double* u_star, const double* dLdu,
+                            const int32_t* fixed_dofs, int num_fixed, int io_mem, int precision, double cg_tolerance,
+                            double* lambda_out);
+
 /* Per-mesh outcome of lpg_batch_newton_solve (status as lpg_newton_result.status). */
 typedef struct {
     int status;

@@ -133,6 +133,7 @@ SIGNATURES = [
                                 ctypes.POINTER(NewtonResultC)]),
     ("lpg_newton_solve_terms", _int, [_vp, ctypes.POINTER(NewtonTermsC), _ip, _int, _vp, _vp, _int,
                                       ctypes.POINTER(NewtonOptionsC), _vp, ctypes.POINTER(NewtonResultC)]),
+    ("lpg_adjoint_solve_terms", _int, [_vp, ctypes.POINTER(NewtonTermsC), _vp, _vp, _ip, _int, _int, _int, _dbl, _vp]),
     ("lpg_batch_newton_solve", _int, [_vp, _int, _ip, _ip, _ip, _int, _vp, _vp, _int, ctypes.POINTER(NewtonOptionsC),
                                       _vp, ctypes.POINTER(BatchMeshResultC), ctypes.POINTER(NewtonResultC)]),
     ("lpg_adjoint_theta", _int, [_vp, _vp, _vp, _ip, _int, _int, _int, _dbl, _int, _vp, _vp]),

@@ -909,6 +909,17 @@ int lpg_newton_solve_terms(lpg_fem_t h, const lpg_newton_terms* terms, const int
     });
 }
 
+int lpg_adjoint_solve_terms(lpg_fem_t h, const lpg_newton_terms* terms, const double* u_star, const double* dLdu,
+                            const int32_t* fixed, int nfixed, int io_mem, int precision, double cg_tolerance,
+                            double* lambda_out) {
+    return guarded([&] {
+        if (!h || !u_star || !dLdu || !lambda_out) fail(LPG_EINVAL, "lpg_adjoint_solve_terms: null argument");
+        BusyGuard busy(h->busy);
+        LPG_CUDA(cudaSetDevice(h->device));
+        adjoint_lambda(*h, terms, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, lambda_out);
+    });
+}
+
 int lpg_fem_set_fp(lpg_fem_t h, const double* Fp, int fp_per_element) {
     return guarded([&] {
         if (!h) fail(LPG_EINVAL, "null handle");

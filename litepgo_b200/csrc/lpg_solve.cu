@@ -1285,10 +1285,13 @@ namespace {
 // Exact FP64 Hessian K at u*, then mask K lambda = mask dL/du by PCG with FP64 refinement and
 // the reference's residual check. Returns lambda (device) and u* (device) through out-params.
 void adjoint_solve(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
-                   int precision, double cg_tolerance, const double** u_dev, double** lam_dev) {
+                   int precision, double cg_tolerance, const double** u_dev, double** lam_dev,
+                   const lpg_newton_terms* terms = nullptr) {
     if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
     if (!(cg_tolerance > 0) || !std::isfinite(cg_tolerance)) fail(LPG_EINVAL, "adjoint: cg_tolerance must be positive");
-    Solver S(h);
+    Potential pot;
+    build_potential(h, terms, pot);
+    Solver S(h, &pot);
     const size_t n = S.n;
     const int V = S.V;
     cudaStream_t s = h.stream;
@@ -1308,8 +1311,9 @@ void adjoint_solve(lpg_fem& h, const double* u_star, const double* dLdu, const i
     const size_t nv = h.plan.sell_values();
     double* K64 = h.s_hess64.as<double>(std::max<size_t>(nv, 1));
     LPG_CUDA(cudaMemsetAsync(K64, 0, nv * sizeof(double), s));
-    h.eval_async(u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutSell, K64, nullptr);
+    eval_elastic_async(h, terms, u, nullptr, LPG_HESSIAN_EXACT, LPG_PRECISION_F64, kLayoutSell, K64);
     raise_status(h.take_status());
+    S.compose_hessian(K64);
     double* rhs = h.s_g.as<double>(std::max<size_t>(n, 1));
     LPG_CUDA(cudaMemcpyAsync(rhs, w, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     Solver::PcgOut po;
@@ -1338,6 +1342,15 @@ void copy_lambda(lpg_fem& h, const double* lam, int io_mem, double* lambda_out) 
 }
 
 } // namespace
+
+void adjoint_lambda(lpg_fem& h, const lpg_newton_terms* terms, const double* u_star, const double* dLdu,
+                    const int32_t* fixed, int nfixed, int io_mem, int precision, double cg_tolerance, double* lambda_out) {
+    const double* u = nullptr;
+    double* lam = nullptr;
+    adjoint_solve(h, u_star, dLdu, fixed, nfixed, io_mem, precision, cg_tolerance, &u, &lam, terms);
+    copy_lambda(h, lam, io_mem, lambda_out);
+    LPG_CUDA(cudaStreamSynchronize(h.stream));
+}
 
 void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                    int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out) {

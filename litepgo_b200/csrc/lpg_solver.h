@@ -72,6 +72,10 @@ namespace lpg {
 void newton_solve(lpg_fem& h, const int32_t* fixed, int nfixed, const double* f_ext, const double* x0, int io_mem,
                   const lpg_newton_options& o, double* x_out, lpg_newton_result* res,
                   const lpg_newton_terms* terms = nullptr);
+// The adjoint solve alone over a weighted-sum potential (terms may be null): lambda of
+// K_ff lambda = dL/du_free with the potential's Exact Hessian at u*.
+void adjoint_lambda(lpg_fem& h, const lpg_newton_terms* terms, const double* u_star, const double* dLdu,
+                    const int32_t* fixed, int nfixed, int io_mem, int precision, double cg_tolerance, double* lambda_out);
 void adjoint_theta(lpg_fem& h, const double* u_star, const double* dLdu, const int32_t* fixed, int nfixed, int io_mem,
                    int precision, double cg_tolerance, int per_element, double* dtheta, double* lambda_out);
 void batch_newton_solve(lpg_fem& h, int num_meshes, const int32_t* vertex_offsets, const int32_t* element_offsets,

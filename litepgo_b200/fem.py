@@ -1247,6 +1247,81 @@ class VolumetricFemEnergyPyMaterialHexQ1GL4(VolumetricFemEnergyPyMaterialHexQ1):
     _geometry_cls = VolumetricFemEnergyHexQ1GL4
 
 
+class VolumetricFemForceMaterialResponsePyTetP1:
+    """VolumetricFemForceMaterialResponse[Material, TetP1Basis, TetCentroidQuadrature] for a
+    PyVolumetricMaterial subclass ``material`` (set by the template; the reference's binding,
+    src/binding/detail/fem_helpers.hpp:76-98, with a Python material in the Material slot): the
+    force g(u; p) at a fixed displacement as a response of the material parameters, ConstantDofMap
+    (one theta for every element) or ElementDofMap (one per element). Its VJP is
+    (dg/dtheta_e)^T w = vol_e (d2W/dF dtheta) : grad w_e, with the material's d2W_dF_dtheta at every
+    element's F (one material row per element, on the GPU) and grad w_e = F(w) - I from the library."""
+
+    material = None
+
+    def __init__(self, parameter_map, displacement_map, rest_position_fields, displacement, Fp, batch_size=256):
+        import torch
+
+        mat = self.material
+        k = getattr(mat, "num_parameters", None)
+        if mat is None or not isinstance(k, int) or k <= 0:
+            raise ValueError("PyVolumetricMaterial: num_parameters must be a positive int for a material response")
+        if isinstance(batch_size, bool) or int(batch_size) <= 0:
+            raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
+        if not isinstance(parameter_map, (ConstantDofMap, ElementDofMap)):
+            raise TypeError("parameter_map must be a ConstantDofMap or an ElementDofMap")
+        width = parameter_map.num_dofs if isinstance(parameter_map, ConstantDofMap) else parameter_map.dofs_per_element
+        if parameter_map.num_elements != displacement_map.num_elements:
+            raise ValueError("VolumetricFemForceResponse: incompatible element count or batch size")
+        if width != k:
+            raise ValueError("VolumetricFemForceResponse: invalid parameter count")
+        self.per_element = isinstance(parameter_map, ElementDofMap)
+        T, V = displacement_map.num_elements, displacement_map.num_vertices
+        u = np.ascontiguousarray(displacement, dtype=np.float64)
+        if u.size != displacement_map.num_dofs or not np.all(np.isfinite(u)):
+            raise ValueError("VolumetricFemForceResponse: incompatible map, displacement or responses")
+        # The parameters enter through the material only; any value builds the energy's geometry.
+        self._energy = _py_energy_class(mat)(displacement_map, rest_position_fields, Fp, np.ones(k), batch_size)
+        X, Xe = _rest_geometry(rest_position_fields, V, T)
+        corners = Xe.reshape(T, 4, 3) if Xe is not None else X[displacement_map.cells]
+        D = corners[:, 1:] - corners[:, :1]
+        vol = np.einsum("ij,ij->i", D[:, 0], np.cross(D[:, 1], D[:, 2])) / 6.0
+        self._vol = torch.as_tensor(vol, device=self._energy.device)
+        self._F = self._energy.deformation_gradients(u)
+        self._k, self._T = k, T
+        self.displacement = u
+        self.num_inputs = parameter_map.num_dofs
+        self.num_outputs = displacement_map.num_dofs
+
+    def eval_vjp(self, p, w):
+        """(d g / d p)^T w: (k,) for a ConstantDofMap, (k T,) for an ElementDofMap."""
+        import torch
+
+        p = np.asarray(p, dtype=np.float64).ravel()
+        if p.size != self.num_inputs or not np.all(np.isfinite(p)):
+            raise ValueError("Response: p must have num_inputs finite entries")
+        wv = np.ascontiguousarray(w, dtype=np.float64)
+        if wv.size != self.num_outputs:
+            raise ValueError("Response: weights must have num_outputs entries")
+        T, k, dev = self._T, self._k, self._energy.device
+        th = p.reshape(T, k) if self.per_element else np.broadcast_to(p, (T, k))
+        theta = torch.as_tensor(np.ascontiguousarray(th), device=dev)
+        Gw = self._energy.deformation_gradients(wv) - torch.eye(3, dtype=torch.float64, device=dev)
+        out = self.material.eval(self._F, self._energy._Fp, theta, outputs=("dW_dF", "d2W_dF_dtheta"))
+        Dt = _cuda_f64(out["d2W_dF_dtheta"], (T, 3, 3, k), dev)
+        per = self._vol[:, None] * torch.einsum("nija,nij->na", Dt, Gw)
+        if not bool(torch.all(torch.isfinite(per))):
+            raise ValueError("PyVolumetricMaterial.eval returned non-finite values")
+        return (per.reshape(-1) if self.per_element else per.sum(0)).cpu().numpy()
+
+
+def _py_response_class(material, basis=TetP1Basis, quadrature=TetCentroidQuadrature):
+    if (basis, quadrature) != (TetP1Basis, TetCentroidQuadrature):
+        raise TypeError("VolumetricFemForceMaterialResponse of a Python material is instantiated for "
+                        "TetP1Basis, TetCentroidQuadrature")
+    return type(f"VolumetricFemForceMaterialResponse[{material.__name__}, {basis.__name__}, {quadrature.__name__}]",
+                (VolumetricFemForceMaterialResponsePyTetP1,), {"material": material})
+
+
 _PY_ENERGY_BASES = {(TetP1Basis, TetCentroidQuadrature): VolumetricFemEnergyPyMaterialTetP1,
                     (HexQ1Basis, GaussLegendre3D_2): VolumetricFemEnergyPyMaterialHexQ1,
                     (HexQ1Basis, GaussLegendre3D_4): VolumetricFemEnergyPyMaterialHexQ1GL4}
@@ -1273,6 +1348,7 @@ VolumetricFemForceMaterialResponse = Template(
      (NeoHookean, HexQ1Basis, GaussLegendre3D_4): VolumetricFemForceMaterialResponseHexQ1GL4,
      (NeoHookean, HexHermiteBasis, GaussLegendre3D_2): VolumetricFemForceMaterialResponseHexHermite,
      (NeoHookean, HexHermiteBasis, GaussLegendre3D_4): VolumetricFemForceMaterialResponseHexHermiteGL4})
+VolumetricFemForceMaterialResponse.material_factory = _py_response_class
 VolumetricFemForceFpResponse = Template(
     "VolumetricFemForceFpResponse",
     {(NeoHookean, TetP1Basis, TetCentroidQuadrature): VolumetricFemForceFpResponseTetP1})

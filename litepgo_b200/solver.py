@@ -393,11 +393,34 @@ class StaticEquilibriumResponse:
         force = self.make_response(x)
         if force is None or force.num_inputs != self.num_inputs or force.num_outputs != self.num_outputs:
             raise ValueError("StaticEquilibriumResponse: incompatible force response")
-        fem, w, A, _, _ = _split_energy(potential)
-        if w != 1.0 or A is not None:
-            raise ValueError("StaticEquilibriumResponse: the adjoint needs the elastic term plus linear loads")
+        fem, wf, A, _, c = _split_energy(potential)
         fixed_arr = np.ascontiguousarray(self.fixed.fixed_dofs, dtype=np.int32)
         prec = N.PRECISION_F64 if self.precision == "f64" else N.PRECISION_MIXED
+        from .fem import VolumetricFemEnergyPyMaterialTetP1, VolumetricFemForceMaterialResponsePyTetP1
+
+        if (wf != 1.0 or A is not None or isinstance(fem, VolumetricFemEnergyPyMaterialTetP1)
+                or isinstance(force, VolumetricFemForceMaterialResponsePyTetP1)):
+            # The general form (static_equilibrium_response.cpp:43-88): lambda from the potential's
+            # Exact Hessian at x (a Python material evaluated through its callback), then
+            # -(dg/dp)^T lambda from the caller's force response.
+            terms, keep, box = _terms(wf, A, c, None, fem)
+            if terms is not None and terms.material:
+                import torch
+
+                N.check(N.lib.lpg_fem_set_stream(fem.handle,
+                                                 ctypes.c_void_p(torch.cuda.current_stream(fem.device).cuda_stream)))
+            else:
+                N.check(N.lib.lpg_fem_set_stream(fem.handle, None))
+            lam = np.empty(self.num_outputs)
+            code = N.lib.lpg_adjoint_solve_terms(fem.handle, ctypes.byref(terms) if terms is not None else None,
+                                                 N.vptr(np.ascontiguousarray(x)), N.vptr(w), N.iptr(fixed_arr),
+                                                 int(fixed_arr.size), N.MEM_HOST, prec, float(self.adjoint_tolerance),
+                                                 N.vptr(lam))
+            if code == N.LPG_ESTOPPED and box:
+                raise box[0]
+            N.check(code)
+            del keep
+            return -np.asarray(force.eval_vjp(p, lam), dtype=np.float64)
         from .fem import VolumetricFemForceFpResponseTetP1, VolumetricFemForceRestPositionResponseTetP1
 
         if isinstance(force, VolumetricFemForceFpResponseTetP1):

@@ -28,8 +28,8 @@ class TorchVolumetricMaterial(PyVolumetricMaterial):
     Subclass it, set ``num_parameters`` and define ``W(F, Fp, theta)`` as a static or class
     method taking float64 tensors (N,3,3), (N,3,3), (N,k) and returning the (N,) density per
     reference volume; rows must be independent and W twice differentiable in F. ``eval`` takes
-    dW/dF by one backward pass and d2W/dF2 by nine more ([n,i,j,k,l] = d2W/dF_ij dF_kl), on the
-    device of F.
+    dW/dF by one backward pass, d2W/dF2 by nine more ([n,i,j,k,l] = d2W/dF_ij dF_kl) and
+    d2W/dF dtheta by nine more ([n,i,j,a]), on the device of F.
     """
 
     @classmethod
@@ -39,11 +39,13 @@ class TorchVolumetricMaterial(PyVolumetricMaterial):
     @classmethod
     def eval(cls, F, Fp, theta, *, outputs):
         need2 = "d2W_dF2" in outputs
-        need1 = need2 or "dW_dF" in outputs
+        need_th = "d2W_dF_dtheta" in outputs
+        need1 = need2 or need_th or "dW_dF" in outputs
         n = F.shape[0]
         with torch.enable_grad():
             Fv = F.detach().clone().requires_grad_(need1)
-            W = cls.W(Fv, Fp.detach(), theta.detach())
+            th = theta.detach().clone().requires_grad_(need_th)
+            W = cls.W(Fv, Fp.detach(), th)
             if tuple(W.shape) != (n,):
                 raise ValueError(f"TorchVolumetricMaterial.W must return shape ({n},)")
             out = {"W": W.detach()}
@@ -51,9 +53,20 @@ class TorchVolumetricMaterial(PyVolumetricMaterial):
                 if not W.requires_grad:
                     dW = torch.zeros_like(Fv)
                 else:
-                    (dW,) = torch.autograd.grad(W.sum(), Fv, create_graph=need2, allow_unused=True)
+                    (dW,) = torch.autograd.grad(W.sum(), Fv, create_graph=need2 or need_th, allow_unused=True)
                     dW = torch.zeros_like(Fv) if dW is None else dW
                 out["dW_dF"] = dW.detach()
+                if need_th:
+                    # [n, i, j, a] = d2W / dF_ij dtheta_a: one backward pass per entry of F.
+                    k = th.shape[1]
+                    cols = []
+                    for i in range(3):
+                        for j in range(3):
+                            g = None
+                            if dW.requires_grad:
+                                (g,) = torch.autograd.grad(dW[:, i, j].sum(), th, retain_graph=True, allow_unused=True)
+                            cols.append(torch.zeros((n, k), dtype=F.dtype, device=F.device) if g is None else g)
+                    out["d2W_dF_dtheta"] = torch.stack(cols, 1).reshape(n, 3, 3, k).detach()
                 if need2:
                     rows = []
                     for i in range(3):

@@ -268,3 +268,48 @@ def test_newton_over_a_torch_material_matches_the_native_solve():
     bad = build(Broken, {"X": g["X"], "tets": g["tets"], "theta": g["theta"]})
     with pytest.raises(RuntimeError, match="material failed"):
         solver.newton_solve(bad, fixed, np.zeros(n), opts)
+
+
+def test_static_equilibrium_response_over_a_torch_material():
+    """The reference's neural equilibrium fit pattern (examples/fem/fitting/neural_equilibrium_fit.py):
+    StaticEquilibriumResponse over a TorchVolumetricMaterial energy with
+    VolumetricFemForceMaterialResponse[material, ...]. Its value and VJP equal those of the native
+    neo-Hookean response with the same theta (the adjoint through the material's Exact Hessian and
+    d2W/dF dtheta against lpg_adjoint_theta), and the VJP matches central differences."""
+    import scipy.sparse as sp
+
+    from litepgo_b200 import solver
+
+    g = workloads.gravity_box(2, seed=0)
+    X, tets, f = g["X"], g["tets"], g["f"]
+    n, T = X.size, tets.shape[0]
+    topo = mesh.TetTopology(X.shape[0], tets)
+    dmap = dof.VertexDofMap(topo, 3)
+    pmap = dof.ConstantDofMap(topo, 2)
+    load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -50.0 * f)
+    fixed = dof.DofReduction(n, g["fixed"])
+    opts = solver.NewtonOptions(gradient_tolerance=1e-12, stop_rule="relative", max_iterations=100, cg_tolerance=1e-6)
+
+    def make(material):
+        key = (material, fem.TetP1Basis, fem.TetCentroidQuadrature)
+
+        def make_energy(p):
+            return energy.WeightedSumEnergy([(fem.VolumetricFemEnergy[key](dmap, X, None, np.asarray(p)), 1.0),
+                                             (load, 1.0)])
+
+        def make_response(u):
+            return fem.VolumetricFemForceMaterialResponse[key](pmap, dmap, X, u, None)
+
+        return solver.StaticEquilibriumResponse(2, fixed, np.zeros(n), opts, make_energy, make_response)
+
+    p0 = np.array([1.4e5, 3.4e4])
+    torch_model, native_model = make(TorchNeoHookean), make(fem.NeoHookean)
+    xt, xn = torch_model.eval_value(p0), native_model.eval_value(p0)
+    assert rel_err(xt, xn) <= 1e-9
+    w = np.random.default_rng(3).standard_normal(n)
+    vt, vn = torch_model.eval_vjp(p0, w), native_model.eval_vjp(p0, w)
+    assert rel_err(vt, vn) <= 1e-8
+    d = np.array([0.3, -0.7]) * p0
+    h = 1e-4
+    fd = (w @ torch_model.eval_value(p0 + h * d) - w @ torch_model.eval_value(p0 - h * d)) / (2 * h)
+    assert abs(vt @ d - fd) <= 1e-5 * abs(fd)
