@@ -153,7 +153,7 @@ class ClockSampler:
 
 def profile_traffic():
     """Per-launch DRAM bytes of the assembly kernel from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "cluster_kernel_f64_exact_64cube.md"
+    p = ROOT / "profiles" / "tet_cluster_kernel_f64_exact_64cube.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -395,7 +395,7 @@ def run_ours(args):
     ms = max_over_ranks(ms, world)
     ms_per_step = ms / args.steps
     value = whole_job_rate(T * args.steps, ms * 1e-3, world)
-    gpu_launches = 2 * args.steps  # assembly kernel + energy reduction per step
+    gpu_launches = 3 * args.steps  # per step: the assembly kernel and the two-stage energy sum
 
     # Roofline of the assembly kernel: CUDA events on its launching stream, L2 flushed between launches.
     ma, me = ctypes.c_double(), ctypes.c_double()
@@ -407,7 +407,7 @@ def run_ours(args):
     achieved = ab / (ma.value * 1e-3) / 1e9
     traffic = profile_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "cluster_kernel<double, gradient, exact Hessian>", "kernel_ms": ma.value,
+                "traffic": traffic, "kernel": "tet_cluster_kernel<double, gradient, exact Hessian>", "kernel_ms": ma.value,
                 "algorithmic_bytes": ab, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
     # Mixed (FP32 element arithmetic + FP32 Hessian) kernel, reported beside it.
     hess32 = torch.empty(e.nnz, dtype=torch.float32, device=dev)
@@ -458,7 +458,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded structured five-tet box)",
-            "config": dict(workload_config(), parallelism=f"replicas x{world}"),
+            "config": workload_config(),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
             "clocks": clocks.summary(), "mixed_precision_kernel": mixed, "newton_time_to_1e-8": newton,
             "autotune": tuning_summary(e),
