@@ -1096,54 +1096,20 @@ template <typename Kern> int resident_grid(Kern kernel, int threads, size_t smem
 }
 
 // ---------------------------------------------------------------------------
-// Element-once assembly over vertex clusters (Exact Hessian, gradient, energy).
-//
-// One thread block per cluster of owned rows. Phase 1 evaluates every element incident to
-// the cluster once (one thread per element) and keeps, per element, h_a = F^-T grad N_a,
-// the gradient pieces g_a = vol P grad N_a, vol lambda, vol p and vol mu (grad N_a . grad N_b)
-// in shared memory. Phase 2 gives each block slot of the cluster's rows to one thread, which
-// sums the slot's contributions in ascending element order in registers and stores the
-// block once: no atomics, and an off-diagonal slot is evaluated in the orientation of its
-// lower-numbered vertex so that the two blocks of an edge are exact transposes.
+// Block slots of the cluster plan (HostPlan::cl_*), used by the block gather below.
 // ---------------------------------------------------------------------------
 #ifndef LPG_CLUSTER_THREADS
 #define LPG_CLUSTER_THREADS 128
 #endif
-#ifndef LPG_CLUSTER_MIN_BLOCKS_F64
-#define LPG_CLUSTER_MIN_BLOCKS_F64 3
-#endif
-#ifndef LPG_CLUSTER_MIN_BLOCKS_F32
-#define LPG_CLUSTER_MIN_BLOCKS_F32 6
-#endif
-#ifndef LPG_CLUSTER_UNROLL
-#define LPG_CLUSTER_UNROLL 4
-#endif
 constexpr int kClThreads = LPG_CLUSTER_THREADS;
-constexpr int kClUnroll = LPG_CLUSTER_UNROLL;
-// Register-budget variants of the Hessian-writing cluster kernel (resident blocks per SM the
-// allocation must allow), chosen per handle by the autotuner; variant 0 is the default. The
-// variants differ in register allocation only, so their results are bitwise identical.
-template <typename R> constexpr int cl_minb(int v) {
-    return sizeof(R) == 8 ? (v == 0 ? LPG_CLUSTER_MIN_BLOCKS_F64 : v == 1 ? 2 : 4)
-                          : (v == 0 ? LPG_CLUSTER_MIN_BLOCKS_F32 : v == 1 ? 4 : 8);
-}
 
-
-// Shared memory of the cluster kernel: energy partials, per-element data, the row table, and
-// the cluster's slot words and contributor lists (sized by the mesh's largest cluster).
-template <typename R, bool WG, bool WH> constexpr size_t cl_smem_fixed() {
-    return 32 * sizeof(double) + sizeof(R) * static_cast<size_t>(kClusterElems) * ((WH ? 24 : 0) + (WG ? 12 : 0)) +
-           5 * kClusterRows * sizeof(int);
-}
 // Fixed shared memory of the block gather: element ids and a 4-column row table.
 constexpr size_t block_gather_fixed() {
     return (static_cast<size_t>(kClusterElems) + 4 * kClusterRows) * sizeof(int);
 }
-template <typename R, bool WG, bool WH> size_t cl_smem_bytes(const DevMesh& m) {
-    const size_t slots = (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16;
-    return cl_smem_fixed<R, WG, WH>() + slots + 2 * static_cast<size_t>(m.cl_max_ents);
-}
 
+// Position of entry t of block q of a row (first block slot0, nb blocks, solver base sb) in the
+// output layout.
 __device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, int q, int t) {
     if (layout == LPG_LAYOUT_BSR) return 9 * static_cast<size_t>(slot0 + q) + t;
     if (layout == LPG_LAYOUT_CSC) {
@@ -1151,234 +1117,6 @@ __device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, 
         return 9 * static_cast<size_t>(slot0) + static_cast<size_t>(i) * 3 * nb + 3 * q + c;
     }
     return static_cast<size_t>(static_cast<int64_t>(sb) + 32 * static_cast<int64_t>(9 * q + t));
-}
-
-template <typename R, bool WG, bool WH, int MINB>
-__global__ void __launch_bounds__(kClThreads, MINB) cluster_kernel(const DevMesh m, const EvalArgs a) {
-    using X = M<R>;
-    using HT = typename HOut<R>::T;
-    constexpr int E = kClusterElems;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* red = reinterpret_cast<double*>(smem_raw);
-    R* sh = reinterpret_cast<R*>(smem_raw + 32 * sizeof(double));
-    R* hv = sh;                        // [12][E] h_a components (WH)
-    R* cc = sh + 12 * E;               // [10][E] vol mu grad N_a . grad N_b (WH)
-    R* lp = sh + 22 * E;               // [2][E] vol lambda, vol p (WH)
-    R* gv = sh + (WH ? 24 * E : 0);    // [12][E] g_a components (WG)
-    int* rt = reinterpret_cast<int*>(sh + static_cast<size_t>(E) * ((WH ? 24 : 0) + (WG ? 12 : 0)));
-    uint32_t* sslot = reinterpret_cast<uint32_t*>(smem_raw + cl_smem_fixed<R, WG, WH>());
-    uint32_t* sslote = sslot + m.cl_max_slots;
-    uint16_t* sent = reinterpret_cast<uint16_t*>(smem_raw + cl_smem_fixed<R, WG, WH>() +
-                                                 (8 * static_cast<size_t>(m.cl_max_slots) + 15) / 16 * 16);
-    const int tid = threadIdx.x, bd = blockDim.x;
-    unsigned st = 0;
-    // The first element of each thread is fetched one cluster ahead.
-    uint32_t pf_ew = 0;
-    int4 pf_tv = make_int4(0, 0, 0, 0);
-    auto prefetch = [&](int cl) {
-        if (cl < m.ncl) {
-            const int e0 = __ldg(m.cl_el_ptr + cl);
-            if (tid < __ldg(m.cl_el_ptr + cl + 1) - e0) {
-                pf_ew = __ldg(m.cl_els + e0 + tid);
-                pf_tv = __ldg(m.tets + (pf_ew & 0x7fffffffu));
-            }
-        }
-    };
-    prefetch(blockIdx.x);
-    for (int cl = blockIdx.x; cl < m.ncl; cl += gridDim.x) {
-        // Stage the cluster's slot words and contributor lists (asynchronous copies).
-        const int s0 = __ldg(m.cl_slot_ptr + cl), ns = __ldg(m.cl_slot_ptr + cl + 1) - s0;
-        if (WG || WH) {
-            const int eb = __ldg(m.cl_ent_ptr + cl), n16 = (__ldg(m.cl_ent_ptr + cl + 1) - eb) / 8;
-            for (int i = tid; i < ns; i += bd) {
-                __pipeline_memcpy_async(sslot + i, m.cl_slot + s0 + i, 4);
-                __pipeline_memcpy_async(sslote + i, m.cl_slot_ent + s0 + i, 4);
-            }
-            for (int i = tid; i < n16; i += bd)
-                __pipeline_memcpy_async(reinterpret_cast<uint4*>(sent) + i, reinterpret_cast<const uint4*>(m.cl_ents + eb) + i, 16);
-            __pipeline_commit();
-        }
-        // Phase 1: the cluster's elements, once each.
-        const int e0 = __ldg(m.cl_el_ptr + cl), ne = __ldg(m.cl_el_ptr + cl + 1) - e0;
-        double eacc = 0;
-        for (int el = tid; el < ne; el += bd) {
-            const uint32_t ew = el == tid ? pf_ew : __ldg(m.cl_els + e0 + el);
-            const int e = static_cast<int>(ew & 0x7fffffffu);
-            const int4 tv = el == tid ? pf_tv : __ldg(m.tets + e);
-            Kin<R> k;
-            st |= kinematics<R>(m, e, tv, a.u, k);
-            if (ew >> 31) {
-                const R Ee = k.vol * k.psi;
-                eacc += static_cast<double>(Ee);
-                if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
-            }
-            const R p = X::fma(k.lam, k.logJ, -k.mu);
-            if (WG) {
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        R s = 0;
-#pragma unroll
-                        for (int j = 0; j < 3; ++j)
-                            s = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[b][j], s);
-                        gv[(3 * b + i) * E + el] = k.vol * s;
-                    }
-            }
-            if (WH) {
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        hv[(3 * b + i) * E + el] =
-                            X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
-                lp[el] = X::mul(k.vol, k.lam);
-                lp[E + el] = X::mul(k.vol, p);
-                const R mv = X::mul(k.vol, k.mu);
-#pragma unroll
-                for (int x = 0; x < 4; ++x)
-#pragma unroll
-                    for (int y = x; y < 4; ++y)
-                        cc[pair10(x, y) * E + el] =
-                            X::mul(mv, X::fma(k.n[x][2], k.n[y][2], X::fma(k.n[x][1], k.n[y][1], X::mul(k.n[x][0], k.n[y][0]))));
-            }
-        }
-        // Energy of the cluster's own elements: fixed thread order, fixed tree.
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, off);
-        if ((tid & 31) == 0) red[tid >> 5] = eacc;
-        // Row table: vertex, first block, block count, and the row's sliced-ELL base (solver layout).
-        const int r0 = __ldg(m.cl_row_ptr + cl), nr = __ldg(m.cl_row_ptr + cl + 1) - r0;
-        for (int j = tid; j < nr; j += bd) {
-            const int v = __ldg(m.cl_rows + r0 + j);
-            const int sb = __ldg(m.row_ptr + v);
-            rt[j] = v;
-            rt[kClusterRows + j] = sb;
-            rt[2 * kClusterRows + j] = __ldg(m.row_ptr + v + 1) - sb;
-            // Solver layout: own block q - (diagonal position) of the row, so the base is shifted.
-            if (a.layout == kLayoutSell) rt[3 * kClusterRows + j] = __ldg(m.sell_base + v) - 288 * (__ldg(m.diag_slot + v) - sb);
-        }
-        prefetch(cl + gridDim.x);
-        if (WG || WH) __pipeline_wait_prior(0);
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0;
-            for (int w = 0; w < (bd >> 5); ++w) t += red[w];
-            a.cluster_energy[cl] = t;
-            if (!isfinite(t)) st |= ST_NONFINITE_OUT;
-        }
-        // Phase 2: one thread per block slot (off-diagonal slots first, then diagonal slots,
-        // so that warps mostly hold slots of one kind).
-        if (WG || WH) {
-            const int noff = __ldg(m.cl_noff + cl);
-            HT* hout = reinterpret_cast<HT*>(a.hess);
-            // The solver layout skips the slots left of the diagonal (the transposes it does not store).
-            const int first = WH ? (a.layout == kLayoutSell ? __ldg(m.cl_ntr + cl) : 0) : noff;
-            for (int s = first + tid; s < ns; s += bd) {
-                const uint32_t d = sslot[s], de = sslote[s];
-                const int j = d & 0xffu, q = (d >> 8) & 0x3fffffu;
-                const uint16_t* en = sent + (de & 0xfffffu);
-                const int cnt = static_cast<int>(de >> 20);
-                const int slot0 = rt[kClusterRows + j], nb = rt[2 * kClusterRows + j];
-                const int sb = rt[3 * kClusterRows + j];
-                if (d >> 31) {
-                    // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient.
-                    R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
-#pragma unroll kClUnroll
-                    for (int c = 0; c < cnt; ++c) {
-                        const int w = en[c];
-                        const int el = w >> 4, la = (w >> 2) & 3;
-                        if (WG) {
-#pragma unroll
-                            for (int i = 0; i < 3; ++i) gs[i] = X::add(gs[i], gv[(3 * la + i) * E + el]);
-                        }
-                        if (WH) {
-                            // H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
-                            const R hh[3] = {hv[(3 * la) * E + el], hv[(3 * la + 1) * E + el], hv[(3 * la + 2) * E + el]};
-                            const R dv = X::add(lp[el], -lp[E + el]), mg = cc[pair10(la, la) * E + el];
-                            int u = 0;
-#pragma unroll
-                            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                                for (int kk = i; kk < 3; ++kk, ++u) {
-                                    acc[u] = X::fma(dv, X::mul(hh[i], hh[kk]), acc[u]);
-                                    if (i == kk) acc[u] = X::add(acc[u], mg);
-                                }
-                        }
-                    }
-                    const int v = rt[j];
-                    if (WG) {
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            if (!X::finite(gs[i])) st |= ST_NONFINITE_OUT;
-                            a.grad[3 * static_cast<size_t>(v) + i] = static_cast<double>(gs[i]);
-                        }
-                    }
-                    if (WH) {
-                        constexpr int sym3[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-#pragma unroll
-                        for (int t = 0; t < 9; ++t) {
-                            const R val = acc[sym3[t]];
-                            if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                            hout[cl_pos(a.layout, slot0, nb, sb, q, t)] = static_cast<HT>(val);
-                        }
-                    }
-                } else if (WH) {
-                    // Off-diagonal block in the orientation of the lower vertex (a) -> higher (b):
-                    //   C += vol lambda h_a h_b^T - vol p h_b h_a^T + vol mu (grad N_a . grad N_b) I.
-                    R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll kClUnroll
-                    for (int c = 0; c < cnt; ++c) {
-                        const int w = en[c];
-                        const int el = w >> 4, ra = (w >> 2) & 3, cb = w & 3;
-                        R ha[3], hb[3];
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            ha[i] = hv[(3 * ra + i) * E + el];
-                            hb[i] = hv[(3 * cb + i) * E + el];
-                        }
-                        const R lv = lp[el], pv = lp[E + el], mg = cc[pair10(ra, cb) * E + el];
-                        R A[3], B[3];
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            A[i] = X::mul(lv, ha[i]);
-                            B[i] = X::mul(-pv, ha[i]);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 3; ++i)
-#pragma unroll
-                            for (int kk = 0; kk < 3; ++kk) {
-                                acc[3 * i + kk] = X::fma(B[kk], hb[i], X::fma(A[i], hb[kk], acc[3 * i + kk]));
-                                if (i == kk) acc[3 * i + kk] = X::add(acc[3 * i + kk], mg);
-                            }
-                    }
-                    const bool tr = (d >> 30) & 1u;
-#pragma unroll
-                    for (int t = 0; t < 9; ++t) {
-                        const int i = t / 3, kk = t - 3 * (t / 3);
-                        const R val = tr ? acc[3 * kk + i] : acc[t];
-                        if (!X::finite(val)) st |= ST_NONFINITE_OUT;
-                        hout[cl_pos(a.layout, slot0, nb, sb, q, t)] = static_cast<HT>(val);
-                    }
-                }
-            }
-        }
-        __syncthreads(); // the next cluster reuses the shared element data
-    }
-    st = __reduce_or_sync(0xffffffffu, st);
-    if ((tid & 31) == 0 && st) atomicOr(a.status, st);
-}
-
-template <typename R, bool WG, bool WH, int MINB = cl_minb<R>(0)>
-void launch_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
-    const size_t sm = cl_smem_bytes<R, WG, WH>(m);
-    thread_local LaunchCache cache;
-    const int resident = resident_grid(cluster_kernel<R, WG, WH, MINB>, kClThreads, sm, cache);
-    const int blocks = std::min(resident, m.ncl);
-    if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-    if (blocks > 0) cluster_kernel<R, WG, WH, MINB><<<blocks, kClThreads, sm, s>>>(m, a);
-    if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
-    LPG_CUDA(cudaGetLastError());
 }
 
 

@@ -69,7 +69,7 @@ struct HostPlan {
     std::vector<uint32_t> cl_slot, cl_slot_ent;
     std::vector<int32_t> cl_ent_ptr;
     std::vector<uint16_t> cl_ents;
-    // Tet assembly clusters (cluster_kernel of tet meshes; empty for other cells). A cluster owns
+    // Tet assembly clusters (tet_cluster_kernel; empty for other cells). A cluster owns
     // up to kTcRows rows; its elements (those incident to the rows, ascending, at most kTcElems;
     // bit 31 on the ones whose energy it counts: those whose first vertex it owns) touch at most
     // kTcVerts vertices (tc_verts, ascending); tc_loc packs each element's four local vertex
