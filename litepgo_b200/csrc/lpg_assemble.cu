@@ -1143,9 +1143,14 @@ constexpr int kTcThreads = LPG_TC_THREADS;
 // Per-element data in shared memory, one component per kTcElems-long array: h_a (3 a + i),
 // vol mu grad N_a . grad N_b (pair order), vol lambda, vol p, g_a (3 a + i).
 constexpr int kTcH = 0, kTcCC = 12, kTcL = 22, kTcP = 23, kTcG = 24, kTcComp = 36;
+// Launch variants of the Exact-Hessian kernel (autotuner): threads per block and the resident
+// blocks per SM the register allocation must allow. FP64 variant 2 runs 128 threads (two elements
+// per thread in the element pass); the arithmetic is the same, so every variant's results are
+// bitwise identical.
 template <typename R> constexpr int tc_minb(int v) {
-    return sizeof(R) == 8 ? (v == 0 ? 2 : v == 1 ? 1 : 2) : (v == 0 ? 3 : v == 1 ? 2 : 4);
+    return sizeof(R) == 8 ? (v == 0 ? 2 : v == 1 ? 1 : 4) : (v == 0 ? 3 : v == 1 ? 2 : 4);
 }
+template <typename R> constexpr int tc_threads(int v) { return sizeof(R) == 8 && v == 2 ? 128 : kTcThreads; }
 template <typename R> constexpr size_t tc_records_bytes() { return static_cast<size_t>(kTcElems) * 12 * sizeof(R); }
 template <typename R> constexpr size_t tc_region_bytes() {
     return tc_records_bytes<R>() + static_cast<size_t>(kTcVerts) * 3 * sizeof(double) >
@@ -1166,8 +1171,8 @@ __device__ __forceinline__ int tc_stage(uint32_t pos, bool csc, int i, int c) {
     return csc ? so + 3 * nb * i + 3 * q + c : so + 9 * q + 3 * i + c;
 }
 
-template <typename R, bool WG, bool WH, int MINB>
-__global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const DevMesh m, const EvalArgs a) {
+template <typename R, bool WG, bool WH, int MINB, int THREADS = kTcThreads>
+__global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMesh m, const EvalArgs a) {
     using X = M<R>;
     using HT = typename HOut<R>::T;
     constexpr int E = kTcElems;
@@ -1391,14 +1396,14 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     if (lane == 0 && st) atomicOr(a.status, st);
 }
 
-template <typename R, bool WG, bool WH, int MINB = tc_minb<R>(0)>
+template <typename R, bool WG, bool WH, int MINB = tc_minb<R>(0), int THREADS = kTcThreads>
 void launch_tet_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = tc_smem_bytes<R>();
     thread_local LaunchCache cache;
-    const int resident = resident_grid(tet_cluster_kernel<R, WG, WH, MINB>, kTcThreads, sm, cache);
+    const int resident = resident_grid(tet_cluster_kernel<R, WG, WH, MINB, THREADS>, THREADS, sm, cache);
     const int blocks = std::min(resident, m.tc_ncl);
     if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-    if (blocks > 0) tet_cluster_kernel<R, WG, WH, MINB><<<blocks, kTcThreads, sm, s>>>(m, a);
+    if (blocks > 0) tet_cluster_kernel<R, WG, WH, MINB, THREADS><<<blocks, THREADS, sm, s>>>(m, a);
     if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
     LPG_CUDA(cudaGetLastError());
 }
@@ -2910,7 +2915,7 @@ __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __re
 template <typename R, bool WG> void launch_tet_variant(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     switch (a.cl_variant) {
     case 1: launch_tet_cluster<R, WG, true, tc_minb<R>(1)>(m, a, s); break;
-    case 2: launch_tet_cluster<R, WG, true, tc_minb<R>(2)>(m, a, s); break;
+    case 2: launch_tet_cluster<R, WG, true, tc_minb<R>(2), tc_threads<R>(2)>(m, a, s); break;
     default: launch_tet_cluster<R, WG, true>(m, a, s); break;
     }
 }
