@@ -2714,6 +2714,9 @@ __global__ void __launch_bounds__(kHermPsdThreads) hermite_psd_kernel(int T, dou
                 }
                 __syncthreads();
                 const int m = s_hi, cnt = s_count;
+                // Every thread holds the sweep's bounds before thread 0 may write the next ones
+                // (after a converged l it goes straight on to l + 1).
+                __syncthreads();
                 if (m == l) break;
                 // Apply rotations i = m-1 .. m-cnt to row r of Q: columns i and i+1.
                 for (int r = tid; r < n; r += bd) {

@@ -7,7 +7,10 @@ may import it. The product package (litepgo_b200) never does.
 """
 
 from .oracle import (  # noqa: F401
+    DOMAIN_ERROR,
     HEX_CORNERS,
+    INVALID_ARGUMENT,
+    LOGIC_ERROR,
     OracleError,
     hex_box,
     hex_dN_dxi,

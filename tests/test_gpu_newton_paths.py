@@ -104,7 +104,10 @@ def test_indefinite_exact_hessian_shift_loop_matches_the_oracle_pcg():
     assert infod["trace"][0]["diagonal_shifts"] > 0  # the direct solve needs the shifts here
     assert r.status == solver.NewtonStatus.Converged and info["status"] == 0
     assert steps[0].diagonal_shifts == int(info["trace"][0]["diagonal_shifts"])
-    assert rel_err(r.x, xo) <= 1e-6 and rel_err(r.x, xd) <= 1e-6
+    assert rel_err(r.x, xo) <= 1e-6
+    # The direct solve's shifted first steps (9, 9, 8, 7 shifts) lead this non-convex energy to
+    # another equilibrium, of higher energy (-14.89 against -17.37).
+    assert infod["status"] == 0 and infod["energy"] > r.energy + 1.0
 
 
 def test_free_vertex_in_no_element_is_a_zero_pivot():
