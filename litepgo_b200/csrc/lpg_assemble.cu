@@ -110,17 +110,41 @@ __device__ __forceinline__ unsigned kinematics(const DevMesh& m, int e, const in
     return kinematics_of<R>(m, e, rec, uu, k);
 }
 
-// The element's kinematics from its record (rec) and its vertices' displacements (uu).
-template <typename R>
-__device__ __forceinline__ unsigned kinematics_of(const DevMesh& m, int e, const R (&rec)[12], const double (&uu)[4][3],
-                                                  Kin<R>& k) {
-    using X = M<R>;
-    unsigned st = 0;
-    R Ds[3][3]; // Ds[i][c] = u_{c+1,i} - u_{0,i}
+// Edge differences of the displacements, formed in FP64 and rounded once: Ds[i][c] =
+// u_{c+1,i} - u_{0,i}; returns whether every displacement is finite.
+template <typename R> __device__ __forceinline__ bool edge_differences(const double (&uu)[4][3], R (&Ds)[3][3]) {
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int i = 0; i < 3; ++i) Ds[i][c] = static_cast<R>(uu[c + 1][i] - uu[0][i]);
+    bool in_ok = true;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) in_ok = in_ok && isfinite(uu[c][i]);
+    return in_ok;
+}
+
+template <typename R>
+__device__ __forceinline__ unsigned kinematics_ds(const DevMesh& m, int e, const R (&rec)[12], const R (&Ds)[3][3],
+                                                  bool in_ok, Kin<R>& k);
+
+// The element's kinematics from its record (rec) and its vertices' displacements (uu).
+template <typename R>
+__device__ __forceinline__ unsigned kinematics_of(const DevMesh& m, int e, const R (&rec)[12], const double (&uu)[4][3],
+                                                  Kin<R>& k) {
+    R Ds[3][3];
+    const bool in_ok = edge_differences<R>(uu, Ds);
+    return kinematics_ds<R>(m, e, rec, Ds, in_ok, k);
+}
+
+// The element's kinematics from its record and its displacement edge differences (in_ok: every
+// displacement was finite).
+template <typename R>
+__device__ __forceinline__ unsigned kinematics_ds(const DevMesh& m, int e, const R (&rec)[12], const R (&Ds)[3][3],
+                                                  bool in_ok, Kin<R>& k) {
+    using X = M<R>;
+    unsigned st = 0;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -186,11 +210,7 @@ __device__ __forceinline__ unsigned kinematics_of(const DevMesh& m, int e, const
     for (int t = 0; t < 9; ++t) k.FiT[t] = C[t] * iJ;
     k.psi = R(0.5) * k.mu * sqm3 - k.mu * k.logJ + R(0.5) * k.lam * k.logJ * k.logJ;
     if (!(J > R(0) && J < R(INFINITY) && k.psi == k.psi && k.psi < R(INFINITY) && k.psi > R(-INFINITY))) {
-        bool in_ok = true, f_ok = true;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) in_ok = in_ok && isfinite(uu[c][i]);
+        bool f_ok = true;
 #pragma unroll
         for (int t = 0; t < 9; ++t) f_ok = f_ok && X::finite(F[t]);
         st |= !in_ok ? ST_BAD_INPUT : !f_ok ? ST_NONFINITE_F : !(J > R(0)) || !X::finite(J) ? ST_BAD_DET
@@ -1123,43 +1143,50 @@ __device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, 
 // ---------------------------------------------------------------------------
 // Tet assembly over the tet clusters (E, gradient and Exact Hessian in the BSR, CSC or solver
 // layout). One thread block per cluster (persistent over clusters), four passes:
-//   stage:   the cluster's vertex displacements and element records are copied into shared
-//            memory by consecutive threads (runs of consecutive ids read coalesced);
+//   stage:   each thread loads one element's record into registers and copies one vertex's
+//            displacement into shared memory; the cluster's item table and contributor lists
+//            are copied into shared memory with cp.async, and the owned rows' offsets are
+//            loaded into registers;
 //   element: one thread per element evaluates it once (kinematics as the reference computes
 //            it) and keeps h_a = F^-T grad N_a, vol mu grad N_a . grad N_b, vol lambda, vol p
 //            and the gradient pieces g_a = vol P grad N_a in shared memory;
 //   items:   one thread per diagonal block (with the row's gradient) or edge block sums the
 //            block's contributors in ascending element order into registers and writes it into
 //            the cluster's output staging (an edge between two owned rows once, at both
-//            positions; the staging reuses the memory of the staged inputs);
+//            positions);
 //   copy:    one warp per owned row copies the row's staged values to the output: the row's
 //            9 nb values are contiguous in the BSR and CSC layouts, so the stores are
 //            coalesced.
+// The passes are software-pipelined across the block's clusters so that no global read waits
+// inside a pass: the next cluster's bounds are read a cluster ahead, its element, vertex and row
+// indices during this cluster's item pass, and its stage is issued before this cluster's copy
+// pass (whose stores do not wait), so its loads arrive while the copy pass runs.
 // ---------------------------------------------------------------------------
-#ifndef LPG_TC_THREADS
-#define LPG_TC_THREADS 256
-#endif
-constexpr int kTcThreads = LPG_TC_THREADS;
+constexpr int kTcThreads = 256;
+static_assert(kTcThreads >= kTcElems && kTcThreads >= kTcVerts && kTcThreads >= kTcRows,
+              "one element, one vertex and one row per thread in the stage");
 // Per-element data in shared memory, one component per kTcElems-long array: h_a (3 a + i),
 // vol mu grad N_a . grad N_b (pair order), vol lambda, vol p, g_a (3 a + i).
 constexpr int kTcH = 0, kTcCC = 12, kTcL = 22, kTcP = 23, kTcG = 24, kTcComp = 36;
-// Launch variants of the Exact-Hessian kernel (autotuner): threads per block and the resident
-// blocks per SM the register allocation must allow. FP64 variant 2 runs 128 threads (two elements
-// per thread in the element pass); the arithmetic is the same, so every variant's results are
-// bitwise identical.
-template <typename R> constexpr int tc_minb(int v) {
-    return sizeof(R) == 8 ? (v == 0 ? 2 : v == 1 ? 1 : 4) : (v == 0 ? 3 : v == 1 ? 2 : 4);
+// Owned-row words in shared memory: vertex, staging offset, first block, nb | diagonal block
+// index << 8 (solver layout), solver base.
+constexpr int kTcRowInts = 5;
+// Launch variants of the Exact-Hessian kernel (autotuner): the resident blocks per SM the
+// register allocation must allow, and the unroll depth of the contributor loops. The arithmetic
+// and its order are the same, so every variant's results are bitwise identical.
+template <typename R> constexpr int tc_minb(int v) { return (sizeof(R) == 8 ? 2 : 3) - (v == 2 ? 1 : 0); }
+constexpr int tc_unroll(int v) { return v == 0 ? 1 : 4; }
+template <typename R> constexpr size_t tc_ed_bytes() {
+    return static_cast<size_t>(kTcComp) * kTcElems * sizeof(R);
 }
-template <typename R> constexpr int tc_threads(int v) { return sizeof(R) == 8 && v == 2 ? 128 : kTcThreads; }
-template <typename R> constexpr size_t tc_records_bytes() { return static_cast<size_t>(kTcElems) * 12 * sizeof(R); }
-template <typename R> constexpr size_t tc_region_bytes() {
-    return tc_records_bytes<R>() + static_cast<size_t>(kTcVerts) * 3 * sizeof(double) >
-                   static_cast<size_t>(kTcVals) * sizeof(R)
-               ? tc_records_bytes<R>() + static_cast<size_t>(kTcVerts) * 3 * sizeof(double)
-               : static_cast<size_t>(kTcVals) * sizeof(R);
-}
+static_assert(3 * kTcVerts * sizeof(double) <= tc_ed_bytes<float>(), "staged displacements fit the element data");
+// Shared memory: reduction scratch (32 doubles), the element data (whose first 3 kTcVerts
+// doubles hold the staged displacements until the element pass has read them), the output
+// staging, the item table, the contributor lists and two buffers of owned-row words.
 template <typename R> constexpr size_t tc_smem_bytes() {
-    return 32 * sizeof(double) + static_cast<size_t>(kTcComp) * kTcElems * sizeof(R) + tc_region_bytes<R>();
+    return 32 * sizeof(double) + tc_ed_bytes<R>() + static_cast<size_t>(kTcVals) * sizeof(R) +
+           static_cast<size_t>(kTcItems) * sizeof(uint4) + static_cast<size_t>(kTcEnts) * sizeof(uint16_t) +
+           2 * static_cast<size_t>(kTcRows) * kTcRowInts * sizeof(int);
 }
 
 // Staging index of entry (i, c) of the block at packed position pos (row offset so, block q,
@@ -1171,56 +1198,165 @@ __device__ __forceinline__ int tc_stage(uint32_t pos, bool csc, int i, int c) {
     return csc ? so + 3 * nb * i + 3 * q + c : so + 9 * q + 3 * i + c;
 }
 
-template <typename R, bool WG, bool WH, int MINB, int THREADS = kTcThreads>
-__global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMesh m, const EvalArgs a) {
+// Asynchronous global -> shared copies (cp.async; the source is device memory).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Bounds of a tet cluster in the plan's arrays (all zero past the last cluster), field q of
+// TcBounds in the order declared.
+struct TcBounds {
+    int e0 = 0, ne = 0, v0 = 0, nv = 0, i0 = 0, ni = 0, nd = 0, n0 = 0, nn = 0, r0 = 0, nr = 0;
+};
+constexpr int kTcFields = 11;
+__device__ __forceinline__ int tc_field(const DevMesh& m, int cl, int q) {
+    if (cl >= m.tc_ncl) return 0;
+    auto span = [&](const int32_t* ptr, bool count) {
+        const int lo = __ldg(ptr + cl);
+        return count ? __ldg(ptr + cl + 1) - lo : lo;
+    };
+    switch (q) {
+    case 0: case 1: return span(m.tc_el_ptr, q == 1);
+    case 2: case 3: return span(m.tc_vert_ptr, q == 3);
+    case 4: case 5: return span(m.tc_item_ptr, q == 5);
+    case 6: return __ldg(m.tc_ndiag + cl);
+    case 7: case 8: return span(m.tc_ent_ptr, q == 8);
+    case 9: case 10: return span(m.tc_row_ptr, q == 10);
+    default: return 0;
+    }
+}
+__device__ __forceinline__ TcBounds tc_bounds(const int* f) {
+    TcBounds b;
+    b.e0 = f[0], b.ne = f[1], b.v0 = f[2], b.nv = f[3], b.i0 = f[4], b.ni = f[5];
+    b.nd = f[6], b.n0 = f[7], b.nn = f[8], b.r0 = f[9], b.nr = f[10];
+    return b;
+}
+
+// Thread t's indices of a cluster: element t (word and local vertices), vertex t, owned row t.
+struct TcIdx {
+    uint32_t ew = 0, loc = 0;
+    int vert = 0, row = 0, so = 0;
+};
+__device__ __forceinline__ void tc_load_idx(const DevMesh& m, const TcBounds& b, int t, TcIdx& x) {
+    if (t < b.ne) {
+        x.ew = __ldg(m.tc_els + b.e0 + t);
+        x.loc = __ldg(m.tc_loc + b.e0 + t);
+    }
+    if (t < b.nv) x.vert = __ldg(m.tc_verts + b.v0 + t);
+    if (t < b.nr) {
+        x.row = __ldg(m.tc_rows + b.r0 + t);
+        x.so = __ldg(m.tc_row_so + b.r0 + t);
+    }
+}
+
+// Issues thread t's part of a cluster's stage: its element's record into registers, its
+// vertex's displacement and its share of the item table and contributor lists into shared memory
+// (cp.async, one group), and its owned row's words into registers.
+template <typename R, bool ITEMS>
+__device__ __forceinline__ void tc_issue(const DevMesh& m, const double* __restrict__ u, const TcBounds& b,
+                                         const TcIdx& x, int t, bool sell, double* su, uint4* sitems, uint16_t* sents,
+                                         R (&r12)[12], int (&rowv)[kTcRowInts]) {
+    if (t < b.ne) load_rec<R>(rec_ptr<R>(m), static_cast<int>(x.ew & 0x7fffffffu), r12);
+    if (t < b.nv) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) cp_async8(su + 3 * t + i, u + 3 * static_cast<size_t>(x.vert) + i);
+    }
+    if (ITEMS) {
+        for (int k = t; k < b.ni; k += kTcThreads) cp_async16(sitems + k, m.tc_items + b.i0 + k);
+        for (int k = t; k < (b.nn >> 3); k += kTcThreads) cp_async16(sents + 8 * k, m.tc_ents + b.n0 + 8 * k);
+    }
+    cp_async_commit();
+    if (ITEMS && t < b.nr) {
+        const int base = __ldg(m.row_ptr + x.row), nb = __ldg(m.row_ptr + x.row + 1) - base;
+        rowv[0] = x.row;
+        rowv[1] = x.so;
+        rowv[2] = base;
+        rowv[3] = nb;
+        rowv[4] = 0;
+        if (sell) {
+            rowv[3] |= (__ldg(m.diag_slot + x.row) - base) << 8;
+            rowv[4] = __ldg(m.sell_base + x.row);
+        }
+    }
+}
+
+template <typename R, bool WG, bool WH, int MINB, int UNR>
+__global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const DevMesh m, const EvalArgs a) {
     using X = M<R>;
     using HT = typename HOut<R>::T;
     constexpr int E = kTcElems;
-    constexpr int CH = 12 * static_cast<int>(sizeof(R)) / 16; // 16-byte chunks per element record
+    constexpr bool ITEMS = WG || WH;
+    constexpr int nw = kTcThreads / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* red = reinterpret_cast<double*>(smem_raw);
     R* ed = reinterpret_cast<R*>(smem_raw + 32 * sizeof(double));
-    unsigned char* region = smem_raw + 32 * sizeof(double) + static_cast<size_t>(kTcComp) * E * sizeof(R);
-    R* srec = reinterpret_cast<R*>(region);                                        // [ne][12]
-    double* su = reinterpret_cast<double*>(region + tc_records_bytes<R>());       // [nv][3]
-    R* stage = reinterpret_cast<R*>(region);                                       // output staging
-    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
-    const R* rec = rec_ptr<R>(m);
+    double* su = reinterpret_cast<double*>(ed); // [nv][3], until the element pass has read it
+    R* stage = ed + kTcComp * E;
+    uint4* sitems = reinterpret_cast<uint4*>(stage + kTcVals);
+    uint16_t* sents = reinterpret_cast<uint16_t*>(sitems + kTcItems);
+    int* srow = reinterpret_cast<int*>(sents + kTcEnts);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     HT* hout = reinterpret_cast<HT*>(a.hess);
     const bool csc = a.layout == LPG_LAYOUT_CSC, sell = a.layout == kLayoutSell;
+    __shared__ int s_hdr[2][kTcFields]; // bounds of the next cluster, by iteration parity
     unsigned st = 0;
-    for (int cl = blockIdx.x; cl < m.tc_ncl; cl += gridDim.x) {
-        const int e0 = __ldg(m.tc_el_ptr + cl), ne = __ldg(m.tc_el_ptr + cl + 1) - e0;
-        const int v0 = __ldg(m.tc_vert_ptr + cl), nv = __ldg(m.tc_vert_ptr + cl + 1) - v0;
-        // Stage: displacements of the cluster's vertices, then its element records.
-        for (int k = tid; k < 3 * nv; k += bd) {
-            const int j = k / 3;
-            su[k] = __ldg(a.u + 3 * static_cast<size_t>(__ldg(m.tc_verts + v0 + j)) + (k - 3 * j));
-        }
-        for (int k = tid; k < CH * ne; k += bd) {
-            const int j = k / CH;
-            const size_t e = __ldg(m.tc_els + e0 + j) & 0x7fffffffu;
-            reinterpret_cast<uint4*>(srec)[k] = __ldg(reinterpret_cast<const uint4*>(rec) + CH * e + (k - CH * j));
-        }
-        __syncthreads();
-        // Element pass: every element of the cluster once.
-        double eacc = 0;
-        for (int el = tid; el < ne; el += bd) {
-            const uint32_t ew = __ldg(m.tc_els + e0 + el);
-            const int e = static_cast<int>(ew & 0x7fffffffu);
-            const uint32_t loc = __ldg(m.tc_loc + e0 + el);
-            R r12[12];
+    int cl = blockIdx.x;
+    const int grid = static_cast<int>(gridDim.x);
+    // Prologue: the first cluster's stage; threads 0 .. kTcFields - 1 hold one field each of the
+    // bounds one cluster ahead.
+    TcBounds b;
+    {
+        int f[kTcFields];
 #pragma unroll
-            for (int t = 0; t < 12; ++t) r12[t] = srec[12 * el + t];
+        for (int q = 0; q < kTcFields; ++q) f[q] = tc_field(m, cl, q);
+        b = tc_bounds(f);
+    }
+    TcIdx x;
+    tc_load_idx(m, b, tid, x);
+    R r12[12];
+    int rowv[kTcRowInts] = {0, 0, 0, 0, 0};
+    tc_issue<R, ITEMS>(m, a.u, b, x, tid, sell, su, sitems, sents, r12, rowv);
+    int ahead = tid < kTcFields ? tc_field(m, cl + grid, tid) : 0;
+    int ne = b.ne, ni = WH ? b.ni : b.nd, nr = b.nr;
+    for (int buf = 0; cl < m.tc_ncl; cl += grid, buf ^= 1) {
+        int* rows = srow + buf * kTcRows * kTcRowInts;
+        if (ITEMS && tid < nr) {
+#pragma unroll
+            for (int q = 0; q < kTcRowInts; ++q) rows[kTcRowInts * tid + q] = rowv[q];
+        }
+        if (tid < kTcFields) s_hdr[buf][tid] = ahead;
+        cp_async_wait_all();
+        __syncthreads(); // the cluster's stage is complete
+        // Element pass: every element of the cluster once, one per thread.
+        const uint32_t ew = x.ew;
+        R Ds[3][3];
+        bool in_ok = true;
+        if (tid < ne) {
             double uu[4][3];
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                const int lv = static_cast<int>((loc >> (8 * c)) & 0xffu);
+                const int lv = static_cast<int>((x.loc >> (8 * c)) & 0xffu);
 #pragma unroll
                 for (int i = 0; i < 3; ++i) uu[c][i] = su[3 * lv + i];
             }
+            in_ok = edge_differences<R>(uu, Ds);
+        }
+        __syncthreads(); // the displacements are read; their memory holds element data from here
+        double eacc = 0;
+        if (tid < ne) {
+            const int el = tid;
+            const int e = static_cast<int>(ew & 0x7fffffffu);
             Kin<R> k;
-            st |= kinematics_of<R>(m, e, r12, uu, k);
+            st |= kinematics_ds<R>(m, e, r12, Ds, in_ok, k);
             if (ew >> 31) {
                 const R Ee = k.vol * k.psi;
                 eacc += static_cast<double>(Ee);
@@ -1229,61 +1365,62 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
             const R p = X::fma(k.lam, k.logJ, -k.mu);
             if (WG) {
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
+                for (int bb = 0; bb < 4; ++bb)
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
                         R sum = 0;
 #pragma unroll
                         for (int j = 0; j < 3; ++j)
-                            sum = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[b][j], sum);
-                        ed[(kTcG + 3 * b + i) * E + el] = k.vol * sum;
+                            sum = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[bb][j], sum);
+                        ed[(kTcG + 3 * bb + i) * E + el] = k.vol * sum;
                     }
             }
             if (WH) {
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
+                for (int bb = 0; bb < 4; ++bb)
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
-                        ed[(kTcH + 3 * b + i) * E + el] =
-                            X::fma(k.FiT[3 * i + 2], k.n[b][2], X::fma(k.FiT[3 * i + 1], k.n[b][1], X::mul(k.FiT[3 * i], k.n[b][0])));
+                        ed[(kTcH + 3 * bb + i) * E + el] = X::fma(
+                            k.FiT[3 * i + 2], k.n[bb][2], X::fma(k.FiT[3 * i + 1], k.n[bb][1], X::mul(k.FiT[3 * i], k.n[bb][0])));
                 ed[kTcL * E + el] = X::mul(k.vol, k.lam);
                 ed[kTcP * E + el] = X::mul(k.vol, p);
                 const R mv = X::mul(k.vol, k.mu);
 #pragma unroll
-                for (int x = 0; x < 4; ++x)
+                for (int xx = 0; xx < 4; ++xx)
 #pragma unroll
-                    for (int y = x; y < 4; ++y)
-                        ed[(kTcCC + pair10(x, y)) * E + el] =
-                            X::mul(mv, X::fma(k.n[x][2], k.n[y][2], X::fma(k.n[x][1], k.n[y][1], X::mul(k.n[x][0], k.n[y][0]))));
+                    for (int y = xx; y < 4; ++y)
+                        ed[(kTcCC + pair10(xx, y)) * E + el] = X::mul(
+                            mv, X::fma(k.n[xx][2], k.n[y][2], X::fma(k.n[xx][1], k.n[y][1], X::mul(k.n[xx][0], k.n[y][0]))));
             }
         }
         // Energy of the cluster's own elements: fixed thread order, fixed tree.
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, off);
         if (lane == 0) red[warp] = eacc;
-        __syncthreads(); // element data complete; the staged inputs are dead
+        __syncthreads(); // element data complete
         if (tid == 0) {
             double t = 0;
             for (int w = 0; w < nw; ++w) t += red[w];
             a.cluster_energy[cl] = t;
             if (!isfinite(t)) st |= ST_NONFINITE_OUT;
         }
-        if (WG || WH) {
+        // The next cluster's indices, and the bounds of the one after, arrive while the item pass
+        // runs.
+        tc_load_idx(m, tc_bounds(s_hdr[buf]), tid, x);
+        if (tid < kTcFields) ahead = tc_field(m, cl + 2 * grid, tid);
+        if (ITEMS) {
             // Item pass: diagonal blocks (and gradient rows) first, then edge blocks.
-            const int i0 = __ldg(m.tc_item_ptr + cl), nd = __ldg(m.tc_ndiag + cl);
-            const int ni = WH ? __ldg(m.tc_item_ptr + cl + 1) - i0 : nd;
-            const uint16_t* ents = m.tc_ents + __ldg(m.tc_ent_ptr + cl);
-            const int r0 = __ldg(m.tc_row_ptr + cl);
-            for (int k = tid; k < ni; k += bd) {
-                const uint4 it = __ldg(m.tc_items + i0 + k);
-                const uint16_t* en = ents + (it.z & 0xfffffu);
+            for (int kk = tid; kk < ni; kk += kTcThreads) {
+                const uint4 it = sitems[kk];
+                const uint16_t* en = sents + (it.z & 0xfffffu);
                 const int cnt = static_cast<int>(it.z >> 20);
                 if (it.w >> 31) {
                     // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient:
                     //   H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
                     R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
+#pragma unroll UNR
                     for (int c = 0; c < cnt; ++c) {
-                        const int w = __ldg(en + c);
+                        const int w = en[c];
                         const int el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
                         if (WG) {
 #pragma unroll
@@ -1293,18 +1430,18 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
                             const R hh[3] = {ed[(kTcH + 3 * la) * E + el], ed[(kTcH + 3 * la + 1) * E + el],
                                              ed[(kTcH + 3 * la + 2) * E + el]};
                             const R dv = X::add(ed[kTcL * E + el], -ed[kTcP * E + el]), mg = ed[(kTcCC + pr) * E + el];
-                            int u = 0;
+                            int uix = 0;
 #pragma unroll
                             for (int i = 0; i < 3; ++i)
 #pragma unroll
-                                for (int kk = i; kk < 3; ++kk, ++u) {
-                                    acc[u] = X::fma(dv, X::mul(hh[i], hh[kk]), acc[u]);
-                                    if (i == kk) acc[u] = X::add(acc[u], mg);
+                                for (int q = i; q < 3; ++q, ++uix) {
+                                    acc[uix] = X::fma(dv, X::mul(hh[i], hh[q]), acc[uix]);
+                                    if (i == q) acc[uix] = X::add(acc[uix], mg);
                                 }
                         }
                     }
                     if (WG) {
-                        const int v = __ldg(m.tc_rows + r0 + static_cast<int>(it.w & 0xffu));
+                        const int v = rows[kTcRowInts * static_cast<int>(it.w & 0xffu)];
 #pragma unroll
                         for (int i = 0; i < 3; ++i) {
                             if (!X::finite(gs[i])) st |= ST_NONFINITE_OUT;
@@ -1325,8 +1462,9 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
                     // Off-diagonal block in the orientation of the lower vertex (a) -> higher (b):
                     //   C += vol lambda h_a h_b^T - vol p h_b h_a^T + vol mu (grad N_a . grad N_b) I.
                     R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll UNR
                     for (int c = 0; c < cnt; ++c) {
-                        const int w = __ldg(en + c);
+                        const int w = en[c];
                         const int el = w >> 8, pr = (w >> 4) & 15, ra = (w >> 2) & 3, cb = w & 3;
                         R ha[3], hb[3];
 #pragma unroll
@@ -1344,9 +1482,9 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
 #pragma unroll
                         for (int i = 0; i < 3; ++i)
 #pragma unroll
-                            for (int kk = 0; kk < 3; ++kk) {
-                                acc[3 * i + kk] = X::fma(B[kk], hb[i], X::fma(A[i], hb[kk], acc[3 * i + kk]));
-                                if (i == kk) acc[3 * i + kk] = X::add(acc[3 * i + kk], mg);
+                            for (int q = 0; q < 3; ++q) {
+                                acc[3 * i + q] = X::fma(B[q], hb[i], X::fma(A[i], hb[q], acc[3 * i + q]));
+                                if (i == q) acc[3 * i + q] = X::add(acc[3 * i + q], mg);
                             }
                     }
                     const bool tr = (it.w >> 30) & 1u;
@@ -1363,13 +1501,21 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
                 }
             }
         }
+        __syncthreads(); // staging complete; items, contributors and element data are dead
+        // The next cluster's stage, in flight during the copy pass.
+        const int nrc = nr;
+        {
+            const TcBounds bn = tc_bounds(s_hdr[buf]);
+            tc_issue<R, ITEMS>(m, a.u, bn, x, tid, sell, su, sitems, sents, r12, rowv);
+            ne = bn.ne;
+            ni = WH ? bn.ni : bn.nd;
+            nr = bn.nr;
+        }
         if (WH) {
-            __syncthreads(); // staging complete
             // Copy pass: one warp per owned row.
-            const int r0 = __ldg(m.tc_row_ptr + cl), nr = __ldg(m.tc_row_ptr + cl + 1) - r0;
-            for (int j = warp; j < nr; j += nw) {
-                const int v = __ldg(m.tc_rows + r0 + j), so = __ldg(m.tc_row_so + r0 + j);
-                const int base = __ldg(m.row_ptr + v), nb = __ldg(m.row_ptr + v + 1) - base;
+            for (int j = warp; j < nrc; j += nw) {
+                const int* rw = rows + kTcRowInts * j;
+                const int so = rw[1], base = rw[2], nb = rw[3] & 0xff;
                 bool ok = true;
                 if (!sell) {
                     HT* dst = hout + 9 * static_cast<size_t>(base);
@@ -1379,7 +1525,7 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
                         dst[t] = static_cast<HT>(val);
                     }
                 } else {
-                    const int qd = __ldg(m.diag_slot + v) - base, sb = __ldg(m.sell_base + v);
+                    const int qd = rw[3] >> 8, sb = rw[4];
                     for (int t = lane; t < 9 * (nb - qd); t += 32) {
                         const int qq = t / 9, tt = t - 9 * qq;
                         const R val = stage[so + 9 * qd + t];
@@ -1390,20 +1536,20 @@ __global__ void __launch_bounds__(THREADS, MINB) tet_cluster_kernel(const DevMes
                 if (!ok) st |= ST_NONFINITE_OUT;
             }
         }
-        __syncthreads(); // the next cluster reuses the shared memory
     }
+    cp_async_wait_all();
     st = __reduce_or_sync(0xffffffffu, st);
     if (lane == 0 && st) atomicOr(a.status, st);
 }
 
-template <typename R, bool WG, bool WH, int MINB = tc_minb<R>(0), int THREADS = kTcThreads>
+template <typename R, bool WG, bool WH, int MINB = tc_minb<R>(0), int UNR = tc_unroll(0)>
 void launch_tet_cluster(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     const size_t sm = tc_smem_bytes<R>();
     thread_local LaunchCache cache;
-    const int resident = resident_grid(tet_cluster_kernel<R, WG, WH, MINB, THREADS>, THREADS, sm, cache);
+    const int resident = resident_grid(tet_cluster_kernel<R, WG, WH, MINB, UNR>, kTcThreads, sm, cache);
     const int blocks = std::min(resident, m.tc_ncl);
     if (a.ev_begin) LPG_CUDA(cudaEventRecord(a.ev_begin, s));
-    if (blocks > 0) tet_cluster_kernel<R, WG, WH, MINB, THREADS><<<blocks, THREADS, sm, s>>>(m, a);
+    if (blocks > 0) tet_cluster_kernel<R, WG, WH, MINB, UNR><<<blocks, kTcThreads, sm, s>>>(m, a);
     if (a.ev_end) LPG_CUDA(cudaEventRecord(a.ev_end, s));
     LPG_CUDA(cudaGetLastError());
 }
@@ -2659,17 +2805,22 @@ __global__ void __launch_bounds__(kHermPsdThreads) hermite_psd_kernel(int T, dou
             }
             __syncthreads();
         }
-        // Implicit QL with Wilkinson shifts on (d, ev); rotations applied to the rows of Q.
+        // Implicit QL with Wilkinson shifts on (d, ev); rotations applied to the rows of Q. An
+        // off-diagonal entry is negligible below eps times the tridiagonal matrix's norm bound
+        // max |d_i| + |e_i| (as tql2 tests): the element's rigid-body modes are exact zero
+        // eigenvalues, next to which a test relative to the neighbouring diagonal entries alone
+        // never deflates.
         if (tid == 0) s_bad = 0;
         __syncthreads();
+        double tnorm = 0.0;
+        if (tid == 0)
+            for (int i = 0; i < n; ++i) tnorm = fmax(tnorm, fabs(d[i]) + fabs(ev[i]));
         for (int l = 0; l < n; ++l) {
             for (int iter = 0;; ++iter) {
                 if (tid == 0) {
                     int m = l;
-                    for (; m < n - 1; ++m) {
-                        const double dd = fabs(d[m]) + fabs(d[m + 1]);
-                        if (fabs(ev[m]) <= 2.220446049250313e-16 * dd) break;
-                    }
+                    for (; m < n - 1; ++m)
+                        if (fabs(ev[m]) <= 2.220446049250313e-16 * tnorm) break;
                     s_hi = m;
                     s_count = 0;
                     if (m != l) {
@@ -2914,11 +3065,11 @@ __global__ void set_theta_kernel(double* rec64, float* rec32, const double* __re
     rec32[12 * static_cast<size_t>(e) + 11] = static_cast<float>(mu);
 }
 
-// The Hessian-writing tet cluster kernel in the register-budget variant a.cl_variant.
+// The Hessian-writing tet cluster kernel in the launch variant a.cl_variant.
 template <typename R, bool WG> void launch_tet_variant(const DevMesh& m, const EvalArgs& a, cudaStream_t s) {
     switch (a.cl_variant) {
-    case 1: launch_tet_cluster<R, WG, true, tc_minb<R>(1)>(m, a, s); break;
-    case 2: launch_tet_cluster<R, WG, true, tc_minb<R>(2), tc_threads<R>(2)>(m, a, s); break;
+    case 1: launch_tet_cluster<R, WG, true, tc_minb<R>(1), tc_unroll(1)>(m, a, s); break;
+    case 2: launch_tet_cluster<R, WG, true, tc_minb<R>(2), tc_unroll(2)>(m, a, s); break;
     default: launch_tet_cluster<R, WG, true>(m, a, s); break;
     }
 }

@@ -121,12 +121,20 @@ constexpr int kClusterElems = LPG_CLUSTER_ELEMS;
 #define LPG_TC_ELEMS 256
 #endif
 #ifndef LPG_TC_VALS
-#define LPG_TC_VALS 4608
+#define LPG_TC_VALS 3072
+#endif
+#ifndef LPG_TC_ENTS
+#define LPG_TC_ENTS 2048
 #endif
 constexpr int kTcRows = LPG_TC_ROWS;
 constexpr int kTcElems = LPG_TC_ELEMS;
 constexpr int kTcVerts = 256;
 constexpr int kTcVals = LPG_TC_VALS; // output staging values of a cluster (its rows' 9 nb)
+// Items of a cluster (at most one per block of its rows) and contributor words (padded to a
+// multiple of 8); both are staged in shared memory.
+constexpr int kTcItems = kTcVals / 9;
+constexpr int kTcEnts = LPG_TC_ENTS;
+static_assert(kTcEnts % 8 == 0, "contributor lists are staged in 16-byte chunks");
 static_assert(kTcElems <= 256 && kTcRows <= 256, "tet cluster indices are 8-bit");
 // Clusters of 64-node cells (Hermite hexes: 8 slot rows per vertex, ~216 blocks per row) hold at
 // most one vertex's rows, so a cluster's slot and contributor tables fit in shared memory.

@@ -185,7 +185,7 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
         const int c = ncl++;
         queue.assign(1, seed);
         qstamp[seed] = c;
-        int nr = 0, ne = 0, nv = 0, nvals = 0;
+        int nr = 0, ne = 0, nv = 0, nvals = 0, nents = 0;
         for (size_t qi = 0; qi < queue.size() && nr < kTcRows; ++qi) {
             const int v = queue[qi];
             if (cl_of[v] >= 0) continue;
@@ -207,7 +207,10 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
                 for (int a = 0; a < 4; ++a)
                     if (vstamp[vert(inc[k] & kMaskE, a)] == -2 - c) vstamp[vert(inc[k] & kMaskE, a)] = -1;
             const int add_vals = 9 * (p.row_ptr[v + 1] - p.row_ptr[v]);
-            if (ne + add_e > kTcElems || nv + add_v > kTcVerts || nvals + add_vals > kTcVals) {
+            // Contributor words of the row's blocks: at most four per incident element.
+            const int add_ents = 4 * (p.inc_ptr[v + 1] - p.inc_ptr[v]);
+            if (ne + add_e > kTcElems || nv + add_v > kTcVerts || nvals + add_vals > kTcVals ||
+                nents + add_ents > kTcEnts - 7) {
                 if (nr == 0) fail(LPG_EINVAL, "vertex neighbourhood exceeds the assembly cluster limits");
                 continue;
             }
@@ -216,6 +219,7 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
             ne += add_e;
             nv += add_v;
             nvals += add_vals;
+            nents += add_ents;
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
                 const int e = inc[k] & kMaskE;
                 estamp[e] = c;
@@ -625,6 +629,11 @@ void check_tet_clusters(const HostPlan& p, const int32_t* tets) {
         const int e0 = p.tc_el_ptr[c], ne = p.tc_el_ptr[c + 1] - e0;
         const int v0 = p.tc_vert_ptr[c], nv = p.tc_vert_ptr[c + 1] - v0;
         if (nr > kTcRows || ne > kTcElems || nv > kTcVerts) bad("cluster over its limits");
+        if (p.tc_item_ptr[c + 1] - p.tc_item_ptr[c] > kTcItems) bad("cluster items over their limit");
+        {
+            const int nn = p.tc_ent_ptr[c + 1] - p.tc_ent_ptr[c];
+            if (nn > kTcEnts || nn % 8 != 0 || p.tc_ent_ptr[c] % 8 != 0) bad("cluster contributor lists over their limit");
+        }
         if (nr == 0) bad("cluster without rows");
         {
             const int vl = p.tc_rows[r0 + nr - 1];

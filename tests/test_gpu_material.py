@@ -288,7 +288,7 @@ def test_static_equilibrium_response_over_a_torch_material():
     pmap = dof.ConstantDofMap(topo, 2)
     load = energy.QuadraticEnergy(sp.csc_matrix((n, n)), -50.0 * f)
     fixed = dof.DofReduction(n, g["fixed"])
-    opts = solver.NewtonOptions(gradient_tolerance=1e-12, stop_rule="relative", max_iterations=100, cg_tolerance=1e-6)
+    opts = solver.NewtonOptions(gradient_tolerance=1e-10, stop_rule="relative", max_iterations=100, cg_tolerance=1e-8)
 
     def make(material):
         key = (material, fem.TetP1Basis, fem.TetCentroidQuadrature)
