@@ -1165,6 +1165,7 @@ __device__ __forceinline__ size_t cl_pos(int layout, int slot0, int nb, int sb, 
 constexpr int kTcThreads = 256;
 static_assert(kTcThreads >= kTcElems && kTcThreads >= kTcVerts && kTcThreads >= kTcRows,
               "one element, one vertex and one row per thread in the stage");
+static_assert(((2 * kTcRows + 31) & ~31) < kTcThreads, "the diagonal lane pairs leave lanes for the edge items");
 // Per-element data in shared memory, one component per kTcElems-long array: h_a (3 a + i),
 // vol mu grad N_a . grad N_b (pair order), vol lambda, vol p, g_a (3 a + i).
 constexpr int kTcH = 0, kTcCC = 12, kTcL = 22, kTcP = 23, kTcG = 24, kTcComp = 36;
@@ -1326,7 +1327,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     int rowv[kTcRowInts] = {0, 0, 0, 0, 0};
     tc_issue<R, ITEMS>(m, a.u, b, x, tid, sell, su, sitems, sents, r12, rowv);
     int ahead = tid < kTcFields ? tc_field(m, cl + grid, tid) : 0;
-    int ne = b.ne, ni = WH ? b.ni : b.nd, nr = b.nr;
+    int ne = b.ne, ni = WH ? b.ni : b.nd, nr = b.nr, ndc = b.nd;
     for (int buf = 0; cl < m.tc_ncl; cl += grid, buf ^= 1) {
         int* rows = srow + buf * kTcRows * kTcRowInts;
         if (ITEMS && tid < nr) {
@@ -1409,17 +1410,26 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         tc_load_idx(m, tc_bounds(s_hdr[buf]), tid, x);
         if (tid < kTcFields) ahead = tc_field(m, cl + 2 * grid, tid);
         if (ITEMS) {
-            // Item pass: diagonal blocks (and gradient rows) first, then edge blocks.
-            for (int kk = tid; kk < ni; kk += kTcThreads) {
-                const uint4 it = sitems[kk];
-                const uint16_t* en = sents + (it.z & 0xfffffu);
-                const int cnt = static_cast<int>(it.z >> 20);
-                if (it.w >> 31) {
-                    // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient:
-                    //   H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
-                    R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
+            // Item pass. The nd diagonal items (the first nd) are summed by lane pairs, each lane
+            // over half the contributor list in ascending order, the two halves added by a
+            // shuffle; they fill whole warps (2 nd lanes rounded up to 32), and the edge items
+            // follow on the remaining lanes, so no warp runs both kinds and the diagonal sums
+            // (the longest lists) take about as long as an edge block.
+            const int nd = ndc, dl = 2 * nd, dpad = (dl + 31) & ~31;
+            if (tid < dpad) {
+                // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient:
+                //   H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
+                const bool active = tid < dl;
+                const int part = tid & 1;
+                uint4 it = make_uint4(0u, 0u, 0u, 0u);
+                R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
+                if (active) {
+                    it = sitems[tid >> 1];
+                    const uint16_t* en = sents + (it.z & 0xfffffu);
+                    const int cnt = static_cast<int>(it.z >> 20), half = (cnt + 1) >> 1;
+                    const int c1 = part ? cnt : half;
 #pragma unroll UNR
-                    for (int c = 0; c < cnt; ++c) {
+                    for (int c = part ? half : 0; c < c1; ++c) {
                         const int w = en[c];
                         const int el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
                         if (WG) {
@@ -1440,6 +1450,17 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
                                 }
                         }
                     }
+                }
+                // First half + second half (the same sum on both lanes of the pair).
+                if (WG) {
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) gs[i] = X::add(gs[i], __shfl_xor_sync(0xffffffffu, gs[i], 1));
+                }
+                if (WH) {
+#pragma unroll
+                    for (int u6 = 0; u6 < 6; ++u6) acc[u6] = X::add(acc[u6], __shfl_xor_sync(0xffffffffu, acc[u6], 1));
+                }
+                if (active && part == 0) {
                     if (WG) {
                         const int v = rows[kTcRowInts * static_cast<int>(it.w & 0xffu)];
 #pragma unroll
@@ -1455,10 +1476,15 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
 #pragma unroll
                             for (int c = 0; c < 3; ++c) stage[tc_stage(it.x, csc, i, c)] = acc[sym3[3 * i + c]];
                     }
-                } else if (WH) {
+                }
+            } else if (WH) {
+                for (int kk = nd + tid - dpad; kk < ni; kk += kTcThreads - dpad) {
+                    const uint4 it = sitems[kk];
                     // The solver layout keeps only blocks right of the diagonal: an edge to a
                     // lower-numbered row of another cluster is not needed there.
                     if (sell && ((it.w >> 30) & 1u)) continue;
+                    const uint16_t* en = sents + (it.z & 0xfffffu);
+                    const int cnt = static_cast<int>(it.z >> 20);
                     // Off-diagonal block in the orientation of the lower vertex (a) -> higher (b):
                     //   C += vol lambda h_a h_b^T - vol p h_b h_a^T + vol mu (grad N_a . grad N_b) I.
                     R acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -1510,6 +1536,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
             ne = bn.ne;
             ni = WH ? bn.ni : bn.nd;
             nr = bn.nr;
+            ndc = bn.nd;
         }
         if (WH) {
             // Copy pass: one warp per owned row.

@@ -38,6 +38,27 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     __syncthreads();
     return r;
 }
+// Two block sums at once (sh holds 2 doubles per warp), each in block_sum's order.
+__device__ __forceinline__ double2 block_sum2(double a, double b, double* sh) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh[2 * (threadIdx.x >> 5)] = a;
+        sh[2 * (threadIdx.x >> 5) + 1] = b;
+    }
+    __syncthreads();
+    double ra = 0, rb = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (blockDim.x >> 5); ++w) {
+            ra += sh[2 * w];
+            rb += sh[2 * w + 1];
+        }
+    __syncthreads();
+    return make_double2(ra, rb);
+}
 __device__ __forceinline__ double block_max(double v, double* sh) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
@@ -512,7 +533,7 @@ template <typename R>
 __global__ void __launch_bounds__(kThreads) pcg_update(PcgState* st, const R* __restrict__ dinv, R* x, R* r, R* z,
                                                        const R* __restrict__ p, const R* __restrict__ Ap, int V,
                                                        double* part) {
-    __shared__ double sh[kThreads / 32];
+    __shared__ double sh[2 * (kThreads / 32)];
     __shared__ bool last;
     if (st->done) return;
     const R alpha = static_cast<R>(st->alpha);
@@ -539,11 +560,10 @@ __global__ void __launch_bounds__(kThreads) pcg_update(PcgState* st, const R* __
             rr += static_cast<double>(rv[i]) * rv[i];
         }
     }
-    rz = block_sum(rz, sh);
-    rr = block_sum(rr, sh);
+    const double2 sums = block_sum2(rz, rr, sh);
     if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = rz;
-        part[2 * blockIdx.x + 1] = rr;
+        part[2 * blockIdx.x] = sums.x;
+        part[2 * blockIdx.x + 1] = sums.y;
         __threadfence(); // this thread wrote the partials
         last = atomicAdd(&st->count_b, 1u) == gridDim.x - 1;
     }
@@ -554,8 +574,11 @@ __global__ void __launch_bounds__(kThreads) pcg_update(PcgState* st, const R* __
         a += __ldcg(part + 2 * i);
         b += __ldcg(part + 2 * i + 1);
     }
-    a = block_sum(a, sh);
-    b = block_sum(b, sh);
+    {
+        const double2 t = block_sum2(a, b, sh);
+        a = t.x;
+        b = t.y;
+    }
     if (threadIdx.x == 0) {
         st->count_b = 0;
         st->iters += 1;

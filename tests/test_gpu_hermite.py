@@ -217,7 +217,8 @@ def test_projected_hessian_matches_the_oracle(precision, tol):
     _, _, Hr = oracle.hex_hermite_eval(X, cells, theta, u, projected=True)
     assert rel_err(Hp.toarray(), Hr) <= tol
     assert rel_err(He.toarray(), Hr) > 1e-3  # the clamp changed the matrix
-    assert np.linalg.eigvalsh(Hp.toarray()).min() >= -1e-10 * np.abs(Hr).max()
+    # Semi-definite up to the rounding of the stored values (FP32 records in mixed precision).
+    assert np.linalg.eigvalsh(Hp.toarray()).min() >= -10 * tol * np.abs(Hr).max()
     D = (Hp - Hp.T).tocsc()
     D.eliminate_zeros()
     assert D.nnz == 0  # bitwise symmetric

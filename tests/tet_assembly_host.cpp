@@ -134,15 +134,22 @@ extern "C" int tet_assemble(int V, const double* X, int T, const int32_t* tets, 
                 const uint16_t* en = ents + (it[2] & 0xfffffu);
                 const int cnt = static_cast<int>(it[2] >> 20);
                 if (it[3] >> 31) {
+                    // Two halves of the list summed apart (the kernel's lane pair), then added.
                     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
-                    for (int c = 0; c < cnt; ++c) {
-                        const int w = en[c], el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
-                        for (int i = 0; i < 3; ++i) gs[i] += ed[(24 + 3 * la + i) * E + el];
-                        const double dv = ed[22 * E + el] - ed[23 * E + el], mg = ed[(12 + pr) * E + el];
-                        for (int i = 0; i < 3; ++i)
-                            for (int cc = 0; cc < 3; ++cc)
-                                acc[3 * i + cc] += dv * (ed[(3 * la + i) * E + el] * ed[(3 * la + cc) * E + el]) +
-                                                   (i == cc ? mg : 0.0);
+                    const int half = (cnt + 1) >> 1;
+                    for (int part = 0; part < 2; ++part) {
+                        double ap[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gp[3] = {0, 0, 0};
+                        for (int c = part ? half : 0; c < (part ? cnt : half); ++c) {
+                            const int w = en[c], el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
+                            for (int i = 0; i < 3; ++i) gp[i] += ed[(24 + 3 * la + i) * E + el];
+                            const double dv = ed[22 * E + el] - ed[23 * E + el], mg = ed[(12 + pr) * E + el];
+                            for (int i = 0; i < 3; ++i)
+                                for (int cc = 0; cc < 3; ++cc)
+                                    ap[3 * i + cc] += dv * (ed[(3 * la + i) * E + el] * ed[(3 * la + cc) * E + el]) +
+                                                      (i == cc ? mg : 0.0);
+                        }
+                        for (int t = 0; t < 9; ++t) acc[t] += ap[t];
+                        for (int i = 0; i < 3; ++i) gs[i] += gp[i];
                     }
                     const int v = p.tc_rows[r0 + static_cast<int>(it[3] & 0xffu)];
                     for (int i = 0; i < 3; ++i) grad[3 * v + i] = gs[i];
