@@ -252,7 +252,9 @@ def test_newton_over_a_torch_material_matches_the_native_solve():
                              on_iteration=steps_p.append)
     assert rn.status == rp.status == solver.NewtonStatus.Converged
     assert rel_err(rp.x, rn.x) <= 1e-8
-    assert rp.iterations == rn.iterations and len(steps_p) == len(steps_n)
+    # The two evaluate the same energy with different summation orders, so the last step that
+    # crosses the 1e-10 stopping bound may come one iteration apart.
+    assert abs(rp.iterations - rn.iterations) <= 1 and abs(len(steps_p) - len(steps_n)) <= 1
     for a, b in zip(steps_p, steps_n):
         assert abs(a.energy - b.energy) <= 1e-9 * abs(b.energy) + 1e-300
     # A device start works too; a failing material stops the solve with its own exception.
