@@ -9,7 +9,6 @@
 // are two-stage with a fixed block -> index map, so results do not depend on scheduling.
 
 #include <algorithm>
-#include <cstdlib>
 #include <chrono>
 #include <array>
 #include <cmath>
@@ -59,6 +58,13 @@ __device__ __forceinline__ double2 block_sum2(double a, double b, double* sh) {
         }
     __syncthreads();
     return make_double2(ra, rb);
+}
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may
+// start while the kernel before it drains; it waits here until that kernel has completed and
+// its memory is visible (a no-op for an ordinary launch), then lets its own dependent launch.
+__device__ __forceinline__ void pdl_wait_then_release() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 __device__ __forceinline__ double block_max(double v, double* sh) {
 #pragma unroll
@@ -269,6 +275,7 @@ __global__ void __launch_bounds__(kThreads, (SpmvCfg<TK, VAR>::minb)) spmv_sell(
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
     using A = typename std::conditional<(sizeof(TK) == 4 && sizeof(TV) == 4), float, double>::type;
+    if (PCG) pdl_wait_then_release();
     if (PCG && st->done) return;
     const TV beta = PCG ? static_cast<TV>(st->beta) : TV(0);
     const int lane = threadIdx.x & 31;
@@ -536,6 +543,7 @@ __global__ void __launch_bounds__(kThreads) pcg_update(PcgState* st, const R* __
                                                        double* part) {
     __shared__ double sh[2 * (kThreads / 32)];
     __shared__ bool last;
+    pdl_wait_then_release();
     if (st->done) return;
     const R alpha = static_cast<R>(st->alpha);
     double rz = 0, rr = 0;
@@ -703,58 +711,6 @@ template <typename Kern> int one_wave(Kern kernel, size_t work) {
     return static_cast<int>(std::max<size_t>(1, std::min(work, wave)));
 }
 
-// L2 residency of the PCG matrix. Every PCG iteration streams the solver matrix's values; when
-// they fit the L2's persisting set-aside (the FP32 matrix of a 64^3 box: ~69 MB of the 126 MB L2),
-// marking them persisting keeps them in L2 across the iterations instead of re-reading them from
-// HBM. The window covers the values array ([base, base + bytes)); hit ratio = set-aside / window
-// when the matrix is larger. The set-aside is a limit of this process's context; the persisting
-// lines are released after each solve (release()). LPG_L2_PERSIST=0 turns it off.
-struct L2Window {
-    cudaAccessPolicyWindow w{};
-    bool on = false;
-    // Sizes the set-aside for `bytes` at `base` on the current device (once per size).
-    void setup(const void* base, size_t bytes) {
-        on = false;
-        const char* env = std::getenv("LPG_L2_PERSIST");
-        if ((env && env[0] == '0') || bytes == 0) return;
-        int dev = 0, max_persist = 0, max_window = 0;
-        LPG_CUDA(cudaGetDevice(&dev));
-        LPG_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
-        LPG_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
-        if (max_persist <= 0 || max_window <= 0) return;
-        const size_t carve = std::min(bytes, static_cast<size_t>(max_persist));
-        size_t current = 0;
-        LPG_CUDA(cudaDeviceGetLimit(&current, cudaLimitPersistingL2CacheSize));
-        if (current < carve) LPG_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve));
-        w.base_ptr = const_cast<void*>(base);
-        w.num_bytes = std::min(bytes, static_cast<size_t>(max_window));
-        w.hitRatio = static_cast<float>(std::min(1.0, static_cast<double>(carve) / static_cast<double>(w.num_bytes)));
-        w.hitProp = cudaAccessPropertyPersisting;
-        w.missProp = cudaAccessPropertyStreaming;
-        on = true;
-    }
-    // Applies the window to every kernel node of a captured graph.
-    void apply(cudaGraph_t g) const {
-        if (!on) return;
-        size_t n = 0;
-        LPG_CUDA(cudaGraphGetNodes(g, nullptr, &n));
-        std::vector<cudaGraphNode_t> nodes(n);
-        LPG_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
-        cudaKernelNodeAttrValue v{};
-        v.accessPolicyWindow = w;
-        for (cudaGraphNode_t nd : nodes) {
-            cudaGraphNodeType t;
-            LPG_CUDA(cudaGraphNodeGetType(nd, &t));
-            if (t == cudaGraphNodeTypeKernel)
-                LPG_CUDA(cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v));
-        }
-    }
-    // Returns the persisting lines to normal (after a solve, so later work has the whole L2).
-    void release() const {
-        if (on) LPG_CUDA(cudaCtxResetPersistingL2Cache());
-    }
-};
-
 // ---------------------------------------------------------------------------
 // Host-side helpers bound to one handle.
 // ---------------------------------------------------------------------------
@@ -915,11 +871,29 @@ struct Solver {
     void enqueue_iterations_v(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA,
                               R* pB, R* Ap, PcgState* st, double* part, int pairs) {
         const int sg = spmv_grid(0), ug = std::max(1, grid(static_cast<size_t>(V)));
+        // Each kernel is launched as a programmatic dependent of the one before it (it waits in
+        // griddepcontrol.wait), so its launch overlaps the previous kernel's last blocks.
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cs{}, cu{};
+        cs.gridDim = dim3(static_cast<unsigned>(sg));
+        cu.gridDim = dim3(static_cast<unsigned>(ug));
+        cs.blockDim = cu.blockDim = dim3(kThreads);
+        cs.stream = cu.stream = gs;
+        cs.attrs = cu.attrs = attr;
+        cs.numAttrs = cu.numAttrs = 1;
+        const DevMesh& dm = h.dm;
+        const R* zc = z;
         for (int i = 0; i < pairs; ++i) {
-            spmv_sell<R, R, R, true, false, 4, VAR><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pA, mask4, Ap, pB, st, part);
-            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pB, Ap, V, part);
-            spmv_sell<R, R, R, true, false, 4, VAR><<<sg, kThreads, 0, gs>>>(h.dm, K, z, pB, mask4, Ap, pA, st, part);
-            pcg_update<R><<<ug, kThreads, 0, gs>>>(st, dinv, x, r, z, pA, Ap, V, part);
+            LPG_CUDA(cudaLaunchKernelEx(&cs, spmv_sell<R, R, R, true, false, 4, VAR>, dm, K, zc,
+                                        static_cast<const R*>(pA), static_cast<const R*>(mask4), Ap, pB, st, part));
+            LPG_CUDA(cudaLaunchKernelEx(&cu, pcg_update<R>, st, dinv, x, r, z, static_cast<const R*>(pB),
+                                        static_cast<const R*>(Ap), V, part));
+            LPG_CUDA(cudaLaunchKernelEx(&cs, spmv_sell<R, R, R, true, false, 4, VAR>, dm, K, zc,
+                                        static_cast<const R*>(pB), static_cast<const R*>(mask4), Ap, pA, st, part));
+            LPG_CUDA(cudaLaunchKernelEx(&cu, pcg_update<R>, st, dinv, x, r, z, static_cast<const R*>(pA),
+                                        static_cast<const R*>(Ap), V, part));
         }
     }
     // The same with the handle's tuned SpMV variant for precision R.
@@ -962,16 +936,12 @@ struct Solver {
         const double bnorm = std::sqrt(stats<double, double>(b64, nullptr, mask)[1]);
         if (bnorm == 0) return out;
         pad_rhs<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(mask, mask, mask4, V); // 0/1 values: mask^2 = mask
-        // The graph of 16 iteration pairs, captured on the handle's own stream and cached; its
-        // kernels carry the matrix's L2 persisting window.
-        L2Window l2;
-        l2.setup(Kin, h.plan.sell_values() * sizeof(R));
+        // The graph of 16 iteration pairs, captured on the handle's own stream and cached.
         constexpr int kPairs = 16;
         constexpr int kKey = 12;
         const void* key[kKey] = {Kin, dinv, mask4, x, r, z, pA, pB, Ap, st, part,
-                                 reinterpret_cast<const void*>(((sizeof(R) * 1000003u + V) * 4u +
-                                                                h.tune.spmv[sizeof(R) == 8 ? 0 : 1]) * 2u +
-                                                               (l2.on ? 1u : 0u))};
+                                 reinterpret_cast<const void*>((sizeof(R) * 1000003u + V) * 4u +
+                                                               h.tune.spmv[sizeof(R) == 8 ? 0 : 1])};
         bool same = h.pcg_graph != nullptr;
         for (int i = 0; i < kKey && same; ++i) same = h.pcg_graph_key[i] == key[i];
         cudaStream_t gs = h.own_stream;
@@ -984,7 +954,6 @@ struct Solver {
             LPG_CUDA(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
             enqueue_iterations<R>(gs, static_cast<const R*>(Kin), dinv, mask4, x, r, z, pA, pB, Ap, st, part, kPairs);
             LPG_CUDA(cudaStreamEndCapture(gs, &g));
-            l2.apply(g);
             LPG_CUDA(cudaGraphInstantiate(&h.pcg_graph, g, 0));
             cudaGraphDestroy(g);
             for (int i = 0; i < kKey; ++i) h.pcg_graph_key[i] = key[i];
@@ -1024,8 +993,6 @@ struct Solver {
             if (out.breakdown || !(rnorm > tol * bnorm) || out.iters >= max_iters || !std::isfinite(rnorm)) break;
         }
         cudaEventDestroy(ev);
-        LPG_CUDA(cudaStreamSynchronize(gs));
-        l2.release();
         return out;
     }
 };
