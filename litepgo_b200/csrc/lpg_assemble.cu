@@ -912,8 +912,10 @@ __device__ __forceinline__ void jacobi_round(R (&A)[45], VA& V, const int rd) {
         const R apq = A[sym9(P, Q)];
         const R d = A[sym9(Q, Q)] - A[sym9(P, P)], a2 = R(2) * apq;
         const R num = d > R(0) ? a2 : (d < R(0) ? -a2 : fabs(a2));
-        const R tk = num / (fabs(d) + sqrt(d * d + a2 * a2));
-        t[k] = apq == R(0) ? R(0) : tk;
+        const R den = fabs(d) + sqrt(d * d + a2 * a2);
+        // den is 0 only when d = 0 and a2^2 underflows (FP32: |apq| below ~1e-23 of the largest
+        // entry): the pair is already diagonal to far below the sweep threshold, so no rotation.
+        t[k] = (apq == R(0) || !(den > R(0))) ? R(0) : num / den;
         c[k] = rsqrt(R(1) + t[k] * t[k]);
         sn[k] = t[k] * c[k];
     }
