@@ -1192,6 +1192,69 @@ template <typename R> constexpr size_t tc_smem_bytes() {
            2 * static_cast<size_t>(kTcRows) * kTcRowInts * sizeof(int);
 }
 
+// One contributor of an edge block: acc(i, q) = B_q hb_i + (A_i hb_q + acc(i, q)) (A = vol lambda
+// h_a, B = -vol p h_a), then + mg on the diagonal entries. In FP32 the nine chains run as packed
+// pairs (sm_100 f32x2 FMA); each lane of a pair is rounded as the scalar FMA, so the results are
+// bitwise those of the scalar form.
+template <typename R>
+__device__ __forceinline__ void edge_contrib(R (&acc)[9], const R (&A)[3], const R (&B)[3], const R (&hb)[3], R mg) {
+    using X = M<R>;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            acc[3 * i + q] = X::fma(B[q], hb[i], X::fma(A[i], hb[q], acc[3 * i + q]));
+            if (i == q) acc[3 * i + q] = X::add(acc[3 * i + q], mg);
+        }
+}
+template <>
+__device__ __forceinline__ void edge_contrib<float>(float (&acc)[9], const float (&A)[3], const float (&B)[3],
+                                                    const float (&hb)[3], float mg) {
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+        const int i0 = u / 3, q0 = u % 3, i1 = (u + 1) / 3, q1 = (u + 1) % 3;
+        float2 t = __ffma2_rn(make_float2(A[i0], A[i1]), make_float2(hb[q0], hb[q1]), make_float2(acc[u], acc[u + 1]));
+        t = __ffma2_rn(make_float2(B[q0], B[q1]), make_float2(hb[i0], hb[i1]), t);
+        acc[u] = t.x;
+        acc[u + 1] = t.y;
+    }
+    acc[8] = __fmaf_rn(B[2], hb[2], __fmaf_rn(A[2], hb[2], acc[8]));
+    acc[0] = __fadd_rn(acc[0], mg);
+    acc[4] = __fadd_rn(acc[4], mg);
+    acc[8] = __fadd_rn(acc[8], mg);
+}
+
+// One contributor of a diagonal block (its upper triangle, 6 sums): acc(i, q) += dv (hh_i hh_q),
+// then + mg on the diagonal; FP32 in packed pairs, bitwise as the scalar form.
+template <typename R> __device__ __forceinline__ void diag_contrib(R (&acc)[6], const R (&hh)[3], R dv, R mg) {
+    using X = M<R>;
+    int uix = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int q = i; q < 3; ++q, ++uix) {
+            acc[uix] = X::fma(dv, X::mul(hh[i], hh[q]), acc[uix]);
+            if (i == q) acc[uix] = X::add(acc[uix], mg);
+        }
+}
+template <>
+__device__ __forceinline__ void diag_contrib<float>(float (&acc)[6], const float (&hh)[3], float dv, float mg) {
+    // Upper-triangle order: (0,0) (0,1) (0,2) (1,1) (1,2) (2,2).
+    const float2 p01 = __fmul2_rn(make_float2(hh[0], hh[0]), make_float2(hh[0], hh[1]));
+    const float2 p23 = __fmul2_rn(make_float2(hh[0], hh[1]), make_float2(hh[2], hh[1]));
+    const float2 p45 = __fmul2_rn(make_float2(hh[1], hh[2]), make_float2(hh[2], hh[2]));
+    const float2 dd = make_float2(dv, dv);
+    const float2 a01 = __ffma2_rn(dd, p01, make_float2(acc[0], acc[1]));
+    const float2 a23 = __ffma2_rn(dd, p23, make_float2(acc[2], acc[3]));
+    const float2 a45 = __ffma2_rn(dd, p45, make_float2(acc[4], acc[5]));
+    acc[0] = __fadd_rn(a01.x, mg);
+    acc[1] = a01.y;
+    acc[2] = a23.x;
+    acc[3] = __fadd_rn(a23.y, mg);
+    acc[4] = a45.x;
+    acc[5] = __fadd_rn(a45.y, mg);
+}
+
 // Staging index of entry (i, c) of the block at packed position pos (row offset so, block q,
 // row length nb): BSR and solver layouts keep blocks row-major one after the other, CSC keeps
 // the row's three scalar rows one after the other.
@@ -1268,7 +1331,8 @@ template <typename R, bool ITEMS>
 __device__ __forceinline__ void tc_issue(const DevMesh& m, const double* __restrict__ u, const TcBounds& b,
                                          const TcIdx& x, int t, bool sell, double* su, uint4* sitems, uint16_t* sents,
                                          R (&r12)[12], int (&rowv)[kTcRowInts]) {
-    if (t < b.ne) load_rec<R>(rec_ptr<R>(m), static_cast<int>(x.ew & 0x7fffffffu), r12);
+    // Without items (energy only) an element the cluster does not own contributes nothing.
+    if (t < b.ne && (ITEMS || (x.ew >> 31))) load_rec<R>(rec_ptr<R>(m), static_cast<int>(x.ew & 0x7fffffffu), r12);
     if (t < b.nv) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) cp_async8(su + 3 * t + i, u + 3 * static_cast<size_t>(x.vert) + i);
@@ -1343,7 +1407,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         const uint32_t ew = x.ew;
         R Ds[3][3];
         bool in_ok = true;
-        if (tid < ne) {
+        if (tid < ne && (ITEMS || (ew >> 31))) {
             double uu[4][3];
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -1355,7 +1419,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         }
         __syncthreads(); // the displacements are read; their memory holds element data from here
         double eacc = 0;
-        if (tid < ne) {
+        if (tid < ne && (ITEMS || (ew >> 31))) {
             const int el = tid;
             const int e = static_cast<int>(ew & 0x7fffffffu);
             Kin<R> k;
@@ -1442,14 +1506,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
                             const R hh[3] = {ed[(kTcH + 3 * la) * E + el], ed[(kTcH + 3 * la + 1) * E + el],
                                              ed[(kTcH + 3 * la + 2) * E + el]};
                             const R dv = X::add(ed[kTcL * E + el], -ed[kTcP * E + el]), mg = ed[(kTcCC + pr) * E + el];
-                            int uix = 0;
-#pragma unroll
-                            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                                for (int q = i; q < 3; ++q, ++uix) {
-                                    acc[uix] = X::fma(dv, X::mul(hh[i], hh[q]), acc[uix]);
-                                    if (i == q) acc[uix] = X::add(acc[uix], mg);
-                                }
+                            diag_contrib<R>(acc, hh, dv, mg);
                         }
                     }
                 }
@@ -1507,13 +1564,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
                             A[i] = X::mul(lv, ha[i]);
                             B[i] = X::mul(-pv, ha[i]);
                         }
-#pragma unroll
-                        for (int i = 0; i < 3; ++i)
-#pragma unroll
-                            for (int q = 0; q < 3; ++q) {
-                                acc[3 * i + q] = X::fma(B[q], hb[i], X::fma(A[i], hb[q], acc[3 * i + q]));
-                                if (i == q) acc[3 * i + q] = X::add(acc[3 * i + q], mg);
-                            }
+                        edge_contrib<R>(acc, A, B, hb, mg);
                     }
                     const bool tr = (it.w >> 30) & 1u;
 #pragma unroll
