@@ -26,6 +26,7 @@
 #include <cuda_pipeline.h>
 
 #include "lpg_internal.h"
+#include "lpg_clamp9.h"
 #include "lpg_psd.h"
 
 namespace lpg {
@@ -223,10 +224,6 @@ template <typename R> struct HOut;
 template <> struct HOut<double> { using T = double; };
 template <> struct HOut<float> { using T = float; };
 
-// Packed upper-triangle index of a symmetric 9x9 matrix.
-__host__ __device__ constexpr int sym9(int r, int c) {
-    return r <= c ? r * 9 - (r * (r - 1)) / 2 + (c - r) : c * 9 - (c * (c - 1)) / 2 + (r - c);
-}
 
 // Orthonormal basis of {x in R^4 : sum x = 0}: q = 1/2 [[1,1,1],[1,-1,-1],[-1,1,-1],[-1,-1,1]].
 // P1 shape gradients satisfy grad N = q (q^T grad N), so the element Hessian is
@@ -734,9 +731,6 @@ template <typename R, typename MA> __device__ __forceinline__ void blocks_from_q
 constexpr int kProjThreads = 64;
 constexpr int kProjStride = 127; // 45 (M) + 81 (V) + 1: odd stride, conflict-free 8-byte lanes
 
-template <typename R> struct Eps;
-template <> struct Eps<double> { static constexpr double v = 2.220446049250313e-16; };
-template <> struct Eps<float> { static constexpr float v = 1.1920929e-7f; };
 
 // Tangent sources of the projection pass: each forms the element's 9x9 tangent M in the q basis
 // (packed upper triangle into A; V is 81 values of per-thread scratch) and returns status bits.
@@ -889,93 +883,6 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
     if ((threadIdx.x & 31) == 0 && st) atomicOr(status, st);
 }
 
-// One round of parallel-ordered Jacobi on a symmetric 9x9 (round-robin ordering: in round r
-// index r idles and the pairs (r+i, r-i) mod 9, i = 1..4, are disjoint, so a sweep of 9 rounds
-// meets each of the 36 pairs once; Golub & Van Loan 8.5.3 and 8.6 for the ordering). The four
-// rotations (Alg. 8.4.1 sym.schur2) are computed from the same A, i.e. four independent
-// dependency chains, and applied together as A <- J^T A J with J the block rotation, then
-// accumulated into V's columns.
-// A is kept relabelled by the round, A_cur(i, j) = A((i + r) mod 9, (j + r) mod 9), so every
-// round rotates the fixed pairs (1, 8), (2, 7), (3, 6), (4, 5) of A_cur with literal register
-// indices; after the round A_cur is shifted by one label. The loop over rounds therefore stays
-// a loop (a fully unrolled sweep of nine rounds overflows the instruction cache). V (register
-// array, VREG) is shifted with A; V in shared memory is addressed with the round's offset.
-template <typename R, bool VREG, typename VA>
-__device__ __forceinline__ void jacobi_round(R (&A)[45], VA& V, const int rd) {
-    R c[4], sn[4], t[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int P = k + 1, Q = 8 - k;
-        // t = sign(tau) / (|tau| + sqrt(1 + tau^2)), tau = d / a2, written with one square
-        // root and one division: t = +-|a2| / (|d| + sqrt(d^2 + a2^2)) (A is scaled to
-        // max |entry| <= 1, so the squares cannot overflow); c = 1 / sqrt(1 + t^2), s = t c.
-        const R apq = A[sym9(P, Q)];
-        const R d = A[sym9(Q, Q)] - A[sym9(P, P)], a2 = R(2) * apq;
-        const R num = d > R(0) ? a2 : (d < R(0) ? -a2 : fabs(a2));
-        const R den = fabs(d) + sqrt(d * d + a2 * a2);
-        // den is 0 only when d = 0 and a2^2 underflows (FP32: |apq| below ~1e-23 of the largest
-        // entry): the pair is already diagonal to far below the sweep threshold, so no rotation.
-        t[k] = (apq == R(0) || !(den > R(0))) ? R(0) : num / den;
-        c[k] = rsqrt(R(1) + t[k] * t[k]);
-        sn[k] = t[k] * c[k];
-    }
-    // Off-diagonal 2x2 blocks between pairs k < l: R_k^T A_kl R_l, R = [[c, s], [-s, c]].
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int l = k + 1; l < 4; ++l) {
-            const int Pk = k + 1, Qk = 8 - k, Pl = l + 1, Ql = 8 - l;
-            const R a = A[sym9(Pk, Pl)], b = A[sym9(Pk, Ql)];
-            const R d = A[sym9(Qk, Pl)], e = A[sym9(Qk, Ql)];
-            const R a1 = c[l] * a - sn[l] * b, b1 = sn[l] * a + c[l] * b;
-            const R d1 = c[l] * d - sn[l] * e, e1 = sn[l] * d + c[l] * e;
-            A[sym9(Pk, Pl)] = c[k] * a1 - sn[k] * d1;
-            A[sym9(Pk, Ql)] = c[k] * b1 - sn[k] * e1;
-            A[sym9(Qk, Pl)] = sn[k] * a1 + c[k] * d1;
-            A[sym9(Qk, Ql)] = sn[k] * b1 + c[k] * e1;
-        }
-    // The idle index 0 against each pair, then each pair's own 2x2 block, then V.
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int P = k + 1, Q = 8 - k;
-        const R a = A[sym9(0, P)], b = A[sym9(0, Q)];
-        A[sym9(0, P)] = c[k] * a - sn[k] * b;
-        A[sym9(0, Q)] = sn[k] * a + c[k] * b;
-        const R apq = A[sym9(P, Q)];
-        A[sym9(P, P)] -= t[k] * apq;
-        A[sym9(Q, Q)] += t[k] * apq;
-        A[sym9(P, Q)] = R(0);
-        int vp_col = P, vq_col = Q;
-        if constexpr (!VREG) {
-            vp_col = P + rd >= 9 ? P + rd - 9 : P + rd;
-            vq_col = Q + rd >= 9 ? Q + rd - 9 : Q + rd;
-        }
-#pragma unroll
-        for (int x = 0; x < 9; ++x) {
-            const R vp = V[9 * x + vp_col], vq = V[9 * x + vq_col];
-            V[9 * x + vp_col] = c[k] * vp - sn[k] * vq;
-            V[9 * x + vq_col] = sn[k] * vp + c[k] * vq;
-        }
-    }
-    // Relabel for the next round: A_next(i, j) = A_cur(i + 1, j + 1) (indices mod 9).
-    R B[45];
-#pragma unroll
-    for (int u = 0; u < 45; ++u) B[u] = A[u];
-#pragma unroll
-    for (int i = 0; i < 9; ++i)
-#pragma unroll
-        for (int j = i; j < 9; ++j) A[sym9(i, j)] = B[sym9((i + 1) % 9, (j + 1) % 9)];
-    if constexpr (VREG) {
-#pragma unroll
-        for (int x = 0; x < 9; ++x) {
-            const R v0 = V[9 * x];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) V[9 * x + j] = V[9 * x + j + 1];
-            V[9 * x + 8] = v0;
-        }
-    }
-}
-
 // Eigenvalue clamp of the listed elements' 9x9 tangents (parallel-ordered cyclic Jacobi):
 // M = V max(Lambda, 0) V^T, in place; grid-stride over the list whose length pass 1 counted.
 // One thread per element with the packed matrix and the rotations in registers; in FP64 the
@@ -984,54 +891,9 @@ __device__ __forceinline__ void jacobi_round(R (&A)[45], VA& V, const int rd) {
 template <typename R, bool VREG, typename VA>
 __device__ __forceinline__ void clamp9(R* __restrict__ out, VA& V) {
     R A[45];
-    R amax = 0;
 #pragma unroll
-    for (int t = 0; t < 45; ++t) {
-        A[t] = out[t];
-        amax = fmax(amax, fabs(A[t]));
-    }
-    // Exact power-of-two scaling to max |entry| in [0.5, 1): no overflow in the rotations.
-    int ex = 0;
-    if (amax > R(0) && amax < R(INFINITY)) frexp(amax, &ex);
-    const R down = ldexp(R(1), -ex), up = ldexp(R(1), ex);
-    R total = 0;
-#pragma unroll
-    for (int t = 0; t < 45; ++t) {
-        A[t] *= down;
-        total += A[t] * A[t];
-    }
-#pragma unroll
-    for (int t = 0; t < 81; ++t) V[t] = (t % 10 == 0) ? R(1) : R(0);
-    const R thr = R(16) * Eps<R>::v * Eps<R>::v * total;
-#pragma unroll 1
-    for (int sweep = 0; sweep < 20; ++sweep) {
-        R off = 0;
-#pragma unroll
-        for (int r = 0; r < 9; ++r)
-#pragma unroll
-            for (int c = r + 1; c < 9; ++c) off += A[sym9(r, c)] * A[sym9(r, c)];
-        if (!(off > thr)) break;
-#pragma unroll 1
-        for (int rd = 0; rd < 9; ++rd) jacobi_round<R, VREG>(A, V, rd);
-    }
-    R lam[9];
-#pragma unroll
-    for (int t = 0; t < 9; ++t) lam[t] = fmax(A[sym9(t, t)], R(0)) * up;
-#pragma unroll
-    for (int k = 0; k < 45; ++k) A[k] = R(0);
-    // M+ = sum_t lam_t v_t v_t^T, one eigenvector column at a time (A reused as the sum).
-#pragma unroll
-    for (int t = 0; t < 9; ++t) {
-        R col[9];
-#pragma unroll
-        for (int r = 0; r < 9; ++r) col[r] = V[9 * r + t];
-#pragma unroll
-        for (int r = 0; r < 9; ++r) {
-            const R lr = lam[t] * col[r];
-#pragma unroll
-            for (int c = r; c < 9; ++c) A[sym9(r, c)] += lr * col[c];
-        }
-    }
+    for (int t = 0; t < 45; ++t) A[t] = out[t];
+    clamp9_packed<R, VREG>(A, V);
     blocks_from_q<R>(A, out); // the clamped M's ten blocks replace M in the element's record
 }
 
@@ -1255,6 +1117,92 @@ __device__ __forceinline__ void diag_contrib<float>(float (&acc)[6], const float
     acc[5] = __fadd_rn(a45.y, mg);
 }
 
+// The element pass's outputs for element el: g_a = vol P grad N_a (with the gradient), and
+// h_a = F^-T grad N_a, vol lambda, vol p, vol mu grad N_a . grad N_b (with the Hessian), into the
+// component-major shared arrays. In FP32 pairs of outputs are formed with packed f32x2 operations,
+// each lane rounded as the scalar operation, so the values are bitwise those of the scalar form.
+template <typename R, bool WG, bool WH>
+__device__ __forceinline__ void tc_element_data(const Kin<R>& k, R p, R* ed, int el) {
+    using X = M<R>;
+    constexpr int E = kTcElems;
+    if constexpr (sizeof(R) == 4) {
+        if (WG) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                R P[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) P[j] = X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j]));
+#pragma unroll
+                for (int b0 = 0; b0 < 4; b0 += 2) {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        t = __ffma2_rn(make_float2(P[j], P[j]), make_float2(k.n[b0][j], k.n[b0 + 1][j]), t);
+                    t = __fmul2_rn(make_float2(k.vol, k.vol), t);
+                    ed[(kTcG + 3 * b0 + i) * E + el] = t.x;
+                    ed[(kTcG + 3 * (b0 + 1) + i) * E + el] = t.y;
+                }
+            }
+        }
+        if (WH) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int b0 = 0; b0 < 4; b0 += 2) {
+                    float2 t = __fmul2_rn(make_float2(k.FiT[3 * i], k.FiT[3 * i]), make_float2(k.n[b0][0], k.n[b0 + 1][0]));
+                    t = __ffma2_rn(make_float2(k.FiT[3 * i + 1], k.FiT[3 * i + 1]), make_float2(k.n[b0][1], k.n[b0 + 1][1]), t);
+                    t = __ffma2_rn(make_float2(k.FiT[3 * i + 2], k.FiT[3 * i + 2]), make_float2(k.n[b0][2], k.n[b0 + 1][2]), t);
+                    ed[(kTcH + 3 * b0 + i) * E + el] = t.x;
+                    ed[(kTcH + 3 * (b0 + 1) + i) * E + el] = t.y;
+                }
+            ed[kTcL * E + el] = X::mul(k.vol, k.lam);
+            ed[kTcP * E + el] = X::mul(k.vol, p);
+            const R mv = X::mul(k.vol, k.mu);
+            constexpr int px[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3}, py[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+#pragma unroll
+            for (int c = 0; c < 10; c += 2) {
+                const int x1 = px[c], y1 = py[c], x2 = px[c + 1], y2 = py[c + 1];
+                float2 t = __fmul2_rn(make_float2(k.n[x1][0], k.n[x2][0]), make_float2(k.n[y1][0], k.n[y2][0]));
+                t = __ffma2_rn(make_float2(k.n[x1][1], k.n[x2][1]), make_float2(k.n[y1][1], k.n[y2][1]), t);
+                t = __ffma2_rn(make_float2(k.n[x1][2], k.n[x2][2]), make_float2(k.n[y1][2], k.n[y2][2]), t);
+                t = __fmul2_rn(make_float2(mv, mv), t);
+                ed[(kTcCC + pair10(x1, y1)) * E + el] = t.x;
+                ed[(kTcCC + pair10(x2, y2)) * E + el] = t.y;
+            }
+        }
+    } else {
+        if (WG) {
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    R sum = 0;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        sum = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[bb][j], sum);
+                    ed[(kTcG + 3 * bb + i) * E + el] = k.vol * sum;
+                }
+        }
+        if (WH) {
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    ed[(kTcH + 3 * bb + i) * E + el] = X::fma(
+                        k.FiT[3 * i + 2], k.n[bb][2], X::fma(k.FiT[3 * i + 1], k.n[bb][1], X::mul(k.FiT[3 * i], k.n[bb][0])));
+            ed[kTcL * E + el] = X::mul(k.vol, k.lam);
+            ed[kTcP * E + el] = X::mul(k.vol, p);
+            const R mv = X::mul(k.vol, k.mu);
+#pragma unroll
+            for (int xx = 0; xx < 4; ++xx)
+#pragma unroll
+                for (int y = xx; y < 4; ++y)
+                    ed[(kTcCC + pair10(xx, y)) * E + el] = X::mul(
+                        mv, X::fma(k.n[xx][2], k.n[y][2], X::fma(k.n[xx][1], k.n[y][1], X::mul(k.n[xx][0], k.n[y][0]))));
+        }
+    }
+}
+
 // Staging index of entry (i, c) of the block at packed position pos (row offset so, block q,
 // row length nb): BSR and solver layouts keep blocks row-major one after the other, CSC keeps
 // the row's three scalar rows one after the other.
@@ -1430,35 +1378,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
                 if (a.elem_energy) a.elem_energy[e] = static_cast<double>(Ee);
             }
             const R p = X::fma(k.lam, k.logJ, -k.mu);
-            if (WG) {
-#pragma unroll
-                for (int bb = 0; bb < 4; ++bb)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        R sum = 0;
-#pragma unroll
-                        for (int j = 0; j < 3; ++j)
-                            sum = X::fma(X::fma(k.mu, k.F[3 * i + j], X::mul(p, k.FiT[3 * i + j])), k.n[bb][j], sum);
-                        ed[(kTcG + 3 * bb + i) * E + el] = k.vol * sum;
-                    }
-            }
-            if (WH) {
-#pragma unroll
-                for (int bb = 0; bb < 4; ++bb)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        ed[(kTcH + 3 * bb + i) * E + el] = X::fma(
-                            k.FiT[3 * i + 2], k.n[bb][2], X::fma(k.FiT[3 * i + 1], k.n[bb][1], X::mul(k.FiT[3 * i], k.n[bb][0])));
-                ed[kTcL * E + el] = X::mul(k.vol, k.lam);
-                ed[kTcP * E + el] = X::mul(k.vol, p);
-                const R mv = X::mul(k.vol, k.mu);
-#pragma unroll
-                for (int xx = 0; xx < 4; ++xx)
-#pragma unroll
-                    for (int y = xx; y < 4; ++y)
-                        ed[(kTcCC + pair10(xx, y)) * E + el] = X::mul(
-                            mv, X::fma(k.n[xx][2], k.n[y][2], X::fma(k.n[xx][1], k.n[y][1], X::mul(k.n[xx][0], k.n[y][0]))));
-            }
+            tc_element_data<R, WG, WH>(k, p, ed, el);
         }
         // Energy of the cluster's own elements: fixed thread order, fixed tree.
 #pragma unroll

@@ -1,7 +1,9 @@
-// Test harness: the GPU's element projection (litepgo_b200/csrc/lpg_psd.h) run on the host by a
-// team of one lane, for tests/test_psd_jacobi.py (built there with g++ into a temporary folder).
+// Test harness: the GPU's element projections run on the host, for tests/test_psd_jacobi.py (built
+// there with g++ into a temporary folder): the hex projection (litepgo_b200/csrc/lpg_psd.h) by a
+// team of one lane, and the tet tangent's 9x9 clamp (litepgo_b200/csrc/lpg_clamp9.h).
 #include <vector>
 
+#include "lpg_clamp9.h"
 #include "lpg_psd.h"
 
 namespace {
@@ -51,4 +53,22 @@ extern "C" int psd_semidefinite9f(const float* V, float tol) {
     float W[81];
     for (int i = 0; i < 81; ++i) W[i] = V[i];
     return lpg::semidefinite_ldlt<9>(W, tol) ? 1 : 0;
+}
+
+// The 9x9 clamp of the row-major symmetric matrix in (upper triangle used) into out, in FP32
+// (fp32 != 0) or FP64, as clamp_kernel runs it.
+template <typename R> void clamp9_run(const double* in, double* out) {
+    R A[45];
+    R V[81];
+    for (int r = 0; r < 9; ++r)
+        for (int c = r; c < 9; ++c) A[lpg::sym9(r, c)] = static_cast<R>(in[9 * r + c]);
+    lpg::clamp9_packed<R, true>(A, V);
+    for (int r = 0; r < 9; ++r)
+        for (int c = 0; c < 9; ++c) out[9 * r + c] = static_cast<double>(A[lpg::sym9(r, c)]);
+}
+extern "C" void clamp9_host(int fp32, const double* in, double* out) {
+    if (fp32)
+        clamp9_run<float>(in, out);
+    else
+        clamp9_run<double>(in, out);
 }

@@ -28,6 +28,7 @@ def psd(tmp_path_factory):
     lib.psd_round_pairs.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.psd_semidefinite9.argtypes = [_dp, ctypes.c_double]
     lib.psd_semidefinite9f.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_float]
+    lib.clamp9_host.argtypes = [ctypes.c_int, _dp, _dp]
 
     def run(H):
         H = np.ascontiguousarray(H, dtype=np.float64)
@@ -167,3 +168,39 @@ def test_semidefinite_test_in_fp32(psd):
     assert run(np.r_[np.zeros(3), np.linspace(0.1, 2, 6)]) == 1
     assert run(np.r_[-1e-2, np.linspace(0.1, 2, 8)]) == 0
 
+
+
+def clamp9(psd, M, fp32):
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    out = np.empty((9, 9))
+    psd.lib.clamp9_host(1 if fp32 else 0, M.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
+    return out
+
+
+@pytest.mark.parametrize("fp32,tol", [(False, 1e-13), (True, 2e-6)])
+def test_tet_tangent_clamp_matches_the_oracle(psd, fp32, tol):
+    """The tet tangent's 9x9 clamp (lpg_clamp9.h, run by clamp_kernel) against the oracle's
+    eigensolver projection, on indefinite neo-Hookean tangents and random symmetric matrices."""
+    rng = np.random.default_rng(21)
+    mats = [nh_tangent_rowmajor(np.diag([1.0, 1.0, s]) + 0.03 * rng.standard_normal((3, 3)), 1.4e5, 3.4e4)
+            for s in (0.6, 1.6, 0.35)]
+    mats += [(lambda B: 0.5 * (B + B.T))(rng.standard_normal((9, 9)) * 10.0 ** k) for k in (-6, 0, 6)]
+    for M in mats:
+        M = np.asarray(M, dtype=np.float32 if fp32 else np.float64).astype(np.float64)
+        ref = oracle.project_psd(M)
+        P = clamp9(psd, M, fp32)
+        assert np.all(np.isfinite(P))
+        assert np.linalg.norm(P - ref) <= tol * np.linalg.norm(M)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_tet_tangent_clamp_with_an_underflowing_rotation(psd, fp32):
+    """Two equal diagonal entries coupled by an off-diagonal entry so small (1e-30 of the largest)
+    that d^2 + (2 a_pq)^2 underflows in FP32: the pair is left unrotated instead of producing a
+    NaN, and the clamp still matches the oracle's."""
+    M = np.diag([1.0, -0.5, 0.25, 0.25, 2.0, -1.0, 0.5, 3.0, 0.75])
+    M[2, 3] = M[3, 2] = 1e-30
+    M[0, 4] = M[4, 0] = 0.1
+    P = clamp9(psd, M, fp32)
+    assert np.all(np.isfinite(P))
+    assert np.linalg.norm(P - oracle.project_psd(M)) <= (2e-6 if fp32 else 1e-13) * np.linalg.norm(M)
