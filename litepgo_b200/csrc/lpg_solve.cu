@@ -1659,6 +1659,10 @@ __global__ void __launch_bounds__(kThreads, (SpmvCfg<R, 0>::minb))
     const int row = __ldg(m.sell_row + 32 * static_cast<size_t>(c) + lane);
     const int mesh = row >= 0 ? __ldg(mov + row) : 0;
     const bool live = row >= 0 && !st.done[mesh];
+    // A chunk whose rows all belong to finished meshes does nothing: their products, p and
+    // row dots are read by no one (the update and the per-mesh reductions skip finished meshes),
+    // so the lockstep iterations after most meshes have converged cost only the live chunks.
+    if (!__any_sync(0xffffffffu, live)) return;
     const R beta = live ? static_cast<R>(st.beta[mesh]) : R(0);
     const int s0 = __ldg(m.sell_ptr + c);
     const int width = (__ldg(m.sell_ptr + c + 1) - s0) >> 5;
