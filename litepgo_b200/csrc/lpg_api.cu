@@ -234,7 +234,7 @@ const double* lpg_fem::stage_in(const double* p, int mem, DeviceBuffer& buf, siz
 
 void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int precision, int layout, void* dhess,
                          double* delem, cudaEvent_t ev_begin, cudaEvent_t ev_end, const int* emesh,
-                         const int* mesh_exact) {
+                         const int* mesh_exact, const unsigned char* tc_skip, const unsigned char* cl_skip) {
     if (hessian != LPG_HESSIAN_NONE && hessian != LPG_HESSIAN_EXACT && hessian != LPG_HESSIAN_PROJECTED)
         fail(LPG_EINVAL, "Energy: invalid Hessian kind");
     if (precision != LPG_PRECISION_F64 && precision != LPG_PRECISION_MIXED) fail(LPG_EINVAL, "invalid precision");
@@ -254,6 +254,8 @@ void lpg_fem::eval_async(const double* du, double* dgrad, int hessian, int preci
     a.ev_end = ev_end;
     const int pi = precision == LPG_PRECISION_F64 ? 0 : 1;
     a.cl_variant = tune.cl[pi];
+    a.tc_skip = tc_skip;
+    a.cl_skip = cl_skip;
     if (dm.K == 64) {
         const bool projected = hessian == LPG_HESSIAN_PROJECTED;
         const size_t T = static_cast<size_t>(dm.T);

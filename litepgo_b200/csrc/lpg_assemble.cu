@@ -371,11 +371,13 @@ __device__ double positive_det_step(const double* A, const double* dA, unsigned&
 
 __global__ void __launch_bounds__(256) feasible_kernel(const DevMesh m, const double* __restrict__ u,
                                                        const double* __restrict__ du, double* block_min,
-                                                       unsigned* status, double* per_elem) {
+                                                       unsigned* status, double* per_elem,
+                                                       const int* __restrict__ emesh, const int* __restrict__ mstate) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double alpha = 1.0;
     unsigned st = 0;
-    if (e < m.T) {
+    // Batched solves: an element of a finished mesh (state 2) is skipped (step 1, no constraint).
+    if (e < m.T && !(emesh != nullptr && mstate[emesh[e]] == 2)) {
         const int4 tv = __ldg(m.tets + e);
         const int vs[4] = {tv.x, tv.y, tv.z, tv.w};
         double rec[12];
@@ -849,10 +851,12 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const DevMesh m, 
     R* V = A + 45;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned st = 0;
-    if (e < m.T) {
+    // Per-mesh state of a batched solve: 0 projected, 1 exact, 2 finished (the element is skipped).
+    const int state = (e < m.T && emesh != nullptr) ? mesh_exact[emesh[e]] : 0;
+    if (e < m.T && state != 2) {
         st |= form_tangent<R>(src, m, e, A, V);
         // Elements of a mesh marked exact keep their tangent unclamped (the Exact Hessian).
-        const bool keep = keeps_exact(src) || (emesh != nullptr && mesh_exact[emesh[e]] != 0);
+        const bool keep = keeps_exact(src) || state == 1;
         // Positive semi-definiteness test: LDL^T with diagonal pivoting on a copy in the V area
         // (row-major 9x9). Pivots above tol are eliminated; once none is left, M is semi-definite
         // if the remaining Schur complement is below tol everywhere (tol = 64 eps max|diag M|:
@@ -1231,9 +1235,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 struct TcBounds {
     int e0 = 0, ne = 0, v0 = 0, nv = 0, i0 = 0, ni = 0, nd = 0, n0 = 0, nn = 0, r0 = 0, nr = 0;
 };
-constexpr int kTcFields = 11;
-__device__ __forceinline__ int tc_field(const DevMesh& m, int cl, int q) {
+constexpr int kTcFields = 12; // the bounds, then the cluster's skip flag (batched solves)
+__device__ __forceinline__ int tc_field(const DevMesh& m, const unsigned char* skip, int cl, int q) {
     if (cl >= m.tc_ncl) return 0;
+    if (q == 11) return skip != nullptr && __ldg(skip + cl) != 0;
     auto span = [&](const int32_t* ptr, bool count) {
         const int lo = __ldg(ptr + cl);
         return count ? __ldg(ptr + cl + 1) - lo : lo;
@@ -1248,8 +1253,10 @@ __device__ __forceinline__ int tc_field(const DevMesh& m, int cl, int q) {
     default: return 0;
     }
 }
+// A skipped cluster has empty bounds: nothing is staged, evaluated or written.
 __device__ __forceinline__ TcBounds tc_bounds(const int* f) {
     TcBounds b;
+    if (f[11]) return b;
     b.e0 = f[0], b.ne = f[1], b.v0 = f[2], b.nv = f[3], b.i0 = f[4], b.ni = f[5];
     b.nd = f[6], b.n0 = f[7], b.nn = f[8], b.r0 = f[9], b.nr = f[10];
     return b;
@@ -1332,7 +1339,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     {
         int f[kTcFields];
 #pragma unroll
-        for (int q = 0; q < kTcFields; ++q) f[q] = tc_field(m, cl, q);
+        for (int q = 0; q < kTcFields; ++q) f[q] = tc_field(m, a.tc_skip, cl, q);
         b = tc_bounds(f);
     }
     TcIdx x;
@@ -1340,7 +1347,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     R r12[12];
     int rowv[kTcRowInts] = {0, 0, 0, 0, 0};
     tc_issue<R, ITEMS>(m, a.u, b, x, tid, sell, su, sitems, sents, r12, rowv);
-    int ahead = tid < kTcFields ? tc_field(m, cl + grid, tid) : 0;
+    int ahead = tid < kTcFields ? tc_field(m, a.tc_skip, cl + grid, tid) : 0;
     int ne = b.ne, ni = WH ? b.ni : b.nd, nr = b.nr, ndc = b.nd;
     for (int buf = 0; cl < m.tc_ncl; cl += grid, buf ^= 1) {
         int* rows = srow + buf * kTcRows * kTcRowInts;
@@ -1394,7 +1401,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         // The next cluster's indices, and the bounds of the one after, arrive while the item pass
         // runs.
         tc_load_idx(m, tc_bounds(s_hdr[buf]), tid, x);
-        if (tid < kTcFields) ahead = tc_field(m, cl + 2 * grid, tid);
+        if (tid < kTcFields) ahead = tc_field(m, a.tc_skip, cl + 2 * grid, tid);
         if (ITEMS) {
             // Item pass. The nd diagonal items (the first nd) are summed by lane pairs, each lane
             // over half the contributor list in ascending order, the two halves added by a
@@ -1608,6 +1615,7 @@ __global__ void __launch_bounds__(kClThreads) block_gather_kernel(const DevMesh 
     const int tid = threadIdx.x, bd = blockDim.x;
     unsigned st = 0;
     for (int cl = blockIdx.x; cl < m.ncl; cl += gridDim.x) {
+        if (a.cl_skip != nullptr && __ldg(a.cl_skip + cl) != 0) continue; // its mesh has finished
         const int s0 = __ldg(m.cl_slot_ptr + cl), ns = __ldg(m.cl_slot_ptr + cl + 1) - s0;
         const int eb = __ldg(m.cl_ent_ptr + cl), n16 = (__ldg(m.cl_ent_ptr + cl + 1) - eb) / 8;
         for (int i = tid; i < ns; i += bd) {
@@ -3209,7 +3217,8 @@ void launch_clamp_sample(int precision, void* proj, int* list, int n, cudaStream
 int feasible_blocks(const DevMesh& m) { return (m.T + 255) / 256; }
 
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
-                     double* alpha, unsigned* status, cudaStream_t s, double* per_elem) {
+                     double* alpha, unsigned* status, cudaStream_t s, double* per_elem, const int* emesh,
+                     const int* mstate) {
     if (m.K != 4 && per_elem) fail(LPG_EINVAL, "per-element feasible steps are available for tet meshes only");
     if (m.K == 8) {
         launch_hex_feasible(m, u, du, block_min, nblocks, alpha, status, s);
@@ -3221,7 +3230,7 @@ void launch_feasible(const DevMesh& m, const double* u, const double* du, double
         LPG_CUDA(cudaGetLastError());
         return;
     }
-    if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status, per_elem);
+    if (nblocks > 0) feasible_kernel<<<nblocks, 256, 0, s>>>(m, u, du, block_min, status, per_elem, emesh, mstate);
     min_kernel<<<1, 1024, 0, s>>>(block_min, nblocks, alpha);
     LPG_CUDA(cudaGetLastError());
 }

@@ -231,6 +231,10 @@ struct EvalArgs {
     unsigned* status = nullptr;    // device status word
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr; // optional: bracket the assembly kernel
     int cl_variant = 0; // register-budget variant of the Exact-Hessian cluster kernel (autotuner)
+    // Batched solves: per-cluster flags (tet clusters, block-gather clusters) of clusters whose
+    // mesh has finished; such a cluster writes nothing. Null: every cluster runs.
+    const unsigned char* tc_skip = nullptr;
+    const unsigned char* cl_skip = nullptr;
 };
 
 // Autotuned launch variants (register budgets and unroll depths; every variant of a kernel
@@ -272,8 +276,11 @@ constexpr int kHexRecord = 324;
 constexpr int kHermiteRecord = 2080 * 9; // tricubic Hermite hex: 64 nodes, 2080 blocks (a <= b)
 constexpr int kHermiteTable = 193;       // per quadrature point: 64 x 3 reference derivatives, weight
 // per_elem (T doubles, optional) receives each element's step.
+// With emesh / mstate (batched solves: element -> mesh, per-mesh state), the elements of a mesh in
+// state 2 (finished) are skipped.
 void launch_feasible(const DevMesh& m, const double* u, const double* du, double* block_min, int nblocks,
-                     double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr);
+                     double* alpha, unsigned* status, cudaStream_t s, double* per_elem = nullptr,
+                     const int* emesh = nullptr, const int* mstate = nullptr);
 int feasible_blocks(const DevMesh& m);
 void launch_force_vjp(const DevMesh& m, const double* u, const double* w, double* out_per_elem, unsigned* status,
                       cudaStream_t s);

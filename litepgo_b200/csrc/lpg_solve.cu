@@ -1796,10 +1796,23 @@ __global__ void __launch_bounds__(256) pcg_b_beta(BatchPcg st, const double* __r
 }
 
 // Device arrays of one batched solve.
+// Skip flags of the two cluster plans from the per-mesh states (2 = finished): a cluster's rows
+// all belong to the mesh of its first row (meshes are disconnected, clusters grow through
+// vertex adjacency).
+__global__ void cluster_skip_kernel(const int* __restrict__ row_ptr, const int* __restrict__ rows, int ncl,
+                                    const int* __restrict__ mov, const int* __restrict__ mstate,
+                                    unsigned char* __restrict__ skip) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncl) return;
+    const int r0 = __ldg(row_ptr + c);
+    skip[c] = (__ldg(row_ptr + c + 1) > r0 && mstate[__ldg(mov + __ldg(rows + r0))] == 2) ? 1 : 0;
+}
+
 struct BatchDev {
     int M = 0;
     int *voff = nullptr, *eoff = nullptr, *mov = nullptr, *emesh = nullptr;
     int *act = nullptr, *take = nullptr, *exact = nullptr;
+    unsigned char *tc_skip = nullptr, *cl_skip = nullptr;
     double *stats = nullptr, *esum = nullptr, *fdot = nullptr, *amin = nullptr, *alpha = nullptr, *tol = nullptr;
     double *rowdot = nullptr, *rowdot2 = nullptr, *elem = nullptr;
     BatchPcg pcg{};
@@ -1832,7 +1845,8 @@ struct BatchSolver {
     }
     // Per-mesh energy at x: element energies summed per mesh, minus f . x.
     std::vector<double> energies(const double* x, const double* f, double* g, int hk, int precision, void* K) {
-        h.eval_async(x, g, hk, precision, kLayoutSell, K, d.elem, nullptr, nullptr, d.emesh, d.exact);
+        h.eval_async(x, g, hk, precision, kLayoutSell, K, d.elem, nullptr, nullptr, d.emesh, d.exact, d.tc_skip,
+                     d.cl_skip);
         seg_elem<<<M, 256, 0, s>>>(d.elem, d.eoff, 0, d.esum);
         LPG_CUDA(cudaGetLastError());
         raise_status(h.take_status());
@@ -2025,6 +2039,8 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
     d.take = h.bt_int[4].as<int>(M);
     d.emesh = h.bt_int[6].as<int>(std::max(T, 1));
     d.exact = h.bt_int[7].as<int>(M);
+    d.tc_skip = h.bt_skip[0].as<unsigned char>(static_cast<size_t>(std::max(h.dm.tc_ncl, 1)));
+    d.cl_skip = h.bt_skip[1].as<unsigned char>(static_cast<size_t>(std::max(h.dm.ncl, 1)));
     int* pcg_ints = h.bt_int[5].as<int>(3 * static_cast<size_t>(M) + 1);
     d.pcg.done = pcg_ints;
     d.pcg.iters = pcg_ints + M + 1;
@@ -2102,7 +2118,21 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
     std::vector<int> exact(M, o.hessian == LPG_HESSIAN_EXACT ? 1 : 0);
     int it = 0;
     for (;; ++it) {
-        B.up(d.exact, exact);
+        // Per-mesh state of this iteration's evaluations: 0 projected, 1 exact, 2 finished (its
+        // elements and clusters are skipped; its results were recorded when it finished).
+        {
+            std::vector<int> state(exact);
+            for (int m = 0; m < M; ++m)
+                if (status[m] >= 0) state[m] = 2;
+            B.up(d.exact, state);
+            if (h.dm.tc_ncl > 0)
+                cluster_skip_kernel<<<grid(static_cast<size_t>(h.dm.tc_ncl)), kThreads, 0, s>>>(
+                    h.dm.tc_row_ptr, h.dm.tc_rows, h.dm.tc_ncl, d.mov, d.exact, d.tc_skip);
+            if (h.dm.ncl > 0)
+                cluster_skip_kernel<<<grid(static_cast<size_t>(h.dm.ncl)), kThreads, 0, s>>>(
+                    h.dm.cl_row_ptr, h.dm.cl_rows, h.dm.ncl, d.mov, d.exact, d.cl_skip);
+            LPG_CUDA(cudaGetLastError());
+        }
         bool all_exact = true;
         for (int m = 0; m < M; ++m) all_exact = all_exact && (exact[m] || !act[m]);
         const int hk = all_exact ? LPG_HESSIAN_EXACT : LPG_HESSIAN_PROJECTED;
@@ -2111,11 +2141,11 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
         if (f) load_gradient<<<grid(n), kThreads, 0, s>>>(g, f, n);
         const auto gs = B.stats(g, nullptr, mask);
         for (int m = 0; m < M; ++m) {
+            if (status[m] >= 0) continue; // finished: skipped by this iteration's evaluation
             E[m] = e[m];
             g2[m] = std::sqrt(gs[4 * m + 1]);
             gmax[m] = gs[4 * m + 2];
             if (g0[m] < 0) g0[m] = g2[m];
-            if (status[m] >= 0) continue;
             if (!act[m]) {
                 status[m] = 0;
                 secs[m] = elapsed();
@@ -2135,7 +2165,7 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
         if (!f64) {
             // The flags of this iteration's start (d.exact), as the FP64 path uses.
             h.eval_async(x, nullptr, hk, LPG_PRECISION_MIXED, kLayoutSell, K, nullptr, nullptr, nullptr, d.emesh,
-                         d.exact);
+                         d.exact, d.tc_skip, d.cl_skip);
             raise_status(h.take_status());
         }
         // Descent directions: per-mesh PCG on the block-diagonal system, forcing term per mesh.
@@ -2170,7 +2200,7 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
         }
         for (int m = 0; m < M; ++m) gd[m] = gds[4 * m];
         // Line search per mesh from its feasible step.
-        launch_feasible(h.dm, x, dir, bm, nfeas, al, h.d_status.as<unsigned>(1), s, d.elem);
+        launch_feasible(h.dm, x, dir, bm, nfeas, al, h.d_status.as<unsigned>(1), s, d.elem, d.emesh, d.exact);
         seg_elem<<<M, 256, 0, s>>>(d.elem, d.eoff, 1, d.amin);
         raise_status(h.take_status());
         std::vector<double> amin;

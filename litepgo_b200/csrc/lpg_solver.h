@@ -41,7 +41,7 @@ struct lpg_fem {
     lpg::DeviceBuffer b_cl[11]; // assembly clusters
     lpg::DeviceBuffer b_tc[13]; // tet assembly clusters
     lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers
-    lpg::DeviceBuffer bt_int[8], bt_dbl[4]; // batched Newton
+    lpg::DeviceBuffer bt_int[8], bt_dbl[4], bt_skip[2]; // batched Newton (bt_skip: per-cluster skip flags)
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_plist, d_pcount; // elements listed for the projection's eigenvalue clamp
     lpg::DeviceBuffer d_mat[6];          // material outputs (W, P, A), per-element energies, F and G
@@ -64,7 +64,8 @@ struct lpg_fem {
     // Enqueues one evaluation on the handle's stream (no synchronisation).
     void eval_async(const double* du, double* dgrad, int hessian, int precision, int layout, void* dhess,
                     double* delem, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
-                    const int* emesh = nullptr, const int* mesh_exact = nullptr);
+                    const int* emesh = nullptr, const int* mesh_exact = nullptr,
+                    const unsigned char* tc_skip = nullptr, const unsigned char* cl_skip = nullptr);
 };
 
 namespace lpg {
