@@ -66,9 +66,6 @@ __device__ __forceinline__ void pdl_wait_then_release() {
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
-// L2 prefetch of the line holding p (issued before griddepcontrol.wait for data that the kernel
-// being waited for does not write, so the fetch overlaps that kernel's last blocks).
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 __device__ __forceinline__ double block_max(double v, double* sh) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
@@ -278,22 +275,7 @@ __global__ void __launch_bounds__(kThreads, (SpmvCfg<TK, VAR>::minb)) spmv_sell(
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
     using A = typename std::conditional<(sizeof(TK) == 4 && sizeof(TV) == 4), float, double>::type;
-    if (PCG) {
-        // The matrix is constant during the solve: fetch this warp's first chunk's first slots
-        // into L2 while the previous kernel finishes.
-        const int c0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        if (c0 < m.n_sell) {
-            const int ln = threadIdx.x & 31, s0 = __ldg(m.sell_ptr + c0);
-            const int w = (__ldg(m.sell_ptr + c0 + 1) - s0) >> 5, b0 = __ldg(m.sell_bptr + c0);
-            const int bw = (__ldg(m.sell_bptr + c0 + 1) - b0) >> 5;
-            for (int q = 0; q < w && q < 2; ++q) {
-                prefetch_l2(m.sell_col + s0 + 32 * q + ln);
-                if (ln < 9) prefetch_l2(val + 9 * static_cast<size_t>(s0) + 288 * static_cast<size_t>(q) + 32 * ln);
-            }
-            for (int q = 0; q < bw && q < 2; ++q) prefetch_l2(m.sell_bref + b0 + 32 * q + ln);
-        }
-        pdl_wait_then_release();
-    }
+    if (PCG) pdl_wait_then_release();
     if (PCG && st->done) return;
     const TV beta = PCG ? static_cast<TV>(st->beta) : TV(0);
     const int lane = threadIdx.x & 31;
@@ -561,16 +543,6 @@ __global__ void __launch_bounds__(kThreads) pcg_update(PcgState* st, const R* __
                                                        double* part) {
     __shared__ double sh[2 * (kThreads / 32)];
     __shared__ bool last;
-    {
-        // x, r (from the update before) and the preconditioner are not written by the SpMV this
-        // kernel follows: fetch this thread's first vertex's into L2 while it finishes.
-        const int v0 = blockIdx.x * blockDim.x + threadIdx.x;
-        if (v0 < V) {
-            prefetch_l2(x + 4 * static_cast<size_t>(v0));
-            prefetch_l2(r + 4 * static_cast<size_t>(v0));
-            prefetch_l2(dinv + 12 * static_cast<size_t>(v0));
-        }
-    }
     pdl_wait_then_release();
     if (st->done) return;
     const R alpha = static_cast<R>(st->alpha);
