@@ -1049,18 +1049,13 @@ template <typename R> constexpr size_t tc_ed_bytes() {
     return static_cast<size_t>(kTcComp) * kTcElems * sizeof(R);
 }
 static_assert(3 * kTcVerts * sizeof(double) <= tc_ed_bytes<float>(), "staged displacements fit the element data");
-// Where the staged displacements live: in FP32 in a region of their own (3 blocks per SM still
-// fit), so the element pass needs no barrier between reading them and writing element data; in
-// FP64 in the element data's first bytes (two blocks per SM only fit that way).
-template <typename R> constexpr bool tc_su_apart() { return sizeof(R) == 4; }
 // Shared memory: reduction scratch (32 doubles), the element data (whose first 3 kTcVerts
 // doubles hold the staged displacements until the element pass has read them), the output
 // staging, the item table, the contributor lists and two buffers of owned-row words.
 template <typename R> constexpr size_t tc_smem_bytes() {
     return 32 * sizeof(double) + tc_ed_bytes<R>() + static_cast<size_t>(kTcVals) * sizeof(R) +
            static_cast<size_t>(kTcItems) * sizeof(uint4) + static_cast<size_t>(kTcEnts) * sizeof(uint16_t) +
-           2 * static_cast<size_t>(kTcRows) * kTcRowInts * sizeof(int) +
-           (tc_su_apart<R>() ? 3 * static_cast<size_t>(kTcVerts) * sizeof(double) : 0);
+           2 * static_cast<size_t>(kTcRows) * kTcRowInts * sizeof(int);
 }
 
 // One contributor of an edge block: acc(i, q) = B_q hb_i + (A_i hb_q + acc(i, q)) (A = vol lambda
@@ -1326,13 +1321,11 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* red = reinterpret_cast<double*>(smem_raw);
     R* ed = reinterpret_cast<R*>(smem_raw + 32 * sizeof(double));
+    double* su = reinterpret_cast<double*>(ed); // [nv][3], until the element pass has read it
     R* stage = ed + kTcComp * E;
     uint4* sitems = reinterpret_cast<uint4*>(stage + kTcVals);
     uint16_t* sents = reinterpret_cast<uint16_t*>(sitems + kTcItems);
     int* srow = reinterpret_cast<int*>(sents + kTcEnts);
-    // [nv][3] staged displacements (see tc_su_apart)
-    double* su = tc_su_apart<R>() ? reinterpret_cast<double*>(srow + 2 * kTcRows * kTcRowInts)
-                                  : reinterpret_cast<double*>(ed);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     HT* hout = reinterpret_cast<HT*>(a.hess);
     const bool csc = a.layout == LPG_LAYOUT_CSC, sell = a.layout == kLayoutSell;
@@ -1379,7 +1372,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
             }
             in_ok = edge_differences<R>(uu, Ds);
         }
-        if (!tc_su_apart<R>()) __syncthreads(); // the displacements are read; their memory holds element data from here
+        __syncthreads(); // the displacements are read; their memory holds element data from here
         double eacc = 0;
         if (tid < ne && (ITEMS || (ew >> 31))) {
             const int el = tid;
