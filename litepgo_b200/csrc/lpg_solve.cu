@@ -1652,90 +1652,75 @@ template <typename R>
 __global__ void __launch_bounds__(kThreads, (SpmvCfg<R, 0>::minb))
     spmv_sell_batch(const DevMesh m, const R* __restrict__ val, const R* __restrict__ z, const R* __restrict__ p_old,
                     const R* __restrict__ mask, R* __restrict__ y, R* __restrict__ p_new, BatchPcg st,
-                    const int* __restrict__ mov, double* __restrict__ rowdot, const int* __restrict__ chunks,
-                    const int* __restrict__ nchunks) {
-    const int lane = threadIdx.x & 31;
-    const int nw = gridDim.x * (blockDim.x >> 5), nc = *nchunks;
-    // The chunks holding rows of the meshes of this solve (any order: every row is its own sum).
-    for (int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); idx < nc; idx += nw) {
-        const int c = __ldg(chunks + idx);
-        const int row = __ldg(m.sell_row + 32 * static_cast<size_t>(c) + lane);
-        const int mesh = row >= 0 ? __ldg(mov + row) : 0;
-        const bool live = row >= 0 && !st.done[mesh];
-        // A chunk whose rows all belong to meshes whose PCG has finished does nothing: their
-        // products, p and row dots are read by no one.
-        if (!__any_sync(0xffffffffu, live)) continue;
-        const R beta = live ? static_cast<R>(st.beta[mesh]) : R(0);
-        const int s0 = __ldg(m.sell_ptr + c);
-        const int width = (__ldg(m.sell_ptr + c + 1) - s0) >> 5;
-        const int* cp = m.sell_col + s0 + lane;
-        const R* vp = val + 9 * static_cast<size_t>(s0) + lane;
-        R a0 = 0, a1 = 0, a2 = 0;
-        // A block's rows and columns belong to one mesh, so the row's beta applies to its columns.
-        auto gather = [&](size_t col, R xv[3]) {
-            R xz[3], xp[3];
-            ld3<4>(z, col, xz);
-            ld3<4>(p_old, col, xp);
-#pragma unroll
-            for (int i = 0; i < 3; ++i) xv[i] = xz[i] + beta * xp[i];
-        };
-#pragma unroll (SpmvCfg<R, 0>::unroll)
-        for (int q = 0; q < width; ++q) {
-            R xv[3];
-            gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
-            const R* vq = vp + 288 * static_cast<size_t>(q);
-            R kv[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) kv[e] = __ldg(vq + 32 * e);
-            a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
-            a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
-            a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
-        }
-        const int b0 = __ldg(m.sell_bptr + c);
-        const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
-        const int2* bp = m.sell_bref + b0 + lane;
-#pragma unroll (SpmvCfg<R, 0>::unroll)
-        for (int q = 0; q < bwidth; ++q) {
-            const int2 ref = __ldg(bp + 32 * q);
-            R xv[3];
-            gather(static_cast<size_t>(ref.y), xv);
-            const R* vq = val + static_cast<size_t>(ref.x);
-            R kv[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) kv[e] = __ldg(vq + 32 * e);
-            a0 += kv[0] * xv[0] + kv[3] * xv[1] + kv[6] * xv[2];
-            a1 += kv[1] * xv[0] + kv[4] * xv[1] + kv[7] * xv[2];
-            a2 += kv[2] * xv[0] + kv[5] * xv[1] + kv[8] * xv[2];
-        }
-        if (row < 0) continue;
-        const size_t o = static_cast<size_t>(row);
-        R mv[3], xz[3], xp[3];
-        ld3<4>(mask, o, mv);
-        ld3<4>(z, o, xz);
-        ld3<4>(p_old, o, xp);
-        const R yv[3] = {mv[0] * a0, mv[1] * a1, mv[2] * a2};
-        st3<4, R>(y, o, yv[0], yv[1], yv[2]);
-        R pv[3];
-        double dot = 0;
-        for (int i = 0; i < 3; ++i) {
-            pv[i] = xz[i] + beta * xp[i];
-            dot += static_cast<double>(pv[i]) * static_cast<double>(yv[i]);
-        }
-        st3<4, R>(p_new, o, pv[0], pv[1], pv[2]);
-        rowdot[o] = live ? dot : 0.0;
-    }
-}
-
-// The chunks of the sliced ELL holding a row of an active mesh, compacted into chunks[0 .. *count)
-// (*count zeroed before; the order is immaterial).
-__global__ void active_chunks_kernel(const DevMesh m, const int* __restrict__ mov, const int* __restrict__ act,
-                                     int* __restrict__ chunks, int* __restrict__ count) {
+                    const int* __restrict__ mov, double* __restrict__ rowdot) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= m.n_sell) return;
     const int row = __ldg(m.sell_row + 32 * static_cast<size_t>(c) + lane);
-    const bool live = row >= 0 && act[__ldg(mov + row)] != 0;
-    if (__any_sync(0xffffffffu, live) && lane == 0) chunks[atomicAdd(count, 1)] = c;
+    const int mesh = row >= 0 ? __ldg(mov + row) : 0;
+    const bool live = row >= 0 && !st.done[mesh];
+    // A chunk whose rows all belong to finished meshes does nothing: their products, p and
+    // row dots are read by no one (the update and the per-mesh reductions skip finished meshes),
+    // so the lockstep iterations after most meshes have converged cost only the live chunks.
+    if (!__any_sync(0xffffffffu, live)) return;
+    const R beta = live ? static_cast<R>(st.beta[mesh]) : R(0);
+    const int s0 = __ldg(m.sell_ptr + c);
+    const int width = (__ldg(m.sell_ptr + c + 1) - s0) >> 5;
+    const int* cp = m.sell_col + s0 + lane;
+    const R* vp = val + 9 * static_cast<size_t>(s0) + lane;
+    R a0 = 0, a1 = 0, a2 = 0;
+    // A block's rows and columns belong to one mesh, so the row's beta applies to its columns.
+    auto gather = [&](size_t col, R xv[3]) {
+        R xz[3], xp[3];
+        ld3<4>(z, col, xz);
+        ld3<4>(p_old, col, xp);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) xv[i] = xz[i] + beta * xp[i];
+    };
+#pragma unroll (SpmvCfg<R, 0>::unroll)
+    for (int q = 0; q < width; ++q) {
+        R xv[3];
+        gather(static_cast<size_t>(__ldg(cp + 32 * q)), xv);
+        const R* vq = vp + 288 * static_cast<size_t>(q);
+        R kv[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) kv[e] = __ldg(vq + 32 * e);
+        a0 += kv[0] * xv[0] + kv[1] * xv[1] + kv[2] * xv[2];
+        a1 += kv[3] * xv[0] + kv[4] * xv[1] + kv[5] * xv[2];
+        a2 += kv[6] * xv[0] + kv[7] * xv[1] + kv[8] * xv[2];
+    }
+    const int b0 = __ldg(m.sell_bptr + c);
+    const int bwidth = (__ldg(m.sell_bptr + c + 1) - b0) >> 5;
+    const int2* bp = m.sell_bref + b0 + lane;
+#pragma unroll (SpmvCfg<R, 0>::unroll)
+    for (int q = 0; q < bwidth; ++q) {
+        const int2 ref = __ldg(bp + 32 * q);
+        R xv[3];
+        gather(static_cast<size_t>(ref.y), xv);
+        const R* vq = val + static_cast<size_t>(ref.x);
+        R kv[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) kv[e] = __ldg(vq + 32 * e);
+        a0 += kv[0] * xv[0] + kv[3] * xv[1] + kv[6] * xv[2];
+        a1 += kv[1] * xv[0] + kv[4] * xv[1] + kv[7] * xv[2];
+        a2 += kv[2] * xv[0] + kv[5] * xv[1] + kv[8] * xv[2];
+    }
+    if (row < 0) return;
+    const size_t o = static_cast<size_t>(row);
+    R mv[3], xz[3], xp[3];
+    ld3<4>(mask, o, mv);
+    ld3<4>(z, o, xz);
+    ld3<4>(p_old, o, xp);
+    const R yv[3] = {mv[0] * a0, mv[1] * a1, mv[2] * a2};
+    st3<4, R>(y, o, yv[0], yv[1], yv[2]);
+    R pv[3];
+    double dot = 0;
+    for (int i = 0; i < 3; ++i) {
+        pv[i] = xz[i] + beta * xp[i];
+        dot += static_cast<double>(pv[i]) * static_cast<double>(yv[i]);
+    }
+    st3<4, R>(p_new, o, pv[0], pv[1], pv[2]);
+    rowdot[o] = live ? dot : 0.0;
 }
 
 __global__ void __launch_bounds__(256) pcg_b_alpha(BatchPcg st, const double* __restrict__ rowdot,
@@ -1756,46 +1741,40 @@ __global__ void __launch_bounds__(256) pcg_b_alpha(BatchPcg st, const double* __
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kThreads) pcg_b_update(BatchPcg st, const DevMesh m, const int* __restrict__ mov,
+__global__ void __launch_bounds__(kThreads) pcg_b_update(BatchPcg st, const int* __restrict__ mov,
                                                          const R* __restrict__ dinv, R* x, R* r, R* z,
-                                                         const R* __restrict__ p, const R* __restrict__ Ap,
-                                                         double* __restrict__ rowdot2, const int* __restrict__ chunks,
-                                                         const int* __restrict__ nchunks) {
-    const int lane = threadIdx.x & 31;
-    const int nw = gridDim.x * (blockDim.x >> 5), nc = *nchunks;
-    // The rows of the active chunks (every row of an active mesh lies in one of them).
-    for (int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); idx < nc; idx += nw) {
-        const int v = __ldg(m.sell_row + 32 * static_cast<size_t>(__ldg(chunks + idx)) + lane);
-        if (v < 0) continue;
-        const int mesh = __ldg(mov + v);
-        if (st.done[mesh]) {
-            rowdot2[2 * static_cast<size_t>(v)] = 0;
-            rowdot2[2 * static_cast<size_t>(v) + 1] = 0;
-            continue;
-        }
-        const R alpha = static_cast<R>(st.alpha[mesh]);
-        const size_t o = 4 * static_cast<size_t>(v);
-        R xv[4], pv[4], rv[4], av[4], zv[3];
-        ld4c(x + o, xv);
-        ld4(p + o, pv);
-        ld4c(r + o, rv);
-        ld4(Ap + o, av);
-        for (int i = 0; i < 3; ++i) {
-            xv[i] += alpha * pv[i];
-            rv[i] = rv[i] - alpha * av[i];
-        }
-        apply_dinv(dinv + 12 * static_cast<size_t>(v), rv, zv);
-        st4(x + o, xv[0], xv[1], xv[2]);
-        st4(r + o, rv[0], rv[1], rv[2]);
-        st4(z + o, zv[0], zv[1], zv[2]);
-        double rz = 0, rr = 0;
-        for (int i = 0; i < 3; ++i) {
-            rz += static_cast<double>(rv[i]) * zv[i];
-            rr += static_cast<double>(rv[i]) * rv[i];
-        }
-        rowdot2[2 * static_cast<size_t>(v)] = rz;
-        rowdot2[2 * static_cast<size_t>(v) + 1] = rr;
+                                                         const R* __restrict__ p, const R* __restrict__ Ap, int V,
+                                                         double* __restrict__ rowdot2) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int mesh = __ldg(mov + v);
+    if (st.done[mesh]) {
+        rowdot2[2 * static_cast<size_t>(v)] = 0;
+        rowdot2[2 * static_cast<size_t>(v) + 1] = 0;
+        return;
     }
+    const R alpha = static_cast<R>(st.alpha[mesh]);
+    const size_t o = 4 * static_cast<size_t>(v);
+    R xv[4], pv[4], rv[4], av[4], zv[3];
+    ld4c(x + o, xv);
+    ld4(p + o, pv);
+    ld4c(r + o, rv);
+    ld4(Ap + o, av);
+    for (int i = 0; i < 3; ++i) {
+        xv[i] += alpha * pv[i];
+        rv[i] = rv[i] - alpha * av[i];
+    }
+    apply_dinv(dinv + 12 * static_cast<size_t>(v), rv, zv);
+    st4(x + o, xv[0], xv[1], xv[2]);
+    st4(r + o, rv[0], rv[1], rv[2]);
+    st4(z + o, zv[0], zv[1], zv[2]);
+    double rz = 0, rr = 0;
+    for (int i = 0; i < 3; ++i) {
+        rz += static_cast<double>(rv[i]) * zv[i];
+        rr += static_cast<double>(rv[i]) * rv[i];
+    }
+    rowdot2[2 * static_cast<size_t>(v)] = rz;
+    rowdot2[2 * static_cast<size_t>(v) + 1] = rr;
 }
 
 __global__ void __launch_bounds__(256) pcg_b_beta(BatchPcg st, const double* __restrict__ rowdot2,
@@ -1834,7 +1813,6 @@ struct BatchDev {
     int *voff = nullptr, *eoff = nullptr, *mov = nullptr, *emesh = nullptr;
     int *act = nullptr, *take = nullptr, *exact = nullptr;
     unsigned char *tc_skip = nullptr, *cl_skip = nullptr;
-    int *chunks = nullptr, *nchunks = nullptr; // active sliced-ELL chunks of the current PCG solve
     double *stats = nullptr, *esum = nullptr, *fdot = nullptr, *amin = nullptr, *alpha = nullptr, *tol = nullptr;
     double *rowdot = nullptr, *rowdot2 = nullptr, *elem = nullptr;
     BatchPcg pcg{};
@@ -1889,19 +1867,14 @@ struct BatchSolver {
     template <typename R>
     void enqueue(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA, R* pB, R* Ap,
                  int pairs) {
-        // Grid-stride over the active chunk list: at most one wave of warps, so the lockstep
-        // iterations after most meshes have finished launch a grid the size of the work left.
-        const size_t chunk_warps = static_cast<size_t>(std::max(1, (h.dm.n_sell + 7) / 8));
-        const int sg = one_wave(spmv_sell_batch<R>, chunk_warps), vg = one_wave(pcg_b_update<R>, chunk_warps);
+        const int sg = std::max(1, (h.dm.n_sell + 7) / 8), vg = grid(static_cast<size_t>(V));
         for (int i = 0; i < pairs; ++i)
             for (int half = 0; half < 2; ++half) {
                 R* po = half ? pB : pA;
                 R* pn = half ? pA : pB;
-                spmv_sell_batch<R><<<sg, kThreads, 0, gs>>>(h.dm, K, z, po, mask4, Ap, pn, d.pcg, d.mov, d.rowdot,
-                                                            d.chunks, d.nchunks);
+                spmv_sell_batch<R><<<sg, kThreads, 0, gs>>>(h.dm, K, z, po, mask4, Ap, pn, d.pcg, d.mov, d.rowdot);
                 pcg_b_alpha<<<M, 256, 0, gs>>>(d.pcg, d.rowdot, d.voff);
-                pcg_b_update<R><<<vg, kThreads, 0, gs>>>(d.pcg, h.dm, d.mov, dinv, x, r, z, pn, Ap, d.rowdot2,
-                                                         d.chunks, d.nchunks);
+                pcg_b_update<R><<<vg, kThreads, 0, gs>>>(d.pcg, d.mov, dinv, x, r, z, pn, Ap, V, d.rowdot2);
                 pcg_b_beta<<<M, 256, 0, gs>>>(d.pcg, d.rowdot2, d.voff);
             }
     }
@@ -1967,10 +1940,6 @@ struct BatchSolver {
                                  : 1.0;
             up(d.tol, itol);
             up(d.act, act);
-            LPG_CUDA(cudaMemsetAsync(d.nchunks, 0, sizeof(int), s));
-            if (h.dm.n_sell > 0)
-                active_chunks_kernel<<<std::max(1, (h.dm.n_sell + 7) / 8), kThreads, 0, s>>>(h.dm, d.mov, d.act,
-                                                                                          d.chunks, d.nchunks);
             pad_rhs<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(r64, mask, bR, V);
             pcg_b_init<R><<<grid(static_cast<size_t>(V)), kThreads, 0, s>>>(bR, dinv, x, r, z, pA, V, d.rowdot2);
             pcg_b_start<<<M, 256, 0, s>>>(d.pcg, d.rowdot2, d.voff, d.tol, d.act);
@@ -2072,8 +2041,6 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
     d.exact = h.bt_int[7].as<int>(M);
     d.tc_skip = h.bt_skip[0].as<unsigned char>(static_cast<size_t>(std::max(h.dm.tc_ncl, 1)));
     d.cl_skip = h.bt_skip[1].as<unsigned char>(static_cast<size_t>(std::max(h.dm.ncl, 1)));
-    d.chunks = h.bt_chunks.as<int>(static_cast<size_t>(std::max(h.dm.n_sell, 1)) + 1);
-    d.nchunks = d.chunks + std::max(h.dm.n_sell, 1);
     int* pcg_ints = h.bt_int[5].as<int>(3 * static_cast<size_t>(M) + 1);
     d.pcg.done = pcg_ints;
     d.pcg.iters = pcg_ints + M + 1;

@@ -41,7 +41,7 @@ struct lpg_fem {
     lpg::DeviceBuffer b_cl[11]; // assembly clusters
     lpg::DeviceBuffer b_tc[13]; // tet assembly clusters
     lpg::DeviceBuffer b_sell[6]; // sliced-ELL pattern of the solvers
-    lpg::DeviceBuffer bt_int[8], bt_dbl[4], bt_skip[2], bt_chunks; // batched Newton (per-cluster skip flags, active chunks)
+    lpg::DeviceBuffer bt_int[8], bt_dbl[4], bt_skip[2]; // batched Newton (bt_skip: per-cluster skip flags)
     // Scratch of the evaluation entry points.
     lpg::DeviceBuffer d_plist, d_pcount; // elements listed for the projection's eigenvalue clamp
     lpg::DeviceBuffer d_mat[6];          // material outputs (W, P, A), per-element energies, F and G
