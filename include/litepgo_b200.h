@@ -409,7 +409,8 @@ typedef struct {
 
 /*
  * Batched newton_solve (no reference counterpart; the reference solves one energy per call):
- * num_meshes independent meshes stored in one handle as contiguous vertex ranges
+ * num_meshes independent tet meshes (a tet handle; others fail with LPG_EINVAL) stored in one
+ * handle as contiguous vertex ranges
  * [vertex_offsets[m], vertex_offsets[m+1]) and element ranges [element_offsets[m],
  * element_offsets[m+1]) (every element inside its mesh's vertices). Assembly and SpMV run once
  * over all meshes; every mesh has its own stop test, PCG scalars (one block-Jacobi PCG per mesh,
@@ -419,7 +420,8 @@ typedef struct {
  * unfinished mesh meets the threshold. fixed_dofs, f_ext, x0 and x_out are over the whole
  * handle. per_mesh[num_meshes] receives the per-mesh outcomes; result (may be NULL) the totals
  * (status = the worst mesh's, iterations = Newton iterations run, cg_iterations = lockstep PCG
- * iterations, energy = the sum).
+ * iterations, energy = the sum). A finished mesh is skipped by the later iterations' assembly,
+ * projection, feasible step and PCG.
  */
 int lpg_batch_newton_solve(lpg_fem_t h, int num_meshes, const int32_t* vertex_offsets, const int32_t* element_offsets,
                            const int32_t* fixed_dofs, int num_fixed, const double* f_ext, const double* x0, int io_mem,

@@ -2007,6 +2007,7 @@ void batch_newton_solve(lpg_fem& h, int M, const int32_t* voff_h, const int32_t*
         fail(LPG_EINVAL, "newton_solve: invalid precision");
     if (!(o.exact_below >= 0.0) || !std::isfinite(o.exact_below))
         fail(LPG_EINVAL, "newton_solve: exact_below must be finite and non-negative");
+    if (h.dm.K != 4) fail(LPG_EINVAL, "batch_newton_solve: batched solves are available for tet meshes only");
     // Meshes: contiguous vertex and element ranges; every element inside its mesh's vertices.
     if (voff_h[0] != 0 || voff_h[M] != V || eoff_h[0] != 0 || eoff_h[M] != T)
         fail(LPG_EINVAL, "batch_newton_solve: mesh offsets must start at 0 and end at the vertex / element counts");
