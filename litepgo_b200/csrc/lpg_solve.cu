@@ -1653,7 +1653,6 @@ __global__ void __launch_bounds__(kThreads, (SpmvCfg<R, 0>::minb))
     spmv_sell_batch(const DevMesh m, const R* __restrict__ val, const R* __restrict__ z, const R* __restrict__ p_old,
                     const R* __restrict__ mask, R* __restrict__ y, R* __restrict__ p_new, BatchPcg st,
                     const int* __restrict__ mov, double* __restrict__ rowdot) {
-    pdl_wait_then_release();
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= m.n_sell) return;
@@ -1726,7 +1725,6 @@ __global__ void __launch_bounds__(kThreads, (SpmvCfg<R, 0>::minb))
 
 __global__ void __launch_bounds__(256) pcg_b_alpha(BatchPcg st, const double* __restrict__ rowdot,
                                                    const int* __restrict__ voff) {
-    pdl_wait_then_release();
     const int m = blockIdx.x;
     if (st.done[m]) return;
     double res[1];
@@ -1747,7 +1745,6 @@ __global__ void __launch_bounds__(kThreads) pcg_b_update(BatchPcg st, const int*
                                                          const R* __restrict__ dinv, R* x, R* r, R* z,
                                                          const R* __restrict__ p, const R* __restrict__ Ap, int V,
                                                          double* __restrict__ rowdot2) {
-    pdl_wait_then_release();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
     const int mesh = __ldg(mov + v);
@@ -1782,7 +1779,6 @@ __global__ void __launch_bounds__(kThreads) pcg_b_update(BatchPcg st, const int*
 
 __global__ void __launch_bounds__(256) pcg_b_beta(BatchPcg st, const double* __restrict__ rowdot2,
                                                   const int* __restrict__ voff) {
-    pdl_wait_then_release();
     const int m = blockIdx.x;
     if (st.done[m]) return;
     double res[2];
@@ -1872,35 +1868,14 @@ struct BatchSolver {
     void enqueue(cudaStream_t gs, const R* K, const R* dinv, const R* mask4, R* x, R* r, R* z, R* pA, R* pB, R* Ap,
                  int pairs) {
         const int sg = std::max(1, (h.dm.n_sell + 7) / 8), vg = grid(static_cast<size_t>(V));
-        // Each kernel a programmatic dependent of the one before (griddepcontrol.wait first): in
-        // the long tail after most meshes have finished the kernels are a few microseconds, and
-        // their launch latency is what remains.
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        auto cfg = [&](int blocks, int threads) {
-            cudaLaunchConfig_t c{};
-            c.gridDim = dim3(static_cast<unsigned>(blocks));
-            c.blockDim = dim3(static_cast<unsigned>(threads));
-            c.stream = gs;
-            c.attrs = attr;
-            c.numAttrs = 1;
-            return c;
-        };
-        const cudaLaunchConfig_t cs = cfg(sg, kThreads), cu = cfg(vg, kThreads), cm = cfg(M, 256);
         for (int i = 0; i < pairs; ++i)
             for (int half = 0; half < 2; ++half) {
                 R* po = half ? pB : pA;
                 R* pn = half ? pA : pB;
-                LPG_CUDA(cudaLaunchKernelEx(&cs, spmv_sell_batch<R>, h.dm, K, static_cast<const R*>(z),
-                                            static_cast<const R*>(po), static_cast<const R*>(mask4), Ap, pn, d.pcg,
-                                            static_cast<const int*>(d.mov), d.rowdot));
-                LPG_CUDA(cudaLaunchKernelEx(&cm, pcg_b_alpha, d.pcg, static_cast<const double*>(d.rowdot),
-                                            static_cast<const int*>(d.voff)));
-                LPG_CUDA(cudaLaunchKernelEx(&cu, pcg_b_update<R>, d.pcg, static_cast<const int*>(d.mov), dinv, x, r, z,
-                                            static_cast<const R*>(pn), static_cast<const R*>(Ap), V, d.rowdot2));
-                LPG_CUDA(cudaLaunchKernelEx(&cm, pcg_b_beta, d.pcg, static_cast<const double*>(d.rowdot2),
-                                            static_cast<const int*>(d.voff)));
+                spmv_sell_batch<R><<<sg, kThreads, 0, gs>>>(h.dm, K, z, po, mask4, Ap, pn, d.pcg, d.mov, d.rowdot);
+                pcg_b_alpha<<<M, 256, 0, gs>>>(d.pcg, d.rowdot, d.voff);
+                pcg_b_update<R><<<vg, kThreads, 0, gs>>>(d.pcg, d.mov, dinv, x, r, z, pn, Ap, V, d.rowdot2);
+                pcg_b_beta<<<M, 256, 0, gs>>>(d.pcg, d.rowdot2, d.voff);
             }
     }
 
