@@ -1502,7 +1502,6 @@ __global__ void __launch_bounds__(256) seg_stats(const double* __restrict__ a, c
     const int m = blockIdx.x;
     const size_t lo = 3 * static_cast<size_t>(voff[m]), hi = 3 * static_cast<size_t>(voff[m + 1]);
     double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-#pragma unroll 8
     for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const double w = mask ? mask[i] : 1.0, av = a[i], bv = b ? b[i] : 0.0;
         s0 += w * av * bv;
@@ -1539,7 +1538,6 @@ __global__ void __launch_bounds__(256) seg_elem(const double* __restrict__ x, co
     __shared__ double sh[8];
     const int m = blockIdx.x;
     double v = min_mode ? 1.0 : 0.0;
-#pragma unroll 8
     for (int e = eoff[m] + threadIdx.x; e < eoff[m + 1]; e += blockDim.x) v = min_mode ? fmin(v, x[e]) : v + x[e];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -1614,8 +1612,6 @@ __device__ __forceinline__ void seg_rows(const double* __restrict__ rd, const in
     const int m = blockIdx.x;
     double v[K];
     for (int k = 0; k < K; ++k) v[k] = 0;
-    // Unrolled so that eight rows' loads are in flight (the sums keep their order).
-#pragma unroll 8
     for (int r = voff[m] + threadIdx.x; r < voff[m + 1]; r += blockDim.x)
         for (int k = 0; k < K; ++k) v[k] += rd[K * static_cast<size_t>(r) + k];
     for (int k = 0; k < K; ++k) {
