@@ -1236,22 +1236,28 @@ struct TcBounds {
     int e0 = 0, ne = 0, v0 = 0, nv = 0, i0 = 0, ni = 0, nd = 0, n0 = 0, nn = 0, r0 = 0, nr = 0;
 };
 constexpr int kTcFields = 12; // the bounds, then the cluster's skip flag (batched solves)
+// Field q of cluster cl as the words it is made of: {first, end} of a count field (the count is
+// end - first), {value, 0} otherwise. The lanes reading the fields of one cluster take no
+// divergent path (the array is selected, the second word's load predicated), and nothing here
+// waits on the loads: the count is formed by tc_field_value where the field is used.
+__device__ __forceinline__ bool tc_count_field(int q) { return q == 1 || q == 3 || q == 5 || q == 8 || q == 10; }
+__device__ __forceinline__ int2 tc_field_words(const DevMesh& m, const unsigned char* skip, int cl, int q) {
+    int2 w = make_int2(0, 0);
+    if (cl >= m.tc_ncl) return w;
+    const int32_t* ptr = q < 2 ? m.tc_el_ptr
+                       : q < 4 ? m.tc_vert_ptr
+                       : q < 6 ? m.tc_item_ptr
+                       : q == 6 ? m.tc_ndiag
+                       : q < 9 ? m.tc_ent_ptr
+                       : m.tc_row_ptr;
+    if (q < 11) w.x = __ldg(ptr + cl);
+    if (tc_count_field(q)) w.y = __ldg(ptr + cl + 1);
+    if (q == 11 && skip != nullptr) w.x = __ldg(skip + cl) != 0;
+    return w;
+}
+__device__ __forceinline__ int tc_field_value(int2 w, int q) { return tc_count_field(q) ? w.y - w.x : w.x; }
 __device__ __forceinline__ int tc_field(const DevMesh& m, const unsigned char* skip, int cl, int q) {
-    if (cl >= m.tc_ncl) return 0;
-    if (q == 11) return skip != nullptr && __ldg(skip + cl) != 0;
-    auto span = [&](const int32_t* ptr, bool count) {
-        const int lo = __ldg(ptr + cl);
-        return count ? __ldg(ptr + cl + 1) - lo : lo;
-    };
-    switch (q) {
-    case 0: case 1: return span(m.tc_el_ptr, q == 1);
-    case 2: case 3: return span(m.tc_vert_ptr, q == 3);
-    case 4: case 5: return span(m.tc_item_ptr, q == 5);
-    case 6: return __ldg(m.tc_ndiag + cl);
-    case 7: case 8: return span(m.tc_ent_ptr, q == 8);
-    case 9: case 10: return span(m.tc_row_ptr, q == 10);
-    default: return 0;
-    }
+    return tc_field_value(tc_field_words(m, skip, cl, q), q);
 }
 // A skipped cluster has empty bounds: nothing is staged, evaluated or written.
 __device__ __forceinline__ TcBounds tc_bounds(const int* f) {
@@ -1347,7 +1353,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     R r12[12];
     int rowv[kTcRowInts] = {0, 0, 0, 0, 0};
     tc_issue<R, ITEMS>(m, a.u, b, x, tid, sell, su, sitems, sents, r12, rowv);
-    int ahead = tid < kTcFields ? tc_field(m, a.tc_skip, cl + grid, tid) : 0;
+    int2 ahead = tid < kTcFields ? tc_field_words(m, a.tc_skip, cl + grid, tid) : make_int2(0, 0);
     int ne = b.ne, ni = WH ? b.ni : b.nd, nr = b.nr, ndc = b.nd;
     for (int buf = 0; cl < m.tc_ncl; cl += grid, buf ^= 1) {
         int* rows = srow + buf * kTcRows * kTcRowInts;
@@ -1355,7 +1361,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
 #pragma unroll
             for (int q = 0; q < kTcRowInts; ++q) rows[kTcRowInts * tid + q] = rowv[q];
         }
-        if (tid < kTcFields) s_hdr[buf][tid] = ahead;
+        if (tid < kTcFields) s_hdr[buf][tid] = tc_field_value(ahead, tid);
         cp_async_wait_all();
         __syncthreads(); // the cluster's stage is complete
         // Element pass: every element of the cluster once, one per thread.
@@ -1401,7 +1407,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         // The next cluster's indices, and the bounds of the one after, arrive while the item pass
         // runs.
         tc_load_idx(m, tc_bounds(s_hdr[buf]), tid, x);
-        if (tid < kTcFields) ahead = tc_field(m, a.tc_skip, cl + 2 * grid, tid);
+        if (tid < kTcFields) ahead = tc_field_words(m, a.tc_skip, cl + 2 * grid, tid);
         if (ITEMS) {
             // Item pass. The nd diagonal items (the first nd) are summed by lane pairs, each lane
             // over half the contributor list in ascending order, the two halves added by a
