@@ -1034,6 +1034,10 @@ constexpr int kTcThreads = 256;
 static_assert(kTcThreads >= kTcElems && kTcThreads >= kTcVerts && kTcThreads >= kTcRows,
               "one element, one vertex and one row per thread in the stage");
 static_assert(((2 * kTcRows + 31) & ~31) < kTcThreads, "the diagonal lane pairs leave lanes for the edge items");
+// Lanes per diagonal item of a cluster with nd owned rows: 4 while they leave at least one warp
+// for the edge items, else 2. Part k of the item's S lanes sums contributors
+// [ceil(cnt k / S), ceil(cnt (k + 1) / S)); the parts are added as (p0 + p1) + (p2 + p3).
+__host__ __device__ constexpr int tc_diag_split(int nd) { return 4 * nd + 32 <= kTcThreads ? 4 : 2; }
 // Per-element data in shared memory, one component per kTcElems-long array: h_a (3 a + i),
 // vol mu grad N_a . grad N_b (pair order), vol lambda, vol p, g_a (3 a + i).
 constexpr int kTcH = 0, kTcCC = 12, kTcL = 22, kTcP = 23, kTcG = 24, kTcComp = 36;
@@ -1409,26 +1413,27 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         tc_load_idx(m, tc_bounds(s_hdr[buf]), tid, x);
         if (tid < kTcFields) ahead = tc_field_words(m, a.tc_skip, cl + 2 * grid, tid);
         if (ITEMS) {
-            // Item pass. The nd diagonal items (the first nd) are summed by lane pairs, each lane
-            // over half the contributor list in ascending order, the two halves added by a
-            // shuffle; they fill whole warps (2 nd lanes rounded up to 32), and the edge items
-            // follow on the remaining lanes, so no warp runs both kinds and the diagonal sums
-            // (the longest lists) take about as long as an edge block.
-            const int nd = ndc, dl = 2 * nd, dpad = (dl + 31) & ~31;
+            // Item pass. The nd diagonal items (the first nd) are summed by groups of S lanes
+            // (tc_diag_split), each lane over a contiguous part of the contributor list in
+            // ascending order, the parts added by shuffles; they fill whole warps (S nd lanes
+            // rounded up to 32), and the edge items follow on the remaining lanes, so no warp runs
+            // both kinds and the diagonal sums (the longest lists) take about as long as an edge
+            // block.
+            const int nd = ndc, sd = tc_diag_split(nd), lsd = sd == 4 ? 2 : 1, dl = sd * nd, dpad = (dl + 31) & ~31;
             if (tid < dpad) {
                 // Diagonal block (symmetric: 6 sums, mirrored) and the row's gradient:
                 //   H_aa = (vol lambda - vol p) h_a h_a^T + vol mu |grad N_a|^2 I.
                 const bool active = tid < dl;
-                const int part = tid & 1;
+                const int part = tid & (sd - 1);
                 uint4 it = make_uint4(0u, 0u, 0u, 0u);
                 R acc[6] = {0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
                 if (active) {
-                    it = sitems[tid >> 1];
+                    it = sitems[tid >> lsd];
                     const uint16_t* en = sents + (it.z & 0xfffffu);
-                    const int cnt = static_cast<int>(it.z >> 20), half = (cnt + 1) >> 1;
-                    const int c1 = part ? cnt : half;
+                    const int cnt = static_cast<int>(it.z >> 20);
+                    const int c0 = (cnt * part + sd - 1) >> lsd, c1 = (cnt * (part + 1) + sd - 1) >> lsd;
 #pragma unroll UNR
-                    for (int c = part ? half : 0; c < c1; ++c) {
+                    for (int c = c0; c < c1; ++c) {
                         const int w = en[c];
                         const int el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
                         if (WG) {
@@ -1443,14 +1448,17 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
                         }
                     }
                 }
-                // First half + second half (the same sum on both lanes of the pair).
-                if (WG) {
+                // The parts added pairwise: (p0 + p1) + (p2 + p3) on the group's first lane.
+                for (int off = 1; off < sd; off <<= 1) {
+                    if (WG) {
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) gs[i] = X::add(gs[i], __shfl_xor_sync(0xffffffffu, gs[i], 1));
-                }
-                if (WH) {
+                        for (int i = 0; i < 3; ++i) gs[i] = X::add(gs[i], __shfl_xor_sync(0xffffffffu, gs[i], off));
+                    }
+                    if (WH) {
 #pragma unroll
-                    for (int u6 = 0; u6 < 6; ++u6) acc[u6] = X::add(acc[u6], __shfl_xor_sync(0xffffffffu, acc[u6], 1));
+                        for (int u6 = 0; u6 < 6; ++u6)
+                            acc[u6] = X::add(acc[u6], __shfl_xor_sync(0xffffffffu, acc[u6], off));
+                    }
                 }
                 if (active && part == 0) {
                     if (WG) {

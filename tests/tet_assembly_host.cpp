@@ -134,12 +134,15 @@ extern "C" int tet_assemble(int V, const double* X, int T, const int32_t* tets, 
                 const uint16_t* en = ents + (it[2] & 0xfffffu);
                 const int cnt = static_cast<int>(it[2] >> 20);
                 if (it[3] >> 31) {
-                    // Two halves of the list summed apart (the kernel's lane pair), then added.
-                    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gs[3] = {0, 0, 0};
-                    const int half = (cnt + 1) >> 1;
-                    for (int part = 0; part < 2; ++part) {
-                        double ap[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gp[3] = {0, 0, 0};
-                        for (int c = part ? half : 0; c < (part ? cnt : half); ++c) {
+                    // The list in S contiguous parts summed apart (the kernel's lane group: S = 4
+                    // while 4 nd + 32 <= 256, else 2), then added as (p0 + p1) + (p2 + p3).
+                    const int nd = p.tc_ndiag[cl], S = 4 * nd + 32 <= 256 ? 4 : 2;
+                    double pa[4][9] = {}, pg[4][3] = {};
+                    for (int part = 0; part < S; ++part) {
+                        double* ap = pa[part];
+                        double* gp = pg[part];
+                        const int c0 = (cnt * part + S - 1) / S, c1 = (cnt * (part + 1) + S - 1) / S;
+                        for (int c = c0; c < c1; ++c) {
                             const int w = en[c], el = w >> 8, pr = (w >> 4) & 15, la = (w >> 2) & 3;
                             for (int i = 0; i < 3; ++i) gp[i] += ed[(24 + 3 * la + i) * E + el];
                             const double dv = ed[22 * E + el] - ed[23 * E + el], mg = ed[(12 + pr) * E + el];
@@ -148,9 +151,14 @@ extern "C" int tet_assemble(int V, const double* X, int T, const int32_t* tets, 
                                     ap[3 * i + cc] += dv * (ed[(3 * la + i) * E + el] * ed[(3 * la + cc) * E + el]) +
                                                       (i == cc ? mg : 0.0);
                         }
-                        for (int t = 0; t < 9; ++t) acc[t] += ap[t];
-                        for (int i = 0; i < 3; ++i) gs[i] += gp[i];
                     }
+                    for (int off = 1; off < S; off <<= 1)
+                        for (int part = 0; part < S; part += 2 * off) {
+                            for (int t = 0; t < 9; ++t) pa[part][t] += pa[part + off][t];
+                            for (int i = 0; i < 3; ++i) pg[part][i] += pg[part + off][i];
+                        }
+                    const double* acc = pa[0];
+                    const double* gs = pg[0];
                     const int v = p.tc_rows[r0 + static_cast<int>(it[3] & 0xffu)];
                     for (int i = 0; i < 3; ++i) grad[3 * v + i] = gs[i];
                     for (int i = 0; i < 3; ++i)
