@@ -1042,8 +1042,10 @@ __host__ __device__ constexpr int tc_diag_split(int nd) { return 4 * nd + 32 <= 
 // vol mu grad N_a . grad N_b (pair order), vol lambda, vol p, g_a (3 a + i).
 constexpr int kTcH = 0, kTcCC = 12, kTcL = 22, kTcP = 23, kTcG = 24, kTcComp = 36;
 // Owned-row words in shared memory: vertex, staging offset, first block, nb | diagonal block
-// index << 8 (solver layout), solver base.
-constexpr int kTcRowInts = 5;
+// index << 8 (solver layout), solver base. A thread holds them one cluster ahead as the words
+// loaded (vertex, staging offset, first block, end block, solver base, diagonal slot), so that
+// nothing waits on those loads before the next cluster's stage completes.
+constexpr int kTcRowInts = 5, kTcRowRaw = 6;
 // Launch variants of the Exact-Hessian kernel (autotuner): the resident blocks per SM the
 // register allocation must allow, and the unroll depth of the contributor loops. The arithmetic
 // and its order are the same, so every variant's results are bitwise identical.
@@ -1295,7 +1297,7 @@ __device__ __forceinline__ void tc_load_idx(const DevMesh& m, const TcBounds& b,
 template <typename R, bool ITEMS>
 __device__ __forceinline__ void tc_issue(const DevMesh& m, const double* __restrict__ u, const TcBounds& b,
                                          const TcIdx& x, int t, bool sell, double* su, uint4* sitems, uint16_t* sents,
-                                         R (&r12)[12], int (&rowv)[kTcRowInts]) {
+                                         R (&r12)[12], int (&rowv)[kTcRowRaw]) {
     // Without items (energy only) an element the cluster does not own contributes nothing.
     if (t < b.ne && (ITEMS || (x.ew >> 31))) load_rec<R>(rec_ptr<R>(m), static_cast<int>(x.ew & 0x7fffffffu), r12);
     if (t < b.nv) {
@@ -1308,15 +1310,15 @@ __device__ __forceinline__ void tc_issue(const DevMesh& m, const double* __restr
     }
     cp_async_commit();
     if (ITEMS && t < b.nr) {
-        const int base = __ldg(m.row_ptr + x.row), nb = __ldg(m.row_ptr + x.row + 1) - base;
         rowv[0] = x.row;
         rowv[1] = x.so;
-        rowv[2] = base;
-        rowv[3] = nb;
+        rowv[2] = __ldg(m.row_ptr + x.row);
+        rowv[3] = __ldg(m.row_ptr + x.row + 1);
         rowv[4] = 0;
+        rowv[5] = 0;
         if (sell) {
-            rowv[3] |= (__ldg(m.diag_slot + x.row) - base) << 8;
             rowv[4] = __ldg(m.sell_base + x.row);
+            rowv[5] = __ldg(m.diag_slot + x.row);
         }
     }
 }
@@ -1355,7 +1357,7 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
     TcIdx x;
     tc_load_idx(m, b, tid, x);
     R r12[12];
-    int rowv[kTcRowInts] = {0, 0, 0, 0, 0};
+    int rowv[kTcRowRaw] = {0, 0, 0, 0, 0, 0};
     tc_issue<R, ITEMS>(m, a.u, b, x, tid, sell, su, sitems, sents, r12, rowv);
     int2 ahead = tid < kTcFields ? tc_field_words(m, a.tc_skip, cl + grid, tid) : make_int2(0, 0);
     int ne = b.ne, ni = WH ? b.ni : b.nd, nr = b.nr, ndc = b.nd;
@@ -1363,7 +1365,9 @@ __global__ void __launch_bounds__(kTcThreads, MINB) tet_cluster_kernel(const Dev
         int* rows = srow + buf * kTcRows * kTcRowInts;
         if (ITEMS && tid < nr) {
 #pragma unroll
-            for (int q = 0; q < kTcRowInts; ++q) rows[kTcRowInts * tid + q] = rowv[q];
+            for (int q = 0; q < 3; ++q) rows[kTcRowInts * tid + q] = rowv[q];
+            rows[kTcRowInts * tid + 3] = (rowv[3] - rowv[2]) | (sell ? (rowv[5] - rowv[2]) << 8 : 0);
+            rows[kTcRowInts * tid + 4] = rowv[4];
         }
         if (tid < kTcFields) s_hdr[buf][tid] = tc_field_value(ahead, tid);
         cp_async_wait_all();
