@@ -57,3 +57,18 @@ def rel_err(a, b):
     b = np.asarray(b, dtype=float)
     scale = max(np.max(np.abs(b)), 1e-300)
     return float(np.max(np.abs(a - b)) / scale)
+
+
+def corner_chain(k):
+    """k tets in a chain sharing only corner vertices: tet i = (a_i, b_i, c_i, a_i+1). Every vertex
+    has 4 or 7 Hessian blocks in its row, so the tet assembly's clusters reach their 64-row limit
+    (the diagonal items then fall back from four lanes to two)."""
+    a = np.stack([2.0 * np.arange(k + 1), np.zeros(k + 1), np.zeros(k + 1)], 1)
+    i = np.arange(k)
+    b = np.stack([2.0 * i + 1, np.ones(k), np.zeros(k)], 1)
+    c = np.stack([2.0 * i + 1, np.full(k, 0.5), np.full(k, 0.9)], 1)
+    X = np.concatenate([a, b, c])
+    tets = np.stack([i, k + 1 + i, 2 * k + 1 + i, i + 1], 1).astype(np.int32)
+    neg = np.linalg.det(X[tets[:, 1:]] - X[tets[:, :1]]) < 0
+    tets[neg, 1], tets[neg, 2] = tets[neg, 2].copy(), tets[neg, 1].copy()
+    return X, tets

@@ -10,7 +10,7 @@ import pytest
 import scipy.sparse as sp
 
 import oracle
-from conftest import TWO_TET_CELLS, TWO_TET_THETA, TWO_TET_X, rel_err, two_tet_states
+from conftest import TWO_TET_CELLS, TWO_TET_THETA, TWO_TET_X, corner_chain, rel_err, two_tet_states
 from litepgo_b200 import dof, energy, fem, mesh, workloads
 
 pytestmark = pytest.mark.gpu
@@ -278,6 +278,23 @@ def test_valence_above_32():
     assert rel_err(H.data, vr) <= TOL64
 
 
+def test_full_clusters_corner_chain():
+    """Assembly clusters at their 64-row limit (a chain of tets sharing corners): the diagonal
+    items are summed by lane pairs there and by lane quads in the smaller clusters; Exact and
+    Projected Hessians against the oracle."""
+    X, tets = corner_chain(200)
+    theta = np.array([1.4e5, 3.4e4])
+    u = 0.01 * np.random.default_rng(8).standard_normal(X.size)
+    gpu = fem.VolumetricFemEnergyTetP1.from_arrays(X, tets, theta)
+    orc = oracle.OracleMesh(X, tets, theta)
+    for kind, code, tol in ((Exact, 1, TOL64), (Projected, 2, 1e-11)):
+        E, g, H = gpu.eval(u, gradient=True, hessian=kind)
+        Er, gr, vr = orc.eval(u, True, code)
+        assert abs(E - Er) <= TOL64 * abs(Er)
+        assert rel_err(g, gr) <= TOL64
+        assert rel_err(H.data, vr) <= tol
+
+
 def sell_layout(e):
     import ctypes
 
@@ -305,7 +322,7 @@ def solver_values(e, u, hessian, precision, layout, nvalues):
     return hess.cpu().numpy()
 
 
-@pytest.mark.parametrize("case", ["box", "ragged", "valence"])
+@pytest.mark.parametrize("case", ["box", "ragged", "valence", "chain"])
 def test_solver_sliced_ell_layout_holds_the_upper_bsr_blocks(case):
     """The Newton / adjoint solvers keep the upper triangle of the Hessian (blocks with column >=
     row, diagonal first) in sliced ELL (chunks of 32 rows sorted by block count within 128-row
@@ -320,6 +337,9 @@ def test_solver_sliced_ell_layout_holds_the_upper_bsr_blocks(case):
     elif case == "ragged":
         X, t = mesh.make_box(4)
         tets = t[np.random.default_rng(5).random(t.shape[0]) < 0.6]
+        theta, u = np.array([1.4e5, 3.4e4]), 0.01 * rng.standard_normal(X.size)
+    elif case == "chain":
+        X, tets = corner_chain(200)
         theta, u = np.array([1.4e5, 3.4e4]), 0.01 * rng.standard_normal(X.size)
     else:
         k = 40

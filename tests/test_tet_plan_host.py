@@ -15,7 +15,7 @@ import pytest
 import scipy.sparse as sp
 
 import oracle
-from conftest import ROOT, rel_err
+from conftest import ROOT, corner_chain, rel_err
 from litepgo_b200 import mesh
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -97,6 +97,13 @@ def test_shuffled_numbering_and_per_element_theta(host):
 def test_delaunay_ball(host):
     X, tets = mesh.delaunay_ball(1500, seed=9)
     check(host, X, tets, THETA, deformed(X, 4, 1e-5))
+
+
+def test_corner_chain_full_clusters(host):
+    """Clusters of 64 owned rows (the limit): the diagonal items are summed by lane pairs there
+    and by lane quads in the smaller clusters."""
+    X, tets = corner_chain(200)
+    check(host, X, tets, THETA, deformed(X, 6, 0.01))
 
 
 def test_bunny_asset(host):
