@@ -83,13 +83,15 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
     p.cl_slot_ent.clear();
     p.cl_ents.clear();
     std::vector<int32_t> eloc(static_cast<size_t>(T), -1), els;
-    std::vector<std::vector<uint32_t>> bucket;
-    std::vector<std::vector<uint32_t>> diag;
+    // A row's off-diagonal contributor words grouped by block (counting sort, each block's words
+    // in iteration order), and the cluster's diagonal words row after row.
+    std::vector<uint32_t> roww, rowpool, dpool;
+    std::vector<int32_t> rowq, qstart, qfill, dstart;
     // Appends a contributor list to cl_ents: one 16-bit word each, or two for wide cells.
-    auto append = [&](const std::vector<uint32_t>& list) {
-        for (uint32_t w : list) {
-            p.cl_ents.push_back(static_cast<uint16_t>(w & 0xffffu));
-            if (wide) p.cl_ents.push_back(static_cast<uint16_t>(w >> 16));
+    auto append = [&](const uint32_t* first, const uint32_t* last) {
+        for (; first != last; ++first) {
+            p.cl_ents.push_back(static_cast<uint16_t>(*first & 0xffffu));
+            if (wide) p.cl_ents.push_back(static_cast<uint16_t>(*first >> 16));
         }
     };
     std::vector<std::pair<uint32_t, uint32_t>> left, right; // (slot word, entry word)
@@ -98,10 +100,16 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
         els.clear();
         for (int j = 0; j < nr; ++j) {
             const int v = p.cl_rows[r0 + j];
-            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) els.push_back(inc[k] & kMaskE);
+            // Each distinct element once (eloc -2 marks one already listed), then ascending.
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
+                const int e = inc[k] & kMaskE;
+                if (eloc[e] == -1) {
+                    eloc[e] = -2;
+                    els.push_back(e);
+                }
+            }
         }
         std::sort(els.begin(), els.end());
-        els.erase(std::unique(els.begin(), els.end()), els.end());
         for (size_t i = 0; i < els.size(); ++i) {
             const int e = els[i];
             eloc[e] = static_cast<int32_t>(i);
@@ -110,36 +118,46 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
         }
         p.cl_el_ptr.push_back(static_cast<int32_t>(p.cl_els.size()));
         const size_t ent0 = p.cl_ents.size();
-        diag.assign(static_cast<size_t>(nr), {});
+        dpool.clear();
+        dstart.assign(static_cast<size_t>(nr) + 1, 0);
         left.clear();
         right.clear();
         int noff = 0;
         for (int j = 0; j < nr; ++j) {
             const int v = p.cl_rows[r0 + j];
             const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
-            bucket.assign(static_cast<size_t>(nb), {});
+            rowq.clear();
+            roww.clear();
+            qstart.assign(static_cast<size_t>(nb) + 1, 0);
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
                 const int e = inc[k] & kMaskE, a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> ishift);
                 const uint32_t el = static_cast<uint32_t>(eloc[e]) << (2 * sh);
                 for (int b = 0; b < K; ++b) {
                     const int w = tets[K * static_cast<size_t>(e) + b];
                     if (w == v) {
-                        diag[j].push_back(el | static_cast<uint32_t>((a << sh) | a));
+                        dpool.push_back(el | static_cast<uint32_t>((a << sh) | a));
                         continue;
                     }
                     const int32_t* beg = p.col_idx.data() + rb;
                     const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
-                    bucket[q].push_back(el | static_cast<uint32_t>(v < w ? ((a << sh) | b) : ((b << sh) | a)));
+                    rowq.push_back(q);
+                    roww.push_back(el | static_cast<uint32_t>(v < w ? ((a << sh) | b) : ((b << sh) | a)));
+                    ++qstart[static_cast<size_t>(q) + 1];
                 }
             }
+            dstart[j + 1] = static_cast<int32_t>(dpool.size());
+            for (int q = 0; q < nb; ++q) qstart[q + 1] += qstart[q];
+            rowpool.resize(roww.size());
+            qfill.assign(qstart.begin(), qstart.end() - 1);
+            for (size_t i = 0; i < roww.size(); ++i) rowpool[qfill[rowq[i]]++] = roww[i];
             for (int q = 0; q < nb; ++q) {
                 const int w = p.col_idx[rb + q];
                 if (w == v) continue;
                 const uint32_t word = static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (v > w ? 1u << 30 : 0u);
                 const uint32_t ent = static_cast<uint32_t>(p.cl_ents.size() - ent0) |
-                                     (static_cast<uint32_t>(bucket[q].size()) << 20);
+                                     (static_cast<uint32_t>(qstart[q + 1] - qstart[q]) << 20);
                 (v > w ? left : right).emplace_back(word, ent);
-                append(bucket[q]);
+                append(rowpool.data() + qstart[q], rowpool.data() + qstart[q + 1]);
                 ++noff;
             }
         }
@@ -155,8 +173,8 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
             const int q = p.diag_slot[v] - p.row_ptr[v];
             p.cl_slot.push_back(static_cast<uint32_t>(j) | (static_cast<uint32_t>(q) << 8) | (1u << 31));
             p.cl_slot_ent.push_back(static_cast<uint32_t>(p.cl_ents.size() - ent0) |
-                                    (static_cast<uint32_t>(diag[j].size()) << 20));
-            append(diag[j]);
+                                    (static_cast<uint32_t>(dstart[j + 1] - dstart[j]) << 20));
+            append(dpool.data() + dstart[j], dpool.data() + dstart[j + 1]);
         }
         if (p.cl_ents.size() - ent0 >= (1u << 20) ||
             p.cl_ents.size() >= static_cast<size_t>(std::numeric_limits<int32_t>::max()))
@@ -257,11 +275,14 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
     p.tc_ents.clear();
     std::vector<int32_t> eloc(static_cast<size_t>(T), -1), vloc(static_cast<size_t>(V), -1), rloc(static_cast<size_t>(V), -1);
     std::vector<int32_t> els, verts;
+    // An item's contributor words are pool[start, start + cnt): the cluster's words, block by block.
     struct Item {
         uint32_t w0, w1, w3;
-        std::vector<uint16_t> ents;
+        int start, cnt;
     };
     std::vector<Item> diag, edge;
+    std::vector<uint16_t> pool, roww;
+    std::vector<int32_t> rowq, qstart, qfill;
     auto pack = [](int so, int q, int nb) {
         return static_cast<uint32_t>(so) | (static_cast<uint32_t>(q) << 16) | (static_cast<uint32_t>(nb) << 24);
     };
@@ -277,15 +298,24 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
             const int nb = p.row_ptr[v + 1] - p.row_ptr[v];
             if (nb > 255) fail(LPG_EINVAL, "vertex has more than 254 neighbours (assembly plan limit)");
             so += 9 * nb;
-            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) els.push_back(inc[k] & kMaskE);
+            // Each distinct element once (eloc -2 marks one already listed), then ascending.
+            for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
+                const int e = inc[k] & kMaskE;
+                if (eloc[e] == -1) {
+                    eloc[e] = -2;
+                    els.push_back(e);
+                }
+            }
         }
         if (so > 65535) fail(LPG_EINVAL, "assembly cluster output exceeds its staging index range");
         std::sort(els.begin(), els.end());
-        els.erase(std::unique(els.begin(), els.end()), els.end());
         for (int e : els)
-            for (int a = 0; a < 4; ++a) verts.push_back(vert(e, a));
+            for (int a = 0; a < 4; ++a)
+                if (vloc[vert(e, a)] == -1) {
+                    vloc[vert(e, a)] = -2;
+                    verts.push_back(vert(e, a));
+                }
         std::sort(verts.begin(), verts.end());
-        verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
         for (size_t i = 0; i < verts.size(); ++i) {
             vloc[verts[i]] = static_cast<int32_t>(i);
             p.tc_verts.push_back(verts[i]);
@@ -301,11 +331,16 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
         }
         diag.clear();
         edge.clear();
+        pool.clear();
         for (int j = 0; j < nr; ++j) {
             const int v = p.tc_rows[r0 + j];
             const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
-            // Contributors of every block of row v, in element order (the incidence is ascending).
-            std::vector<std::vector<uint16_t>> bucket(static_cast<size_t>(nb));
+            // Contributors of every block of row v, in element order (the incidence is ascending):
+            // each incident element gives one word to each of four blocks; the words are counted
+            // per block and then placed block after block, each block's in that order.
+            rowq.clear();
+            roww.clear();
+            qstart.assign(static_cast<size_t>(nb) + 1, 0);
             for (int k = p.inc_ptr[v]; k < p.inc_ptr[v + 1]; ++k) {
                 const int e = inc[k] & kMaskE;
                 const int a = static_cast<int>(static_cast<uint32_t>(inc[k]) >> inc_shift(4));
@@ -317,40 +352,46 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
                     const int lo = v <= w ? a : b, hi = v <= w ? b : a;
                     const int x = std::min(a, b), y = std::max(a, b);
                     const int pr = x * 4 - (x * (x - 1)) / 2 + (y - x); // element block pair index (a <= b order)
-                    bucket[q].push_back(static_cast<uint16_t>(el | static_cast<uint32_t>((pr << 4) | (lo << 2) | hi)));
+                    rowq.push_back(q);
+                    roww.push_back(static_cast<uint16_t>(el | static_cast<uint32_t>((pr << 4) | (lo << 2) | hi)));
+                    ++qstart[static_cast<size_t>(q) + 1];
                 }
             }
+            for (int q = 0; q < nb; ++q) qstart[q + 1] += qstart[q];
+            const int base = static_cast<int>(pool.size());
+            pool.resize(pool.size() + roww.size());
+            qfill.assign(qstart.begin(), qstart.end() - 1);
+            for (size_t i = 0; i < roww.size(); ++i) pool[base + qfill[rowq[i]]++] = roww[i];
             for (int q = 0; q < nb; ++q) {
                 const int w = p.col_idx[rb + q];
+                const int start = base + qstart[q], cnt = qstart[q + 1] - qstart[q];
                 if (w == v) {
                     diag.push_back({pack(p.tc_row_so[r0 + j], q, nb), 0xffffffffu, 0x80000000u | static_cast<uint32_t>(j),
-                                    std::move(bucket[q])});
+                                    start, cnt});
                 } else if (cl_of[w] == c) {
                     if (v > w) continue; // summed with the lower row's item
                     const int k = rloc[w];
                     const int wb = p.row_ptr[w], wn = p.row_ptr[w + 1] - wb;
                     const int qw = static_cast<int>(std::lower_bound(p.col_idx.data() + wb, p.col_idx.data() + wb + wn, v) -
                                                     (p.col_idx.data() + wb));
-                    edge.push_back({pack(p.tc_row_so[r0 + j], q, nb), pack(p.tc_row_so[r0 + k], qw, wn), 0u,
-                                    std::move(bucket[q])});
+                    edge.push_back({pack(p.tc_row_so[r0 + j], q, nb), pack(p.tc_row_so[r0 + k], qw, wn), 0u, start, cnt});
                 } else {
-                    edge.push_back({pack(p.tc_row_so[r0 + j], q, nb), 0xffffffffu, v > w ? 0x40000000u : 0u,
-                                    std::move(bucket[q])});
+                    edge.push_back({pack(p.tc_row_so[r0 + j], q, nb), 0xffffffffu, v > w ? 0x40000000u : 0u, start, cnt});
                 }
             }
         }
-        auto by_count = [](const Item& x, const Item& y) { return x.ents.size() > y.ents.size(); };
+        auto by_count = [](const Item& x, const Item& y) { return x.cnt > y.cnt; };
         std::stable_sort(diag.begin(), diag.end(), by_count);
         std::stable_sort(edge.begin(), edge.end(), by_count);
         const size_t ent0 = p.tc_ents.size();
         for (const auto* group : {&diag, &edge})
             for (const Item& it : *group) {
                 const size_t first = p.tc_ents.size() - ent0;
-                if (first >= (1u << 20) || it.ents.size() >= (1u << 12))
+                if (first >= (1u << 20) || it.cnt >= (1 << 12))
                     fail(LPG_EINVAL, "mesh too large for the assembly plan's index ranges");
                 p.tc_items.insert(p.tc_items.end(),
-                                  {it.w0, it.w1, static_cast<uint32_t>(first) | (static_cast<uint32_t>(it.ents.size()) << 20), it.w3});
-                p.tc_ents.insert(p.tc_ents.end(), it.ents.begin(), it.ents.end());
+                                  {it.w0, it.w1, static_cast<uint32_t>(first) | (static_cast<uint32_t>(it.cnt) << 20), it.w3});
+                p.tc_ents.insert(p.tc_ents.end(), pool.begin() + it.start, pool.begin() + it.start + it.cnt);
             }
         while (p.tc_ents.size() % 8 != 0) p.tc_ents.push_back(0); // 16-byte aligned per cluster
         p.tc_ndiag.push_back(static_cast<int32_t>(diag.size()));
