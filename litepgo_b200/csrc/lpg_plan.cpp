@@ -10,8 +10,10 @@
 
 #include <algorithm>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <string>
+#include <thread>
 #include <utility>
 
 #include "lpg_internal.h"
@@ -82,7 +84,7 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
     p.cl_slot.clear();
     p.cl_slot_ent.clear();
     p.cl_ents.clear();
-    std::vector<int32_t> eloc(static_cast<size_t>(T), -1), els;
+    std::vector<int32_t> eloc(static_cast<size_t>(T), -1), els, colq(static_cast<size_t>(V), -1);
     // A row's off-diagonal contributor words grouped by block (counting sort, each block's words
     // in iteration order), and the cluster's diagonal words row after row.
     std::vector<uint32_t> roww, rowpool, dpool;
@@ -126,6 +128,9 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
         for (int j = 0; j < nr; ++j) {
             const int v = p.cl_rows[r0 + j];
             const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
+            // Block index within the row of each column: every vertex of an element incident to v
+            // is in v's pattern, so the entries looked up below are always this row's.
+            for (int q = 0; q < nb; ++q) colq[p.col_idx[rb + q]] = q;
             rowq.clear();
             roww.clear();
             qstart.assign(static_cast<size_t>(nb) + 1, 0);
@@ -138,8 +143,7 @@ void build_clusters(HostPlan& p, const int32_t* tets, const std::vector<int32_t>
                         dpool.push_back(el | static_cast<uint32_t>((a << sh) | a));
                         continue;
                     }
-                    const int32_t* beg = p.col_idx.data() + rb;
-                    const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
+                    const int q = colq[w];
                     rowq.push_back(q);
                     roww.push_back(el | static_cast<uint32_t>(v < w ? ((a << sh) | b) : ((b << sh) | a)));
                     ++qstart[static_cast<size_t>(q) + 1];
@@ -274,6 +278,7 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
     p.tc_ndiag.clear();
     p.tc_ents.clear();
     std::vector<int32_t> eloc(static_cast<size_t>(T), -1), vloc(static_cast<size_t>(V), -1), rloc(static_cast<size_t>(V), -1);
+    std::vector<int32_t> colq(static_cast<size_t>(V), -1);
     std::vector<int32_t> els, verts;
     // An item's contributor words are pool[start, start + cnt): the cluster's words, block by block.
     struct Item {
@@ -335,6 +340,9 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
         for (int j = 0; j < nr; ++j) {
             const int v = p.tc_rows[r0 + j];
             const int rb = p.row_ptr[v], nb = p.row_ptr[v + 1] - rb;
+            // Block index within the row of each column: every vertex of an element incident to v
+            // is in v's pattern, so the entries looked up below are always this row's.
+            for (int q = 0; q < nb; ++q) colq[p.col_idx[rb + q]] = q;
             // Contributors of every block of row v, in element order (the incidence is ascending):
             // each incident element gives one word to each of four blocks; the words are counted
             // per block and then placed block after block, each block's in that order.
@@ -347,8 +355,7 @@ void build_tet_clusters(HostPlan& p, const int32_t* tets, const std::vector<int3
                 const uint32_t el = static_cast<uint32_t>(eloc[e]) << 8;
                 for (int b = 0; b < 4; ++b) {
                     const int w = vert(e, b);
-                    const int32_t* beg = p.col_idx.data() + rb;
-                    const int q = static_cast<int>(std::lower_bound(beg, beg + nb, w) - beg);
+                    const int q = colq[w];
                     const int lo = v <= w ? a : b, hi = v <= w ? b : a;
                     const int x = std::min(a, b), y = std::max(a, b);
                     const int pr = x * 4 - (x * (x - 1)) / 2 + (y - x); // element block pair index (a <= b order)
@@ -548,8 +555,29 @@ void build_plan(int V, int T, const int32_t* tets, HostPlan& p, int K) {
     p.unused_rows.clear();
     for (int v = 0; v < V; ++v)
         if (p.inc_ptr[v + 1] == p.inc_ptr[v]) p.unused_rows.push_back(v); // no element: zero gradient, no blocks
-    build_clusters(p, tets, inc);
-    if (K == 4) build_tet_clusters(p, tets, inc);
+    if (K != 4) {
+        build_clusters(p, tets, inc);
+        return;
+    }
+    // The two cluster plans read the pattern and incidence only and write disjoint fields (cl_*
+    // and tc_*): they are built side by side. An error of the first is reported before one of
+    // the second, as when they ran in turn.
+    std::exception_ptr tet_error;
+    std::thread tet([&] {
+        try {
+            build_tet_clusters(p, tets, inc);
+        } catch (...) {
+            tet_error = std::current_exception();
+        }
+    });
+    try {
+        build_clusters(p, tets, inc);
+    } catch (...) {
+        tet.join();
+        throw;
+    }
+    tet.join();
+    if (tet_error) std::rethrow_exception(tet_error);
 }
 
 void check_clusters(const HostPlan& p, const int32_t* tets) {
